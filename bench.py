@@ -1,0 +1,310 @@
+#!/usr/bin/env python
+"""Benchmark of the classic 2D wave-propagation step (ClawSolver2D.step ->
+step2/flux2) on the B200.
+
+Workload: 2D Euler, Roe 4-wave solver with entropy fix, gamma = 1.4, 1024 x
+1024 cells on [0,1]^2, FP64, extrapolation BCs, MC limiter, unsplit step with
+transverse corrections (trans_cor); four-quadrant Riemann data split at
+x = y = 0.8.  A step is one pass of the hot path: device ghost-cell fill +
+the fused step2 kernel + the grid-wide CFL reduction, with q resident in HBM.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  `value` is device-timed (CUDA events on the
+stream the kernels run on, L2 flushed between steps, max over ranks); `e2e`
+is the same metric through the public patch API with a pinned host -> device
+upload of q and a device -> host download of the result inside every step.
+`--impl reference` times the CPU restatement of the reference's Fortran
+step2 (the oracle; the reference's Fortran cannot be compiled in this image)
+on all host cores.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s on 1 B200 (FP64, % HBM roofline); batched & learned-guess speedup"
+UNIT = "cell-updates/s"
+N = 1024
+MEQN = 4
+BYTES_PER_CELL = 2 * MEQN * 8  # read q^n + write q^{n+1}, FP64
+WORKLOAD = "euler_quadrants_roe_1024x1024_unsplit_trans_cor_mc"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--cpu-sample-s", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def config(extra=None):
+    c = {"workload": WORKLOAD, "mx": N, "my": N, "num_eqn": MEQN, "riemann": "euler_4wave_2D (Roe, efix)",
+         "limiter": "MC", "transverse": "trans_cor", "dimensional_split": False, "bc": "extrap",
+         "l2": "flushed between timed steps (256 MiB write, not timed)"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region (NVML reads only)
+# ---------------------------------------------------------------------------
+class ClockSampler(object):
+    REASONS = {0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap",
+               0x8: "hw_slowdown", 0x10: "sync_boost", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting"}
+
+    def __init__(self, index):
+        self.samples, self.reasons = [], set()
+        self._stop = threading.Event()
+        self.max_mhz = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self._nv = pynvml
+            self._h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self._nv = None
+
+    def _run(self):
+        nv = self._nv
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
+                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+                for b, name in self.REASONS.items():
+                    if bits & b and name != "gpu_idle":
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.02)
+
+    def __enter__(self):
+        if self._nv is not None:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._nv is not None:
+            self._t.join()
+
+    def summary(self):
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None,
+                "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# CPU legs (the oracle): single-thread baseline and the all-core reference arm
+# ---------------------------------------------------------------------------
+def cpu_rate(threads, budget_s, max_steps=None):
+    """cell-updates/s of the oracle's step2 on the benchmark workload."""
+    from oracle import pyoracle
+    from pyclaw_b200 import workloads
+    pyoracle.set_threads(threads)
+    claw = workloads.euler_quadrants_unsplit(pyoracle.make_solver_class(), n=N)
+    s, sol = claw.solver, claw.solution
+    s.setup(sol)
+    s.dt = 2.5e-4
+    s.step_hyperbolic(sol)  # warm-up (also sets dt near CFL 0.9)
+    s.dt = s.dt * 0.9 / max(s.cfl.get_cached_max(), 1e-12)
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        s.step_hyperbolic(sol)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s or (max_steps is not None and steps >= max_steps):
+            break
+    return N * N * steps / el, steps, el
+
+
+def run_reference(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return 0
+    ncores = len(os.sched_getaffinity(0))
+    budget = max(5.0, min(120.0, 0.5 * args.steps))
+    value, steps, el = cpu_rate(ncores, budget, max_steps=args.steps)
+    sample = ("%d full steps of the %dx%d workload (oracle step2 + host ghost fill), OpenMP over row "
+              "colours, %.1f s" % (steps, N, N, el))
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
+            "warmup": 1, "ms_per_step": 1e3 * el / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": config({"reference": "C++ restatement of step2.f90/flux2.f90/limiter.f90/philim.f90 "
+                                           "(oracle/claw_oracle.cpp); the reference Fortran needs gfortran, "
+                                           "absent from this image"}),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": ncores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU leg
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from pyclaw_b200 import _lib, workloads
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+
+    # weak scaling: every rank steps its own copy of the workload (the
+    # single-grid step has no cross-rank exchange unless a domain is split)
+    claw = workloads.euler_quadrants_unsplit(n=N)
+    solver, sol = claw.solver, claw.solution
+    solver.device = local
+    solver.setup(sol)
+    patch = solver._dev
+    patch.set_stream(stream.cuda_stream)
+    patch.set_timing(True)
+
+    # dt for CFL 0.9 from a probe step
+    cfl = patch.step(2.5e-4)
+    patch.accept(False)
+    dt = 2.5e-4 * 0.9 / cfl
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    for _ in range(args.warmup):
+        flush.zero_()
+        patch.step(dt, want_cfl=False)
+        patch.accept(True)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    kern_ms = []
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record(stream)
+            patch.step(dt, want_cfl=False)
+            patch.accept(True)
+            ev[k][1].record(stream)
+            kern_ms.append(patch.kernel_ms())
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = sum(step_ms)
+    patch.sync()  # raises if any step produced a non-finite value
+    last_cfl = patch.cfl()
+
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    cells = N * N
+    value = world * cells * args.steps / (total_ms * 1e-3)
+
+    # roofline of the dominant kernel (the fused step)
+    peaks, peak_src = measured_peaks()
+    kms = statistics.mean(kern_ms)
+    achieved = cells * BYTES_PER_CELL / (kms * 1e-3) / 1e9
+    fp64 = ctypes.c_double(0.0)
+    _lib.check(_lib.load().claw2_probe_fp64(local, ctypes.byref(fp64)))
+
+    # end to end through the public patch API with pinned host buffers
+    e2e = None
+    if args.e2e_steps > 0:
+        qh = torch.empty((N * N * MEQN,), dtype=torch.float64, pin_memory=True).numpy()
+        qh[:] = sol.state.get_q_global().reshape(-1, order="F")
+        qd = torch.empty_like(torch.from_numpy(qh)).pin_memory().numpy()
+        L = _lib.load()
+        h = patch.h
+        cflv = ctypes.c_double(0.0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for k in range(args.e2e_steps):
+            _lib.check(L.claw2_patch_upload_q(h, _lib.dptr(qh)))
+            _lib.check(L.claw2_patch_step(h, ctypes.c_double(dt), ctypes.byref(cflv)))
+            _lib.check(L.claw2_patch_accept(h, 1))
+            _lib.check(L.claw2_patch_download_q(h, _lib.dptr(qd)))
+        el = time.perf_counter() - t0
+        e2e_val = cells * args.e2e_steps / el
+        if world > 1:
+            t = torch.tensor([el], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_val = world * cells * args.e2e_steps / float(t.item())
+        e2e = {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": qh.nbytes,
+               "d2h_bytes_per_step": qd.nbytes + 8, "steps": args.e2e_steps,
+               "path": "claw2_patch_upload_q + claw2_patch_step (returns CFL) + claw2_patch_accept + "
+                       "claw2_patch_download_q, pinned host buffers, wall clock"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, s, el = cpu_rate(1, args.cpu_sample_s)
+        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": "%d full %dx%d steps of the oracle step2 (single thread), %.1f s" % (s, N, N, el)}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "ours",
+                "config": config({"dt": dt, "cfl_last": last_cfl}),
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                             "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                             "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_src,
+                             "kernel": "k_step_unsplit<RPEulerRoe,128>", "kernel_ms": kms,
+                             "algorithmic_bytes_per_launch": cells * BYTES_PER_CELL,
+                             "fp64_probe_tflops": fp64.value,
+                             "fp64_flops_per_cell_est": None},
+                "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
+                "gpu_launches": 2 * args.steps}
+        print(json.dumps(line), flush=True)
+    solver._dev.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

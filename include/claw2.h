@@ -1,0 +1,165 @@
+/*
+ * claw2.h -- C ABI of the B200 (sm_100a) classic Clawpack 2D step.
+ *
+ * Drop-in boundary.  In the reference, ClawSolver2D.step_hyperbolic
+ * (src/pyclaw/classic/solver.py:498-549) calls the f2py-wrapped Fortran
+ * routines step2 (src/pyclaw/classic/step2.f90:2-5) and step2ds
+ * (src/pyclaw/classic/step2ds.f90:2-6), which call the Riemann solvers through
+ * raw Fortran function pointers (classic/solver.py:516-521).  This library
+ * replaces those routines.  Plain C types only; every function returns an
+ * int status (CLAW2_OK = 0) and never aborts; claw2_last_error() describes
+ * the last failure on the calling thread.
+ *
+ * Riemann solvers cannot cross the ABI as host function pointers, so they are
+ * selected by id (CLAW2_RP_*) and their parameters (the reference's COMMON
+ * /cparam/, src/pyclaw/state.py:206-231) are passed as a double array.
+ *
+ * Layouts.  Host arrays use the reference's Fortran order:
+ *   qbc  (num_eqn, mx+2*num_ghost, my+2*num_ghost)   for claw2_step2/_step2ds
+ *   q    (num_eqn, mx, my)                            for the patch upload/download
+ * (src/pyclaw/state.py:330-335, solver.py:343-345).  On the device the library
+ * keeps structure-of-arrays planes with a 2-cell ghost ring and a padded pitch.
+ */
+#ifndef CLAW2_H
+#define CLAW2_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CLAW2_MAX_PARAMS 8
+#define CLAW2_MAX_WAVES 8
+
+/* Riemann solver ids and their cparam layouts. */
+enum {
+    CLAW2_RP_ADVECTION = 1,    /* advection_2D:               {u, v}                 */
+    CLAW2_RP_ACOUSTICS = 2,    /* acoustics_2D:               {rho, bulk, cc, zz}    */
+    CLAW2_RP_EULER_ROE = 3,    /* euler_4wave_2D:             {gamma, efix}          */
+    CLAW2_RP_SHALLOW_ROE = 4,  /* shallow_roe_with_efix_2D:   {grav, efix}           */
+    CLAW2_RP_EULER_EXACT = 5   /* exact Euler (no reference counterpart): {gamma, tol, guess} */
+};
+
+/* Boundary-condition codes: pyclaw.BC (src/pyclaw/solver.py:13-19). */
+enum { CLAW2_BC_CUSTOM = 0, CLAW2_BC_EXTRAP = 1, CLAW2_BC_PERIODIC = 2, CLAW2_BC_WALL = 3 };
+
+/* Status codes. */
+enum {
+    CLAW2_OK = 0,
+    CLAW2_EINVAL = 1,      /* bad argument (sizes, ids, null pointers)           */
+    CLAW2_ECUDA = 2,       /* a CUDA runtime call failed                         */
+    CLAW2_ENONFINITE = 3,  /* the step produced a non-finite value               */
+    CLAW2_ETIMEOUT = 4,    /* a bounded device-side wait gave up                 */
+    CLAW2_ENOMEM = 5,      /* device allocation failed                           */
+    CLAW2_EUNSUPPORTED = 6 /* valid request this build does not implement        */
+};
+
+/* Patch description: the state of one ClawSolver2D after setup()
+ * (classic/solver.py:195-234, solver.py:158-242). */
+typedef struct claw2_desc {
+    int mx, my;               /* interior cells                                        */
+    int num_eqn, num_waves;   /* must match the Riemann solver                         */
+    int num_aux;              /* 0 (aux-carrying solvers are not in this build)        */
+    int num_ghost;            /* must be 2                                              */
+    int riemann;              /* CLAW2_RP_*                                             */
+    int order;                /* method(2): 1 or 2                                      */
+    int transverse;           /* method(3): 0, 1, 2 (unsplit)                           */
+    int dimensional_split;    /* 1: step2ds x then y (method(3) = -1)                   */
+    int fwave;                /* use_fwave                                              */
+    int mthlim[CLAW2_MAX_WAVES];
+    int bc_lower[2], bc_upper[2];
+    double dx, dy;
+    double cparam[CLAW2_MAX_PARAMS];
+    int ncparam;
+    int device;               /* CUDA device ordinal                                    */
+} claw2_desc;
+
+typedef struct claw2_patch claw2_patch;
+
+/* ---- stateless drop-ins for the f2py routines (host buffers) ------------- */
+
+/* Replaces step2 (src/pyclaw/classic/step2.f90:2-5; called at
+ * classic/solver.py:539-541).  qold/qnew: qbc layout, ghost cells already
+ * filled; qnew must equal qold on entry.  method[7] and mthlim[num_waves] as
+ * built by classic/solver.py:162-193.  On return the interior cells of qnew
+ * hold the updated solution and *cfl the Courant number over the same
+ * interfaces as the reference (flux2.f90:111-119 over step2.f90:92,172
+ * slices).  Ghost cells of qnew are left as they were on entry (the next BC
+ * fill overwrites them; the reference's partial ghost updates are never read). */
+int claw2_step2(int maxm, int num_eqn, int num_waves, int num_aux, int num_ghost,
+                int mx, int my, const double* qold, double* qnew, const double* aux,
+                double dx, double dy, double dt, const int* method, const int* mthlim,
+                double* cfl, int use_fwave, int riemann, const double* cparam,
+                int ncparam);
+
+/* Replaces step2ds (src/pyclaw/classic/step2ds.f90:2-6; called twice at
+ * classic/solver.py:527-535).  ids = 1: x-sweep over every row including the
+ * ghost rows; ids = 2: y-sweep.  qold may alias qnew. */
+int claw2_step2ds(int maxm, int num_eqn, int num_waves, int num_aux, int num_ghost,
+                  int mx, int my, const double* qold, double* qnew, const double* aux,
+                  double dx, double dy, double dt, const int* method, const int* mthlim,
+                  double* cfl, int ids, int use_fwave, int riemann,
+                  const double* cparam, int ncparam);
+
+/* Replaces Solver._apply_bcs for q (src/pyclaw/solver.py:351-519) on a host
+ * qbc array: extrap / periodic / wall, dimension 0 then 1. */
+int claw2_bc_fill(int num_eqn, int num_ghost, int mx, int my, double* qbc,
+                  const int* bc_lower, const int* bc_upper);
+
+/* ---- device-resident patch (the fast path) ------------------------------- */
+
+/* Allocates the device state (two q buffers, CFL and status words) for one
+ * ClawSolver2D (replaces ClawSolver2D._allocate_workspace and
+ * Solver._allocate_bc_arrays, classic/solver.py:466-494, solver.py:321-349). */
+int claw2_patch_create(const claw2_desc* desc, claw2_patch** out);
+int claw2_patch_destroy(claw2_patch* p);
+
+/* Replaces state.set_cparam (state.py:206-231). */
+int claw2_patch_set_cparam(claw2_patch* p, const double* cparam, int ncparam);
+
+/* Host <-> device copies of State.q, shape (num_eqn, mx, my), Fortran order. */
+int claw2_patch_upload_q(claw2_patch* p, const double* q);
+int claw2_patch_download_q(claw2_patch* p, double* q);
+
+/* One hyperbolic step from the current q: ghost fill on the device, then the
+ * unsplit (or split) step into the pending buffer.  If cfl is non-NULL the
+ * call waits and returns the Courant number; with NULL it only enqueues. */
+int claw2_patch_step(claw2_patch* p, double dt, double* cfl);
+
+/* Accept (1) or reject (0) the pending step (solver.py:619-651): accept makes
+ * it the current q; reject keeps the old q.  No copy either way. */
+int claw2_patch_accept(claw2_patch* p, int accept);
+
+/* Courant number of the last step (waits for it). */
+int claw2_patch_cfl(claw2_patch* p, double* cfl);
+
+/* Waits for the patch's stream and reports device-side error flags. */
+int claw2_patch_sync(claw2_patch* p);
+
+/* Raw device pointer of the current q planes and the layout, for callers that
+ * share the device buffers (layout[0..3] = mx+4, my+4, pitch, plane). */
+int claw2_patch_device_q(claw2_patch* p, double** q, long long* layout);
+
+/* Run the patch's work on a caller-owned CUDA stream (a cudaStream_t passed
+ * as void*); NULL returns to the patch's own stream. */
+int claw2_patch_set_stream(claw2_patch* p, void* stream);
+
+/* Kernel timing with CUDA events recorded on the patch's stream around the
+ * step kernel(s) of each claw2_patch_step (ghost fill excluded).  After a
+ * step, claw2_patch_kernel_ms waits for it and returns the elapsed time. */
+int claw2_patch_set_timing(claw2_patch* p, int on);
+int claw2_patch_kernel_ms(claw2_patch* p, float* ms);
+
+/* FP64 FMA throughput of the current device, TFLOP/s (2 flops per FMA): a
+ * roofline denominator for the FP64-bound Riemann solvers. */
+int claw2_probe_fp64(int device, double* tflops);
+
+/* Description of the last error on this thread (never NULL). */
+const char* claw2_last_error(void);
+
+/* Library version string. */
+const char* claw2_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,902 @@
+// claw_oracle.cpp -- CPU oracle (test infrastructure only; see claw_oracle.h).
+//
+// A restatement, in the reference's loop and operation order, of the classic
+// Clawpack 2D kernels.  Index helpers below use the Fortran index ranges of the
+// reference so each loop reads like the file:line it cites.  Component indices
+// m and wave indices mw are 0-based; cell/interface indices i, j keep the
+// Fortran ranges (1-mbc .. mx+mbc).
+#include "claw_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+int g_threads = 1;
+
+// ---------------------------------------------------------------------------
+// Slice views with Fortran index ranges.
+// ---------------------------------------------------------------------------
+struct Slice {  // (meqn, 1-mbc:maxm+mbc)
+    double* p; int meqn, mbc;
+    double& operator()(int m, int i) const { return p[(size_t)(i + mbc - 1) * meqn + m]; }
+};
+struct CSlice {
+    const double* p; int meqn, mbc;
+    double operator()(int m, int i) const { return p[(size_t)(i + mbc - 1) * meqn + m]; }
+};
+struct Waves {  // (meqn, mwaves, 1-mbc:maxm+mbc)
+    double* p; int meqn, mwaves, mbc;
+    double& operator()(int m, int mw, int i) const {
+        return p[((size_t)(i + mbc - 1) * mwaves + mw) * meqn + m];
+    }
+};
+struct Speeds {  // (mwaves, 1-mbc:maxm+mbc)
+    double* p; int mwaves, mbc;
+    double& operator()(int mw, int i) const { return p[(size_t)(i + mbc - 1) * mwaves + mw]; }
+};
+struct Gadd {  // (meqn, 2, 1-mbc:maxm+mbc); k = 0 (below) or 1 (above)
+    double* p; int meqn, mbc;
+    double& operator()(int m, int k, int i) const {
+        return p[((size_t)(i + mbc - 1) * 2 + k) * meqn + m];
+    }
+};
+struct Grid2 {  // (meqn, 1-mbc:mx+mbc, 1-mbc:my+mbc), Fortran order
+    double* p; int meqn, mbc, mx;
+    double& operator()(int m, int i, int j) const {
+        return p[((size_t)(j + mbc - 1) * (mx + 2 * mbc) + (i + mbc - 1)) * meqn + m];
+    }
+};
+
+// ---------------------------------------------------------------------------
+// philim.f90:16-35
+// ---------------------------------------------------------------------------
+double philim(double a, double b, int meth) {
+    double r = b / a;
+    switch (meth) {
+        case 1: return std::max(0.0, std::min(1.0, r));                                   // minmod
+        case 2: return std::max(0.0, std::max(std::min(1.0, 2.0 * r), std::min(2.0, r)));  // superbee
+        case 3: return (r + std::fabs(r)) / (1.0 + std::fabs(r));                          // van Leer
+        case 4: {                                                                          // MC
+            double c = (1.0 + r) / 2.0;
+            return std::max(0.0, std::min(c, std::min(2.0, 2.0 * r)));
+        }
+        case 5: return r;                                                                  // Beam-Warming
+        default: return 0.0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// limiter.f90:29-53
+// ---------------------------------------------------------------------------
+void limiter(int mx, int meqn, int mwaves, const Waves& wave, const Speeds& s,
+             const int* mthlim) {
+    for (int mw = 0; mw < mwaves; ++mw) {
+        if (mthlim[mw] == 0) continue;
+        double dotr = 0.0;
+        for (int i = 0; i <= mx + 1; ++i) {
+            double wnorm2 = 0.0;
+            double dotl = dotr;
+            dotr = 0.0;
+            for (int m = 0; m < meqn; ++m) {
+                wnorm2 = wnorm2 + wave(m, mw, i) * wave(m, mw, i);
+                dotr = dotr + wave(m, mw, i) * wave(m, mw, i + 1);
+            }
+            if (i == 0) continue;
+            if (wnorm2 == 0.0) continue;
+            double wlimitr;
+            if (s(mw, i) > 0.0)
+                wlimitr = philim(wnorm2, dotl, mthlim[mw]);
+            else
+                wlimitr = philim(wnorm2, dotr, mthlim[mw]);
+            for (int m = 0; m < meqn; ++m) wave(m, mw, i) = wlimitr * wave(m, mw, i);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Riemann solvers (external clawpack/riemann package; restated from the
+// mathematics, Fortran slice ABI: interface i has left state qr(:,i-1) and
+// right state ql(:,i); flux2 passes ql = qr = q1d).
+// ---------------------------------------------------------------------------
+
+// advection_2D: q_t + u q_x + v q_y = 0 (LeVeque 2002, sec. 20.5).
+void rpn2_advection(int ixy, int mbc, int mx, int meqn, int mwaves, const CSlice& ql,
+                    const CSlice& qr, const Waves& wave, const Speeds& s, const Slice& amdq,
+                    const Slice& apdq, const double* cp) {
+    const double vel = (ixy == 1) ? cp[0] : cp[1];
+    (void)meqn; (void)mwaves;
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        wave(0, 0, i) = ql(0, i) - qr(0, i - 1);
+        s(0, i) = vel;
+        amdq(0, i) = std::min(s(0, i), 0.0) * wave(0, 0, i);
+        apdq(0, i) = std::max(s(0, i), 0.0) * wave(0, 0, i);
+    }
+}
+void rpt2_advection(int ixy, int mbc, int mx, const Slice& asdq, const Slice& bmasdq,
+                    const Slice& bpasdq, const double* cp) {
+    const double stran = (ixy == 1) ? cp[1] : cp[0];
+    const double stranm = std::min(stran, 0.0), stranp = std::max(stran, 0.0);
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        bmasdq(0, i) = stranm * asdq(0, i);
+        bpasdq(0, i) = stranp * asdq(0, i);
+    }
+}
+
+// acoustics_2D: p_t + K(u_x+v_y) = 0, rho u_t + p_x = 0, rho v_t + p_y = 0.
+// Eigenvectors (-Z,1,0) with speed -c and (Z,1,0) with speed c in the normal
+// direction (LeVeque 2002, sec. 18.2, 21.7).  cparam = rho, bulk, cc, zz.
+void rpn2_acoustics(int ixy, int mbc, int mx, const CSlice& ql, const CSlice& qr,
+                    const Waves& wave, const Speeds& s, const Slice& amdq, const Slice& apdq,
+                    const double* cp, int meqn) {
+    const double cc = cp[2], zz = cp[3];
+    const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        double delta1 = ql(0, i) - qr(0, i - 1);
+        double delta2 = ql(mu, i) - qr(mu, i - 1);
+        double a1 = (-delta1 + zz * delta2) / (2.0 * zz);
+        double a2 = (delta1 + zz * delta2) / (2.0 * zz);
+        wave(0, 0, i) = -a1 * zz;
+        wave(mu, 0, i) = a1;
+        wave(mv, 0, i) = 0.0;
+        s(0, i) = -cc;
+        wave(0, 1, i) = a2 * zz;
+        wave(mu, 1, i) = a2;
+        wave(mv, 1, i) = 0.0;
+        s(1, i) = cc;
+    }
+    for (int m = 0; m < meqn; ++m)
+        for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+            amdq(m, i) = s(0, i) * wave(m, 0, i);
+            apdq(m, i) = s(1, i) * wave(m, 1, i);
+        }
+}
+void rpt2_acoustics(int ixy, int mbc, int mx, const Slice& asdq, const Slice& bmasdq,
+                    const Slice& bpasdq, const double* cp) {
+    const double cc = cp[2], zz = cp[3];
+    const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        double a1 = (-asdq(0, i) + zz * asdq(mv, i)) / (2.0 * zz);
+        double a2 = (asdq(0, i) + zz * asdq(mv, i)) / (2.0 * zz);
+        bmasdq(0, i) = cc * a1 * zz;
+        bmasdq(mu, i) = 0.0;
+        bmasdq(mv, i) = -cc * a1;
+        bpasdq(0, i) = cc * a2 * zz;
+        bpasdq(mu, i) = 0.0;
+        bpasdq(mv, i) = cc * a2;
+    }
+}
+
+// Euler equations, Roe solver with 4 waves (u-c, entropy, shear, u+c) and an
+// optional Harten-Hyman entropy fix (LeVeque 2002, sec. 15.3.5 and 18.8;
+// Roe 1981).  The wave layout follows the reference's vendored 5-wave solver
+// development/rp_approaches/rpn2_euler_5wave.f:87-298 minus the tracer wave.
+// cparam = gamma, efix.
+void rpn2_euler_roe(int ixy, int mbc, int mx, int meqn, int mwaves, const CSlice& ql,
+                    const CSlice& qr, const Waves& wave, const Speeds& s, const Slice& amdq,
+                    const Slice& apdq, const double* cp) {
+    const double gamma = cp[0];
+    const bool efix = cp[1] != 0.0;
+    const double gamma1 = gamma - 1.0;
+    const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        double rhsqrtl = std::sqrt(qr(0, i - 1));
+        double rhsqrtr = std::sqrt(ql(0, i));
+        double pl = gamma1 * (qr(3, i - 1) - 0.5 * (qr(1, i - 1) * qr(1, i - 1) +
+                                                    qr(2, i - 1) * qr(2, i - 1)) / qr(0, i - 1));
+        double pr = gamma1 * (ql(3, i) - 0.5 * (ql(1, i) * ql(1, i) + ql(2, i) * ql(2, i)) / ql(0, i));
+        double rhsq2 = rhsqrtl + rhsqrtr;
+        double u = (qr(mu, i - 1) / rhsqrtl + ql(mu, i) / rhsqrtr) / rhsq2;
+        double v = (qr(mv, i - 1) / rhsqrtl + ql(mv, i) / rhsqrtr) / rhsq2;
+        double enth = (((qr(3, i - 1) + pl) / rhsqrtl + (ql(3, i) + pr) / rhsqrtr)) / rhsq2;
+        double u2v2 = u * u + v * v;
+        double a2 = gamma1 * (enth - 0.5 * u2v2);
+        double a = std::sqrt(a2);
+        double g1a2 = gamma1 / a2;
+        double euv = enth - u2v2;
+
+        double delta0 = ql(0, i) - qr(0, i - 1);
+        double delta1 = ql(mu, i) - qr(mu, i - 1);
+        double delta2 = ql(mv, i) - qr(mv, i - 1);
+        double delta3 = ql(3, i) - qr(3, i - 1);
+        double b3 = g1a2 * (euv * delta0 + u * delta1 + v * delta2 - delta3);
+        double b2 = delta2 - v * delta0;
+        double b4 = (delta1 + (a - u) * delta0 - a * b3) / (2.0 * a);
+        double b1 = delta0 - b3 - b4;
+
+        wave(0, 0, i) = b1;
+        wave(mu, 0, i) = b1 * (u - a);
+        wave(mv, 0, i) = b1 * v;
+        wave(3, 0, i) = b1 * (enth - u * a);
+        s(0, i) = u - a;
+
+        wave(0, 1, i) = b3;
+        wave(mu, 1, i) = b3 * u;
+        wave(mv, 1, i) = b3 * v;
+        wave(3, 1, i) = b3 * 0.5 * u2v2;
+        s(1, i) = u;
+
+        wave(0, 2, i) = 0.0;
+        wave(mu, 2, i) = 0.0;
+        wave(mv, 2, i) = b2;
+        wave(3, 2, i) = b2 * v;
+        s(2, i) = u;
+
+        wave(0, 3, i) = b4;
+        wave(mu, 3, i) = b4 * (u + a);
+        wave(mv, 3, i) = b4 * v;
+        wave(3, 3, i) = b4 * (enth + u * a);
+        s(3, i) = u + a;
+    }
+
+    if (!efix) {
+        for (int m = 0; m < meqn; ++m)
+            for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+                amdq(m, i) = 0.0;
+                apdq(m, i) = 0.0;
+                for (int mw = 0; mw < mwaves; ++mw) {
+                    if (s(mw, i) < 0.0)
+                        amdq(m, i) = amdq(m, i) + s(mw, i) * wave(m, mw, i);
+                    else
+                        apdq(m, i) = apdq(m, i) + s(mw, i) * wave(m, mw, i);
+                }
+            }
+        return;
+    }
+
+    // Harten-Hyman entropy fix: split a transonic rarefaction's flux
+    // difference using the characteristic speeds on either side of it.
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        // 1-wave (u - c)
+        double rhoim1 = qr(0, i - 1);
+        double pim1 = gamma1 * (qr(3, i - 1) - 0.5 * (qr(mu, i - 1) * qr(mu, i - 1) +
+                                                      qr(mv, i - 1) * qr(mv, i - 1)) / rhoim1);
+        double cim1 = std::sqrt(gamma * pim1 / rhoim1);
+        double s0 = qr(mu, i - 1) / rhoim1 - cim1;
+        if (s0 >= 0.0 && s(0, i) > 0.0) {
+            for (int m = 0; m < meqn; ++m) amdq(m, i) = 0.0;
+            goto done;
+        }
+        {
+            double rho1 = qr(0, i - 1) + wave(0, 0, i);
+            double rhou1 = qr(mu, i - 1) + wave(mu, 0, i);
+            double rhov1 = qr(mv, i - 1) + wave(mv, 0, i);
+            double en1 = qr(3, i - 1) + wave(3, 0, i);
+            double p1 = gamma1 * (en1 - 0.5 * (rhou1 * rhou1 + rhov1 * rhov1) / rho1);
+            double c1 = std::sqrt(gamma * p1 / rho1);
+            double s1 = rhou1 / rho1 - c1;
+            double sfract;
+            if (s0 < 0.0 && s1 > 0.0)
+                sfract = s0 * (s1 - s(0, i)) / (s1 - s0);
+            else if (s(0, i) < 0.0)
+                sfract = s(0, i);
+            else
+                sfract = 0.0;
+            for (int m = 0; m < meqn; ++m) amdq(m, i) = sfract * wave(m, 0, i);
+        }
+        // 2- and 3-waves (speed u)
+        if (s(1, i) >= 0.0) goto done;
+        for (int m = 0; m < meqn; ++m)
+            amdq(m, i) = amdq(m, i) + s(1, i) * wave(m, 1, i) + s(2, i) * wave(m, 2, i);
+        {
+            // 4-wave (u + c)
+            double rhoi = ql(0, i);
+            double pi = gamma1 * (ql(3, i) - 0.5 * (ql(mu, i) * ql(mu, i) + ql(mv, i) * ql(mv, i)) / rhoi);
+            double ci = std::sqrt(gamma * pi / rhoi);
+            double s3 = ql(mu, i) / rhoi + ci;
+            double rho2 = ql(0, i) - wave(0, 3, i);
+            double rhou2 = ql(mu, i) - wave(mu, 3, i);
+            double rhov2 = ql(mv, i) - wave(mv, 3, i);
+            double en2 = ql(3, i) - wave(3, 3, i);
+            double p2 = gamma1 * (en2 - 0.5 * (rhou2 * rhou2 + rhov2 * rhov2) / rho2);
+            double c2 = std::sqrt(gamma * p2 / rho2);
+            double s2 = rhou2 / rho2 + c2;
+            double sfract;
+            if (s2 < 0.0 && s3 > 0.0)
+                sfract = s2 * (s3 - s(3, i)) / (s3 - s2);
+            else if (s(3, i) < 0.0)
+                sfract = s(3, i);
+            else
+                goto done;
+            for (int m = 0; m < meqn; ++m) amdq(m, i) = amdq(m, i) + sfract * wave(m, 3, i);
+        }
+    done:;
+    }
+    for (int m = 0; m < meqn; ++m)
+        for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+            double df = 0.0;
+            for (int mw = 0; mw < mwaves; ++mw) df = df + s(mw, i) * wave(m, mw, i);
+            apdq(m, i) = df - amdq(m, i);
+        }
+}
+
+// Transverse Roe split for Euler: decompose asdq on the eigenvectors of the
+// transverse Jacobian at the same Roe-averaged state and keep the down- and
+// up-going parts (LeVeque 2002, sec. 21.6; reference structure
+// development/rp_approaches/rpt2_euler_5wave.f:47-95 minus the tracer).
+void rpt2_euler_roe(int ixy, int mbc, int mx, int meqn, int mwaves, const CSlice& ql,
+                    const CSlice& qr, const Slice& asdq, const Slice& bmasdq,
+                    const Slice& bpasdq, const double* cp) {
+    const double gamma = cp[0];
+    const double gamma1 = gamma - 1.0;
+    const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
+    double waveb[4][4], sb[4];
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        double rhsqrtl = std::sqrt(qr(0, i - 1));
+        double rhsqrtr = std::sqrt(ql(0, i));
+        double pl = gamma1 * (qr(3, i - 1) - 0.5 * (qr(1, i - 1) * qr(1, i - 1) +
+                                                    qr(2, i - 1) * qr(2, i - 1)) / qr(0, i - 1));
+        double pr = gamma1 * (ql(3, i) - 0.5 * (ql(1, i) * ql(1, i) + ql(2, i) * ql(2, i)) / ql(0, i));
+        double rhsq2 = rhsqrtl + rhsqrtr;
+        double u = (qr(mu, i - 1) / rhsqrtl + ql(mu, i) / rhsqrtr) / rhsq2;
+        double v = (qr(mv, i - 1) / rhsqrtl + ql(mv, i) / rhsqrtr) / rhsq2;
+        double enth = (((qr(3, i - 1) + pl) / rhsqrtl + (ql(3, i) + pr) / rhsqrtr)) / rhsq2;
+        double u2v2 = u * u + v * v;
+        double a2 = gamma1 * (enth - 0.5 * u2v2);
+        double a = std::sqrt(a2);
+        double g1a2 = gamma1 / a2;
+        double euv = enth - u2v2;
+
+        double b3 = g1a2 * (euv * asdq(0, i) + u * asdq(mu, i) + v * asdq(mv, i) - asdq(3, i));
+        double b2 = asdq(mu, i) - u * asdq(0, i);
+        double b4 = (asdq(mv, i) + (a - v) * asdq(0, i) - a * b3) / (2.0 * a);
+        double b1 = asdq(0, i) - b3 - b4;
+
+        waveb[0][0] = b1; waveb[0][mu] = b1 * u; waveb[0][mv] = b1 * (v - a);
+        waveb[0][3] = b1 * (enth - v * a); sb[0] = v - a;
+        waveb[1][0] = b3; waveb[1][mu] = b3 * u; waveb[1][mv] = b3 * v;
+        waveb[1][3] = b3 * 0.5 * u2v2; sb[1] = v;
+        waveb[2][0] = 0.0; waveb[2][mu] = b2; waveb[2][mv] = 0.0;
+        waveb[2][3] = b2 * u; sb[2] = v;
+        waveb[3][0] = b4; waveb[3][mu] = b4 * u; waveb[3][mv] = b4 * (v + a);
+        waveb[3][3] = b4 * (enth + v * a); sb[3] = v + a;
+
+        for (int m = 0; m < meqn; ++m) {
+            bmasdq(m, i) = 0.0;
+            bpasdq(m, i) = 0.0;
+            for (int mw = 0; mw < mwaves; ++mw) {
+                bmasdq(m, i) = bmasdq(m, i) + std::min(sb[mw], 0.0) * waveb[mw][m];
+                bpasdq(m, i) = bpasdq(m, i) + std::max(sb[mw], 0.0) * waveb[mw][m];
+            }
+        }
+    }
+}
+
+// Shallow water equations, Roe solver with Harten-Hyman entropy fix
+// (LeVeque 2002, sec. 15.3 and 21.6).  cparam = grav, efix.
+void rpn2_shallow_roe(int ixy, int mbc, int mx, int meqn, int mwaves, const CSlice& ql,
+                      const CSlice& qr, const Waves& wave, const Speeds& s, const Slice& amdq,
+                      const Slice& apdq, const double* cp) {
+    const double grav = cp[0];
+    const bool efix = cp[1] != 0.0;
+    const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        double h = (qr(0, i - 1) + ql(0, i)) * 0.50;
+        double hsqrtl = std::sqrt(qr(0, i - 1));
+        double hsqrtr = std::sqrt(ql(0, i));
+        double hsq2 = hsqrtl + hsqrtr;
+        double u = (qr(mu, i - 1) / hsqrtl + ql(mu, i) / hsqrtr) / hsq2;
+        double v = (qr(mv, i - 1) / hsqrtl + ql(mv, i) / hsqrtr) / hsq2;
+        double a = std::sqrt(grav * h);
+
+        double delta0 = ql(0, i) - qr(0, i - 1);
+        double delta1 = ql(mu, i) - qr(mu, i - 1);
+        double delta2 = ql(mv, i) - qr(mv, i - 1);
+        double a1 = ((u + a) * delta0 - delta1) * (0.50 / a);
+        double a2 = -v * delta0 + delta2;
+        double a3 = (-(u - a) * delta0 + delta1) * (0.50 / a);
+
+        wave(0, 0, i) = a1;
+        wave(mu, 0, i) = a1 * (u - a);
+        wave(mv, 0, i) = a1 * v;
+        s(0, i) = u - a;
+        wave(0, 1, i) = 0.0;
+        wave(mu, 1, i) = 0.0;
+        wave(mv, 1, i) = a2;
+        s(1, i) = u;
+        wave(0, 2, i) = a3;
+        wave(mu, 2, i) = a3 * (u + a);
+        wave(mv, 2, i) = a3 * v;
+        s(2, i) = u + a;
+    }
+
+    if (!efix) {
+        for (int m = 0; m < meqn; ++m)
+            for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+                amdq(m, i) = 0.0;
+                apdq(m, i) = 0.0;
+                for (int mw = 0; mw < mwaves; ++mw) {
+                    if (s(mw, i) < 0.0)
+                        amdq(m, i) = amdq(m, i) + s(mw, i) * wave(m, mw, i);
+                    else
+                        apdq(m, i) = apdq(m, i) + s(mw, i) * wave(m, mw, i);
+                }
+            }
+        return;
+    }
+
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        // 1-wave
+        double him1 = qr(0, i - 1);
+        double s0 = qr(mu, i - 1) / him1 - std::sqrt(grav * him1);
+        if (s0 >= 0.0 && s(0, i) > 0.0) {
+            for (int m = 0; m < meqn; ++m) amdq(m, i) = 0.0;
+            continue;
+        }
+        {
+            double h1 = qr(0, i - 1) + wave(0, 0, i);
+            double hu1 = qr(mu, i - 1) + wave(mu, 0, i);
+            double s1 = hu1 / h1 - std::sqrt(grav * h1);
+            double sfract;
+            if (s0 < 0.0 && s1 > 0.0)
+                sfract = s0 * ((s1 - s(0, i)) / (s1 - s0));
+            else if (s(0, i) < 0.0)
+                sfract = s(0, i);
+            else
+                sfract = 0.0;
+            for (int m = 0; m < meqn; ++m) amdq(m, i) = sfract * wave(m, 0, i);
+        }
+        // 2-wave
+        if (s(1, i) > 0.0) continue;
+        for (int m = 0; m < meqn; ++m) amdq(m, i) = amdq(m, i) + s(1, i) * wave(m, 1, i);
+        {
+            // 3-wave
+            double hi = ql(0, i);
+            double s03 = ql(mu, i) / hi + std::sqrt(grav * hi);
+            double h3 = ql(0, i) - wave(0, 2, i);
+            double hu3 = ql(mu, i) - wave(mu, 2, i);
+            double s3 = hu3 / h3 + std::sqrt(grav * h3);
+            double sfract;
+            if (s3 < 0.0 && s03 > 0.0)
+                sfract = s3 * ((s03 - s(2, i)) / (s03 - s3));
+            else if (s(2, i) < 0.0)
+                sfract = s(2, i);
+            else
+                continue;
+            for (int m = 0; m < meqn; ++m) amdq(m, i) = amdq(m, i) + sfract * wave(m, 2, i);
+        }
+    }
+    for (int m = 0; m < meqn; ++m)
+        for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+            double df = 0.0;
+            for (int mw = 0; mw < mwaves; ++mw) df = df + s(mw, i) * wave(m, mw, i);
+            apdq(m, i) = df - amdq(m, i);
+        }
+}
+
+void rpt2_shallow_roe(int ixy, int mbc, int mx, int meqn, int mwaves, const CSlice& ql,
+                      const CSlice& qr, const Slice& asdq, const Slice& bmasdq,
+                      const Slice& bpasdq, const double* cp) {
+    const double grav = cp[0];
+    const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
+    double waveb[3][3], sb[3];
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        double hsqrtl = std::sqrt(qr(0, i - 1));
+        double hsqrtr = std::sqrt(ql(0, i));
+        double hsq2 = hsqrtl + hsqrtr;
+        double ubar = (qr(mu, i - 1) / hsqrtl + ql(mu, i) / hsqrtr) / hsq2;
+        double vbar = (qr(mv, i - 1) / hsqrtl + ql(mv, i) / hsqrtr) / hsq2;
+        double cbar = std::sqrt(0.5 * grav * (qr(0, i - 1) + ql(0, i)));
+
+        double a1 = (0.5 / cbar) * ((vbar + cbar) * asdq(0, i) - asdq(mv, i));
+        double a2 = -ubar * asdq(0, i) + asdq(mu, i);
+        double a3 = (0.5 / cbar) * (-(vbar - cbar) * asdq(0, i) + asdq(mv, i));
+
+        waveb[0][0] = a1; waveb[0][mu] = a1 * ubar; waveb[0][mv] = a1 * (vbar - cbar);
+        sb[0] = vbar - cbar;
+        waveb[1][0] = 0.0; waveb[1][mu] = a2; waveb[1][mv] = 0.0;
+        sb[1] = vbar;
+        waveb[2][0] = a3; waveb[2][mu] = a3 * ubar; waveb[2][mv] = a3 * (vbar + cbar);
+        sb[2] = vbar + cbar;
+
+        for (int m = 0; m < meqn; ++m) {
+            bmasdq(m, i) = 0.0;
+            bpasdq(m, i) = 0.0;
+            for (int mw = 0; mw < mwaves; ++mw) {
+                bmasdq(m, i) = bmasdq(m, i) + std::min(sb[mw], 0.0) * waveb[mw][m];
+                bpasdq(m, i) = bpasdq(m, i) + std::max(sb[mw], 0.0) * waveb[mw][m];
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Dispatch
+// ---------------------------------------------------------------------------
+bool rp_known(int rp) {
+    return rp == ORC_RP_ADVECTION || rp == ORC_RP_ACOUSTICS || rp == ORC_RP_EULER_ROE ||
+           rp == ORC_RP_SHALLOW_ROE;
+}
+
+void call_rpn2(int rp, int ixy, int mbc, int mx, int meqn, int mwaves, const CSlice& q,
+               const Waves& wave, const Speeds& s, const Slice& amdq, const Slice& apdq,
+               const double* cp) {
+    switch (rp) {
+        case ORC_RP_ADVECTION: rpn2_advection(ixy, mbc, mx, meqn, mwaves, q, q, wave, s, amdq, apdq, cp); break;
+        case ORC_RP_ACOUSTICS: rpn2_acoustics(ixy, mbc, mx, q, q, wave, s, amdq, apdq, cp, meqn); break;
+        case ORC_RP_EULER_ROE: rpn2_euler_roe(ixy, mbc, mx, meqn, mwaves, q, q, wave, s, amdq, apdq, cp); break;
+        case ORC_RP_SHALLOW_ROE: rpn2_shallow_roe(ixy, mbc, mx, meqn, mwaves, q, q, wave, s, amdq, apdq, cp); break;
+    }
+}
+void call_rpt2(int rp, int ixy, int mbc, int mx, int meqn, int mwaves, const CSlice& q,
+               const Slice& asdq, const Slice& bm, const Slice& bp, const double* cp) {
+    switch (rp) {
+        case ORC_RP_ADVECTION: rpt2_advection(ixy, mbc, mx, asdq, bm, bp, cp); break;
+        case ORC_RP_ACOUSTICS: rpt2_acoustics(ixy, mbc, mx, asdq, bm, bp, cp); break;
+        case ORC_RP_EULER_ROE: rpt2_euler_roe(ixy, mbc, mx, meqn, mwaves, q, q, asdq, bm, bp, cp); break;
+        case ORC_RP_SHALLOW_ROE: rpt2_shallow_roe(ixy, mbc, mx, meqn, mwaves, q, q, asdq, bm, bp, cp); break;
+    }
+}
+
+// Per-slice scratch (the reference's `work` partition, step2.f90:53-71, plus
+// the optional q1d/qadd/fadd/gadd/dtdx1d arrays).
+struct Work {
+    int n;  // maxm + 2*mbc
+    std::vector<double> q1d, qadd, fadd, gadd, dtdx1d, dtdy1d, wave, s, amdq, apdq, cqxx,
+        bmasdq, bpasdq;
+    Work(int maxm, int mbc, int meqn, int mwaves) {
+        n = maxm + 2 * mbc;
+        q1d.assign((size_t)n * meqn, 0.0);
+        qadd.assign((size_t)n * meqn, 0.0);
+        fadd.assign((size_t)n * meqn, 0.0);
+        gadd.assign((size_t)n * meqn * 2, 0.0);
+        dtdx1d.assign(n, 0.0);
+        dtdy1d.assign(n, 0.0);
+        wave.assign((size_t)n * meqn * mwaves, 0.0);
+        s.assign((size_t)n * mwaves, 0.0);
+        amdq.assign((size_t)n * meqn, 0.0);
+        apdq.assign((size_t)n * meqn, 0.0);
+        cqxx.assign((size_t)n * meqn, 0.0);
+        bmasdq.assign((size_t)n * meqn, 0.0);
+        bpasdq.assign((size_t)n * meqn, 0.0);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// flux2.f90:82-204.  dtdx1d has the Fortran range 1-mbc:maxm+mbc.
+// ---------------------------------------------------------------------------
+void flux2(int ixy, int mbc, int mx, int meqn, int mwaves, Work& w, const int* method,
+           const int* mthlim, double* cfl1d, bool use_fwave, int rp, const double* cp) {
+    Slice q1d{w.q1d.data(), meqn, mbc};
+    Slice qadd{w.qadd.data(), meqn, mbc};
+    Slice fadd{w.fadd.data(), meqn, mbc};
+    Gadd gadd{w.gadd.data(), meqn, mbc};
+    Slice amdq{w.amdq.data(), meqn, mbc}, apdq{w.apdq.data(), meqn, mbc};
+    Slice cqxx{w.cqxx.data(), meqn, mbc};
+    Slice bmasdq{w.bmasdq.data(), meqn, mbc}, bpasdq{w.bpasdq.data(), meqn, mbc};
+    Waves wave{w.wave.data(), meqn, mwaves, mbc};
+    Speeds s{w.s.data(), mwaves, mbc};
+    auto dtdx1d = [&](int i) -> double& { return w.dtdx1d[(size_t)(i + mbc - 1)]; };
+    CSlice q{w.q1d.data(), meqn, mbc};
+
+    bool limit = false;
+    for (int mw = 0; mw < mwaves; ++mw)
+        if (mthlim[mw] > 0) limit = true;
+
+    // flux2.f90:90-95
+    for (int i = 1 - mbc; i <= mx + mbc; ++i)
+        for (int m = 0; m < meqn; ++m) {
+            qadd(m, i) = 0.0;
+            fadd(m, i) = 0.0;
+            gadd(m, 0, i) = 0.0;
+            gadd(m, 1, i) = 0.0;
+        }
+    (void)q1d;
+
+    // flux2.f90:101
+    call_rpn2(rp, ixy, mbc, mx, meqn, mwaves, q, wave, s, amdq, apdq, cp);
+
+    // flux2.f90:104-108 (forall: first statement over all i, then the second)
+    for (int i = 1; i <= mx + 1; ++i)
+        for (int m = 0; m < meqn; ++m) qadd(m, i) = qadd(m, i) - dtdx1d(i) * apdq(m, i);
+    for (int i = 1; i <= mx + 1; ++i)
+        for (int m = 0; m < meqn; ++m) qadd(m, i - 1) = qadd(m, i - 1) - dtdx1d(i - 1) * amdq(m, i);
+
+    // flux2.f90:111-119
+    double c = 0.0;
+    for (int mw = 0; mw < mwaves; ++mw)
+        for (int i = 1; i <= mx + 1; ++i)
+            c = std::max(c, std::max(dtdx1d(i) * s(mw, i), -dtdx1d(i - 1) * s(mw, i)));
+    *cfl1d = c;
+
+    if (method[1] != 1) {
+        // flux2.f90:127
+        if (limit) limiter(mx, meqn, mwaves, wave, s, mthlim);
+        // flux2.f90:134-160
+        for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+            double dtdxave = 0.5 * (dtdx1d(i - 1) + dtdx1d(i));
+            for (int m = 0; m < meqn; ++m) {
+                cqxx(m, i) = 0.0;
+                for (int mw = 0; mw < mwaves; ++mw) {
+                    double sc = use_fwave ? std::copysign(1.0, s(mw, i)) : std::fabs(s(mw, i));
+                    cqxx(m, i) = cqxx(m, i) + sc * (1.0 - std::fabs(s(mw, i)) * dtdxave) * wave(m, mw, i);
+                }
+                fadd(m, i) = fadd(m, i) + 0.5 * cqxx(m, i);
+            }
+        }
+    }
+
+    // flux2.f90:163
+    if (method[2] <= 0) return;
+
+    // flux2.f90:165-172
+    if (method[1] > 1 && method[2] == 2) {
+        for (int i = 1; i <= mx + 1; ++i)
+            for (int m = 0; m < meqn; ++m) {
+                amdq(m, i) = amdq(m, i) + cqxx(m, i);
+                apdq(m, i) = apdq(m, i) - cqxx(m, i);
+            }
+    }
+
+    // flux2.f90:181-190
+    call_rpt2(rp, ixy, mbc, mx, meqn, mwaves, q, amdq, bmasdq, bpasdq, cp);
+    for (int i = 1; i <= mx + 1; ++i)
+        for (int m = 0; m < meqn; ++m) gadd(m, 0, i - 1) = gadd(m, 0, i - 1) - 0.5 * dtdx1d(i - 1) * bmasdq(m, i);
+    for (int i = 1; i <= mx + 1; ++i)
+        for (int m = 0; m < meqn; ++m) gadd(m, 1, i - 1) = gadd(m, 1, i - 1) - 0.5 * dtdx1d(i - 1) * bpasdq(m, i);
+
+    // flux2.f90:194-203
+    call_rpt2(rp, ixy, mbc, mx, meqn, mwaves, q, apdq, bmasdq, bpasdq, cp);
+    for (int i = 1; i <= mx + 1; ++i)
+        for (int m = 0; m < meqn; ++m) gadd(m, 0, i) = gadd(m, 0, i) - 0.5 * dtdx1d(i) * bmasdq(m, i);
+    for (int i = 1; i <= mx + 1; ++i)
+        for (int m = 0; m < meqn; ++m) gadd(m, 1, i) = gadd(m, 1, i) - 0.5 * dtdx1d(i) * bpasdq(m, i);
+}
+
+int check_args(int meqn, int mwaves, int mbc, int mx, int my, int rp) {
+    if (meqn < 1 || mwaves < 1 || mbc != 2 || mx < 1 || my < 1) return 1;
+    if (!rp_known(rp)) return 2;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+void oracle_set_threads(int n) { g_threads = n < 1 ? 1 : n; }
+int oracle_get_threads(void) { return g_threads; }
+
+// step2.f90:74-247
+int oracle_step2(int maxm, int meqn, int mwaves, int maux, int mbc, int mx, int my,
+                 const double* qold_p, double* qnew_p, const double* aux_p, double dx,
+                 double dy, double dt, const int* method, const int* mthlim, double* cfl_out,
+                 int use_fwave, int rp, const double* cp) {
+    int e = check_args(meqn, mwaves, mbc, mx, my, rp);
+    if (e) return e;
+    if (maxm < std::max(mx, my)) return 3;
+    const int index_capa = method[5];
+    if (index_capa > 0 && (aux_p == nullptr || maux < index_capa)) return 4;
+    Grid2 qold{const_cast<double*>(qold_p), meqn, mbc, mx};
+    Grid2 qnew{qnew_p, meqn, mbc, mx};
+    Grid2 aux{const_cast<double*>(aux_p), maux > 0 ? maux : 1, mbc, mx};
+    const double dtdx = dt / dx, dtdy = dt / dy;
+    double cfl = 0.0;
+
+    // Rows interact through the j-1/j+1 scatter, so a parallel x-sweep colours
+    // rows by j mod 3 (any row set with distinct colours has disjoint targets).
+    // With one thread this is exactly the reference's sequential order.
+    const int nthr = g_threads;
+    auto sweep = [&](int ixy) {
+        const int nslab = (ixy == 1) ? my + 2 : mx + 2;  // j (or i) = 0 .. n+1
+        const int n = (ixy == 1) ? mx : my;
+        const double d_norm = (ixy == 1) ? dtdx : dtdy;
+        const int ncolor = nthr > 1 ? 3 : 1;
+        double cfl_s = 0.0;
+        for (int color = 0; color < ncolor; ++color) {
+#ifdef _OPENMP
+#pragma omp parallel num_threads(nthr) reduction(max : cfl_s) if (nthr > 1)
+#endif
+            {
+                Work w(maxm, mbc, meqn, mwaves);
+#ifdef _OPENMP
+#pragma omp for schedule(static)
+#endif
+                for (int k = 0; k < nslab; ++k) {
+                    if (ncolor > 1 && (k % 3) != color) continue;
+                    const int js = k;  // slice index 0 .. n_other+1
+                    for (int i = 1 - mbc; i <= maxm + mbc; ++i) {
+                        w.dtdx1d[(size_t)(i + mbc - 1)] = d_norm;
+                    }
+                    for (int m = 0; m < meqn; ++m)
+                        for (int i = 1 - mbc; i <= n + mbc; ++i)
+                            w.q1d[(size_t)(i + mbc - 1) * meqn + m] =
+                                (ixy == 1) ? qold(m, i, js) : qold(m, js, i);
+                    if (index_capa > 0)
+                        for (int i = 1 - mbc; i <= n + mbc; ++i)
+                            w.dtdx1d[(size_t)(i + mbc - 1)] =
+                                d_norm / ((ixy == 1) ? aux(index_capa - 1, i, js) : aux(index_capa - 1, js, i));
+                    double c1d = 0.0;
+                    flux2(ixy, mbc, n, meqn, mwaves, w, method, mthlim, &c1d, use_fwave != 0, rp, cp);
+                    cfl_s = std::max(cfl_s, c1d);
+                    Slice qadd{w.qadd.data(), meqn, mbc};
+                    Slice fadd{w.fadd.data(), meqn, mbc};
+                    Gadd gadd{w.gadd.data(), meqn, mbc};
+                    for (int m = 0; m < meqn; ++m)
+                        for (int i = 1; i <= n; ++i) {
+                            if (ixy == 1) {
+                                const int j = js;
+                                if (index_capa == 0) {
+                                    qnew(m, i, j) = qnew(m, i, j) + qadd(m, i) - dtdx * (fadd(m, i + 1) - fadd(m, i)) -
+                                                    dtdy * (gadd(m, 1, i) - gadd(m, 0, i));
+                                    qnew(m, i, j - 1) = qnew(m, i, j - 1) - dtdy * gadd(m, 0, i);
+                                    qnew(m, i, j + 1) = qnew(m, i, j + 1) + dtdy * gadd(m, 1, i);
+                                } else {
+                                    qnew(m, i, j) = qnew(m, i, j) + qadd(m, i) -
+                                                    (dtdx * (fadd(m, i + 1) - fadd(m, i)) +
+                                                     dtdy * (gadd(m, 1, i) - gadd(m, 0, i))) /
+                                                        aux(index_capa - 1, i, j);
+                                    qnew(m, i, j - 1) = qnew(m, i, j - 1) - dtdy * gadd(m, 0, i) / aux(index_capa - 1, i, j - 1);
+                                    qnew(m, i, j + 1) = qnew(m, i, j + 1) + dtdy * gadd(m, 1, i) / aux(index_capa - 1, i, j + 1);
+                                }
+                            } else {
+                                const int ii = js, j = i;
+                                if (index_capa == 0) {
+                                    qnew(m, ii, j) = qnew(m, ii, j) + (qadd(m, j) - dtdy * (fadd(m, j + 1) - fadd(m, j)) -
+                                                                       dtdx * (gadd(m, 1, j) - gadd(m, 0, j)));
+                                    qnew(m, ii - 1, j) = qnew(m, ii - 1, j) - dtdx * gadd(m, 0, j);
+                                    qnew(m, ii + 1, j) = qnew(m, ii + 1, j) + dtdx * gadd(m, 1, j);
+                                } else {
+                                    qnew(m, ii, j) = qnew(m, ii, j) + qadd(m, j) -
+                                                     (dtdy * (fadd(m, j + 1) - fadd(m, j)) +
+                                                      dtdx * (gadd(m, 1, j) - gadd(m, 0, j))) /
+                                                         aux(index_capa - 1, ii, j);
+                                    qnew(m, ii - 1, j) = qnew(m, ii - 1, j) - dtdx * gadd(m, 0, j) / aux(index_capa - 1, ii - 1, j);
+                                    qnew(m, ii + 1, j) = qnew(m, ii + 1, j) + dtdx * gadd(m, 1, j) / aux(index_capa - 1, ii + 1, j);
+                                }
+                            }
+                        }
+                }
+            }
+        }
+        cfl = std::max(cfl, cfl_s);
+    };
+    sweep(1);
+    sweep(2);
+    *cfl_out = cfl;
+    return 0;
+}
+
+// step2ds.f90:72-261 (no transverse terms; method[2] is -1 for split runs)
+int oracle_step2ds(int maxm, int meqn, int mwaves, int maux, int mbc, int mx, int my,
+                   const double* qold_p, double* qnew_p, const double* aux_p, double dx,
+                   double dy, double dt, const int* method, const int* mthlim, double* cfl_out,
+                   int ids, int use_fwave, int rp, const double* cp) {
+    int e = check_args(meqn, mwaves, mbc, mx, my, rp);
+    if (e) return e;
+    if (maxm < std::max(mx, my)) return 3;
+    if (ids != 1 && ids != 2) return 5;
+    const int index_capa = method[5];
+    if (index_capa > 0 && (aux_p == nullptr || maux < index_capa)) return 4;
+    Grid2 qold{const_cast<double*>(qold_p), meqn, mbc, mx};
+    Grid2 qnew{qnew_p, meqn, mbc, mx};
+    Grid2 aux{const_cast<double*>(aux_p), maux > 0 ? maux : 1, mbc, mx};
+    const double dtdx = dt / dx, dtdy = dt / dy;
+    double cfl = 0.0;
+    const int ixy = ids;
+    const int n = (ixy == 1) ? mx : my;
+    const int nother = (ixy == 1) ? my : mx;
+    const double d_norm = (ixy == 1) ? dtdx : dtdy;
+    // Slices are independent in a split sweep.  The q1d gather copies the whole
+    // slice before any write, so qold may alias qnew as in the reference.
+    const int nthr = g_threads;
+#ifdef _OPENMP
+#pragma omp parallel num_threads(nthr) reduction(max : cfl) if (nthr > 1)
+#endif
+    {
+        Work w(maxm, mbc, meqn, mwaves);
+#ifdef _OPENMP
+#pragma omp for schedule(static)
+#endif
+        for (int k = 1 - mbc; k <= nother + mbc; ++k) {
+            for (int i = 1 - mbc; i <= maxm + mbc; ++i) w.dtdx1d[(size_t)(i + mbc - 1)] = d_norm;
+            for (int m = 0; m < meqn; ++m)
+                for (int i = 1 - mbc; i <= n + mbc; ++i)
+                    w.q1d[(size_t)(i + mbc - 1) * meqn + m] = (ixy == 1) ? qold(m, i, k) : qold(m, k, i);
+            if (index_capa > 0)
+                for (int i = 1 - mbc; i <= n + mbc; ++i)
+                    w.dtdx1d[(size_t)(i + mbc - 1)] =
+                        d_norm / ((ixy == 1) ? aux(index_capa - 1, i, k) : aux(index_capa - 1, k, i));
+            double c1d = 0.0;
+            flux2(ixy, mbc, n, meqn, mwaves, w, method, mthlim, &c1d, use_fwave != 0, rp, cp);
+            cfl = std::max(cfl, c1d);
+            Slice qadd{w.qadd.data(), meqn, mbc};
+            Slice fadd{w.fadd.data(), meqn, mbc};
+            for (int m = 0; m < meqn; ++m)
+                for (int i = 1; i <= n; ++i) {
+                    double* t = (ixy == 1) ? &qnew(m, i, k) : &qnew(m, k, i);
+                    const double dd = (ixy == 1) ? dtdx : dtdy;
+                    if (index_capa == 0)
+                        *t = *t + qadd(m, i) - dd * (fadd(m, i + 1) - fadd(m, i));
+                    else
+                        *t = *t + qadd(m, i) - dd * (fadd(m, i + 1) - fadd(m, i)) /
+                                                   ((ixy == 1) ? aux(index_capa - 1, i, k) : aux(index_capa - 1, k, i));
+                }
+        }
+    }
+    *cfl_out = cfl;
+    return 0;
+}
+
+// solver.py:351-519 for q: dimension 0 lower, upper, then dimension 1 lower,
+// upper; each dimension fills its ghost layers across the full extent of the
+// other index (so corners come from the dimension-1 pass).
+int oracle_bc_fill(int meqn, int mbc, int mx, int my, double* qbc, const int* bcl, const int* bcu) {
+    Grid2 q{qbc, meqn, mbc, mx};
+    const int reflect[2] = {1, 2};
+    for (int idim = 0; idim < 2; ++idim) {
+        const int n = idim == 0 ? mx : my;
+        const int lo_other = 1 - mbc, hi_other = (idim == 0 ? my : mx) + mbc;
+        auto at = [&](int m, int a, int b) -> double& {  // a along idim, b along the other
+            return idim == 0 ? q(m, a, b) : q(m, b, a);
+        };
+        for (int side = 0; side < 2; ++side) {
+            const int bc = side == 0 ? bcl[idim] : bcu[idim];
+            for (int b = lo_other; b <= hi_other; ++b) {
+                for (int g = 0; g < mbc; ++g) {
+                    // Python index g along the rolled axis: cell 1-mbc+g (lower) or n+mbc-g (upper)
+                    const int ghost = side == 0 ? (1 - mbc + g) : (n + mbc - g);
+                    int src;
+                    if (bc == 1) {
+                        src = side == 0 ? 1 : n;
+                    } else if (bc == 2) {
+                        src = side == 0 ? (n - mbc + 1 + g) : (mbc - g);
+                    } else if (bc == 3) {
+                        src = side == 0 ? (mbc - g) : (n - mbc + 1 + g);
+                    } else {
+                        return 6;
+                    }
+                    for (int m = 0; m < meqn; ++m) {
+                        double v = at(m, src, b);
+                        if (bc == 3 && m == reflect[idim]) v = -v;
+                        at(m, ghost, b) = v;
+                    }
+                }
+            }
+        }
+    }
+    return 0;
+}
+
+int oracle_rpn2(int rp, int ixy, int maxm, int meqn, int mwaves, int mbc, int mx, const double* ql,
+                const double* qr, double* wave, double* s, double* amdq, double* apdq, const double* cp) {
+    if (!rp_known(rp) || mx > maxm) return 2;
+    CSlice l{ql, meqn, mbc}, r{qr, meqn, mbc};
+    Waves w{wave, meqn, mwaves, mbc};
+    Speeds sp{s, mwaves, mbc};
+    Slice am{amdq, meqn, mbc}, ap{apdq, meqn, mbc};
+    switch (rp) {
+        case ORC_RP_ADVECTION: rpn2_advection(ixy, mbc, mx, meqn, mwaves, l, r, w, sp, am, ap, cp); break;
+        case ORC_RP_ACOUSTICS: rpn2_acoustics(ixy, mbc, mx, l, r, w, sp, am, ap, cp, meqn); break;
+        case ORC_RP_EULER_ROE: rpn2_euler_roe(ixy, mbc, mx, meqn, mwaves, l, r, w, sp, am, ap, cp); break;
+        case ORC_RP_SHALLOW_ROE: rpn2_shallow_roe(ixy, mbc, mx, meqn, mwaves, l, r, w, sp, am, ap, cp); break;
+    }
+    return 0;
+}
+
+int oracle_rpt2(int rp, int ixy, int imp, int maxm, int meqn, int mwaves, int mbc, int mx,
+                const double* ql, const double* qr, const double* asdq, double* bmasdq, double* bpasdq,
+                const double* cp) {
+    (void)imp;
+    if (!rp_known(rp) || mx > maxm) return 2;
+    CSlice l{ql, meqn, mbc}, r{qr, meqn, mbc};
+    Slice as{const_cast<double*>(asdq), meqn, mbc}, bm{bmasdq, meqn, mbc}, bp{bpasdq, meqn, mbc};
+    switch (rp) {
+        case ORC_RP_ADVECTION: rpt2_advection(ixy, mbc, mx, as, bm, bp, cp); break;
+        case ORC_RP_ACOUSTICS: rpt2_acoustics(ixy, mbc, mx, as, bm, bp, cp); break;
+        case ORC_RP_EULER_ROE: rpt2_euler_roe(ixy, mbc, mx, meqn, mwaves, l, r, as, bm, bp, cp); break;
+        case ORC_RP_SHALLOW_ROE: rpt2_shallow_roe(ixy, mbc, mx, meqn, mwaves, l, r, as, bm, bp, cp); break;
+    }
+    return 0;
+}
+
+int oracle_exact_star(double, double, double, double, double, double, double, double, int,
+                      double*, double*, int*) {
+    return 99;  // filled in with the exact solver
+}
+
+}  // extern "C"

@@ -1,0 +1,149 @@
+"""Python access to the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+The oracle restates the reference's classic 2D kernels in C++
+(oracle/claw_oracle.cpp; see its header for the file:line map).  This module
+loads it with ctypes and provides ``OracleClawSolver2D``, a ClawSolver2D whose
+step_hyperbolic is the reference's host algorithm
+(src/pyclaw/classic/solver.py:498-549: ghost fill, ``qold = qbc.copy('F')``,
+step2 or the step2ds pair, CFL update, ``set_q_from_qbc``) on host arrays, and
+whose reject path restores a host backup like src/pyclaw/solver.py:610-645.
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use it.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libclaw_oracle.so")
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        build()
+    lib = ctypes.CDLL(LIB_PATH)
+    i = ctypes.c_int
+    d = ctypes.c_double
+    lib.oracle_step2.argtypes = [i] * 7 + [_dp, _dp, _dp, d, d, d, _ip, _ip, _dp, i, i, _dp]
+    lib.oracle_step2ds.argtypes = [i] * 7 + [_dp, _dp, _dp, d, d, d, _ip, _ip, _dp, i, i, i, _dp]
+    lib.oracle_bc_fill.argtypes = [i, i, i, i, _dp, _ip, _ip]
+    lib.oracle_rpn2.argtypes = [i] * 7 + [_dp, _dp, _dp, _dp, _dp, _dp, _dp]
+    lib.oracle_rpt2.argtypes = [i] * 8 + [_dp, _dp, _dp, _dp, _dp, _dp]
+    lib.oracle_exact_star.argtypes = [d] * 8 + [i, _dp, _dp, _ip]
+    lib.oracle_set_threads.argtypes = [i]
+    lib.oracle_set_threads.restype = None
+    _lib = lib
+    return lib
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _i(a):
+    return np.ascontiguousarray(a, dtype=np.intc).ctypes.data_as(_ip)
+
+
+def set_threads(n):
+    load().oracle_set_threads(int(n))
+
+
+def step2(qold, qnew, dx, dy, dt, method, mthlim, rp_id, cparam, use_fwave=False):
+    """Oracle step2 on qbc arrays (meqn, mx+4, my+4) F-order; returns cfl."""
+    lib = load()
+    meqn, nxg, nyg = qold.shape
+    mx, my = nxg - 4, nyg - 4
+    cfl = ctypes.c_double(0.0)
+    cp = np.asarray(list(cparam) + [0.0] * 8, dtype=np.float64)
+    method = np.ascontiguousarray(method, dtype=np.intc)
+    mthlim = np.ascontiguousarray(mthlim, dtype=np.intc)
+    rc = lib.oracle_step2(max(mx, my), meqn, len(mthlim), 0, 2, mx, my, _d(qold), _d(qnew), None,
+                          dx, dy, dt, _i(method), _i(mthlim), ctypes.byref(cfl), int(use_fwave),
+                          rp_id, _d(cp))
+    if rc:
+        raise RuntimeError("oracle_step2 returned %d" % rc)
+    return cfl.value
+
+
+def step2ds(qold, qnew, dx, dy, dt, method, mthlim, ids, rp_id, cparam, use_fwave=False):
+    lib = load()
+    meqn, nxg, nyg = qold.shape
+    mx, my = nxg - 4, nyg - 4
+    cfl = ctypes.c_double(0.0)
+    cp = np.asarray(list(cparam) + [0.0] * 8, dtype=np.float64)
+    method = np.ascontiguousarray(method, dtype=np.intc)
+    mthlim = np.ascontiguousarray(mthlim, dtype=np.intc)
+    rc = lib.oracle_step2ds(max(mx, my), meqn, len(mthlim), 0, 2, mx, my, _d(qold), _d(qnew), None,
+                            dx, dy, dt, _i(method), _i(mthlim), ctypes.byref(cfl), ids, int(use_fwave),
+                            rp_id, _d(cp))
+    if rc:
+        raise RuntimeError("oracle_step2ds returned %d" % rc)
+    return cfl.value
+
+
+def bc_fill(qbc, bc_lower, bc_upper):
+    lib = load()
+    meqn, nxg, nyg = qbc.shape
+    assert qbc.flags.f_contiguous
+    rc = lib.oracle_bc_fill(meqn, 2, nxg - 4, nyg - 4, _d(qbc), _i(bc_lower), _i(bc_upper))
+    if rc:
+        raise RuntimeError("oracle_bc_fill returned %d" % rc)
+
+
+def make_solver_class():
+    """ClawSolver2D running the oracle on host arrays (built lazily so that
+    importing this module does not import the product package)."""
+    from pyclaw_b200.classic import ClawSolver2D
+
+    class OracleClawSolver2D(ClawSolver2D):
+        def __init__(self, riemann_solver=None, claw_package=None):
+            self._backup = None
+            super().__init__(riemann_solver, claw_package)
+
+        def setup(self, solution):
+            self._check_cfl_settings()
+            self._set_mthlim()
+            state = solution.states[0]
+            self._set_method(state)
+            mx, my = state.grid.num_cells
+            self.qbc = np.zeros((state.num_eqn, mx + 4, my + 4), order='F')
+            self._is_set_up = True
+
+        def _begin_step(self, solution):
+            self._backup = solution.state._q.copy('F')
+
+        def _end_step(self, solution, accept):
+            if not accept:
+                solution.state._q = self._backup
+
+        def step_hyperbolic(self, solution):
+            state = solution.states[0]
+            dx, dy = state.grid.delta
+            qbc = self.qbc
+            qbc[:, 2:-2, 2:-2] = state._q
+            bc_fill(qbc, self.bc_lower, self.bc_upper)
+            qold = qbc.copy('F')
+            cp = self.rp.cparam(state.problem_data)
+            if self.dimensional_split:
+                c1 = step2ds(qold, qbc, dx, dy, self.dt, self._method, self._mthlim, 1, self.rp.rp_id, cp)
+                c2 = step2ds(qbc, qbc, dx, dy, self.dt, self._method, self._mthlim, 2, self.rp.rp_id, cp)
+                cfl = max(c1, c2)
+            else:
+                cfl = step2(qold, qbc, dx, dy, self.dt, self._method, self._mthlim, self.rp.rp_id, cp)
+            self.cfl.update_global_max(cfl)
+            state._q = np.asfortranarray(qbc[:, 2:-2, 2:-2].copy())
+
+    return OracleClawSolver2D

@@ -1,0 +1,122 @@
+"""ctypes binding of ``lib/libclaw2.so`` (C ABI declared in ``include/claw2.h``).
+
+The library is the only compute path of this package: if it is missing or
+cannot be loaded, every solver call raises; there is no CPU fallback.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libclaw2.so")
+
+CLAW2_MAX_PARAMS = 8
+CLAW2_MAX_WAVES = 8
+
+RP_ADVECTION, RP_ACOUSTICS, RP_EULER_ROE, RP_SHALLOW_ROE, RP_EULER_EXACT = 1, 2, 3, 4, 5
+
+OK, EINVAL, ECUDA, ENONFINITE, ETIMEOUT, ENOMEM, EUNSUPPORTED = 0, 1, 2, 3, 4, 5, 6
+
+_c_int_p = ctypes.POINTER(ctypes.c_int)
+_c_double_p = ctypes.POINTER(ctypes.c_double)
+
+
+class Claw2Desc(ctypes.Structure):
+    """Mirror of ``claw2_desc``."""
+    _fields_ = [
+        ("mx", ctypes.c_int), ("my", ctypes.c_int),
+        ("num_eqn", ctypes.c_int), ("num_waves", ctypes.c_int),
+        ("num_aux", ctypes.c_int), ("num_ghost", ctypes.c_int),
+        ("riemann", ctypes.c_int), ("order", ctypes.c_int),
+        ("transverse", ctypes.c_int), ("dimensional_split", ctypes.c_int),
+        ("fwave", ctypes.c_int),
+        ("mthlim", ctypes.c_int * CLAW2_MAX_WAVES),
+        ("bc_lower", ctypes.c_int * 2), ("bc_upper", ctypes.c_int * 2),
+        ("dx", ctypes.c_double), ("dy", ctypes.c_double),
+        ("cparam", ctypes.c_double * CLAW2_MAX_PARAMS),
+        ("ncparam", ctypes.c_int),
+        ("device", ctypes.c_int),
+    ]
+
+
+class Claw2Error(RuntimeError):
+    """A status code other than CLAW2_OK, with the library's message."""
+
+    def __init__(self, code, msg):
+        super().__init__("claw2 error %d: %s" % (code, msg))
+        self.code = code
+
+
+class NonFiniteError(Claw2Error):
+    pass
+
+
+# name -> (restype, argtypes); exactly the declarations of include/claw2.h
+_SIGNATURES = {
+    "claw2_step2": (ctypes.c_int, [ctypes.c_int] * 7 + [_c_double_p, _c_double_p, _c_double_p,
+                                                        ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                                        _c_int_p, _c_int_p, _c_double_p, ctypes.c_int,
+                                                        ctypes.c_int, _c_double_p, ctypes.c_int]),
+    "claw2_step2ds": (ctypes.c_int, [ctypes.c_int] * 7 + [_c_double_p, _c_double_p, _c_double_p,
+                                                          ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                                          _c_int_p, _c_int_p, _c_double_p, ctypes.c_int,
+                                                          ctypes.c_int, ctypes.c_int, _c_double_p,
+                                                          ctypes.c_int]),
+    "claw2_bc_fill": (ctypes.c_int, [ctypes.c_int] * 4 + [_c_double_p, _c_int_p, _c_int_p]),
+    "claw2_patch_create": (ctypes.c_int, [ctypes.POINTER(Claw2Desc), ctypes.POINTER(ctypes.c_void_p)]),
+    "claw2_patch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "claw2_patch_set_cparam": (ctypes.c_int, [ctypes.c_void_p, _c_double_p, ctypes.c_int]),
+    "claw2_patch_upload_q": (ctypes.c_int, [ctypes.c_void_p, _c_double_p]),
+    "claw2_patch_download_q": (ctypes.c_int, [ctypes.c_void_p, _c_double_p]),
+    "claw2_patch_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _c_double_p]),
+    "claw2_patch_accept": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "claw2_patch_cfl": (ctypes.c_int, [ctypes.c_void_p, _c_double_p]),
+    "claw2_patch_sync": (ctypes.c_int, [ctypes.c_void_p]),
+    "claw2_patch_device_q": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(_c_double_p),
+                                            ctypes.POINTER(ctypes.c_longlong)]),
+    "claw2_patch_set_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "claw2_patch_set_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "claw2_patch_kernel_ms": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]),
+    "claw2_probe_fp64": (ctypes.c_int, [ctypes.c_int, _c_double_p]),
+    "claw2_last_error": (ctypes.c_char_p, []),
+    "claw2_version": (ctypes.c_char_p, []),
+}
+
+_lib = None
+
+
+def load():
+    """Load the CUDA library once; raise with a clear message if it is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("pyclaw_b200: CUDA extension %s is missing; build it with "
+                          "`python -m pyclaw_b200.build` (no CPU fallback exists)" % LIB_PATH)
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in _SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(rc):
+    if rc != OK:
+        msg = load().claw2_last_error().decode()
+        if rc == ENONFINITE:
+            raise NonFiniteError(rc, msg)
+        raise Claw2Error(rc, msg)
+
+
+def dptr(a):
+    """double* of a C- or F-contiguous float64 array."""
+    assert a.dtype == np.float64 and (a.flags.c_contiguous or a.flags.f_contiguous)
+    return a.ctypes.data_as(_c_double_p)
+
+
+def iptr(a):
+    assert a.dtype == np.intc and a.flags.c_contiguous
+    return a.ctypes.data_as(_c_int_p)

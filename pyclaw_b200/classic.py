@@ -1,0 +1,199 @@
+"""Classic Clawpack solvers with a CUDA kernel language.
+
+Host mirror of src/pyclaw/classic/solver.py: ClawSolver (:19-234) and
+ClawSolver2D (:393-549).  ``kernel_language = 'CUDA'`` (the default here, and
+the only language of this package) runs each hyperbolic step on the GPU
+through the C ABI of include/claw2.h: ghost-cell fill, the unsplit step2 (or
+the split step2ds pair) and the CFL reduction all happen on the device, and q
+stays there between steps.
+"""
+from .limiters import tvd
+from .solver import BC, Solver
+from . import _lib
+
+
+class ClawSolver(Solver):
+    """Generic classic solver (classic/solver.py:19-234)."""
+
+    def __init__(self, riemann_solver=None, claw_package=None):
+        self.num_ghost = 2
+        self.limiters = tvd.minmod
+        self.order = 2
+        self.source_split = 1
+        self.fwave = False
+        self.step_source = None
+        self.kernel_language = 'CUDA'
+        self.verbosity = 0
+        self.cfl_max = 1.0
+        self.cfl_desired = 0.9
+        self._mthlim = self.limiters
+        self._method = None
+        self.dt_old = None
+        super(ClawSolver, self).__init__(riemann_solver, claw_package)
+
+    def step(self, solution, take_one_step, tstart, tend):
+        """classic/solver.py:96-146."""
+        self.get_dt(solution.t, tstart, tend, take_one_step)
+        self.cfl.set_global_max(0.)
+        if self.source_split == 2 and self.step_source is not None:
+            self.step_source(self, solution.states[0], self.dt / 2.0)
+        self.step_hyperbolic(solution)
+        if self.cfl.get_cached_max() >= self.cfl_max:
+            return False
+        if self.step_source is not None:
+            if self.source_split == 2:
+                self.step_source(self, solution.states[0], self.dt / 2.0)
+            if self.source_split == 1:
+                self.step_source(self, solution.states[0], self.dt)
+        return True
+
+    def _check_cfl_settings(self):
+        pass
+
+    def _set_mthlim(self):
+        """classic/solver.py:162-171."""
+        self._mthlim = self.limiters
+        if not isinstance(self.limiters, list):
+            self._mthlim = [self._mthlim]
+        if len(self._mthlim) == 1:
+            self._mthlim = self._mthlim * self.num_waves
+        if len(self._mthlim) != self.num_waves:
+            raise Exception('Length of solver.limiters is not equal to 1 or to solver.num_waves')
+
+    def _set_method(self, state):
+        """method[7] as classic/solver.py:173-193 builds it."""
+        import numpy as np
+        self._method = np.empty(7, dtype=int, order='F')
+        self._method[0] = self.dt_variable
+        self._method[1] = self.order
+        if self.num_dim == 1:
+            self._method[2] = 0
+        elif self.dimensional_split:
+            self._method[2] = -1
+        else:
+            self._method[2] = self.transverse_waves
+        self._method[3] = self.verbosity
+        self._method[4] = 0
+        self._method[5] = state.index_capa + 1
+        self._method[6] = state.num_aux
+
+    def step_hyperbolic(self, solution):
+        raise Exception("Dummy routine, please override!")
+
+
+class ClawSolver2D(ClawSolver):
+    """2D classic solver (classic/solver.py:393-549)."""
+
+    no_trans = 0
+    trans_inc = 1
+    trans_cor = 2
+
+    def __init__(self, riemann_solver=None, claw_package=None):
+        self.dimensional_split = True
+        self.transverse_waves = self.trans_inc
+        self.num_dim = 2
+        self.reflect_index = [1, 2]
+        self.aux1 = None
+        self.aux2 = None
+        self.aux3 = None
+        self.work = None
+        self.device = 0
+        self._dev = None
+        super(ClawSolver2D, self).__init__(riemann_solver, claw_package)
+
+    def _check_cfl_settings(self):
+        if (not self.dimensional_split) and (self.transverse_waves == 0):
+            cfl_recommended = 0.5
+        else:
+            cfl_recommended = 1.0
+        if self.cfl_max > cfl_recommended:
+            import warnings
+            warnings.warn('cfl_max is set higher than the recommended value of %s' % cfl_recommended)
+            warnings.warn(str(self.cfl_desired))
+
+    def setup(self, solution):
+        """classic/solver.py:195-219 with the device patch in place of the f2py
+        module, its workspace and the qbc arrays."""
+        self._check_cfl_settings()
+        self._set_mthlim()
+        if self.kernel_language != 'CUDA':
+            raise Exception("pyclaw_b200 runs kernel_language='CUDA' only (got %r)" % self.kernel_language)
+        state = solution.states[0]
+        self._set_method(state)
+        self._make_device_patch(solution)
+        super(ClawSolver, self).setup(solution)
+
+    def _device_desc(self, solution):
+        state = solution.states[0]
+        grid = state.grid
+        if self.rp is None or not hasattr(self.rp, 'rp_id'):
+            raise Exception("ClawSolver2D needs a pyclaw_b200.riemann solver")
+        if state.num_aux > 0 or state.index_capa >= 0:
+            raise NotImplementedError("aux arrays and capacity functions are not in this build")
+        if self.step_source is not None:
+            raise NotImplementedError("source terms (step_source) are not in this build")
+        for b in list(self.bc_lower) + list(self.bc_upper):
+            if b is None:
+                raise Exception('One of the boundary conditions has not been set.')
+            if b == BC.custom:
+                raise NotImplementedError("custom boundary conditions are not in this build")
+        if self.fwave:
+            raise NotImplementedError("f-wave Riemann solvers are not in this build")
+        d = _lib.Claw2Desc()
+        d.mx, d.my = grid.num_cells
+        d.num_eqn, d.num_waves = state.num_eqn, self.num_waves
+        if state.num_eqn != self.rp.num_eqn:
+            raise ValueError("state has num_eqn=%d, Riemann solver %s needs %d"
+                             % (state.num_eqn, self.rp.name, self.rp.num_eqn))
+        d.num_aux = 0
+        d.num_ghost = self.num_ghost
+        d.riemann = self.rp.rp_id
+        d.order = self.order
+        d.transverse = int(self.transverse_waves)
+        d.dimensional_split = 1 if self.dimensional_split else 0
+        d.fwave = 0
+        for k, v in enumerate(self._mthlim):
+            d.mthlim[k] = int(v)
+        d.bc_lower[0], d.bc_lower[1] = self.bc_lower
+        d.bc_upper[0], d.bc_upper[1] = self.bc_upper
+        d.dx, d.dy = grid.delta
+        vals = self.rp.cparam(state.problem_data)
+        for k, v in enumerate(vals):
+            d.cparam[k] = v
+        d.ncparam = len(vals)
+        d.device = int(self.device)
+        return d
+
+    def _make_device_patch(self, solution):
+        from .device import DevicePatch
+        if self._dev is not None:
+            self._dev.close()
+        state = solution.states[0]
+        self._dev = DevicePatch(self._device_desc(solution))
+        state._mirror = self._dev
+        self._dev.push(state)
+
+    # ---- per-step hooks ------------------------------------------------------
+    def _begin_step(self, solution):
+        pass  # the device keeps the current q untouched until accept
+
+    def _end_step(self, solution, accept):
+        self._dev.accept(accept)
+
+    def step_hyperbolic(self, solution):
+        """classic/solver.py:498-549 on the device: BC fill + step2 (or the
+        step2ds pair) + CFL; the result is pending until accepted."""
+        state = solution.states[0]
+        dev = self._dev
+        if dev is None or state._mirror is not dev:
+            self._make_device_patch(solution)
+            dev = self._dev
+        if dev.host_dirty:
+            dev.push(state)
+        cfl = dev.step(self.dt)
+        self.cfl.update_global_max(cfl)
+
+    def __del__(self):
+        if getattr(self, '_dev', None) is not None:
+            self._dev.close()
+        self._is_set_up = False

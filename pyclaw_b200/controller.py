@@ -1,0 +1,81 @@
+"""Controller: the output-time loop (host mirror of src/pyclaw/controller.py:85-397)."""
+import copy
+import logging
+
+import numpy as np
+
+
+class Controller(object):
+    def __init__(self):
+        self.logger = logging.getLogger('pyclaw.controller')
+        self.solver = None
+        self.solution = None
+        self.outdir = './_output'
+        self.output_format = None   # frames are kept in memory (keep_copy); no files
+        self.output_file_prefix = None
+        self.output_options = {}
+        self.write_aux_init = False
+        self.write_aux_always = False
+        self.keep_copy = False
+        self.frames = []
+        self.output_style = 1
+        self.num_output_times = 10
+        self.out_times = np.linspace(0.0, 1.0, 11)
+        self.nstepout = 1
+        self.tfinal = 1.0
+        self.verbosity = 0
+        self.setplot = None
+        self.compute_p = None
+        self.compute_F = None
+        self.overwrite = True
+        self.start_frame = 0
+
+    @property
+    def t(self):
+        return self.solution.t if self.solution is not None else None
+
+    def check_validity(self):
+        valid, reason = self.solver.is_valid()
+        if not valid:
+            raise Exception("The solver failed to initialize properly: %s" % reason)
+        if not self.solution.is_valid():
+            raise Exception("Initial solution is not valid.")
+
+    def run(self):
+        """controller.py:275-397 without file output."""
+        if self.solver is None or self.solution is None:
+            raise Exception('To run, a Controller must have a Solver and a Solution.')
+        if self.output_format is not None:
+            raise NotImplementedError("file output is not part of pyclaw_b200; set output_format=None "
+                                      "and keep_copy=True")
+        self.start_frame = self.solution.start_frame
+        frame = self.start_frame
+        if not self.solver._is_set_up:
+            self.solver.setup(self.solution)
+            self.solver.dt = self.solver.dt_initial
+        self.check_validity()
+        if self.output_style == 1:
+            output_times = np.linspace(self.solution.t, self.tfinal, self.num_output_times + 1)
+        elif self.output_style == 2:
+            output_times = self.out_times
+        elif self.output_style == 3:
+            output_times = np.ones((self.num_output_times + 1 - self.start_frame))
+        else:
+            raise Exception("Invalid output style %s" % self.output_style)
+        if len(output_times) == 0:
+            return None
+        if self.keep_copy:
+            self.frames.append(copy.deepcopy(self.solution))
+        status = None
+        for t in output_times[1:]:
+            if self.output_style < 3:
+                status = self.solver.evolve_to_time(self.solution, t)
+            else:
+                for n in range(self.nstepout):
+                    status = self.solver.evolve_to_time(self.solution)
+            frame += 1
+            if self.keep_copy:
+                self.frames.append(copy.deepcopy(self.solution))
+            self.logger.info("Solution %s computed for time t=%f" % (frame, self.solution.t))
+        self.solution._start_frame = len(self.frames)
+        return status

@@ -1,0 +1,648 @@
+// claw2.cu -- C ABI of the classic 2D step (declarations: include/claw2.h).
+//
+// Host side of the drop-in: argument checks with the reference's error
+// behaviour mapped to status codes, the device-resident patch (two q buffers,
+// CFL and status words, one stream), and the stateless replacements of the
+// f2py step2/step2ds routines.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "step_kernels.cuh"
+
+using namespace claw2;
+
+namespace {
+
+thread_local std::string g_err = "no error";
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                      \
+    do {                                                                                    \
+        cudaError_t e_ = (expr);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return fail(CLAW2_ECUDA, "%s failed: %s", #expr, cudaGetErrorString(e_));      \
+    } while (0)
+
+constexpr int NT_UNSPLIT = 128;  // threads per strip (124 output columns)
+constexpr int NT_SPLIT_X = 128;
+constexpr int NT_SPLIT_Y = 128;
+
+int rp_shape(int rp, int* meqn, int* mwaves) {
+    switch (rp) {
+        case CLAW2_RP_ADVECTION: *meqn = 1; *mwaves = 1; return 0;
+        case CLAW2_RP_ACOUSTICS: *meqn = 3; *mwaves = 2; return 0;
+        case CLAW2_RP_EULER_ROE: *meqn = 4; *mwaves = 4; return 0;
+        case CLAW2_RP_SHALLOW_ROE: *meqn = 3; *mwaves = 3; return 0;
+        default: return -1;
+    }
+}
+
+RPParams make_params(int rp, const double* cparam, int n) {
+    RPParams p;
+    for (int k = 0; k < CLAW2_MAX_PARAMS; ++k) p.c[k] = (cparam && k < n) ? cparam[k] : 0.0;
+    p.flags = 0;
+    if (rp == CLAW2_RP_EULER_ROE || rp == CLAW2_RP_SHALLOW_ROE) p.flags = (p.c[1] != 0.0) ? 1 : 0;
+    return p;
+}
+
+Layout make_layout(int mx, int my) {
+    Layout L;
+    L.mx = mx;
+    L.my = my;
+    L.pitch = ((mx + 4 + 31) / 32) * 32;
+    L.plane = (long long)L.pitch * (my + 4);
+    L.plane = ((L.plane + 31) / 32) * 32;  // 256-byte aligned planes
+    return L;
+}
+
+int pick_rows(int nstrips, int nrows) {
+    // about three CTAs per SM on a 148-SM part, 8..64 rows per CTA
+    const int want_blocks = std::max(1, (3 * 148 + nstrips - 1) / nstrips);
+    int H = (nrows + want_blocks - 1) / want_blocks;
+    return std::max(8, std::min(64, H));
+}
+
+// ---- launches, one instantiation per Riemann solver -----------------------
+template <class RP>
+void launch_unsplit(const StepArgs& a, cudaStream_t st) {
+    constexpr int W = NT_UNSPLIT - 4;
+    const int ns = (a.L.mx + W - 1) / W;
+    StepArgs b = a;
+    b.H = pick_rows(ns, a.L.my);
+    dim3 grid(ns, (a.L.my + b.H - 1) / b.H);
+    constexpr int smem = (int)sizeof(UnsplitSmem<RP, NT_UNSPLIT>);
+    static unsigned long long attr_set = 0;  // one bit per device, per instantiation
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 64 && !(attr_set & (1ull << dev))) {
+        cudaFuncSetAttribute(k_step_unsplit<RP, NT_UNSPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        attr_set |= 1ull << dev;
+    }
+    k_step_unsplit<RP, NT_UNSPLIT><<<grid, NT_UNSPLIT, smem, st>>>(b);
+}
+
+template <class RP>
+void launch_split(const StepArgs& ax, const StepArgs& ay, cudaStream_t st, int which) {
+    if (which & 1) {
+        constexpr int W = NT_SPLIT_X - 4;
+        const int ns = (ax.L.mx + W - 1) / W;
+        StepArgs b = ax;
+        b.H = pick_rows(ns, ax.L.my + 4);
+        dim3 grid(ns, (ax.L.my + 4 + b.H - 1) / b.H);
+        k_split_x<RP, NT_SPLIT_X><<<grid, NT_SPLIT_X, 0, st>>>(b);
+    }
+    if (which & 2) {
+        const int ns = (ay.L.mx + 4 + NT_SPLIT_Y - 1) / NT_SPLIT_Y;
+        StepArgs b = ay;
+        b.H = pick_rows(ns, ay.L.my);
+        dim3 grid(ns, (ay.L.my + b.H - 1) / b.H);
+        k_split_y<RP, NT_SPLIT_Y><<<grid, NT_SPLIT_Y, 0, st>>>(b);
+    }
+}
+
+template <template <class> class F, class... A>
+int dispatch(int rp, A&&... args) {
+    switch (rp) {
+        case CLAW2_RP_ADVECTION: F<RPAdvection>::run(args...); return 0;
+        case CLAW2_RP_ACOUSTICS: F<RPAcoustics>::run(args...); return 0;
+        case CLAW2_RP_EULER_ROE: F<RPEulerRoe>::run(args...); return 0;
+        case CLAW2_RP_SHALLOW_ROE: F<RPShallowRoe>::run(args...); return 0;
+        default: return -1;
+    }
+}
+template <class RP>
+struct UnsplitF {
+    static void run(const StepArgs& a, cudaStream_t st) { launch_unsplit<RP>(a, st); }
+};
+template <class RP>
+struct SplitF {
+    static void run(const StepArgs& ax, const StepArgs& ay, cudaStream_t st, int which) {
+        launch_split<RP>(ax, ay, st, which);
+    }
+};
+
+void launch_bc(double* q, const Layout& L, int meqn, const int* bcl, const int* bcu,
+               unsigned long long* cfl_bits, cudaStream_t st) {
+    BCArgs b;
+    b.q = q;
+    b.L = L;
+    b.meqn = meqn;
+    b.bcl[0] = bcl[0]; b.bcl[1] = bcl[1];
+    b.bcu[0] = bcu[0]; b.bcu[1] = bcu[1];
+    b.cfl_bits = cfl_bits;
+    const int n = 4 * (L.mx + 4) + 4 * L.my;
+    k_bc_fill<<<(n + 255) / 256, 256, 0, st>>>(b);
+}
+
+int check_method(int order, int trans, const int* mthlim, int mwaves, int fwave) {
+    if (order != 1 && order != 2) return fail(CLAW2_EINVAL, "order must be 1 or 2 (got %d)", order);
+    if (trans < -1 || trans > 2) return fail(CLAW2_EINVAL, "transverse must be -1..2 (got %d)", trans);
+    if (fwave) return fail(CLAW2_EUNSUPPORTED, "f-wave Riemann solvers are not in this build");
+    for (int k = 0; k < mwaves; ++k)
+        if (mthlim[k] < 0 || mthlim[k] > 5) return fail(CLAW2_EINVAL, "limiter %d out of range", mthlim[k]);
+    return CLAW2_OK;
+}
+
+int check_bc(const int* bcl, const int* bcu, int mx, int my) {
+    for (int d = 0; d < 2; ++d) {
+        const int n = d == 0 ? mx : my;
+        // a wall or periodic ghost cell copies one of the first/last two
+        // interior cells; with one cell that source would itself be a ghost
+        if (n < 2 && (bcl[d] != CLAW2_BC_EXTRAP || bcu[d] != CLAW2_BC_EXTRAP))
+            return fail(CLAW2_EINVAL, "wall/periodic BCs need at least 2 cells in dimension %d", d);
+        for (int v : {bcl[d], bcu[d]}) {
+            if (v == CLAW2_BC_CUSTOM)
+                return fail(CLAW2_EUNSUPPORTED, "custom BCs are applied by the host (dimension %d)", d);
+            if (v < 1 || v > 3) return fail(CLAW2_EINVAL, "boundary condition %d not implemented", v);
+        }
+        if ((bcl[d] == CLAW2_BC_PERIODIC) != (bcu[d] == CLAW2_BC_PERIODIC))
+            return fail(CLAW2_EINVAL, "periodic BC must be set on both sides of dimension %d", d);
+    }
+    return CLAW2_OK;
+}
+
+// Scratch used by the stateless entry points (grown on demand, reused).
+struct Scratch {
+    std::mutex mu;
+    int device = -1;
+    size_t cap = 0;  // doubles per buffer
+    double *a = nullptr, *b = nullptr, *c = nullptr, *stage = nullptr;
+    size_t stage_cap = 0;
+    unsigned long long* cfl = nullptr;
+    int* status = nullptr;
+    cudaStream_t st = nullptr;
+};
+Scratch g_scr;
+
+int scratch_reserve(size_t n, size_t nstage) {
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (g_scr.device != dev) {
+        g_scr.cap = g_scr.stage_cap = 0;
+        g_scr.a = g_scr.b = g_scr.c = g_scr.stage = nullptr;
+        g_scr.cfl = nullptr;
+        g_scr.status = nullptr;
+        g_scr.st = nullptr;
+        g_scr.device = dev;
+    }
+    if (!g_scr.st) CUDA_TRY(cudaStreamCreateWithFlags(&g_scr.st, cudaStreamNonBlocking));
+    if (!g_scr.cfl) {
+        CUDA_TRY(cudaMalloc(&g_scr.cfl, sizeof(unsigned long long)));
+        CUDA_TRY(cudaMalloc(&g_scr.status, sizeof(int)));
+    }
+    if (n > g_scr.cap) {
+        cudaFree(g_scr.a); cudaFree(g_scr.b); cudaFree(g_scr.c);
+        g_scr.a = g_scr.b = g_scr.c = nullptr;
+        g_scr.cap = 0;
+        if (cudaMalloc(&g_scr.a, n * 8) != cudaSuccess || cudaMalloc(&g_scr.b, n * 8) != cudaSuccess ||
+            cudaMalloc(&g_scr.c, n * 8) != cudaSuccess)
+            return fail(CLAW2_ENOMEM, "device allocation of %zu doubles failed", n);
+        g_scr.cap = n;
+    }
+    if (nstage > g_scr.stage_cap) {
+        cudaFree(g_scr.stage);
+        g_scr.stage = nullptr;
+        g_scr.stage_cap = 0;
+        if (cudaMalloc(&g_scr.stage, nstage * 8) != cudaSuccess)
+            return fail(CLAW2_ENOMEM, "device allocation of %zu doubles failed", nstage);
+        g_scr.stage_cap = nstage;
+    }
+    return CLAW2_OK;
+}
+
+int grid_blocks(long long n) { return (int)std::min<long long>((n + 255) / 256, 148LL * 16); }
+
+// Shared body of claw2_step2 / claw2_step2ds: host qbc -> device planes ->
+// kernels -> host qbc (interior cells).
+int host_step(int maxm, int meqn, int mwaves, int maux, int mbc, int mx, int my, const double* qold,
+              double* qnew, double dx, double dy, double dt, const int* method, const int* mthlim,
+              double* cfl, int ids, int use_fwave, int rp, const double* cparam, int ncparam) {
+    if (!qold || !qnew || !method || !mthlim || !cfl) return fail(CLAW2_EINVAL, "null pointer argument");
+    int me = 0, mw = 0;
+    if (rp_shape(rp, &me, &mw) != 0) return fail(CLAW2_EINVAL, "unknown Riemann solver id %d", rp);
+    if (me != meqn || mw != mwaves)
+        return fail(CLAW2_EINVAL, "solver %d has num_eqn=%d num_waves=%d (got %d, %d)", rp, me, mw, meqn, mwaves);
+    if (mbc != 2) return fail(CLAW2_EINVAL, "num_ghost must be 2 (got %d)", mbc);
+    if (mx < 1 || my < 1 || maxm < std::max(mx, my))
+        return fail(CLAW2_EINVAL, "bad sizes mx=%d my=%d maxm=%d", mx, my, maxm);
+    if (maux != 0 && method[6] != 0) return fail(CLAW2_EUNSUPPORTED, "aux arrays are not in this build");
+    if (method[5] != 0) return fail(CLAW2_EUNSUPPORTED, "capacity functions are not in this build");
+    if (!(dx > 0.0) || !(dy > 0.0)) return fail(CLAW2_EINVAL, "dx, dy must be positive");
+    int rc = check_method(method[1], method[2], mthlim, mwaves, use_fwave);
+    if (rc) return rc;
+
+    std::lock_guard<std::mutex> lock(g_scr.mu);
+    const Layout L = make_layout(mx, my);
+    const size_t nplanes = (size_t)meqn * L.plane;
+    const size_t nstage = (size_t)meqn * (mx + 4) * (my + 4);
+    rc = scratch_reserve(nplanes, nstage);
+    if (rc) return rc;
+    cudaStream_t st = g_scr.st;
+
+    CUDA_TRY(cudaMemcpyAsync(g_scr.stage, qold, nstage * 8, cudaMemcpyHostToDevice, st));
+    k_aos_to_planes<<<grid_blocks((long long)(mx + 4) * (my + 4)), 256, 0, st>>>(g_scr.stage, g_scr.a, L, meqn, 2);
+    CUDA_TRY(cudaMemsetAsync(g_scr.cfl, 0, sizeof(unsigned long long), st));
+    CUDA_TRY(cudaMemsetAsync(g_scr.status, 0, sizeof(int), st));
+
+    StepArgs a;
+    a.L = L;
+    a.dtdx = dt / dx;
+    a.dtdy = dt / dy;
+    a.H = 0;
+    a.rp = make_params(rp, cparam, ncparam);
+    a.meth.order = method[1];
+    a.meth.transverse = method[2];
+    a.meth.fwave = use_fwave;
+    for (int k = 0; k < CLAW2_MAX_WAVES; ++k) a.meth.mthlim[k] = k < mwaves ? mthlim[k] : 0;
+    a.cfl_bits = g_scr.cfl;
+    a.status = g_scr.status;
+
+    a.qold = g_scr.a;
+    a.qnew = g_scr.b;
+    const int bad = (ids == 0) ? dispatch<UnsplitF>(rp, a, st) : dispatch<SplitF>(rp, a, a, st, ids);
+    if (bad) return fail(CLAW2_EINVAL, "unknown Riemann solver id %d", rp);
+    CUDA_TRY(cudaGetLastError());
+    k_planes_to_aos<<<grid_blocks((long long)(mx + 4) * (my + 4)), 256, 0, st>>>(g_scr.b, g_scr.stage, L, meqn, 2);
+    CUDA_TRY(cudaGetLastError());
+    unsigned long long bits = 0;
+    int status = 0;
+    CUDA_TRY(cudaMemcpyAsync(&bits, g_scr.cfl, sizeof bits, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(&status, g_scr.status, sizeof status, cudaMemcpyDeviceToHost, st));
+    if (ids == 1) {
+        // the x-sweep of the split step updates every row, ghost rows included,
+        // and leaves ghost columns as they were: the whole qbc is the result
+        CUDA_TRY(cudaMemcpyAsync(qnew, g_scr.stage, nstage * 8, cudaMemcpyDeviceToHost, st));
+    } else {
+        // interior cells only; ghost cells of qnew keep their entry values
+        const size_t rowb = (size_t)meqn * (mx + 4) * 8;
+        const size_t off = (size_t)meqn * ((size_t)(mx + 4) * 2 + 2);
+        CUDA_TRY(cudaMemcpy2DAsync(qnew + off, rowb, g_scr.stage + off, rowb, (size_t)meqn * mx * 8, my,
+                                   cudaMemcpyDeviceToHost, st));
+    }
+    CUDA_TRY(cudaStreamSynchronize(st));
+    double c;
+    std::memcpy(&c, &bits, sizeof c);
+    *cfl = c;
+    if (status & 1) return fail(CLAW2_ENONFINITE, "the step produced a non-finite value");
+    return CLAW2_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// Device-resident patch
+// ===========================================================================
+struct claw2_patch {
+    claw2_desc d;
+    Layout L;
+    RPParams rp;
+    Method meth;
+    int device = 0;
+    double* q[2] = {nullptr, nullptr};  // current / pending (ping-pong)
+    double* tmp = nullptr;              // intermediate of the split step
+    double* stage = nullptr;            // AoS staging for host copies
+    unsigned long long* cfl = nullptr;
+    int* status = nullptr;
+    unsigned long long* h_cfl = nullptr;  // pinned
+    int* h_status = nullptr;              // pinned
+    cudaStream_t st = nullptr;      // the stream work is issued on
+    cudaStream_t own_st = nullptr;  // the patch's own stream
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    bool timing = false;
+    int cur = 0;
+    bool pending = false;
+};
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+StepArgs patch_args(claw2_patch* p, double dt) {
+    StepArgs a;
+    a.L = p->L;
+    a.dtdx = dt / p->d.dx;
+    a.dtdy = dt / p->d.dy;
+    a.H = 0;
+    a.rp = p->rp;
+    a.meth = p->meth;
+    a.cfl_bits = p->cfl;
+    a.status = p->status;
+    a.qold = p->q[p->cur];
+    a.qnew = p->q[p->cur ^ 1];
+    return a;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* claw2_last_error(void) { return g_err.c_str(); }
+const char* claw2_version(void) { return "claw2 0.1 (sm_100a, FP64)"; }
+
+int claw2_step2(int maxm, int num_eqn, int num_waves, int num_aux, int num_ghost, int mx, int my,
+                const double* qold, double* qnew, const double* aux, double dx, double dy, double dt,
+                const int* method, const int* mthlim, double* cfl, int use_fwave, int riemann,
+                const double* cparam, int ncparam) {
+    (void)aux;
+    if (method && method[2] < 0)
+        return fail(CLAW2_EINVAL, "method(3) = -1 selects the split step: call claw2_step2ds");
+    return host_step(maxm, num_eqn, num_waves, num_aux, num_ghost, mx, my, qold, qnew, dx, dy, dt, method,
+                     mthlim, cfl, 0, use_fwave, riemann, cparam, ncparam);
+}
+
+int claw2_step2ds(int maxm, int num_eqn, int num_waves, int num_aux, int num_ghost, int mx, int my,
+                  const double* qold, double* qnew, const double* aux, double dx, double dy, double dt,
+                  const int* method, const int* mthlim, double* cfl, int ids, int use_fwave, int riemann,
+                  const double* cparam, int ncparam) {
+    (void)aux;
+    if (ids != 1 && ids != 2) return fail(CLAW2_EINVAL, "ids must be 1 or 2 (got %d)", ids);
+    return host_step(maxm, num_eqn, num_waves, num_aux, num_ghost, mx, my, qold, qnew, dx, dy, dt, method,
+                     mthlim, cfl, ids, use_fwave, riemann, cparam, ncparam);
+}
+
+int claw2_bc_fill(int num_eqn, int num_ghost, int mx, int my, double* qbc, const int* bcl, const int* bcu) {
+    if (!qbc || !bcl || !bcu) return fail(CLAW2_EINVAL, "null pointer argument");
+    if (num_ghost != 2 || mx < 1 || my < 1 || num_eqn < 1)
+        return fail(CLAW2_EINVAL, "bad sizes num_eqn=%d num_ghost=%d mx=%d my=%d", num_eqn, num_ghost, mx, my);
+    int rc = check_bc(bcl, bcu, mx, my);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lock(g_scr.mu);
+    const Layout L = make_layout(mx, my);
+    const size_t nplanes = (size_t)num_eqn * L.plane;
+    const size_t nstage = (size_t)num_eqn * (mx + 4) * (my + 4);
+    rc = scratch_reserve(nplanes, nstage);
+    if (rc) return rc;
+    cudaStream_t st = g_scr.st;
+    CUDA_TRY(cudaMemcpyAsync(g_scr.stage, qbc, nstage * 8, cudaMemcpyHostToDevice, st));
+    k_aos_to_planes<<<grid_blocks((long long)(mx + 4) * (my + 4)), 256, 0, st>>>(g_scr.stage, g_scr.a, L, num_eqn, 2);
+    launch_bc(g_scr.a, L, num_eqn, bcl, bcu, nullptr, st);
+    k_planes_to_aos<<<grid_blocks((long long)(mx + 4) * (my + 4)), 256, 0, st>>>(g_scr.a, g_scr.stage, L, num_eqn, 2);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(qbc, g_scr.stage, nstage * 8, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return CLAW2_OK;
+}
+
+int claw2_patch_create(const claw2_desc* d, claw2_patch** out) {
+    if (!d || !out) return fail(CLAW2_EINVAL, "null pointer argument");
+    *out = nullptr;
+    int me = 0, mw = 0;
+    if (rp_shape(d->riemann, &me, &mw) != 0) return fail(CLAW2_EINVAL, "unknown Riemann solver id %d", d->riemann);
+    if (d->num_eqn != me || d->num_waves != mw)
+        return fail(CLAW2_EINVAL, "solver %d has num_eqn=%d num_waves=%d (got %d, %d)", d->riemann, me, mw,
+                    d->num_eqn, d->num_waves);
+    if (d->num_ghost != 2) return fail(CLAW2_EINVAL, "num_ghost must be 2 (got %d)", d->num_ghost);
+    if (d->num_aux != 0) return fail(CLAW2_EUNSUPPORTED, "aux arrays are not in this build");
+    if (d->mx < 1 || d->my < 1) return fail(CLAW2_EINVAL, "bad sizes mx=%d my=%d", d->mx, d->my);
+    if (!(d->dx > 0.0) || !(d->dy > 0.0)) return fail(CLAW2_EINVAL, "dx, dy must be positive");
+    const int trans = d->dimensional_split ? -1 : d->transverse;
+    int rc = check_method(d->order, trans, d->mthlim, mw, d->fwave);
+    if (rc) return rc;
+    rc = check_bc(d->bc_lower, d->bc_upper, d->mx, d->my);
+    if (rc) return rc;
+    int ndev = 0;
+    CUDA_TRY(cudaGetDeviceCount(&ndev));
+    if (d->device < 0 || d->device >= ndev) return fail(CLAW2_EINVAL, "device %d not present", d->device);
+
+    claw2_patch* p = new claw2_patch();
+    p->d = *d;
+    p->device = d->device;
+    p->L = make_layout(d->mx, d->my);
+    p->rp = make_params(d->riemann, d->cparam, d->ncparam);
+    p->meth.order = d->order;
+    p->meth.transverse = trans;
+    p->meth.fwave = d->fwave;
+    for (int k = 0; k < CLAW2_MAX_WAVES; ++k) p->meth.mthlim[k] = k < mw ? d->mthlim[k] : 0;
+    DeviceGuard g(p->device);
+    const size_t nb = (size_t)me * p->L.plane * 8;
+    const size_t ns = (size_t)me * d->mx * d->my * 8;
+    bool ok = cudaMalloc(&p->q[0], nb) == cudaSuccess && cudaMalloc(&p->q[1], nb) == cudaSuccess &&
+              cudaMalloc(&p->stage, ns) == cudaSuccess &&
+              cudaMalloc(&p->cfl, sizeof(unsigned long long)) == cudaSuccess &&
+              cudaMalloc(&p->status, sizeof(int)) == cudaSuccess &&
+              cudaMallocHost(&p->h_cfl, sizeof(unsigned long long)) == cudaSuccess &&
+              cudaMallocHost(&p->h_status, sizeof(int)) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&p->own_st, cudaStreamNonBlocking) == cudaSuccess;
+    p->st = p->own_st;
+    if (ok && d->dimensional_split) ok = cudaMalloc(&p->tmp, nb) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        claw2_patch_destroy(p);
+        return fail(CLAW2_ENOMEM, "device allocation for a %dx%d patch failed", d->mx, d->my);
+    }
+    // zero everything once so padding and ghost cells are defined
+    cudaMemsetAsync(p->q[0], 0, nb, p->st);
+    cudaMemsetAsync(p->q[1], 0, nb, p->st);
+    if (p->tmp) cudaMemsetAsync(p->tmp, 0, nb, p->st);
+    cudaMemsetAsync(p->cfl, 0, sizeof(unsigned long long), p->st);
+    cudaMemsetAsync(p->status, 0, sizeof(int), p->st);
+    if (cudaStreamSynchronize(p->st) != cudaSuccess) {
+        claw2_patch_destroy(p);
+        return fail(CLAW2_ECUDA, "patch initialisation failed");
+    }
+    *out = p;
+    return CLAW2_OK;
+}
+
+int claw2_patch_destroy(claw2_patch* p) {
+    if (!p) return CLAW2_OK;
+    {
+        DeviceGuard g(p->device);
+        if (p->st) cudaStreamSynchronize(p->st);
+        cudaFree(p->q[0]);
+        cudaFree(p->q[1]);
+        cudaFree(p->tmp);
+        cudaFree(p->stage);
+        cudaFree(p->cfl);
+        cudaFree(p->status);
+        cudaFreeHost(p->h_cfl);
+        cudaFreeHost(p->h_status);
+        if (p->ev0) cudaEventDestroy(p->ev0);
+        if (p->ev1) cudaEventDestroy(p->ev1);
+        if (p->own_st) cudaStreamDestroy(p->own_st);
+    }
+    delete p;
+    return CLAW2_OK;
+}
+
+int claw2_patch_set_cparam(claw2_patch* p, const double* cparam, int n) {
+    if (!p) return fail(CLAW2_EINVAL, "null patch");
+    if (n < 0 || n > CLAW2_MAX_PARAMS) return fail(CLAW2_EINVAL, "ncparam %d out of range", n);
+    p->rp = make_params(p->d.riemann, cparam, n);
+    return CLAW2_OK;
+}
+
+int claw2_patch_upload_q(claw2_patch* p, const double* q) {
+    if (!p || !q) return fail(CLAW2_EINVAL, "null pointer argument");
+    DeviceGuard g(p->device);
+    const size_t n = (size_t)p->d.num_eqn * p->d.mx * p->d.my;
+    CUDA_TRY(cudaMemcpyAsync(p->stage, q, n * 8, cudaMemcpyHostToDevice, p->st));
+    k_aos_to_planes<<<grid_blocks((long long)p->d.mx * p->d.my), 256, 0, p->st>>>(p->stage, p->q[p->cur], p->L,
+                                                                                   p->d.num_eqn, 0);
+    CUDA_TRY(cudaGetLastError());
+    p->pending = false;
+    return CLAW2_OK;
+}
+
+int claw2_patch_download_q(claw2_patch* p, double* q) {
+    if (!p || !q) return fail(CLAW2_EINVAL, "null pointer argument");
+    DeviceGuard g(p->device);
+    const size_t n = (size_t)p->d.num_eqn * p->d.mx * p->d.my;
+    k_planes_to_aos<<<grid_blocks((long long)p->d.mx * p->d.my), 256, 0, p->st>>>(p->q[p->cur], p->stage, p->L,
+                                                                                   p->d.num_eqn, 0);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(q, p->stage, n * 8, cudaMemcpyDeviceToHost, p->st));
+    CUDA_TRY(cudaStreamSynchronize(p->st));
+    return CLAW2_OK;
+}
+
+int claw2_patch_step(claw2_patch* p, double dt, double* cfl) {
+    if (!p) return fail(CLAW2_EINVAL, "null patch");
+    if (!(dt >= 0.0) || !std::isfinite(dt)) return fail(CLAW2_EINVAL, "dt must be finite and >= 0");
+    DeviceGuard g(p->device);
+    double* qc = p->q[p->cur];
+    launch_bc(qc, p->L, p->d.num_eqn, p->d.bc_lower, p->d.bc_upper, p->cfl, p->st);
+    StepArgs a = patch_args(p, dt);
+    if (p->timing) CUDA_TRY(cudaEventRecord(p->ev0, p->st));
+    if (p->d.dimensional_split) {
+        StepArgs ax = a, ay = a;
+        ax.qnew = p->tmp;
+        ay.qold = p->tmp;
+        dispatch<SplitF>(p->d.riemann, ax, ay, p->st, 3);
+    } else {
+        dispatch<UnsplitF>(p->d.riemann, a, p->st);
+    }
+    if (p->timing) CUDA_TRY(cudaEventRecord(p->ev1, p->st));
+    CUDA_TRY(cudaGetLastError());
+    p->pending = true;
+    if (cfl) return claw2_patch_cfl(p, cfl);
+    return CLAW2_OK;
+}
+
+int claw2_patch_accept(claw2_patch* p, int accept) {
+    if (!p) return fail(CLAW2_EINVAL, "null patch");
+    if (!p->pending) return fail(CLAW2_EINVAL, "no pending step to accept or reject");
+    if (accept) p->cur ^= 1;
+    p->pending = false;
+    return CLAW2_OK;
+}
+
+int claw2_patch_cfl(claw2_patch* p, double* cfl) {
+    if (!p || !cfl) return fail(CLAW2_EINVAL, "null pointer argument");
+    DeviceGuard g(p->device);
+    CUDA_TRY(cudaMemcpyAsync(p->h_cfl, p->cfl, sizeof(unsigned long long), cudaMemcpyDeviceToHost, p->st));
+    CUDA_TRY(cudaMemcpyAsync(p->h_status, p->status, sizeof(int), cudaMemcpyDeviceToHost, p->st));
+    CUDA_TRY(cudaStreamSynchronize(p->st));
+    double c;
+    std::memcpy(&c, p->h_cfl, sizeof c);
+    *cfl = c;
+    if (*p->h_status & 1) {
+        cudaMemsetAsync(p->status, 0, sizeof(int), p->st);
+        return fail(CLAW2_ENONFINITE, "the step produced a non-finite value");
+    }
+    return CLAW2_OK;
+}
+
+int claw2_patch_sync(claw2_patch* p) {
+    if (!p) return fail(CLAW2_EINVAL, "null patch");
+    DeviceGuard g(p->device);
+    CUDA_TRY(cudaMemcpyAsync(p->h_status, p->status, sizeof(int), cudaMemcpyDeviceToHost, p->st));
+    CUDA_TRY(cudaStreamSynchronize(p->st));
+    if (*p->h_status & 1) {
+        cudaMemsetAsync(p->status, 0, sizeof(int), p->st);
+        return fail(CLAW2_ENONFINITE, "a step produced a non-finite value");
+    }
+    return CLAW2_OK;
+}
+
+int claw2_patch_set_stream(claw2_patch* p, void* stream) {
+    if (!p) return fail(CLAW2_EINVAL, "null patch");
+    DeviceGuard g(p->device);
+    CUDA_TRY(cudaStreamSynchronize(p->st));
+    p->st = stream ? (cudaStream_t)stream : p->own_st;
+    return CLAW2_OK;
+}
+
+int claw2_patch_set_timing(claw2_patch* p, int on) {
+    if (!p) return fail(CLAW2_EINVAL, "null patch");
+    DeviceGuard g(p->device);
+    if (on && !p->ev0) {
+        CUDA_TRY(cudaEventCreate(&p->ev0));
+        CUDA_TRY(cudaEventCreate(&p->ev1));
+    }
+    p->timing = on != 0;
+    return CLAW2_OK;
+}
+
+int claw2_patch_kernel_ms(claw2_patch* p, float* ms) {
+    if (!p || !ms) return fail(CLAW2_EINVAL, "null pointer argument");
+    if (!p->timing) return fail(CLAW2_EINVAL, "timing is off (claw2_patch_set_timing)");
+    DeviceGuard g(p->device);
+    CUDA_TRY(cudaEventSynchronize(p->ev1));
+    CUDA_TRY(cudaEventElapsedTime(ms, p->ev0, p->ev1));
+    return CLAW2_OK;
+}
+
+int claw2_probe_fp64(int device, double* tflops) {
+    if (!tflops) return fail(CLAW2_EINVAL, "null pointer argument");
+    DeviceGuard g(device);
+    int nsm = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+    const int blocks = nsm * 8, threads = 256, iters = 4096;
+    double* out = nullptr;
+    CUDA_TRY(cudaMalloc(&out, sizeof(double) * blocks * threads));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    k_fp64_fma<<<blocks, threads>>>(out, iters, 1.0000001);  // warm-up
+    cudaEventRecord(e0);
+    k_fp64_fma<<<blocks, threads>>>(out, iters, 1.0000001);
+    cudaEventRecord(e1);
+    cudaError_t e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    if (e != cudaSuccess) return fail(CLAW2_ECUDA, "fp64 probe failed: %s", cudaGetErrorString(e));
+    const double flops = 2.0 * 16.0 * iters * (double)blocks * threads;
+    *tflops = flops / (ms * 1e-3) / 1e12;
+    return CLAW2_OK;
+}
+
+int claw2_patch_device_q(claw2_patch* p, double** q, long long* layout) {
+    if (!p || !q || !layout) return fail(CLAW2_EINVAL, "null pointer argument");
+    *q = p->q[p->cur];
+    layout[0] = p->d.mx + 4;
+    layout[1] = p->d.my + 4;
+    layout[2] = p->L.pitch;
+    layout[3] = p->L.plane;
+    return CLAW2_OK;
+}
+
+}  // extern "C"

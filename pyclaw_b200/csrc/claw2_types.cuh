@@ -1,0 +1,36 @@
+// claw2_types.cuh -- plain-old-data types shared by the kernels and the C-ABI.
+#pragma once
+
+#include <cstdint>
+
+#include "../../include/claw2.h"
+
+namespace claw2 {
+
+// Riemann-solver parameters (the reference's Fortran COMMON /cparam/,
+// src/pyclaw/state.py:206-231), passed by value into every launch.
+struct RPParams {
+    double c[CLAW2_MAX_PARAMS];
+    int flags;  // solver switch, e.g. the entropy fix of the Roe solvers
+};
+
+// Method switches (src/pyclaw/classic/solver.py:173-193: method(2), method(3))
+// and the per-wave limiter codes (mthlim, limiter.f90 / philim.f90).
+struct Method {
+    int order;       // 1 = Godunov, 2 = high-resolution corrections
+    int transverse;  // 0 none, 1 increment waves, 2 increment + correction waves
+    int fwave;       // 1 if waves are f-waves (sign(s) instead of |s| in cqxx)
+    int mthlim[CLAW2_MAX_WAVES];
+};
+
+// Device grid layout: structure-of-arrays planes, one per component.
+// Element (m, c, r) with padded column c in [0, mx+4) and padded row r in
+// [0, my+4) is at base[m * plane + r * pitch + c].  Padded index = Fortran
+// index + 1 (num_ghost = 2): padded 0,1 are the lower ghost cells.
+struct Layout {
+    int mx, my;       // interior cells
+    int pitch;        // doubles per row (>= mx + 4, multiple of 32)
+    long long plane;  // doubles per component plane
+};
+
+}  // namespace claw2

@@ -1,0 +1,709 @@
+// step_kernels.cuh -- the classic 2D wave-propagation step on sm_100a.
+//
+// Reference: src/pyclaw/classic/step2.f90:74-247 (unsplit), step2ds.f90:72-261
+// (split), flux2.f90:82-204, limiter.f90:29-53, philim.f90:16-35.
+//
+// Design ("column march").  A CTA owns a strip of NT padded columns and a
+// block of H interior rows.  Thread t owns padded column cp = strip*W + t,
+// W = NT - 4 (2 halo columns each side).  The CTA marches down the rows; at
+// row R every thread
+//   * solves the x-interface between (cp-1, R) and (cp, R)   [rpn2, ixy = 1]
+//   * solves the y-interface between (cp, R-1) and (cp, R)    [rpn2, ixy = 2]
+//   * finishes the y-interface between (cp, R-2) and (cp, R-1) (limiter with
+//     the waves below and above it, second-order correction, rpt2 x 2)
+//   * finishes its x-interface (limiter with the neighbours' waves, read from
+//     shared memory; correction; rpt2 x 2)
+//   * routes every increment to the cell that receives it: its own column's
+//     increments stay in registers (4 rows in flight), the left/right
+//     neighbours' go through shared memory,
+// and writes qnew for row R-2, whose increments are then complete.  Every
+// interface is solved once per CTA; the only recomputation is the 2-column
+// halo of the strip and 2-3 halo rows of the row block.
+//
+// The reference reads qold for both sweeps (step2.f90:97,177), so the x and y
+// increments are independent and one pass over qold gives exactly its update;
+// only the order in which the increments of a cell are summed differs.
+#pragma once
+
+#include "riemann.cuh"
+
+namespace claw2 {
+
+struct StepArgs {
+    const double* __restrict__ qold;
+    double* __restrict__ qnew;
+    Layout L;
+    double dtdx, dtdy;
+    int H;  // interior rows per CTA
+    RPParams rp;
+    Method meth;
+    unsigned long long* cfl_bits;  // atomicMax of non-negative double bit patterns
+    int* status;                   // bit 0: non-finite output
+};
+
+// philim.f90:16-35
+__device__ __forceinline__ double philim(double a, double b, int meth) {
+    const double r = b / a;
+    switch (meth) {
+        case 1: return fmax(0.0, fmin(1.0, r));
+        case 2: return fmax(0.0, fmax(fmin(1.0, 2.0 * r), fmin(2.0, r)));
+        case 3: return (r + fabs(r)) / (1.0 + fabs(r));
+        case 4: return fmax(0.0, fmin((1.0 + r) / 2.0, fmin(2.0, 2.0 * r)));
+        case 5: return r;
+        default: return 0.0;
+    }
+}
+
+__device__ __forceinline__ void cfl_commit(double cfl, double* s_red, unsigned long long* slot) {
+    // warp max, then block max, then one 64-bit atomicMax per CTA
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cfl = fmax(cfl, __shfl_xor_sync(0xffffffffu, cfl, o));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) s_red[warp] = cfl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, s_red[w]);
+        // non-negative doubles order like their bit patterns
+        atomicMax(slot, (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+template <int ME>
+__device__ __forceinline__ bool all_finite(const double (&v)[ME]) {
+    bool ok = true;
+#pragma unroll
+    for (int m = 0; m < ME; ++m) ok = ok && isfinite(v[m]);
+    return ok;
+}
+
+// ---------------------------------------------------------------------------
+// Unsplit step (step2.f90), fused x + y sweeps.
+// ---------------------------------------------------------------------------
+template <class RP, int NT>
+struct UnsplitSmem {
+    static constexpr int ME = RP::MEQN, MW = RP::MWAVES;
+    double q[2][ME][NT];   // q of row R (double-buffered by row parity)
+    double w[MW][ME][NT];  // unlimited x-waves of row R
+    double xl[3][ME][NT];  // x-interface increments for column cp-1: rows R, R-1, R+1
+    double yl[2][ME][NT];  // y-interface increments for column cp-1: rows R-2, R-1
+    double yr[2][ME][NT];  // y-interface increments for column cp+1: rows R-2, R-1
+    double red[NT / 32];
+};
+
+template <class RP, int NT>
+__global__ void __launch_bounds__(NT) k_step_unsplit(const StepArgs a) {
+    constexpr int ME = RP::MEQN, MW = RP::MWAVES, W = NT - 4;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    UnsplitSmem<RP, NT>& S = *reinterpret_cast<UnsplitSmem<RP, NT>*>(smem_raw);
+
+    const int t = threadIdx.x;
+    const int mx = a.L.mx, my = a.L.my;
+    const int pitch = a.L.pitch;
+    const long long plane = a.L.plane;
+    const int cp = blockIdx.x * W + t;
+    const int cpl = min(cp, mx + 3);
+    const int rb = blockIdx.y * a.H;
+    const int Hb = min(a.H, my - rb);
+    const int R0 = rb, R1 = rb + Hb + 3;
+    const bool out_col = (t >= 2) && (t < W + 2) && (cp <= mx + 1);
+    const bool xcfl_col = (t >= 2) && (t <= W + 2) && (cp <= mx + 2);
+    const bool ycfl_col = (t >= 1) && (t <= W + 2) && (cp <= mx + 2);
+    const int tl = (t > 0) ? t - 1 : 0;
+    const int tr = (t < NT - 1) ? t + 1 : NT - 1;
+    const double dtdx = a.dtdx, dtdy = a.dtdy;
+    const int order = a.meth.order, trans = a.meth.transverse;
+    const bool fw = a.meth.fwave != 0;
+    const bool tc = (order > 1) && (trans == 2);
+    const double* qo = a.qold + cpl;
+    double* qn = a.qnew + cpl;
+
+    double q0[ME], q1[ME], q2[ME], pf[ME];
+    double accA[ME], accB[ME], accC[ME], accD[ME];  // rows R-2, R-1, R, R+1
+    double wY[MW][ME], sY[MW], amY[ME], apY[ME], dY[MW];  // y-interface between R-2 and R-1
+    typename RP::Cache cY;
+    double cfl = 0.0;
+
+#pragma unroll
+    for (int m = 0; m < ME; ++m) {
+        pf[m] = __ldg(qo + m * plane + (long long)R0 * pitch);
+        q0[m] = q1[m] = q2[m] = pf[m];
+        accA[m] = accB[m] = accC[m] = accD[m] = 0.0;
+        amY[m] = apY[m] = 0.0;
+    }
+#pragma unroll
+    for (int mw = 0; mw < MW; ++mw) {
+        sY[mw] = 0.0;
+        dY[mw] = 0.0;
+#pragma unroll
+        for (int m = 0; m < ME; ++m) wY[mw][m] = 0.0;
+    }
+
+    for (int R = R0; R <= R1; ++R) {
+        // ---- rotate the q window and prefetch the next row ----
+#pragma unroll
+        for (int m = 0; m < ME; ++m) {
+            q0[m] = q1[m];
+            q1[m] = q2[m];
+            q2[m] = pf[m];
+        }
+        if (R < R1) {
+#pragma unroll
+            for (int m = 0; m < ME; ++m) pf[m] = __ldg(qo + m * plane + (long long)(R + 1) * pitch);
+        }
+        const int buf = R & 1;
+#pragma unroll
+        for (int m = 0; m < ME; ++m) S.q[buf][m][t] = q2[m];
+        __syncthreads();  // S1: row R visible; previous exchange fully consumed
+
+        // ---- y: solve the interface (R-1 | R), finish (R-2 | R-1) ----
+        {
+            double wN[MW][ME], sN[MW], amN[ME], apN[ME];
+            typename RP::Cache cN;
+            RP::template rpn2<2>(q1, q2, a.rp, wN, sN, amN, apN, cN);
+            double dn[MW];
+#pragma unroll
+            for (int mw = 0; mw < MW; ++mw) {
+                double d = 0.0;
+#pragma unroll
+                for (int m = 0; m < ME; ++m) d = d + wY[mw][m] * wN[mw][m];
+                dn[mw] = d;
+            }
+            double ylB[ME], ylA[ME], yrB[ME], yrA[ME];
+#pragma unroll
+            for (int m = 0; m < ME; ++m) ylB[m] = ylA[m] = yrB[m] = yrA[m] = 0.0;
+            if (R >= R0 + 3) {
+                if (ycfl_col) {
+#pragma unroll
+                    for (int mw = 0; mw < MW; ++mw) cfl = fmax(cfl, fabs(dtdy * sY[mw]));
+                }
+                double cq[ME];
+#pragma unroll
+                for (int m = 0; m < ME; ++m) cq[m] = 0.0;
+                if (order != 1) {
+#pragma unroll
+                    for (int mw = 0; mw < MW; ++mw) {
+                        const int lim = a.meth.mthlim[mw];
+                        double wn2 = 0.0;
+#pragma unroll
+                        for (int m = 0; m < ME; ++m) wn2 = wn2 + wY[mw][m] * wY[mw][m];
+                        double phi = 1.0;
+                        if (lim != 0 && wn2 != 0.0) phi = philim(wn2, (sY[mw] > 0.0) ? dY[mw] : dn[mw], lim);
+                        const double as = fabs(sY[mw]);
+                        const double coef = (fw ? copysign(1.0, sY[mw]) : as) * (1.0 - as * dtdy);
+#pragma unroll
+                        for (int m = 0; m < ME; ++m) cq[m] = cq[m] + coef * (phi * wY[mw][m]);
+                    }
+                }
+#pragma unroll
+                for (int m = 0; m < ME; ++m) {
+                    const double f = 0.5 * cq[m];
+                    accA[m] = accA[m] - dtdy * (amY[m] + f);
+                    accB[m] = accB[m] - dtdy * (apY[m] - f);
+                }
+                if (trans > 0) {
+                    double as2[ME], bm[ME], bp[ME];
+                    const double h = 0.5 * dtdy;
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) as2[m] = tc ? amY[m] + cq[m] : amY[m];
+                    RP::template rpt2<2>(cY, a.rp, as2, bm, bp);  // imp = 1 -> row R-2
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) {
+                        const double gb = h * bm[m], ga = h * bp[m];
+                        accA[m] = accA[m] + dtdx * (ga - gb);
+                        ylB[m] = dtdx * gb;
+                        yrB[m] = -dtdx * ga;
+                    }
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) as2[m] = tc ? apY[m] - cq[m] : apY[m];
+                    RP::template rpt2<2>(cY, a.rp, as2, bm, bp);  // imp = 2 -> row R-1
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) {
+                        const double gb = h * bm[m], ga = h * bp[m];
+                        accB[m] = accB[m] + dtdx * (ga - gb);
+                        ylA[m] = dtdx * gb;
+                        yrA[m] = -dtdx * ga;
+                    }
+                }
+            }
+#pragma unroll
+            for (int m = 0; m < ME; ++m) {
+                S.yl[0][m][t] = ylB[m];
+                S.yl[1][m][t] = ylA[m];
+                S.yr[0][m][t] = yrB[m];
+                S.yr[1][m][t] = yrA[m];
+            }
+            // shift the pipeline: (R-1 | R) becomes the pending interface
+#pragma unroll
+            for (int mw = 0; mw < MW; ++mw) {
+                sY[mw] = sN[mw];
+                dY[mw] = dn[mw];
+#pragma unroll
+                for (int m = 0; m < ME; ++m) wY[mw][m] = wN[mw][m];
+            }
+#pragma unroll
+            for (int m = 0; m < ME; ++m) { amY[m] = amN[m]; apY[m] = apN[m]; }
+            cY = cN;
+        }
+
+        // ---- x: the interface between (cp-1, R) and (cp, R) ----
+        const bool xrow = (R > R0) && (R < R1);  // rows R0+1 .. R1-1
+        double wX[MW][ME], sX[MW], amX[ME], apX[ME];
+        typename RP::Cache cX;
+        {
+            double qL[ME];
+#pragma unroll
+            for (int m = 0; m < ME; ++m) qL[m] = S.q[buf][m][tl];
+            RP::template rpn2<1>(qL, q2, a.rp, wX, sX, amX, apX, cX);
+        }
+#pragma unroll
+        for (int mw = 0; mw < MW; ++mw)
+#pragma unroll
+            for (int m = 0; m < ME; ++m) S.w[mw][m][t] = wX[mw][m];
+        __syncthreads();  // S2: x-waves of row R visible
+
+        {
+            double xcL[ME], xbL[ME], xaL[ME];
+#pragma unroll
+            for (int m = 0; m < ME; ++m) xcL[m] = xbL[m] = xaL[m] = 0.0;
+            if (xrow) {
+                if (xcfl_col) {
+#pragma unroll
+                    for (int mw = 0; mw < MW; ++mw) cfl = fmax(cfl, fabs(dtdx * sX[mw]));
+                }
+                double cq[ME];
+#pragma unroll
+                for (int m = 0; m < ME; ++m) cq[m] = 0.0;
+                if (order != 1) {
+#pragma unroll
+                    for (int mw = 0; mw < MW; ++mw) {
+                        const int lim = a.meth.mthlim[mw];
+                        double wn2 = 0.0, dl = 0.0, dr = 0.0;
+#pragma unroll
+                        for (int m = 0; m < ME; ++m) {
+                            const double w = wX[mw][m];
+                            wn2 = wn2 + w * w;
+                            dl = dl + S.w[mw][m][tl] * w;
+                            dr = dr + w * S.w[mw][m][tr];
+                        }
+                        double phi = 1.0;
+                        if (lim != 0 && wn2 != 0.0) phi = philim(wn2, (sX[mw] > 0.0) ? dl : dr, lim);
+                        const double as = fabs(sX[mw]);
+                        const double coef = (fw ? copysign(1.0, sX[mw]) : as) * (1.0 - as * dtdx);
+#pragma unroll
+                        for (int m = 0; m < ME; ++m) cq[m] = cq[m] + coef * (phi * wX[mw][m]);
+                    }
+                }
+#pragma unroll
+                for (int m = 0; m < ME; ++m) {
+                    const double f = 0.5 * cq[m];
+                    accC[m] = accC[m] - dtdx * (apX[m] - f);
+                    xcL[m] = -dtdx * (amX[m] + f);
+                }
+                if (trans > 0) {
+                    double as2[ME], bm[ME], bp[ME];
+                    const double h = 0.5 * dtdx;
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) as2[m] = tc ? amX[m] + cq[m] : amX[m];
+                    RP::template rpt2<1>(cX, a.rp, as2, bm, bp);  // imp = 1 -> column cp-1
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) {
+                        const double gb = h * bm[m], ga = h * bp[m];
+                        xcL[m] = xcL[m] + dtdy * (ga - gb);
+                        xbL[m] = dtdy * gb;
+                        xaL[m] = -dtdy * ga;
+                    }
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) as2[m] = tc ? apX[m] - cq[m] : apX[m];
+                    RP::template rpt2<1>(cX, a.rp, as2, bm, bp);  // imp = 2 -> column cp
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) {
+                        const double gb = h * bm[m], ga = h * bp[m];
+                        accC[m] = accC[m] + dtdy * (ga - gb);
+                        accB[m] = accB[m] + dtdy * gb;
+                        accD[m] = accD[m] - dtdy * ga;
+                    }
+                }
+            }
+#pragma unroll
+            for (int m = 0; m < ME; ++m) {
+                S.xl[0][m][t] = xcL[m];
+                S.xl[1][m][t] = xbL[m];
+                S.xl[2][m][t] = xaL[m];
+            }
+        }
+        __syncthreads();  // S3: neighbour increments visible
+#pragma unroll
+        for (int m = 0; m < ME; ++m) {
+            accA[m] = accA[m] + S.yl[0][m][tr] + S.yr[0][m][tl];
+            accB[m] = accB[m] + S.xl[1][m][tr] + S.yl[1][m][tr] + S.yr[1][m][tl];
+            accC[m] = accC[m] + S.xl[0][m][tr];
+            accD[m] = accD[m] + S.xl[2][m][tr];
+        }
+
+        // ---- row R-2 is complete ----
+        if (R >= R0 + 4 && out_col) {
+            double v[ME];
+#pragma unroll
+            for (int m = 0; m < ME; ++m) v[m] = q0[m] + accA[m];
+#pragma unroll
+            for (int m = 0; m < ME; ++m) qn[m * plane + (long long)(R - 2) * pitch] = v[m];
+            if (!all_finite<ME>(v)) atomicOr(a.status, 1);
+        }
+#pragma unroll
+        for (int m = 0; m < ME; ++m) {
+            accA[m] = accB[m];
+            accB[m] = accC[m];
+            accC[m] = accD[m];
+            accD[m] = 0.0;
+        }
+    }
+    cfl_commit(cfl, S.red, a.cfl_bits);
+}
+
+// ---------------------------------------------------------------------------
+// Split step, x-sweep (step2ds.f90:86-172): every padded row, no transverse
+// terms.  Writes the interior columns of qtmp and copies the ghost columns.
+// ---------------------------------------------------------------------------
+template <class RP, int NT>
+__global__ void __launch_bounds__(NT) k_split_x(const StepArgs a) {
+    constexpr int ME = RP::MEQN, MW = RP::MWAVES, W = NT - 4;
+    __shared__ double sQ[2][ME][NT];
+    __shared__ double sW[MW][ME][NT];
+    __shared__ double sXL[ME][NT];
+    __shared__ double sRed[NT / 32];
+
+    const int t = threadIdx.x;
+    const int mx = a.L.mx, my = a.L.my;
+    const int pitch = a.L.pitch;
+    const long long plane = a.L.plane;
+    const int cp = blockIdx.x * W + t;
+    const int cpl = min(cp, mx + 3);
+    const int rb = blockIdx.y * a.H;               // first padded row of this block
+    const int re = min(rb + a.H, my + 4);          // one past the last
+    const bool out_col = (t >= 2) && (t < W + 2) && (cp <= mx + 1);
+    const bool ghost_copy = (cp <= mx + 3) && ((cp < 2 && t == cp) || (cp >= mx + 2 && t >= 2));
+    const bool xcfl_col = (t >= 2) && (t <= W + 2) && (cp <= mx + 2);
+    const int tl = (t > 0) ? t - 1 : 0;
+    const int tr = (t < NT - 1) ? t + 1 : NT - 1;
+    const double dtdx = a.dtdx;
+    const bool fw = a.meth.fwave != 0;
+    const double* qo = a.qold + cpl;
+    double* qn = a.qnew + cpl;
+    double cfl = 0.0;
+
+    for (int R = rb; R < re; ++R) {
+        const int buf = R & 1;
+        double q[ME];
+#pragma unroll
+        for (int m = 0; m < ME; ++m) {
+            q[m] = __ldg(qo + m * plane + (long long)R * pitch);
+            sQ[buf][m][t] = q[m];
+        }
+        __syncthreads();
+        double wX[MW][ME], sX[MW], amX[ME], apX[ME];
+        typename RP::Cache cX;
+        {
+            double qL[ME];
+#pragma unroll
+            for (int m = 0; m < ME; ++m) qL[m] = sQ[buf][m][tl];
+            RP::template rpn2<1>(qL, q, a.rp, wX, sX, amX, apX, cX);
+        }
+#pragma unroll
+        for (int mw = 0; mw < MW; ++mw)
+#pragma unroll
+            for (int m = 0; m < ME; ++m) sW[mw][m][t] = wX[mw][m];
+        __syncthreads();
+        if (xcfl_col) {
+#pragma unroll
+            for (int mw = 0; mw < MW; ++mw) cfl = fmax(cfl, fabs(dtdx * sX[mw]));
+        }
+        double fX[ME];
+#pragma unroll
+        for (int m = 0; m < ME; ++m) fX[m] = 0.0;
+        if (a.meth.order != 1) {
+            double cq[ME];
+#pragma unroll
+            for (int m = 0; m < ME; ++m) cq[m] = 0.0;
+#pragma unroll
+            for (int mw = 0; mw < MW; ++mw) {
+                const int lim = a.meth.mthlim[mw];
+                double wn2 = 0.0, dl = 0.0, dr = 0.0;
+#pragma unroll
+                for (int m = 0; m < ME; ++m) {
+                    const double w = wX[mw][m];
+                    wn2 = wn2 + w * w;
+                    dl = dl + sW[mw][m][tl] * w;
+                    dr = dr + w * sW[mw][m][tr];
+                }
+                if (lim != 0 && wn2 != 0.0) {
+                    const double phi = philim(wn2, (sX[mw] > 0.0) ? dl : dr, lim);
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) wX[mw][m] = phi * wX[mw][m];
+                }
+                const double as = fabs(sX[mw]);
+                const double coef = (fw ? copysign(1.0, sX[mw]) : as) * (1.0 - as * dtdx);
+#pragma unroll
+                for (int m = 0; m < ME; ++m) cq[m] = cq[m] + coef * wX[mw][m];
+            }
+#pragma unroll
+            for (int m = 0; m < ME; ++m) fX[m] = 0.5 * cq[m];
+        }
+#pragma unroll
+        for (int m = 0; m < ME; ++m) sXL[m][t] = -dtdx * (amX[m] + fX[m]);
+        __syncthreads();
+        if (out_col) {
+            double v[ME];
+#pragma unroll
+            for (int m = 0; m < ME; ++m) {
+                v[m] = q[m] + (-dtdx * (apX[m] - fX[m]) + sXL[m][tr]);
+                qn[m * plane + (long long)R * pitch] = v[m];
+            }
+            if (!all_finite<ME>(v)) atomicOr(a.status, 1);
+        } else if (ghost_copy) {
+#pragma unroll
+            for (int m = 0; m < ME; ++m) qn[m * plane + (long long)R * pitch] = q[m];
+        }
+    }
+    cfl_commit(cfl, sRed, a.cfl_bits);
+}
+
+// ---------------------------------------------------------------------------
+// Split step, y-sweep (step2ds.f90:174-261): every padded column, one thread
+// per column marching down the rows; limiter neighbours come from the
+// register pipeline.  Writes the interior cells of qnew.
+// ---------------------------------------------------------------------------
+template <class RP, int NT>
+__global__ void __launch_bounds__(NT) k_split_y(const StepArgs a) {
+    constexpr int ME = RP::MEQN, MW = RP::MWAVES;
+    __shared__ double sRed[NT / 32];
+    const int mx = a.L.mx, my = a.L.my;
+    const int pitch = a.L.pitch;
+    const long long plane = a.L.plane;
+    const int cp = blockIdx.x * NT + threadIdx.x;
+    const int cpl = min(cp, mx + 3);
+    const bool valid = cp <= mx + 3;
+    const bool out_col = (cp >= 2) && (cp <= mx + 1);
+    const int rb = blockIdx.y * a.H;
+    const int Hb = min(a.H, my - rb);
+    const int R0 = rb, R1 = rb + Hb + 3;
+    const double dtdy = a.dtdy;
+    const bool fw = a.meth.fwave != 0;
+    const double* qo = a.qold + cpl;
+    double* qn = a.qnew + cpl;
+
+    double q0[ME], q1[ME], q2[ME], acc0[ME], acc1[ME];
+    double wY[MW][ME], sY[MW], amY[ME], apY[ME], dY[MW];
+    double cfl = 0.0;
+#pragma unroll
+    for (int m = 0; m < ME; ++m) {
+        q2[m] = __ldg(qo + m * plane + (long long)R0 * pitch);
+        q1[m] = q0[m] = q2[m];
+        acc0[m] = acc1[m] = 0.0;
+        amY[m] = apY[m] = 0.0;
+    }
+#pragma unroll
+    for (int mw = 0; mw < MW; ++mw) {
+        sY[mw] = dY[mw] = 0.0;
+#pragma unroll
+        for (int m = 0; m < ME; ++m) wY[mw][m] = 0.0;
+    }
+    for (int R = R0 + 1; R <= R1; ++R) {
+#pragma unroll
+        for (int m = 0; m < ME; ++m) {
+            q0[m] = q1[m];
+            q1[m] = q2[m];
+            q2[m] = __ldg(qo + m * plane + (long long)R * pitch);
+        }
+        double wN[MW][ME], sN[MW], amN[ME], apN[ME];
+        typename RP::Cache cN;
+        RP::template rpn2<2>(q1, q2, a.rp, wN, sN, amN, apN, cN);
+        double dn[MW];
+#pragma unroll
+        for (int mw = 0; mw < MW; ++mw) {
+            double d = 0.0;
+#pragma unroll
+            for (int m = 0; m < ME; ++m) d = d + wY[mw][m] * wN[mw][m];
+            dn[mw] = d;
+        }
+        // acc0 <-> row R-2, acc1 <-> row R-1
+        if (R >= R0 + 3) {
+            if (valid) {
+#pragma unroll
+                for (int mw = 0; mw < MW; ++mw) cfl = fmax(cfl, fabs(dtdy * sY[mw]));
+            }
+            double fY[ME];
+#pragma unroll
+            for (int m = 0; m < ME; ++m) fY[m] = 0.0;
+            if (a.meth.order != 1) {
+                double cq[ME];
+#pragma unroll
+                for (int m = 0; m < ME; ++m) cq[m] = 0.0;
+#pragma unroll
+                for (int mw = 0; mw < MW; ++mw) {
+                    const int lim = a.meth.mthlim[mw];
+                    double wn2 = 0.0;
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) wn2 = wn2 + wY[mw][m] * wY[mw][m];
+                    if (lim != 0 && wn2 != 0.0) {
+                        const double phi = philim(wn2, (sY[mw] > 0.0) ? dY[mw] : dn[mw], lim);
+#pragma unroll
+                        for (int m = 0; m < ME; ++m) wY[mw][m] = phi * wY[mw][m];
+                    }
+                    const double as = fabs(sY[mw]);
+                    const double coef = (fw ? copysign(1.0, sY[mw]) : as) * (1.0 - as * dtdy);
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) cq[m] = cq[m] + coef * wY[mw][m];
+                }
+#pragma unroll
+                for (int m = 0; m < ME; ++m) fY[m] = 0.5 * cq[m];
+            }
+#pragma unroll
+            for (int m = 0; m < ME; ++m) {
+                acc0[m] = acc0[m] - dtdy * (amY[m] + fY[m]);
+                acc1[m] = acc1[m] - dtdy * (apY[m] - fY[m]);
+            }
+        }
+        if (R >= R0 + 4 && out_col) {
+            double v[ME];
+#pragma unroll
+            for (int m = 0; m < ME; ++m) {
+                v[m] = q0[m] + acc0[m];
+                qn[m * plane + (long long)(R - 2) * pitch] = v[m];
+            }
+            if (!all_finite<ME>(v)) atomicOr(a.status, 1);
+        }
+#pragma unroll
+        for (int m = 0; m < ME; ++m) {
+            acc0[m] = acc1[m];
+            acc1[m] = 0.0;
+            amY[m] = amN[m];
+            apY[m] = apN[m];
+        }
+#pragma unroll
+        for (int mw = 0; mw < MW; ++mw) {
+            sY[mw] = sN[mw];
+            dY[mw] = dn[mw];
+#pragma unroll
+            for (int m = 0; m < ME; ++m) wY[mw][m] = wN[mw][m];
+        }
+    }
+    cfl_commit(cfl, sRed, a.cfl_bits);
+}
+
+// ---------------------------------------------------------------------------
+// Ghost-cell fill (solver.py:351-519) in one pass: a ghost cell takes its
+// value from the interior source its x rule and/or y rule name, with the
+// normal-momentum sign flips of a wall.  Sources are always interior cells, so
+// the fill runs in place.  Also clears the CFL word of the step that follows.
+// ---------------------------------------------------------------------------
+struct BCArgs {
+    double* q;
+    Layout L;
+    int meqn;
+    int bcl[2], bcu[2];
+    unsigned long long* cfl_bits;
+};
+
+__device__ __forceinline__ int bc_src(int c, int n, int lo, int up, bool& flip) {
+    // c padded index in [0, n+4); returns the padded source index
+    flip = false;
+    if (c < 2) {
+        if (lo == CLAW2_BC_EXTRAP) return 2;
+        if (lo == CLAW2_BC_PERIODIC) return c + n;
+        flip = true;
+        return 3 - c;  // wall
+    }
+    if (c >= n + 2) {
+        if (up == CLAW2_BC_EXTRAP) return n + 1;
+        if (up == CLAW2_BC_PERIODIC) return c - n;
+        flip = true;
+        return 2 * n + 3 - c;  // wall
+    }
+    return c;
+}
+
+__global__ void k_bc_fill(const BCArgs a) {
+    const int mx = a.L.mx, my = a.L.my;
+    const int nrow = 4 * (mx + 4);   // cells of the 4 ghost rows
+    const int ncol = 4 * my;         // ghost-column cells of interior rows
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k == 0 && a.cfl_bits) *a.cfl_bits = 0ull;
+    if (k >= nrow + ncol) return;
+    int c, r;
+    if (k < nrow) {
+        const int g = k / (mx + 4);
+        c = k - g * (mx + 4);
+        r = (g < 2) ? g : my + g;  // 0, 1, my+2, my+3
+    } else {
+        const int kk = k - nrow;
+        const int g = kk & 3;
+        r = 2 + (kk >> 2);
+        c = (g < 2) ? g : mx + g;
+    }
+    bool fx, fy;
+    const int cs = bc_src(c, mx, a.bcl[0], a.bcu[0], fx);
+    const int rs = bc_src(r, my, a.bcl[1], a.bcu[1], fy);
+    const long long src = (long long)rs * a.L.pitch + cs, dst = (long long)r * a.L.pitch + c;
+    for (int m = 0; m < a.meqn; ++m) {
+        double v = a.q[m * a.L.plane + src];
+        if (fx && m == 1) v = -v;
+        if (fy && m == 2) v = -v;
+        a.q[m * a.L.plane + dst] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Layout conversion between the host's Fortran-ordered arrays (component
+// fastest) and the device planes.  `ghost` = 2 when the host array is qbc
+// (with ghost cells), 0 when it is State.q (interior only).
+// ---------------------------------------------------------------------------
+__global__ void k_aos_to_planes(const double* __restrict__ src, double* __restrict__ dst, Layout L,
+                                int meqn, int ghost) {
+    const int nx = L.mx + 2 * ghost, ny = L.my + 2 * ghost;
+    const long long n = (long long)nx * ny;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+         k += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(k % nx), j = (int)(k / nx);
+        const long long d = (long long)(j + 2 - ghost) * L.pitch + (i + 2 - ghost);
+        for (int m = 0; m < meqn; ++m) dst[m * L.plane + d] = src[k * meqn + m];
+    }
+}
+
+__global__ void k_planes_to_aos(const double* __restrict__ src, double* __restrict__ dst, Layout L,
+                                int meqn, int ghost) {
+    const int nx = L.mx + 2 * ghost, ny = L.my + 2 * ghost;
+    const long long n = (long long)nx * ny;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+         k += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(k % nx), j = (int)(k / nx);
+        const long long s = (long long)(j + 2 - ghost) * L.pitch + (i + 2 - ghost);
+        for (int m = 0; m < meqn; ++m) dst[k * meqn + m] = src[m * L.plane + s];
+    }
+}
+
+// Interior-only copy of qbc-layout planes (for the "ghosts unchanged" rule of
+// claw2_step2: qnew starts as a copy of qold).
+__global__ void k_copy_planes(const double* __restrict__ src, double* __restrict__ dst, long long n) {
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+         k += (long long)gridDim.x * blockDim.x)
+        dst[k] = src[k];
+}
+
+// FP64 FMA throughput probe: 16 independent dependency chains per thread.
+__global__ void k_fp64_fma(double* out, int iters, double b) {
+    double a[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) a[k] = 1.0 + 1e-3 * (threadIdx.x + k);
+    const double c = 1e-9 * blockIdx.x;
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) a[k] = fma(a[k], b, c);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) s += a[k];
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+}  // namespace claw2

@@ -1,0 +1,92 @@
+"""Device-resident patch: owner of the CUDA copy of one State's q.
+
+Wraps the ``claw2_patch_*`` entry points of include/claw2.h.  The patch holds
+two q buffers on the GPU; a step writes the pending one, and accept/reject
+either swaps them or drops the result, so neither the reference's
+``q_backup = state.q.copy('F')`` (src/pyclaw/solver.py:611) nor its
+``qold = self.qbc.copy('F')`` (classic/solver.py:514) is ever made.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+
+class DevicePatch(object):
+    def __init__(self, desc):
+        lib = _lib.load()
+        self._lib = lib
+        h = ctypes.c_void_p()
+        _lib.check(lib.claw2_patch_create(ctypes.byref(desc), ctypes.byref(h)))
+        self.h = h
+        self.desc = desc
+        self.shape = (desc.num_eqn, desc.mx, desc.my)
+        self.device_newer = False   # device q is ahead of the host copy
+        self.host_dirty = True      # host q must be uploaded before the next step
+        self._cfl = ctypes.c_double(0.0)
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self._lib.claw2_patch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- residency protocol used by State ----------------------------------
+    def pull_to_host(self, state):
+        if self.device_newer:
+            q = np.empty(self.shape, order='F')
+            _lib.check(self._lib.claw2_patch_download_q(self.h, _lib.dptr(q)))
+            state._q = q
+            self.device_newer = False
+
+    def host_modified(self, pulled=False):
+        if pulled:
+            self.device_newer = False
+        self.host_dirty = True
+
+    def push(self, state):
+        q = np.asfortranarray(state._q, dtype=np.float64)
+        _lib.check(self._lib.claw2_patch_upload_q(self.h, _lib.dptr(q)))
+        self.host_dirty = False
+        self.device_newer = False
+
+    # ---- stepping -----------------------------------------------------------
+    def set_cparam(self, vals):
+        arr = (ctypes.c_double * len(vals))(*vals)
+        _lib.check(self._lib.claw2_patch_set_cparam(self.h, arr, len(vals)))
+
+    def step(self, dt, want_cfl=True):
+        if want_cfl:
+            _lib.check(self._lib.claw2_patch_step(self.h, ctypes.c_double(dt), ctypes.byref(self._cfl)))
+            return self._cfl.value
+        _lib.check(self._lib.claw2_patch_step(self.h, ctypes.c_double(dt), None))
+        return None
+
+    def accept(self, accept):
+        _lib.check(self._lib.claw2_patch_accept(self.h, 1 if accept else 0))
+        if accept:
+            self.device_newer = True
+
+    def cfl(self):
+        _lib.check(self._lib.claw2_patch_cfl(self.h, ctypes.byref(self._cfl)))
+        return self._cfl.value
+
+    def set_stream(self, stream_ptr):
+        _lib.check(self._lib.claw2_patch_set_stream(self.h, ctypes.c_void_p(stream_ptr or None)))
+
+    def set_timing(self, on):
+        _lib.check(self._lib.claw2_patch_set_timing(self.h, 1 if on else 0))
+
+    def kernel_ms(self):
+        ms = ctypes.c_float(0.0)
+        _lib.check(self._lib.claw2_patch_kernel_ms(self.h, ctypes.byref(ms)))
+        return ms.value
+
+    def sync(self):
+        _lib.check(self._lib.claw2_patch_sync(self.h))

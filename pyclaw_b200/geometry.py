@@ -1,0 +1,143 @@
+"""Grid geometry: Dimension, Grid, Patch, Domain.
+
+Host-side mirror of src/pyclaw/geometry.py (Dimension :476-640, Grid :16-470,
+Patch :647-743, Domain :744-800) restricted to what the classic 2D step and its
+callers use: cell sizes, centers, nodes and the serial on-boundary flags.
+"""
+import numpy as np
+
+
+class Dimension(object):
+    """One coordinate direction: ``Dimension(lower, upper, num_cells, name='x')``
+    (geometry.py:476-560)."""
+
+    def __init__(self, lower, upper, num_cells, name='x', on_lower_boundary=None,
+                 on_upper_boundary=None, units=None):
+        if upper <= lower:
+            raise ValueError('Dimension.upper must be greater than lower')
+        if int(num_cells) < 1:
+            raise ValueError('Dimension.num_cells must be positive')
+        self._lower = float(lower)
+        self._upper = float(upper)
+        self.num_cells = int(num_cells)
+        self.name = name
+        self.units = units
+        self.on_lower_boundary = True if on_lower_boundary is None else on_lower_boundary
+        self.on_upper_boundary = True if on_upper_boundary is None else on_upper_boundary
+
+    lower = property(lambda self: self._lower)
+    upper = property(lambda self: self._upper)
+
+    @property
+    def delta(self):
+        """(upper - lower) / num_cells (geometry.py:521-523)."""
+        return (self.upper - self.lower) / float(self.num_cells)
+
+    @property
+    def nodes(self):
+        return np.array([self.lower + i * self.delta for i in range(self.num_cells + 1)])
+
+    @property
+    def centers(self):
+        """lower + (i + 1/2) delta, evaluated like geometry.py:547-554."""
+        return np.array([self.lower + (i + 0.5) * self.delta for i in range(self.num_cells)])
+
+    def centers_with_ghost(self, num_ghost):
+        return np.array([self.lower + (i + 0.5) * self.delta
+                         for i in range(-num_ghost, self.num_cells + num_ghost)])
+
+    def __str__(self):
+        return "Dimension %s:  (num_cells,delta,[lower,upper]) = (%s,%s,[%s,%s])" % (
+            self.name, self.num_cells, self.delta, self.lower, self.upper)
+
+
+class Grid(object):
+    """Cartesian product of Dimensions (geometry.py:16-470)."""
+
+    def __init__(self, dimensions):
+        if isinstance(dimensions, Dimension):
+            dimensions = [dimensions]
+        self._dims = list(dimensions)
+        self.gauges = []
+        self.gauge_files = []
+        self.mapc2p = lambda *xs: list(xs)
+
+    dimensions = property(lambda self: list(self._dims))
+    num_dim = property(lambda self: len(self._dims))
+    num_cells = property(lambda self: [d.num_cells for d in self._dims])
+    delta = property(lambda self: [d.delta for d in self._dims])
+    lower = property(lambda self: [d.lower for d in self._dims])
+    upper = property(lambda self: [d.upper for d in self._dims])
+    on_lower_boundary = property(lambda self: [d.on_lower_boundary for d in self._dims])
+    on_upper_boundary = property(lambda self: [d.on_upper_boundary for d in self._dims])
+
+    def get_dim_attribute(self, attr):
+        return [getattr(d, attr) for d in self._dims]
+
+    @property
+    def c_centers(self):
+        """Cell-center coordinate arrays, indexing 'ij' (geometry.py:165-300)."""
+        idx = np.indices(self.num_cells)
+        return [d.centers[idx[i, ...]] for i, d in enumerate(self._dims)]
+
+    @property
+    def c_nodes(self):
+        idx = np.indices([n + 1 for n in self.num_cells])
+        return [d.nodes[idx[i, ...]] for i, d in enumerate(self._dims)]
+
+    @property
+    def p_centers(self):
+        return self.mapc2p(*self.c_centers)
+
+    @property
+    def p_nodes(self):
+        return self.mapc2p(*self.c_nodes)
+
+    def __getattr__(self, name):
+        # grid.x, grid.y address the dimensions by name, as in the reference
+        for d in self.__dict__.get('_dims', []):
+            if d.name == name:
+                return d
+        raise AttributeError(name)
+
+
+class Patch(object):
+    """A logically rectangular piece of the domain (geometry.py:647-743)."""
+
+    def __init__(self, dimensions):
+        self.grid = Grid(dimensions)
+        self.level = 1
+        self.patch_index = 1
+
+    num_dim = property(lambda self: self.grid.num_dim)
+    dimensions = property(lambda self: self.grid.dimensions)
+    delta = property(lambda self: self.grid.delta)
+    num_cells_global = property(lambda self: self.grid.num_cells)
+    lower_global = property(lambda self: self.grid.lower)
+    upper_global = property(lambda self: self.grid.upper)
+
+
+class Domain(object):
+    """``Domain(lower, upper, num_cells)`` or ``Domain([dims])`` / ``Domain(patch)``
+    (geometry.py:744-800)."""
+
+    def __init__(self, *arg):
+        if len(arg) > 1:
+            lower, upper, n = arg[0], arg[1], arg[2]
+            names = ['x', 'y', 'z'][:len(n)]
+            self.patches = [Patch([Dimension(lo, up, nn, name=nm)
+                                   for lo, up, nn, nm in zip(lower, upper, n, names)])]
+        else:
+            geom = arg[0]
+            if not isinstance(geom, (list, tuple)):
+                geom = [geom]
+            if isinstance(geom[0], Patch):
+                self.patches = list(geom)
+            elif isinstance(geom[0], Dimension):
+                self.patches = [Patch(geom)]
+            else:
+                raise TypeError("Domain needs Dimensions, Patches or (lower, upper, num_cells)")
+
+    patch = property(lambda self: self.patches[0])
+    grid = property(lambda self: self.patches[0].grid)
+    num_dim = property(lambda self: self.patches[0].num_dim)

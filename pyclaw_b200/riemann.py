@@ -1,0 +1,62 @@
+"""Riemann solvers available to the CUDA step.
+
+Stands in for the external ``clawpack.riemann`` package (not vendored in the
+reference; used at src/pyclaw/solver.py:230-238 and
+classic/solver.py:516-521).  Each solver object is what a user passes to
+``ClawSolver2D(...)``: its ``__name__`` ends in the reference's module name, the
+``static`` tables give num_eqn/num_waves/fwave by that name, and ``cparam``
+lists the ``problem_data`` keys that become its parameter vector (the
+reference's COMMON /cparam/, state.py:206-231).  The device functors live in
+csrc/riemann.cuh.
+"""
+import types
+
+from . import _lib
+
+
+class RiemannSolver(object):
+    def __init__(self, name, rp_id, num_eqn, num_waves, cparam, fwave=False, efix=None):
+        self.__name__ = 'clawpack.riemann.' + name
+        self.name = name
+        self.rp_id = rp_id
+        self.num_eqn = num_eqn
+        self.num_waves = num_waves
+        self.cparam_names = tuple(cparam)
+        self.fwave = fwave
+        self.efix = efix  # entropy fix switch (a compile-time constant in Fortran)
+
+    def cparam(self, problem_data):
+        """Parameter vector for the C ABI from ``problem_data``."""
+        missing = [k for k in self.cparam_names if k not in problem_data]
+        if missing:
+            raise Exception("Some required value(s) in the cparam common block in the Riemann "
+                            "solver have not been set in problem_data: %s" % ", ".join(missing))
+        vals = [float(problem_data[k]) for k in self.cparam_names]
+        if self.efix is not None:
+            vals.append(1.0 if problem_data.get('efix', self.efix) else 0.0)
+        return vals
+
+    def __repr__(self):
+        return "<Riemann solver %s>" % self.name
+
+
+advection_2D = RiemannSolver('advection_2D', _lib.RP_ADVECTION, 1, 1, ('u', 'v'))
+acoustics_2D = RiemannSolver('acoustics_2D', _lib.RP_ACOUSTICS, 3, 2, ('rho', 'bulk', 'cc', 'zz'))
+euler_4wave_2D = RiemannSolver('euler_4wave_2D', _lib.RP_EULER_ROE, 4, 4, ('gamma',), efix=True)
+shallow_roe_with_efix_2D = RiemannSolver('shallow_roe_with_efix_2D', _lib.RP_SHALLOW_ROE, 3, 3,
+                                         ('grav',), efix=True)
+
+_ALL = [advection_2D, acoustics_2D, euler_4wave_2D, shallow_roe_with_efix_2D]
+
+static = types.SimpleNamespace(
+    num_eqn={s.name: s.num_eqn for s in _ALL},
+    num_waves={s.name: s.num_waves for s in _ALL},
+    fwave={s.name: s.fwave for s in _ALL},
+)
+
+# component-index constants modules (clawpack.riemann.<name>_constants)
+euler_4wave_2D_constants = types.SimpleNamespace(density=0, x_momentum=1, y_momentum=2, energy=3,
+                                                 num_eqn=4)
+shallow_roe_with_efix_2D_constants = types.SimpleNamespace(depth=0, x_momentum=1, y_momentum=2,
+                                                           num_eqn=3)
+acoustics_2D_constants = types.SimpleNamespace(pressure=0, x_velocity=1, y_velocity=2, num_eqn=3)

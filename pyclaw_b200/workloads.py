@@ -1,0 +1,242 @@
+"""Problem setups: the reference's 2D classic regression examples and the
+benchmark workloads, each returning a ready-to-run Controller.
+
+The regression examples restate the setups of the reference's examples
+(initial data evaluated with the same numpy expressions, so the grids match
+bit for bit):
+  advection_2d              examples/advection_2d/advection_2d.py:19-81
+  acoustics_2d_homogeneous  examples/acoustics_2d_homogeneous/acoustics_2d.py:20-106
+  quadrants                 examples/euler_2d/quadrants.py:73-126
+  radial_dam_break          examples/shallow_2d/radial_dam_break.py:23-87
+The benchmark workloads are the acoustics, Euler-quadrant and shallow-water
+dam-break problems at the benchmark sizes (unsplit step, transverse
+corrections, MC limiter).
+
+``solver_class`` lets tests run the same setup through another ClawSolver2D
+subclass; by default the CUDA solver is used.
+"""
+import numpy as np
+
+from . import riemann
+from .classic import ClawSolver2D
+from .controller import Controller
+from .geometry import Dimension, Domain
+from .limiters import tvd
+from .solution import Solution
+from .solver import BC
+from .state import State
+
+
+def _controller(solver, solution, tfinal, num_output_times=10, keep_copy=True):
+    claw = Controller()
+    claw.solution = solution
+    claw.solver = solver
+    claw.tfinal = tfinal
+    claw.num_output_times = num_output_times
+    claw.keep_copy = keep_copy
+    claw.output_format = None
+    return claw
+
+
+def advection_2d(solver_class=None, dimensional_split=True, transverse_waves=0, mx=50, my=50):
+    cls = solver_class or ClawSolver2D
+    solver = cls(riemann.advection_2D)
+    solver.dimensional_split = dimensional_split
+    solver.transverse_waves = transverse_waves
+    solver.limiters = tvd.vanleer
+    solver.bc_lower[0] = BC.periodic
+    solver.bc_upper[0] = BC.periodic
+    solver.bc_lower[1] = BC.periodic
+    solver.bc_upper[1] = BC.periodic
+    if not dimensional_split and not transverse_waves:
+        solver.cfl_max = 0.5
+        solver.cfl_desired = 0.45
+    else:
+        solver.cfl_max = 1.0
+        solver.cfl_desired = 0.9
+    x = Dimension(0.0, 1.0, mx, name='x')
+    y = Dimension(0.0, 1.0, my, name='y')
+    domain = Domain([x, y])
+    state = State(domain, 1)
+    state.problem_data['u'] = 0.5
+    state.problem_data['v'] = 1.0
+    X, Y = state.grid.p_centers
+    state.q[0, :, :] = 0.9 * (0.1 < X) * (X < 0.6) * (0.1 < Y) * (Y < 0.6) + 0.1
+    return _controller(solver, Solution(state, domain), 2.0)
+
+
+def acoustics_2d_homogeneous(solver_class=None, mx=100, my=100):
+    cls = solver_class or ClawSolver2D
+    solver = cls(riemann.acoustics_2D)
+    solver.dimensional_split = True
+    solver.cfl_max = 0.5
+    solver.cfl_desired = 0.45
+    solver.limiters = tvd.MC
+    solver.bc_lower[0] = BC.extrap
+    solver.bc_upper[0] = BC.extrap
+    solver.bc_lower[1] = BC.extrap
+    solver.bc_upper[1] = BC.extrap
+    x = Dimension(-1.0, 1.0, mx, name='x')
+    y = Dimension(-1.0, 1.0, my, name='y')
+    domain = Domain([x, y])
+    state = State(domain, 3)
+    rho = 1.0
+    bulk = 4.0
+    cc = np.sqrt(bulk / rho)
+    zz = rho * cc
+    state.problem_data['rho'] = rho
+    state.problem_data['bulk'] = bulk
+    state.problem_data['zz'] = zz
+    state.problem_data['cc'] = cc
+    solver.dt_initial = np.min(domain.grid.delta) / state.problem_data['cc'] * solver.cfl_desired
+    X, Y = state.grid.p_centers
+    r = np.sqrt(X ** 2 + Y ** 2)
+    width = 0.2
+    state.q[0, :, :] = (np.abs(r - 0.5) <= width) * (1. + np.cos(np.pi * (r - 0.5) / width))
+    state.q[1, :, :] = 0.
+    state.q[2, :, :] = 0.
+    return _controller(solver, Solution(state, domain), 0.12)
+
+
+def quadrants(solver_class=None, mx=100, my=100, efix=None):
+    cls = solver_class or ClawSolver2D
+    solver = cls(riemann.euler_4wave_2D)
+    solver.transverse_waves = 2
+    solver.all_bcs = BC.extrap
+    domain = Domain([0., 0.], [1., 1.], [mx, my])
+    solution = Solution(4, domain)
+    gamma = 1.4
+    solution.problem_data['gamma'] = gamma
+    if efix is not None:
+        solution.problem_data['efix'] = efix
+    xx, yy = domain.grid.p_centers
+    l = xx < 0.8
+    r = xx >= 0.8
+    b = yy < 0.8
+    t = yy >= 0.8
+    q = solution.q
+    q[0, ...] = 1.5 * r * t + 0.532258064516129 * l * t \
+        + 0.137992831541219 * l * b \
+        + 0.532258064516129 * r * b
+    u = 0.0 * r * t + 1.206045378311055 * l * t \
+        + 1.206045378311055 * l * b \
+        + 0.0 * r * b
+    v = 0.0 * r * t + 0.0 * l * t \
+        + 1.206045378311055 * l * b \
+        + 1.206045378311055 * r * b
+    p = 1.5 * r * t + 0.3 * l * t + 0.029032258064516 * l * b + 0.3 * r * b
+    q[1, ...] = q[0, ...] * u
+    q[2, ...] = q[0, ...] * v
+    q[3, ...] = 0.5 * q[0, ...] * (u ** 2 + v ** 2) + p / (gamma - 1.0)
+    return _controller(solver, solution, 0.8)
+
+
+def radial_dam_break(solver_class=None, mx=150, my=150, h_in=2., h_out=1., dam_radius=0.5):
+    cls = solver_class or ClawSolver2D
+    solver = cls(riemann.shallow_roe_with_efix_2D)
+    solver.limiters = tvd.MC
+    solver.dimensional_split = 1
+    solver.bc_lower[0] = BC.extrap
+    solver.bc_upper[0] = BC.wall
+    solver.bc_lower[1] = BC.extrap
+    solver.bc_upper[1] = BC.wall
+    x = Dimension(-2.5, 2.5, mx, name='x')
+    y = Dimension(-2.5, 2.5, my, name='y')
+    domain = Domain([x, y])
+    state = State(domain, 3)
+    state.problem_data['grav'] = 1.0
+    X, Y = state.p_centers
+    r = np.sqrt((X - 0.) ** 2 + (Y - 0.) ** 2)
+    state.q[0, :, :] = h_in * (r <= dam_radius) + h_out * (r > dam_radius)
+    state.q[1, :, :] = 0.
+    state.q[2, :, :] = 0.
+    return _controller(solver, Solution(state, domain), 2.5)
+
+
+# ---------------------------------------------------------------------------
+# Benchmark workloads (unsplit step2 with transverse corrections)
+# ---------------------------------------------------------------------------
+def acoustics_wall(solver_class=None, n=200, tfinal=0.6):
+    """Linear acoustics, rho=1, K=4 (c=2), [-1,1]^2, wall BCs, MC limiter,
+    unsplit trans_cor, CFL 0.9; p = exp(-100((x-0.25)^2 + y^2)), u = v = 0."""
+    cls = solver_class or ClawSolver2D
+    solver = cls(riemann.acoustics_2D)
+    solver.dimensional_split = False
+    solver.transverse_waves = 2
+    solver.limiters = tvd.MC
+    solver.cfl_max = 1.0
+    solver.cfl_desired = 0.9
+    solver.all_bcs = BC.wall
+    domain = Domain([-1.0, -1.0], [1.0, 1.0], [n, n])
+    state = State(domain, 3)
+    rho, bulk = 1.0, 4.0
+    cc = np.sqrt(bulk / rho)
+    state.problem_data.update(rho=rho, bulk=bulk, cc=cc, zz=rho * cc)
+    X, Y = state.grid.p_centers
+    state.q[0, ...] = np.exp(-100.0 * ((X - 0.25) ** 2 + Y ** 2))
+    state.q[1, ...] = 0.0
+    state.q[2, ...] = 0.0
+    solver.dt_initial = np.min(domain.grid.delta) / cc * solver.cfl_desired
+    return _controller(solver, Solution(state, domain), tfinal)
+
+
+QUADRANT_STATES = {  # (rho, u, v, p) per quadrant, split at x = y = 0.8
+    'NE': (1.5, 0.0, 0.0, 1.5),
+    'NW': (0.5323, 1.206, 0.0, 0.3),
+    'SW': (0.138, 1.206, 1.206, 0.029),
+    'SE': (0.5323, 0.0, 1.206, 0.3),
+}
+
+
+def euler_quadrants_unsplit(solver_class=None, n=1024, tfinal=0.8, split=(0.8, 0.8), states=None,
+                            gamma=1.4):
+    """Four-quadrant Euler Riemann problem on [0,1]^2, Roe 4-wave solver,
+    extrapolation BCs, MC limiter, unsplit with transverse corrections."""
+    cls = solver_class or ClawSolver2D
+    solver = cls(riemann.euler_4wave_2D)
+    solver.dimensional_split = False
+    solver.transverse_waves = 2
+    solver.limiters = tvd.MC
+    solver.all_bcs = BC.extrap
+    domain = Domain([0., 0.], [1., 1.], [n, n])
+    solution = Solution(4, domain)
+    solution.problem_data['gamma'] = gamma
+    st = states or QUADRANT_STATES
+    xx, yy = domain.grid.p_centers
+    xs, ys = split
+    masks = {'NE': (xx >= xs) & (yy >= ys), 'NW': (xx < xs) & (yy >= ys),
+             'SW': (xx < xs) & (yy < ys), 'SE': (xx >= xs) & (yy < ys)}
+    rho = np.zeros_like(xx)
+    u = np.zeros_like(xx)
+    v = np.zeros_like(xx)
+    p = np.zeros_like(xx)
+    for k, msk in masks.items():
+        rho[msk], u[msk], v[msk], p[msk] = st[k]
+    q = solution.q
+    q[0, ...] = rho
+    q[1, ...] = rho * u
+    q[2, ...] = rho * v
+    q[3, ...] = 0.5 * rho * (u ** 2 + v ** 2) + p / (gamma - 1.0)
+    return _controller(solver, solution, tfinal)
+
+
+def shallow_dam_break_unsplit(solver_class=None, n=4096, tfinal=1.0):
+    """Radial dam break, g=1, [-2.5,2.5]^2, h=2 for r<0.5 else 1, Roe solver
+    with entropy fix, extrapolation BCs, MC limiter, unsplit trans_cor, CFL 0.9."""
+    cls = solver_class or ClawSolver2D
+    solver = cls(riemann.shallow_roe_with_efix_2D)
+    solver.dimensional_split = False
+    solver.transverse_waves = 2
+    solver.limiters = tvd.MC
+    solver.cfl_desired = 0.9
+    solver.cfl_max = 1.0
+    solver.all_bcs = BC.extrap
+    domain = Domain([-2.5, -2.5], [2.5, 2.5], [n, n])
+    state = State(domain, 3)
+    state.problem_data['grav'] = 1.0
+    X, Y = state.p_centers
+    r = np.sqrt(X ** 2 + Y ** 2)
+    state.q[0, ...] = 2.0 * (r < 0.5) + 1.0 * (r >= 0.5)
+    state.q[1, ...] = 0.0
+    state.q[2, ...] = 0.0
+    return _controller(solver, Solution(state, domain), tfinal)

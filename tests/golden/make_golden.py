@@ -1,0 +1,42 @@
+"""Extract the reference's own 2D classic regression goldens into
+tests/golden/reference_goldens.npz.
+
+Run in a container where the reference tree is mounted (default
+/root/reference, or pass its path).  Sources, all produced by the reference's
+Fortran step2/step2ds with clawpack/riemann solvers:
+  examples/advection_2d/expected_sols.npy            (test_2d_advection.py:9-35)
+  examples/acoustics_2d_homogeneous/verify_classic.txt (test_2d_acoustics.py:6-15)
+  examples/euler_2d/expected_sols.npy['quadrants_roe'] (test_euler2d.py:6-29)
+  examples/shallow_2d/expected_sols.npy['radialdambreak_classic_roe']
+                                                     (test_shallow2d.py:9-28)
+"""
+import os
+import sys
+
+import numpy as np
+
+REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_goldens.npz")
+
+
+def main():
+    ex = os.path.join(REF, "examples")
+    adv = np.load(os.path.join(ex, "advection_2d", "expected_sols.npy"), allow_pickle=True).item()
+    eul = np.load(os.path.join(ex, "euler_2d", "expected_sols.npy"), allow_pickle=True).item()
+    sw = np.load(os.path.join(ex, "shallow_2d", "expected_sols.npy"), allow_pickle=True).item()
+    ac = np.loadtxt(os.path.join(ex, "acoustics_2d_homogeneous", "verify_classic.txt"))
+    out = {
+        "advection_classic_dim_split": adv["classic_dim_split"],
+        "advection_classic_unsplit_no_trans": adv["classic_unsplit_no_trans"],
+        "advection_classic_unsplit_trans_inc": adv["classic_unsplit_trans_inc"],
+        "advection_classic_unsplit_trans_cor": adv["classic_unsplit_trans_cor"],
+        "acoustics_verify_classic": ac,
+        "euler_quadrants_roe": eul["quadrants_roe"],
+        "shallow_radialdambreak_classic_roe": sw["radialdambreak_classic_roe"],
+    }
+    np.savez_compressed(OUT, **{k: np.asarray(v, dtype=np.float64) for k, v in out.items()})
+    print("wrote", OUT, {k: np.asarray(v).shape for k, v in out.items()})
+
+
+if __name__ == "__main__":
+    main()

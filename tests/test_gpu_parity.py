@@ -1,0 +1,114 @@
+"""Parity of the CUDA step against the CPU oracle (the reference's step2 /
+step2ds / flux2 / limiter / philim restated), called through the C ABI.
+
+Bar: interior cells within 1e-12 relative in the max norm, CFL within 1e-12
+relative, on identical inputs (FP64; the only differences are the order of
+the per-cell increment sums and fused multiply-adds).
+"""
+import numpy as np
+import pytest
+
+from helpers import PARITY_RTOL, RP_INFO, max_rel, method_vector, random_qbc, set_cparam
+from pyclaw_b200 import _lib, classic2
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [(1, 1), (3, 5), (37, 23), (130, 70), (257, 9), (9, 300)]
+
+
+def _dt_for(oracle, qbc, rp, cp, method, mthlim, dx, dy, target=0.8, split=False):
+    q2 = qbc.copy(order="F")
+    if split:
+        c = oracle.step2ds(qbc, q2, dx, dy, 1e-3, method, mthlim, 1, rp, cp)
+    else:
+        c = oracle.step2(qbc, q2, dx, dy, 1e-3, method, mthlim, rp, cp)
+    return 1e-3 * target / max(c, 1e-12)
+
+
+@pytest.mark.parametrize("rp", sorted(RP_INFO))
+@pytest.mark.parametrize("transverse", [0, 1, 2])
+@pytest.mark.parametrize("mx,my", SIZES)
+def test_step2_unsplit(oracle, rp, transverse, mx, my):
+    name, meqn, mwaves, cp = RP_INFO[rp]
+    qbc = random_qbc(rp, mx, my, seed=mx * 1000 + my + transverse)
+    method = method_vector(2, transverse)
+    mthlim = np.full(mwaves, 4, dtype=np.intc)
+    dx, dy = 1.0 / mx, 1.3 / my
+    dt = _dt_for(oracle, qbc, rp, cp, method, mthlim, dx, dy)
+    q_o = qbc.copy(order="F")
+    cfl_o = oracle.step2(qbc, q_o, dx, dy, dt, method, mthlim, rp, cp)
+    set_cparam(classic2, rp)
+    q_g, cfl_g = classic2.step2(max(mx, my), 2, mx, my, qbc, qbc.copy(order="F"), None, dx, dy, dt, method,
+                                mthlim, rpn2=rp)
+    assert abs(cfl_g - cfl_o) <= PARITY_RTOL * cfl_o
+    assert max_rel(q_g[:, 2:-2, 2:-2], q_o[:, 2:-2, 2:-2]) <= PARITY_RTOL
+    # ghost cells are returned as they were on entry
+    assert np.array_equal(q_g[:, :2, :], qbc[:, :2, :])
+
+
+@pytest.mark.parametrize("rp", sorted(RP_INFO))
+@pytest.mark.parametrize("lim", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("order", [1, 2])
+def test_step2_limiters_and_order(oracle, rp, lim, order):
+    name, meqn, mwaves, cp = RP_INFO[rp]
+    mx, my = 61, 47
+    qbc = random_qbc(rp, mx, my, seed=7 + lim)
+    method = method_vector(order, 2)
+    mthlim = np.array([(lim + k) % 6 if lim else 0 for k in range(mwaves)], dtype=np.intc)
+    dx, dy = 0.02, 0.015
+    dt = _dt_for(oracle, qbc, rp, cp, method, mthlim, dx, dy)
+    q_o = qbc.copy(order="F")
+    cfl_o = oracle.step2(qbc, q_o, dx, dy, dt, method, mthlim, rp, cp)
+    set_cparam(classic2, rp)
+    q_g, cfl_g = classic2.step2(max(mx, my), 2, mx, my, qbc, qbc.copy(order="F"), None, dx, dy, dt, method,
+                                mthlim, rpn2=rp)
+    assert abs(cfl_g - cfl_o) <= PARITY_RTOL * cfl_o
+    assert max_rel(q_g[:, 2:-2, 2:-2], q_o[:, 2:-2, 2:-2]) <= PARITY_RTOL
+
+
+@pytest.mark.parametrize("rp", sorted(RP_INFO))
+@pytest.mark.parametrize("ids", [1, 2])
+@pytest.mark.parametrize("mx,my", [(1, 1), (37, 23), (130, 70), (250, 260)])
+def test_step2ds_sweeps(oracle, rp, ids, mx, my):
+    name, meqn, mwaves, cp = RP_INFO[rp]
+    qbc = random_qbc(rp, mx, my, seed=31 * mx + my + ids)
+    method = method_vector(2, 0, split=True)
+    mthlim = np.full(mwaves, 4, dtype=np.intc)
+    dx, dy = 1.0 / mx, 1.0 / my
+    dt = _dt_for(oracle, qbc, rp, cp, method, mthlim, dx, dy, split=True)
+    q_o = qbc.copy(order="F")
+    cfl_o = oracle.step2ds(qbc, q_o, dx, dy, dt, method, mthlim, ids, rp, cp)
+    set_cparam(classic2, rp)
+    q_g, cfl_g = classic2.step2ds(max(mx, my), 2, mx, my, qbc, qbc.copy(order="F"), None, dx, dy, dt, method,
+                                  mthlim, ids=ids, rpn2=rp)
+    assert abs(cfl_g - cfl_o) <= PARITY_RTOL * cfl_o
+    if ids == 1:
+        # the x-sweep result covers every row, ghost rows included
+        assert max_rel(q_g[:, 2:-2, :], q_o[:, 2:-2, :]) <= PARITY_RTOL
+        assert np.array_equal(q_g[:, :2, :], q_o[:, :2, :])
+    else:
+        assert max_rel(q_g[:, 2:-2, 2:-2], q_o[:, 2:-2, 2:-2]) <= PARITY_RTOL
+
+
+@pytest.mark.parametrize("bcl,bcu", [((1, 1), (1, 1)), ((2, 2), (2, 2)), ((3, 3), (3, 3)), ((1, 3), (3, 1)),
+                                     ((2, 1), (2, 3)), ((3, 2), (1, 2))])
+@pytest.mark.parametrize("mx,my", [(2, 2), (2, 3), (17, 29)])
+def test_bc_fill(oracle, bcl, bcu, mx, my):
+    qbc = random_qbc(_lib.RP_EULER_ROE, mx, my, seed=mx + 100 * my)
+    q_o = qbc.copy(order="F")
+    oracle.bc_fill(q_o, bcl, bcu)
+    q_g = classic2.bc_fill(qbc.copy(order="F"), bcl, bcu)
+    assert np.array_equal(q_g, q_o)
+
+
+def test_bc_fill_single_cell_extrap(oracle):
+    qbc = random_qbc(_lib.RP_SHALLOW_ROE, 1, 1, seed=5)
+    q_o = qbc.copy(order="F")
+    oracle.bc_fill(q_o, (1, 1), (1, 1))
+    assert np.array_equal(classic2.bc_fill(qbc.copy(order="F"), (1, 1), (1, 1)), q_o)
+
+
+def test_bc_fill_rejects_wall_on_single_cell():
+    qbc = random_qbc(_lib.RP_SHALLOW_ROE, 1, 4, seed=5)
+    with pytest.raises(_lib.Claw2Error):
+        classic2.bc_fill(qbc, (3, 1), (3, 1))

@@ -1,0 +1,141 @@
+"""The device-resident path (ghost fill, fused step and CFL on the GPU, q kept
+on the device) driven by the package's Controller/Solver loop.
+
+* whole runs of the reference's regression examples against the reference's
+  own goldens (the same checks tests/test_oracle_golden.py makes of the oracle);
+* step-by-step parity with the oracle on the benchmark problems: from the same
+  state, one GPU step (ghost fill + step2 + CFL on the device) and one oracle
+  step (ghost fill + step2 on the host) must agree to 1e-12 relative;
+* conservation on closed (wall) domains.
+"""
+import numpy as np
+import pytest
+
+from helpers import PARITY_RTOL, max_rel
+from pyclaw_b200 import workloads
+
+pytestmark = pytest.mark.gpu
+
+
+def _l1(claw, expected, comp=None):
+    q = claw.frames[claw.num_output_times].state.get_q_global()
+    if comp is not None:
+        q = q[comp]
+    dx, dy = claw.solution.domain.grid.delta
+    return dx * dy * np.sum(np.abs(q.reshape([-1]) - expected))
+
+
+@pytest.mark.parametrize("key,kw", [
+    ("advection_classic_dim_split", dict(dimensional_split=True)),
+    ("advection_classic_unsplit_no_trans", dict(dimensional_split=False, transverse_waves=0)),
+    ("advection_classic_unsplit_trans_inc", dict(dimensional_split=False, transverse_waves=1)),
+    ("advection_classic_unsplit_trans_cor", dict(dimensional_split=False, transverse_waves=2)),
+])
+def test_cuda_advection_goldens(goldens, key, kw):
+    claw = workloads.advection_2d(**kw)
+    claw.run()
+    err = _l1(claw, goldens[key])
+    assert err < 1e-6
+    assert err < 1e-12
+
+
+def test_cuda_acoustics_goldens(goldens):
+    claw = workloads.acoustics_2d_homogeneous()
+    claw.run()
+    exp = goldens["acoustics_verify_classic"]
+    rel = np.linalg.norm(exp - claw.frames[-1].q[0]) / np.linalg.norm(exp)
+    assert rel < 1e-3
+
+
+def test_cuda_euler_goldens(goldens):
+    claw = workloads.quadrants()
+    claw.run()
+    err = _l1(claw, goldens["euler_quadrants_roe"], comp=0)
+    assert err < 1e-6
+    assert err < 1e-11
+
+
+def test_cuda_shallow_goldens(goldens):
+    claw = workloads.radial_dam_break()
+    claw.run()
+    err = _l1(claw, goldens["shallow_radialdambreak_classic_roe"], comp=0)
+    assert err < 1e-5
+    assert err < 1e-11
+
+
+def _stepwise(oracle, claw, nsteps):
+    """Advance the GPU solver step by step; before each step run the oracle on
+    the same state and dt and compare the results."""
+    solver, sol = claw.solver, claw.solution
+    solver.setup(sol)
+    solver.dt = solver.dt_initial
+    st = sol.state
+    dx, dy = st.grid.delta
+    mx, my = st.grid.num_cells
+    cp = solver.rp.cparam(st.problem_data)
+    worst = 0.0
+    for n in range(nsteps):
+        q0 = st.get_q_global()
+        qbc = np.zeros((q0.shape[0], mx + 4, my + 4), order="F")
+        qbc[:, 2:-2, 2:-2] = q0
+        oracle.bc_fill(qbc, solver.bc_lower, solver.bc_upper)
+        qold = qbc.copy(order="F")
+        solver.evolve_to_time(sol)  # one step (take_one_step)
+        dt = solver.dt
+        cfl_o = oracle.step2(qold, qbc, dx, dy, dt, solver._method, solver._mthlim, solver.rp.rp_id, cp)
+        if not solver.accept_step:
+            continue
+        q1 = st.get_q_global()
+        worst = max(worst, max_rel(q1, qbc[:, 2:-2, 2:-2]))
+        assert abs(solver.cfl.get_cached_max() - cfl_o) <= PARITY_RTOL * cfl_o
+        assert worst <= PARITY_RTOL, (n, worst)
+    return worst
+
+
+def test_stepwise_acoustics_wall_full_run(oracle):
+    # acoustics, 200x200, walls, MC, trans_cor: every step to t = 0.6
+    claw = workloads.acoustics_wall(n=200, tfinal=0.6)
+    _stepwise(oracle, claw, nsteps=140)
+
+
+def test_stepwise_euler_quadrants(oracle):
+    claw = workloads.euler_quadrants_unsplit(n=160)
+    _stepwise(oracle, claw, nsteps=40)
+
+
+def test_stepwise_shallow_dam_break(oracle):
+    claw = workloads.shallow_dam_break_unsplit(n=192)
+    _stepwise(oracle, claw, nsteps=30)
+
+
+def test_acoustics_wall_conserves_pressure_sum():
+    claw = workloads.acoustics_wall(n=200, tfinal=0.6)
+    p0 = claw.solution.state.get_q_global()[0].sum()
+    scale = np.abs(claw.solution.state.get_q_global()[0]).sum()
+    claw.run()
+    p1 = claw.frames[-1].q[0].sum()
+    assert abs(p1 - p0) <= 1e-13 * scale
+
+
+def test_whole_run_acoustics_matches_oracle(oracle):
+    claw_g = workloads.acoustics_wall(n=200, tfinal=0.6)
+    claw_g.run()
+    claw_o = workloads.acoustics_wall(oracle.make_solver_class(), n=200, tfinal=0.6)
+    claw_o.run()
+    assert claw_g.solver.status['numsteps'] == claw_o.solver.status['numsteps']
+    assert max_rel(claw_g.frames[-1].q, claw_o.frames[-1].q) <= 1e-11
+
+
+def test_reject_and_retake_on_device():
+    # a first dt far above the CFL limit must be rejected and retaken
+    claw = workloads.acoustics_wall(n=64, tfinal=0.05)
+    claw.solver.dt_initial = 1.0
+    q0 = claw.solution.state.get_q_global()
+    claw.solver.setup(claw.solution)
+    claw.solver.dt = claw.solver.dt_initial
+    claw.solver.evolve_to_time(claw.solution)
+    assert not claw.solver.accept_step
+    assert np.array_equal(claw.solution.state.get_q_global(), q0)
+    assert claw.solution.t == 0.0
+    claw.solver.evolve_to_time(claw.solution)
+    assert claw.solver.accept_step and claw.solution.t > 0.0
