@@ -39,8 +39,12 @@ enum {
     CLAW2_RP_EULER_EXACT = 5   /* exact Euler (no reference counterpart): {gamma, tol, guess} */
 };
 
-/* Boundary-condition codes: pyclaw.BC (src/pyclaw/solver.py:13-19). */
-enum { CLAW2_BC_CUSTOM = 0, CLAW2_BC_EXTRAP = 1, CLAW2_BC_PERIODIC = 2, CLAW2_BC_WALL = 3 };
+/* Boundary-condition codes: pyclaw.BC (src/pyclaw/solver.py:13-19), plus
+ * CLAW2_BC_NONE for a side whose ghost rows the caller fills (a neighbour's
+ * halo in a domain split across ranks, as petclaw's DMDA globalToLocal does,
+ * src/petclaw/state.py:223-229); only the x rule is applied to its corners. */
+enum { CLAW2_BC_NONE = -1, CLAW2_BC_CUSTOM = 0, CLAW2_BC_EXTRAP = 1, CLAW2_BC_PERIODIC = 2,
+       CLAW2_BC_WALL = 3 };
 
 /* Status codes. */
 enum {

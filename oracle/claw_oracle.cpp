@@ -836,6 +836,7 @@ int oracle_bc_fill(int meqn, int mbc, int mx, int my, double* qbc, const int* bc
         };
         for (int side = 0; side < 2; ++side) {
             const int bc = side == 0 ? bcl[idim] : bcu[idim];
+            if (bc == -1) continue;  // ghost cells filled by the caller (a neighbour's halo)
             for (int b = lo_other; b <= hi_other; ++b) {
                 for (int g = 0; g < mbc; ++g) {
                     // Python index g along the rolled axis: cell 1-mbc+g (lower) or n+mbc-g (upper)

@@ -61,7 +61,8 @@ int oracle_step2ds(int maxm, int meqn, int mwaves, int maux, int mbc, int mx, in
                    int rp_id, const double* cparam);
 
 /* Ghost-cell fill of qbc (solver.py:351-519, q only).  bc codes follow
- * pyclaw.BC: 1 extrap, 2 periodic, 3 wall.  reflect_index = {1,2}. */
+ * pyclaw.BC: 1 extrap, 2 periodic, 3 wall; -1 leaves that side to the caller
+ * (a halo filled by a neighbouring rank).  reflect_index = {1,2}. */
 int oracle_bc_fill(int meqn, int mbc, int mx, int my, double* qbc,
                    const int* bc_lower, const int* bc_upper);
 

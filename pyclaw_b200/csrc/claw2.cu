@@ -164,12 +164,17 @@ int check_bc(const int* bcl, const int* bcu, int mx, int my) {
         const int n = d == 0 ? mx : my;
         // a wall or periodic ghost cell copies one of the first/last two
         // interior cells; with one cell that source would itself be a ghost
-        if (n < 2 && (bcl[d] != CLAW2_BC_EXTRAP || bcu[d] != CLAW2_BC_EXTRAP))
+        const bool lo_ok = bcl[d] == CLAW2_BC_EXTRAP || bcl[d] == CLAW2_BC_NONE;
+        const bool up_ok = bcu[d] == CLAW2_BC_EXTRAP || bcu[d] == CLAW2_BC_NONE;
+        if (n < 2 && !(lo_ok && up_ok))
             return fail(CLAW2_EINVAL, "wall/periodic BCs need at least 2 cells in dimension %d", d);
         for (int v : {bcl[d], bcu[d]}) {
             if (v == CLAW2_BC_CUSTOM)
                 return fail(CLAW2_EUNSUPPORTED, "custom BCs are applied by the host (dimension %d)", d);
-            if (v < 1 || v > 3) return fail(CLAW2_EINVAL, "boundary condition %d not implemented", v);
+            if (v == CLAW2_BC_NONE && d == 0)
+                return fail(CLAW2_EINVAL, "caller-filled ghost cells are supported in dimension 1 only");
+            if (v != CLAW2_BC_NONE && (v < 1 || v > 3))
+                return fail(CLAW2_EINVAL, "boundary condition %d not implemented", v);
         }
         if ((bcl[d] == CLAW2_BC_PERIODIC) != (bcu[d] == CLAW2_BC_PERIODIC))
             return fail(CLAW2_EINVAL, "periodic BC must be set on both sides of dimension %d", d);

@@ -609,12 +609,14 @@ __device__ __forceinline__ int bc_src(int c, int n, int lo, int up, bool& flip) 
     // c padded index in [0, n+4); returns the padded source index
     flip = false;
     if (c < 2) {
+        if (lo == CLAW2_BC_NONE) return c;
         if (lo == CLAW2_BC_EXTRAP) return 2;
         if (lo == CLAW2_BC_PERIODIC) return c + n;
         flip = true;
         return 3 - c;  // wall
     }
     if (c >= n + 2) {
+        if (up == CLAW2_BC_NONE) return c;
         if (up == CLAW2_BC_EXTRAP) return n + 1;
         if (up == CLAW2_BC_PERIODIC) return c - n;
         flip = true;
