@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--n", type=int, default=N, help="grid size override (profiling runs only)")
+    ap.add_argument("--shape", default=None, help="fixed launch shape 'variant,rows' (skips the autotuner)")
     ap.add_argument("--pre-t", type=float, default=0.4,
                     help="advance the problem to this time (untimed) before warm-up")
     return ap.parse_args()
@@ -216,6 +217,13 @@ def run_ours(args):
     cfl = patch.step(dt)
     patch.accept(False)
     dt = dt * 0.9 / cfl
+    # launch shape from the autotuner (trial steps are rejected: state unchanged)
+    from pyclaw_b200 import tune
+    if args.shape:
+        shape, trials = tuple(int(x) for x in args.shape.split(",")), {}
+        tune.set_shape(patch.desc.riemann, *shape)
+    else:
+        shape, trials = tune.autotune(patch, dt)
     patch.set_timing(True)
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
@@ -298,6 +306,9 @@ def run_ours(args):
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "ours",
                 "config": config({"dt": dt, "cfl_last": last_cfl, "mx": n, "my": n,
+                                  "launch_shape": {"variant": shape[0], "rows": shape[1],
+                                                   "trials_ms": {"%d/%d" % k: round(v, 4)
+                                                                 for k, v in sorted(trials.items())}},
                                   "state": "quadrant problem advanced to t=%g before warm-up" % args.pre_t}),
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                              "frac": achieved / peaks["hbm_gbs"], "traffic": None,

@@ -153,6 +153,13 @@ int claw2_patch_set_stream(claw2_patch* p, void* stream);
 int claw2_patch_set_timing(claw2_patch* p, int on);
 int claw2_patch_kernel_ms(claw2_patch* p, float* ms);
 
+/* Launch shape of the unsplit step kernel for one Riemann solver: variant 0
+ * compiles for 2 blocks per SM (no register cap), 1 for 3 blocks per SM;
+ * rows = row-block height (0 = heuristic).  Process-wide; set by an autotuner
+ * (pyclaw_b200.tune) or by hand. */
+int claw2_tune_set(int riemann, int variant, int rows);
+int claw2_tune_get(int riemann, int* variant, int* rows);
+
 /* FP64 FMA throughput of the current device, TFLOP/s (2 flops per FMA): a
  * roofline denominator for the FP64-bound Riemann solvers. */
 int claw2_probe_fp64(int device, double* tflops);

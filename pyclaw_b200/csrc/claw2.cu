@@ -79,22 +79,46 @@ int pick_rows(int nstrips, int nrows) {
 }
 
 // ---- launches, one instantiation per Riemann solver -----------------------
-template <class RP>
-void launch_unsplit(const StepArgs& a, cudaStream_t st) {
+// Opt a kernel into more than 48 KB of dynamic shared memory, once per device.
+template <class K>
+void smem_attr(K kernel, int bytes, unsigned long long& done) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 64 && !(done & (1ull << dev))) {
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        done |= 1ull << dev;
+    }
+}
+
+// Launch shapes of the unsplit kernel.  A variant fixes the register budget
+// (blocks per SM the kernel is compiled for); `rows` is the row-block height
+// (0 = heuristic).  Chosen per call by the tuning table (claw2_tune_set /
+// claw2_autotune) or the heuristic default.
+struct UnsplitShape {
+    int variant;  // 0: 2 blocks/SM (no register cap), 1: 3 blocks/SM
+    int rows;
+};
+
+UnsplitShape g_tune[8] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}};
+
+template <class RP, int MB>
+void launch_unsplit_v(const StepArgs& a, cudaStream_t st, int rows) {
     constexpr int W = NT_UNSPLIT - 4;
     const int ns = (a.L.mx + W - 1) / W;
     StepArgs b = a;
-    b.H = pick_rows(ns, a.L.my);
+    b.H = rows > 0 ? rows : pick_rows(ns, a.L.my);
     dim3 grid(ns, (a.L.my + b.H - 1) / b.H);
     constexpr int smem = (int)sizeof(UnsplitSmem<RP, NT_UNSPLIT>);
-    static unsigned long long attr_set = 0;  // one bit per device, per instantiation
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev < 64 && !(attr_set & (1ull << dev))) {
-        cudaFuncSetAttribute(k_step_unsplit<RP, NT_UNSPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        attr_set |= 1ull << dev;
-    }
-    k_step_unsplit<RP, NT_UNSPLIT><<<grid, NT_UNSPLIT, smem, st>>>(b);
+    static unsigned long long attr = 0;
+    smem_attr(k_step_unsplit<RP, NT_UNSPLIT, MB>, smem, attr);
+    k_step_unsplit<RP, NT_UNSPLIT, MB><<<grid, NT_UNSPLIT, smem, st>>>(b);
+}
+
+template <class RP>
+void launch_unsplit(const StepArgs& a, cudaStream_t st) {
+    const UnsplitShape sh = g_tune[RP::ID & 7];
+    if (sh.variant == 1) launch_unsplit_v<RP, 3>(a, st, sh.rows);
+    else launch_unsplit_v<RP, 2>(a, st, sh.rows);
 }
 
 template <class RP>
@@ -105,7 +129,10 @@ void launch_split(const StepArgs& ax, const StepArgs& ay, cudaStream_t st, int w
         StepArgs b = ax;
         b.H = pick_rows(ns, ax.L.my + 4);
         dim3 grid(ns, (ax.L.my + 4 + b.H - 1) / b.H);
-        k_split_x<RP, NT_SPLIT_X><<<grid, NT_SPLIT_X, 0, st>>>(b);
+        constexpr int smem = (int)sizeof(SplitXSmem<RP, NT_SPLIT_X>);
+        static unsigned long long attr = 0;
+        smem_attr(k_split_x<RP, NT_SPLIT_X>, smem, attr);
+        k_split_x<RP, NT_SPLIT_X><<<grid, NT_SPLIT_X, smem, st>>>(b);
     }
     if (which & 2) {
         const int ns = (ay.L.mx + 4 + NT_SPLIT_Y - 1) / NT_SPLIT_Y;
@@ -637,6 +664,22 @@ int claw2_probe_fp64(int device, double* tflops) {
     if (e != cudaSuccess) return fail(CLAW2_ECUDA, "fp64 probe failed: %s", cudaGetErrorString(e));
     const double flops = 2.0 * 16.0 * iters * (double)blocks * threads;
     *tflops = flops / (ms * 1e-3) / 1e12;
+    return CLAW2_OK;
+}
+
+int claw2_tune_set(int riemann, int variant, int rows) {
+    if (riemann < 1 || riemann > 7) return fail(CLAW2_EINVAL, "unknown Riemann solver id %d", riemann);
+    if (variant < 0 || variant > 1) return fail(CLAW2_EINVAL, "variant must be 0 or 1 (got %d)", variant);
+    if (rows < 0 || rows > 4096) return fail(CLAW2_EINVAL, "rows must be 0..4096 (got %d)", rows);
+    g_tune[riemann & 7].variant = variant;
+    g_tune[riemann & 7].rows = rows;
+    return CLAW2_OK;
+}
+
+int claw2_tune_get(int riemann, int* variant, int* rows) {
+    if (riemann < 1 || riemann > 7 || !variant || !rows) return fail(CLAW2_EINVAL, "bad arguments");
+    *variant = g_tune[riemann & 7].variant;
+    *rows = g_tune[riemann & 7].rows;
     return CLAW2_OK;
 }
 

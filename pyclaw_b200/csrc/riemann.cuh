@@ -5,20 +5,33 @@
 // rpt2(ixy,imp,...,asdq,bmasdq,bpasdq) (call sites src/pyclaw/classic/flux2.f90:101,
 // 181, 194).  Here each solver is a struct of inline functions for ONE
 // interface, with the direction (ixy) and the system size as compile-time
-// constants so that waves, speeds and fluctuations stay in registers.
+// constants so everything stays in registers:
 //
-//   rpn2<IXY>(qL, qR, prm, wave, s, amdq, apdq, cache)
-//       qL = state of the cell below/left of the interface, qR = above/right.
-//   rpt2<IXY>(cache, qL, qR, prm, asdq, bmasdq, bpasdq)
-//       split asdq into down-going and up-going parts; `cache` carries the
-//       Roe-averaged state that rpn2 computed for the same interface so it is
-//       not recomputed (the reuse the reference's
-//       development/rp_approaches/report.tex:37-39 measures as a 10% gain).
+//   prepare(q, p, c)            per-cell quantities (velocities, pressure,
+//                               sqrt(density), sound speed ...) computed once
+//                               per cell instead of once per interface side;
+//                               c[0..MEQN) is q itself
+//   solve<IXY>(cL, cR, p, f, amdq, apdq)
+//                               rpn2: wave strengths + Roe state into the
+//                               compact interface record f, and the
+//                               fluctuations A-dq, A+dq (entropy fix included)
+//   speeds<IXY>(f, p, s)        the wave speeds
+//   waves<IXY>(f, p, w)         the waves, rebuilt from f (strength x eigenvector)
+//   rpt2<IXY>(f, p, asdq, bm, bp)
+//                               transverse split of asdq at the same Roe state,
+//                               summed in eigen-coefficient form
+//
+// cL is the cell below/left of the interface, cR above/right.  Reusing the
+// interface's Roe state in rpt2 is the reuse the reference's
+// development/rp_approaches/report.tex:37-39 measures as a 10% gain.
 //
 // The formulas are the published ones (LeVeque, Finite Volume Methods for
 // Hyperbolic Problems, 2002: advection sec. 20.5, acoustics sec. 18.2/21.7,
-// Roe Euler sec. 15.3 and 18.8, Roe shallow water sec. 15.3, transverse
-// solvers sec. 21.6) and match, operation for operation, the CPU oracle.
+// Roe Euler sec. 15.3 and 18.8, Roe shallow water sec. 15.3, Harten-Hyman
+// entropy fix sec. 15.3.5, transverse solvers sec. 21.6).  They equal the CPU
+// oracle's (which keeps the reference's operation order) up to rounding:
+// Roe averages are formed with one reciprocal and per-cell velocities, and
+// 1/a comes from rsqrt.
 #pragma once
 
 #include "claw2_types.cuh"
@@ -31,27 +44,60 @@ struct Dir {
     static constexpr int MV = (IXY == 1) ? 2 : 1;  // transverse momentum component
 };
 
+// Sum s*w over waves into amdq (s < 0) and apdq (s >= 0): no entropy fix.
+template <int ME, int MW>
+__device__ __forceinline__ void split_fluct(const double (&s)[MW], const double (&w)[MW][ME], double (&amdq)[ME],
+                                            double (&apdq)[ME]) {
+#pragma unroll
+    for (int m = 0; m < ME; ++m) {
+        double am = 0.0, ap = 0.0;
+#pragma unroll
+        for (int k = 0; k < MW; ++k) {
+            if (s[k] < 0.0) am = am + s[k] * w[k][m];
+            else ap = ap + s[k] * w[k][m];
+        }
+        amdq[m] = am;
+        apdq[m] = ap;
+    }
+}
+
+// One wave family K, rebuilt from the compact interface record.
+template <class RP, int IXY, int K>
+__device__ __forceinline__ void wave_k(const typename RP::Iface& f, const RPParams& p, double (&w)[RP::MEQN]) {
+    double all[RP::MWAVES][RP::MEQN];
+    RP::template waves<IXY>(f, p, all);
+#pragma unroll
+    for (int m = 0; m < RP::MEQN; ++m) w[m] = all[K][m];
+}
+
 // ---------------------------------------------------------------------------
 // advection_2D: cparam = {u, v}
 // ---------------------------------------------------------------------------
 struct RPAdvection {
-    static constexpr int MEQN = 1, MWAVES = 1, ID = CLAW2_RP_ADVECTION;
-    struct Cache {};
-    template <int IXY>
-    __device__ __forceinline__ static void rpn2(const double (&qL)[MEQN], const double (&qR)[MEQN],
-                                                const RPParams& p, double (&wave)[MWAVES][MEQN],
-                                                double (&s)[MWAVES], double (&amdq)[MEQN],
-                                                double (&apdq)[MEQN], Cache&) {
-        const double vel = (IXY == 1) ? p.c[0] : p.c[1];
-        wave[0][0] = qR[0] - qL[0];
-        s[0] = vel;
-        amdq[0] = fmin(s[0], 0.0) * wave[0][0];
-        apdq[0] = fmax(s[0], 0.0) * wave[0][0];
+    static constexpr int MEQN = 1, MWAVES = 1, NC = 1, ID = CLAW2_RP_ADVECTION;
+    struct Iface { double alpha[1]; };
+    __device__ __forceinline__ static void prepare(const double (&q)[MEQN], const RPParams&, double (&c)[NC]) {
+        c[0] = q[0];
     }
     template <int IXY>
-    __device__ __forceinline__ static void rpt2(const Cache&, const RPParams& p,
-                                                const double (&asdq)[MEQN], double (&bm)[MEQN],
-                                                double (&bp)[MEQN]) {
+    __device__ __forceinline__ static void speeds(const Iface&, const RPParams& p, double (&s)[MWAVES]) {
+        s[0] = (IXY == 1) ? p.c[0] : p.c[1];
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void waves(const Iface& f, const RPParams&, double (&w)[MWAVES][MEQN]) {
+        w[0][0] = f.alpha[0];
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void solve(const double (&cL)[NC], const double (&cR)[NC], const RPParams& p,
+                                                 Iface& f, double (&amdq)[MEQN], double (&apdq)[MEQN]) {
+        const double vel = (IXY == 1) ? p.c[0] : p.c[1];
+        f.alpha[0] = cR[0] - cL[0];
+        amdq[0] = fmin(vel, 0.0) * f.alpha[0];
+        apdq[0] = fmax(vel, 0.0) * f.alpha[0];
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void rpt2(const Iface&, const RPParams& p, const double (&asdq)[MEQN],
+                                                double (&bm)[MEQN], double (&bp)[MEQN]) {
         const double stran = (IXY == 1) ? p.c[1] : p.c[0];
         bm[0] = fmin(stran, 0.0) * asdq[0];
         bp[0] = fmax(stran, 0.0) * asdq[0];
@@ -60,33 +106,43 @@ struct RPAdvection {
 
 // ---------------------------------------------------------------------------
 // acoustics_2D: cparam = {rho, bulk, cc, zz}; q = (p, u, v)
+// Eigenvectors (-Z, 1, 0) at speed -c and (Z, 1, 0) at speed c.
 // ---------------------------------------------------------------------------
 struct RPAcoustics {
-    static constexpr int MEQN = 3, MWAVES = 2, ID = CLAW2_RP_ACOUSTICS;
-    struct Cache {};
-    template <int IXY>
-    __device__ __forceinline__ static void rpn2(const double (&qL)[MEQN], const double (&qR)[MEQN],
-                                                const RPParams& p, double (&wave)[MWAVES][MEQN],
-                                                double (&s)[MWAVES], double (&amdq)[MEQN],
-                                                double (&apdq)[MEQN], Cache&) {
-        constexpr int MU = Dir<IXY>::MU, MV = Dir<IXY>::MV;
-        const double cc = p.c[2], zz = p.c[3];
-        const double delta1 = qR[0] - qL[0];
-        const double delta2 = qR[MU] - qL[MU];
-        const double a1 = (-delta1 + zz * delta2) / (2.0 * zz);
-        const double a2 = (delta1 + zz * delta2) / (2.0 * zz);
-        wave[0][0] = -a1 * zz; wave[0][MU] = a1; wave[0][MV] = 0.0; s[0] = -cc;
-        wave[1][0] = a2 * zz;  wave[1][MU] = a2; wave[1][MV] = 0.0; s[1] = cc;
-#pragma unroll
-        for (int m = 0; m < MEQN; ++m) {
-            amdq[m] = s[0] * wave[0][m];
-            apdq[m] = s[1] * wave[1][m];
-        }
+    static constexpr int MEQN = 3, MWAVES = 2, NC = 3, ID = CLAW2_RP_ACOUSTICS;
+    struct Iface { double alpha[2]; };
+    __device__ __forceinline__ static void prepare(const double (&q)[MEQN], const RPParams&, double (&c)[NC]) {
+        c[0] = q[0]; c[1] = q[1]; c[2] = q[2];
     }
     template <int IXY>
-    __device__ __forceinline__ static void rpt2(const Cache&, const RPParams& p,
-                                                const double (&asdq)[MEQN], double (&bm)[MEQN],
-                                                double (&bp)[MEQN]) {
+    __device__ __forceinline__ static void speeds(const Iface&, const RPParams& p, double (&s)[MWAVES]) {
+        s[0] = -p.c[2];
+        s[1] = p.c[2];
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void waves(const Iface& f, const RPParams& p, double (&w)[MWAVES][MEQN]) {
+        constexpr int MU = Dir<IXY>::MU, MV = Dir<IXY>::MV;
+        const double zz = p.c[3];
+        w[0][0] = -f.alpha[0] * zz; w[0][MU] = f.alpha[0]; w[0][MV] = 0.0;
+        w[1][0] = f.alpha[1] * zz;  w[1][MU] = f.alpha[1]; w[1][MV] = 0.0;
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void solve(const double (&cL)[NC], const double (&cR)[NC], const RPParams& p,
+                                                 Iface& f, double (&amdq)[MEQN], double (&apdq)[MEQN]) {
+        constexpr int MU = Dir<IXY>::MU, MV = Dir<IXY>::MV;
+        const double cc = p.c[2], zz = p.c[3];
+        const double delta1 = cR[0] - cL[0];
+        const double delta2 = cR[MU] - cL[MU];
+        const double a1 = (-delta1 + zz * delta2) / (2.0 * zz);
+        const double a2 = (delta1 + zz * delta2) / (2.0 * zz);
+        f.alpha[0] = a1;
+        f.alpha[1] = a2;
+        amdq[0] = -cc * (-a1 * zz); amdq[MU] = -cc * a1; amdq[MV] = 0.0;
+        apdq[0] = cc * (a2 * zz);   apdq[MU] = cc * a2;  apdq[MV] = 0.0;
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void rpt2(const Iface&, const RPParams& p, const double (&asdq)[MEQN],
+                                                double (&bm)[MEQN], double (&bp)[MEQN]) {
         constexpr int MU = Dir<IXY>::MU, MV = Dir<IXY>::MV;
         const double cc = p.c[2], zz = p.c[3];
         const double a1 = (-asdq[0] + zz * asdq[MV]) / (2.0 * zz);
@@ -99,113 +155,112 @@ struct RPAcoustics {
 // ---------------------------------------------------------------------------
 // euler_4wave_2D (Roe): cparam = {gamma, efix}; q = (rho, rho u, rho v, E)
 // Waves: 1 = u-c acoustic, 2 = entropy (u), 3 = shear (u), 4 = u+c acoustic.
+// Cell: q, sqrt(rho), u, v, H = (E + p)/rho, c = sqrt(gamma p / rho).
+// Iface: strengths in wave order + Roe state (normal u, transverse v, a, 1/a, H).
 // ---------------------------------------------------------------------------
 struct RPEulerRoe {
-    static constexpr int MEQN = 4, MWAVES = 4, ID = CLAW2_RP_EULER_ROE;
-    struct Cache { double u, v, a, enth, u2v2, g1a2, euv; };
+    static constexpr int MEQN = 4, MWAVES = 4, NC = 9, ID = CLAW2_RP_EULER_ROE;
+    enum { RS = 4, UX = 5, UY = 6, HH = 7, CS = 8 };
+    struct Iface { double alpha[4]; double u, v, a, ia, H; };
 
+    __device__ __forceinline__ static void prepare(const double (&q)[MEQN], const RPParams& p, double (&c)[NC]) {
+        const double gamma = p.c[0], gamma1 = gamma - 1.0;
+        const double irho = 1.0 / q[0];
+        const double u = q[1] * irho, v = q[2] * irho;
+        const double pr = gamma1 * (q[3] - 0.5 * (q[1] * u + q[2] * v));
+        c[0] = q[0]; c[1] = q[1]; c[2] = q[2]; c[3] = q[3];
+        c[RS] = sqrt(q[0]);
+        c[UX] = u;
+        c[UY] = v;
+        c[HH] = (q[3] + pr) * irho;
+        c[CS] = sqrt(gamma * pr * irho);
+    }
     template <int IXY>
-    __device__ __forceinline__ static void roe_state(const double (&qL)[MEQN], const double (&qR)[MEQN],
-                                                     double gamma1, Cache& c) {
+    __device__ __forceinline__ static void speeds(const Iface& f, const RPParams&, double (&s)[MWAVES]) {
+        s[0] = f.u - f.a;
+        s[1] = f.u;
+        s[2] = f.u;
+        s[3] = f.u + f.a;
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void waves(const Iface& f, const RPParams&, double (&w)[MWAVES][MEQN]) {
         constexpr int MU = Dir<IXY>::MU, MV = Dir<IXY>::MV;
-        const double rhsqrtl = sqrt(qL[0]);
-        const double rhsqrtr = sqrt(qR[0]);
-        const double pl = gamma1 * (qL[3] - 0.5 * (qL[1] * qL[1] + qL[2] * qL[2]) / qL[0]);
-        const double pr = gamma1 * (qR[3] - 0.5 * (qR[1] * qR[1] + qR[2] * qR[2]) / qR[0]);
-        const double rhsq2 = rhsqrtl + rhsqrtr;
-        c.u = (qL[MU] / rhsqrtl + qR[MU] / rhsqrtr) / rhsq2;
-        c.v = (qL[MV] / rhsqrtl + qR[MV] / rhsqrtr) / rhsq2;
-        c.enth = (((qL[3] + pl) / rhsqrtl + (qR[3] + pr) / rhsqrtr)) / rhsq2;
-        c.u2v2 = c.u * c.u + c.v * c.v;
-        const double a2 = gamma1 * (c.enth - 0.5 * c.u2v2);
-        c.a = sqrt(a2);
-        c.g1a2 = gamma1 / a2;
-        c.euv = c.enth - c.u2v2;
+        const double u = f.u, v = f.v, a = f.a, H = f.H;
+        const double b1 = f.alpha[0], b3 = f.alpha[1], b2 = f.alpha[2], b4 = f.alpha[3];
+        w[0][0] = b1; w[0][MU] = b1 * (u - a); w[0][MV] = b1 * v; w[0][3] = b1 * (H - u * a);
+        w[1][0] = b3; w[1][MU] = b3 * u; w[1][MV] = b3 * v; w[1][3] = b3 * 0.5 * (u * u + v * v);
+        w[2][0] = 0.0; w[2][MU] = 0.0; w[2][MV] = b2; w[2][3] = b2 * v;
+        w[3][0] = b4; w[3][MU] = b4 * (u + a); w[3][MV] = b4 * v; w[3][3] = b4 * (H + u * a);
     }
 
     template <int IXY>
-    __device__ __forceinline__ static void rpn2(const double (&qL)[MEQN], const double (&qR)[MEQN],
-                                                const RPParams& p, double (&wave)[MWAVES][MEQN],
-                                                double (&s)[MWAVES], double (&amdq)[MEQN],
-                                                double (&apdq)[MEQN], Cache& c) {
+    __device__ __forceinline__ static void solve(const double (&cL)[NC], const double (&cR)[NC], const RPParams& p,
+                                                 Iface& f, double (&amdq)[MEQN], double (&apdq)[MEQN]) {
         constexpr int MU = Dir<IXY>::MU, MV = Dir<IXY>::MV;
-        const double gamma = p.c[0];
-        const double gamma1 = gamma - 1.0;
-        roe_state<IXY>(qL, qR, gamma1, c);
-        const double u = c.u, v = c.v, a = c.a, enth = c.enth;
-        const double delta0 = qR[0] - qL[0];
-        const double delta1 = qR[MU] - qL[MU];
-        const double delta2 = qR[MV] - qL[MV];
-        const double delta3 = qR[3] - qL[3];
-        const double b3 = c.g1a2 * (c.euv * delta0 + u * delta1 + v * delta2 - delta3);
-        const double b2 = delta2 - v * delta0;
-        const double b4 = (delta1 + (a - u) * delta0 - a * b3) / (2.0 * a);
-        const double b1 = delta0 - b3 - b4;
+        constexpr int UN = (IXY == 1) ? UX : UY, UT = (IXY == 1) ? UY : UX;
+        const double gamma = p.c[0], gamma1 = gamma - 1.0;
+        // Roe averages with weights sqrt(rho) / (sqrt(rho_L) + sqrt(rho_R))
+        const double inv = 1.0 / (cL[RS] + cR[RS]);
+        const double wl = cL[RS] * inv, wr = cR[RS] * inv;
+        const double u = wl * cL[UN] + wr * cR[UN];
+        const double v = wl * cL[UT] + wr * cR[UT];
+        const double H = wl * cL[HH] + wr * cR[HH];
+        const double u2v2 = u * u + v * v;
+        const double a2 = gamma1 * (H - 0.5 * u2v2);
+        const double ia = rsqrt(a2);
+        const double a = a2 * ia;
+        const double g1a2 = gamma1 * ia * ia;
+        const double euv = H - u2v2;
+        const double d0 = cR[0] - cL[0], d1 = cR[MU] - cL[MU], d2 = cR[MV] - cL[MV], d3 = cR[3] - cL[3];
+        const double b3 = g1a2 * (euv * d0 + u * d1 + v * d2 - d3);
+        const double b2 = d2 - v * d0;
+        const double b4 = (d1 + (a - u) * d0 - a * b3) * (0.5 * ia);
+        const double b1 = d0 - b3 - b4;
+        f.alpha[0] = b1; f.alpha[1] = b3; f.alpha[2] = b2; f.alpha[3] = b4;
+        f.u = u; f.v = v; f.a = a; f.ia = ia; f.H = H;
 
-        wave[0][0] = b1; wave[0][MU] = b1 * (u - a); wave[0][MV] = b1 * v;
-        wave[0][3] = b1 * (enth - u * a); s[0] = u - a;
-        wave[1][0] = b3; wave[1][MU] = b3 * u; wave[1][MV] = b3 * v;
-        wave[1][3] = b3 * 0.5 * c.u2v2; s[1] = u;
-        wave[2][0] = 0.0; wave[2][MU] = 0.0; wave[2][MV] = b2;
-        wave[2][3] = b2 * v; s[2] = u;
-        wave[3][0] = b4; wave[3][MU] = b4 * (u + a); wave[3][MV] = b4 * v;
-        wave[3][3] = b4 * (enth + u * a); s[3] = u + a;
-
+        double w[MWAVES][MEQN], s[MWAVES];
+        waves<IXY>(f, p, w);
+        speeds<IXY>(f, p, s);
         if (p.flags == 0) {
-#pragma unroll
-            for (int m = 0; m < MEQN; ++m) {
-                double am = 0.0, ap = 0.0;
-#pragma unroll
-                for (int mw = 0; mw < MWAVES; ++mw) {
-                    if (s[mw] < 0.0) am = am + s[mw] * wave[mw][m];
-                    else ap = ap + s[mw] * wave[mw][m];
-                }
-                amdq[m] = am;
-                apdq[m] = ap;
-            }
+            split_fluct<MEQN, MWAVES>(s, w, amdq, apdq);
             return;
         }
-        // Harten-Hyman entropy fix (same branch structure as the oracle).
+        // Harten-Hyman entropy fix (branch structure of the oracle)
         bool done = false;
         {
-            const double rhoim1 = qL[0];
-            const double pim1 = gamma1 * (qL[3] - 0.5 * (qL[MU] * qL[MU] + qL[MV] * qL[MV]) / rhoim1);
-            const double cim1 = sqrt(gamma * pim1 / rhoim1);
-            const double s0 = qL[MU] / rhoim1 - cim1;
+            const double s0 = cL[UN] - cL[CS];  // u - c in the left state
             if (s0 >= 0.0 && s[0] > 0.0) {
 #pragma unroll
                 for (int m = 0; m < MEQN; ++m) amdq[m] = 0.0;
                 done = true;
             } else {
-                const double rho1 = qL[0] + wave[0][0];
-                const double rhou1 = qL[MU] + wave[0][MU];
-                const double rhov1 = qL[MV] + wave[0][MV];
-                const double en1 = qL[3] + wave[0][3];
-                const double p1 = gamma1 * (en1 - 0.5 * (rhou1 * rhou1 + rhov1 * rhov1) / rho1);
-                const double c1 = sqrt(gamma * p1 / rho1);
-                const double s1 = rhou1 / rho1 - c1;
+                const double rho1 = cL[0] + w[0][0];
+                const double rhou1 = cL[MU] + w[0][MU];
+                const double rhov1 = cL[MV] + w[0][MV];
+                const double en1 = cL[3] + w[0][3];
+                const double ir1 = 1.0 / rho1;
+                const double p1 = gamma1 * (en1 - 0.5 * (rhou1 * rhou1 + rhov1 * rhov1) * ir1);
+                const double s1 = rhou1 * ir1 - sqrt(gamma * p1 * ir1);  // u - c right of the 1-wave
                 double sfract;
                 if (s0 < 0.0 && s1 > 0.0) sfract = s0 * (s1 - s[0]) / (s1 - s0);
                 else if (s[0] < 0.0) sfract = s[0];
                 else sfract = 0.0;
 #pragma unroll
-                for (int m = 0; m < MEQN; ++m) amdq[m] = sfract * wave[0][m];
+                for (int m = 0; m < MEQN; ++m) amdq[m] = sfract * w[0][m];
             }
         }
         if (!done && !(s[1] >= 0.0)) {
 #pragma unroll
-            for (int m = 0; m < MEQN; ++m) amdq[m] = amdq[m] + s[1] * wave[1][m] + s[2] * wave[2][m];
-            const double rhoi = qR[0];
-            const double pi = gamma1 * (qR[3] - 0.5 * (qR[MU] * qR[MU] + qR[MV] * qR[MV]) / rhoi);
-            const double ci = sqrt(gamma * pi / rhoi);
-            const double s3 = qR[MU] / rhoi + ci;
-            const double rho2 = qR[0] - wave[3][0];
-            const double rhou2 = qR[MU] - wave[3][MU];
-            const double rhov2 = qR[MV] - wave[3][MV];
-            const double en2 = qR[3] - wave[3][3];
-            const double p2 = gamma1 * (en2 - 0.5 * (rhou2 * rhou2 + rhov2 * rhov2) / rho2);
-            const double c2 = sqrt(gamma * p2 / rho2);
-            const double s2 = rhou2 / rho2 + c2;
+            for (int m = 0; m < MEQN; ++m) amdq[m] = amdq[m] + s[1] * w[1][m] + s[2] * w[2][m];
+            const double s3 = cR[UN] + cR[CS];  // u + c in the right state
+            const double rho2 = cR[0] - w[3][0];
+            const double rhou2 = cR[MU] - w[3][MU];
+            const double rhov2 = cR[MV] - w[3][MV];
+            const double en2 = cR[3] - w[3][3];
+            const double ir2 = 1.0 / rho2;
+            const double p2 = gamma1 * (en2 - 0.5 * (rhou2 * rhou2 + rhov2 * rhov2) * ir2);
+            const double s2 = rhou2 * ir2 + sqrt(gamma * p2 * ir2);  // u + c left of the 4-wave
             double sfract = 0.0;
             bool add = true;
             if (s2 < 0.0 && s3 > 0.0) sfract = s2 * (s3 - s[3]) / (s3 - s2);
@@ -213,121 +268,136 @@ struct RPEulerRoe {
             else add = false;
             if (add) {
 #pragma unroll
-                for (int m = 0; m < MEQN; ++m) amdq[m] = amdq[m] + sfract * wave[3][m];
+                for (int m = 0; m < MEQN; ++m) amdq[m] = amdq[m] + sfract * w[3][m];
             }
         }
 #pragma unroll
         for (int m = 0; m < MEQN; ++m) {
             double df = 0.0;
 #pragma unroll
-            for (int mw = 0; mw < MWAVES; ++mw) df = df + s[mw] * wave[mw][m];
+            for (int k = 0; k < MWAVES; ++k) df = df + s[k] * w[k][m];
             apdq[m] = df - amdq[m];
         }
     }
 
+    // Transverse eigenvectors at the Roe state (v is now the "normal" speed):
+    // r1 = (1, u, v-a, H-va), r2 = (1, u, v, |u|^2/2), r3 = (0, 1, 0, u), r4 = (1, u, v+a, H+va);
+    // B-dq = sum min(s_k,0) b_k r_k, B+dq = sum max(s_k,0) b_k r_k.
     template <int IXY>
-    __device__ __forceinline__ static void rpt2(const Cache& c, const RPParams&,
-                                                const double (&asdq)[MEQN], double (&bm)[MEQN],
-                                                double (&bp)[MEQN]) {
+    __device__ __forceinline__ static void rpt2(const Iface& f, const RPParams& p, const double (&asdq)[MEQN],
+                                                double (&bm)[MEQN], double (&bp)[MEQN]) {
         constexpr int MU = Dir<IXY>::MU, MV = Dir<IXY>::MV;
-        const double u = c.u, v = c.v, a = c.a, enth = c.enth;
-        const double b3 = c.g1a2 * (c.euv * asdq[0] + u * asdq[MU] + v * asdq[MV] - asdq[3]);
+        const double gamma1 = p.c[0] - 1.0;
+        const double u = f.u, v = f.v, a = f.a, H = f.H;
+        const double u2v2 = u * u + v * v;
+        const double g1a2 = gamma1 * f.ia * f.ia;
+        const double euv = H - u2v2;
+        const double b3 = g1a2 * (euv * asdq[0] + u * asdq[MU] + v * asdq[MV] - asdq[3]);
         const double b2 = asdq[MU] - u * asdq[0];
-        const double b4 = (asdq[MV] + (a - v) * asdq[0] - a * b3) / (2.0 * a);
+        const double b4 = (asdq[MV] + (a - v) * asdq[0] - a * b3) * (0.5 * f.ia);
         const double b1 = asdq[0] - b3 - b4;
-        double wb[MWAVES][MEQN], sb[MWAVES];
-        wb[0][0] = b1; wb[0][MU] = b1 * u; wb[0][MV] = b1 * (v - a); wb[0][3] = b1 * (enth - v * a); sb[0] = v - a;
-        wb[1][0] = b3; wb[1][MU] = b3 * u; wb[1][MV] = b3 * v; wb[1][3] = b3 * 0.5 * c.u2v2; sb[1] = v;
-        wb[2][0] = 0.0; wb[2][MU] = b2; wb[2][MV] = 0.0; wb[2][3] = b2 * u; sb[2] = v;
-        wb[3][0] = b4; wb[3][MU] = b4 * u; wb[3][MV] = b4 * (v + a); wb[3][3] = b4 * (enth + v * a); sb[3] = v + a;
-#pragma unroll
-        for (int m = 0; m < MEQN; ++m) {
-            double xm = 0.0, xp = 0.0;
-#pragma unroll
-            for (int mw = 0; mw < MWAVES; ++mw) {
-                xm = xm + fmin(sb[mw], 0.0) * wb[mw][m];
-                xp = xp + fmax(sb[mw], 0.0) * wb[mw][m];
-            }
-            bm[m] = xm;
-            bp[m] = xp;
-        }
+        const double s1 = v - a, s4 = v + a;
+        const double m1 = fmin(s1, 0.0) * b1, m3 = fmin(v, 0.0) * b3, m2 = fmin(v, 0.0) * b2, m4 = fmin(s4, 0.0) * b4;
+        const double p1 = fmax(s1, 0.0) * b1, p3 = fmax(v, 0.0) * b3, p2 = fmax(v, 0.0) * b2, p4 = fmax(s4, 0.0) * b4;
+        const double va = v * a, hke = 0.5 * u2v2;
+        double sm = m1 + m3 + m4, sp = p1 + p3 + p4;
+        bm[0] = sm;
+        bm[MU] = u * sm + m2;
+        bm[MV] = v * sm + a * (m4 - m1);
+        bm[3] = H * (m1 + m4) + va * (m4 - m1) + hke * m3 + u * m2;
+        bp[0] = sp;
+        bp[MU] = u * sp + p2;
+        bp[MV] = v * sp + a * (p4 - p1);
+        bp[3] = H * (p1 + p4) + va * (p4 - p1) + hke * p3 + u * p2;
     }
 };
 
 // ---------------------------------------------------------------------------
 // shallow_roe_with_efix_2D: cparam = {grav, efix}; q = (h, hu, hv)
+// Cell: q, sqrt(h), u, v, c = sqrt(g h).  Iface: strengths + (u, v, a, 1/a).
 // ---------------------------------------------------------------------------
 struct RPShallowRoe {
-    static constexpr int MEQN = 3, MWAVES = 3, ID = CLAW2_RP_SHALLOW_ROE;
-    struct Cache { double u, v, a; };
+    static constexpr int MEQN = 3, MWAVES = 3, NC = 7, ID = CLAW2_RP_SHALLOW_ROE;
+    enum { RS = 3, UX = 4, UY = 5, CS = 6 };
+    struct Iface { double alpha[3]; double u, v, a, ia; };
+
+    __device__ __forceinline__ static void prepare(const double (&q)[MEQN], const RPParams& p, double (&c)[NC]) {
+        const double grav = p.c[0];
+        const double ih = 1.0 / q[0];
+        c[0] = q[0]; c[1] = q[1]; c[2] = q[2];
+        c[RS] = sqrt(q[0]);
+        c[UX] = q[1] * ih;
+        c[UY] = q[2] * ih;
+        c[CS] = sqrt(grav * q[0]);
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void speeds(const Iface& f, const RPParams&, double (&s)[MWAVES]) {
+        s[0] = f.u - f.a;
+        s[1] = f.u;
+        s[2] = f.u + f.a;
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void waves(const Iface& f, const RPParams&, double (&w)[MWAVES][MEQN]) {
+        constexpr int MU = Dir<IXY>::MU, MV = Dir<IXY>::MV;
+        const double u = f.u, v = f.v, a = f.a;
+        const double a1 = f.alpha[0], a2 = f.alpha[1], a3 = f.alpha[2];
+        w[0][0] = a1; w[0][MU] = a1 * (u - a); w[0][MV] = a1 * v;
+        w[1][0] = 0.0; w[1][MU] = 0.0; w[1][MV] = a2;
+        w[2][0] = a3; w[2][MU] = a3 * (u + a); w[2][MV] = a3 * v;
+    }
 
     template <int IXY>
-    __device__ __forceinline__ static void rpn2(const double (&qL)[MEQN], const double (&qR)[MEQN],
-                                                const RPParams& p, double (&wave)[MWAVES][MEQN],
-                                                double (&s)[MWAVES], double (&amdq)[MEQN],
-                                                double (&apdq)[MEQN], Cache& c) {
+    __device__ __forceinline__ static void solve(const double (&cL)[NC], const double (&cR)[NC], const RPParams& p,
+                                                 Iface& f, double (&amdq)[MEQN], double (&apdq)[MEQN]) {
         constexpr int MU = Dir<IXY>::MU, MV = Dir<IXY>::MV;
+        constexpr int UN = (IXY == 1) ? UX : UY, UT = (IXY == 1) ? UY : UX;
         const double grav = p.c[0];
-        const double h = (qL[0] + qR[0]) * 0.50;
-        const double hsqrtl = sqrt(qL[0]);
-        const double hsqrtr = sqrt(qR[0]);
-        const double hsq2 = hsqrtl + hsqrtr;
-        const double u = (qL[MU] / hsqrtl + qR[MU] / hsqrtr) / hsq2;
-        const double v = (qL[MV] / hsqrtl + qR[MV] / hsqrtr) / hsq2;
-        const double a = sqrt(grav * h);
-        c.u = u; c.v = v; c.a = a;
-        const double delta0 = qR[0] - qL[0];
-        const double delta1 = qR[MU] - qL[MU];
-        const double delta2 = qR[MV] - qL[MV];
-        const double a1 = ((u + a) * delta0 - delta1) * (0.50 / a);
-        const double a2 = -v * delta0 + delta2;
-        const double a3 = (-(u - a) * delta0 + delta1) * (0.50 / a);
-        wave[0][0] = a1; wave[0][MU] = a1 * (u - a); wave[0][MV] = a1 * v; s[0] = u - a;
-        wave[1][0] = 0.0; wave[1][MU] = 0.0; wave[1][MV] = a2; s[1] = u;
-        wave[2][0] = a3; wave[2][MU] = a3 * (u + a); wave[2][MV] = a3 * v; s[2] = u + a;
+        const double inv = 1.0 / (cL[RS] + cR[RS]);
+        const double wl = cL[RS] * inv, wr = cR[RS] * inv;
+        const double u = wl * cL[UN] + wr * cR[UN];
+        const double v = wl * cL[UT] + wr * cR[UT];
+        const double gh = grav * ((cL[0] + cR[0]) * 0.50);
+        const double ia = rsqrt(gh);
+        const double a = gh * ia;
+        const double d0 = cR[0] - cL[0], d1 = cR[MU] - cL[MU], d2 = cR[MV] - cL[MV];
+        f.alpha[0] = ((u + a) * d0 - d1) * (0.50 * ia);
+        f.alpha[1] = -v * d0 + d2;
+        f.alpha[2] = (-(u - a) * d0 + d1) * (0.50 * ia);
+        f.u = u; f.v = v; f.a = a; f.ia = ia;
 
+        double w[MWAVES][MEQN], s[MWAVES];
+        waves<IXY>(f, p, w);
+        speeds<IXY>(f, p, s);
         if (p.flags == 0) {
-#pragma unroll
-            for (int m = 0; m < MEQN; ++m) {
-                double am = 0.0, ap = 0.0;
-#pragma unroll
-                for (int mw = 0; mw < MWAVES; ++mw) {
-                    if (s[mw] < 0.0) am = am + s[mw] * wave[mw][m];
-                    else ap = ap + s[mw] * wave[mw][m];
-                }
-                amdq[m] = am;
-                apdq[m] = ap;
-            }
+            split_fluct<MEQN, MWAVES>(s, w, amdq, apdq);
             return;
         }
         bool done = false;
         {
-            const double him1 = qL[0];
-            const double s0 = qL[MU] / him1 - sqrt(grav * him1);
+            const double s0 = cL[UN] - cL[CS];
             if (s0 >= 0.0 && s[0] > 0.0) {
 #pragma unroll
                 for (int m = 0; m < MEQN; ++m) amdq[m] = 0.0;
                 done = true;
             } else {
-                const double h1 = qL[0] + wave[0][0];
-                const double hu1 = qL[MU] + wave[0][MU];
-                const double s1 = hu1 / h1 - sqrt(grav * h1);
+                const double h1 = cL[0] + w[0][0];
+                const double hu1 = cL[MU] + w[0][MU];
+                const double s1 = hu1 / h1 - sqrt(grav * h1);  // speed just right of the 1-wave
                 double sfract;
                 if (s0 < 0.0 && s1 > 0.0) sfract = s0 * ((s1 - s[0]) / (s1 - s0));
                 else if (s[0] < 0.0) sfract = s[0];
                 else sfract = 0.0;
 #pragma unroll
-                for (int m = 0; m < MEQN; ++m) amdq[m] = sfract * wave[0][m];
+                for (int m = 0; m < MEQN; ++m) amdq[m] = sfract * w[0][m];
             }
         }
         if (!done && !(s[1] > 0.0)) {
 #pragma unroll
-            for (int m = 0; m < MEQN; ++m) amdq[m] = amdq[m] + s[1] * wave[1][m];
-            const double hi = qR[0];
-            const double s03 = qR[MU] / hi + sqrt(grav * hi);
-            const double h3 = qR[0] - wave[2][0];
-            const double hu3 = qR[MU] - wave[2][MU];
-            const double s3 = hu3 / h3 + sqrt(grav * h3);
+            for (int m = 0; m < MEQN; ++m) amdq[m] = amdq[m] + s[1] * w[1][m];
+            const double s03 = cR[UN] + cR[CS];
+            const double h3 = cR[0] - w[2][0];
+            const double hu3 = cR[MU] - w[2][MU];
+            const double s3 = hu3 / h3 + sqrt(grav * h3);  // speed just left of the 3-wave
             double sfract = 0.0;
             bool add = true;
             if (s3 < 0.0 && s03 > 0.0) sfract = s3 * ((s03 - s[2]) / (s03 - s3));
@@ -335,43 +405,36 @@ struct RPShallowRoe {
             else add = false;
             if (add) {
 #pragma unroll
-                for (int m = 0; m < MEQN; ++m) amdq[m] = amdq[m] + sfract * wave[2][m];
+                for (int m = 0; m < MEQN; ++m) amdq[m] = amdq[m] + sfract * w[2][m];
             }
         }
 #pragma unroll
         for (int m = 0; m < MEQN; ++m) {
             double df = 0.0;
 #pragma unroll
-            for (int mw = 0; mw < MWAVES; ++mw) df = df + s[mw] * wave[mw][m];
+            for (int k = 0; k < MWAVES; ++k) df = df + s[k] * w[k][m];
             apdq[m] = df - amdq[m];
         }
     }
 
+    // transverse eigenvectors r1 = (1, u, v-c), r2 = (0, 1, 0), r3 = (1, u, v+c)
     template <int IXY>
-    __device__ __forceinline__ static void rpt2(const Cache& c, const RPParams&,
-                                                const double (&asdq)[MEQN], double (&bm)[MEQN],
-                                                double (&bp)[MEQN]) {
+    __device__ __forceinline__ static void rpt2(const Iface& f, const RPParams&, const double (&asdq)[MEQN],
+                                                double (&bm)[MEQN], double (&bp)[MEQN]) {
         constexpr int MU = Dir<IXY>::MU, MV = Dir<IXY>::MV;
-        // transverse speeds at the Roe state: v -+ c, v (cbar = sqrt(g*hbar))
-        const double ubar = c.u, vbar = c.v, cbar = c.a;
-        const double a1 = (0.5 / cbar) * ((vbar + cbar) * asdq[0] - asdq[MV]);
-        const double a2 = -ubar * asdq[0] + asdq[MU];
-        const double a3 = (0.5 / cbar) * (-(vbar - cbar) * asdq[0] + asdq[MV]);
-        double wb[MWAVES][MEQN], sb[MWAVES];
-        wb[0][0] = a1; wb[0][MU] = a1 * ubar; wb[0][MV] = a1 * (vbar - cbar); sb[0] = vbar - cbar;
-        wb[1][0] = 0.0; wb[1][MU] = a2; wb[1][MV] = 0.0; sb[1] = vbar;
-        wb[2][0] = a3; wb[2][MU] = a3 * ubar; wb[2][MV] = a3 * (vbar + cbar); sb[2] = vbar + cbar;
-#pragma unroll
-        for (int m = 0; m < MEQN; ++m) {
-            double xm = 0.0, xp = 0.0;
-#pragma unroll
-            for (int mw = 0; mw < MWAVES; ++mw) {
-                xm = xm + fmin(sb[mw], 0.0) * wb[mw][m];
-                xp = xp + fmax(sb[mw], 0.0) * wb[mw][m];
-            }
-            bm[m] = xm;
-            bp[m] = xp;
-        }
+        const double u = f.u, v = f.v, a = f.a;
+        const double a1 = (0.5 * f.ia) * ((v + a) * asdq[0] - asdq[MV]);
+        const double a2 = -u * asdq[0] + asdq[MU];
+        const double a3 = (0.5 * f.ia) * (-(v - a) * asdq[0] + asdq[MV]);
+        const double s1 = v - a, s3 = v + a;
+        const double m1 = fmin(s1, 0.0) * a1, m2 = fmin(v, 0.0) * a2, m3 = fmin(s3, 0.0) * a3;
+        const double p1 = fmax(s1, 0.0) * a1, p2 = fmax(v, 0.0) * a2, p3 = fmax(s3, 0.0) * a3;
+        bm[0] = m1 + m3;
+        bm[MU] = u * (m1 + m3) + m2;
+        bm[MV] = v * (m1 + m3) + a * (m3 - m1);
+        bp[0] = p1 + p3;
+        bp[MU] = u * (p1 + p3) + p2;
+        bp[MV] = v * (p1 + p3) + a * (p3 - p1);
     }
 };
 

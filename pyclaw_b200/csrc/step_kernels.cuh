@@ -78,22 +78,66 @@ __device__ __forceinline__ bool all_finite(const double (&v)[ME]) {
 }
 
 // ---------------------------------------------------------------------------
+// Shared pieces of the interface work
+// ---------------------------------------------------------------------------
+
+// Limiter (limiter.f90:29-53 / philim.f90) and second-order correction
+// cqxx = sum_k coef_k * phi_k * w_k (flux2.f90:134-160) for one interface.
+// dl / dr are the dot products of each unlimited wave with the same family's
+// unlimited wave at the interface below/left and above/right.
+template <class RP, int IXY>
+__device__ __forceinline__ void correction(const typename RP::Iface& f, const RPParams& p, const Method& meth,
+                                           double dtdx, const double (&dl)[RP::MWAVES],
+                                           const double (&dr)[RP::MWAVES], double (&cq)[RP::MEQN]) {
+    constexpr int ME = RP::MEQN, MW = RP::MWAVES;
+    double s[MW];
+    RP::template speeds<IXY>(f, p, s);
+    double w[MW][ME];
+    RP::template waves<IXY>(f, p, w);
+#pragma unroll
+    for (int m = 0; m < ME; ++m) cq[m] = 0.0;
+#pragma unroll
+    for (int k = 0; k < MW; ++k) {
+        const int lim = meth.mthlim[k];
+        double wn2 = 0.0;
+#pragma unroll
+        for (int m = 0; m < ME; ++m) wn2 = wn2 + w[k][m] * w[k][m];
+        double phi = 1.0;
+        if (lim != 0 && wn2 != 0.0) phi = philim(wn2, (s[k] > 0.0) ? dl[k] : dr[k], lim);
+        const double as = fabs(s[k]);
+        const double coef = ((meth.fwave != 0) ? copysign(1.0, s[k]) : as) * (1.0 - as * dtdx);
+#pragma unroll
+        for (int m = 0; m < ME; ++m) cq[m] = cq[m] + coef * (phi * w[k][m]);
+    }
+}
+
+template <class RP, int IXY>
+__device__ __forceinline__ double iface_cfl(const typename RP::Iface& f, const RPParams& p, double dtdx) {
+    double s[RP::MWAVES];
+    RP::template speeds<IXY>(f, p, s);
+    double c = 0.0;
+#pragma unroll
+    for (int k = 0; k < RP::MWAVES; ++k) c = fmax(c, fabs(dtdx * s[k]));
+    return c;
+}
+
+// ---------------------------------------------------------------------------
 // Unsplit step (step2.f90), fused x + y sweeps.
 // ---------------------------------------------------------------------------
 template <class RP, int NT>
 struct UnsplitSmem {
-    static constexpr int ME = RP::MEQN, MW = RP::MWAVES;
-    double q[2][ME][NT];   // q of row R (double-buffered by row parity)
-    double w[MW][ME][NT];  // unlimited x-waves of row R
-    double xl[3][ME][NT];  // x-interface increments for column cp-1: rows R, R-1, R+1
-    double yl[2][ME][NT];  // y-interface increments for column cp-1: rows R-2, R-1
-    double yr[2][ME][NT];  // y-interface increments for column cp+1: rows R-2, R-1
+    static constexpr int ME = RP::MEQN, MW = RP::MWAVES, NC = RP::NC;
+    double cell[3][NC][NT];  // prepared cells of rows R-2, R-1, R (ring)
+    double w[MW][ME][NT];    // unlimited x-waves of row R
+    double xl[4][ME][NT];    // increments for column cp-1: rows R-2, R-1, R, R+1
+    double yr[2][ME][NT];    // increments for column cp+1: rows R-2, R-1
     double red[NT / 32];
 };
 
-template <class RP, int NT>
-__global__ void __launch_bounds__(NT) k_step_unsplit(const StepArgs a) {
-    constexpr int ME = RP::MEQN, MW = RP::MWAVES, W = NT - 4;
+template <class RP, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_step_unsplit(const StepArgs a) {
+    constexpr int ME = RP::MEQN, MW = RP::MWAVES, NC = RP::NC, W = NT - 4;
+    using Iface = typename RP::Iface;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     UnsplitSmem<RP, NT>& S = *reinterpret_cast<UnsplitSmem<RP, NT>*>(smem_raw);
 
@@ -112,88 +156,80 @@ __global__ void __launch_bounds__(NT) k_step_unsplit(const StepArgs a) {
     const int tl = (t > 0) ? t - 1 : 0;
     const int tr = (t < NT - 1) ? t + 1 : NT - 1;
     const double dtdx = a.dtdx, dtdy = a.dtdy;
+    const RPParams& P = a.rp;
     const int order = a.meth.order, trans = a.meth.transverse;
-    const bool fw = a.meth.fwave != 0;
     const bool tc = (order > 1) && (trans == 2);
     const double* qo = a.qold + cpl;
     double* qn = a.qnew + cpl;
 
-    double q0[ME], q1[ME], q2[ME], pf[ME];
+    double pf[ME];
     double accA[ME], accB[ME], accC[ME], accD[ME];  // rows R-2, R-1, R, R+1
-    double wY[MW][ME], sY[MW], amY[ME], apY[ME], dY[MW];  // y-interface between R-2 and R-1
-    typename RP::Cache cY;
+    Iface fY;                                       // y-interface (R-2 | R-1)
+    double amY[ME], apY[ME], dY[MW];
     double cfl = 0.0;
-
 #pragma unroll
     for (int m = 0; m < ME; ++m) {
         pf[m] = __ldg(qo + m * plane + (long long)R0 * pitch);
-        q0[m] = q1[m] = q2[m] = pf[m];
         accA[m] = accB[m] = accC[m] = accD[m] = 0.0;
         amY[m] = apY[m] = 0.0;
     }
 #pragma unroll
-    for (int mw = 0; mw < MW; ++mw) {
-        sY[mw] = 0.0;
-        dY[mw] = 0.0;
-#pragma unroll
-        for (int m = 0; m < ME; ++m) wY[mw][m] = 0.0;
-    }
+    for (int k = 0; k < MW; ++k) dY[k] = 0.0;
+    memset(&fY, 0, sizeof(fY));
 
+    int s2 = 0, s1 = 2, s0 = 1;  // ring slots of rows R, R-1, R-2
     for (int R = R0; R <= R1; ++R) {
-        // ---- rotate the q window and prefetch the next row ----
-#pragma unroll
-        for (int m = 0; m < ME; ++m) {
-            q0[m] = q1[m];
-            q1[m] = q2[m];
-            q2[m] = pf[m];
-        }
-        if (R < R1) {
-#pragma unroll
-            for (int m = 0; m < ME; ++m) pf[m] = __ldg(qo + m * plane + (long long)(R + 1) * pitch);
-        }
-        const int buf = R & 1;
-#pragma unroll
-        for (int m = 0; m < ME; ++m) S.q[buf][m][t] = q2[m];
-        __syncthreads();  // S1: row R visible; previous exchange fully consumed
-
-        // ---- y: solve the interface (R-1 | R), finish (R-2 | R-1) ----
+        // ---- row R: prepare this column's cell, prefetch the next row ----
         {
-            double wN[MW][ME], sN[MW], amN[ME], apN[ME];
-            typename RP::Cache cN;
-            RP::template rpn2<2>(q1, q2, a.rp, wN, sN, amN, apN, cN);
-            double dn[MW];
+            double q[ME], c[NC];
 #pragma unroll
-            for (int mw = 0; mw < MW; ++mw) {
-                double d = 0.0;
+            for (int m = 0; m < ME; ++m) q[m] = pf[m];
+            if (R < R1) {
 #pragma unroll
-                for (int m = 0; m < ME; ++m) d = d + wY[mw][m] * wN[mw][m];
-                dn[mw] = d;
+                for (int m = 0; m < ME; ++m) pf[m] = __ldg(qo + m * plane + (long long)(R + 1) * pitch);
             }
-            double ylB[ME], ylA[ME], yrB[ME], yrA[ME];
+            RP::prepare(q, P, c);
 #pragma unroll
-            for (int m = 0; m < ME; ++m) ylB[m] = ylA[m] = yrB[m] = yrA[m] = 0.0;
-            if (R >= R0 + 3) {
-                if (ycfl_col) {
+            for (int k = 0; k < NC; ++k) S.cell[s2][k][t] = c[k];
+        }
+        __syncthreads();  // S1: cells of row R visible; previous exchange consumed
+
+        double ylB[ME], ylA[ME], yrB[ME], yrA[ME];
 #pragma unroll
-                    for (int mw = 0; mw < MW; ++mw) cfl = fmax(cfl, fabs(dtdy * sY[mw]));
+        for (int m = 0; m < ME; ++m) ylB[m] = ylA[m] = yrB[m] = yrA[m] = 0.0;
+
+        // ---- y: solve (R-1 | R), finish (R-2 | R-1) ----
+        if (R > R0) {
+            double cB[NC], cA[NC];
+#pragma unroll
+            for (int k = 0; k < NC; ++k) {
+                cB[k] = S.cell[s1][k][t];
+                cA[k] = S.cell[s2][k][t];
+            }
+            Iface fN;
+            double amN[ME], apN[ME];
+            RP::template solve<2>(cB, cA, P, fN, amN, apN);
+            double dn[MW];
+            {
+                double wY[MW][ME], wN[MW][ME];
+                RP::template waves<2>(fY, P, wY);
+                RP::template waves<2>(fN, P, wN);
+#pragma unroll
+                for (int k = 0; k < MW; ++k) {
+                    double d = 0.0;
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) d = d + wY[k][m] * wN[k][m];
+                    dn[k] = d;
                 }
+            }
+            if (R >= R0 + 3) {
+                if (ycfl_col) cfl = fmax(cfl, iface_cfl<RP, 2>(fY, P, dtdy));
                 double cq[ME];
-#pragma unroll
-                for (int m = 0; m < ME; ++m) cq[m] = 0.0;
                 if (order != 1) {
+                    correction<RP, 2>(fY, P, a.meth, dtdy, dY, dn, cq);
+                } else {
 #pragma unroll
-                    for (int mw = 0; mw < MW; ++mw) {
-                        const int lim = a.meth.mthlim[mw];
-                        double wn2 = 0.0;
-#pragma unroll
-                        for (int m = 0; m < ME; ++m) wn2 = wn2 + wY[mw][m] * wY[mw][m];
-                        double phi = 1.0;
-                        if (lim != 0 && wn2 != 0.0) phi = philim(wn2, (sY[mw] > 0.0) ? dY[mw] : dn[mw], lim);
-                        const double as = fabs(sY[mw]);
-                        const double coef = (fw ? copysign(1.0, sY[mw]) : as) * (1.0 - as * dtdy);
-#pragma unroll
-                        for (int m = 0; m < ME; ++m) cq[m] = cq[m] + coef * (phi * wY[mw][m]);
-                    }
+                    for (int m = 0; m < ME; ++m) cq[m] = 0.0;
                 }
 #pragma unroll
                 for (int m = 0; m < ME; ++m) {
@@ -202,150 +238,133 @@ __global__ void __launch_bounds__(NT) k_step_unsplit(const StepArgs a) {
                     accB[m] = accB[m] - dtdy * (apY[m] - f);
                 }
                 if (trans > 0) {
+                    const double h = 0.5 * dtdy * dtdx;
                     double as2[ME], bm[ME], bp[ME];
-                    const double h = 0.5 * dtdy;
 #pragma unroll
                     for (int m = 0; m < ME; ++m) as2[m] = tc ? amY[m] + cq[m] : amY[m];
-                    RP::template rpt2<2>(cY, a.rp, as2, bm, bp);  // imp = 1 -> row R-2
+                    RP::template rpt2<2>(fY, P, as2, bm, bp);  // imp = 1 -> row R-2
 #pragma unroll
                     for (int m = 0; m < ME; ++m) {
-                        const double gb = h * bm[m], ga = h * bp[m];
-                        accA[m] = accA[m] + dtdx * (ga - gb);
-                        ylB[m] = dtdx * gb;
-                        yrB[m] = -dtdx * ga;
+                        accA[m] = accA[m] + h * (bp[m] - bm[m]);
+                        ylB[m] = h * bm[m];
+                        yrB[m] = -h * bp[m];
                     }
 #pragma unroll
                     for (int m = 0; m < ME; ++m) as2[m] = tc ? apY[m] - cq[m] : apY[m];
-                    RP::template rpt2<2>(cY, a.rp, as2, bm, bp);  // imp = 2 -> row R-1
+                    RP::template rpt2<2>(fY, P, as2, bm, bp);  // imp = 2 -> row R-1
 #pragma unroll
                     for (int m = 0; m < ME; ++m) {
-                        const double gb = h * bm[m], ga = h * bp[m];
-                        accB[m] = accB[m] + dtdx * (ga - gb);
-                        ylA[m] = dtdx * gb;
-                        yrA[m] = -dtdx * ga;
+                        accB[m] = accB[m] + h * (bp[m] - bm[m]);
+                        ylA[m] = h * bm[m];
+                        yrA[m] = -h * bp[m];
                     }
                 }
             }
-#pragma unroll
-            for (int m = 0; m < ME; ++m) {
-                S.yl[0][m][t] = ylB[m];
-                S.yl[1][m][t] = ylA[m];
-                S.yr[0][m][t] = yrB[m];
-                S.yr[1][m][t] = yrA[m];
-            }
-            // shift the pipeline: (R-1 | R) becomes the pending interface
-#pragma unroll
-            for (int mw = 0; mw < MW; ++mw) {
-                sY[mw] = sN[mw];
-                dY[mw] = dn[mw];
-#pragma unroll
-                for (int m = 0; m < ME; ++m) wY[mw][m] = wN[mw][m];
-            }
+            fY = fN;
 #pragma unroll
             for (int m = 0; m < ME; ++m) { amY[m] = amN[m]; apY[m] = apN[m]; }
-            cY = cN;
+#pragma unroll
+            for (int k = 0; k < MW; ++k) dY[k] = dn[k];
         }
 
-        // ---- x: the interface between (cp-1, R) and (cp, R) ----
+        // ---- x: the interface (cp-1 | cp) on row R ----
         const bool xrow = (R > R0) && (R < R1);  // rows R0+1 .. R1-1
-        double wX[MW][ME], sX[MW], amX[ME], apX[ME];
-        typename RP::Cache cX;
+        Iface fX;
+        double amX[ME], apX[ME];
         {
-            double qL[ME];
+            double cL[NC], cR[NC];
 #pragma unroll
-            for (int m = 0; m < ME; ++m) qL[m] = S.q[buf][m][tl];
-            RP::template rpn2<1>(qL, q2, a.rp, wX, sX, amX, apX, cX);
+            for (int k = 0; k < NC; ++k) {
+                cL[k] = S.cell[s2][k][tl];
+                cR[k] = S.cell[s2][k][t];
+            }
+            RP::template solve<1>(cL, cR, P, fX, amX, apX);
+            double wX[MW][ME];
+            RP::template waves<1>(fX, P, wX);
+#pragma unroll
+            for (int k = 0; k < MW; ++k)
+#pragma unroll
+                for (int m = 0; m < ME; ++m) S.w[k][m][t] = wX[k][m];
         }
-#pragma unroll
-        for (int mw = 0; mw < MW; ++mw)
-#pragma unroll
-            for (int m = 0; m < ME; ++m) S.w[mw][m][t] = wX[mw][m];
         __syncthreads();  // S2: x-waves of row R visible
 
-        {
-            double xcL[ME], xbL[ME], xaL[ME];
+        double xcL[ME], xbL[ME], xaL[ME];
 #pragma unroll
-            for (int m = 0; m < ME; ++m) xcL[m] = xbL[m] = xaL[m] = 0.0;
-            if (xrow) {
-                if (xcfl_col) {
+        for (int m = 0; m < ME; ++m) xcL[m] = xbL[m] = xaL[m] = 0.0;
+        if (xrow) {
+            if (xcfl_col) cfl = fmax(cfl, iface_cfl<RP, 1>(fX, P, dtdx));
+            double cq[ME];
+            if (order != 1) {
+                double dl[MW], dr[MW];
 #pragma unroll
-                    for (int mw = 0; mw < MW; ++mw) cfl = fmax(cfl, fabs(dtdx * sX[mw]));
+                for (int k = 0; k < MW; ++k) {
+                    double x = 0.0, y = 0.0;
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) {
+                        const double w = S.w[k][m][t];
+                        x = x + S.w[k][m][tl] * w;
+                        y = y + w * S.w[k][m][tr];
+                    }
+                    dl[k] = x;
+                    dr[k] = y;
                 }
-                double cq[ME];
+                correction<RP, 1>(fX, P, a.meth, dtdx, dl, dr, cq);
+            } else {
 #pragma unroll
                 for (int m = 0; m < ME; ++m) cq[m] = 0.0;
-                if (order != 1) {
-#pragma unroll
-                    for (int mw = 0; mw < MW; ++mw) {
-                        const int lim = a.meth.mthlim[mw];
-                        double wn2 = 0.0, dl = 0.0, dr = 0.0;
-#pragma unroll
-                        for (int m = 0; m < ME; ++m) {
-                            const double w = wX[mw][m];
-                            wn2 = wn2 + w * w;
-                            dl = dl + S.w[mw][m][tl] * w;
-                            dr = dr + w * S.w[mw][m][tr];
-                        }
-                        double phi = 1.0;
-                        if (lim != 0 && wn2 != 0.0) phi = philim(wn2, (sX[mw] > 0.0) ? dl : dr, lim);
-                        const double as = fabs(sX[mw]);
-                        const double coef = (fw ? copysign(1.0, sX[mw]) : as) * (1.0 - as * dtdx);
-#pragma unroll
-                        for (int m = 0; m < ME; ++m) cq[m] = cq[m] + coef * (phi * wX[mw][m]);
-                    }
-                }
-#pragma unroll
-                for (int m = 0; m < ME; ++m) {
-                    const double f = 0.5 * cq[m];
-                    accC[m] = accC[m] - dtdx * (apX[m] - f);
-                    xcL[m] = -dtdx * (amX[m] + f);
-                }
-                if (trans > 0) {
-                    double as2[ME], bm[ME], bp[ME];
-                    const double h = 0.5 * dtdx;
-#pragma unroll
-                    for (int m = 0; m < ME; ++m) as2[m] = tc ? amX[m] + cq[m] : amX[m];
-                    RP::template rpt2<1>(cX, a.rp, as2, bm, bp);  // imp = 1 -> column cp-1
-#pragma unroll
-                    for (int m = 0; m < ME; ++m) {
-                        const double gb = h * bm[m], ga = h * bp[m];
-                        xcL[m] = xcL[m] + dtdy * (ga - gb);
-                        xbL[m] = dtdy * gb;
-                        xaL[m] = -dtdy * ga;
-                    }
-#pragma unroll
-                    for (int m = 0; m < ME; ++m) as2[m] = tc ? apX[m] - cq[m] : apX[m];
-                    RP::template rpt2<1>(cX, a.rp, as2, bm, bp);  // imp = 2 -> column cp
-#pragma unroll
-                    for (int m = 0; m < ME; ++m) {
-                        const double gb = h * bm[m], ga = h * bp[m];
-                        accC[m] = accC[m] + dtdy * (ga - gb);
-                        accB[m] = accB[m] + dtdy * gb;
-                        accD[m] = accD[m] - dtdy * ga;
-                    }
-                }
             }
 #pragma unroll
             for (int m = 0; m < ME; ++m) {
-                S.xl[0][m][t] = xcL[m];
-                S.xl[1][m][t] = xbL[m];
-                S.xl[2][m][t] = xaL[m];
+                const double f = 0.5 * cq[m];
+                accC[m] = accC[m] - dtdx * (apX[m] - f);
+                xcL[m] = -dtdx * (amX[m] + f);
             }
+            if (trans > 0) {
+                const double h = 0.5 * dtdx * dtdy;
+                double as2[ME], bm[ME], bp[ME];
+#pragma unroll
+                for (int m = 0; m < ME; ++m) as2[m] = tc ? amX[m] + cq[m] : amX[m];
+                RP::template rpt2<1>(fX, P, as2, bm, bp);  // imp = 1 -> column cp-1
+#pragma unroll
+                for (int m = 0; m < ME; ++m) {
+                    xcL[m] = xcL[m] + h * (bp[m] - bm[m]);
+                    xbL[m] = h * bm[m];
+                    xaL[m] = -h * bp[m];
+                }
+#pragma unroll
+                for (int m = 0; m < ME; ++m) as2[m] = tc ? apX[m] - cq[m] : apX[m];
+                RP::template rpt2<1>(fX, P, as2, bm, bp);  // imp = 2 -> column cp
+#pragma unroll
+                for (int m = 0; m < ME; ++m) {
+                    accC[m] = accC[m] + h * (bp[m] - bm[m]);
+                    accB[m] = accB[m] + h * bm[m];
+                    accD[m] = accD[m] - h * bp[m];
+                }
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < ME; ++m) {
+            S.xl[0][m][t] = ylB[m];
+            S.xl[1][m][t] = xbL[m] + ylA[m];
+            S.xl[2][m][t] = xcL[m];
+            S.xl[3][m][t] = xaL[m];
+            S.yr[0][m][t] = yrB[m];
+            S.yr[1][m][t] = yrA[m];
         }
         __syncthreads();  // S3: neighbour increments visible
 #pragma unroll
         for (int m = 0; m < ME; ++m) {
-            accA[m] = accA[m] + S.yl[0][m][tr] + S.yr[0][m][tl];
-            accB[m] = accB[m] + S.xl[1][m][tr] + S.yl[1][m][tr] + S.yr[1][m][tl];
-            accC[m] = accC[m] + S.xl[0][m][tr];
-            accD[m] = accD[m] + S.xl[2][m][tr];
+            accA[m] = accA[m] + S.xl[0][m][tr] + S.yr[0][m][tl];
+            accB[m] = accB[m] + S.xl[1][m][tr] + S.yr[1][m][tl];
+            accC[m] = accC[m] + S.xl[2][m][tr];
+            accD[m] = accD[m] + S.xl[3][m][tr];
         }
 
         // ---- row R-2 is complete ----
         if (R >= R0 + 4 && out_col) {
             double v[ME];
 #pragma unroll
-            for (int m = 0; m < ME; ++m) v[m] = q0[m] + accA[m];
+            for (int m = 0; m < ME; ++m) v[m] = S.cell[s0][m][t] + accA[m];
 #pragma unroll
             for (int m = 0; m < ME; ++m) qn[m * plane + (long long)(R - 2) * pitch] = v[m];
             if (!all_finite<ME>(v)) atomicOr(a.status, 1);
@@ -357,6 +376,10 @@ __global__ void __launch_bounds__(NT) k_step_unsplit(const StepArgs a) {
             accC[m] = accD[m];
             accD[m] = 0.0;
         }
+        const int tmp = s0;
+        s0 = s1;
+        s1 = s2;
+        s2 = tmp;
     }
     cfl_commit(cfl, S.red, a.cfl_bits);
 }
@@ -366,12 +389,20 @@ __global__ void __launch_bounds__(NT) k_step_unsplit(const StepArgs a) {
 // terms.  Writes the interior columns of qtmp and copies the ghost columns.
 // ---------------------------------------------------------------------------
 template <class RP, int NT>
+struct SplitXSmem {
+    static constexpr int ME = RP::MEQN, MW = RP::MWAVES, NC = RP::NC;
+    double cell[2][NC][NT];
+    double w[MW][ME][NT];
+    double xl[ME][NT];
+    double red[NT / 32];
+};
+
+template <class RP, int NT>
 __global__ void __launch_bounds__(NT) k_split_x(const StepArgs a) {
-    constexpr int ME = RP::MEQN, MW = RP::MWAVES, W = NT - 4;
-    __shared__ double sQ[2][ME][NT];
-    __shared__ double sW[MW][ME][NT];
-    __shared__ double sXL[ME][NT];
-    __shared__ double sRed[NT / 32];
+    constexpr int ME = RP::MEQN, MW = RP::MWAVES, NC = RP::NC, W = NT - 4;
+    using Iface = typename RP::Iface;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SplitXSmem<RP, NT>& S = *reinterpret_cast<SplitXSmem<RP, NT>*>(smem_raw);
 
     const int t = threadIdx.x;
     const int mx = a.L.mx, my = a.L.my;
@@ -379,15 +410,15 @@ __global__ void __launch_bounds__(NT) k_split_x(const StepArgs a) {
     const long long plane = a.L.plane;
     const int cp = blockIdx.x * W + t;
     const int cpl = min(cp, mx + 3);
-    const int rb = blockIdx.y * a.H;               // first padded row of this block
-    const int re = min(rb + a.H, my + 4);          // one past the last
+    const int rb = blockIdx.y * a.H;       // first padded row of this block
+    const int re = min(rb + a.H, my + 4);  // one past the last
     const bool out_col = (t >= 2) && (t < W + 2) && (cp <= mx + 1);
     const bool ghost_copy = (cp <= mx + 3) && ((cp < 2 && t == cp) || (cp >= mx + 2 && t >= 2));
     const bool xcfl_col = (t >= 2) && (t <= W + 2) && (cp <= mx + 2);
     const int tl = (t > 0) ? t - 1 : 0;
     const int tr = (t < NT - 1) ? t + 1 : NT - 1;
     const double dtdx = a.dtdx;
-    const bool fw = a.meth.fwave != 0;
+    const RPParams& P = a.rp;
     const double* qo = a.qold + cpl;
     double* qn = a.qnew + cpl;
     double cfl = 0.0;
@@ -395,68 +426,62 @@ __global__ void __launch_bounds__(NT) k_split_x(const StepArgs a) {
     for (int R = rb; R < re; ++R) {
         const int buf = R & 1;
         double q[ME];
-#pragma unroll
-        for (int m = 0; m < ME; ++m) {
-            q[m] = __ldg(qo + m * plane + (long long)R * pitch);
-            sQ[buf][m][t] = q[m];
-        }
-        __syncthreads();
-        double wX[MW][ME], sX[MW], amX[ME], apX[ME];
-        typename RP::Cache cX;
         {
-            double qL[ME];
+            double c[NC];
 #pragma unroll
-            for (int m = 0; m < ME; ++m) qL[m] = sQ[buf][m][tl];
-            RP::template rpn2<1>(qL, q, a.rp, wX, sX, amX, apX, cX);
+            for (int m = 0; m < ME; ++m) q[m] = __ldg(qo + m * plane + (long long)R * pitch);
+            RP::prepare(q, P, c);
+#pragma unroll
+            for (int k = 0; k < NC; ++k) S.cell[buf][k][t] = c[k];
         }
-#pragma unroll
-        for (int mw = 0; mw < MW; ++mw)
-#pragma unroll
-            for (int m = 0; m < ME; ++m) sW[mw][m][t] = wX[mw][m];
         __syncthreads();
-        if (xcfl_col) {
+        Iface fX;
+        double amX[ME], apX[ME];
+        {
+            double cL[NC], cR[NC];
 #pragma unroll
-            for (int mw = 0; mw < MW; ++mw) cfl = fmax(cfl, fabs(dtdx * sX[mw]));
+            for (int k = 0; k < NC; ++k) {
+                cL[k] = S.cell[buf][k][tl];
+                cR[k] = S.cell[buf][k][t];
+            }
+            RP::template solve<1>(cL, cR, P, fX, amX, apX);
+            double wX[MW][ME];
+            RP::template waves<1>(fX, P, wX);
+#pragma unroll
+            for (int k = 0; k < MW; ++k)
+#pragma unroll
+                for (int m = 0; m < ME; ++m) S.w[k][m][t] = wX[k][m];
         }
-        double fX[ME];
-#pragma unroll
-        for (int m = 0; m < ME; ++m) fX[m] = 0.0;
+        __syncthreads();
+        if (xcfl_col) cfl = fmax(cfl, iface_cfl<RP, 1>(fX, P, dtdx));
+        double cq[ME];
         if (a.meth.order != 1) {
-            double cq[ME];
+            double dl[MW], dr[MW];
 #pragma unroll
-            for (int m = 0; m < ME; ++m) cq[m] = 0.0;
-#pragma unroll
-            for (int mw = 0; mw < MW; ++mw) {
-                const int lim = a.meth.mthlim[mw];
-                double wn2 = 0.0, dl = 0.0, dr = 0.0;
+            for (int k = 0; k < MW; ++k) {
+                double x = 0.0, y = 0.0;
 #pragma unroll
                 for (int m = 0; m < ME; ++m) {
-                    const double w = wX[mw][m];
-                    wn2 = wn2 + w * w;
-                    dl = dl + sW[mw][m][tl] * w;
-                    dr = dr + w * sW[mw][m][tr];
+                    const double w = S.w[k][m][t];
+                    x = x + S.w[k][m][tl] * w;
+                    y = y + w * S.w[k][m][tr];
                 }
-                if (lim != 0 && wn2 != 0.0) {
-                    const double phi = philim(wn2, (sX[mw] > 0.0) ? dl : dr, lim);
-#pragma unroll
-                    for (int m = 0; m < ME; ++m) wX[mw][m] = phi * wX[mw][m];
-                }
-                const double as = fabs(sX[mw]);
-                const double coef = (fw ? copysign(1.0, sX[mw]) : as) * (1.0 - as * dtdx);
-#pragma unroll
-                for (int m = 0; m < ME; ++m) cq[m] = cq[m] + coef * wX[mw][m];
+                dl[k] = x;
+                dr[k] = y;
             }
+            correction<RP, 1>(fX, P, a.meth, dtdx, dl, dr, cq);
+        } else {
 #pragma unroll
-            for (int m = 0; m < ME; ++m) fX[m] = 0.5 * cq[m];
+            for (int m = 0; m < ME; ++m) cq[m] = 0.0;
         }
 #pragma unroll
-        for (int m = 0; m < ME; ++m) sXL[m][t] = -dtdx * (amX[m] + fX[m]);
+        for (int m = 0; m < ME; ++m) S.xl[m][t] = -dtdx * (amX[m] + 0.5 * cq[m]);
         __syncthreads();
         if (out_col) {
             double v[ME];
 #pragma unroll
             for (int m = 0; m < ME; ++m) {
-                v[m] = q[m] + (-dtdx * (apX[m] - fX[m]) + sXL[m][tr]);
+                v[m] = q[m] + (-dtdx * (apX[m] - 0.5 * cq[m]) + S.xl[m][tr]);
                 qn[m * plane + (long long)R * pitch] = v[m];
             }
             if (!all_finite<ME>(v)) atomicOr(a.status, 1);
@@ -465,7 +490,7 @@ __global__ void __launch_bounds__(NT) k_split_x(const StepArgs a) {
             for (int m = 0; m < ME; ++m) qn[m * plane + (long long)R * pitch] = q[m];
         }
     }
-    cfl_commit(cfl, sRed, a.cfl_bits);
+    cfl_commit(cfl, S.red, a.cfl_bits);
 }
 
 // ---------------------------------------------------------------------------
@@ -475,7 +500,8 @@ __global__ void __launch_bounds__(NT) k_split_x(const StepArgs a) {
 // ---------------------------------------------------------------------------
 template <class RP, int NT>
 __global__ void __launch_bounds__(NT) k_split_y(const StepArgs a) {
-    constexpr int ME = RP::MEQN, MW = RP::MWAVES;
+    constexpr int ME = RP::MEQN, MW = RP::MWAVES, NC = RP::NC;
+    using Iface = typename RP::Iface;
     __shared__ double sRed[NT / 32];
     const int mx = a.L.mx, my = a.L.my;
     const int pitch = a.L.pitch;
@@ -488,80 +514,64 @@ __global__ void __launch_bounds__(NT) k_split_y(const StepArgs a) {
     const int Hb = min(a.H, my - rb);
     const int R0 = rb, R1 = rb + Hb + 3;
     const double dtdy = a.dtdy;
-    const bool fw = a.meth.fwave != 0;
+    const RPParams& P = a.rp;
     const double* qo = a.qold + cpl;
     double* qn = a.qnew + cpl;
 
-    double q0[ME], q1[ME], q2[ME], acc0[ME], acc1[ME];
-    double wY[MW][ME], sY[MW], amY[ME], apY[ME], dY[MW];
+    double q0[ME], q1[ME], cB[NC], acc0[ME], acc1[ME];
+    Iface fY;
+    double amY[ME], apY[ME], dY[MW];
     double cfl = 0.0;
+    {
+        double q[ME];
 #pragma unroll
-    for (int m = 0; m < ME; ++m) {
-        q2[m] = __ldg(qo + m * plane + (long long)R0 * pitch);
-        q1[m] = q0[m] = q2[m];
-        acc0[m] = acc1[m] = 0.0;
-        amY[m] = apY[m] = 0.0;
-    }
-#pragma unroll
-    for (int mw = 0; mw < MW; ++mw) {
-        sY[mw] = dY[mw] = 0.0;
-#pragma unroll
-        for (int m = 0; m < ME; ++m) wY[mw][m] = 0.0;
-    }
-    for (int R = R0 + 1; R <= R1; ++R) {
+        for (int m = 0; m < ME; ++m) q[m] = __ldg(qo + m * plane + (long long)R0 * pitch);
+        RP::prepare(q, P, cB);
 #pragma unroll
         for (int m = 0; m < ME; ++m) {
-            q0[m] = q1[m];
-            q1[m] = q2[m];
-            q2[m] = __ldg(qo + m * plane + (long long)R * pitch);
+            q0[m] = q1[m] = q[m];
+            acc0[m] = acc1[m] = 0.0;
+            amY[m] = apY[m] = 0.0;
         }
-        double wN[MW][ME], sN[MW], amN[ME], apN[ME];
-        typename RP::Cache cN;
-        RP::template rpn2<2>(q1, q2, a.rp, wN, sN, amN, apN, cN);
+    }
+#pragma unroll
+    for (int k = 0; k < MW; ++k) dY[k] = 0.0;
+    memset(&fY, 0, sizeof(fY));
+    for (int R = R0 + 1; R <= R1; ++R) {
+        double q2[ME], cA[NC];
+#pragma unroll
+        for (int m = 0; m < ME; ++m) q2[m] = __ldg(qo + m * plane + (long long)R * pitch);
+        RP::prepare(q2, P, cA);
+        Iface fN;
+        double amN[ME], apN[ME];
+        RP::template solve<2>(cB, cA, P, fN, amN, apN);
         double dn[MW];
+        {
+            double wY[MW][ME], wN[MW][ME];
+            RP::template waves<2>(fY, P, wY);
+            RP::template waves<2>(fN, P, wN);
 #pragma unroll
-        for (int mw = 0; mw < MW; ++mw) {
-            double d = 0.0;
+            for (int k = 0; k < MW; ++k) {
+                double d = 0.0;
 #pragma unroll
-            for (int m = 0; m < ME; ++m) d = d + wY[mw][m] * wN[mw][m];
-            dn[mw] = d;
+                for (int m = 0; m < ME; ++m) d = d + wY[k][m] * wN[k][m];
+                dn[k] = d;
+            }
         }
         // acc0 <-> row R-2, acc1 <-> row R-1
         if (R >= R0 + 3) {
-            if (valid) {
-#pragma unroll
-                for (int mw = 0; mw < MW; ++mw) cfl = fmax(cfl, fabs(dtdy * sY[mw]));
-            }
-            double fY[ME];
-#pragma unroll
-            for (int m = 0; m < ME; ++m) fY[m] = 0.0;
+            if (valid) cfl = fmax(cfl, iface_cfl<RP, 2>(fY, P, dtdy));
+            double cq[ME];
             if (a.meth.order != 1) {
-                double cq[ME];
+                correction<RP, 2>(fY, P, a.meth, dtdy, dY, dn, cq);
+            } else {
 #pragma unroll
                 for (int m = 0; m < ME; ++m) cq[m] = 0.0;
-#pragma unroll
-                for (int mw = 0; mw < MW; ++mw) {
-                    const int lim = a.meth.mthlim[mw];
-                    double wn2 = 0.0;
-#pragma unroll
-                    for (int m = 0; m < ME; ++m) wn2 = wn2 + wY[mw][m] * wY[mw][m];
-                    if (lim != 0 && wn2 != 0.0) {
-                        const double phi = philim(wn2, (sY[mw] > 0.0) ? dY[mw] : dn[mw], lim);
-#pragma unroll
-                        for (int m = 0; m < ME; ++m) wY[mw][m] = phi * wY[mw][m];
-                    }
-                    const double as = fabs(sY[mw]);
-                    const double coef = (fw ? copysign(1.0, sY[mw]) : as) * (1.0 - as * dtdy);
-#pragma unroll
-                    for (int m = 0; m < ME; ++m) cq[m] = cq[m] + coef * wY[mw][m];
-                }
-#pragma unroll
-                for (int m = 0; m < ME; ++m) fY[m] = 0.5 * cq[m];
             }
 #pragma unroll
             for (int m = 0; m < ME; ++m) {
-                acc0[m] = acc0[m] - dtdy * (amY[m] + fY[m]);
-                acc1[m] = acc1[m] - dtdy * (apY[m] - fY[m]);
+                acc0[m] = acc0[m] - dtdy * (amY[m] + 0.5 * cq[m]);
+                acc1[m] = acc1[m] - dtdy * (apY[m] - 0.5 * cq[m]);
             }
         }
         if (R >= R0 + 4 && out_col) {
@@ -579,14 +589,14 @@ __global__ void __launch_bounds__(NT) k_split_y(const StepArgs a) {
             acc1[m] = 0.0;
             amY[m] = amN[m];
             apY[m] = apN[m];
+            q0[m] = q1[m];
+            q1[m] = q2[m];
         }
 #pragma unroll
-        for (int mw = 0; mw < MW; ++mw) {
-            sY[mw] = sN[mw];
-            dY[mw] = dn[mw];
+        for (int k = 0; k < NC; ++k) cB[k] = cA[k];
 #pragma unroll
-            for (int m = 0; m < ME; ++m) wY[mw][m] = wN[mw][m];
-        }
+        for (int k = 0; k < MW; ++k) dY[k] = dn[k];
+        fY = fN;
     }
     cfl_commit(cfl, sRed, a.cfl_bits);
 }
