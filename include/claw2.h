@@ -164,6 +164,28 @@ int claw2_tune_get(int riemann, int* variant, int* rows);
  * roofline denominator for the FP64-bound Riemann solvers. */
 int claw2_probe_fp64(int device, double* tflops);
 
+/* ---- no counterpart in the reference ------------------------------------
+ * The split step (x-sweep then y-sweep, as claw2_step2ds with ids = 1 then 2)
+ * for callers that cannot allocate device memory: frameworks that reserve the
+ * GPU's memory in their own pool, where a library cudaMalloc would fail or
+ * fragment it, and loops that cannot take cudaMalloc's implicit device
+ * synchronisation.  It allocates nothing: the caller passes the device q
+ * planes (qold with its ghost cells filled, qnew; element (m, c, r) at
+ * q[m*plane + r*pitch + c], padded column c in [0, mx+4), row r in [0, my+4)),
+ * and the intermediate state plus the CFL/status words live in one fixed
+ * device array of CLAW2_NOALLOC_SCRATCH_BYTES held by every GPU that loads
+ * the library until exit.  Grids needing more than that (256 bytes +
+ * num_eqn*plane*8 bytes) are rejected with CLAW2_EINVAL.  Every
+ * call reuses that array: the call clears the words that must start at zero;
+ * calls whose GPU work overlaps race and must be serialised.  The first call
+ * on a device looks up the array's address; make it before any stream
+ * capture.  The call runs on `stream` (NULL: the legacy default stream),
+ * waits for it, writes the Courant number to *cfl (host memory) and writes
+ * the interior cells of qnew only. */
+#define CLAW2_NOALLOC_SCRATCH_BYTES (32ll << 20)
+int claw2_step2ds_noalloc(const claw2_desc* desc, const double* qold, double* qnew, long long pitch,
+                          long long plane, double dt, double* cfl, void* stream);
+
 /* Description of the last error on this thread (never NULL). */
 const char* claw2_last_error(void);
 

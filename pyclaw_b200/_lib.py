@@ -13,6 +13,7 @@ LIB_PATH = os.path.join(_HERE, "lib", "libclaw2.so")
 
 CLAW2_MAX_PARAMS = 8
 CLAW2_MAX_WAVES = 8
+CLAW2_NOALLOC_SCRATCH_BYTES = 32 << 20
 
 RP_ADVECTION, RP_ACOUSTICS, RP_EULER_ROE, RP_SHALLOW_ROE, RP_EULER_EXACT = 1, 2, 3, 4, 5
 
@@ -81,6 +82,9 @@ _SIGNATURES = {
     "claw2_probe_fp64": (ctypes.c_int, [ctypes.c_int, _c_double_p]),
     "claw2_tune_set": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "claw2_tune_get": (ctypes.c_int, [ctypes.c_int, _c_int_p, _c_int_p]),
+    "claw2_step2ds_noalloc": (ctypes.c_int, [ctypes.POINTER(Claw2Desc), ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_longlong, ctypes.c_longlong, ctypes.c_double, _c_double_p,
+                                             ctypes.c_void_p]),
     "claw2_last_error": (ctypes.c_char_p, []),
     "claw2_version": (ctypes.c_char_p, []),
 }

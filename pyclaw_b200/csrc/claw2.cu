@@ -393,6 +393,10 @@ StepArgs patch_args(claw2_patch* p, double dt) {
 
 extern "C" {
 
+// Lets other translation units of this library report errors through
+// claw2_last_error(); hidden, so it is not part of the exported ABI.
+__attribute__((visibility("hidden"))) void claw2_internal_set_error(const char* msg) { g_err = msg; }
+
 const char* claw2_last_error(void) { return g_err.c_str(); }
 const char* claw2_version(void) { return "claw2 0.1 (sm_100a, FP64)"; }
 

@@ -635,7 +635,7 @@ __device__ __forceinline__ int bc_src(int c, int n, int lo, int up, bool& flip) 
     return c;
 }
 
-__global__ void k_bc_fill(const BCArgs a) {
+static __global__ void k_bc_fill(const BCArgs a) {
     const int mx = a.L.mx, my = a.L.my;
     const int nrow = 4 * (mx + 4);   // cells of the 4 ghost rows
     const int ncol = 4 * my;         // ghost-column cells of interior rows
@@ -670,7 +670,7 @@ __global__ void k_bc_fill(const BCArgs a) {
 // fastest) and the device planes.  `ghost` = 2 when the host array is qbc
 // (with ghost cells), 0 when it is State.q (interior only).
 // ---------------------------------------------------------------------------
-__global__ void k_aos_to_planes(const double* __restrict__ src, double* __restrict__ dst, Layout L,
+static __global__ void k_aos_to_planes(const double* __restrict__ src, double* __restrict__ dst, Layout L,
                                 int meqn, int ghost) {
     const int nx = L.mx + 2 * ghost, ny = L.my + 2 * ghost;
     const long long n = (long long)nx * ny;
@@ -682,7 +682,7 @@ __global__ void k_aos_to_planes(const double* __restrict__ src, double* __restri
     }
 }
 
-__global__ void k_planes_to_aos(const double* __restrict__ src, double* __restrict__ dst, Layout L,
+static __global__ void k_planes_to_aos(const double* __restrict__ src, double* __restrict__ dst, Layout L,
                                 int meqn, int ghost) {
     const int nx = L.mx + 2 * ghost, ny = L.my + 2 * ghost;
     const long long n = (long long)nx * ny;
@@ -696,14 +696,14 @@ __global__ void k_planes_to_aos(const double* __restrict__ src, double* __restri
 
 // Interior-only copy of qbc-layout planes (for the "ghosts unchanged" rule of
 // claw2_step2: qnew starts as a copy of qold).
-__global__ void k_copy_planes(const double* __restrict__ src, double* __restrict__ dst, long long n) {
+static __global__ void k_copy_planes(const double* __restrict__ src, double* __restrict__ dst, long long n) {
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
          k += (long long)gridDim.x * blockDim.x)
         dst[k] = src[k];
 }
 
 // FP64 FMA throughput probe: 16 independent dependency chains per thread.
-__global__ void k_fp64_fma(double* out, int iters, double b) {
+static __global__ void k_fp64_fma(double* out, int iters, double b) {
     double a[16];
 #pragma unroll
     for (int k = 0; k < 16; ++k) a[k] = 1.0 + 1e-3 * (threadIdx.x + k);
