@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--n", type=int, default=N, help="grid size override (profiling runs only)")
+    ap.add_argument("--secondary", type=int, default=1, help="also time the other benchmark problems")
     ap.add_argument("--shape", default=None, help="fixed launch shape 'variant,rows' (skips the autotuner)")
     ap.add_argument("--pre-t", type=float, default=0.4,
                     help="advance the problem to this time (untimed) before warm-up")
@@ -179,6 +180,84 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # GPU leg
 # ---------------------------------------------------------------------------
+def time_patch(patch, dt, steps, flush, stream):
+    """Mean step and step-kernel times (ms) of a device patch, L2 flushed
+    between steps; the state advances (every step accepted)."""
+    import torch
+    patch.set_stream(stream.cuda_stream)
+    patch.set_timing(True)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    kern = []
+    for k in range(steps):
+        flush.zero_()
+        ev[k][0].record(stream)
+        patch.step(dt, want_cfl=False)
+        patch.accept(True)
+        ev[k][1].record(stream)
+        kern.append(patch.kernel_ms())
+    torch.cuda.synchronize()
+    patch.sync()
+    return statistics.mean(a.elapsed_time(b) for a, b in ev), statistics.mean(kern)
+
+
+def batched_workload(n_instances=512, steps=100):
+    """The batched form: n independent Euler quadrant problems of uneven size
+    (side 64..512), 100 steps with per-problem dt; aggregate cell-updates/s of
+    the graph-captured persistent form and of the plain per-problem loop."""
+    import numpy as np
+    from pyclaw_b200 import batch as pb, workloads
+    claws, sides = workloads.batched_quadrants(n_instances)
+    bat = pb.Batch(claws)
+    dt0 = [c.solver.dt_initial for c in claws]
+    rows, trials, choice = pb.autotune_rows(bat, sides)
+    cells = sides.astype(np.float64) ** 2
+    out = {"instances": n_instances, "cells_total": float(cells.sum()), "steps": steps,
+           "rows_per_bucket": [int(c) for c in choice], "bucket_edges": [128, 256]}
+    for mode, name in ((0, "graph_persistent"), (2, "plain_per_instance_loop")):
+        bat.upload()
+        bat.set_time(dt0, 0.0, 1e99)
+        bat.run(1, mode=mode)  # warm (captures the graph for 1 step)
+        bat.upload()
+        bat.set_time(dt0, 0.0, 1e99)
+        ms = bat.run(steps, mode=mode)
+        st = bat.state()
+        upd = float((cells * st["nsteps"]).sum())
+        out[name] = {"ms": ms, "value": upd / (ms * 1e-3), "unit": UNIT,
+                     "accepted_steps": int(st["nsteps"].sum()), "rejected_steps": int(st["nreject"].sum()),
+                     "failed_instances": int(st["failed"].sum())}
+    out["speedup"] = out["graph_persistent"]["value"] / out["plain_per_instance_loop"]["value"]
+    ntiles, grid = bat.tiles()
+    out["tiles"], out["persistent_grid"] = ntiles, grid
+    bat.close()
+    return out
+
+
+def secondary_workloads(stream, flush, peaks, steps=20):
+    """The shallow-water dam break at 4096^2 (48 B/cell) and the walled
+    acoustics problem at 200^2, unsplit trans_cor, MC, CFL 0.9."""
+    from pyclaw_b200 import tune, workloads
+    out = {}
+    for name, make, bpc in [("shallow_roe_dam_break_4096", lambda: workloads.shallow_dam_break_unsplit(n=4096), 48),
+                            ("acoustics_wall_200", lambda: workloads.acoustics_wall(n=200), 48)]:
+        claw = make()
+        s, sol = claw.solver, claw.solution
+        s.setup(sol)
+        p = s._dev
+        p.set_stream(stream.cuda_stream)
+        dt = s.dt_initial if name.startswith("acoustics") else 1e-4
+        cfl = p.step(dt)
+        p.accept(False)
+        dt = dt * 0.9 / cfl
+        shape, _ = tune.autotune(p, dt)
+        step_ms, kern_ms = time_patch(p, dt, steps, flush, stream)
+        n = sol.state.grid.num_cells[0] * sol.state.grid.num_cells[1]
+        gbs = n * bpc / (kern_ms * 1e-3) / 1e9
+        out[name] = {"value": n / (step_ms * 1e-3), "unit": UNIT, "ms_per_step": step_ms, "kernel_ms": kern_ms,
+                     "bytes_per_cell": bpc, "achieved_gbs": gbs, "hbm_frac": gbs / peaks["hbm_gbs"],
+                     "launch_shape": list(shape), "steps": steps}
+        p.close()
+    return out
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -295,6 +374,11 @@ def run_ours(args):
                "path": "claw2_patch_upload_q + claw2_patch_step (returns CFL) + claw2_patch_accept + "
                        "claw2_patch_download_q, pinned host buffers, wall clock"}
 
+    secondary = {}
+    if rank == 0 and world == 1 and args.secondary:
+        secondary = secondary_workloads(stream, flush, peaks)
+        secondary["batched_quadrants_512"] = batched_workload()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and n == N:
         v, s, el = cpu_rate(1, args.cpu_sample_s)
@@ -318,6 +402,7 @@ def run_ours(args):
                              "fp64_probe_tflops": fp64.value,
                              "fp64_flops_per_cell_est": None},
                 "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
+                "secondary": secondary,
                 "gpu_launches": 2 * args.steps}
         print(json.dumps(line), flush=True)
     solver._dev.close()

@@ -186,6 +186,35 @@ int claw2_probe_fp64(int device, double* tflops);
 int claw2_step2ds_noalloc(const claw2_desc* desc, const double* qold, double* qnew, long long pitch,
                           long long plane, double dt, double* cfl, void* stream);
 
+/* ---- batches of independent problems (the batched form) ------------------
+ * n problems of different sizes with the same solver, method, BCs and
+ * parameters (the unsplit step), each with its own dt and time.  One batch
+ * step = ghost fill of every instance + one persistent kernel over a flat
+ * list of (instance, strip, row block) tiles + a per-instance accept/reject
+ * and dt update on the device (solver.py:524-552, 619-651).  Replaces a host
+ * loop of ClawSolver2D.evolve_to_time calls, one per problem. */
+typedef struct claw2_batch claw2_batch;
+int claw2_batch_create(const claw2_desc* descs, int n, claw2_batch** out);
+int claw2_batch_destroy(claw2_batch* b);
+/* Row-block height per instance (0 = heuristic); rebuilds the tile list. */
+int claw2_batch_set_rows(claw2_batch* b, const int* rows);
+int claw2_batch_upload_q(claw2_batch* b, int i, const double* q);
+int claw2_batch_download_q(claw2_batch* b, int i, double* q);
+/* Initial dt per instance, start/end time and the dt rule's constants. */
+int claw2_batch_set_time(claw2_batch* b, const double* dt0, double t0, double tend, double cfl_desired,
+                         double cfl_max, double dt_max);
+/* nsteps batch steps; mode 0: the steps captured in one CUDA graph (captured
+ * on first use for that nsteps), 1: the same launches issued directly,
+ * 2: the plain loop -- one ghost-fill / step / finalize launch sequence per
+ * instance.  *ms = device time of the whole run (CUDA events). */
+int claw2_batch_run(claw2_batch* b, int nsteps, int mode, float* ms);
+/* Per-instance state (arrays of n; any pointer may be NULL).  status bit 0:
+ * a step produced a non-finite value; that step was discarded and the
+ * instance retired at its last good state (the others go on). */
+int claw2_batch_get_state(claw2_batch* b, double* t, double* dt, int* nsteps, int* nreject, double* cfl_last,
+                          int* status);
+int claw2_batch_tiles(claw2_batch* b, int* ntiles, int* persistent_grid);
+
 /* Description of the last error on this thread (never NULL). */
 const char* claw2_last_error(void);
 

@@ -85,6 +85,16 @@ _SIGNATURES = {
     "claw2_step2ds_noalloc": (ctypes.c_int, [ctypes.POINTER(Claw2Desc), ctypes.c_void_p, ctypes.c_void_p,
                                              ctypes.c_longlong, ctypes.c_longlong, ctypes.c_double, _c_double_p,
                                              ctypes.c_void_p]),
+    "claw2_batch_create": (ctypes.c_int, [ctypes.POINTER(Claw2Desc), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "claw2_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "claw2_batch_set_rows": (ctypes.c_int, [ctypes.c_void_p, _c_int_p]),
+    "claw2_batch_upload_q": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _c_double_p]),
+    "claw2_batch_download_q": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _c_double_p]),
+    "claw2_batch_set_time": (ctypes.c_int, [ctypes.c_void_p, _c_double_p] + [ctypes.c_double] * 5),
+    "claw2_batch_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]),
+    "claw2_batch_get_state": (ctypes.c_int, [ctypes.c_void_p, _c_double_p, _c_double_p, _c_int_p, _c_int_p,
+                                             _c_double_p, _c_int_p]),
+    "claw2_batch_tiles": (ctypes.c_int, [ctypes.c_void_p, _c_int_p, _c_int_p]),
     "claw2_last_error": (ctypes.c_char_p, []),
     "claw2_version": (ctypes.c_char_p, []),
 }

@@ -14,7 +14,11 @@
 #include <mutex>
 #include <string>
 
+#include "batch.cuh"
 #include "step_kernels.cuh"
+
+#include <vector>
+#include <numeric>
 
 using namespace claw2;
 
@@ -694,6 +698,364 @@ int claw2_patch_device_q(claw2_patch* p, double** q, long long* layout) {
     layout[1] = p->d.my + 4;
     layout[2] = p->L.pitch;
     layout[3] = p->L.plane;
+    return CLAW2_OK;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Batches of independent problems
+// ===========================================================================
+struct claw2_batch {
+    int device = 0;
+    int n = 0;
+    claw2_desc d0;                   // shared solver / method / BC settings
+    std::vector<claw2_desc> descs;
+    std::vector<BatchInst> h_inst;
+    std::vector<int> order;          // instances by decreasing size
+    std::vector<int> tile_first, tile_count;
+    std::vector<int2> h_tiles;
+    BatchInst* d_inst = nullptr;
+    BatchState* d_st = nullptr;
+    int2* d_tiles = nullptr;
+    double* arena = nullptr;
+    double* stage = nullptr;
+    size_t stage_doubles = 0;
+    RPParams rp;
+    Method meth;
+    BatchCtl ctl;
+    cudaStream_t st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    int persistent_grid = 0;
+};
+
+namespace {
+
+int batch_build_tiles(claw2_batch* b, const int* rows) {
+    constexpr int W = NT_UNSPLIT - 4;
+    b->h_tiles.clear();
+    b->tile_first.assign(b->n, 0);
+    b->tile_count.assign(b->n, 0);
+    for (int i : b->order) {
+        BatchInst& in = b->h_inst[i];
+        in.nstrips = (in.L.mx + W - 1) / W;
+        in.H = (rows && rows[i] > 0) ? rows[i] : pick_rows(in.nstrips, in.L.my);
+        const int nblk = (in.L.my + in.H - 1) / in.H;
+        b->tile_first[i] = (int)b->h_tiles.size();
+        b->tile_count[i] = in.nstrips * nblk;
+        for (int k = 0; k < in.nstrips * nblk; ++k) b->h_tiles.push_back(make_int2(i, k));
+    }
+    DeviceGuard g(b->device);
+    cudaFree(b->d_tiles);
+    b->d_tiles = nullptr;
+    CUDA_TRY(cudaMalloc(&b->d_tiles, sizeof(int2) * b->h_tiles.size()));
+    CUDA_TRY(cudaMemcpy(b->d_tiles, b->h_tiles.data(), sizeof(int2) * b->h_tiles.size(), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(b->d_inst, b->h_inst.data(), sizeof(BatchInst) * b->n, cudaMemcpyHostToDevice));
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+        b->graph_steps = 0;
+    }
+    return CLAW2_OK;
+}
+
+BatchArgs batch_args(claw2_batch* b) {
+    BatchArgs a;
+    a.inst = b->d_inst;
+    a.st = b->d_st;
+    a.tiles = b->d_tiles;
+    a.ntiles = (int)b->h_tiles.size();
+    a.ninst = b->n;
+    a.rp = b->rp;
+    a.meth = b->meth;
+    a.ctl = b->ctl;
+    return a;
+}
+
+// Shared-memory opt-in of the batched step kernel; done at batch creation,
+// before any graph capture.
+template <class RP>
+int batch_smem_attr() {
+    constexpr int smem = (int)sizeof(UnsplitSmem<RP, NT_UNSPLIT>);
+    static unsigned long long attr = 0;
+    smem_attr(k_batch_step<RP, NT_UNSPLIT, 2>, smem, attr);
+    return smem;
+}
+
+template <class RP>
+struct BatchStepF {
+    static void run(const BatchArgs& a, int first, int count, int grid, cudaStream_t st) {
+        constexpr int smem = (int)sizeof(UnsplitSmem<RP, NT_UNSPLIT>);
+        k_batch_step<RP, NT_UNSPLIT, 2><<<grid, NT_UNSPLIT, smem, st>>>(a, first, count);
+    }
+};
+
+template <class RP>
+struct BatchOccF {
+    static void run(int* nb) {
+        const int smem = batch_smem_attr<RP>();
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(nb, k_batch_step<RP, NT_UNSPLIT, 2>, NT_UNSPLIT, smem);
+    }
+};
+
+// One batched step: ghost fill of every instance, the persistent step, finalize.
+void batch_step_all(claw2_batch* b) {
+    const BatchArgs a = batch_args(b);
+    int maxg = 0;
+    for (const auto& in : b->h_inst) maxg = std::max(maxg, 4 * (in.L.mx + 4) + 4 * in.L.my);
+    dim3 gbc((maxg + 255) / 256, b->n);
+    k_batch_bc<<<gbc, 256, 0, b->st>>>(a, 0, b->d0.bc_lower[0], b->d0.bc_lower[1], b->d0.bc_upper[0],
+                                      b->d0.bc_upper[1], b->d0.num_eqn);
+    dispatch<BatchStepF>(b->d0.riemann, a, 0, a.ntiles, b->persistent_grid, b->st);
+    k_batch_finalize<<<(b->n + 127) / 128, 128, 0, b->st>>>(a, 0, b->n);
+}
+
+// The same step as one independent launch sequence per instance.
+void batch_step_each(claw2_batch* b) {
+    const BatchArgs a = batch_args(b);
+    for (int i = 0; i < b->n; ++i) {
+        const BatchInst& in = b->h_inst[i];
+        const int ng = 4 * (in.L.mx + 4) + 4 * in.L.my;
+        k_batch_bc<<<dim3((ng + 255) / 256, 1), 256, 0, b->st>>>(a, i, b->d0.bc_lower[0], b->d0.bc_lower[1],
+                                                                 b->d0.bc_upper[0], b->d0.bc_upper[1],
+                                                                 b->d0.num_eqn);
+        dispatch<BatchStepF>(b->d0.riemann, a, b->tile_first[i], b->tile_count[i], b->tile_count[i], b->st);
+        k_batch_finalize<<<1, 32, 0, b->st>>>(a, i, 1);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int claw2_batch_create(const claw2_desc* descs, int n, claw2_batch** out) {
+    if (!descs || !out || n < 1) return fail(CLAW2_EINVAL, "bad arguments");
+    *out = nullptr;
+    const claw2_desc& d0 = descs[0];
+    int me = 0, mw = 0;
+    if (rp_shape(d0.riemann, &me, &mw) != 0) return fail(CLAW2_EINVAL, "unknown Riemann solver id %d", d0.riemann);
+    for (int i = 0; i < n; ++i) {
+        const claw2_desc& d = descs[i];
+        if (d.riemann != d0.riemann || d.order != d0.order || d.transverse != d0.transverse || d.fwave != d0.fwave ||
+            d.dimensional_split || d.num_eqn != me || d.num_waves != mw || d.num_ghost != 2 || d.num_aux != 0 ||
+            d.device != d0.device || std::memcmp(d.mthlim, d0.mthlim, sizeof d.mthlim) ||
+            std::memcmp(d.bc_lower, d0.bc_lower, sizeof d.bc_lower) ||
+            std::memcmp(d.bc_upper, d0.bc_upper, sizeof d.bc_upper) || d.ncparam != d0.ncparam ||
+            std::memcmp(d.cparam, d0.cparam, sizeof d.cparam))
+            return fail(CLAW2_EINVAL, "instance %d: batched instances share solver, method, BCs and parameters "
+                                      "(unsplit step only)", i);
+        if (d.mx < 2 || d.my < 2 || !(d.dx > 0.0) || !(d.dy > 0.0))
+            return fail(CLAW2_EINVAL, "instance %d: bad sizes", i);
+    }
+    int rc = check_method(d0.order, d0.transverse, d0.mthlim, mw, d0.fwave);
+    if (rc) return rc;
+    rc = check_bc(d0.bc_lower, d0.bc_upper, 2, 2);
+    if (rc) return rc;
+
+    claw2_batch* b = new claw2_batch();
+    b->device = d0.device;
+    b->n = n;
+    b->d0 = d0;
+    b->descs.assign(descs, descs + n);
+    b->rp = make_params(d0.riemann, d0.cparam, d0.ncparam);
+    b->meth.order = d0.order;
+    b->meth.transverse = d0.transverse;
+    b->meth.fwave = d0.fwave;
+    for (int k = 0; k < CLAW2_MAX_WAVES; ++k) b->meth.mthlim[k] = k < mw ? d0.mthlim[k] : 0;
+    b->ctl.cfl_desired = 0.9;
+    b->ctl.cfl_max = 1.0;
+    b->ctl.dt_max = 1e99;
+    b->ctl.tend = 1e99;
+    DeviceGuard g(b->device);
+    size_t total = 0;
+    b->h_inst.resize(n);
+    for (int i = 0; i < n; ++i) {
+        BatchInst& in = b->h_inst[i];
+        in.L = make_layout(descs[i].mx, descs[i].my);
+        in.dx = descs[i].dx;
+        in.dy = descs[i].dy;
+        total += 2 * (size_t)me * in.L.plane;
+        b->stage_doubles = std::max(b->stage_doubles, (size_t)me * descs[i].mx * descs[i].my);
+    }
+    b->order.resize(n);
+    std::iota(b->order.begin(), b->order.end(), 0);
+    std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) {
+        return (long long)descs[x].mx * descs[x].my > (long long)descs[y].mx * descs[y].my;
+    });
+    bool ok = cudaMalloc(&b->arena, total * 8) == cudaSuccess &&
+              cudaMalloc(&b->stage, b->stage_doubles * 8) == cudaSuccess &&
+              cudaMalloc(&b->d_inst, sizeof(BatchInst) * n) == cudaSuccess &&
+              cudaMalloc(&b->d_st, sizeof(BatchState) * n) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreate(&b->e0) == cudaSuccess && cudaEventCreate(&b->e1) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        claw2_batch_destroy(b);
+        return fail(CLAW2_ENOMEM, "device allocation for a batch of %d instances failed", n);
+    }
+    cudaMemset(b->arena, 0, total * 8);
+    cudaMemset(b->d_st, 0, sizeof(BatchState) * n);
+    size_t off = 0;
+    for (int i = 0; i < n; ++i) {
+        BatchInst& in = b->h_inst[i];
+        in.q[0] = b->arena + off;
+        off += (size_t)me * in.L.plane;
+        in.q[1] = b->arena + off;
+        off += (size_t)me * in.L.plane;
+    }
+    rc = batch_build_tiles(b, nullptr);
+    if (rc) {
+        claw2_batch_destroy(b);
+        return rc;
+    }
+    int nb = 0, nsm = 0;
+    dispatch<BatchOccF>(d0.riemann, &nb);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->device);
+    b->persistent_grid = std::max(1, nb) * std::max(1, nsm);
+    *out = b;
+    return CLAW2_OK;
+}
+
+int claw2_batch_destroy(claw2_batch* b) {
+    if (!b) return CLAW2_OK;
+    {
+        DeviceGuard g(b->device);
+        if (b->st) cudaStreamSynchronize(b->st);
+        if (b->graph) cudaGraphExecDestroy(b->graph);
+        cudaFree(b->arena);
+        cudaFree(b->stage);
+        cudaFree(b->d_inst);
+        cudaFree(b->d_st);
+        cudaFree(b->d_tiles);
+        if (b->e0) cudaEventDestroy(b->e0);
+        if (b->e1) cudaEventDestroy(b->e1);
+        if (b->st) cudaStreamDestroy(b->st);
+    }
+    delete b;
+    return CLAW2_OK;
+}
+
+int claw2_batch_set_rows(claw2_batch* b, const int* rows) {
+    if (!b) return fail(CLAW2_EINVAL, "null batch");
+    return batch_build_tiles(b, rows);
+}
+
+int claw2_batch_upload_q(claw2_batch* b, int i, const double* q) {
+    if (!b || !q || i < 0 || i >= b->n) return fail(CLAW2_EINVAL, "bad arguments");
+    DeviceGuard g(b->device);
+    BatchState s;
+    CUDA_TRY(cudaMemcpy(&s, b->d_st + i, sizeof s, cudaMemcpyDeviceToHost));
+    const BatchInst& in = b->h_inst[i];
+    const size_t n = (size_t)b->d0.num_eqn * in.L.mx * in.L.my;
+    CUDA_TRY(cudaMemcpyAsync(b->stage, q, n * 8, cudaMemcpyHostToDevice, b->st));
+    k_aos_to_planes<<<grid_blocks((long long)in.L.mx * in.L.my), 256, 0, b->st>>>(b->stage, in.q[s.cur], in.L,
+                                                                                  b->d0.num_eqn, 0);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(b->st));
+    return CLAW2_OK;
+}
+
+int claw2_batch_download_q(claw2_batch* b, int i, double* q) {
+    if (!b || !q || i < 0 || i >= b->n) return fail(CLAW2_EINVAL, "bad arguments");
+    DeviceGuard g(b->device);
+    BatchState s;
+    CUDA_TRY(cudaMemcpy(&s, b->d_st + i, sizeof s, cudaMemcpyDeviceToHost));
+    const BatchInst& in = b->h_inst[i];
+    const size_t n = (size_t)b->d0.num_eqn * in.L.mx * in.L.my;
+    k_planes_to_aos<<<grid_blocks((long long)in.L.mx * in.L.my), 256, 0, b->st>>>(in.q[s.cur], b->stage, in.L,
+                                                                                  b->d0.num_eqn, 0);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(q, b->stage, n * 8, cudaMemcpyDeviceToHost, b->st));
+    CUDA_TRY(cudaStreamSynchronize(b->st));
+    return CLAW2_OK;
+}
+
+int claw2_batch_set_time(claw2_batch* b, const double* dt0, double t0, double tend, double cfl_desired,
+                         double cfl_max, double dt_max) {
+    if (!b || !dt0) return fail(CLAW2_EINVAL, "bad arguments");
+    if (!(cfl_desired > 0.0) || cfl_desired > cfl_max) return fail(CLAW2_EINVAL, "need 0 < cfl_desired <= cfl_max");
+    DeviceGuard g(b->device);
+    std::vector<BatchState> s(b->n);
+    for (int i = 0; i < b->n; ++i) {
+        std::memset(&s[i], 0, sizeof(BatchState));
+        s[i].dt = dt0[i];
+        s[i].t = t0;
+        s[i].done = t0 >= tend;
+    }
+    CUDA_TRY(cudaStreamSynchronize(b->st));
+    // keep the current buffer index of each instance
+    std::vector<BatchState> old(b->n);
+    CUDA_TRY(cudaMemcpy(old.data(), b->d_st, sizeof(BatchState) * b->n, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < b->n; ++i) s[i].cur = old[i].cur;
+    CUDA_TRY(cudaMemcpy(b->d_st, s.data(), sizeof(BatchState) * b->n, cudaMemcpyHostToDevice));
+    b->ctl.cfl_desired = cfl_desired;
+    b->ctl.cfl_max = cfl_max;
+    b->ctl.dt_max = dt_max;
+    b->ctl.tend = tend;
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+        b->graph_steps = 0;
+    }
+    return CLAW2_OK;
+}
+
+int claw2_batch_run(claw2_batch* b, int nsteps, int mode, float* ms) {
+    if (!b || nsteps < 0 || mode < 0 || mode > 2) return fail(CLAW2_EINVAL, "bad arguments");
+    DeviceGuard g(b->device);
+    if (mode == 0 && b->graph_steps != nsteps) {
+        if (b->graph) cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+        cudaGraph_t graph = nullptr;
+        CUDA_TRY(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+        for (int k = 0; k < nsteps; ++k) batch_step_all(b);
+        CUDA_TRY(cudaStreamEndCapture(b->st, &graph));
+        cudaError_t e = cudaGraphInstantiate(&b->graph, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return fail(CLAW2_ECUDA, "graph instantiation failed: %s", cudaGetErrorString(e));
+        b->graph_steps = nsteps;
+    }
+    CUDA_TRY(cudaEventRecord(b->e0, b->st));
+    if (mode == 0) {
+        CUDA_TRY(cudaGraphLaunch(b->graph, b->st));
+    } else if (mode == 1) {
+        for (int k = 0; k < nsteps; ++k) batch_step_all(b);
+    } else {
+        for (int k = 0; k < nsteps; ++k) batch_step_each(b);
+    }
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaEventRecord(b->e1, b->st));
+    CUDA_TRY(cudaEventSynchronize(b->e1));
+    float t = 0.f;
+    CUDA_TRY(cudaEventElapsedTime(&t, b->e0, b->e1));
+    if (ms) *ms = t;
+    return CLAW2_OK;
+}
+
+int claw2_batch_get_state(claw2_batch* b, double* t, double* dt, int* nsteps, int* nreject, double* cfl_last,
+                          int* status) {
+    if (!b) return fail(CLAW2_EINVAL, "null batch");
+    DeviceGuard g(b->device);
+    std::vector<BatchState> s(b->n);
+    CUDA_TRY(cudaStreamSynchronize(b->st));
+    CUDA_TRY(cudaMemcpy(s.data(), b->d_st, sizeof(BatchState) * b->n, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < b->n; ++i) {
+        if (t) t[i] = s[i].t;
+        if (dt) dt[i] = s[i].dt;
+        if (nsteps) nsteps[i] = s[i].nsteps;
+        if (nreject) nreject[i] = s[i].nreject;
+        if (cfl_last) cfl_last[i] = s[i].cfl_last;
+        if (status) status[i] = s[i].status;
+    }
+    return CLAW2_OK;
+}
+
+int claw2_batch_tiles(claw2_batch* b, int* ntiles, int* persistent_grid) {
+    if (!b || !ntiles || !persistent_grid) return fail(CLAW2_EINVAL, "bad arguments");
+    *ntiles = (int)b->h_tiles.size();
+    *persistent_grid = b->persistent_grid;
     return CLAW2_OK;
 }
 

@@ -134,20 +134,22 @@ struct UnsplitSmem {
     double red[NT / 32];
 };
 
-template <class RP, int NT, int MINB>
-__global__ void __launch_bounds__(NT, MINB) k_step_unsplit(const StepArgs a) {
+// One tile: the strip `strip` (columns strip*W .. strip*W+NT-1, padded) and
+// the interior rows [rb, rb + H) of one grid.  Returns this thread's CFL
+// contribution in `cfl`; the caller reduces it (the tile ends with every
+// shared-memory read done, so a persistent CTA can start the next tile).
+template <class RP, int NT>
+__device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int rb, UnsplitSmem<RP, NT>& S,
+                                             double& cfl) {
     constexpr int ME = RP::MEQN, MW = RP::MWAVES, NC = RP::NC, W = NT - 4;
     using Iface = typename RP::Iface;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    UnsplitSmem<RP, NT>& S = *reinterpret_cast<UnsplitSmem<RP, NT>*>(smem_raw);
 
     const int t = threadIdx.x;
     const int mx = a.L.mx, my = a.L.my;
     const int pitch = a.L.pitch;
     const long long plane = a.L.plane;
-    const int cp = blockIdx.x * W + t;
+    const int cp = strip * W + t;
     const int cpl = min(cp, mx + 3);
-    const int rb = blockIdx.y * a.H;
     const int Hb = min(a.H, my - rb);
     const int R0 = rb, R1 = rb + Hb + 3;
     const bool out_col = (t >= 2) && (t < W + 2) && (cp <= mx + 1);
@@ -166,7 +168,6 @@ __global__ void __launch_bounds__(NT, MINB) k_step_unsplit(const StepArgs a) {
     double accA[ME], accB[ME], accC[ME], accD[ME];  // rows R-2, R-1, R, R+1
     Iface fY;                                       // y-interface (R-2 | R-1)
     double amY[ME], apY[ME], dY[MW];
-    double cfl = 0.0;
 #pragma unroll
     for (int m = 0; m < ME; ++m) {
         pf[m] = __ldg(qo + m * plane + (long long)R0 * pitch);
@@ -381,6 +382,14 @@ __global__ void __launch_bounds__(NT, MINB) k_step_unsplit(const StepArgs a) {
         s1 = s2;
         s2 = tmp;
     }
+}
+
+template <class RP, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_step_unsplit(const StepArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    UnsplitSmem<RP, NT>& S = *reinterpret_cast<UnsplitSmem<RP, NT>*>(smem_raw);
+    double cfl = 0.0;
+    unsplit_tile<RP, NT>(a, blockIdx.x, blockIdx.y * a.H, S, cfl);
     cfl_commit(cfl, S.red, a.cfl_bits);
 }
 

@@ -240,3 +240,29 @@ def shallow_dam_break_unsplit(solver_class=None, n=4096, tfinal=1.0):
     state.q[1, ...] = 0.0
     state.q[2, ...] = 0.0
     return _controller(solver, Solution(state, domain), tfinal)
+
+
+def batched_quadrants(n_instances=512, seed=2024, sides=tuple(range(64, 513, 16)), solver_class=None):
+    """The batched workload: independent four-quadrant Euler problems on
+    [0,1]^2, side drawn uniformly from `sides` (multiples of 16), split point
+    uniform in [0.3,0.7]^2, per quadrant rho and p uniform in [0.1,2] and u, v
+    uniform in [-1,1]; Roe solver, MC, unsplit trans_cor, extrapolation BCs.
+    Each problem's first dt is 0.45 of its cell-speed CFL limit at t = 0 (the
+    Roe-averaged speed at a quadrant interface can exceed both sides')"""
+    rng = np.random.default_rng(seed)
+    claws, drawn = [], []
+    for i in range(n_instances):
+        side = int(rng.choice(sides))
+        xs, ys = rng.uniform(0.3, 0.7, size=2)
+        states = {}
+        for quad in ('NE', 'NW', 'SW', 'SE'):
+            rho, p = rng.uniform(0.1, 2.0, size=2)
+            u, v = rng.uniform(-1.0, 1.0, size=2)
+            states[quad] = (rho, u, v, p)
+        claw = euler_quadrants_unsplit(solver_class, n=side, split=(xs, ys), states=states)
+        smax = max(abs(u) + np.sqrt(1.4 * p / rho) for rho, u, v, p in states.values())
+        smax = max(smax, max(abs(v) + np.sqrt(1.4 * p / rho) for rho, u, v, p in states.values()))
+        claw.solver.dt_initial = 0.45 * (1.0 / side) / smax
+        claws.append(claw)
+        drawn.append(side)
+    return claws, np.array(drawn)
