@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--n", type=int, default=N, help="grid size override (profiling runs only)")
     ap.add_argument("--secondary", type=int, default=1, help="also time the other benchmark problems")
+    ap.add_argument("--learned", type=int, default=1, help="include the learned-guess exact solver")
     ap.add_argument("--shape", default=None, help="fixed launch shape 'variant,rows' (skips the autotuner)")
     ap.add_argument("--pre-t", type=float, default=0.4,
                     help="advance the problem to this time (untimed) before warm-up")
@@ -232,6 +233,71 @@ def batched_workload(n_instances=512, steps=100):
     return out
 
 
+def learned_workload(stream, flush, n=2048, steps=10, n_train=1 << 24, epochs=16, pre_t=0.4):
+    """Exact Euler solver on the quadrant problem (n^2, unsplit trans_cor, MC),
+    Newton started from the adaptive PVRS guess vs from the learned guess of a
+    network trained here on n_train seeded problems by the library's kernels."""
+    import numpy as np
+    import torch
+    from pyclaw_b200 import learned, riemann, workloads
+    out = {"n": n, "train_problems": n_train, "epochs": epochs}
+    t0 = time.perf_counter()
+    net = learned.Network(seed=2024)
+    out["valid_problems"] = net.generate(n_train, seed=7)
+    torch.cuda.synchronize()
+    out["generate_s"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    out["final_loss"] = net.train(epochs=epochs, batch=16384, lr=3e-3)
+    out["train_s"] = time.perf_counter() - t0
+    # advance the Roe problem to mid-run, then hand the state to the exact solver
+    claw = workloads.euler_quadrants_unsplit(n=n)
+    s, sol = claw.solver, claw.solution
+    s.setup(sol)
+    p = s._dev
+    t, dt, cfl = 0.0, 1e-4, None
+    while t < pre_t:
+        dt = min(dt if cfl is None else dt * 0.9 / cfl, pre_t - t)
+        cfl = p.step(dt)
+        p.accept(cfl <= 1.0)
+        if cfl <= 1.0:
+            t += dt
+    q_mid = sol.state.get_q_global()
+    p.close()
+    res = {}
+    for mode in ("pvrs", "learned"):
+        ce = workloads.euler_quadrants_unsplit(n=n)
+        ce.solver.rp = riemann.euler_exact_2D
+        ce.solver.num_waves = 3
+        ce.solution.state.q = q_mid
+        ce.solver.setup(ce.solution)
+        pe = ce.solver._dev
+        learned.attach(ce.solver, net if mode == "learned" else None)
+        c1 = pe.step(dt)
+        pe.accept(False)
+        dte = dt * 0.9 / c1
+        learned.counters(ce.solver)
+        step_ms, kern_ms = time_patch(pe, dte, steps, flush, stream)
+        it, ns = learned.counters(ce.solver)
+        res[mode] = {"value": n * n / (step_ms * 1e-3), "unit": UNIT, "ms_per_step": step_ms,
+                     "kernel_ms": kern_ms, "newton_per_interface": it / max(ns, 1), "solves": ns}
+        # one step from the same state for the same-answer check
+        ce.solution.state.q = q_mid
+        pe.push(ce.solution.state)
+        pe.step(dte, want_cfl=False)
+        pe.accept(True)
+        res[mode]["_q"] = ce.solution.state.get_q_global()
+        pe.close()
+    qa, qb = res["pvrs"].pop("_q"), res["learned"].pop("_q")
+    out["pvrs_guess"], out["learned_guess"] = res["pvrs"], res["learned"]
+    out["max_rel_diff_one_step"] = float(np.max(np.abs(qa - qb)) / np.max(np.abs(qa)))
+    out["speedup"] = res["learned"]["value"] / res["pvrs"]["value"]
+    out["note"] = ("kernel_ms of the learned guess includes its tensor-core guess pre-pass; "
+                   "Newton updates counted as in csrc/exact_euler.h (a final step below "
+                   "tolerance is applied but not counted)")
+    net.close()
+    return out
+
+
 def secondary_workloads(stream, flush, peaks, steps=20):
     """The shallow-water dam break at 4096^2 (48 B/cell) and the walled
     acoustics problem at 200^2, unsplit trans_cor, MC, CFL 0.9."""
@@ -378,6 +444,8 @@ def run_ours(args):
     if rank == 0 and world == 1 and args.secondary:
         secondary = secondary_workloads(stream, flush, peaks)
         secondary["batched_quadrants_512"] = batched_workload()
+        if args.learned:
+            secondary["learned_exact_euler_2048"] = learned_workload(stream, flush)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and n == N:

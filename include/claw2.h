@@ -215,6 +215,35 @@ int claw2_batch_get_state(claw2_batch* b, double* t, double* dt, int* nsteps, in
                           int* status);
 int claw2_batch_tiles(claw2_batch* b, int* ntiles, int* persistent_grid);
 
+/* ---- the exact Euler solver's learned Newton guess (no reference counterpart)
+ * A 6-32-32-1 tanh network predicting log(p_star / p_pvrs) / w from the normalised
+ * left/right states (w = J^2/(1+J^2), J a normalised jump size), trained on
+ * the device by the library's own forward/backward kernels and Adam, and
+ * evaluated in BF16 on the tensor cores (FP32 accumulation) for every
+ * interface before each exact-solver step. */
+typedef struct claw2_mlp claw2_mlp;
+int claw2_mlp_create(int device, unsigned long long seed, claw2_mlp** out);
+int claw2_mlp_destroy(claw2_mlp* m);
+int claw2_mlp_set_params(claw2_mlp* m, const float* p, int n);  /* n = 1313 */
+int claw2_mlp_get_params(claw2_mlp* m, float* p, int n);
+/* n seeded Riemann problems (rho, p log-uniform in [1e-2, 1e2], u in [-3, 3])
+ * solved to tol by FP64 Newton; *nvalid = problems without vacuum. */
+int claw2_mlp_generate(claw2_mlp* m, unsigned long long seed, long long n, double gamma, double tol,
+                       long long* nvalid);
+/* Host copies of samples [first, first+count): 8 floats of features each
+ * (6 inputs, jump weight, 0), the target and the validity flag. */
+int claw2_mlp_samples(claw2_mlp* m, long long first, int count, float* x8, float* y, int* ok);
+/* Gradient of 0.5 * mean squared error over samples [first, first+count). */
+int claw2_mlp_gradient(claw2_mlp* m, long long first, int count, float* grad, float* loss);
+/* Adam over all samples in minibatches; *last_loss = mean loss of the last epoch. */
+int claw2_mlp_train(claw2_mlp* m, int epochs, int batch, float lr, float* last_loss);
+/* Network outputs for n rows of 8 floats (BF16 tensor cores, FP32 accumulation). */
+int claw2_mlp_infer(claw2_mlp* m, const float* x8, int n, float* y);
+/* Exact-solver patches: start Newton from the network's guesses (NULL: the
+ * adaptive PVRS guess); Newton updates and Riemann solves since the last reset. */
+int claw2_patch_set_mlp(claw2_patch* p, claw2_mlp* m);
+int claw2_patch_counters(claw2_patch* p, unsigned long long* iters_and_solves, int reset);
+
 /* Description of the last error on this thread (never NULL). */
 const char* claw2_last_error(void);
 

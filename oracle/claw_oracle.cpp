@@ -505,12 +505,190 @@ void rpt2_shallow_roe(int ixy, int mbc, int mx, int meqn, int mwaves, const CSli
     }
 }
 
+
+// ---------------------------------------------------------------------------
+// Exact Euler Riemann solver (no reference counterpart), restated from Toro,
+// Riemann Solvers and Numerical Methods for Fluid Dynamics (3rd ed., 2009):
+// guess (sec. 9.5.1 adaptive PVRS / TRRS / TSRS), pressure functions
+// (eqs. 4.6-4.7, 4.37), Newton with the relative-change test of sec. 4.3.2,
+// star velocity (eq. 4.9) and sampling at x/t = 0 (sec. 4.5).
+// ---------------------------------------------------------------------------
+struct ExGas {
+    double g, g1, g2, g3, g4, g5, g6, g7;
+    explicit ExGas(double gamma) : g(gamma) {
+        g1 = (g - 1.0) / (2.0 * g); g2 = (g + 1.0) / (2.0 * g); g3 = 2.0 * g / (g - 1.0);
+        g4 = 2.0 / (g - 1.0); g5 = 2.0 / (g + 1.0); g6 = (g - 1.0) / (g + 1.0); g7 = (g - 1.0) / 2.0;
+    }
+};
+
+void ex_prefun(const ExGas& G, double p, double dk, double pk, double ck, double& f, double& fd) {
+    if (p <= pk) {
+        double prat = p / pk;
+        f = G.g4 * ck * (std::pow(prat, G.g1) - 1.0);
+        fd = (1.0 / (dk * ck)) * std::pow(prat, -G.g2);
+    } else {
+        double ak = G.g5 / dk, bk = G.g6 * pk, qrt = std::sqrt(ak / (bk + p));
+        f = (p - pk) * qrt;
+        fd = (1.0 - 0.5 * (p - pk) / (bk + p)) * qrt;
+    }
+}
+
+double ex_guess(const ExGas& G, double dl, double ul, double pl, double cl, double dr, double ur, double pr, double cr) {
+    double cup = 0.25 * (dl + dr) * (cl + cr);
+    double ppv = std::max(0.0, 0.5 * (pl + pr) + 0.5 * (ul - ur) * cup);
+    double pmin = std::min(pl, pr), pmax = std::max(pl, pr), qmax = pmax / pmin;
+    if (qmax <= 2.0 && pmin <= ppv && ppv <= pmax) return ppv;
+    if (ppv < pmin) {
+        double pq = std::pow(pl / pr, G.g1);
+        double um = (pq * ul / cl + ur / cr + G.g4 * (pq - 1.0)) / (pq / cl + 1.0 / cr);
+        double ptl = 1.0 + G.g7 * (ul - um) / cl, ptr = 1.0 + G.g7 * (um - ur) / cr;
+        return 0.5 * (pl * std::pow(ptl, G.g3) + pr * std::pow(ptr, G.g3));
+    }
+    double gel = std::sqrt((G.g5 / dl) / (G.g6 * pl + ppv));
+    double ger = std::sqrt((G.g5 / dr) / (G.g6 * pr + ppv));
+    return (gel * pl + ger * pr - (ur - ul)) / (gel + ger);
+}
+
+// returns false on vacuum
+bool ex_starpu(const ExGas& G, double dl, double ul, double pl, double dr, double ur, double pr, double tol,
+               double& p, double& u, int& iters) {
+    double cl = std::sqrt(G.g * pl / dl), cr = std::sqrt(G.g * pr / dr);
+    iters = 0;
+    if (G.g4 * (cl + cr) <= ur - ul) return false;
+    if (dl == dr && ul == ur && pl == pr) { p = pl; u = ul; return true; }
+    double pold = std::max(ex_guess(G, dl, ul, pl, cl, dr, ur, pr, cr), tol);
+    double udiff = ur - ul, fl = 0, fr = 0, fld, frd;
+    for (int i = 1; i <= 100; ++i) {
+        ex_prefun(G, pold, dl, pl, cl, fl, fld);
+        ex_prefun(G, pold, dr, pr, cr, fr, frd);
+        p = pold - (fl + fr + udiff) / (fld + frd);
+        double change = 2.0 * std::fabs((p - pold) / (p + pold));
+        ++iters;
+        if (change <= tol) break;
+        if (p < 0.0) p = tol;
+        pold = p;
+    }
+    ex_prefun(G, p, dl, pl, cl, fl, fld);
+    ex_prefun(G, p, dr, pr, cr, fr, frd);
+    u = 0.5 * (ul + ur + fr - fl);
+    return true;
+}
+
+// state at x/t = 0 (Toro SAMPLE with S = 0); left = point left of the contact
+void ex_sample0(const ExGas& G, double pm, double um, double dl, double ul, double pl, double dr, double ur, double pr,
+                double& d, double& u, double& p, bool& left) {
+    double cl = std::sqrt(G.g * pl / dl), cr = std::sqrt(G.g * pr / dr);
+    const double s = 0.0;
+    left = s <= um;
+    if (left) {
+        if (pm <= pl) {
+            double shl = ul - cl;
+            if (s <= shl) { d = dl; u = ul; p = pl; return; }
+            double cml = cl * std::pow(pm / pl, G.g1), stl = um - cml;
+            if (s > stl) { d = dl * std::pow(pm / pl, 1.0 / G.g); u = um; p = pm; return; }
+            u = G.g5 * (cl + G.g7 * ul + s);
+            double c = G.g5 * (cl + G.g7 * (ul - s));
+            d = dl * std::pow(c / cl, G.g4);
+            p = pl * std::pow(c / cl, G.g3);
+        } else {
+            double pml = pm / pl, sl = ul - cl * std::sqrt(G.g2 * pml + G.g1);
+            if (s <= sl) { d = dl; u = ul; p = pl; }
+            else { d = dl * (pml + G.g6) / (pml * G.g6 + 1.0); u = um; p = pm; }
+        }
+    } else {
+        if (pm > pr) {
+            double pmr = pm / pr, sr = ur + cr * std::sqrt(G.g2 * pmr + G.g1);
+            if (s >= sr) { d = dr; u = ur; p = pr; }
+            else { d = dr * (pmr + G.g6) / (pmr * G.g6 + 1.0); u = um; p = pm; }
+        } else {
+            double shr = ur + cr;
+            if (s >= shr) { d = dr; u = ur; p = pr; return; }
+            double cmr = cr * std::pow(pm / pr, G.g1), str = um + cmr;
+            if (s <= str) { d = dr * std::pow(pm / pr, 1.0 / G.g); u = um; p = pm; return; }
+            u = G.g5 * (-cr + G.g7 * ur + s);
+            double c = G.g5 * (cr - G.g7 * (ur - s));
+            d = dr * std::pow(c / cr, G.g4);
+            p = pr * std::pow(c / cr, G.g3);
+        }
+    }
+}
+
+int g_exact_vacuum = 0;
+
+// Wave-propagation form of the exact solver on a slice: waves Q*L - QL,
+// Q*R - Q*L, QR - Q*R; speeds = shock speed or the fan's mean speed, u*;
+// fluctuations from the Godunov flux F(Q(0)).  cparam = gamma, tol.
+void rpn2_euler_exact(int ixy, int mbc, int mx, int meqn, int mwaves, const CSlice& ql, const CSlice& qr,
+                      const Waves& wave, const Speeds& s, const Slice& amdq, const Slice& apdq, const double* cp) {
+    (void)meqn; (void)mwaves;
+    const double gamma = cp[0], tol = cp[1], g1 = gamma - 1.0;
+    const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
+    ExGas G(gamma);
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        double QL[4], QR[4];
+        for (int m = 0; m < 4; ++m) { QL[m] = qr(m, i - 1); QR[m] = ql(m, i); }
+        double dl = QL[0], ul = QL[mu] / dl, vl = QL[mv] / dl, pl = g1 * (QL[3] - 0.5 * dl * (ul * ul + vl * vl));
+        double dr = QR[0], ur = QR[mu] / dr, vr = QR[mv] / dr, pr = g1 * (QR[3] - 0.5 * dr * (ur * ur + vr * vr));
+        double pm, um;
+        int it;
+        if (!ex_starpu(G, dl, ul, pl, dr, ur, pr, tol, pm, um, it)) {
+            g_exact_vacuum = 1;
+            pm = 0.5 * (pl + pr); um = 0.5 * (ul + ur);
+        }
+        double cl = std::sqrt(gamma * pl / dl), cr = std::sqrt(gamma * pr / dr);
+        double dsl, dsr, s1, s3;
+        if (pm > pl) {
+            double pml = pm / pl;
+            dsl = dl * (pml + G.g6) / (pml * G.g6 + 1.0);
+            s1 = ul - cl * std::sqrt(G.g2 * pml + G.g1);
+        } else {
+            dsl = dl * std::pow(pm / pl, 1.0 / gamma);
+            s1 = 0.5 * ((ul - cl) + (um - cl * std::pow(pm / pl, G.g1)));
+        }
+        if (pm > pr) {
+            double pmr = pm / pr;
+            dsr = dr * (pmr + G.g6) / (pmr * G.g6 + 1.0);
+            s3 = ur + cr * std::sqrt(G.g2 * pmr + G.g1);
+        } else {
+            dsr = dr * std::pow(pm / pr, 1.0 / gamma);
+            s3 = 0.5 * ((ur + cr) + (um + cr * std::pow(pm / pr, G.g1)));
+        }
+        auto cons = [&](double d, double un, double ut, double p, double* Q) {
+            Q[0] = d; Q[mu] = d * un; Q[mv] = d * ut; Q[3] = p / g1 + 0.5 * d * (un * un + ut * ut);
+        };
+        auto flux = [&](double d, double un, double ut, double p, double* F) {
+            double E = p / g1 + 0.5 * d * (un * un + ut * ut);
+            F[0] = d * un; F[mu] = d * un * un + p; F[mv] = d * un * ut; F[3] = un * (E + p);
+        };
+        double QsL[4], QsR[4];
+        cons(dsl, um, vl, pm, QsL);
+        cons(dsr, um, vr, pm, QsR);
+        for (int m = 0; m < 4; ++m) {
+            wave(m, 0, i) = QsL[m] - QL[m];
+            wave(m, 1, i) = QsR[m] - QsL[m];
+            wave(m, 2, i) = QR[m] - QsR[m];
+        }
+        s(0, i) = s1; s(1, i) = um; s(2, i) = s3;
+        double d0, u0, p0;
+        bool left;
+        ex_sample0(G, pm, um, dl, ul, pl, dr, ur, pr, d0, u0, p0, left);
+        double F0[4], FL[4], FR[4];
+        flux(d0, u0, left ? vl : vr, p0, F0);
+        flux(dl, ul, vl, pl, FL);
+        flux(dr, ur, vr, pr, FR);
+        for (int m = 0; m < 4; ++m) {
+            amdq(m, i) = F0[m] - FL[m];
+            apdq(m, i) = FR[m] - F0[m];
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Dispatch
 // ---------------------------------------------------------------------------
 bool rp_known(int rp) {
     return rp == ORC_RP_ADVECTION || rp == ORC_RP_ACOUSTICS || rp == ORC_RP_EULER_ROE ||
-           rp == ORC_RP_SHALLOW_ROE;
+           rp == ORC_RP_SHALLOW_ROE || rp == ORC_RP_EULER_EXACT;
 }
 
 void call_rpn2(int rp, int ixy, int mbc, int mx, int meqn, int mwaves, const CSlice& q,
@@ -521,6 +699,7 @@ void call_rpn2(int rp, int ixy, int mbc, int mx, int meqn, int mwaves, const CSl
         case ORC_RP_ACOUSTICS: rpn2_acoustics(ixy, mbc, mx, q, q, wave, s, amdq, apdq, cp, meqn); break;
         case ORC_RP_EULER_ROE: rpn2_euler_roe(ixy, mbc, mx, meqn, mwaves, q, q, wave, s, amdq, apdq, cp); break;
         case ORC_RP_SHALLOW_ROE: rpn2_shallow_roe(ixy, mbc, mx, meqn, mwaves, q, q, wave, s, amdq, apdq, cp); break;
+        case ORC_RP_EULER_EXACT: rpn2_euler_exact(ixy, mbc, mx, meqn, mwaves, q, q, wave, s, amdq, apdq, cp); break;
     }
 }
 void call_rpt2(int rp, int ixy, int mbc, int mx, int meqn, int mwaves, const CSlice& q,
@@ -530,6 +709,7 @@ void call_rpt2(int rp, int ixy, int mbc, int mx, int meqn, int mwaves, const CSl
         case ORC_RP_ACOUSTICS: rpt2_acoustics(ixy, mbc, mx, asdq, bm, bp, cp); break;
         case ORC_RP_EULER_ROE: rpt2_euler_roe(ixy, mbc, mx, meqn, mwaves, q, q, asdq, bm, bp, cp); break;
         case ORC_RP_SHALLOW_ROE: rpt2_shallow_roe(ixy, mbc, mx, meqn, mwaves, q, q, asdq, bm, bp, cp); break;
+        case ORC_RP_EULER_EXACT: rpt2_euler_roe(ixy, mbc, mx, meqn, 4, q, q, asdq, bm, bp, cp); break;
     }
 }
 
@@ -875,6 +1055,7 @@ int oracle_rpn2(int rp, int ixy, int maxm, int meqn, int mwaves, int mbc, int mx
         case ORC_RP_ACOUSTICS: rpn2_acoustics(ixy, mbc, mx, l, r, w, sp, am, ap, cp, meqn); break;
         case ORC_RP_EULER_ROE: rpn2_euler_roe(ixy, mbc, mx, meqn, mwaves, l, r, w, sp, am, ap, cp); break;
         case ORC_RP_SHALLOW_ROE: rpn2_shallow_roe(ixy, mbc, mx, meqn, mwaves, l, r, w, sp, am, ap, cp); break;
+        case ORC_RP_EULER_EXACT: rpn2_euler_exact(ixy, mbc, mx, meqn, mwaves, l, r, w, sp, am, ap, cp); break;
     }
     return 0;
 }
@@ -895,9 +1076,11 @@ int oracle_rpt2(int rp, int ixy, int imp, int maxm, int meqn, int mwaves, int mb
     return 0;
 }
 
-int oracle_exact_star(double, double, double, double, double, double, double, double, int,
-                      double*, double*, int*) {
-    return 99;  // filled in with the exact solver
+int oracle_exact_star(double gamma, double rl, double ul, double pl, double rr, double ur, double pr, double tol,
+                      int guess, double* pstar, double* ustar, int* iters) {
+    (void)guess;
+    ExGas G(gamma);
+    return ex_starpu(G, rl, ul, pl, rr, ur, pr, tol, *pstar, *ustar, *iters) ? 0 : 7;
 }
 
 }  // extern "C"

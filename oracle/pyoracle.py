@@ -43,6 +43,7 @@ def load():
     lib.oracle_rpn2.argtypes = [i] * 7 + [_dp, _dp, _dp, _dp, _dp, _dp, _dp]
     lib.oracle_rpt2.argtypes = [i] * 8 + [_dp, _dp, _dp, _dp, _dp, _dp]
     lib.oracle_exact_star.argtypes = [d] * 8 + [i, _dp, _dp, _ip]
+    lib.oracle_rpn2.argtypes = [i] * 7 + [_dp] * 7
     lib.oracle_set_threads.argtypes = [i]
     lib.oracle_set_threads.restype = None
     _lib = lib

@@ -95,6 +95,22 @@ _SIGNATURES = {
     "claw2_batch_get_state": (ctypes.c_int, [ctypes.c_void_p, _c_double_p, _c_double_p, _c_int_p, _c_int_p,
                                              _c_double_p, _c_int_p]),
     "claw2_batch_tiles": (ctypes.c_int, [ctypes.c_void_p, _c_int_p, _c_int_p]),
+    "claw2_mlp_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_void_p)]),
+    "claw2_mlp_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "claw2_mlp_set_params": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float), ctypes.c_int]),
+    "claw2_mlp_get_params": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float), ctypes.c_int]),
+    "claw2_mlp_generate": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_longlong, ctypes.c_double,
+                                          ctypes.c_double, ctypes.POINTER(ctypes.c_longlong)]),
+    "claw2_mlp_samples": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_int,
+                                         ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), _c_int_p]),
+    "claw2_mlp_gradient": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_int,
+                                          ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
+    "claw2_mlp_train": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                       ctypes.POINTER(ctypes.c_float)]),
+    "claw2_mlp_infer": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float), ctypes.c_int,
+                                       ctypes.POINTER(ctypes.c_float)]),
+    "claw2_patch_set_mlp": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "claw2_patch_counters": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_int]),
     "claw2_last_error": (ctypes.c_char_p, []),
     "claw2_version": (ctypes.c_char_p, []),
 }

@@ -106,6 +106,8 @@ __global__ void __launch_bounds__(NT, MINB) k_batch_step(const BatchArgs b, int 
         a.meth = b.meth;
         a.cfl_bits = &s.cfl_bits;
         a.status = &s.status;
+        a.guess = nullptr;
+        a.counters = nullptr;
         const int strip = tl.y % in.nstrips, rblk = tl.y / in.nstrips;
         double cfl = 0.0;
         unsplit_tile<RP, NT>(a, strip, rblk * in.H, S, cfl);

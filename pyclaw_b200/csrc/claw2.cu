@@ -15,6 +15,7 @@
 #include <string>
 
 #include "batch.cuh"
+#include "mlp.cuh"
 #include "step_kernels.cuh"
 
 #include <vector>
@@ -36,6 +37,17 @@ int fail(int code, const char* fmt, ...) {
     return code;
 }
 
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
 #define CUDA_TRY(expr)                                                                      \
     do {                                                                                    \
         cudaError_t e_ = (expr);                                                            \
@@ -53,6 +65,7 @@ int rp_shape(int rp, int* meqn, int* mwaves) {
         case CLAW2_RP_ACOUSTICS: *meqn = 3; *mwaves = 2; return 0;
         case CLAW2_RP_EULER_ROE: *meqn = 4; *mwaves = 4; return 0;
         case CLAW2_RP_SHALLOW_ROE: *meqn = 3; *mwaves = 3; return 0;
+        case CLAW2_RP_EULER_EXACT: *meqn = 4; *mwaves = 3; return 0;
         default: return -1;
     }
 }
@@ -154,6 +167,7 @@ int dispatch(int rp, A&&... args) {
         case CLAW2_RP_ACOUSTICS: F<RPAcoustics>::run(args...); return 0;
         case CLAW2_RP_EULER_ROE: F<RPEulerRoe>::run(args...); return 0;
         case CLAW2_RP_SHALLOW_ROE: F<RPShallowRoe>::run(args...); return 0;
+        case CLAW2_RP_EULER_EXACT: F<RPEulerExact>::run(args...); return 0;
         default: return -1;
     }
 }
@@ -308,6 +322,8 @@ int host_step(int maxm, int meqn, int mwaves, int maux, int mbc, int mx, int my,
     for (int k = 0; k < CLAW2_MAX_WAVES; ++k) a.meth.mthlim[k] = k < mwaves ? mthlim[k] : 0;
     a.cfl_bits = g_scr.cfl;
     a.status = g_scr.status;
+    a.guess = nullptr;
+    a.counters = nullptr;
 
     a.qold = g_scr.a;
     a.qnew = g_scr.b;
@@ -341,9 +357,215 @@ int host_step(int maxm, int meqn, int mwaves, int maux, int mbc, int mx, int my,
 
 }  // namespace
 
+
+// ===========================================================================
+// The learned Newton guess (mlp.cuh)
+// ===========================================================================
+struct claw2_mlp {
+    int device = 0;
+    float* P = nullptr;      // parameters (FP32)
+    float* G = nullptr;      // gradient accumulator
+    float* M1 = nullptr;     // Adam moments
+    float* M2 = nullptr;
+    float* loss = nullptr;
+    MlpPacked* packed = nullptr;
+    int adam_step = 0;
+    float* x = nullptr;      // samples: 8 floats each
+    float* y = nullptr;
+    int* ok = nullptr;
+    long long nsamples = 0, cap = 0;
+    cudaStream_t st = nullptr;
+};
+
+namespace {
+
+int mlp_repack(claw2_mlp* m) {
+    std::vector<float> h(MLP_NPARAM);
+    CUDA_TRY(cudaMemcpy(h.data(), m->P, MLP_NPARAM * 4, cudaMemcpyDeviceToHost));
+    MlpPacked pk;
+    mlp_pack(h.data(), pk);
+    CUDA_TRY(cudaMemcpy(m->packed, &pk, sizeof pk, cudaMemcpyHostToDevice));
+    return CLAW2_OK;
+}
+
+void mlp_guess_launch(claw2_mlp* m, const double* q, const Layout& L, double gamma, double* guess, cudaStream_t st) {
+    dim3 grid((L.mx + 4 + 31) / 32, (L.my + 4 + 3) / 4);
+    k_mlp_guess<<<grid, 128, 0, st>>>(m->packed, q, L, gamma, guess);
+}
+
+}  // namespace
+
+extern "C" {
+
+int claw2_mlp_create(int device, unsigned long long seed, claw2_mlp** out) {
+    if (!out) return fail(CLAW2_EINVAL, "null pointer argument");
+    *out = nullptr;
+    claw2_mlp* m = new claw2_mlp();
+    m->device = device;
+    DeviceGuard g(device);
+    bool ok = cudaMalloc(&m->P, MLP_NPARAM * 4) == cudaSuccess && cudaMalloc(&m->G, MLP_NPARAM * 4) == cudaSuccess &&
+              cudaMalloc(&m->M1, MLP_NPARAM * 4) == cudaSuccess && cudaMalloc(&m->M2, MLP_NPARAM * 4) == cudaSuccess &&
+              cudaMalloc(&m->loss, 4) == cudaSuccess && cudaMalloc(&m->packed, sizeof(MlpPacked)) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&m->st, cudaStreamNonBlocking) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        claw2_mlp_destroy(m);
+        return fail(CLAW2_ENOMEM, "device allocation for the network failed");
+    }
+    // Glorot-uniform weights from the counter RNG, zero biases
+    std::vector<float> h(MLP_NPARAM, 0.f);
+    auto fill = [&](int off, int fan_out, int fan_in) {
+        const double a = std::sqrt(6.0 / (fan_in + fan_out));
+        for (int k = 0; k < fan_out * fan_in; ++k) h[off + k] = (float)(a * (2.0 * u01(seed, off + k, 7) - 1.0));
+    };
+    fill(OFF_W1, MLP_H, MLP_IN);
+    fill(OFF_W2, MLP_H, MLP_H);
+    fill(OFF_W3, 1, MLP_H);
+    cudaMemcpy(m->P, h.data(), MLP_NPARAM * 4, cudaMemcpyHostToDevice);
+    cudaMemset(m->G, 0, MLP_NPARAM * 4);
+    cudaMemset(m->M1, 0, MLP_NPARAM * 4);
+    cudaMemset(m->M2, 0, MLP_NPARAM * 4);
+    int rc = mlp_repack(m);
+    if (rc) {
+        claw2_mlp_destroy(m);
+        return rc;
+    }
+    *out = m;
+    return CLAW2_OK;
+}
+
+int claw2_mlp_destroy(claw2_mlp* m) {
+    if (!m) return CLAW2_OK;
+    {
+        DeviceGuard g(m->device);
+        if (m->st) cudaStreamSynchronize(m->st);
+        cudaFree(m->P); cudaFree(m->G); cudaFree(m->M1); cudaFree(m->M2); cudaFree(m->loss);
+        cudaFree(m->packed); cudaFree(m->x); cudaFree(m->y); cudaFree(m->ok);
+        if (m->st) cudaStreamDestroy(m->st);
+    }
+    delete m;
+    return CLAW2_OK;
+}
+
+int claw2_mlp_set_params(claw2_mlp* m, const float* p, int n) {
+    if (!m || !p || n != MLP_NPARAM) return fail(CLAW2_EINVAL, "need %d parameters", MLP_NPARAM);
+    DeviceGuard g(m->device);
+    CUDA_TRY(cudaMemcpy(m->P, p, MLP_NPARAM * 4, cudaMemcpyHostToDevice));
+    return mlp_repack(m);
+}
+
+int claw2_mlp_get_params(claw2_mlp* m, float* p, int n) {
+    if (!m || !p || n != MLP_NPARAM) return fail(CLAW2_EINVAL, "need %d parameters", MLP_NPARAM);
+    DeviceGuard g(m->device);
+    CUDA_TRY(cudaMemcpy(p, m->P, MLP_NPARAM * 4, cudaMemcpyDeviceToHost));
+    return CLAW2_OK;
+}
+
+int claw2_mlp_generate(claw2_mlp* m, unsigned long long seed, long long n, double gamma, double tol,
+                       long long* nvalid) {
+    if (!m || n < 1 || n > (1ll << 28)) return fail(CLAW2_EINVAL, "bad sample count");
+    DeviceGuard g(m->device);
+    if (n > m->cap) {
+        cudaFree(m->x); cudaFree(m->y); cudaFree(m->ok);
+        m->x = nullptr; m->y = nullptr; m->ok = nullptr; m->cap = 0;
+        if (cudaMalloc(&m->x, n * 8 * 4) != cudaSuccess || cudaMalloc(&m->y, n * 4) != cudaSuccess ||
+            cudaMalloc(&m->ok, n * 4) != cudaSuccess)
+            return fail(CLAW2_ENOMEM, "device allocation for %lld samples failed", n);
+        m->cap = n;
+    }
+    const int chunk = 1 << 22;
+    for (long long f = 0; f < n; f += chunk) {
+        const int c = (int)std::min<long long>(chunk, n - f);
+        k_gen_samples<<<(c + 255) / 256, 256, 0, m->st>>>(seed, f, c, gamma, tol, m->x + f * 8, m->y + f,
+                                                          m->ok + f, nullptr);
+    }
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(m->st));
+    m->nsamples = n;
+    if (nvalid) {
+        std::vector<int> h(n);
+        CUDA_TRY(cudaMemcpy(h.data(), m->ok, n * 4, cudaMemcpyDeviceToHost));
+        long long s = 0;
+        for (long long k = 0; k < n; ++k) s += h[k];
+        *nvalid = s;
+    }
+    return CLAW2_OK;
+}
+
+int claw2_mlp_samples(claw2_mlp* m, long long first, int count, float* x8, float* y, int* ok) {
+    if (!m || first < 0 || count < 0 || first + count > m->nsamples) return fail(CLAW2_EINVAL, "bad sample range");
+    DeviceGuard g(m->device);
+    if (x8) CUDA_TRY(cudaMemcpy(x8, m->x + first * 8, (size_t)count * 32, cudaMemcpyDeviceToHost));
+    if (y) CUDA_TRY(cudaMemcpy(y, m->y + first, (size_t)count * 4, cudaMemcpyDeviceToHost));
+    if (ok) CUDA_TRY(cudaMemcpy(ok, m->ok + first, (size_t)count * 4, cudaMemcpyDeviceToHost));
+    return CLAW2_OK;
+}
+
+int claw2_mlp_gradient(claw2_mlp* m, long long first, int count, float* grad, float* loss) {
+    if (!m || !grad || first < 0 || count < 1 || first + count > m->nsamples)
+        return fail(CLAW2_EINVAL, "bad sample range");
+    DeviceGuard g(m->device);
+    CUDA_TRY(cudaMemsetAsync(m->G, 0, MLP_NPARAM * 4, m->st));
+    CUDA_TRY(cudaMemsetAsync(m->loss, 0, 4, m->st));
+    k_train_grad<<<(count + 255) / 256, 256, 0, m->st>>>(m->P, m->x, m->y, m->ok, first, count, 1.f / count, m->G,
+                                                         m->loss);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(grad, m->G, MLP_NPARAM * 4, cudaMemcpyDeviceToHost, m->st));
+    if (loss) CUDA_TRY(cudaMemcpyAsync(loss, m->loss, 4, cudaMemcpyDeviceToHost, m->st));
+    CUDA_TRY(cudaStreamSynchronize(m->st));
+    CUDA_TRY(cudaMemset(m->G, 0, MLP_NPARAM * 4));
+    return CLAW2_OK;
+}
+
+int claw2_mlp_train(claw2_mlp* m, int epochs, int batch, float lr, float* last_loss) {
+    if (!m || epochs < 0 || batch < 32 || m->nsamples < batch) return fail(CLAW2_EINVAL, "bad training arguments");
+    DeviceGuard g(m->device);
+    const long long nb = m->nsamples / batch;
+    float l = 0.f;
+    for (int e = 0; e < epochs; ++e) {
+        CUDA_TRY(cudaMemsetAsync(m->loss, 0, 4, m->st));
+        for (long long b = 0; b < nb; ++b) {
+            k_train_grad<<<(batch + 255) / 256, 256, 0, m->st>>>(m->P, m->x, m->y, m->ok, b * batch, batch,
+                                                                 1.f / batch, m->G, m->loss);
+            ++m->adam_step;
+            // step size decays linearly to a tenth over the run
+            const float frac = (float)(e * nb + b) / (float)(epochs * nb);
+            k_adam<<<(MLP_NPARAM + 255) / 256, 256, 0, m->st>>>(m->P, m->G, m->M1, m->M2, lr * (1.f - 0.9f * frac),
+                                                                0.9f, 0.999f, 1e-8f, m->adam_step);
+        }
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaMemcpyAsync(&l, m->loss, 4, cudaMemcpyDeviceToHost, m->st));
+        CUDA_TRY(cudaStreamSynchronize(m->st));
+        l /= (float)nb;
+    }
+    if (last_loss) *last_loss = l;
+    return mlp_repack(m);
+}
+
+int claw2_mlp_infer(claw2_mlp* m, const float* x8, int n, float* y) {
+    if (!m || !x8 || !y || n < 1) return fail(CLAW2_EINVAL, "bad arguments");
+    DeviceGuard g(m->device);
+    float *dx = nullptr, *dy = nullptr;
+    if (cudaMalloc(&dx, (size_t)n * 32) != cudaSuccess || cudaMalloc(&dy, (size_t)n * 4) != cudaSuccess) {
+        cudaFree(dx);
+        return fail(CLAW2_ENOMEM, "device allocation failed");
+    }
+    cudaMemcpy(dx, x8, (size_t)n * 32, cudaMemcpyHostToDevice);
+    k_mlp_eval<<<(n + 255) / 256, 128, 0, m->st>>>(m->packed, dx, n, dy);
+    cudaError_t e = cudaStreamSynchronize(m->st);
+    if (e == cudaSuccess) e = cudaMemcpy(y, dy, (size_t)n * 4, cudaMemcpyDeviceToHost);
+    cudaFree(dx);
+    cudaFree(dy);
+    if (e != cudaSuccess) return fail(CLAW2_ECUDA, "inference failed: %s", cudaGetErrorString(e));
+    return CLAW2_OK;
+}
+
+}  // extern "C"
+
 // ===========================================================================
 // Device-resident patch
 // ===========================================================================
+struct claw2_mlp;
 struct claw2_patch {
     claw2_desc d;
     Layout L;
@@ -361,22 +583,15 @@ struct claw2_patch {
     cudaStream_t own_st = nullptr;  // the patch's own stream
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool timing = false;
+    double* guess = nullptr;                  // exact solver: learned guesses, x and y planes
+    unsigned long long* counters = nullptr;   // exact solver: Newton iterations, solves
+    claw2_mlp* mlp = nullptr;
     int cur = 0;
     bool pending = false;
 };
 
 namespace {
 
-struct DeviceGuard {
-    int prev = -1;
-    explicit DeviceGuard(int dev) {
-        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
-        if (prev != dev) cudaSetDevice(dev);
-    }
-    ~DeviceGuard() {
-        if (prev >= 0) cudaSetDevice(prev);
-    }
-};
 
 StepArgs patch_args(claw2_patch* p, double dt) {
     StepArgs a;
@@ -388,6 +603,8 @@ StepArgs patch_args(claw2_patch* p, double dt) {
     a.meth = p->meth;
     a.cfl_bits = p->cfl;
     a.status = p->status;
+    a.guess = nullptr;
+    a.counters = p->counters;
     a.qold = p->q[p->cur];
     a.qnew = p->q[p->cur ^ 1];
     return a;
@@ -490,6 +707,9 @@ int claw2_patch_create(const claw2_desc* d, claw2_patch** out) {
               cudaStreamCreateWithFlags(&p->own_st, cudaStreamNonBlocking) == cudaSuccess;
     p->st = p->own_st;
     if (ok && d->dimensional_split) ok = cudaMalloc(&p->tmp, nb) == cudaSuccess;
+    if (ok && d->riemann == CLAW2_RP_EULER_EXACT)
+        ok = cudaMalloc(&p->guess, 2 * (size_t)p->L.plane * 8) == cudaSuccess &&
+             cudaMalloc(&p->counters, 2 * sizeof(unsigned long long)) == cudaSuccess;
     if (!ok) {
         cudaGetLastError();
         claw2_patch_destroy(p);
@@ -499,6 +719,7 @@ int claw2_patch_create(const claw2_desc* d, claw2_patch** out) {
     cudaMemsetAsync(p->q[0], 0, nb, p->st);
     cudaMemsetAsync(p->q[1], 0, nb, p->st);
     if (p->tmp) cudaMemsetAsync(p->tmp, 0, nb, p->st);
+    if (p->counters) cudaMemsetAsync(p->counters, 0, 2 * sizeof(unsigned long long), p->st);
     cudaMemsetAsync(p->cfl, 0, sizeof(unsigned long long), p->st);
     cudaMemsetAsync(p->status, 0, sizeof(int), p->st);
     if (cudaStreamSynchronize(p->st) != cudaSuccess) {
@@ -517,6 +738,8 @@ int claw2_patch_destroy(claw2_patch* p) {
         cudaFree(p->q[0]);
         cudaFree(p->q[1]);
         cudaFree(p->tmp);
+        cudaFree(p->guess);
+        cudaFree(p->counters);
         cudaFree(p->stage);
         cudaFree(p->cfl);
         cudaFree(p->status);
@@ -569,6 +792,10 @@ int claw2_patch_step(claw2_patch* p, double dt, double* cfl) {
     launch_bc(qc, p->L, p->d.num_eqn, p->d.bc_lower, p->d.bc_upper, p->cfl, p->st);
     StepArgs a = patch_args(p, dt);
     if (p->timing) CUDA_TRY(cudaEventRecord(p->ev0, p->st));
+    if (p->d.riemann == CLAW2_RP_EULER_EXACT && p->mlp && !p->d.dimensional_split) {
+        mlp_guess_launch(p->mlp, qc, p->L, p->rp.c[0], p->guess, p->st);
+        a.guess = p->guess;
+    }
     if (p->d.dimensional_split) {
         StepArgs ax = a, ay = a;
         ax.qnew = p->tmp;
@@ -688,6 +915,26 @@ int claw2_tune_get(int riemann, int* variant, int* rows) {
     if (riemann < 1 || riemann > 7 || !variant || !rows) return fail(CLAW2_EINVAL, "bad arguments");
     *variant = g_tune[riemann & 7].variant;
     *rows = g_tune[riemann & 7].rows;
+    return CLAW2_OK;
+}
+
+int claw2_patch_set_mlp(claw2_patch* p, claw2_mlp* m) {
+    if (!p) return fail(CLAW2_EINVAL, "null patch");
+    if (m && p->d.riemann != CLAW2_RP_EULER_EXACT)
+        return fail(CLAW2_EINVAL, "learned guesses apply to the exact Euler solver only");
+    if (m && m->device != p->device) return fail(CLAW2_EINVAL, "network and patch are on different devices");
+    p->mlp = m;
+    return CLAW2_OK;
+}
+
+int claw2_patch_counters(claw2_patch* p, unsigned long long* out, int reset) {
+    if (!p || !out) return fail(CLAW2_EINVAL, "null pointer argument");
+    out[0] = out[1] = 0;
+    if (!p->counters) return CLAW2_OK;
+    DeviceGuard g(p->device);
+    CUDA_TRY(cudaMemcpyAsync(out, p->counters, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, p->st));
+    CUDA_TRY(cudaStreamSynchronize(p->st));
+    if (reset) CUDA_TRY(cudaMemsetAsync(p->counters, 0, 2 * sizeof(unsigned long long), p->st));
     return CLAW2_OK;
 }
 

@@ -170,6 +170,8 @@ int claw2_step2ds_noalloc(const claw2_desc* d, const double* qold, double* qnew,
     for (int k = 0; k < CLAW2_MAX_WAVES; ++k) a.meth.mthlim[k] = k < mwaves ? d->mthlim[k] : 0;
     a.cfl_bits = cfl_bits;
     a.status = status;
+    a.guess = nullptr;
+    a.counters = nullptr;
     StepArgs ax = a, ay = a;
     ax.qold = qold;
     ax.qnew = qtmp;  // x-sweep: every row of the interior columns, ghost columns copied

@@ -1,0 +1,228 @@
+// exact_euler.h -- exact Riemann solver of the 1D Euler equations (the normal
+// direction of a 2D interface), used by the CUDA kernels (the CPU oracle
+// restates it independently in oracle/claw_oracle.cpp).
+//
+// Method: Toro, Riemann Solvers and Numerical Methods for Fluid Dynamics, 3rd
+// ed., Springer 2009, ch. 4: p* is the root of
+//     f(p) = f_L(p) + f_R(p) + (u_R - u_L),
+// f_K = shock branch (p > p_K) or rarefaction branch (p <= p_K) (eqs. 4.6-4.7,
+// derivatives 4.37), found by Newton's method; u* from eq. 4.9; star densities
+// from the shock / isentropic relations; the state at x/t = 0 by sampling the
+// wave fan (sec. 4.5).  Initial guesses: the adaptive PVRS / two-rarefaction /
+// two-shock choice of sec. 9.5.1 ("plain" guess), or a caller-supplied one
+// (the learned guess), which is used only if finite and positive.
+//
+// Stopping rule: each Newton step |f/f'| is compared with tol * p; a step
+// below it is the last one (applied, since f and f' are already at hand, which
+// leaves p* at machine precision) and is not counted: `iters` counts the
+// steps that were needed, so a guess already within tolerance costs none.
+//
+// Plain C++ with EX_HD on every function, so host code of the library can use
+// it too.
+#pragma once
+
+#include <math.h>
+
+#ifdef __CUDACC__
+#define EX_HD __host__ __device__ __forceinline__
+#else
+#define EX_HD inline
+#endif
+
+namespace exact_euler {
+
+struct Gas {
+    double g, g1, g2, g3, g4, g5, g6, g7;  // gamma and Toro's constants G1..G7
+};
+
+EX_HD Gas make_gas(double gamma) {
+    Gas G;
+    G.g = gamma;
+    G.g1 = (gamma - 1.0) / (2.0 * gamma);
+    G.g2 = (gamma + 1.0) / (2.0 * gamma);
+    G.g3 = 2.0 * gamma / (gamma - 1.0);
+    G.g4 = 2.0 / (gamma - 1.0);
+    G.g5 = 2.0 / (gamma + 1.0);
+    G.g6 = (gamma - 1.0) / (gamma + 1.0);
+    G.g7 = (gamma - 1.0) / 2.0;
+    return G;
+}
+
+// f_K and f_K' at pressure p (Toro eqs. 4.6, 4.7, 4.37)
+EX_HD void prefun(const Gas& G, double p, double rk, double pk, double ck, double& f, double& fd) {
+    if (p <= pk) {
+        const double prat = p / pk;
+        const double pw = pow(prat, G.g1);
+        f = G.g4 * ck * (pw - 1.0);
+        fd = pw / (prat * rk * ck);  // (1/(rho c)) * prat^(-g2), with prat^(-g2) = prat^g1 / prat
+    } else {
+        const double ak = G.g5 / rk;
+        const double bk = G.g6 * pk;
+        const double qrt = sqrt(ak / (bk + p));
+        f = (p - pk) * qrt;
+        fd = (1.0 - 0.5 * (p - pk) / (bk + p)) * qrt;
+    }
+}
+
+// Adaptive noniterative guess (Toro sec. 9.5.1): PVRS when the pressure ratio
+// is small and PVRS stays inside [pmin, pmax], else two-rarefaction (TRRS)
+// below pmin or two-shock (TSRS) above.
+EX_HD double guess_pvrs(const Gas& G, double rl, double ul, double pl, double cl, double rr, double ur, double pr,
+                        double cr) {
+    const double cup = 0.25 * (rl + rr) * (cl + cr);
+    double ppv = 0.5 * (pl + pr) + 0.5 * (ul - ur) * cup;
+    ppv = fmax(0.0, ppv);
+    const double pmin = fmin(pl, pr), pmax = fmax(pl, pr);
+    const double qmax = pmax / pmin;
+    if (qmax <= 2.0 && pmin <= ppv && ppv <= pmax) return ppv;
+    if (ppv < pmin) {
+        const double pq = pow(pl / pr, G.g1);
+        const double um = (pq * ul / cl + ur / cr + G.g4 * (pq - 1.0)) / (pq / cl + 1.0 / cr);
+        const double ptl = 1.0 + G.g7 * (ul - um) / cl;
+        const double ptr = 1.0 + G.g7 * (um - ur) / cr;
+        return 0.5 * (pl * pow(ptl, G.g3) + pr * pow(ptr, G.g3));
+    }
+    const double gel = sqrt((G.g5 / rl) / (G.g6 * pl + ppv));
+    const double ger = sqrt((G.g5 / rr) / (G.g6 * pr + ppv));
+    return (gel * pl + ger * pr - (ur - ul)) / (gel + ger);
+}
+
+// true if the data generate vacuum (Toro eq. 4.82)
+EX_HD bool vacuum(const Gas& G, double ul, double cl, double ur, double cr) { return G.g4 * (cl + cr) <= ur - ul; }
+
+// Newton iteration for p*; returns p*, u*; `iters` = updates applied.
+// p0: starting pressure (<= 0 or non-finite: use the adaptive guess).
+EX_HD void star(const Gas& G, double rl, double ul, double pl, double cl, double rr, double ur, double pr, double cr,
+                double p0, double tol, int maxit, double& pstar, double& ustar, int& iters) {
+    iters = 0;
+    if (rl == rr && ul == ur && pl == pr) {
+        pstar = pl;
+        ustar = ul;
+        return;
+    }
+    double p = p0;
+    if (!(p > 0.0) || !(p < 1e300)) p = guess_pvrs(G, rl, ul, pl, cl, rr, ur, pr, cr);
+    if (!(p > tol)) p = tol;
+    const double du = ur - ul;
+    double fl = 0.0, fr = 0.0;
+    for (int k = 0; k <= maxit; ++k) {
+        double fld, frd;
+        prefun(G, p, rl, pl, cl, fl, fld);
+        prefun(G, p, rr, pr, cr, fr, frd);
+        const double step = (fl + fr + du) / (fld + frd);
+        double pn = p - step;
+        if (pn < 0.0) pn = tol;
+        if (fabs(step) <= tol * p || k == maxit) {
+            if (k < maxit) {
+                p = pn;
+                prefun(G, p, rl, pl, cl, fl, fld);
+                prefun(G, p, rr, pr, cr, fr, frd);
+            }
+            break;
+        }
+        p = pn;
+        ++iters;
+    }
+    pstar = p;
+    ustar = 0.5 * (ul + ur + fr - fl);
+}
+
+// Primitive state at x/t = s of the solution with star values (ps, us)
+// (Toro sec. 4.5, SAMPLE).  Also returns the star densities and the two
+// acoustic wave speeds used by the wave-propagation correction (shock speed,
+// or the mean of head and tail speeds of a rarefaction).
+struct Fan {
+    double rsl, rsr;  // rho*_L, rho*_R
+    double s1, s3;    // left / right acoustic wave speeds
+};
+
+EX_HD Fan fan(const Gas& G, double rl, double ul, double pl, double cl, double rr, double ur, double pr, double cr,
+              double ps, double us) {
+    Fan F;
+    if (ps > pl) {
+        const double pml = ps / pl;
+        F.rsl = rl * (pml + G.g6) / (pml * G.g6 + 1.0);
+        F.s1 = ul - cl * sqrt(G.g2 * pml + G.g1);
+    } else {
+        const double pw = pow(ps / pl, 1.0 / G.g);
+        F.rsl = rl * pw;
+        const double cml = cl * pow(ps / pl, G.g1);
+        F.s1 = 0.5 * ((ul - cl) + (us - cml));
+    }
+    if (ps > pr) {
+        const double pmr = ps / pr;
+        F.rsr = rr * (pmr + G.g6) / (pmr * G.g6 + 1.0);
+        F.s3 = ur + cr * sqrt(G.g2 * pmr + G.g1);
+    } else {
+        const double pw = pow(ps / pr, 1.0 / G.g);
+        F.rsr = rr * pw;
+        const double cmr = cr * pow(ps / pr, G.g1);
+        F.s3 = 0.5 * ((ur + cr) + (us + cmr));
+    }
+    return F;
+}
+
+// Sample at x/t = 0: returns (rho, u, p) and whether the point is left of the contact.
+EX_HD void sample0(const Gas& G, double rl, double ul, double pl, double cl, double rr, double ur, double pr, double cr,
+                   double ps, double us, const Fan& F, double& r, double& u, double& p, bool& left) {
+    const double s = 0.0;
+    left = s <= us;
+    if (left) {
+        if (ps <= pl) {
+            const double shl = ul - cl;
+            if (s <= shl) { r = rl; u = ul; p = pl; return; }
+            const double cml = cl * pow(ps / pl, G.g1);
+            const double stl = us - cml;
+            if (s > stl) { r = F.rsl; u = us; p = ps; return; }
+            u = G.g5 * (cl + G.g7 * ul + s);
+            const double c = G.g5 * (cl + G.g7 * (ul - s));
+            r = rl * pow(c / cl, G.g4);
+            p = pl * pow(c / cl, G.g3);
+        } else {
+            const double pml = ps / pl;
+            const double sl = ul - cl * sqrt(G.g2 * pml + G.g1);
+            if (s <= sl) { r = rl; u = ul; p = pl; }
+            else { r = F.rsl; u = us; p = ps; }
+        }
+    } else {
+        if (ps > pr) {
+            const double pmr = ps / pr;
+            const double sr = ur + cr * sqrt(G.g2 * pmr + G.g1);
+            if (s >= sr) { r = rr; u = ur; p = pr; }
+            else { r = F.rsr; u = us; p = ps; }
+        } else {
+            const double shr = ur + cr;
+            if (s >= shr) { r = rr; u = ur; p = pr; return; }
+            const double cmr = cr * pow(ps / pr, G.g1);
+            const double str = us + cmr;
+            if (s <= str) { r = F.rsr; u = us; p = ps; return; }
+            u = G.g5 * (-cr + G.g7 * ur + s);
+            const double c = G.g5 * (cr - G.g7 * (ur - s));
+            r = rr * pow(c / cr, G.g4);
+            p = pr * pow(c / cr, G.g3);
+        }
+    }
+}
+
+// The learned guess's input features and scaling (see pyclaw_b200/learned.py):
+// x = (log rho_L/rb, log rho_R/rb, u_L/cb, u_R/cb, log p_L/pb, log p_R/pb) with
+// rb = sqrt(rho_L rho_R), pb = sqrt(p_L p_R), cb = sqrt(gamma pb / rb); the
+// network predicts y and the guess is p0 * exp(w y), w = J^2/(1+J^2),
+// J^2 = (drho/rb)^2 + (dp/pb)^2 + (du/cb)^2, p0 the adaptive guess.
+EX_HD void features(const Gas& G, double rl, double ul, double pl, double rr, double ur, double pr, float* x,
+                    double& w) {
+    const double rb = sqrt(rl * rr), pb = sqrt(pl * pr);
+    const double cb = sqrt(G.g * pb / rb);
+    const double lr = 0.5 * log(rl / rr), lp = 0.5 * log(pl / pr);
+    x[0] = (float)lr;
+    x[1] = (float)(-lr);
+    x[2] = (float)(ul / cb);
+    x[3] = (float)(ur / cb);
+    x[4] = (float)lp;
+    x[5] = (float)(-lp);
+    const double dr = (rr - rl) / rb, dp = (pr - pl) / pb, du = (ur - ul) / cb;
+    const double j2 = dr * dr + dp * dp + du * du;
+    w = j2 / (1.0 + j2);
+}
+
+}  // namespace exact_euler

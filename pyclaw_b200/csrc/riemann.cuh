@@ -35,6 +35,7 @@
 #pragma once
 
 #include "claw2_types.cuh"
+#include "exact_euler.h"
 
 namespace claw2 {
 
@@ -436,6 +437,187 @@ struct RPShallowRoe {
         bp[MU] = u * (p1 + p3) + p2;
         bp[MV] = v * (p1 + p3) + a * (p3 - p1);
     }
+};
+
+
+// ---------------------------------------------------------------------------
+// Exact Euler solver (no counterpart in the reference): cparam = {gamma, tol}.
+// rpn2: p* by Newton (exact_euler.h) from the adaptive PVRS guess or from a
+// per-interface guess (the learned one, computed by k_mlp_guess); three waves
+// W1 = Q*L - QL, W2 = Q*R - Q*L (contact and shear), W3 = QR - Q*R with the
+// shock speed or the fan's mean speed, and the Godunov fluctuations
+// A-dq = F(Q(0)) - F(QL), A+dq = F(QR) - F(Q(0)) from the state at x/t = 0, so
+// no entropy fix is needed.  rpt2: the Roe transverse split at the Roe state.
+// Data that generate vacuum fall back to the Roe solver for that interface.
+// ---------------------------------------------------------------------------
+struct RPEulerExact {
+    static constexpr int MEQN = 4, MWAVES = 3, NC = 10, ID = CLAW2_RP_EULER_EXACT;
+    static constexpr bool USES_GUESS = true, COUNTS = true;
+    enum { RS = 4, UX = 5, UY = 6, HH = 7, CS = 8, PP = 9 };
+    struct Iface {
+        double w[3][4];
+        double s[3];
+        double u, v, a, ia, H;  // Roe state for rpt2
+        int iters;
+    };
+
+    __device__ __forceinline__ static void prepare(const double (&q)[MEQN], const RPParams& p, double (&c)[NC]) {
+        const double gamma = p.c[0], gamma1 = gamma - 1.0;
+        const double irho = 1.0 / q[0];
+        const double u = q[1] * irho, v = q[2] * irho;
+        const double pr = gamma1 * (q[3] - 0.5 * (q[1] * u + q[2] * v));
+        c[0] = q[0]; c[1] = q[1]; c[2] = q[2]; c[3] = q[3];
+        c[RS] = sqrt(q[0]);
+        c[UX] = u;
+        c[UY] = v;
+        c[HH] = (q[3] + pr) * irho;
+        c[CS] = sqrt(gamma * pr * irho);
+        c[PP] = pr;
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void speeds(const Iface& f, const RPParams&, double (&s)[MWAVES]) {
+        s[0] = f.s[0]; s[1] = f.s[1]; s[2] = f.s[2];
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void waves(const Iface& f, const RPParams&, double (&w)[MWAVES][MEQN]) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int m = 0; m < 4; ++m) w[k][m] = f.w[k][m];
+    }
+    // normal flux of a primitive state (rho, un, ut, p) in components (0, MU, MV, 3)
+    template <int IXY>
+    __device__ __forceinline__ static void flux(double r, double un, double ut, double pr, double g1inv,
+                                                double (&F)[MEQN]) {
+        constexpr int MU = Dir<IXY>::MU, MV = Dir<IXY>::MV;
+        const double E = pr * g1inv + 0.5 * r * (un * un + ut * ut);
+        F[0] = r * un;
+        F[MU] = r * un * un + pr;
+        F[MV] = r * un * ut;
+        F[3] = un * (E + pr);
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void cons(double r, double un, double ut, double pr, double g1inv,
+                                                double (&Q)[MEQN]) {
+        constexpr int MU = Dir<IXY>::MU, MV = Dir<IXY>::MV;
+        Q[0] = r;
+        Q[MU] = r * un;
+        Q[MV] = r * ut;
+        Q[3] = pr * g1inv + 0.5 * r * (un * un + ut * ut);
+    }
+
+    template <int IXY>
+    __device__ __forceinline__ static void solve_g(const double (&cL)[NC], const double (&cR)[NC], const RPParams& p,
+                                                   double guess, Iface& f, double (&amdq)[MEQN],
+                                                   double (&apdq)[MEQN]) {
+        constexpr int MU = Dir<IXY>::MU, MV = Dir<IXY>::MV;
+        constexpr int UN = (IXY == 1) ? UX : UY, UT = (IXY == 1) ? UY : UX;
+        const double gamma = p.c[0], gamma1 = gamma - 1.0, g1inv = 1.0 / gamma1;
+        const double tol = p.c[1];
+        // Roe state for the transverse solver
+        {
+            const double inv = 1.0 / (cL[RS] + cR[RS]);
+            const double wl = cL[RS] * inv, wr = cR[RS] * inv;
+            f.u = wl * cL[UN] + wr * cR[UN];
+            f.v = wl * cL[UT] + wr * cR[UT];
+            f.H = wl * cL[HH] + wr * cR[HH];
+            const double a2 = gamma1 * (f.H - 0.5 * (f.u * f.u + f.v * f.v));
+            f.ia = rsqrt(a2);
+            f.a = a2 * f.ia;
+        }
+        const exact_euler::Gas G = exact_euler::make_gas(gamma);
+        const double rl = cL[0], ul = cL[UN], vl = cL[UT], pl = cL[PP], cl = cL[CS];
+        const double rr = cR[0], ur = cR[UN], vr = cR[UT], pr = cR[PP], cr = cR[CS];
+        if (exact_euler::vacuum(G, ul, cl, ur, cr)) {
+            // vacuum: the Roe solution for this interface
+            RPEulerRoe::Iface fr;
+            double cl9[9], cr9[9];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) { cl9[k] = cL[k]; cr9[k] = cR[k]; }
+            RPParams pp = p;
+            pp.flags = 1;
+            RPEulerRoe::template solve<IXY>(cl9, cr9, pp, fr, amdq, apdq);
+            double w4[4][4];
+            RPEulerRoe::template waves<IXY>(fr, pp, w4);
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                f.w[0][m] = w4[0][m];
+                f.w[1][m] = w4[1][m] + w4[2][m];
+                f.w[2][m] = w4[3][m];
+            }
+            f.s[0] = fr.u - fr.a; f.s[1] = fr.u; f.s[2] = fr.u + fr.a;
+            f.iters = 0;
+            return;
+        }
+        double ps, us;
+        int it;
+        exact_euler::star(G, rl, ul, pl, cl, rr, ur, pr, cr, guess, tol, 50, ps, us, it);
+        f.iters = it;
+        const exact_euler::Fan F = exact_euler::fan(G, rl, ul, pl, cl, rr, ur, pr, cr, ps, us);
+        double QL[MEQN], QR[MEQN], QsL[MEQN], QsR[MEQN];
+#pragma unroll
+        for (int m = 0; m < MEQN; ++m) { QL[m] = cL[m]; QR[m] = cR[m]; }
+        cons<IXY>(F.rsl, us, vl, ps, g1inv, QsL);
+        cons<IXY>(F.rsr, us, vr, ps, g1inv, QsR);
+#pragma unroll
+        for (int m = 0; m < MEQN; ++m) {
+            f.w[0][m] = QsL[m] - QL[m];
+            f.w[1][m] = QsR[m] - QsL[m];
+            f.w[2][m] = QR[m] - QsR[m];
+        }
+        f.s[0] = F.s1;
+        f.s[1] = us;
+        f.s[2] = F.s3;
+        double r0, u0, p0;
+        bool left;
+        exact_euler::sample0(G, rl, ul, pl, cl, rr, ur, pr, cr, ps, us, F, r0, u0, p0, left);
+        double F0[MEQN], FL[MEQN], FR[MEQN];
+        flux<IXY>(r0, u0, left ? vl : vr, p0, g1inv, F0);
+        flux<IXY>(rl, ul, vl, pl, g1inv, FL);
+        flux<IXY>(rr, ur, vr, pr, g1inv, FR);
+#pragma unroll
+        for (int m = 0; m < MEQN; ++m) {
+            amdq[m] = F0[m] - FL[m];
+            apdq[m] = FR[m] - F0[m];
+        }
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void solve(const double (&cL)[NC], const double (&cR)[NC], const RPParams& p,
+                                                 Iface& f, double (&amdq)[MEQN], double (&apdq)[MEQN]) {
+        solve_g<IXY>(cL, cR, p, 0.0, f, amdq, apdq);
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void rpt2(const Iface& f, const RPParams& p, const double (&asdq)[MEQN],
+                                                double (&bm)[MEQN], double (&bp)[MEQN]) {
+        RPEulerRoe::Iface r;
+        r.u = f.u; r.v = f.v; r.a = f.a; r.ia = f.ia; r.H = f.H;
+        RPEulerRoe::template rpt2<IXY>(r, p, asdq, bm, bp);
+    }
+    __device__ __forceinline__ static int count(const Iface& f) { return f.iters; }
+};
+
+// Traits for the optional per-interface guess and iteration count.
+template <class RP, class = void>
+struct GuessTraits {
+    static constexpr bool USES = false;
+    template <int IXY>
+    __device__ __forceinline__ static void solve(const double (&cL)[RP::NC], const double (&cR)[RP::NC],
+                                                 const RPParams& p, double, typename RP::Iface& f,
+                                                 double (&am)[RP::MEQN], double (&ap)[RP::MEQN]) {
+        RP::template solve<IXY>(cL, cR, p, f, am, ap);
+    }
+    __device__ __forceinline__ static int count(const typename RP::Iface&) { return 0; }
+};
+template <class RP>
+struct GuessTraits<RP, decltype((void)RP::USES_GUESS, void())> {
+    static constexpr bool USES = RP::USES_GUESS;
+    template <int IXY>
+    __device__ __forceinline__ static void solve(const double (&cL)[RP::NC], const double (&cR)[RP::NC],
+                                                 const RPParams& p, double g, typename RP::Iface& f,
+                                                 double (&am)[RP::MEQN], double (&ap)[RP::MEQN]) {
+        RP::template solve_g<IXY>(cL, cR, p, g, f, am, ap);
+    }
+    __device__ __forceinline__ static int count(const typename RP::Iface& f) { return RP::count(f); }
 };
 
 }  // namespace claw2

@@ -39,6 +39,8 @@ struct StepArgs {
     Method meth;
     unsigned long long* cfl_bits;  // atomicMax of non-negative double bit patterns
     int* status;                   // bit 0: non-finite output
+    const double* guess;           // optional per-interface p* guesses: x plane, then y plane
+    unsigned long long* counters;  // optional: [0] Newton iterations, [1] Riemann solves
 };
 
 // philim.f90:16-35
@@ -66,6 +68,19 @@ __device__ __forceinline__ void cfl_commit(double cfl, double* s_red, unsigned l
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, s_red[w]);
         // non-negative doubles order like their bit patterns
         atomicMax(slot, (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+// Warp-sum two counters and add them once per warp.
+__device__ __forceinline__ void counter_commit(unsigned long long* c, unsigned long long a, unsigned long long b) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+    }
+    if ((threadIdx.x & 31) == 0 && c) {
+        atomicAdd(c, a);
+        atomicAdd(c + 1, b);
     }
 }
 
@@ -168,6 +183,7 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
     double accA[ME], accB[ME], accC[ME], accD[ME];  // rows R-2, R-1, R, R+1
     Iface fY;                                       // y-interface (R-2 | R-1)
     double amY[ME], apY[ME], dY[MW];
+    unsigned long long n_it = 0, n_solve = 0;
 #pragma unroll
     for (int m = 0; m < ME; ++m) {
         pf[m] = __ldg(qo + m * plane + (long long)R0 * pitch);
@@ -209,7 +225,13 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
             }
             Iface fN;
             double amN[ME], apN[ME];
-            RP::template solve<2>(cB, cA, P, fN, amN, apN);
+            double gy = 0.0;
+            if (GuessTraits<RP>::USES && a.guess) gy = a.guess[plane + (long long)R * pitch + cpl];
+            GuessTraits<RP>::template solve<2>(cB, cA, P, gy, fN, amN, apN);
+            if (GuessTraits<RP>::USES && cp <= mx + 3) {
+                n_it += GuessTraits<RP>::count(fN);
+                n_solve += 1;
+            }
             double dn[MW];
             {
                 double wY[MW][ME], wN[MW][ME];
@@ -279,7 +301,13 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
                 cL[k] = S.cell[s2][k][tl];
                 cR[k] = S.cell[s2][k][t];
             }
-            RP::template solve<1>(cL, cR, P, fX, amX, apX);
+            double gx = 0.0;
+            if (GuessTraits<RP>::USES && a.guess) gx = a.guess[(long long)R * pitch + cpl];
+            GuessTraits<RP>::template solve<1>(cL, cR, P, gx, fX, amX, apX);
+            if (GuessTraits<RP>::USES && cp <= mx + 3 && t > 0) {
+                n_it += GuessTraits<RP>::count(fX);
+                n_solve += 1;
+            }
             double wX[MW][ME];
             RP::template waves<1>(fX, P, wX);
 #pragma unroll
@@ -382,6 +410,7 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
         s1 = s2;
         s2 = tmp;
     }
+    if (GuessTraits<RP>::USES && a.counters) counter_commit(a.counters, n_it, n_solve);
 }
 
 template <class RP, int NT, int MINB>

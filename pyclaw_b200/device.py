@@ -25,6 +25,7 @@ class DevicePatch(object):
         self.device_newer = False   # device q is ahead of the host copy
         self.host_dirty = True      # host q must be uploaded before the next step
         self._cfl = ctypes.c_double(0.0)
+        self.mlp = None
 
     def close(self):
         if getattr(self, "h", None) is not None and self.h.value:

@@ -15,7 +15,7 @@ from . import _lib
 
 
 class RiemannSolver(object):
-    def __init__(self, name, rp_id, num_eqn, num_waves, cparam, fwave=False, efix=None):
+    def __init__(self, name, rp_id, num_eqn, num_waves, cparam, fwave=False, efix=None, extra=()):
         self.__name__ = 'clawpack.riemann.' + name
         self.name = name
         self.rp_id = rp_id
@@ -24,6 +24,7 @@ class RiemannSolver(object):
         self.cparam_names = tuple(cparam)
         self.fwave = fwave
         self.efix = efix  # entropy fix switch (a compile-time constant in Fortran)
+        self.extra = tuple(extra)  # (problem_data key, default) pairs appended to cparam
 
     def cparam(self, problem_data):
         """Parameter vector for the C ABI from ``problem_data``."""
@@ -34,6 +35,8 @@ class RiemannSolver(object):
         vals = [float(problem_data[k]) for k in self.cparam_names]
         if self.efix is not None:
             vals.append(1.0 if problem_data.get('efix', self.efix) else 0.0)
+        for key, default in self.extra:
+            vals.append(float(problem_data.get(key, default)))
         return vals
 
     def __repr__(self):
@@ -46,7 +49,12 @@ euler_4wave_2D = RiemannSolver('euler_4wave_2D', _lib.RP_EULER_ROE, 4, 4, ('gamm
 shallow_roe_with_efix_2D = RiemannSolver('shallow_roe_with_efix_2D', _lib.RP_SHALLOW_ROE, 3, 3,
                                          ('grav',), efix=True)
 
-_ALL = [advection_2D, acoustics_2D, euler_4wave_2D, shallow_roe_with_efix_2D]
+# Exact Euler solver (no counterpart in clawpack/riemann): Newton for p* to
+# relative tolerance `exact_tol`; three waves (1-wave, contact+shear, 3-wave).
+euler_exact_2D = RiemannSolver('euler_exact_2D', _lib.RP_EULER_EXACT, 4, 3, ('gamma',),
+                               extra=(('exact_tol', 1e-12),))
+
+_ALL = [advection_2D, acoustics_2D, euler_4wave_2D, shallow_roe_with_efix_2D, euler_exact_2D]
 
 static = types.SimpleNamespace(
     num_eqn={s.name: s.num_eqn for s in _ALL},
@@ -55,6 +63,7 @@ static = types.SimpleNamespace(
 )
 
 # component-index constants modules (clawpack.riemann.<name>_constants)
+euler_exact_2D_constants = types.SimpleNamespace(density=0, x_momentum=1, y_momentum=2, energy=3, num_eqn=4)
 euler_4wave_2D_constants = types.SimpleNamespace(density=0, x_momentum=1, y_momentum=2, energy=3,
                                                  num_eqn=4)
 shallow_roe_with_efix_2D_constants = types.SimpleNamespace(depth=0, x_momentum=1, y_momentum=2,

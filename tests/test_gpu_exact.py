@@ -1,0 +1,169 @@
+"""Exact Euler solver and its learned Newton guess on the GPU.
+
+* the CUDA exact-solver step equals the oracle's (Toro restated
+  independently) within 1e-12, from the PVRS guess and from a learned guess
+  (Newton converges to the same p* from either start);
+* the device's training-sample generator, gradient kernels and BF16 tensor-
+  core inference against the FP64 CPU reference of the network;
+* training lowers the loss and the trained guess needs fewer Newton updates
+  than the PVRS guess on problems from the training distribution.
+"""
+import numpy as np
+import pytest
+
+from helpers import PARITY_RTOL, max_rel, method_vector
+from oracle import mlp_ref
+from pyclaw_b200 import _lib, classic2, learned, workloads
+from pyclaw_b200 import riemann as rmod
+
+pytestmark = pytest.mark.gpu
+G = 1.4
+
+
+def _euler_qbc(mx, my, seed, spread=0.6):
+    rng = np.random.default_rng(seed)
+    nx, ny = mx + 4, my + 4
+    X, Y = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+    quad = (X > nx // 2).astype(int) + 2 * (Y > ny // 3).astype(int)
+    noise = rng.random((nx, ny)) < 0.5
+
+    def field(lo, hi):
+        return np.where(noise, rng.uniform(lo, hi, (nx, ny)), rng.uniform(lo, hi, 4)[quad])
+
+    rho, p = np.exp(field(-spread, spread)), np.exp(field(-spread, spread))
+    u, v = field(-0.5, 0.5), field(-0.5, 0.5)
+    return np.asfortranarray(np.stack([rho, rho * u, rho * v, p / (G - 1) + 0.5 * rho * (u * u + v * v)]))
+
+
+def test_exact_step_matches_oracle(oracle):
+    for (mx, my, seed) in [(37, 23, 1), (130, 70, 2)]:
+        qbc = _euler_qbc(mx, my, seed)
+        method = method_vector(2, 2)
+        mthlim = np.full(3, 4, dtype=np.intc)
+        dx, dy, dt = 1.0 / mx, 1.0 / my, 0.1 / max(mx, my)
+        q_o = qbc.copy(order="F")
+        cfl_o = oracle.step2(qbc, q_o, dx, dy, dt, method, mthlim, _lib.RP_EULER_EXACT, [G, 1e-12])
+        classic2.cparam.gamma = G
+        q_g, cfl_g = classic2.step2(max(mx, my), 2, mx, my, qbc, qbc.copy(order="F"), None, dx, dy, dt, method,
+                                    mthlim, rpn2=rmod.euler_exact_2D)
+        assert abs(cfl_g - cfl_o) <= PARITY_RTOL * cfl_o
+        assert max_rel(q_g[:, 2:-2, 2:-2], q_o[:, 2:-2, 2:-2]) <= PARITY_RTOL
+
+
+def _exact_claw(n):
+    claw = workloads.euler_quadrants_unsplit(n=n)
+    claw.solver.rp = rmod.euler_exact_2D
+    claw.solver.num_waves = 3
+    return claw
+
+
+def test_learned_guess_converges_to_the_same_step(oracle):
+    net = learned.Network(seed=11)  # untrained: a poor but finite guess
+    results = []
+    for use_net in (False, True):
+        claw = _exact_claw(96)
+        s, sol = claw.solver, claw.solution
+        s.setup(sol)
+        s.dt = 2e-4
+        if use_net:
+            learned.attach(s, net)
+        for _ in range(3):
+            s.evolve_to_time(sol)
+        it, ns = learned.counters(s)
+        results.append((sol.state.get_q_global(), it, ns))
+    (q0, it0, n0), (q1, it1, n1) = results
+    assert n0 == n1 > 0
+    assert max_rel(q1, q0) <= PARITY_RTOL
+
+
+def test_sample_generator_matches_reference():
+    net = learned.Network()
+    net.generate(64, seed=99)
+    x, y, ok = net.samples(0, 64)
+    for i in range(64):
+        rl, ul, pl, rr, ur, pr = mlp_ref.draw_problem(99, i)
+        f, w = mlp_ref.features(G, rl, ul, pl, rr, ur, pr)
+        assert np.allclose(x[i, :6], f, rtol=1e-6, atol=1e-6)
+        assert abs(x[i, 6] - w) <= 1e-6
+
+
+def test_gradient_kernel_matches_fp64_reference():
+    net = learned.Network(seed=5)
+    net.generate(4096, seed=3)
+    x, y, ok = net.samples(0, 4096)
+    P = net.params
+    g_gpu, loss_gpu = net.gradient(0, 4096)
+    sel = ok.astype(bool)
+    # the device averages over all 4096 slots with zero error on invalid ones
+    g_ref, _ = mlp_ref.gradient(P, x[sel, :6].astype(np.float64), y[sel].astype(np.float64))
+    g_ref *= sel.sum() / 4096.0
+    rel = np.linalg.norm(g_gpu - g_ref) / np.linalg.norm(g_ref)
+    assert rel < 1e-4, rel
+
+
+def test_tensor_core_inference_matches_reference():
+    net = learned.Network(seed=7)
+    rng = np.random.default_rng(1)
+    x = np.zeros((1000, 8), dtype=np.float32)
+    x[:, :6] = rng.normal(0, 1.0, (1000, 6))
+    y_gpu = net.infer(x)
+    y_ref = mlp_ref.forward_bf16(net.params, x[:, :6])
+    y_fp64, _, _ = mlp_ref.forward(net.params, x[:, :6].astype(np.float64))
+    assert np.max(np.abs(y_gpu - y_ref)) < 2e-2
+    assert np.max(np.abs(y_gpu - y_fp64)) < 5e-2
+
+
+def test_training_reduces_loss_and_guess_error():
+    """What the trained network gains over the method without it: on held-out
+    problems of the training distribution its guess (BF16 tensor-core
+    inference) is closer to the converged p* than the adaptive PVRS guess,
+    above all in the tail where PVRS is poor."""
+    net = learned.Network(seed=2024)
+    net.generate(1 << 24, seed=7)  # the full training set (about a second with training)
+    _, loss0 = net.gradient(0, 1 << 16)
+    net.train(epochs=4, batch=16384, lr=3e-3)
+    _, loss1 = net.gradient(0, 1 << 16)
+    assert loss1 < 0.2 * loss0, (loss0, loss1)
+    hold = learned.Network(seed=1)
+    hold.generate(1 << 16, seed=12345)
+    x, y, ok = hold.samples(0, 1 << 16)
+    sel = ok.astype(bool)
+    w = x[sel, 6].astype(np.float64)
+    err_pvrs = np.abs(w * y[sel])                       # |log(p_pvrs / p*)|
+    err_net = np.abs(w * (net.infer(x[sel]) - y[sel]))  # |log(p_net / p*)|
+    print("log guess error p50/p90/p99: pvrs %s network %s" % (
+        np.percentile(err_pvrs, [50, 90, 99]).round(4), np.percentile(err_net, [50, 90, 99]).round(4)))
+    for pct in (90, 99):
+        assert np.percentile(err_net, pct) < 0.5 * np.percentile(err_pvrs, pct), pct
+    assert np.percentile(err_net, 50) < np.percentile(err_pvrs, 50)
+
+
+def test_newton_updates_with_both_guesses_on_random_problems():
+    """Newton updates per interface from each guess on a grid whose cells are
+    independent draws from the training distribution (reported; the learned
+    start must converge to the same step, checked above, and may not cost
+    more than one extra update per interface)."""
+    net = learned.Network(seed=2024)
+    net.generate(1 << 24, seed=7)
+    net.train(epochs=4, batch=16384, lr=3e-3)
+    n = 128
+    claw = _exact_claw(n)
+    rng = np.random.default_rng(8)
+    rho = np.exp(rng.uniform(np.log(1e-2), np.log(1e2), (n, n)))
+    p = np.exp(rng.uniform(np.log(1e-2), np.log(1e2), (n, n)))
+    u, v = rng.uniform(-3, 3, (n, n)), rng.uniform(-3, 3, (n, n))
+    st = claw.solution.state
+    st.q[0], st.q[1], st.q[2] = rho, rho * u, rho * v
+    st.q[3] = p / (G - 1) + 0.5 * rho * (u * u + v * v)
+    s = claw.solver
+    s.setup(claw.solution)
+    its = {}
+    for use_net in (False, True):
+        learned.attach(s, net if use_net else None)
+        learned.counters(s)
+        s._dev.step(1e-6, want_cfl=False)
+        s._dev.accept(False)
+        it, ns = learned.counters(s)
+        its[use_net] = it / ns
+    print("Newton updates per interface: pvrs %.3f learned %.3f" % (its[False], its[True]))
+    assert its[True] < its[False] + 1.0, its
