@@ -139,3 +139,32 @@ def test_reject_and_retake_on_device():
     assert claw.solution.t == 0.0
     claw.solver.evolve_to_time(claw.solution)
     assert claw.solver.accept_step and claw.solution.t > 0.0
+
+
+def _sums(claw):
+    q = claw.solution.state.get_q_global()
+    return q.sum(axis=(1, 2)), np.abs(q).sum(axis=(1, 2))
+
+
+def test_euler_periodic_run_conserves_every_component():
+    # the quadrant problem on a periodic domain: mass, both momenta and energy
+    # stay at their initial sums to roundoff over a whole run
+    from pyclaw_b200 import BC
+    claw = workloads.euler_quadrants_unsplit(n=256, tfinal=0.3)
+    for d in (0, 1):
+        claw.solver.bc_lower[d] = BC.periodic
+        claw.solver.bc_upper[d] = BC.periodic
+    s0, scale = _sums(claw)
+    claw.run()
+    assert claw.solver.status['numsteps'] > 50
+    q1 = claw.frames[-1].q
+    assert np.all(np.abs(q1.sum(axis=(1, 2)) - s0) <= 1e-13 * scale)
+
+
+def test_shallow_dam_break_conserves_mass():
+    # the front stays inside the domain, so the extrapolation boundaries carry no flux
+    claw = workloads.shallow_dam_break_unsplit(n=256, tfinal=0.5)
+    s0, scale = _sums(claw)
+    claw.run()
+    h1 = claw.frames[-1].q[0].sum()
+    assert abs(h1 - s0[0]) <= 1e-13 * scale[0]
