@@ -55,6 +55,15 @@ def parse():
     ap.add_argument("--shape", default=None, help="fixed launch shape 'variant,rows' (skips the autotuner)")
     ap.add_argument("--pre-t", type=float, default=0.4,
                     help="advance the problem to this time (untimed) before warm-up")
+    ap.add_argument("--only", default=None, choices=["shallow_4096", "acoustics_200", "batched_512", "learned_2048"],
+                    help="profiling aid: run one of the other workloads alone (with --shape: no autotuning) "
+                         "and print its JSON")
+    ap.add_argument("--train-problems", type=int, default=1 << 24,
+                    help="training-set size of the learned guess (2^24 in the benchmark)")
+    ap.add_argument("--epochs", type=int, default=16, help="training epochs of the learned guess")
+    ap.add_argument("--state", default=None,
+                    help="profiling aid: .npy file of the advanced state; loaded if it exists (no "
+                         "advance), else written after the advance")
     return ap.parse_args()
 
 
@@ -201,10 +210,11 @@ def time_patch(patch, dt, steps, flush, stream):
     return statistics.mean(a.elapsed_time(b) for a, b in ev), statistics.mean(kern)
 
 
-def batched_workload(n_instances=512, steps=100):
+def batched_workload(n_instances=512, steps=100, plain=True):
     """The batched form: n independent Euler quadrant problems of uneven size
     (side 64..512), 100 steps with per-problem dt; aggregate cell-updates/s of
-    the graph-captured persistent form and of the plain per-problem loop."""
+    the graph-captured persistent form and (plain=True) of the plain
+    per-problem loop."""
     import numpy as np
     from pyclaw_b200 import batch as pb, workloads
     claws, sides = workloads.batched_quadrants(n_instances)
@@ -213,8 +223,14 @@ def batched_workload(n_instances=512, steps=100):
     rows, trials, choice = pb.autotune_rows(bat, sides)
     cells = sides.astype(np.float64) ** 2
     out = {"instances": n_instances, "cells_total": float(cells.sum()), "steps": steps,
-           "rows_per_bucket": [int(c) for c in choice], "bucket_edges": [128, 256]}
-    for mode, name in ((0, "graph_persistent"), (2, "plain_per_instance_loop")):
+           "rows_per_bucket": [int(c) for c in choice], "bucket_edges": [128, 256],
+           "plain_loop_rows": "single-problem heuristic (0)"}
+    for mode, name in ((0, "graph_persistent"), (2, "plain_per_instance_loop"))[:2 if plain else 1]:
+        if mode == 2:
+            # the plain loop launches each problem alone: give every launch the
+            # single-problem heuristic shape (most CTAs per launch), not the
+            # row heights tuned for the persistent kernel
+            bat.set_rows(np.zeros(n_instances, dtype=np.intc))
         bat.upload()
         bat.set_time(dt0, 0.0, 1e99)
         bat.run(1, mode=mode)  # warm (captures the graph for 1 step)
@@ -226,7 +242,8 @@ def batched_workload(n_instances=512, steps=100):
         out[name] = {"ms": ms, "value": upd / (ms * 1e-3), "unit": UNIT,
                      "accepted_steps": int(st["nsteps"].sum()), "rejected_steps": int(st["nreject"].sum()),
                      "failed_instances": int(st["failed"].sum())}
-    out["speedup"] = out["graph_persistent"]["value"] / out["plain_per_instance_loop"]["value"]
+    if plain:
+        out["speedup"] = out["graph_persistent"]["value"] / out["plain_per_instance_loop"]["value"]
     ntiles, grid = bat.tiles()
     out["tiles"], out["persistent_grid"] = ntiles, grid
     bat.close()
@@ -298,13 +315,17 @@ def learned_workload(stream, flush, n=2048, steps=10, n_train=1 << 24, epochs=16
     return out
 
 
-def secondary_workloads(stream, flush, peaks, steps=20):
-    """The shallow-water dam break at 4096^2 (48 B/cell) and the walled
-    acoustics problem at 200^2, unsplit trans_cor, MC, CFL 0.9."""
+def secondary_workloads(stream, flush, peaks, only=None, shape=None):
+    """The shallow-water dam break at 4096^2, 200 steps at CFL 0.9 from its
+    initial state, and the walled acoustics problem at 200^2 run to t = 0.6
+    at CFL 0.9 (48 B/cell each), unsplit trans_cor, MC."""
+    import math
     from pyclaw_b200 import tune, workloads
     out = {}
     for name, make, bpc in [("shallow_roe_dam_break_4096", lambda: workloads.shallow_dam_break_unsplit(n=4096), 48),
                             ("acoustics_wall_200", lambda: workloads.acoustics_wall(n=200), 48)]:
+        if only is not None and name != only:
+            continue
         claw = make()
         s, sol = claw.solver, claw.solution
         s.setup(sol)
@@ -314,21 +335,50 @@ def secondary_workloads(stream, flush, peaks, steps=20):
         cfl = p.step(dt)
         p.accept(False)
         dt = dt * 0.9 / cfl
-        shape, _ = tune.autotune(p, dt)
+        if shape is not None:
+            use = tuple(shape)
+            tune.set_shape(p.desc.riemann, *use)
+        else:
+            use, _ = tune.autotune(p, dt)
+        steps = 200 if name.startswith("shallow") else int(math.ceil(0.6 / dt))
         step_ms, kern_ms = time_patch(p, dt, steps, flush, stream)
         n = sol.state.grid.num_cells[0] * sol.state.grid.num_cells[1]
         gbs = n * bpc / (kern_ms * 1e-3) / 1e9
         out[name] = {"value": n / (step_ms * 1e-3), "unit": UNIT, "ms_per_step": step_ms, "kernel_ms": kern_ms,
                      "bytes_per_cell": bpc, "achieved_gbs": gbs, "hbm_frac": gbs / peaks["hbm_gbs"],
-                     "launch_shape": list(shape), "steps": steps}
+                     "launch_shape": list(use), "steps": steps}
         p.close()
     return out
+
+def run_one(args):
+    """One of the other workloads alone (profiling aid)."""
+    import torch
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream(torch.device("cuda", 0))
+    torch.cuda.set_stream(stream)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    shape = tuple(int(x) for x in args.shape.split(",")) if args.shape else None
+    if args.only == "shallow_4096":
+        out = secondary_workloads(stream, flush, measured_peaks()[0], "shallow_roe_dam_break_4096", shape)
+    elif args.only == "acoustics_200":
+        out = secondary_workloads(stream, flush, measured_peaks()[0], "acoustics_wall_200", shape)
+    elif args.only == "batched_512":
+        out = {"batched_quadrants_512": batched_workload(plain=False)}
+    else:
+        out = {"learned_exact_euler_2048": learned_workload(stream, flush, n_train=args.train_problems,
+                                                            epochs=args.epochs, pre_t=args.pre_t)}
+    torch.cuda.synchronize()
+    print(json.dumps(out), flush=True)
+    return 0
+
 
 def run_ours(args):
     import torch
     import torch.distributed as dist
     from pyclaw_b200 import _lib, workloads
 
+    if args.only:
+        return run_one(args)
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
     if world > 1:
@@ -351,6 +401,11 @@ def run_ours(args):
     # advance (untimed) to the middle of the run so the timed steps see a
     # developed flow, with the reference's dt rule (cfl_desired 0.9)
     t, dt, cfl = 0.0, 2.5e-4, None
+    if args.state and os.path.exists(args.state):
+        q = np.asfortranarray(np.load(args.state))
+        _lib.check(_lib.load().claw2_patch_upload_q(patch.h, _lib.dptr(q)))
+        patch.host_dirty, patch.device_newer = False, True
+        t = args.pre_t
     while t < args.pre_t:
         dt = min(dt, args.pre_t - t) if cfl is None else min(dt * 0.9 / cfl, args.pre_t - t)
         cfl = patch.step(dt)
@@ -358,6 +413,10 @@ def run_ours(args):
         patch.accept(ok)
         if ok:
             t += dt
+    if args.state and not os.path.exists(args.state):
+        q = np.empty((MEQN, n, n), order="F")
+        _lib.check(_lib.load().claw2_patch_download_q(patch.h, _lib.dptr(q)))
+        np.save(args.state, q)
     # fixed dt for CFL 0.9 from a probe step
     cfl = patch.step(dt)
     patch.accept(False)
@@ -445,7 +504,8 @@ def run_ours(args):
         secondary = secondary_workloads(stream, flush, peaks)
         secondary["batched_quadrants_512"] = batched_workload()
         if args.learned:
-            secondary["learned_exact_euler_2048"] = learned_workload(stream, flush)
+            secondary["learned_exact_euler_2048"] = learned_workload(stream, flush, n_train=args.train_problems,
+                                                                     epochs=args.epochs)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and n == N:

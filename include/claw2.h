@@ -164,6 +164,13 @@ int claw2_tune_get(int riemann, int* variant, int* rows);
  * roofline denominator for the FP64-bound Riemann solvers. */
 int claw2_probe_fp64(int device, double* tflops);
 
+/* Self-test of the reciprocal the step kernels use in place of IEEE division
+ * (no counterpart in the reference; Newton-Raphson refinement of the hardware
+ * approximation): over n seeded values a = +-(1+u)*2^e, e uniform in
+ * [-1000, 1000], *max_ulp = the largest distance in units in the last place
+ * between it and CUDA's IEEE quotient 1.0/a. */
+int claw2_selftest_rcp(int device, int n, unsigned long long seed, double* max_ulp);
+
 /* ---- no counterpart in the reference ------------------------------------
  * The split step (x-sweep then y-sweep, as claw2_step2ds with ids = 1 then 2)
  * for callers that cannot allocate device memory: frameworks that reserve the

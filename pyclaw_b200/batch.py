@@ -121,3 +121,20 @@ def autotune_rows(batch, sides, candidates=(8, 12, 16, 24, 32, 48, 64), steps=2,
     rows = np.array([choice[x] for x in b], dtype=np.intc)
     batch.set_rows(rows)
     return rows, trials, choice
+
+
+def partition_instances(cells, world):
+    """Split a batch over `world` ranks, balanced by cell count: instances in
+    decreasing size, each to the rank with the fewest cells so far (greedy
+    longest-processing-time order).  Instances are independent, so the ranks
+    need no exchange; each builds a Batch of its own list.  Returns one sorted
+    index list per rank; deterministic for equal inputs on every rank."""
+    cells = np.asarray(cells, dtype=np.int64)
+    order = sorted(range(len(cells)), key=lambda i: (-int(cells[i]), i))
+    load = [0] * world
+    parts = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        parts[r].append(i)
+        load[r] += int(cells[i])
+    return [sorted(p) for p in parts]

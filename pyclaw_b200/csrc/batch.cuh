@@ -85,7 +85,7 @@ static __global__ void k_batch_bc(const BatchArgs b, int first, int bcl0, int bc
     }
 }
 
-template <class RP, int NT, int MINB>
+template <class RP, int NT, int MINB, int SPEC>
 __global__ void __launch_bounds__(NT, MINB) k_batch_step(const BatchArgs b, int first, int count) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     UnsplitSmem<RP, NT>& S = *reinterpret_cast<UnsplitSmem<RP, NT>*>(smem_raw);
@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(NT, MINB) k_batch_step(const BatchArgs b, int 
         a.counters = nullptr;
         const int strip = tl.y % in.nstrips, rblk = tl.y / in.nstrips;
         double cfl = 0.0;
-        unsplit_tile<RP, NT>(a, strip, rblk * in.H, S, cfl);
+        unsplit_tile<RP, NT, SPEC>(a, strip, rblk * in.H, S, cfl);
         cfl_commit(cfl, S.red, a.cfl_bits);
     }
 }

@@ -118,24 +118,52 @@ struct UnsplitShape {
 
 UnsplitShape g_tune[8] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}};
 
-template <class RP, int MB>
-void launch_unsplit_v(const StepArgs& a, cudaStream_t st, int rows) {
-    constexpr int W = NT_UNSPLIT - 4;
-    const int ns = (a.L.mx + W - 1) / W;
-    StepArgs b = a;
-    b.H = rows > 0 ? rows : pick_rows(ns, a.L.my);
-    dim3 grid(ns, (a.L.my + b.H - 1) / b.H);
+// true for the method the SPEC_MC2 kernels are compiled for
+bool is_mc2(const Method& m, int mwaves) {
+    if (m.order != 2 || m.transverse != 2 || m.fwave != 0) return false;
+    for (int k = 0; k < mwaves; ++k)
+        if (m.mthlim[k] != 4) return false;
+    return true;
+}
+
+template <class RP, int MB, int SPEC>
+void launch_unsplit_s(const StepArgs& b, dim3 grid, cudaStream_t st) {
     constexpr int smem = (int)sizeof(UnsplitSmem<RP, NT_UNSPLIT>);
     static unsigned long long attr = 0;
-    smem_attr(k_step_unsplit<RP, NT_UNSPLIT, MB>, smem, attr);
-    k_step_unsplit<RP, NT_UNSPLIT, MB><<<grid, NT_UNSPLIT, smem, st>>>(b);
+    smem_attr(k_step_unsplit<RP, NT_UNSPLIT, MB, SPEC>, smem, attr);
+    k_step_unsplit<RP, NT_UNSPLIT, MB, SPEC><<<grid, NT_UNSPLIT, smem, st>>>(b);
+}
+
+// Tiling of the unsplit kernel: strips of NT_UNSPLIT - 4 output columns,
+// row blocks of H rows (the tuned height, else the heuristic).
+void unsplit_tiling(int riemann, int mx, int my, int& nstrips, int& H, int& nblocks) {
+    constexpr int W = NT_UNSPLIT - 4;
+    nstrips = (mx + W - 1) / W;
+    const int rows = g_tune[riemann & 7].rows;
+    H = rows > 0 ? rows : pick_rows(nstrips, my);
+    nblocks = (my + H - 1) / H;
+}
+
+template <class RP, int MB>
+void launch_unsplit_v(const StepArgs& a, cudaStream_t st) {
+    StepArgs b = a;
+    int ns, H, nb;
+    unsplit_tiling(RP::ID, a.L.mx, a.L.my, ns, H, nb);
+    if (b.tile_order == nullptr) {  // a caller with a schedule has fixed H and nstrips already
+        b.H = H;
+        b.nstrips = ns;
+    }
+    const int nbk = (a.L.my + b.H - 1) / b.H;
+    dim3 grid(b.nstrips * nbk);
+    if (is_mc2(a.meth, RP::MWAVES)) launch_unsplit_s<RP, MB, SPEC_MC2>(b, grid, st);
+    else launch_unsplit_s<RP, MB, SPEC_ANY>(b, grid, st);
 }
 
 template <class RP>
 void launch_unsplit(const StepArgs& a, cudaStream_t st) {
     const UnsplitShape sh = g_tune[RP::ID & 7];
-    if (sh.variant == 1) launch_unsplit_v<RP, 3>(a, st, sh.rows);
-    else launch_unsplit_v<RP, 2>(a, st, sh.rows);
+    if (sh.variant == 1) launch_unsplit_v<RP, 3>(a, st);
+    else launch_unsplit_v<RP, 2>(a, st);
 }
 
 template <class RP>
@@ -586,12 +614,63 @@ struct claw2_patch {
     double* guess = nullptr;                  // exact solver: learned guesses, x and y planes
     unsigned long long* counters = nullptr;   // exact solver: Newton iterations, solves
     claw2_mlp* mlp = nullptr;
+    // longest-first tile schedule of the unsplit kernel (k_lpt_order)
+    unsigned int* tile_cost = nullptr;
+    int* tile_order = nullptr;
+    int tile_cap = 0, tile_n = 0, tile_H = 0;
+    unsigned int tile_steps = 0;  // steps run on the current tiling
+    int nsm = 0;                  // SMs of the patch's device
     int cur = 0;
     bool pending = false;
 };
 
 namespace {
 
+
+// Buffers of the longest-first schedule for n tiles of height H; a new
+// tiling starts from the identity order.  Returns non-OK (no schedule) when
+// the tiling is too large for the one-CTA sort or the buffers cannot be had.
+int lpt_prepare(claw2_patch* p, int n, int H) {
+    if (n < 1 || n > LPT_MAX_TILES) return CLAW2_EINVAL;
+    if (n > p->tile_cap) {
+        cudaFree(p->tile_cost);
+        cudaFree(p->tile_order);
+        p->tile_cost = nullptr;
+        p->tile_order = nullptr;
+        p->tile_cap = 0;
+        if (cudaMalloc(&p->tile_cost, sizeof(unsigned int) * n) != cudaSuccess ||
+            cudaMalloc(&p->tile_order, sizeof(int) * n) != cudaSuccess) {
+            cudaFree(p->tile_cost);
+            cudaFree(p->tile_order);
+            p->tile_cost = nullptr;
+            p->tile_order = nullptr;
+            cudaGetLastError();
+            return CLAW2_ENOMEM;
+        }
+        p->tile_cap = n;
+        p->tile_n = 0;
+    }
+    if (p->tile_n != n || p->tile_H != H) {
+        k_iota<<<(n + 255) / 256, 256, 0, p->st>>>(p->tile_order, n);
+        cudaMemsetAsync(p->tile_cost, 0, sizeof(unsigned int) * n, p->st);
+        p->tile_n = n;
+        p->tile_H = H;
+        p->tile_steps = 0;
+    }
+    return CLAW2_OK;
+}
+
+// The tile costs drift slowly with the flow, so the schedule is re-sorted
+// after the first step on a tiling and then every LPT_EVERY steps.
+constexpr unsigned int LPT_EVERY = 4;
+
+void launch_lpt(const unsigned int* cost, int* order, int n, cudaStream_t st) {
+    int N = 1;
+    while (N < n) N <<= 1;
+    static unsigned long long attr = 0;
+    smem_attr(k_lpt_order, (int)sizeof(unsigned long long) * LPT_MAX_TILES, attr);
+    k_lpt_order<<<1, 1024, sizeof(unsigned long long) * N, st>>>(cost, order, n);
+}
 
 StepArgs patch_args(claw2_patch* p, double dt) {
     StepArgs a;
@@ -696,6 +775,7 @@ int claw2_patch_create(const claw2_desc* d, claw2_patch** out) {
     p->meth.fwave = d->fwave;
     for (int k = 0; k < CLAW2_MAX_WAVES; ++k) p->meth.mthlim[k] = k < mw ? d->mthlim[k] : 0;
     DeviceGuard g(p->device);
+    cudaDeviceGetAttribute(&p->nsm, cudaDevAttrMultiProcessorCount, p->device);
     const size_t nb = (size_t)me * p->L.plane * 8;
     const size_t ns = (size_t)me * d->mx * d->my * 8;
     bool ok = cudaMalloc(&p->q[0], nb) == cudaSuccess && cudaMalloc(&p->q[1], nb) == cudaSuccess &&
@@ -740,6 +820,8 @@ int claw2_patch_destroy(claw2_patch* p) {
         cudaFree(p->tmp);
         cudaFree(p->guess);
         cudaFree(p->counters);
+        cudaFree(p->tile_cost);
+        cudaFree(p->tile_order);
         cudaFree(p->stage);
         cudaFree(p->cfl);
         cudaFree(p->status);
@@ -796,15 +878,27 @@ int claw2_patch_step(claw2_patch* p, double dt, double* cfl) {
         mlp_guess_launch(p->mlp, qc, p->L, p->rp.c[0], p->guess, p->st);
         a.guess = p->guess;
     }
+    int lpt_n = 0;
     if (p->d.dimensional_split) {
         StepArgs ax = a, ay = a;
         ax.qnew = p->tmp;
         ay.qold = p->tmp;
         dispatch<SplitF>(p->d.riemann, ax, ay, p->st, 3);
     } else {
+        int ns, H, nb;
+        unsplit_tiling(p->d.riemann, p->L.mx, p->L.my, ns, H, nb);
+        // a schedule only matters when the tiles outnumber the CTA slots (2 per SM)
+        if (ns * nb > 2 * p->nsm && lpt_prepare(p, ns * nb, H) == CLAW2_OK) {
+            lpt_n = ns * nb;
+            a.H = H;
+            a.nstrips = ns;
+            a.tile_order = p->tile_order;
+            a.tile_cost = p->tile_cost;
+        }
         dispatch<UnsplitF>(p->d.riemann, a, p->st);
     }
     if (p->timing) CUDA_TRY(cudaEventRecord(p->ev1, p->st));
+    if (lpt_n > 0 && (p->tile_steps++ % LPT_EVERY) == 0) launch_lpt(p->tile_cost, p->tile_order, lpt_n, p->st);
     CUDA_TRY(cudaGetLastError());
     p->pending = true;
     if (cfl) return claw2_patch_cfl(p, cfl);
@@ -899,6 +993,22 @@ int claw2_probe_fp64(int device, double* tflops) {
     if (e != cudaSuccess) return fail(CLAW2_ECUDA, "fp64 probe failed: %s", cudaGetErrorString(e));
     const double flops = 2.0 * 16.0 * iters * (double)blocks * threads;
     *tflops = flops / (ms * 1e-3) / 1e12;
+    return CLAW2_OK;
+}
+
+int claw2_selftest_rcp(int device, int n, unsigned long long seed, double* max_ulp) {
+    if (!max_ulp) return fail(CLAW2_EINVAL, "null pointer argument");
+    if (n < 1) return fail(CLAW2_EINVAL, "n must be positive (got %d)", n);
+    DeviceGuard g(device);
+    unsigned long long* worst = nullptr;
+    CUDA_TRY(cudaMalloc(&worst, sizeof(unsigned long long)));
+    cudaMemset(worst, 0, sizeof(unsigned long long));
+    k_selftest_rcp<<<(n + 255) / 256, 256>>>(n, seed, worst);
+    unsigned long long h = 0;
+    cudaError_t e = cudaMemcpy(&h, worst, sizeof(h), cudaMemcpyDeviceToHost);
+    cudaFree(worst);
+    if (e != cudaSuccess) return fail(CLAW2_ECUDA, "reciprocal self-test failed: %s", cudaGetErrorString(e));
+    *max_ulp = (double)h;
     return CLAW2_OK;
 }
 
@@ -1026,8 +1136,9 @@ BatchArgs batch_args(claw2_batch* b) {
 template <class RP>
 int batch_smem_attr() {
     constexpr int smem = (int)sizeof(UnsplitSmem<RP, NT_UNSPLIT>);
-    static unsigned long long attr = 0;
-    smem_attr(k_batch_step<RP, NT_UNSPLIT, 2>, smem, attr);
+    static unsigned long long attr = 0, attr2 = 0;
+    smem_attr(k_batch_step<RP, NT_UNSPLIT, 2, SPEC_ANY>, smem, attr);
+    smem_attr(k_batch_step<RP, NT_UNSPLIT, 2, SPEC_MC2>, smem, attr2);
     return smem;
 }
 
@@ -1035,7 +1146,10 @@ template <class RP>
 struct BatchStepF {
     static void run(const BatchArgs& a, int first, int count, int grid, cudaStream_t st) {
         constexpr int smem = (int)sizeof(UnsplitSmem<RP, NT_UNSPLIT>);
-        k_batch_step<RP, NT_UNSPLIT, 2><<<grid, NT_UNSPLIT, smem, st>>>(a, first, count);
+        if (is_mc2(a.meth, RP::MWAVES))
+            k_batch_step<RP, NT_UNSPLIT, 2, SPEC_MC2><<<grid, NT_UNSPLIT, smem, st>>>(a, first, count);
+        else
+            k_batch_step<RP, NT_UNSPLIT, 2, SPEC_ANY><<<grid, NT_UNSPLIT, smem, st>>>(a, first, count);
     }
 };
 
@@ -1043,7 +1157,10 @@ template <class RP>
 struct BatchOccF {
     static void run(int* nb) {
         const int smem = batch_smem_attr<RP>();
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(nb, k_batch_step<RP, NT_UNSPLIT, 2>, NT_UNSPLIT, smem);
+        // sized from the generic kernel: both are compiled for 2 blocks per SM,
+        // and no CTA of the persistent kernel waits on another
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(nb, k_batch_step<RP, NT_UNSPLIT, 2, SPEC_ANY>, NT_UNSPLIT,
+                                                      smem);
     }
 };
 

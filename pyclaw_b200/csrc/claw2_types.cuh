@@ -33,4 +33,24 @@ struct Layout {
     long long plane;  // doubles per component plane
 };
 
+// 1/a by Newton-Raphson refinement of PTX's approximate reciprocal
+// (rcp.approx.ftz.f64): two steps of x <- x + x (1 - a x), each with the
+// residual 1 - a x formed by one fused multiply-add, so the relative error
+// squares per step (Newton's method for f(x) = 1/x - a; Markstein, IBM J.
+// Res. Dev. 34 (1990) 111-119).  Not correctly rounded: within 1 ulp of the
+// IEEE quotient (claw2_selftest_rcp).  Outside [1e-300, 1e300] in magnitude,
+// where the approximation flushes or overflows, the IEEE division is used.
+// Used for the limiter ratio and the reciprocal densities of the Roe solvers,
+// whose results the parity tests hold to 1e-12 of the oracle's IEEE divisions.
+__device__ __forceinline__ double rcp_nr(double a) {
+    const double aa = fabs(a);
+    if (!(aa > 1e-300 && aa < 1e300)) return 1.0 / a;
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(a));
+    double e = fma(-a, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-a, r, 1.0);
+    return fma(r, e, r);
+}
+
 }  // namespace claw2

@@ -166,7 +166,7 @@ struct RPEulerRoe {
 
     __device__ __forceinline__ static void prepare(const double (&q)[MEQN], const RPParams& p, double (&c)[NC]) {
         const double gamma = p.c[0], gamma1 = gamma - 1.0;
-        const double irho = 1.0 / q[0];
+        const double irho = rcp_nr(q[0]);
         const double u = q[1] * irho, v = q[2] * irho;
         const double pr = gamma1 * (q[3] - 0.5 * (q[1] * u + q[2] * v));
         c[0] = q[0]; c[1] = q[1]; c[2] = q[2]; c[3] = q[3];
@@ -201,7 +201,7 @@ struct RPEulerRoe {
         constexpr int UN = (IXY == 1) ? UX : UY, UT = (IXY == 1) ? UY : UX;
         const double gamma = p.c[0], gamma1 = gamma - 1.0;
         // Roe averages with weights sqrt(rho) / (sqrt(rho_L) + sqrt(rho_R))
-        const double inv = 1.0 / (cL[RS] + cR[RS]);
+        const double inv = rcp_nr(cL[RS] + cR[RS]);
         const double wl = cL[RS] * inv, wr = cR[RS] * inv;
         const double u = wl * cL[UN] + wr * cR[UN];
         const double v = wl * cL[UT] + wr * cR[UT];
@@ -240,7 +240,7 @@ struct RPEulerRoe {
                 const double rhou1 = cL[MU] + w[0][MU];
                 const double rhov1 = cL[MV] + w[0][MV];
                 const double en1 = cL[3] + w[0][3];
-                const double ir1 = 1.0 / rho1;
+                const double ir1 = rcp_nr(rho1);
                 const double p1 = gamma1 * (en1 - 0.5 * (rhou1 * rhou1 + rhov1 * rhov1) * ir1);
                 const double s1 = rhou1 * ir1 - sqrt(gamma * p1 * ir1);  // u - c right of the 1-wave
                 double sfract;
@@ -259,7 +259,7 @@ struct RPEulerRoe {
             const double rhou2 = cR[MU] - w[3][MU];
             const double rhov2 = cR[MV] - w[3][MV];
             const double en2 = cR[3] - w[3][3];
-            const double ir2 = 1.0 / rho2;
+            const double ir2 = rcp_nr(rho2);
             const double p2 = gamma1 * (en2 - 0.5 * (rhou2 * rhou2 + rhov2 * rhov2) * ir2);
             const double s2 = rhou2 * ir2 + sqrt(gamma * p2 * ir2);  // u + c left of the 4-wave
             double sfract = 0.0;
@@ -324,7 +324,7 @@ struct RPShallowRoe {
 
     __device__ __forceinline__ static void prepare(const double (&q)[MEQN], const RPParams& p, double (&c)[NC]) {
         const double grav = p.c[0];
-        const double ih = 1.0 / q[0];
+        const double ih = rcp_nr(q[0]);
         c[0] = q[0]; c[1] = q[1]; c[2] = q[2];
         c[RS] = sqrt(q[0]);
         c[UX] = q[1] * ih;
@@ -353,7 +353,7 @@ struct RPShallowRoe {
         constexpr int MU = Dir<IXY>::MU, MV = Dir<IXY>::MV;
         constexpr int UN = (IXY == 1) ? UX : UY, UT = (IXY == 1) ? UY : UX;
         const double grav = p.c[0];
-        const double inv = 1.0 / (cL[RS] + cR[RS]);
+        const double inv = rcp_nr(cL[RS] + cR[RS]);
         const double wl = cL[RS] * inv, wr = cR[RS] * inv;
         const double u = wl * cL[UN] + wr * cR[UN];
         const double v = wl * cL[UT] + wr * cR[UT];
@@ -510,7 +510,6 @@ struct RPEulerExact {
     __device__ __forceinline__ static void solve_g(const double (&cL)[NC], const double (&cR)[NC], const RPParams& p,
                                                    double guess, Iface& f, double (&amdq)[MEQN],
                                                    double (&apdq)[MEQN]) {
-        constexpr int MU = Dir<IXY>::MU, MV = Dir<IXY>::MV;
         constexpr int UN = (IXY == 1) ? UX : UY, UT = (IXY == 1) ? UY : UX;
         const double gamma = p.c[0], gamma1 = gamma - 1.0, g1inv = 1.0 / gamma1;
         const double tol = p.c[1];

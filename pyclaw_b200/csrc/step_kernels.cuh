@@ -41,11 +41,17 @@ struct StepArgs {
     int* status;                   // bit 0: non-finite output
     const double* guess;           // optional per-interface p* guesses: x plane, then y plane
     unsigned long long* counters;  // optional: [0] Newton iterations, [1] Riemann solves
+    // optional tile schedule of k_step_unsplit (1D grid of nstrips * row blocks):
+    // CTA b runs tile tile_order[b] and, with tile_cost, records its cost in
+    // SM clock cycles there (see k_lpt_order)
+    const int* tile_order = nullptr;
+    unsigned int* tile_cost = nullptr;
+    int nstrips = 0;
 };
 
 // philim.f90:16-35
 __device__ __forceinline__ double philim(double a, double b, int meth) {
-    const double r = b / a;
+    const double r = b * rcp_nr(a);
     switch (meth) {
         case 1: return fmax(0.0, fmin(1.0, r));
         case 2: return fmax(0.0, fmax(fmin(1.0, 2.0 * r), fmin(2.0, r)));
@@ -96,11 +102,18 @@ __device__ __forceinline__ bool all_finite(const double (&v)[ME]) {
 // Shared pieces of the interface work
 // ---------------------------------------------------------------------------
 
+// Method specialisations of the step kernels.  SPEC_ANY reads order,
+// transverse mode, limiters and f-wave flag at run time; SPEC_MC2 is the
+// high-resolution method with transverse correction waves and the MC limiter
+// on every family (order 2, trans_cor, mthlim = 4, no f-waves), fixed at
+// compile time so the limiter switch and the method branches fold away.
+enum { SPEC_ANY = 0, SPEC_MC2 = 1 };
+
 // Limiter (limiter.f90:29-53 / philim.f90) and second-order correction
 // cqxx = sum_k coef_k * phi_k * w_k (flux2.f90:134-160) for one interface.
 // dl / dr are the dot products of each unlimited wave with the same family's
 // unlimited wave at the interface below/left and above/right.
-template <class RP, int IXY>
+template <class RP, int IXY, int SPEC = SPEC_ANY>
 __device__ __forceinline__ void correction(const typename RP::Iface& f, const RPParams& p, const Method& meth,
                                            double dtdx, const double (&dl)[RP::MWAVES],
                                            const double (&dr)[RP::MWAVES], double (&cq)[RP::MEQN]) {
@@ -113,14 +126,15 @@ __device__ __forceinline__ void correction(const typename RP::Iface& f, const RP
     for (int m = 0; m < ME; ++m) cq[m] = 0.0;
 #pragma unroll
     for (int k = 0; k < MW; ++k) {
-        const int lim = meth.mthlim[k];
+        const int lim = (SPEC == SPEC_MC2) ? 4 : meth.mthlim[k];
         double wn2 = 0.0;
 #pragma unroll
         for (int m = 0; m < ME; ++m) wn2 = wn2 + w[k][m] * w[k][m];
         double phi = 1.0;
         if (lim != 0 && wn2 != 0.0) phi = philim(wn2, (s[k] > 0.0) ? dl[k] : dr[k], lim);
         const double as = fabs(s[k]);
-        const double coef = ((meth.fwave != 0) ? copysign(1.0, s[k]) : as) * (1.0 - as * dtdx);
+        const bool fw = (SPEC == SPEC_MC2) ? false : (meth.fwave != 0);
+        const double coef = (fw ? copysign(1.0, s[k]) : as) * (1.0 - as * dtdx);
 #pragma unroll
         for (int m = 0; m < ME; ++m) cq[m] = cq[m] + coef * (phi * w[k][m]);
     }
@@ -153,7 +167,7 @@ struct UnsplitSmem {
 // the interior rows [rb, rb + H) of one grid.  Returns this thread's CFL
 // contribution in `cfl`; the caller reduces it (the tile ends with every
 // shared-memory read done, so a persistent CTA can start the next tile).
-template <class RP, int NT>
+template <class RP, int NT, int SPEC = SPEC_ANY>
 __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int rb, UnsplitSmem<RP, NT>& S,
                                              double& cfl) {
     constexpr int ME = RP::MEQN, MW = RP::MWAVES, NC = RP::NC, W = NT - 4;
@@ -174,7 +188,8 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
     const int tr = (t < NT - 1) ? t + 1 : NT - 1;
     const double dtdx = a.dtdx, dtdy = a.dtdy;
     const RPParams& P = a.rp;
-    const int order = a.meth.order, trans = a.meth.transverse;
+    const int order = (SPEC == SPEC_MC2) ? 2 : a.meth.order;
+    const int trans = (SPEC == SPEC_MC2) ? 2 : a.meth.transverse;
     const bool tc = (order > 1) && (trans == 2);
     const double* qo = a.qold + cpl;
     double* qn = a.qnew + cpl;
@@ -249,7 +264,7 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
                 if (ycfl_col) cfl = fmax(cfl, iface_cfl<RP, 2>(fY, P, dtdy));
                 double cq[ME];
                 if (order != 1) {
-                    correction<RP, 2>(fY, P, a.meth, dtdy, dY, dn, cq);
+                    correction<RP, 2, SPEC>(fY, P, a.meth, dtdy, dY, dn, cq);
                 } else {
 #pragma unroll
                     for (int m = 0; m < ME; ++m) cq[m] = 0.0;
@@ -337,7 +352,7 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
                     dl[k] = x;
                     dr[k] = y;
                 }
-                correction<RP, 1>(fX, P, a.meth, dtdx, dl, dr, cq);
+                correction<RP, 1, SPEC>(fX, P, a.meth, dtdx, dl, dr, cq);
             } else {
 #pragma unroll
                 for (int m = 0; m < ME; ++m) cq[m] = 0.0;
@@ -413,13 +428,69 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
     if (GuessTraits<RP>::USES && a.counters) counter_commit(a.counters, n_it, n_solve);
 }
 
-template <class RP, int NT, int MINB>
+// Grid: 1D over the tiles (strip fastest).  Tile t = (strip t % nstrips, row
+// block t / nstrips); CTA b runs tile_order[b] when a schedule is given.
+template <class RP, int NT, int MINB, int SPEC>
 __global__ void __launch_bounds__(NT, MINB) k_step_unsplit(const StepArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     UnsplitSmem<RP, NT>& S = *reinterpret_cast<UnsplitSmem<RP, NT>*>(smem_raw);
+    int tile = blockIdx.x;
+    if (a.tile_order) {
+        const int t = a.tile_order[blockIdx.x];
+        if (t >= 0 && t < (int)gridDim.x) tile = t;  // a schedule is a permutation; anything else is ignored
+    }
+    long long t0 = 0;
+    if (a.tile_cost && threadIdx.x == 0) t0 = clock64();
     double cfl = 0.0;
-    unsplit_tile<RP, NT>(a, blockIdx.x, blockIdx.y * a.H, S, cfl);
+    unsplit_tile<RP, NT, SPEC>(a, tile % a.nstrips, (tile / a.nstrips) * a.H, S, cfl);
     cfl_commit(cfl, S.red, a.cfl_bits);
+    if (a.tile_cost && threadIdx.x == 0) {
+        const long long c = clock64() - t0;
+        a.tile_cost[tile] = (unsigned int)(c < 0 ? 0 : (c > 0xffffffffll ? 0xffffffffll : c));
+    }
+}
+
+// Longest-first tile schedule for the next step from this step's tile costs:
+// one CTA sorts (cost, tile) pairs, n <= LPT_MAX_TILES, descending by cost
+// (ties: lower tile first) with a bitonic network in shared memory, and
+// writes the tile order.  The hardware starts CTAs in block order, so the
+// most expensive tiles (the developed parts of the flow; the cost pattern
+// moves slowly from step to step) start first and the cheap ones fill the
+// tail, which evens out the SMs' finishing times.  The order changes only
+// which SM runs a tile: every result is independent of it.
+constexpr int LPT_MAX_TILES = 8192;
+static __global__ void __launch_bounds__(1024) k_lpt_order(const unsigned int* cost, int* order, int n) {
+    extern __shared__ unsigned long long keys[];
+    int N = 1;
+    while (N < n) N <<= 1;
+    for (int i = threadIdx.x; i < N; i += blockDim.x)
+        keys[i] = (i < n) ? (((unsigned long long)cost[i] << 32) | (unsigned long long)(0xffffffffu - (unsigned)i))
+                          : 0ull;
+    __syncthreads();
+    for (int k = 2; k <= N; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < N; i += blockDim.x) {
+                const int ixj = i ^ j;
+                if (ixj > i) {
+                    const unsigned long long x = keys[i], y = keys[ixj];
+                    // descending overall: blocks with (i & k) == 0 descend, the others ascend
+                    const bool swap = ((i & k) == 0) ? (x < y) : (x > y);
+                    if (swap) {
+                        keys[i] = y;
+                        keys[ixj] = x;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        order[i] = (int)(0xffffffffu - (unsigned)(keys[i] & 0xffffffffull));
+}
+
+static __global__ void k_iota(int* a, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = i;
 }
 
 // ---------------------------------------------------------------------------
@@ -754,6 +825,24 @@ static __global__ void k_fp64_fma(double* out, int iters, double b) {
 #pragma unroll
     for (int k = 0; k < 16; ++k) s += a[k];
     out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+// Self-test of rcp_nr: a = +-(1 + u) 2^e, e uniform in [-1000, 1000], u in
+// [0, 1) from a counter hash of (seed, i); the largest distance in units in
+// the last place between rcp_nr(a) and the IEEE quotient 1.0 / a.
+static __global__ void k_selftest_rcp(int n, unsigned long long seed, unsigned long long* worst) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    unsigned long long z = seed ^ (0x9E3779B97F4A7C15ull * (unsigned long long)(i + 1));
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    const double u = (double)(z >> 11) * (1.0 / 9007199254740992.0);
+    const int e = (int)((z & 2047ull) % 2001ull) - 1000;
+    const double a = ((z >> 63) ? -1.0 : 1.0) * ldexp(1.0 + u, e);
+    const double r = rcp_nr(a), q = 1.0 / a;
+    const long long d = __double_as_longlong(r) - __double_as_longlong(q);
+    atomicMax(worst, (unsigned long long)(d < 0 ? -d : d));
 }
 
 }  // namespace claw2

@@ -52,3 +52,5 @@ def test_bad_arguments_rejected_without_gpu(lib):
                        None, 0)
     assert rc == _lib.EINVAL
     assert b"null" in L.claw2_last_error()
+    rc = L.claw2_selftest_rcp(0, 100, 1, None)
+    assert rc == _lib.EINVAL

@@ -112,3 +112,16 @@ def test_bc_fill_rejects_wall_on_single_cell():
     qbc = random_qbc(_lib.RP_SHALLOW_ROE, 1, 4, seed=5)
     with pytest.raises(_lib.Claw2Error):
         classic2.bc_fill(qbc, (3, 1), (3, 1))
+
+
+def test_kernel_reciprocal_within_one_ulp_of_ieee_division():
+    # the limiter ratio and the Roe solvers' reciprocal densities use a
+    # Newton-Raphson reciprocal; over 2^22 values spanning 2^-1000..2^1000 it
+    # stays within 1 ulp of CUDA's IEEE quotient
+    import ctypes
+    L = _lib.load()
+    for seed in (1, 2024):
+        ulp = ctypes.c_double(-1.0)
+        _lib.check(L.claw2_selftest_rcp(0, 1 << 22, seed, ctypes.byref(ulp)))
+        assert 0.0 <= ulp.value <= 1.0, ulp.value
+

@@ -168,3 +168,28 @@ def test_shallow_dam_break_conserves_mass():
     claw.run()
     h1 = claw.frames[-1].q[0].sum()
     assert abs(h1 - s0[0]) <= 1e-13 * scale[0]
+
+
+def test_whole_run_euler_quadrants_matches_oracle(oracle):
+    # the benchmark's Euler problem at 256^2 run to its final time t = 0.8
+    # (543 steps) on both paths; per-step differences are ~1e-16, so the
+    # whole-run difference measures their growth through a nonlinear run.
+    import os
+    oracle.set_threads(os.cpu_count() or 1)
+    claw_g = workloads.euler_quadrants_unsplit(n=256, tfinal=0.8)
+    claw_g.num_output_times = 1
+    claw_g.run()
+    claw_o = workloads.euler_quadrants_unsplit(oracle.make_solver_class(), n=256, tfinal=0.8)
+    claw_o.num_output_times = 1
+    claw_o.run()
+    oracle.set_threads(1)
+    assert claw_g.solver.status['numsteps'] == claw_o.solver.status['numsteps']
+    qg, qo = claw_g.frames[-1].q, claw_o.frames[-1].q
+    diff = max_rel(qg, qo)
+    # the data are symmetric about x = y (with u <-> v); so is the result
+    qt = np.transpose(qg, (0, 2, 1)).copy()
+    qt[[1, 2]] = qt[[2, 1]]
+    sym = max_rel(qt, qg)
+    print("whole-run max rel diff %.3e, diagonal symmetry %.3e" % (diff, sym))
+    assert diff <= 1e-9
+    assert sym <= 1e-9

@@ -125,3 +125,25 @@ def test_partition_and_bcs():
     assert slabs.local_bcs([1, 3], [1, 3], 1, 2) == ([1, -1], [1, 3])
     assert slabs.local_bcs([2, 2], [2, 2], 0, 2) == ([2, -1], [2, -1])
     assert slabs.neighbours(0, 3, True) == (2, 1) and slabs.neighbours(0, 3, False) == (None, 1)
+
+
+def test_batch_partition_balances_cells_over_ranks():
+    # the batched workload's seeded sides (512 problems, side in {64, 80, ..., 512})
+    from pyclaw_b200.batch import partition_instances
+    rng = np.random.default_rng(2024)
+    sides = []
+    for _ in range(512):
+        sides.append(int(rng.choice(tuple(range(64, 513, 16)))))
+        rng.uniform(0.3, 0.7, size=2)
+        for _q in range(4):
+            rng.uniform(0.1, 2.0, size=2)
+            rng.uniform(-1.0, 1.0, size=2)
+    cells = np.array(sides) ** 2
+    for world in (1, 2, 4, 8):
+        parts = partition_instances(cells, world)
+        flat = sorted(i for p in parts for i in p)
+        assert flat == list(range(512))
+        loads = np.array([cells[p].sum() for p in parts])
+        assert loads.max() <= loads.mean() + cells.max()
+        assert loads.max() / loads.mean() < 1.01
+        assert parts == partition_instances(cells, world)
