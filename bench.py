@@ -38,6 +38,11 @@ N = 1024
 MEQN = 4
 BYTES_PER_CELL = 2 * MEQN * 8  # read q^n + write q^{n+1}, FP64
 WORKLOAD = "euler_quadrants_roe_1024x1024_unsplit_trans_cor_mc"
+# One ncu capture of the step kernel on this workload (profiles/k_step_unsplit_euler_roe_1024.md):
+# dram__bytes_read.sum + dram__bytes_write.sum per launch, and the FP64 pipe's busy fraction.
+# The launch's 33.5 MB of output stays in L2 while it runs, so DRAM shows the reads only.
+NCU_TRAFFIC_BYTES = {1024: 34.275e6 + 0.831e6}
+NCU_FP64_PIPE_ACTIVE = {1024: 0.435}
 
 
 def parse():
@@ -225,6 +230,8 @@ def batched_workload(n_instances=512, steps=100, plain=True):
     out = {"instances": n_instances, "cells_total": float(cells.sum()), "steps": steps,
            "rows_per_bucket": [int(c) for c in choice], "bucket_edges": [128, 256],
            "plain_loop_rows": "single-problem heuristic (0)"}
+    ntiles, grid = bat.tiles()
+    out["tiles"], out["persistent_grid"] = ntiles, grid
     for mode, name in ((0, "graph_persistent"), (2, "plain_per_instance_loop"))[:2 if plain else 1]:
         if mode == 2:
             # the plain loop launches each problem alone: give every launch the
@@ -244,8 +251,6 @@ def batched_workload(n_instances=512, steps=100, plain=True):
                      "failed_instances": int(st["failed"].sum())}
     if plain:
         out["speedup"] = out["graph_persistent"]["value"] / out["plain_per_instance_loop"]["value"]
-    ntiles, grid = bat.tiles()
-    out["tiles"], out["persistent_grid"] = ntiles, grid
     bat.close()
     return out
 
@@ -523,12 +528,16 @@ def run_ours(args):
                                                                  for k, v in sorted(trials.items())}},
                                   "state": "quadrant problem advanced to t=%g before warm-up" % args.pre_t}),
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                             "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                             "frac": achieved / peaks["hbm_gbs"], "traffic": NCU_TRAFFIC_BYTES.get(n),
+                             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch "
+                                               "(profiles/k_step_unsplit_euler_roe_1024.md)",
                              "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_src,
                              "kernel": "k_step_unsplit<RPEulerRoe,128>", "kernel_ms": kms,
                              "algorithmic_bytes_per_launch": cells * BYTES_PER_CELL,
                              "fp64_probe_tflops": fp64.value,
-                             "fp64_flops_per_cell_est": None},
+                             "fp64_pipe_active_ncu": NCU_FP64_PIPE_ACTIVE.get(n),
+                             "note": "FP64-bound kernel: ~870 FP64 instructions per cell-update cap it near "
+                                     "2.1e10 cell-updates/s (21% of HBM) on this part"},
                 "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
                 "secondary": secondary,
                 "gpu_launches": 2 * args.steps}
