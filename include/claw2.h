@@ -129,6 +129,18 @@ int claw2_patch_download_q(claw2_patch* p, double* q);
  * call waits and returns the Courant number; with NULL it only enqueues. */
 int claw2_patch_step(claw2_patch* p, double dt, double* cfl);
 
+/* Many independent steps from host buffers (no counterpart in the reference,
+ * whose step2 call moves one host qbc per step through f2py): for k < nsteps,
+ * q_out[k] = one step (ghost fill, step, CFL) of q_in[k] with dt[k], each
+ * accepted, cfl_out[k] its Courant number.  q_in/q_out are host arrays of
+ * shape (num_eqn, mx, my), Fortran order (pinned memory for overlap).  The
+ * copies of step k+1's input overlap step k's compute and result copy (a copy
+ * stream, two staging buffers per direction).  Afterwards the patch holds the
+ * last result.  Returns CLAW2_ENONFINITE if any step produced a non-finite
+ * value. */
+int claw2_patch_run_host(claw2_patch* p, int nsteps, const double* const* q_in, double* const* q_out,
+                         const double* dt, double* cfl_out);
+
 /* Accept (1) or reject (0) the pending step (solver.py:619-651): accept makes
  * it the current q; reject keeps the old q.  No copy either way. */
 int claw2_patch_accept(claw2_patch* p, int accept);

@@ -619,6 +619,14 @@ struct claw2_patch {
     int* tile_order = nullptr;
     int tile_cap = 0, tile_n = 0, tile_H = 0;
     unsigned int tile_steps = 0;  // steps run on the current tiling
+    // host pipeline of claw2_patch_run_host
+    cudaStream_t cst = nullptr;
+    double* stage_in[2] = {nullptr, nullptr};
+    double* stage_out1 = nullptr;
+    cudaEvent_t h2d_done[2] = {nullptr, nullptr}, in_free[2] = {nullptr, nullptr};
+    unsigned long long* cfl_hist = nullptr;
+    unsigned long long* h_cfl_hist = nullptr;
+    int cfl_hist_cap = 0;
     int nsm = 0;                  // SMs of the patch's device
     int cur = 0;
     bool pending = false;
@@ -635,6 +643,16 @@ int lpt_prepare(claw2_patch* p, int n, int H) {
     if (n > p->tile_cap) {
         cudaFree(p->tile_cost);
         cudaFree(p->tile_order);
+        if (p->cst) cudaStreamSynchronize(p->cst);
+        for (int i = 0; i < 2; ++i) {
+            cudaFree(p->stage_in[i]);
+            if (p->h2d_done[i]) cudaEventDestroy(p->h2d_done[i]);
+            if (p->in_free[i]) cudaEventDestroy(p->in_free[i]);
+        }
+        cudaFree(p->stage_out1);
+        cudaFree(p->cfl_hist);
+        cudaFreeHost(p->h_cfl_hist);
+        if (p->cst) cudaStreamDestroy(p->cst);
         p->tile_cost = nullptr;
         p->tile_order = nullptr;
         p->tile_cap = 0;
@@ -866,10 +884,13 @@ int claw2_patch_download_q(claw2_patch* p, double* q) {
     return CLAW2_OK;
 }
 
-int claw2_patch_step(claw2_patch* p, double dt, double* cfl) {
-    if (!p) return fail(CLAW2_EINVAL, "null patch");
-    if (!(dt >= 0.0) || !std::isfinite(dt)) return fail(CLAW2_EINVAL, "dt must be finite and >= 0");
-    DeviceGuard g(p->device);
+}  // extern "C"
+
+namespace {
+
+// Ghost fill + step (+ learned guess pre-pass, + tile schedule) of a patch on
+// its stream; the result goes to the pending buffer.
+int patch_enqueue_step(claw2_patch* p, double dt) {
     double* qc = p->q[p->cur];
     launch_bc(qc, p->L, p->d.num_eqn, p->d.bc_lower, p->d.bc_upper, p->cfl, p->st);
     StepArgs a = patch_args(p, dt);
@@ -901,7 +922,104 @@ int claw2_patch_step(claw2_patch* p, double dt, double* cfl) {
     if (lpt_n > 0 && (p->tile_steps++ % LPT_EVERY) == 0) launch_lpt(p->tile_cost, p->tile_order, lpt_n, p->st);
     CUDA_TRY(cudaGetLastError());
     p->pending = true;
+    return CLAW2_OK;
+}
+
+// Buffers of claw2_patch_run_host: a copy stream, two input and two output
+// staging buffers, their events and the per-step CFL words.
+int host_pipe_reserve(claw2_patch* p, int nsteps) {
+    const size_t n = (size_t)p->d.num_eqn * p->d.mx * p->d.my;
+    if (!p->cst) {
+        bool ok = cudaStreamCreateWithFlags(&p->cst, cudaStreamNonBlocking) == cudaSuccess;
+        for (int i = 0; i < 2 && ok; ++i)
+            ok = cudaMalloc(&p->stage_in[i], n * 8) == cudaSuccess &&
+                 cudaEventCreateWithFlags(&p->h2d_done[i], cudaEventDisableTiming) == cudaSuccess &&
+                 cudaEventCreateWithFlags(&p->in_free[i], cudaEventDisableTiming) == cudaSuccess;
+        ok = ok && cudaMalloc(&p->stage_out1, n * 8) == cudaSuccess;
+        if (!ok) {
+            cudaGetLastError();
+            return fail(CLAW2_ENOMEM, "staging buffers for the host pipeline could not be allocated");
+        }
+    }
+    if (nsteps > p->cfl_hist_cap) {
+        cudaFree(p->cfl_hist);
+        cudaFreeHost(p->h_cfl_hist);
+        p->cfl_hist = nullptr;
+        p->h_cfl_hist = nullptr;
+        p->cfl_hist_cap = 0;
+        if (cudaMalloc(&p->cfl_hist, sizeof(unsigned long long) * nsteps) != cudaSuccess ||
+            cudaMallocHost(&p->h_cfl_hist, sizeof(unsigned long long) * nsteps) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(CLAW2_ENOMEM, "CFL history of %d steps could not be allocated", nsteps);
+        }
+        p->cfl_hist_cap = nsteps;
+    }
+    return CLAW2_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int claw2_patch_step(claw2_patch* p, double dt, double* cfl) {
+    if (!p) return fail(CLAW2_EINVAL, "null patch");
+    if (!(dt >= 0.0) || !std::isfinite(dt)) return fail(CLAW2_EINVAL, "dt must be finite and >= 0");
+    DeviceGuard g(p->device);
+    const int rc = patch_enqueue_step(p, dt);
+    if (rc) return rc;
     if (cfl) return claw2_patch_cfl(p, cfl);
+    return CLAW2_OK;
+}
+
+int claw2_patch_run_host(claw2_patch* p, int nsteps, const double* const* q_in, double* const* q_out,
+                         const double* dt, double* cfl_out) {
+    if (!p || !q_in || !q_out || !dt || !cfl_out || nsteps < 1) return fail(CLAW2_EINVAL, "bad arguments");
+    for (int k = 0; k < nsteps; ++k) {
+        if (!q_in[k] || !q_out[k]) return fail(CLAW2_EINVAL, "null buffer for step %d", k);
+        if (!(dt[k] >= 0.0) || !std::isfinite(dt[k])) return fail(CLAW2_EINVAL, "dt[%d] must be finite and >= 0", k);
+    }
+    DeviceGuard g(p->device);
+    int rc = host_pipe_reserve(p, nsteps);
+    if (rc) return rc;
+    const size_t n = (size_t)p->d.num_eqn * p->d.mx * p->d.my;
+    const long long cells = (long long)p->d.mx * p->d.my;
+    double* stage_out[2] = {p->stage, p->stage_out1};
+    // both input buffers start free; the first input goes up at once
+    CUDA_TRY(cudaEventRecord(p->in_free[0], p->st));
+    CUDA_TRY(cudaEventRecord(p->in_free[1], p->st));
+    CUDA_TRY(cudaStreamWaitEvent(p->cst, p->in_free[0], 0));
+    CUDA_TRY(cudaMemcpyAsync(p->stage_in[0], q_in[0], n * 8, cudaMemcpyHostToDevice, p->cst));
+    CUDA_TRY(cudaEventRecord(p->h2d_done[0], p->cst));
+    for (int k = 0; k < nsteps; ++k) {
+        const int s = k & 1;
+        if (k + 1 < nsteps) {  // next input on the copy stream while this step computes
+            const int s1 = (k + 1) & 1;
+            CUDA_TRY(cudaStreamWaitEvent(p->cst, p->in_free[s1], 0));
+            CUDA_TRY(cudaMemcpyAsync(p->stage_in[s1], q_in[k + 1], n * 8, cudaMemcpyHostToDevice, p->cst));
+            CUDA_TRY(cudaEventRecord(p->h2d_done[s1], p->cst));
+        }
+        CUDA_TRY(cudaStreamWaitEvent(p->st, p->h2d_done[s], 0));
+        k_aos_to_planes<<<grid_blocks(cells), 256, 0, p->st>>>(p->stage_in[s], p->q[p->cur], p->L, p->d.num_eqn, 0);
+        CUDA_TRY(cudaEventRecord(p->in_free[s], p->st));
+        rc = patch_enqueue_step(p, dt[k]);
+        if (rc) return rc;
+        CUDA_TRY(cudaMemcpyAsync(p->cfl_hist + k, p->cfl, sizeof(unsigned long long), cudaMemcpyDeviceToDevice,
+                                 p->st));
+        p->cur ^= 1;  // accepted
+        p->pending = false;
+        k_planes_to_aos<<<grid_blocks(cells), 256, 0, p->st>>>(p->q[p->cur], stage_out[s], p->L, p->d.num_eqn, 0);
+        CUDA_TRY(cudaMemcpyAsync(q_out[k], stage_out[s], n * 8, cudaMemcpyDeviceToHost, p->st));
+    }
+    CUDA_TRY(cudaMemcpyAsync(p->h_cfl_hist, p->cfl_hist, sizeof(unsigned long long) * nsteps,
+                             cudaMemcpyDeviceToHost, p->st));
+    CUDA_TRY(cudaMemcpyAsync(p->h_status, p->status, sizeof(int), cudaMemcpyDeviceToHost, p->st));
+    CUDA_TRY(cudaStreamSynchronize(p->st));
+    CUDA_TRY(cudaStreamSynchronize(p->cst));
+    for (int k = 0; k < nsteps; ++k) std::memcpy(&cfl_out[k], &p->h_cfl_hist[k], sizeof(double));
+    if (*p->h_status & 1) {
+        cudaMemsetAsync(p->status, 0, sizeof(int), p->st);
+        return fail(CLAW2_ENONFINITE, "a step produced a non-finite value");
+    }
     return CLAW2_OK;
 }
 

@@ -304,6 +304,15 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
 #pragma unroll
             for (int k = 0; k < MW; ++k) dY[k] = dn[k];
         }
+        // Publish the y sweep's neighbour increments now, which ends their live
+        // range before the x work (fewer registers); every read of the previous
+        // row's exchange slots came before S1.
+#pragma unroll
+        for (int m = 0; m < ME; ++m) {
+            S.xl[0][m][t] = ylB[m];
+            S.yr[0][m][t] = yrB[m];
+            S.yr[1][m][t] = yrA[m];
+        }
 
         // ---- x: the interface (cp-1 | cp) on row R ----
         const bool xrow = (R > R0) && (R < R1);  // rows R0+1 .. R1-1
@@ -388,12 +397,9 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
         }
 #pragma unroll
         for (int m = 0; m < ME; ++m) {
-            S.xl[0][m][t] = ylB[m];
             S.xl[1][m][t] = xbL[m] + ylA[m];
             S.xl[2][m][t] = xcL[m];
             S.xl[3][m][t] = xaL[m];
-            S.yr[0][m][t] = yrB[m];
-            S.yr[1][m][t] = yrA[m];
         }
         __syncthreads();  // S3: neighbour increments visible
 #pragma unroll

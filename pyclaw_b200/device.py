@@ -69,6 +69,26 @@ class DevicePatch(object):
         _lib.check(self._lib.claw2_patch_step(self.h, ctypes.c_double(dt), None))
         return None
 
+    def run_host(self, q_in, q_out, dt):
+        """Independent steps from host arrays: q_out[k] = step of q_in[k] with
+        dt[k] (claw2_patch_run_host; copies overlap compute).  q_in / q_out
+        are lists of (num_eqn, mx, my) Fortran-order float64 arrays (pinned
+        for overlap).  Returns the Courant numbers."""
+        n = len(q_in)
+        if len(q_out) != n or len(dt) != n:
+            raise ValueError("q_in, q_out and dt need one entry per step")
+        for a in list(q_in) + list(q_out):
+            if a.shape != self.shape or a.dtype != np.float64 or not a.flags.f_contiguous:
+                raise ValueError("arrays must be float64 %s in Fortran order" % (self.shape,))
+        pin = (ctypes.c_void_p * n)(*[a.ctypes.data for a in q_in])
+        pout = (ctypes.c_void_p * n)(*[a.ctypes.data for a in q_out])
+        dts = np.ascontiguousarray(dt, dtype=np.float64)
+        cfl = np.zeros(n)
+        _lib.check(self._lib.claw2_patch_run_host(self.h, n, pin, pout, _lib.dptr(dts), _lib.dptr(cfl)))
+        self.device_newer = True
+        self.host_dirty = False
+        return cfl
+
     def accept(self, accept):
         _lib.check(self._lib.claw2_patch_accept(self.h, 1 if accept else 0))
         if accept:

@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 from helpers import PARITY_RTOL, max_rel
-from pyclaw_b200 import workloads
+from pyclaw_b200 import _lib, workloads
 
 pytestmark = pytest.mark.gpu
 
@@ -193,3 +193,32 @@ def test_whole_run_euler_quadrants_matches_oracle(oracle):
     print("whole-run max rel diff %.3e, diagonal symmetry %.3e" % (diff, sym))
     assert diff <= 1e-9
     assert sym <= 1e-9
+
+
+def test_run_host_equals_one_call_per_step():
+    # claw2_patch_run_host (overlapped host-to-host steps) gives, step for
+    # step, the same result and CFL as upload + step + accept + download
+    claw = workloads.euler_quadrants_unsplit(n=96, tfinal=0.1)
+    s, sol = claw.solver, claw.solution
+    s.setup(sol)
+    p = s._dev
+    rng = np.random.default_rng(3)
+    q0 = sol.state.get_q_global()
+    qs = [np.asfortranarray(q0 * (1.0 + 0.01 * rng.random(q0.shape))) for _ in range(3)]
+    dts = [2e-4, 3e-4, 1e-4]
+    ref, cref = [], []
+    for q, dt in zip(qs, dts):
+        sol.state.q = q
+        p.push(sol.state)
+        cref.append(p.step(dt))
+        p.accept(True)
+        out = np.empty(q.shape, order="F")
+        _lib.check(p._lib.claw2_patch_download_q(p.h, _lib.dptr(out)))
+        ref.append(out)
+    outs = [np.empty(q.shape, order="F") for q in qs]
+    cfl = p.run_host(qs, outs, dts)
+    for a, b in zip(outs, ref):
+        assert np.array_equal(a, b)
+    assert list(cfl) == cref
+    # the patch holds the last result
+    assert np.array_equal(sol.state.get_q_global(), ref[-1])
