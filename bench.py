@@ -514,7 +514,8 @@ def run_ours(args):
         e2e = {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": qh.nbytes,
                "d2h_bytes_per_step": qd.nbytes + 8, "steps": K,
                "path": "claw2_patch_run_host: per step, pinned host state -> device, ghost fill + step + CFL, "
-                       "result -> pinned host; copies of step k+1 overlap step k; wall clock",
+                       "result -> pinned host; uploads and downloads on their own streams overlap the "
+                       "compute of the neighbouring steps; wall clock",
                "one_call_per_step": {"value": seq_val, "unit": UNIT,
                                      "path": "claw2_patch_upload_q + claw2_patch_step (returns CFL) + "
                                              "claw2_patch_accept + claw2_patch_download_q"}}

@@ -134,10 +134,12 @@ int claw2_patch_step(claw2_patch* p, double dt, double* cfl);
  * q_out[k] = one step (ghost fill, step, CFL) of q_in[k] with dt[k], each
  * accepted, cfl_out[k] its Courant number.  q_in/q_out are host arrays of
  * shape (num_eqn, mx, my), Fortran order (pinned memory for overlap).  The
- * copies of step k+1's input overlap step k's compute and result copy (a copy
- * stream, two staging buffers per direction).  Afterwards the patch holds the
- * last result.  Returns CLAW2_ENONFINITE if any step produced a non-finite
- * value. */
+ * upload of step k+1 and the download of step k overlap step k+1's compute
+ * (an upload and a download stream, two staging buffers per direction), so the
+ * input of a step must not be the output buffer of an earlier step of the
+ * same call (chained steps stay on the device: claw2_patch_step).  Afterwards
+ * the patch holds the last result.  Returns CLAW2_ENONFINITE if any step
+ * produced a non-finite value. */
 int claw2_patch_run_host(claw2_patch* p, int nsteps, const double* const* q_in, double* const* q_out,
                          const double* dt, double* cfl_out);
 

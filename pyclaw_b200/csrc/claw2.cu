@@ -620,10 +620,11 @@ struct claw2_patch {
     int tile_cap = 0, tile_n = 0, tile_H = 0;
     unsigned int tile_steps = 0;  // steps run on the current tiling
     // host pipeline of claw2_patch_run_host
-    cudaStream_t cst = nullptr;
+    cudaStream_t cst = nullptr, dst = nullptr;  // upload and download streams
     double* stage_in[2] = {nullptr, nullptr};
     double* stage_out1 = nullptr;
     cudaEvent_t h2d_done[2] = {nullptr, nullptr}, in_free[2] = {nullptr, nullptr};
+    cudaEvent_t out_ready[2] = {nullptr, nullptr}, out_free[2] = {nullptr, nullptr};
     unsigned long long* cfl_hist = nullptr;
     unsigned long long* h_cfl_hist = nullptr;
     int cfl_hist_cap = 0;
@@ -644,15 +645,19 @@ int lpt_prepare(claw2_patch* p, int n, int H) {
         cudaFree(p->tile_cost);
         cudaFree(p->tile_order);
         if (p->cst) cudaStreamSynchronize(p->cst);
+        if (p->dst) cudaStreamSynchronize(p->dst);
         for (int i = 0; i < 2; ++i) {
             cudaFree(p->stage_in[i]);
             if (p->h2d_done[i]) cudaEventDestroy(p->h2d_done[i]);
             if (p->in_free[i]) cudaEventDestroy(p->in_free[i]);
+            if (p->out_ready[i]) cudaEventDestroy(p->out_ready[i]);
+            if (p->out_free[i]) cudaEventDestroy(p->out_free[i]);
         }
         cudaFree(p->stage_out1);
         cudaFree(p->cfl_hist);
         cudaFreeHost(p->h_cfl_hist);
         if (p->cst) cudaStreamDestroy(p->cst);
+        if (p->dst) cudaStreamDestroy(p->dst);
         p->tile_cost = nullptr;
         p->tile_order = nullptr;
         p->tile_cap = 0;
@@ -930,11 +935,14 @@ int patch_enqueue_step(claw2_patch* p, double dt) {
 int host_pipe_reserve(claw2_patch* p, int nsteps) {
     const size_t n = (size_t)p->d.num_eqn * p->d.mx * p->d.my;
     if (!p->cst) {
-        bool ok = cudaStreamCreateWithFlags(&p->cst, cudaStreamNonBlocking) == cudaSuccess;
+        bool ok = cudaStreamCreateWithFlags(&p->cst, cudaStreamNonBlocking) == cudaSuccess &&
+                  cudaStreamCreateWithFlags(&p->dst, cudaStreamNonBlocking) == cudaSuccess;
         for (int i = 0; i < 2 && ok; ++i)
             ok = cudaMalloc(&p->stage_in[i], n * 8) == cudaSuccess &&
                  cudaEventCreateWithFlags(&p->h2d_done[i], cudaEventDisableTiming) == cudaSuccess &&
-                 cudaEventCreateWithFlags(&p->in_free[i], cudaEventDisableTiming) == cudaSuccess;
+                 cudaEventCreateWithFlags(&p->in_free[i], cudaEventDisableTiming) == cudaSuccess &&
+                 cudaEventCreateWithFlags(&p->out_ready[i], cudaEventDisableTiming) == cudaSuccess &&
+                 cudaEventCreateWithFlags(&p->out_free[i], cudaEventDisableTiming) == cudaSuccess;
         ok = ok && cudaMalloc(&p->stage_out1, n * 8) == cudaSuccess;
         if (!ok) {
             cudaGetLastError();
@@ -984,9 +992,11 @@ int claw2_patch_run_host(claw2_patch* p, int nsteps, const double* const* q_in, 
     const size_t n = (size_t)p->d.num_eqn * p->d.mx * p->d.my;
     const long long cells = (long long)p->d.mx * p->d.my;
     double* stage_out[2] = {p->stage, p->stage_out1};
-    // both input buffers start free; the first input goes up at once
-    CUDA_TRY(cudaEventRecord(p->in_free[0], p->st));
-    CUDA_TRY(cudaEventRecord(p->in_free[1], p->st));
+    // all staging buffers start free; the first input goes up at once
+    for (int i = 0; i < 2; ++i) {
+        CUDA_TRY(cudaEventRecord(p->in_free[i], p->st));
+        CUDA_TRY(cudaEventRecord(p->out_free[i], p->st));
+    }
     CUDA_TRY(cudaStreamWaitEvent(p->cst, p->in_free[0], 0));
     CUDA_TRY(cudaMemcpyAsync(p->stage_in[0], q_in[0], n * 8, cudaMemcpyHostToDevice, p->cst));
     CUDA_TRY(cudaEventRecord(p->h2d_done[0], p->cst));
@@ -1007,14 +1017,22 @@ int claw2_patch_run_host(claw2_patch* p, int nsteps, const double* const* q_in, 
                                  p->st));
         p->cur ^= 1;  // accepted
         p->pending = false;
+        // the result goes down on the download stream while the next step computes
+        CUDA_TRY(cudaStreamWaitEvent(p->st, p->out_free[s], 0));
         k_planes_to_aos<<<grid_blocks(cells), 256, 0, p->st>>>(p->q[p->cur], stage_out[s], p->L, p->d.num_eqn, 0);
-        CUDA_TRY(cudaMemcpyAsync(q_out[k], stage_out[s], n * 8, cudaMemcpyDeviceToHost, p->st));
+        CUDA_TRY(cudaEventRecord(p->out_ready[s], p->st));
+        CUDA_TRY(cudaStreamWaitEvent(p->dst, p->out_ready[s], 0));
+        CUDA_TRY(cudaMemcpyAsync(q_out[k], stage_out[s], n * 8, cudaMemcpyDeviceToHost, p->dst));
+        CUDA_TRY(cudaEventRecord(p->out_free[s], p->dst));
     }
     CUDA_TRY(cudaMemcpyAsync(p->h_cfl_hist, p->cfl_hist, sizeof(unsigned long long) * nsteps,
                              cudaMemcpyDeviceToHost, p->st));
     CUDA_TRY(cudaMemcpyAsync(p->h_status, p->status, sizeof(int), cudaMemcpyDeviceToHost, p->st));
     CUDA_TRY(cudaStreamSynchronize(p->st));
     CUDA_TRY(cudaStreamSynchronize(p->cst));
+    CUDA_TRY(cudaStreamSynchronize(p->dst));
+    // later work on the patch's stream must not overtake the last download
+    CUDA_TRY(cudaStreamWaitEvent(p->st, p->out_free[(nsteps - 1) & 1], 0));
     for (int k = 0; k < nsteps; ++k) std::memcpy(&cfl_out[k], &p->h_cfl_hist[k], sizeof(double));
     if (*p->h_status & 1) {
         cudaMemsetAsync(p->status, 0, sizeof(int), p->st);

@@ -73,7 +73,8 @@ class DevicePatch(object):
         """Independent steps from host arrays: q_out[k] = step of q_in[k] with
         dt[k] (claw2_patch_run_host; copies overlap compute).  q_in / q_out
         are lists of (num_eqn, mx, my) Fortran-order float64 arrays (pinned
-        for overlap).  Returns the Courant numbers."""
+        for overlap); an input must not be an earlier step's output array.
+        Returns the Courant numbers."""
         n = len(q_in)
         if len(q_out) != n or len(dt) != n:
             raise ValueError("q_in, q_out and dt need one entry per step")

@@ -103,6 +103,19 @@ def test_stepwise_euler_quadrants(oracle):
     _stepwise(oracle, claw, nsteps=40)
 
 
+def test_stepwise_euler_on_the_longest_first_schedule(oracle):
+    # 640^2 gives 6 strips x 72 row blocks = 432 tiles, more than the 296 CTA
+    # slots, so the step kernel runs on the measured-cost tile schedule (sorted
+    # after the first step and every fourth step); results must not depend on it
+    import os
+    from pyclaw_b200 import tune
+    tune.set_shape(_lib.RP_EULER_ROE, 0, 0)  # the heuristic row height (9 rows here)
+    oracle.set_threads(os.cpu_count() or 1)
+    claw = workloads.euler_quadrants_unsplit(n=640)
+    _stepwise(oracle, claw, nsteps=7)
+    oracle.set_threads(1)
+
+
 def test_stepwise_shallow_dam_break(oracle):
     claw = workloads.shallow_dam_break_unsplit(n=192)
     _stepwise(oracle, claw, nsteps=30)
