@@ -87,7 +87,7 @@ static __global__ void k_batch_bc(const BatchArgs b, int first, int bcl0, int bc
 
 template <class RP, int NT, int MINB, int SPEC>
 __global__ void __launch_bounds__(NT, MINB) k_batch_step(const BatchArgs b, int first, int count) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     UnsplitSmem<RP, NT>& S = *reinterpret_cast<UnsplitSmem<RP, NT>*>(smem_raw);
     const int end = min(first + count, b.ntiles);
     for (int w = first + blockIdx.x; w < end; w += gridDim.x) {

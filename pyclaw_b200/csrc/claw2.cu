@@ -4,6 +4,8 @@
 // behaviour mapped to status codes, the device-resident patch (two q buffers,
 // CFL and status words, one stream), and the stateless replacements of the
 // f2py step2/step2ds routines.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -88,6 +90,46 @@ Layout make_layout(int mx, int my) {
     return L;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the
+// library links only the CUDA runtime); nullptr when unavailable.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static std::mutex mu;
+    static bool tried = false;
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!tried) {
+        tried = true;
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+// TMA descriptor of one q buffer for the row staging of the unsplit kernel:
+// 3D (columns mx+4, rows my+4, components) with the padded layout's strides,
+// box = one row of one strip (NT columns) over all components; columns past
+// mx+3 read as zeros.  The kernel's box x coordinates are strip*(NT-4), so
+// x * 8 bytes is a multiple of 16 as a tiled copy requires.
+template <int NT>
+bool make_row_tmap(CUtensorMap* tm, double* q, const Layout& L, int meqn) {
+    static_assert(((NT - 4) * 8) % 16 == 0, "strip starts must be 16-byte aligned");
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc || ((unsigned long long)q & 15ull)) return false;
+    cuuint64_t dims[3] = {(cuuint64_t)(L.mx + 4), (cuuint64_t)(L.my + 4), (cuuint64_t)meqn};
+    cuuint64_t strides[2] = {(cuuint64_t)L.pitch * 8, (cuuint64_t)L.plane * 8};
+    cuuint32_t box[3] = {(cuuint32_t)NT, 1, (cuuint32_t)meqn};
+    cuuint32_t estr[3] = {1, 1, 1};
+    return enc(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, q, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 int pick_rows(int nstrips, int nrows) {
     // about three CTAs per SM on a 148-SM part, 8..64 rows per CTA
     const int want_blocks = std::max(1, (3 * 148 + nstrips - 1) / nstrips);
@@ -112,7 +154,7 @@ void smem_attr(K kernel, int bytes, unsigned long long& done) {
 // (0 = heuristic).  Chosen per call by the tuning table (claw2_tune_set /
 // claw2_autotune) or the heuristic default.
 struct UnsplitShape {
-    int variant;  // 0: 2 blocks/SM (no register cap), 1: 3 blocks/SM
+    int variant;  // bit 0: 3 blocks/SM (register cap) instead of 2; bit 1: TMA row staging
     int rows;
 };
 
@@ -126,8 +168,16 @@ bool is_mc2(const Method& m, int mwaves) {
     return true;
 }
 
+// tm: the tensor map of qold for the TMA-staged kernel, or nullptr
 template <class RP, int MB, int SPEC>
-void launch_unsplit_s(const StepArgs& b, dim3 grid, cudaStream_t st) {
+void launch_unsplit_s(const StepArgs& b, dim3 grid, cudaStream_t st, const CUtensorMap* tm) {
+    if (tm) {
+        constexpr int smem = (int)sizeof(UnsplitSmemTma<RP, NT_UNSPLIT>);
+        static unsigned long long attr = 0;
+        smem_attr(k_step_unsplit_tma<RP, NT_UNSPLIT, MB, SPEC>, smem, attr);
+        k_step_unsplit_tma<RP, NT_UNSPLIT, MB, SPEC><<<grid, NT_UNSPLIT, smem, st>>>(b, *tm);
+        return;
+    }
     constexpr int smem = (int)sizeof(UnsplitSmem<RP, NT_UNSPLIT>);
     static unsigned long long attr = 0;
     smem_attr(k_step_unsplit<RP, NT_UNSPLIT, MB, SPEC>, smem, attr);
@@ -145,7 +195,7 @@ void unsplit_tiling(int riemann, int mx, int my, int& nstrips, int& H, int& nblo
 }
 
 template <class RP, int MB>
-void launch_unsplit_v(const StepArgs& a, cudaStream_t st) {
+void launch_unsplit_v(const StepArgs& a, cudaStream_t st, const CUtensorMap* tm) {
     StepArgs b = a;
     int ns, H, nb;
     unsplit_tiling(RP::ID, a.L.mx, a.L.my, ns, H, nb);
@@ -155,15 +205,18 @@ void launch_unsplit_v(const StepArgs& a, cudaStream_t st) {
     }
     const int nbk = (a.L.my + b.H - 1) / b.H;
     dim3 grid(b.nstrips * nbk);
-    if (is_mc2(a.meth, RP::MWAVES)) launch_unsplit_s<RP, MB, SPEC_MC2>(b, grid, st);
-    else launch_unsplit_s<RP, MB, SPEC_ANY>(b, grid, st);
+    if (is_mc2(a.meth, RP::MWAVES)) launch_unsplit_s<RP, MB, SPEC_MC2>(b, grid, st, tm);
+    else launch_unsplit_s<RP, MB, SPEC_ANY>(b, grid, st, tm);
 }
 
+// Variants: bit 0 = 3 blocks per SM (register cap) instead of 2, bit 1 = rows
+// staged by TMA (only where the caller has a tensor map of qold).
 template <class RP>
-void launch_unsplit(const StepArgs& a, cudaStream_t st) {
+void launch_unsplit(const StepArgs& a, cudaStream_t st, const CUtensorMap* tm) {
     const UnsplitShape sh = g_tune[RP::ID & 7];
-    if (sh.variant == 1) launch_unsplit_v<RP, 3>(a, st);
-    else launch_unsplit_v<RP, 2>(a, st);
+    const CUtensorMap* use = (sh.variant & 2) ? tm : nullptr;
+    if (sh.variant & 1) launch_unsplit_v<RP, 3>(a, st, use);
+    else launch_unsplit_v<RP, 2>(a, st, use);
 }
 
 template <class RP>
@@ -201,7 +254,9 @@ int dispatch(int rp, A&&... args) {
 }
 template <class RP>
 struct UnsplitF {
-    static void run(const StepArgs& a, cudaStream_t st) { launch_unsplit<RP>(a, st); }
+    static void run(const StepArgs& a, cudaStream_t st, const CUtensorMap* tm = nullptr) {
+        launch_unsplit<RP>(a, st, tm);
+    }
 };
 template <class RP>
 struct SplitF {
@@ -629,6 +684,8 @@ struct claw2_patch {
     unsigned long long* h_cfl_hist = nullptr;
     int cfl_hist_cap = 0;
     int nsm = 0;                  // SMs of the patch's device
+    CUtensorMap tmap[2];          // TMA descriptors of q[0], q[1]
+    bool has_tmap = false;
     int cur = 0;
     bool pending = false;
 };
@@ -818,6 +875,8 @@ int claw2_patch_create(const claw2_desc* d, claw2_patch** out) {
         claw2_patch_destroy(p);
         return fail(CLAW2_ENOMEM, "device allocation for a %dx%d patch failed", d->mx, d->my);
     }
+    p->has_tmap = make_row_tmap<NT_UNSPLIT>(&p->tmap[0], p->q[0], p->L, me) &&
+                  make_row_tmap<NT_UNSPLIT>(&p->tmap[1], p->q[1], p->L, me);
     // zero everything once so padding and ghost cells are defined
     cudaMemsetAsync(p->q[0], 0, nb, p->st);
     cudaMemsetAsync(p->q[1], 0, nb, p->st);
@@ -921,7 +980,7 @@ int patch_enqueue_step(claw2_patch* p, double dt) {
             a.tile_order = p->tile_order;
             a.tile_cost = p->tile_cost;
         }
-        dispatch<UnsplitF>(p->d.riemann, a, p->st);
+        dispatch<UnsplitF>(p->d.riemann, a, p->st, p->has_tmap ? &p->tmap[p->cur] : nullptr);
     }
     if (p->timing) CUDA_TRY(cudaEventRecord(p->ev1, p->st));
     if (lpt_n > 0 && (p->tile_steps++ % LPT_EVERY) == 0) launch_lpt(p->tile_cost, p->tile_order, lpt_n, p->st);
@@ -1034,6 +1093,10 @@ int claw2_patch_run_host(claw2_patch* p, int nsteps, const double* const* q_in, 
     // later work on the patch's stream must not overtake the last download
     CUDA_TRY(cudaStreamWaitEvent(p->st, p->out_free[(nsteps - 1) & 1], 0));
     for (int k = 0; k < nsteps; ++k) std::memcpy(&cfl_out[k], &p->h_cfl_hist[k], sizeof(double));
+    if (*p->h_status & 2) {
+        cudaMemsetAsync(p->status, 0, sizeof(int), p->st);
+        return fail(CLAW2_ETIMEOUT, "a TMA row copy did not complete within the kernel's wait bound");
+    }
     if (*p->h_status & 1) {
         cudaMemsetAsync(p->status, 0, sizeof(int), p->st);
         return fail(CLAW2_ENONFINITE, "a step produced a non-finite value");
@@ -1058,6 +1121,10 @@ int claw2_patch_cfl(claw2_patch* p, double* cfl) {
     double c;
     std::memcpy(&c, p->h_cfl, sizeof c);
     *cfl = c;
+    if (*p->h_status & 2) {
+        cudaMemsetAsync(p->status, 0, sizeof(int), p->st);
+        return fail(CLAW2_ETIMEOUT, "a TMA row copy did not complete within the kernel's wait bound");
+    }
     if (*p->h_status & 1) {
         cudaMemsetAsync(p->status, 0, sizeof(int), p->st);
         return fail(CLAW2_ENONFINITE, "the step produced a non-finite value");
@@ -1070,6 +1137,10 @@ int claw2_patch_sync(claw2_patch* p) {
     DeviceGuard g(p->device);
     CUDA_TRY(cudaMemcpyAsync(p->h_status, p->status, sizeof(int), cudaMemcpyDeviceToHost, p->st));
     CUDA_TRY(cudaStreamSynchronize(p->st));
+    if (*p->h_status & 2) {
+        cudaMemsetAsync(p->status, 0, sizeof(int), p->st);
+        return fail(CLAW2_ETIMEOUT, "a TMA row copy did not complete within the kernel's wait bound");
+    }
     if (*p->h_status & 1) {
         cudaMemsetAsync(p->status, 0, sizeof(int), p->st);
         return fail(CLAW2_ENONFINITE, "a step produced a non-finite value");
@@ -1150,7 +1221,7 @@ int claw2_selftest_rcp(int device, int n, unsigned long long seed, double* max_u
 
 int claw2_tune_set(int riemann, int variant, int rows) {
     if (riemann < 1 || riemann > 7) return fail(CLAW2_EINVAL, "unknown Riemann solver id %d", riemann);
-    if (variant < 0 || variant > 1) return fail(CLAW2_EINVAL, "variant must be 0 or 1 (got %d)", variant);
+    if (variant < 0 || variant > 3) return fail(CLAW2_EINVAL, "variant must be 0..3 (got %d)", variant);
     if (rows < 0 || rows > 4096) return fail(CLAW2_EINVAL, "rows must be 0..4096 (got %d)", rows);
     g_tune[riemann & 7].variant = variant;
     g_tune[riemann & 7].rows = rows;

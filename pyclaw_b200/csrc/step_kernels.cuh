@@ -25,6 +25,8 @@
 // only the order in which the increments of a cell are summed differs.
 #pragma once
 
+#include <cuda.h>
+
 #include "riemann.cuh"
 
 namespace claw2 {
@@ -151,6 +153,50 @@ __device__ __forceinline__ double iface_cfl(const typename RP::Iface& f, const R
 }
 
 // ---------------------------------------------------------------------------
+// TMA row staging: one thread per CTA copies the next row of a strip (NT
+// columns x 1 row x num_eqn planes) from a 3D tensor map of the q planes into
+// shared memory; an mbarrier (one arrival + the copy's bytes) signals it.
+// Waits are bounded: a copy that does not land within the bound sets status
+// bit 1 (the host reports CLAW2_ETIMEOUT) and the kernel carries on.
+// ---------------------------------------------------------------------------
+constexpr int MBAR_SPIN_LIMIT = 1 << 20;
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// true when the phase with the given parity has completed
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+    const unsigned addr = smem_u32(bar);
+    for (int i = 0; i < MBAR_SPIN_LIMIT; ++i) {
+        unsigned done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(done)
+            : "r"(addr), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// Issue the copy of the box at (x, y, 0) into dst and arm the barrier with its
+// size.  x must be a multiple of 2 (16 bytes of doubles); dst 128-byte aligned.
+__device__ __forceinline__ void tma_row(const CUtensorMap* tm, double* dst, unsigned long long* bar, int x, int y,
+                                        unsigned bytes) {
+    const unsigned b = smem_u32(bar);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes) : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(smem_u32(dst)),
+        "l"(tm), "r"(x), "r"(y), "r"(0), "r"(b)
+        : "memory");
+}
+
+// ---------------------------------------------------------------------------
 // Unsplit step (step2.f90), fused x + y sweeps.
 // ---------------------------------------------------------------------------
 template <class RP, int NT>
@@ -163,13 +209,25 @@ struct UnsplitSmem {
     double red[NT / 32];
 };
 
+// The TMA form's extra shared memory: the staged row (first, 128-byte
+// aligned for the copy) and its barrier.
+template <class RP, int NT>
+struct UnsplitSmemTma {
+    alignas(128) double qrow[RP::MEQN][NT];
+    unsigned long long bar;
+    UnsplitSmem<RP, NT> s;
+};
+
 // One tile: the strip `strip` (columns strip*W .. strip*W+NT-1, padded) and
 // the interior rows [rb, rb + H) of one grid.  Returns this thread's CFL
 // contribution in `cfl`; the caller reduces it (the tile ends with every
 // shared-memory read done, so a persistent CTA can start the next tile).
+// With a tensor map (tm != nullptr; qrow and bar in shared memory) the rows
+// are staged by TMA, else each thread loads its column a row ahead.
 template <class RP, int NT, int SPEC = SPEC_ANY>
 __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int rb, UnsplitSmem<RP, NT>& S,
-                                             double& cfl) {
+                                             double& cfl, const CUtensorMap* tm = nullptr, double* qrow = nullptr,
+                                             unsigned long long* bar = nullptr) {
     constexpr int ME = RP::MEQN, MW = RP::MWAVES, NC = RP::NC, W = NT - 4;
     using Iface = typename RP::Iface;
 
@@ -194,14 +252,24 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
     const double* qo = a.qold + cpl;
     double* qn = a.qnew + cpl;
 
+    // (the copy needs a 128-byte aligned destination; anything else loads directly)
+    const bool tma = (tm != nullptr) && ((smem_u32(qrow) & 127u) == 0);
+    const int x0 = strip * W;                                     // first column of the strip
+    const unsigned row_bytes = (unsigned)(ME * NT * sizeof(double));
+    const int tq = cpl - x0;                                      // this thread's staged column
     double pf[ME];
     double accA[ME], accB[ME], accC[ME], accD[ME];  // rows R-2, R-1, R, R+1
     Iface fY;                                       // y-interface (R-2 | R-1)
     double amY[ME], apY[ME], dY[MW];
     unsigned long long n_it = 0, n_solve = 0;
+    if (tma) {
+        if (t == 0) mbar_init(bar);
+        __syncthreads();
+        if (t == 0) tma_row(tm, qrow, bar, x0, R0, row_bytes);
+    }
 #pragma unroll
     for (int m = 0; m < ME; ++m) {
-        pf[m] = __ldg(qo + m * plane + (long long)R0 * pitch);
+        pf[m] = tma ? 0.0 : __ldg(qo + m * plane + (long long)R0 * pitch);
         accA[m] = accB[m] = accC[m] = accD[m] = 0.0;
         amY[m] = apY[m] = 0.0;
     }
@@ -214,17 +282,28 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
         // ---- row R: prepare this column's cell, prefetch the next row ----
         {
             double q[ME], c[NC];
+            if (tma) {
+                if (!mbar_wait(bar, (unsigned)(R - R0) & 1u)) atomicOr(a.status, 2);
 #pragma unroll
-            for (int m = 0; m < ME; ++m) q[m] = pf[m];
-            if (R < R1) {
+                for (int m = 0; m < ME; ++m) q[m] = qrow[m * NT + tq];
+            } else {
 #pragma unroll
-                for (int m = 0; m < ME; ++m) pf[m] = __ldg(qo + m * plane + (long long)(R + 1) * pitch);
+                for (int m = 0; m < ME; ++m) q[m] = pf[m];
+                if (R < R1) {
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) pf[m] = __ldg(qo + m * plane + (long long)(R + 1) * pitch);
+                }
             }
             RP::prepare(q, P, c);
 #pragma unroll
             for (int k = 0; k < NC; ++k) S.cell[s2][k][t] = c[k];
         }
         __syncthreads();  // S1: cells of row R visible; previous exchange consumed
+        if (tma && t == 0 && R < R1) {
+            // every thread has read row R from the staging buffer (before S1)
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            tma_row(tm, qrow, bar, x0, R + 1, row_bytes);
+        }
 
         double ylB[ME], ylA[ME], yrB[ME], yrA[ME];
 #pragma unroll
@@ -434,11 +513,32 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
     if (GuessTraits<RP>::USES && a.counters) counter_commit(a.counters, n_it, n_solve);
 }
 
+// The same kernel with its rows staged by TMA from the tensor map of qold.
+template <class RP, int NT, int MINB, int SPEC>
+__global__ void __launch_bounds__(NT, MINB) k_step_unsplit_tma(const StepArgs a, const __grid_constant__ CUtensorMap tm) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    UnsplitSmemTma<RP, NT>& S = *reinterpret_cast<UnsplitSmemTma<RP, NT>*>(smem_raw);
+    int tile = blockIdx.x;
+    if (a.tile_order) {
+        const int t = a.tile_order[blockIdx.x];
+        if (t >= 0 && t < (int)gridDim.x) tile = t;
+    }
+    long long t0 = 0;
+    if (a.tile_cost && threadIdx.x == 0) t0 = clock64();
+    double cfl = 0.0;
+    unsplit_tile<RP, NT, SPEC>(a, tile % a.nstrips, (tile / a.nstrips) * a.H, S.s, cfl, &tm, &S.qrow[0][0], &S.bar);
+    cfl_commit(cfl, S.s.red, a.cfl_bits);
+    if (a.tile_cost && threadIdx.x == 0) {
+        const long long c = clock64() - t0;
+        a.tile_cost[tile] = (unsigned int)(c < 0 ? 0 : (c > 0xffffffffll ? 0xffffffffll : c));
+    }
+}
+
 // Grid: 1D over the tiles (strip fastest).  Tile t = (strip t % nstrips, row
 // block t / nstrips); CTA b runs tile_order[b] when a schedule is given.
 template <class RP, int NT, int MINB, int SPEC>
 __global__ void __launch_bounds__(NT, MINB) k_step_unsplit(const StepArgs a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     UnsplitSmem<RP, NT>& S = *reinterpret_cast<UnsplitSmem<RP, NT>*>(smem_raw);
     int tile = blockIdx.x;
     if (a.tile_order) {
@@ -516,7 +616,7 @@ template <class RP, int NT>
 __global__ void __launch_bounds__(NT) k_split_x(const StepArgs a) {
     constexpr int ME = RP::MEQN, MW = RP::MWAVES, NC = RP::NC, W = NT - 4;
     using Iface = typename RP::Iface;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     SplitXSmem<RP, NT>& S = *reinterpret_cast<SplitXSmem<RP, NT>*>(smem_raw);
 
     const int t = threadIdx.x;
