@@ -66,6 +66,10 @@ def parse():
     ap.add_argument("--train-problems", type=int, default=1 << 24,
                     help="training-set size of the learned guess (2^24 in the benchmark)")
     ap.add_argument("--epochs", type=int, default=16, help="training epochs of the learned guess")
+    ap.add_argument("--learned-n", type=int, default=2048,
+                    help="grid size of the learned-guess workload (2048 in the benchmark; smaller for profiling)")
+    ap.add_argument("--learned-pre-t", type=float, default=0.4,
+                    help="time the learned-guess workload's state is advanced to (0.4 in the benchmark)")
     ap.add_argument("--state", default=None,
                     help="profiling aid: .npy file of the advanced state; loaded if it exists (no "
                          "advance), else written after the advance")
@@ -297,11 +301,16 @@ def learned_workload(stream, flush, n=2048, steps=10, n_train=1 << 24, epochs=16
         c1 = pe.step(dt)
         pe.accept(False)
         dte = dt * 0.9 / c1
+        # launch shape tuned once on the PVRS run (cached per solver and size,
+        # so the learned run uses the same one)
+        from pyclaw_b200 import tune
+        shape, _ = tune.autotune(pe, dte)
         learned.counters(ce.solver)
         step_ms, kern_ms = time_patch(pe, dte, steps, flush, stream)
         it, ns = learned.counters(ce.solver)
         res[mode] = {"value": n * n / (step_ms * 1e-3), "unit": UNIT, "ms_per_step": step_ms,
-                     "kernel_ms": kern_ms, "newton_per_interface": it / max(ns, 1), "solves": ns}
+                     "kernel_ms": kern_ms, "newton_per_interface": it / max(ns, 1), "solves": ns,
+                     "launch_shape": list(shape)}
         # one step from the same state for the same-answer check
         ce.solution.state.q = q_mid
         pe.push(ce.solution.state)
@@ -370,8 +379,9 @@ def run_one(args):
     elif args.only == "batched_512":
         out = {"batched_quadrants_512": batched_workload(plain=False)}
     else:
-        out = {"learned_exact_euler_2048": learned_workload(stream, flush, n_train=args.train_problems,
-                                                            epochs=args.epochs, pre_t=args.pre_t)}
+        out = {"learned_exact_euler_%d" % args.learned_n: learned_workload(
+            stream, flush, n=args.learned_n, n_train=args.train_problems, epochs=args.epochs,
+            pre_t=args.learned_pre_t)}
     torch.cuda.synchronize()
     print(json.dumps(out), flush=True)
     return 0
