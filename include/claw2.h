@@ -36,7 +36,8 @@ enum {
     CLAW2_RP_ACOUSTICS = 2,    /* acoustics_2D:               {rho, bulk, cc, zz}    */
     CLAW2_RP_EULER_ROE = 3,    /* euler_4wave_2D:             {gamma, efix}          */
     CLAW2_RP_SHALLOW_ROE = 4,  /* shallow_roe_with_efix_2D:   {grav, efix}           */
-    CLAW2_RP_EULER_EXACT = 5   /* exact Euler (no reference counterpart): {gamma, tol, guess} */
+    CLAW2_RP_EULER_EXACT = 5,  /* exact Euler (no reference counterpart): {gamma, tol, guess} */
+    CLAW2_RP_VC_ACOUSTICS = 6  /* vc_acoustics_2D: no cparam; aux = {rho, c} per cell        */
 };
 
 /* Boundary-condition codes: pyclaw.BC (src/pyclaw/solver.py:13-19), plus

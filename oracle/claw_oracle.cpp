@@ -172,6 +172,60 @@ void rpt2_acoustics(int ixy, int mbc, int mx, const Slice& asdq, const Slice& bm
     }
 }
 
+// vc_acoustics_2D: acoustics in a heterogeneous medium, aux = (rho, c) per
+// cell (LeVeque 2002, sec. 9.6 and 21.5.1).  Normal solve: the jump between
+// cells i-1 and i splits into a left-going wave with cell i-1's impedance
+// Z = rho c and speed -c(i-1) and a right-going wave with cell i's impedance
+// and speed c(i).
+void rpn2_vc_acoustics(int ixy, int mbc, int mx, int meqn, const CSlice& ql, const CSlice& qr,
+                       const CSlice& auxl, const CSlice& auxr, const Waves& wave, const Speeds& s,
+                       const Slice& amdq, const Slice& apdq) {
+    const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        double zi = auxl(0, i) * auxl(1, i);
+        double zim = auxr(0, i - 1) * auxr(1, i - 1);
+        double delta1 = ql(0, i) - qr(0, i - 1);
+        double delta2 = ql(mu, i) - qr(mu, i - 1);
+        double a1 = (-delta1 + zi * delta2) / (zim + zi);
+        double a2 = (delta1 + zim * delta2) / (zim + zi);
+        wave(0, 0, i) = -a1 * zim;
+        wave(mu, 0, i) = a1;
+        wave(mv, 0, i) = 0.0;
+        s(0, i) = -auxr(1, i - 1);
+        wave(0, 1, i) = a2 * zi;
+        wave(mu, 1, i) = a2;
+        wave(mv, 1, i) = 0.0;
+        s(1, i) = auxl(1, i);
+    }
+    for (int m = 0; m < meqn; ++m)
+        for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+            amdq(m, i) = s(0, i) * wave(m, 0, i);
+            apdq(m, i) = s(1, i) * wave(m, 1, i);
+        }
+}
+// Transverse solve: asdq belongs to cell i1 (i-1 for imp = 1, i for imp = 2)
+// with impedance zz; its down-going part is transmitted into the cell below
+// (impedance zm, speed -cm) and its up-going part into the cell above (zp, cp).
+void rpt2_vc_acoustics(int ixy, int imp, int mbc, int mx, const CSlice& aux1, const CSlice& aux2,
+                       const CSlice& aux3, const Slice& asdq, const Slice& bmasdq, const Slice& bpasdq) {
+    const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        const int i1 = (imp == 1) ? i - 1 : i;
+        double zm = aux1(0, i1) * aux1(1, i1);
+        double zz = aux2(0, i1) * aux2(1, i1);
+        double zp = aux3(0, i1) * aux3(1, i1);
+        double cm = aux1(1, i1), cp = aux3(1, i1);
+        double a1 = (-asdq(0, i) + asdq(mv, i) * zz) / (zm + zz);
+        double a2 = (asdq(0, i) + asdq(mv, i) * zz) / (zz + zp);
+        bmasdq(0, i) = cm * a1 * zm;
+        bmasdq(mu, i) = 0.0;
+        bmasdq(mv, i) = -cm * a1;
+        bpasdq(0, i) = cp * a2 * zp;
+        bpasdq(mu, i) = 0.0;
+        bpasdq(mv, i) = cp * a2;
+    }
+}
+
 // Euler equations, Roe solver with 4 waves (u-c, entropy, shear, u+c) and an
 // optional Harten-Hyman entropy fix (LeVeque 2002, sec. 15.3.5 and 18.8;
 // Roe 1981).  The wave layout follows the reference's vendored 5-wave solver
@@ -688,10 +742,10 @@ void rpn2_euler_exact(int ixy, int mbc, int mx, int meqn, int mwaves, const CSli
 // ---------------------------------------------------------------------------
 bool rp_known(int rp) {
     return rp == ORC_RP_ADVECTION || rp == ORC_RP_ACOUSTICS || rp == ORC_RP_EULER_ROE ||
-           rp == ORC_RP_SHALLOW_ROE || rp == ORC_RP_EULER_EXACT;
+           rp == ORC_RP_SHALLOW_ROE || rp == ORC_RP_EULER_EXACT || rp == ORC_RP_VC_ACOUSTICS;
 }
 
-void call_rpn2(int rp, int ixy, int mbc, int mx, int meqn, int mwaves, const CSlice& q,
+void call_rpn2(int rp, int ixy, int mbc, int mx, int meqn, int mwaves, const CSlice& q, const CSlice& aux2,
                const Waves& wave, const Speeds& s, const Slice& amdq, const Slice& apdq,
                const double* cp) {
     switch (rp) {
@@ -700,11 +754,14 @@ void call_rpn2(int rp, int ixy, int mbc, int mx, int meqn, int mwaves, const CSl
         case ORC_RP_EULER_ROE: rpn2_euler_roe(ixy, mbc, mx, meqn, mwaves, q, q, wave, s, amdq, apdq, cp); break;
         case ORC_RP_SHALLOW_ROE: rpn2_shallow_roe(ixy, mbc, mx, meqn, mwaves, q, q, wave, s, amdq, apdq, cp); break;
         case ORC_RP_EULER_EXACT: rpn2_euler_exact(ixy, mbc, mx, meqn, mwaves, q, q, wave, s, amdq, apdq, cp); break;
+        case ORC_RP_VC_ACOUSTICS: rpn2_vc_acoustics(ixy, mbc, mx, meqn, q, q, aux2, aux2, wave, s, amdq, apdq); break;
     }
 }
-void call_rpt2(int rp, int ixy, int mbc, int mx, int meqn, int mwaves, const CSlice& q,
+void call_rpt2(int rp, int ixy, int imp, int mbc, int mx, int meqn, int mwaves, const CSlice& q,
+               const CSlice& aux1, const CSlice& aux2, const CSlice& aux3,
                const Slice& asdq, const Slice& bm, const Slice& bp, const double* cp) {
     switch (rp) {
+        case ORC_RP_VC_ACOUSTICS: rpt2_vc_acoustics(ixy, imp, mbc, mx, aux1, aux2, aux3, asdq, bm, bp); break;
         case ORC_RP_ADVECTION: rpt2_advection(ixy, mbc, mx, asdq, bm, bp, cp); break;
         case ORC_RP_ACOUSTICS: rpt2_acoustics(ixy, mbc, mx, asdq, bm, bp, cp); break;
         case ORC_RP_EULER_ROE: rpt2_euler_roe(ixy, mbc, mx, meqn, mwaves, q, q, asdq, bm, bp, cp); break;
@@ -716,11 +773,16 @@ void call_rpt2(int rp, int ixy, int mbc, int mx, int meqn, int mwaves, const CSl
 // Per-slice scratch (the reference's `work` partition, step2.f90:53-71, plus
 // the optional q1d/qadd/fadd/gadd/dtdx1d arrays).
 struct Work {
-    int n;  // maxm + 2*mbc
+    int n;     // maxm + 2*mbc
+    int maux;  // aux components per cell (>= 1 so the slices exist)
     std::vector<double> q1d, qadd, fadd, gadd, dtdx1d, dtdy1d, wave, s, amdq, apdq, cqxx,
-        bmasdq, bpasdq;
-    Work(int maxm, int mbc, int meqn, int mwaves) {
+        bmasdq, bpasdq, aux1, aux2, aux3;
+    Work(int maxm, int mbc, int meqn, int mwaves, int maux_ = 0) {
         n = maxm + 2 * mbc;
+        maux = maux_ > 0 ? maux_ : 1;
+        aux1.assign((size_t)n * maux, 0.0);
+        aux2.assign((size_t)n * maux, 0.0);
+        aux3.assign((size_t)n * maux, 0.0);
         q1d.assign((size_t)n * meqn, 0.0);
         qadd.assign((size_t)n * meqn, 0.0);
         fadd.assign((size_t)n * meqn, 0.0);
@@ -753,6 +815,7 @@ void flux2(int ixy, int mbc, int mx, int meqn, int mwaves, Work& w, const int* m
     Speeds s{w.s.data(), mwaves, mbc};
     auto dtdx1d = [&](int i) -> double& { return w.dtdx1d[(size_t)(i + mbc - 1)]; };
     CSlice q{w.q1d.data(), meqn, mbc};
+    CSlice a1{w.aux1.data(), w.maux, mbc}, a2{w.aux2.data(), w.maux, mbc}, a3{w.aux3.data(), w.maux, mbc};
 
     bool limit = false;
     for (int mw = 0; mw < mwaves; ++mw)
@@ -769,7 +832,7 @@ void flux2(int ixy, int mbc, int mx, int meqn, int mwaves, Work& w, const int* m
     (void)q1d;
 
     // flux2.f90:101
-    call_rpn2(rp, ixy, mbc, mx, meqn, mwaves, q, wave, s, amdq, apdq, cp);
+    call_rpn2(rp, ixy, mbc, mx, meqn, mwaves, q, a2, wave, s, amdq, apdq, cp);
 
     // flux2.f90:104-108 (forall: first statement over all i, then the second)
     for (int i = 1; i <= mx + 1; ++i)
@@ -814,14 +877,14 @@ void flux2(int ixy, int mbc, int mx, int meqn, int mwaves, Work& w, const int* m
     }
 
     // flux2.f90:181-190
-    call_rpt2(rp, ixy, mbc, mx, meqn, mwaves, q, amdq, bmasdq, bpasdq, cp);
+    call_rpt2(rp, ixy, 1, mbc, mx, meqn, mwaves, q, a1, a2, a3, amdq, bmasdq, bpasdq, cp);
     for (int i = 1; i <= mx + 1; ++i)
         for (int m = 0; m < meqn; ++m) gadd(m, 0, i - 1) = gadd(m, 0, i - 1) - 0.5 * dtdx1d(i - 1) * bmasdq(m, i);
     for (int i = 1; i <= mx + 1; ++i)
         for (int m = 0; m < meqn; ++m) gadd(m, 1, i - 1) = gadd(m, 1, i - 1) - 0.5 * dtdx1d(i - 1) * bpasdq(m, i);
 
     // flux2.f90:194-203
-    call_rpt2(rp, ixy, mbc, mx, meqn, mwaves, q, apdq, bmasdq, bpasdq, cp);
+    call_rpt2(rp, ixy, 2, mbc, mx, meqn, mwaves, q, a1, a2, a3, apdq, bmasdq, bpasdq, cp);
     for (int i = 1; i <= mx + 1; ++i)
         for (int m = 0; m < meqn; ++m) gadd(m, 0, i) = gadd(m, 0, i) - 0.5 * dtdx1d(i) * bmasdq(m, i);
     for (int i = 1; i <= mx + 1; ++i)
@@ -872,7 +935,7 @@ int oracle_step2(int maxm, int meqn, int mwaves, int maux, int mbc, int mx, int 
 #pragma omp parallel num_threads(nthr) reduction(max : cfl_s) if (nthr > 1)
 #endif
             {
-                Work w(maxm, mbc, meqn, mwaves);
+                Work w(maxm, mbc, meqn, mwaves, maux);
 #ifdef _OPENMP
 #pragma omp for schedule(static)
 #endif
@@ -890,6 +953,15 @@ int oracle_step2(int maxm, int meqn, int mwaves, int maux, int mbc, int mx, int 
                         for (int i = 1 - mbc; i <= n + mbc; ++i)
                             w.dtdx1d[(size_t)(i + mbc - 1)] =
                                 d_norm / ((ixy == 1) ? aux(index_capa - 1, i, js) : aux(index_capa - 1, js, i));
+                    // step2.f90: aux1/aux2/aux3 = the aux slices below, at and above this one
+                    if (maux > 0)
+                        for (int ma = 0; ma < maux; ++ma)
+                            for (int i = 1 - mbc; i <= n + mbc; ++i) {
+                                const size_t o = (size_t)(i + mbc - 1) * w.maux + ma;
+                                w.aux1[o] = (ixy == 1) ? aux(ma, i, js - 1) : aux(ma, js - 1, i);
+                                w.aux2[o] = (ixy == 1) ? aux(ma, i, js) : aux(ma, js, i);
+                                w.aux3[o] = (ixy == 1) ? aux(ma, i, js + 1) : aux(ma, js + 1, i);
+                            }
                     double c1d = 0.0;
                     flux2(ixy, mbc, n, meqn, mwaves, w, method, mthlim, &c1d, use_fwave != 0, rp, cp);
                     cfl_s = std::max(cfl_s, c1d);
@@ -968,7 +1040,7 @@ int oracle_step2ds(int maxm, int meqn, int mwaves, int maux, int mbc, int mx, in
 #pragma omp parallel num_threads(nthr) reduction(max : cfl) if (nthr > 1)
 #endif
     {
-        Work w(maxm, mbc, meqn, mwaves);
+        Work w(maxm, mbc, meqn, mwaves, maux);
 #ifdef _OPENMP
 #pragma omp for schedule(static)
 #endif
@@ -981,6 +1053,11 @@ int oracle_step2ds(int maxm, int meqn, int mwaves, int maux, int mbc, int mx, in
                 for (int i = 1 - mbc; i <= n + mbc; ++i)
                     w.dtdx1d[(size_t)(i + mbc - 1)] =
                         d_norm / ((ixy == 1) ? aux(index_capa - 1, i, k) : aux(index_capa - 1, k, i));
+            // the split sweep's Riemann solves see this slice's aux (no transverse solves)
+            if (maux > 0)
+                for (int ma = 0; ma < maux; ++ma)
+                    for (int i = 1 - mbc; i <= n + mbc; ++i)
+                        w.aux2[(size_t)(i + mbc - 1) * w.maux + ma] = (ixy == 1) ? aux(ma, i, k) : aux(ma, k, i);
             double c1d = 0.0;
             flux2(ixy, mbc, n, meqn, mwaves, w, method, mthlim, &c1d, use_fwave != 0, rp, cp);
             cfl = std::max(cfl, c1d);
@@ -1005,9 +1082,13 @@ int oracle_step2ds(int maxm, int meqn, int mwaves, int maux, int mbc, int mx, in
 // solver.py:351-519 for q: dimension 0 lower, upper, then dimension 1 lower,
 // upper; each dimension fills its ghost layers across the full extent of the
 // other index (so corners come from the dimension-1 pass).
-int oracle_bc_fill(int meqn, int mbc, int mx, int my, double* qbc, const int* bcl, const int* bcu) {
+}  // extern "C"
+
+namespace {
+// negate: q (a wall negates the normal momentum) or aux (plain mirror)
+int bc_fill(int meqn, int mbc, int mx, int my, double* qbc, const int* bcl, const int* bcu, bool negate) {
     Grid2 q{qbc, meqn, mbc, mx};
-    const int reflect[2] = {1, 2};
+    const int reflect[2] = {negate ? 1 : -1, negate ? 2 : -1};
     for (int idim = 0; idim < 2; ++idim) {
         const int n = idim == 0 ? mx : my;
         const int lo_other = 1 - mbc, hi_other = (idim == 0 ? my : mx) + mbc;
@@ -1040,6 +1121,38 @@ int oracle_bc_fill(int meqn, int mbc, int mx, int my, double* qbc, const int* bc
             }
         }
     }
+    return 0;
+}
+}  // namespace
+
+extern "C" {
+
+int oracle_bc_fill(int meqn, int mbc, int mx, int my, double* qbc, const int* bcl, const int* bcu) {
+    return bc_fill(meqn, mbc, mx, my, qbc, bcl, bcu, true);
+}
+
+int oracle_bc_fill_aux(int maux, int mbc, int mx, int my, double* auxbc, const int* bcl, const int* bcu) {
+    return bc_fill(maux, mbc, mx, my, auxbc, bcl, bcu, false);
+}
+
+int oracle_rpn2_aux(int rp, int ixy, int maxm, int meqn, int mwaves, int maux, int mbc, int mx, const double* q,
+                    const double* aux, double* wave, double* s, double* amdq, double* apdq, const double* cp) {
+    if (!rp_known(rp) || mx > maxm || maux < 1) return 2;
+    CSlice ql{q, meqn, mbc}, a{aux, maux, mbc};
+    Waves w{wave, meqn, mwaves, mbc};
+    Speeds sp{s, mwaves, mbc};
+    Slice am{amdq, meqn, mbc}, ap{apdq, meqn, mbc};
+    call_rpn2(rp, ixy, mbc, mx, meqn, mwaves, ql, a, w, sp, am, ap, cp);
+    return 0;
+}
+
+int oracle_rpt2_aux(int rp, int ixy, int imp, int maxm, int meqn, int mwaves, int maux, int mbc, int mx,
+                    const double* q, const double* aux1, const double* aux2, const double* aux3, const double* asdq,
+                    double* bmasdq, double* bpasdq, const double* cp) {
+    if (!rp_known(rp) || mx > maxm || maux < 1 || (imp != 1 && imp != 2)) return 2;
+    CSlice ql{q, meqn, mbc}, a1{aux1, maux, mbc}, a2{aux2, maux, mbc}, a3{aux3, maux, mbc};
+    Slice as{const_cast<double*>(asdq), meqn, mbc}, bm{bmasdq, meqn, mbc}, bp{bpasdq, meqn, mbc};
+    call_rpt2(rp, ixy, imp, mbc, mx, meqn, mwaves, ql, a1, a2, a3, as, bm, bp, cp);
     return 0;
 }
 

@@ -38,8 +38,7 @@ enum {
     ORC_RP_EULER_ROE = 3,   /* euler_4wave_2D         cparam: gamma, efix     */
     ORC_RP_SHALLOW_ROE = 4, /* shallow_roe_with_efix_2D cparam: grav, efix    */
     ORC_RP_EULER_EXACT = 5, /* exact Euler (new)      cparam: gamma, tol      */
-    ORC_RP_EULER_HLLE = 6,  /* euler_hlle_2D          cparam: gamma           */
-    ORC_RP_SHALLOW_HLLE = 7 /* shallow_hlle_2D        cparam: grav            */
+    ORC_RP_VC_ACOUSTICS = 6 /* vc_acoustics_2D        aux: rho, c; no cparam  */
 };
 
 /* One unsplit step (step2.f90).  qold, qnew: (meqn, mx+2mbc, my+2mbc) F-order;
@@ -65,6 +64,22 @@ int oracle_step2ds(int maxm, int meqn, int mwaves, int maux, int mbc, int mx, in
  * (a halo filled by a neighbouring rank).  reflect_index = {1,2}. */
 int oracle_bc_fill(int meqn, int mbc, int mx, int my, double* qbc,
                    const int* bc_lower, const int* bc_upper);
+
+/* Ghost-cell fill of an aux array (solver.py:439-519 with name != 'q'): as
+ * oracle_bc_fill, but a wall mirrors without negating any component. */
+int oracle_bc_fill_aux(int maux, int mbc, int mx, int my, double* auxbc,
+                       const int* bc_lower, const int* bc_upper);
+
+/* Riemann solvers with aux slices for unit tests: aux (maux, 1-mbc:mx+mbc)
+ * for the slice itself (auxl = auxr), aux1/aux3 for the slices below/above
+ * (rpt2 only), Fortran ABI. */
+int oracle_rpn2_aux(int rp_id, int ixy, int maxm, int meqn, int mwaves, int maux, int mbc, int mx,
+                    const double* q, const double* aux, double* wave, double* s, double* amdq,
+                    double* apdq, const double* cparam);
+int oracle_rpt2_aux(int rp_id, int ixy, int imp, int maxm, int meqn, int mwaves, int maux, int mbc,
+                    int mx, const double* q, const double* aux1, const double* aux2,
+                    const double* aux3, const double* asdq, double* bmasdq, double* bpasdq,
+                    const double* cparam);
 
 /* Direct Riemann-solver access for unit tests: one slice, Fortran ABI. */
 int oracle_rpn2(int rp_id, int ixy, int maxm, int meqn, int mwaves, int mbc, int mx,

@@ -40,6 +40,9 @@ def load():
     lib.oracle_step2.argtypes = [i] * 7 + [_dp, _dp, _dp, d, d, d, _ip, _ip, _dp, i, i, _dp]
     lib.oracle_step2ds.argtypes = [i] * 7 + [_dp, _dp, _dp, d, d, d, _ip, _ip, _dp, i, i, i, _dp]
     lib.oracle_bc_fill.argtypes = [i, i, i, i, _dp, _ip, _ip]
+    lib.oracle_bc_fill_aux.argtypes = [i, i, i, i, _dp, _ip, _ip]
+    lib.oracle_rpn2_aux.argtypes = [i] * 8 + [_dp] * 7
+    lib.oracle_rpt2_aux.argtypes = [i] * 9 + [_dp] * 8
     lib.oracle_rpn2.argtypes = [i] * 7 + [_dp, _dp, _dp, _dp, _dp, _dp, _dp]
     lib.oracle_rpt2.argtypes = [i] * 8 + [_dp, _dp, _dp, _dp, _dp, _dp]
     lib.oracle_exact_star.argtypes = [d] * 8 + [i, _dp, _dp, _ip]
@@ -62,16 +65,18 @@ def set_threads(n):
     load().oracle_set_threads(int(n))
 
 
-def step2(qold, qnew, dx, dy, dt, method, mthlim, rp_id, cparam, use_fwave=False):
-    """Oracle step2 on qbc arrays (meqn, mx+4, my+4) F-order; returns cfl."""
+def step2(qold, qnew, dx, dy, dt, method, mthlim, rp_id, cparam, use_fwave=False, aux=None):
+    """Oracle step2 on qbc arrays (meqn, mx+4, my+4) F-order, optional auxbc
+    (maux, mx+4, my+4) F-order; returns cfl."""
     lib = load()
     meqn, nxg, nyg = qold.shape
     mx, my = nxg - 4, nyg - 4
+    maux, auxp = _aux(aux)
     cfl = ctypes.c_double(0.0)
     cp = np.asarray(list(cparam) + [0.0] * 8, dtype=np.float64)
     method = np.ascontiguousarray(method, dtype=np.intc)
     mthlim = np.ascontiguousarray(mthlim, dtype=np.intc)
-    rc = lib.oracle_step2(max(mx, my), meqn, len(mthlim), 0, 2, mx, my, _d(qold), _d(qnew), None,
+    rc = lib.oracle_step2(max(mx, my), meqn, len(mthlim), maux, 2, mx, my, _d(qold), _d(qnew), auxp,
                           dx, dy, dt, _i(method), _i(mthlim), ctypes.byref(cfl), int(use_fwave),
                           rp_id, _d(cp))
     if rc:
@@ -79,20 +84,38 @@ def step2(qold, qnew, dx, dy, dt, method, mthlim, rp_id, cparam, use_fwave=False
     return cfl.value
 
 
-def step2ds(qold, qnew, dx, dy, dt, method, mthlim, ids, rp_id, cparam, use_fwave=False):
+def step2ds(qold, qnew, dx, dy, dt, method, mthlim, ids, rp_id, cparam, use_fwave=False, aux=None):
     lib = load()
     meqn, nxg, nyg = qold.shape
     mx, my = nxg - 4, nyg - 4
+    maux, auxp = _aux(aux)
     cfl = ctypes.c_double(0.0)
     cp = np.asarray(list(cparam) + [0.0] * 8, dtype=np.float64)
     method = np.ascontiguousarray(method, dtype=np.intc)
     mthlim = np.ascontiguousarray(mthlim, dtype=np.intc)
-    rc = lib.oracle_step2ds(max(mx, my), meqn, len(mthlim), 0, 2, mx, my, _d(qold), _d(qnew), None,
+    rc = lib.oracle_step2ds(max(mx, my), meqn, len(mthlim), maux, 2, mx, my, _d(qold), _d(qnew), auxp,
                             dx, dy, dt, _i(method), _i(mthlim), ctypes.byref(cfl), ids, int(use_fwave),
                             rp_id, _d(cp))
     if rc:
         raise RuntimeError("oracle_step2ds returned %d" % rc)
     return cfl.value
+
+
+def _aux(aux):
+    if aux is None:
+        return 0, None
+    assert aux.flags.f_contiguous and aux.dtype == np.float64
+    return aux.shape[0], _d(aux)
+
+
+def bc_fill_aux(auxbc, bc_lower, bc_upper):
+    """Ghost cells of an aux array (a wall mirrors without sign change)."""
+    lib = load()
+    maux, nxg, nyg = auxbc.shape
+    assert auxbc.flags.f_contiguous
+    rc = lib.oracle_bc_fill_aux(maux, 2, nxg - 4, nyg - 4, _d(auxbc), _i(bc_lower), _i(bc_upper))
+    if rc:
+        raise RuntimeError("oracle_bc_fill_aux returned %d" % rc)
 
 
 def bc_fill(qbc, bc_lower, bc_upper):
@@ -121,6 +144,7 @@ def make_solver_class():
             self._set_method(state)
             mx, my = state.grid.num_cells
             self.qbc = np.zeros((state.num_eqn, mx + 4, my + 4), order='F')
+            self.auxbc = np.zeros((state.num_aux, mx + 4, my + 4), order='F') if state.num_aux else None
             self._is_set_up = True
 
         def _begin_step(self, solution):
@@ -136,14 +160,19 @@ def make_solver_class():
             qbc = self.qbc
             qbc[:, 2:-2, 2:-2] = state._q
             bc_fill(qbc, self.bc_lower, self.bc_upper)
+            aux = None
+            if self.auxbc is not None:  # solver.py:351-437 fills auxbc with qbc every step
+                aux = self.auxbc
+                aux[:, 2:-2, 2:-2] = state.aux
+                bc_fill_aux(aux, self.aux_bc_lower, self.aux_bc_upper)
             qold = qbc.copy('F')
             cp = self.rp.cparam(state.problem_data)
             if self.dimensional_split:
-                c1 = step2ds(qold, qbc, dx, dy, self.dt, self._method, self._mthlim, 1, self.rp.rp_id, cp)
-                c2 = step2ds(qbc, qbc, dx, dy, self.dt, self._method, self._mthlim, 2, self.rp.rp_id, cp)
+                c1 = step2ds(qold, qbc, dx, dy, self.dt, self._method, self._mthlim, 1, self.rp.rp_id, cp, aux=aux)
+                c2 = step2ds(qbc, qbc, dx, dy, self.dt, self._method, self._mthlim, 2, self.rp.rp_id, cp, aux=aux)
                 cfl = max(c1, c2)
             else:
-                cfl = step2(qold, qbc, dx, dy, self.dt, self._method, self._mthlim, self.rp.rp_id, cp)
+                cfl = step2(qold, qbc, dx, dy, self.dt, self._method, self._mthlim, self.rp.rp_id, cp, aux=aux)
             self.cfl.update_global_max(cfl)
             state._q = np.asfortranarray(qbc[:, 2:-2, 2:-2].copy())
 

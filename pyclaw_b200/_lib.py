@@ -16,6 +16,7 @@ CLAW2_MAX_WAVES = 8
 CLAW2_NOALLOC_SCRATCH_BYTES = 32 << 20
 
 RP_ADVECTION, RP_ACOUSTICS, RP_EULER_ROE, RP_SHALLOW_ROE, RP_EULER_EXACT = 1, 2, 3, 4, 5
+RP_VC_ACOUSTICS = 6
 
 OK, EINVAL, ECUDA, ENONFINITE, ETIMEOUT, ENOMEM, EUNSUPPORTED = 0, 1, 2, 3, 4, 5, 6
 

@@ -54,7 +54,12 @@ shallow_roe_with_efix_2D = RiemannSolver('shallow_roe_with_efix_2D', _lib.RP_SHA
 euler_exact_2D = RiemannSolver('euler_exact_2D', _lib.RP_EULER_EXACT, 4, 3, ('gamma',),
                                extra=(('exact_tol', 1e-12),))
 
-_ALL = [advection_2D, acoustics_2D, euler_4wave_2D, shallow_roe_with_efix_2D, euler_exact_2D]
+# Acoustics with variable coefficients: no cparam; aux = (density, sound speed)
+# per cell (clawpack.riemann.vc_acoustics_2D).
+vc_acoustics_2D = RiemannSolver('vc_acoustics_2D', _lib.RP_VC_ACOUSTICS, 3, 2, ())
+vc_acoustics_2D.num_aux = 2
+
+_ALL = [advection_2D, acoustics_2D, euler_4wave_2D, shallow_roe_with_efix_2D, euler_exact_2D, vc_acoustics_2D]
 
 static = types.SimpleNamespace(
     num_eqn={s.name: s.num_eqn for s in _ALL},
@@ -69,3 +74,4 @@ euler_4wave_2D_constants = types.SimpleNamespace(density=0, x_momentum=1, y_mome
 shallow_roe_with_efix_2D_constants = types.SimpleNamespace(depth=0, x_momentum=1, y_momentum=2,
                                                            num_eqn=3)
 acoustics_2D_constants = types.SimpleNamespace(pressure=0, x_velocity=1, y_velocity=2, num_eqn=3)
+vc_acoustics_2D_constants = types.SimpleNamespace(pressure=0, x_velocity=1, y_velocity=2, num_eqn=3)

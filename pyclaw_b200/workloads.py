@@ -8,6 +8,7 @@ bit for bit):
   acoustics_2d_homogeneous  examples/acoustics_2d_homogeneous/acoustics_2d.py:20-106
   quadrants                 examples/euler_2d/quadrants.py:73-126
   radial_dam_break          examples/shallow_2d/radial_dam_break.py:23-87
+  acoustics_variable        examples/acoustics_2d_variable/acoustics_2d_interface.py:23-96
 The benchmark workloads are the acoustics, Euler-quadrant and shallow-water
 dam-break problems at the benchmark sizes (unsplit step, transverse
 corrections, MC limiter).
@@ -178,6 +179,42 @@ def acoustics_wall(solver_class=None, n=200, tfinal=0.6):
     state.q[2, ...] = 0.0
     solver.dt_initial = np.min(domain.grid.delta) / cc * solver.cfl_desired
     return _controller(solver, Solution(state, domain), tfinal)
+
+
+def acoustics_variable(solver_class=None, n=50, tfinal=0.6, num_output_times=20):
+    """Acoustics in two materials (vc_acoustics_2D, aux = density and sound
+    speed): rho = 4, K = 4 for x < 0 and rho = 1, K = 4 for x >= 0 on
+    [-1,1]^2; a pressure ring of radius 0.25 around (-0.5, 0); wall BCs at
+    the lower and extrapolation at the upper sides for q and aux; MC limiter,
+    unsplit with the reference's default transverse mode (trans_inc)."""
+    cls = solver_class or ClawSolver2D
+    solver = cls(riemann.vc_acoustics_2D)
+    solver.dimensional_split = False
+    solver.limiters = tvd.MC
+    solver.bc_lower[0] = BC.wall
+    solver.bc_upper[0] = BC.extrap
+    solver.bc_lower[1] = BC.wall
+    solver.bc_upper[1] = BC.extrap
+    solver.aux_bc_lower[0] = BC.wall
+    solver.aux_bc_upper[0] = BC.extrap
+    solver.aux_bc_lower[1] = BC.wall
+    solver.aux_bc_upper[1] = BC.extrap
+    x = Dimension(-1.0, 1.0, n, name='x')
+    y = Dimension(-1.0, 1.0, n, name='y')
+    domain = Domain([x, y])
+    state = State(domain, 3, 2)
+    X, Y = state.grid.p_centers
+    rho_left, rho_right, bulk_left, bulk_right = 4.0, 1.0, 4.0, 4.0
+    c_left, c_right = np.sqrt(bulk_left / rho_left), np.sqrt(bulk_right / rho_right)
+    state.aux[0, :, :] = rho_left * (X < 0.) + rho_right * (X >= 0.)
+    state.aux[1, :, :] = c_left * (X < 0.) + c_right * (X >= 0.)
+    x0, y0 = -0.5, 0.
+    r = np.sqrt((X - x0) ** 2 + (Y - y0) ** 2)
+    width, rad = 0.1, 0.25
+    state.q[0, :, :] = (np.abs(r - rad) <= width) * (1. + np.cos(np.pi * (r - rad) / width))
+    state.q[1, :, :] = 0.
+    state.q[2, :, :] = 0.
+    return _controller(solver, Solution(state, domain), tfinal, num_output_times=num_output_times)
 
 
 QUADRANT_STATES = {  # (rho, u, v, p) per quadrant, split at x = y = 0.8

@@ -9,6 +9,9 @@ Fortran step2/step2ds with clawpack/riemann solvers:
   examples/euler_2d/expected_sols.npy['quadrants_roe'] (test_euler2d.py:6-29)
   examples/shallow_2d/expected_sols.npy['radialdambreak_classic_roe']
                                                      (test_shallow2d.py:9-28)
+  examples/acoustics_2d_variable/io_test_verification/fort.q0020, fort.a0000
+                                                     (test_acoustics_2d_variable_io.py:7-58)
+  examples/acoustics_2d_variable/pressure_classic.txt (test_acoustics_2d_variable.py:6-23)
 """
 import os
 import sys
@@ -17,6 +20,18 @@ import numpy as np
 
 REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_goldens.npz")
+
+
+def read_ascii_frame(path, mx, my, nvar):
+    """A PyClaw ascii frame file (fort.qNNNN / fort.aNNNN of one patch): an
+    8-line header, then for each row j the mx cells' values, rows separated by
+    blank lines; returns the array (nvar, mx, my)."""
+    with open(path) as f:
+        lines = f.read().splitlines()[8:]
+    vals = [list(map(float, ln.split())) for ln in lines if ln.strip()]
+    arr = np.array(vals)
+    assert arr.shape == (mx * my, nvar), arr.shape
+    return np.ascontiguousarray(arr.reshape(my, mx, nvar).transpose(2, 1, 0))
 
 
 def main():
@@ -34,6 +49,11 @@ def main():
         "euler_quadrants_roe": eul["quadrants_roe"],
         "shallow_radialdambreak_classic_roe": sw["radialdambreak_classic_roe"],
     }
+    vio = os.path.join(ex, "acoustics_2d_variable", "io_test_verification")
+    out["acoustics_variable_io_q20"] = read_ascii_frame(os.path.join(vio, "fort.q0020"), 50, 50, 3)
+    out["acoustics_variable_io_aux0"] = read_ascii_frame(os.path.join(vio, "fort.a0000"), 50, 50, 2)
+    out["acoustics_variable_pressure_classic"] = np.loadtxt(
+        os.path.join(ex, "acoustics_2d_variable", "pressure_classic.txt"))
     np.savez_compressed(OUT, **{k: np.asarray(v, dtype=np.float64) for k, v in out.items()})
     print("wrote", OUT, {k: np.asarray(v).shape for k, v in out.items()})
 

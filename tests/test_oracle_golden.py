@@ -68,3 +68,20 @@ def test_shallow_roe_goldens(oracle, goldens):
     err = _l1(claw, goldens["shallow_radialdambreak_classic_roe"], comp=0)
     assert err < 1e-5
     assert err < 1e-12
+
+
+def test_vc_acoustics_goldens(oracle, goldens):
+    # examples/acoustics_2d_variable (classic, 50x50, unsplit trans_inc, two
+    # materials in aux): frame 20 of the I/O verification run (reltol 1e-6,
+    # test_acoustics_2d_variable_io.py:42) and the pressure of the classic test
+    # (abstol 0.1 in max norm, test_acoustics_2d_variable.py:14-18)
+    from pyclaw_b200 import workloads
+    claw = workloads.acoustics_variable(oracle.make_solver_class(), n=50)
+    claw.run()
+    assert np.array_equal(claw.frames[0].state.aux, goldens["acoustics_variable_io_aux0"])
+    q = claw.frames[20].q
+    exp = goldens["acoustics_variable_io_q20"]
+    rel = np.linalg.norm(exp - q) / np.linalg.norm(exp)
+    assert rel < 1e-6
+    assert rel < 1e-8  # the golden file has 8 significant digits
+    assert np.max(np.abs(goldens["acoustics_variable_pressure_classic"] - q[0])) < 1e-14
