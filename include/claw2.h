@@ -63,7 +63,7 @@ enum {
 typedef struct claw2_desc {
     int mx, my;               /* interior cells                                        */
     int num_eqn, num_waves;   /* must match the Riemann solver                         */
-    int num_aux;              /* 0 (aux-carrying solvers are not in this build)        */
+    int num_aux;              /* aux components the solver reads (2 for vc_acoustics_2D, else 0) */
     int num_ghost;            /* must be 2                                              */
     int riemann;              /* CLAW2_RP_*                                             */
     int order;                /* method(2): 1 or 2                                      */
@@ -124,6 +124,13 @@ int claw2_patch_set_cparam(claw2_patch* p, const double* cparam, int ncparam);
 /* Host <-> device copies of State.q, shape (num_eqn, mx, my), Fortran order. */
 int claw2_patch_upload_q(claw2_patch* p, const double* q);
 int claw2_patch_download_q(claw2_patch* p, double* q);
+
+/* State.aux, shape (num_aux, mx, my), Fortran order, and its ghost cells from
+ * the aux BCs (solver.py:351-519 with name 'aux': a wall mirrors without
+ * changing sign).  aux is constant in time on the device: upload it again
+ * after changing it. */
+int claw2_patch_upload_aux(claw2_patch* p, const double* aux, const int* aux_bc_lower,
+                           const int* aux_bc_upper);
 
 /* One hyperbolic step from the current q: ghost fill on the device, then the
  * unsplit (or split) step into the pending buffer.  If cfl is non-NULL the

@@ -71,6 +71,7 @@ _SIGNATURES = {
     "claw2_patch_set_cparam": (ctypes.c_int, [ctypes.c_void_p, _c_double_p, ctypes.c_int]),
     "claw2_patch_upload_q": (ctypes.c_int, [ctypes.c_void_p, _c_double_p]),
     "claw2_patch_download_q": (ctypes.c_int, [ctypes.c_void_p, _c_double_p]),
+    "claw2_patch_upload_aux": (ctypes.c_int, [ctypes.c_void_p, _c_double_p, _c_int_p, _c_int_p]),
     "claw2_patch_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _c_double_p]),
     "claw2_patch_run_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
                                             ctypes.POINTER(ctypes.c_void_p), _c_double_p, _c_double_p]),

@@ -99,6 +99,7 @@ class ClawSolver2D(ClawSolver):
         self.work = None
         self.device = 0
         self._dev = None
+        self._aux_pushed = None  # the State.aux array last uploaded to the device
         super(ClawSolver2D, self).__init__(riemann_solver, claw_package)
 
     def _check_cfl_settings(self):
@@ -128,8 +129,18 @@ class ClawSolver2D(ClawSolver):
         grid = state.grid
         if self.rp is None or not hasattr(self.rp, 'rp_id'):
             raise Exception("ClawSolver2D needs a pyclaw_b200.riemann solver")
-        if state.num_aux > 0 or state.index_capa >= 0:
-            raise NotImplementedError("aux arrays and capacity functions are not in this build")
+        need_aux = getattr(self.rp, 'num_aux', 0)
+        if state.index_capa >= 0:
+            raise NotImplementedError("capacity functions are not in this build")
+        if need_aux and state.num_aux != need_aux:
+            raise ValueError("Riemann solver %s reads %d aux components per cell; state has num_aux=%d"
+                             % (self.rp.name, need_aux, state.num_aux))
+        if need_aux:
+            for b in list(self.aux_bc_lower) + list(self.aux_bc_upper):
+                if b is None:
+                    raise Exception('One of the aux boundary conditions has not been set.')
+                if b == BC.custom:
+                    raise NotImplementedError("custom aux boundary conditions are not in this build")
         if self.step_source is not None:
             raise NotImplementedError("source terms (step_source) are not in this build")
         for b in list(self.bc_lower) + list(self.bc_upper):
@@ -145,7 +156,7 @@ class ClawSolver2D(ClawSolver):
         if state.num_eqn != self.rp.num_eqn:
             raise ValueError("state has num_eqn=%d, Riemann solver %s needs %d"
                              % (state.num_eqn, self.rp.name, self.rp.num_eqn))
-        d.num_aux = 0
+        d.num_aux = need_aux  # solvers without aux data ignore State.aux
         d.num_ghost = self.num_ghost
         d.riemann = self.rp.rp_id
         d.order = self.order
@@ -172,6 +183,9 @@ class ClawSolver2D(ClawSolver):
         self._dev = DevicePatch(self._device_desc(solution))
         state._mirror = self._dev
         self._dev.push(state)
+        if getattr(self.rp, 'num_aux', 0):
+            self._dev.push_aux(state.aux, self.aux_bc_lower, self.aux_bc_upper)
+            self._aux_pushed = state.aux
 
     # ---- per-step hooks ------------------------------------------------------
     def _begin_step(self, solution):
@@ -190,6 +204,9 @@ class ClawSolver2D(ClawSolver):
             dev = self._dev
         if dev.host_dirty:
             dev.push(state)
+        if getattr(self.rp, 'num_aux', 0) and state.aux is not getattr(self, '_aux_pushed', None):
+            dev.push_aux(state.aux, self.aux_bc_lower, self.aux_bc_upper)  # a new State.aux array
+            self._aux_pushed = state.aux
         cfl = dev.step(self.dt)
         self.cfl.update_global_max(cfl)
 

@@ -11,8 +11,10 @@ which assigns problem_data entries as attributes of ``fmod.cparam``.  This
 module accepts the same positional arguments and returns the same tuple; the
 step runs on the GPU through claw2_step2 / claw2_step2ds.  ``rpn2`` names the
 Riemann solver: a pyclaw_b200.riemann solver object or its integer id (a
-Fortran function pointer cannot select device code).  ``aux1..3`` and ``work``
-are accepted and ignored (the device allocates its own workspace).
+Fortran function pointer cannot select device code).  ``auxbc`` (ghost cells
+filled) feeds the solvers that read aux data; ``aux1..3`` and ``work`` are
+accepted and ignored (the device gathers the aux rows itself and allocates its
+own workspace).
 """
 import types
 
@@ -41,6 +43,17 @@ def _cparam_vector(rp):
                       dtype=np.float64)
 
 
+def _aux(aux, rp):
+    """(num_aux, array) of an auxbc array (maux, mx+4, my+4), Fortran order,
+    ghost cells filled, for solvers that read aux; (0, None) otherwise."""
+    if not getattr(rp, 'num_aux', 0):
+        return 0, None
+    if aux is None:
+        raise ValueError("Riemann solver %s needs the aux array" % rp.name)
+    a = np.asfortranarray(aux, dtype=np.float64)
+    return a.shape[0], a
+
+
 def _prep(qold, qnew, method, mthlim):
     qold = np.asfortranarray(qold, dtype=np.float64)
     if qnew is qold:
@@ -59,8 +72,10 @@ def step2(maxm, num_ghost, mx, my, qold, qnew, aux, dx, dy, dt, method, mthlim, 
     meqn = qold.shape[0]
     cfl = np.zeros(1)
     cp = _cparam_vector(rp)
-    _lib.check(lib.claw2_step2(int(maxm), meqn, len(mthlim), 0, int(num_ghost), int(mx), int(my),
-                               _lib.dptr(qold), _lib.dptr(out), None, float(dx), float(dy), float(dt),
+    maux, auxa = _aux(aux, rp)
+    _lib.check(lib.claw2_step2(int(maxm), meqn, len(mthlim), maux, int(num_ghost), int(mx), int(my),
+                               _lib.dptr(qold), _lib.dptr(out), _lib.dptr(auxa) if maux else None,
+                               float(dx), float(dy), float(dt),
                                _lib.iptr(method), _lib.iptr(mthlim), _lib.dptr(cfl), int(bool(fwave)),
                                rp.rp_id, _lib.dptr(cp), len(cp)))
     return out, float(cfl[0])
@@ -77,8 +92,10 @@ def step2ds(maxm, num_ghost, mx, my, qold, qnew, aux, dx, dy, dt, method, mthlim
     meqn = qold.shape[0]
     cfl = np.zeros(1)
     cp = _cparam_vector(rp)
-    _lib.check(lib.claw2_step2ds(int(maxm), meqn, len(mthlim), 0, int(num_ghost), int(mx), int(my),
-                                 _lib.dptr(qold), _lib.dptr(out), None, float(dx), float(dy), float(dt),
+    maux, auxa = _aux(aux, rp)
+    _lib.check(lib.claw2_step2ds(int(maxm), meqn, len(mthlim), maux, int(num_ghost), int(mx), int(my),
+                                 _lib.dptr(qold), _lib.dptr(out), _lib.dptr(auxa) if maux else None,
+                                 float(dx), float(dy), float(dt),
                                  _lib.iptr(method), _lib.iptr(mthlim), _lib.dptr(cfl), int(ids),
                                  int(bool(fwave)), rp.rp_id, _lib.dptr(cp), len(cp)))
     return out, float(cfl[0])

@@ -68,9 +68,13 @@ int rp_shape(int rp, int* meqn, int* mwaves) {
         case CLAW2_RP_EULER_ROE: *meqn = 4; *mwaves = 4; return 0;
         case CLAW2_RP_SHALLOW_ROE: *meqn = 3; *mwaves = 3; return 0;
         case CLAW2_RP_EULER_EXACT: *meqn = 4; *mwaves = 3; return 0;
+        case CLAW2_RP_VC_ACOUSTICS: *meqn = 3; *mwaves = 2; return 0;
         default: return -1;
     }
 }
+
+// aux components a solver reads per cell
+int rp_maux(int rp) { return rp == CLAW2_RP_VC_ACOUSTICS ? 2 : 0; }
 
 RPParams make_params(int rp, const double* cparam, int n) {
     RPParams p;
@@ -249,6 +253,7 @@ int dispatch(int rp, A&&... args) {
         case CLAW2_RP_EULER_ROE: F<RPEulerRoe>::run(args...); return 0;
         case CLAW2_RP_SHALLOW_ROE: F<RPShallowRoe>::run(args...); return 0;
         case CLAW2_RP_EULER_EXACT: F<RPEulerExact>::run(args...); return 0;
+        case CLAW2_RP_VC_ACOUSTICS: F<RPVcAcoustics>::run(args...); return 0;
         default: return -1;
     }
 }
@@ -266,8 +271,9 @@ struct SplitF {
 };
 
 void launch_bc(double* q, const Layout& L, int meqn, const int* bcl, const int* bcu,
-               unsigned long long* cfl_bits, cudaStream_t st) {
+               unsigned long long* cfl_bits, cudaStream_t st, int negate = 1) {
     BCArgs b;
+    b.negate = negate;
     b.q = q;
     b.L = L;
     b.meqn = meqn;
@@ -319,6 +325,8 @@ struct Scratch {
     size_t stage_cap = 0;
     unsigned long long* cfl = nullptr;
     int* status = nullptr;
+    double* aux = nullptr;  // aux planes of the stateless step
+    size_t aux_cap = 0;
     cudaStream_t st = nullptr;
 };
 Scratch g_scr;
@@ -331,6 +339,8 @@ int scratch_reserve(size_t n, size_t nstage) {
         g_scr.a = g_scr.b = g_scr.c = g_scr.stage = nullptr;
         g_scr.cfl = nullptr;
         g_scr.status = nullptr;
+        g_scr.aux = nullptr;
+        g_scr.aux_cap = 0;
         g_scr.st = nullptr;
         g_scr.device = dev;
     }
@@ -364,8 +374,8 @@ int grid_blocks(long long n) { return (int)std::min<long long>((n + 255) / 256, 
 // Shared body of claw2_step2 / claw2_step2ds: host qbc -> device planes ->
 // kernels -> host qbc (interior cells).
 int host_step(int maxm, int meqn, int mwaves, int maux, int mbc, int mx, int my, const double* qold,
-              double* qnew, double dx, double dy, double dt, const int* method, const int* mthlim,
-              double* cfl, int ids, int use_fwave, int rp, const double* cparam, int ncparam) {
+              double* qnew, const double* aux, double dx, double dy, double dt, const int* method,
+              const int* mthlim, double* cfl, int ids, int use_fwave, int rp, const double* cparam, int ncparam) {
     if (!qold || !qnew || !method || !mthlim || !cfl) return fail(CLAW2_EINVAL, "null pointer argument");
     int me = 0, mw = 0;
     if (rp_shape(rp, &me, &mw) != 0) return fail(CLAW2_EINVAL, "unknown Riemann solver id %d", rp);
@@ -374,7 +384,10 @@ int host_step(int maxm, int meqn, int mwaves, int maux, int mbc, int mx, int my,
     if (mbc != 2) return fail(CLAW2_EINVAL, "num_ghost must be 2 (got %d)", mbc);
     if (mx < 1 || my < 1 || maxm < std::max(mx, my))
         return fail(CLAW2_EINVAL, "bad sizes mx=%d my=%d maxm=%d", mx, my, maxm);
-    if (maux != 0 && method[6] != 0) return fail(CLAW2_EUNSUPPORTED, "aux arrays are not in this build");
+    const int need_aux = rp_maux(rp);  // solvers without aux data ignore an aux array
+    if (need_aux > 0 && (maux != need_aux || !aux))
+        return fail(CLAW2_EINVAL, "solver %d reads %d aux components per cell (got %d%s)", rp, need_aux, maux,
+                    aux ? "" : ", no aux array");
     if (method[5] != 0) return fail(CLAW2_EUNSUPPORTED, "capacity functions are not in this build");
     if (!(dx > 0.0) || !(dy > 0.0)) return fail(CLAW2_EINVAL, "dx, dy must be positive");
     int rc = check_method(method[1], method[2], mthlim, mwaves, use_fwave);
@@ -383,12 +396,27 @@ int host_step(int maxm, int meqn, int mwaves, int maux, int mbc, int mx, int my,
     std::lock_guard<std::mutex> lock(g_scr.mu);
     const Layout L = make_layout(mx, my);
     const size_t nplanes = (size_t)meqn * L.plane;
-    const size_t nstage = (size_t)meqn * (mx + 4) * (my + 4);
+    const size_t nstage = (size_t)std::max(meqn, need_aux) * (mx + 4) * (my + 4);
     rc = scratch_reserve(nplanes, nstage);
     if (rc) return rc;
     cudaStream_t st = g_scr.st;
 
-    CUDA_TRY(cudaMemcpyAsync(g_scr.stage, qold, nstage * 8, cudaMemcpyHostToDevice, st));
+    if (need_aux > 0) {  // auxbc as the caller filled it, ghost cells included
+        const size_t naux = (size_t)need_aux * L.plane;
+        if (naux > g_scr.aux_cap) {
+            cudaFree(g_scr.aux);
+            g_scr.aux = nullptr;
+            g_scr.aux_cap = 0;
+            if (cudaMalloc(&g_scr.aux, naux * 8) != cudaSuccess)
+                return fail(CLAW2_ENOMEM, "device allocation of %zu doubles failed", naux);
+            g_scr.aux_cap = naux;
+        }
+        const size_t na = (size_t)need_aux * (mx + 4) * (my + 4);
+        CUDA_TRY(cudaMemcpyAsync(g_scr.stage, aux, na * 8, cudaMemcpyHostToDevice, st));
+        k_aos_to_planes<<<grid_blocks((long long)(mx + 4) * (my + 4)), 256, 0, st>>>(g_scr.stage, g_scr.aux, L,
+                                                                                    need_aux, 2);
+    }
+    CUDA_TRY(cudaMemcpyAsync(g_scr.stage, qold, (size_t)meqn * (mx + 4) * (my + 4) * 8, cudaMemcpyHostToDevice, st));
     k_aos_to_planes<<<grid_blocks((long long)(mx + 4) * (my + 4)), 256, 0, st>>>(g_scr.stage, g_scr.a, L, meqn, 2);
     CUDA_TRY(cudaMemsetAsync(g_scr.cfl, 0, sizeof(unsigned long long), st));
     CUDA_TRY(cudaMemsetAsync(g_scr.status, 0, sizeof(int), st));
@@ -407,6 +435,7 @@ int host_step(int maxm, int meqn, int mwaves, int maux, int mbc, int mx, int my,
     a.status = g_scr.status;
     a.guess = nullptr;
     a.counters = nullptr;
+    a.aux = need_aux > 0 ? g_scr.aux : nullptr;
 
     a.qold = g_scr.a;
     a.qnew = g_scr.b;
@@ -657,6 +686,7 @@ struct claw2_patch {
     int device = 0;
     double* q[2] = {nullptr, nullptr};  // current / pending (ping-pong)
     double* tmp = nullptr;              // intermediate of the split step
+    double* aux = nullptr;              // aux planes (solvers with aux data), ghost cells filled at upload
     double* stage = nullptr;            // AoS staging for host copies
     unsigned long long* cfl = nullptr;
     int* status = nullptr;
@@ -761,6 +791,7 @@ StepArgs patch_args(claw2_patch* p, double dt) {
     a.rp = p->rp;
     a.meth = p->meth;
     a.cfl_bits = p->cfl;
+    a.aux = p->aux;
     a.status = p->status;
     a.guess = nullptr;
     a.counters = p->counters;
@@ -784,10 +815,9 @@ int claw2_step2(int maxm, int num_eqn, int num_waves, int num_aux, int num_ghost
                 const double* qold, double* qnew, const double* aux, double dx, double dy, double dt,
                 const int* method, const int* mthlim, double* cfl, int use_fwave, int riemann,
                 const double* cparam, int ncparam) {
-    (void)aux;
     if (method && method[2] < 0)
         return fail(CLAW2_EINVAL, "method(3) = -1 selects the split step: call claw2_step2ds");
-    return host_step(maxm, num_eqn, num_waves, num_aux, num_ghost, mx, my, qold, qnew, dx, dy, dt, method,
+    return host_step(maxm, num_eqn, num_waves, num_aux, num_ghost, mx, my, qold, qnew, aux, dx, dy, dt, method,
                      mthlim, cfl, 0, use_fwave, riemann, cparam, ncparam);
 }
 
@@ -795,9 +825,8 @@ int claw2_step2ds(int maxm, int num_eqn, int num_waves, int num_aux, int num_gho
                   const double* qold, double* qnew, const double* aux, double dx, double dy, double dt,
                   const int* method, const int* mthlim, double* cfl, int ids, int use_fwave, int riemann,
                   const double* cparam, int ncparam) {
-    (void)aux;
     if (ids != 1 && ids != 2) return fail(CLAW2_EINVAL, "ids must be 1 or 2 (got %d)", ids);
-    return host_step(maxm, num_eqn, num_waves, num_aux, num_ghost, mx, my, qold, qnew, dx, dy, dt, method,
+    return host_step(maxm, num_eqn, num_waves, num_aux, num_ghost, mx, my, qold, qnew, aux, dx, dy, dt, method,
                      mthlim, cfl, ids, use_fwave, riemann, cparam, ncparam);
 }
 
@@ -833,7 +862,9 @@ int claw2_patch_create(const claw2_desc* d, claw2_patch** out) {
         return fail(CLAW2_EINVAL, "solver %d has num_eqn=%d num_waves=%d (got %d, %d)", d->riemann, me, mw,
                     d->num_eqn, d->num_waves);
     if (d->num_ghost != 2) return fail(CLAW2_EINVAL, "num_ghost must be 2 (got %d)", d->num_ghost);
-    if (d->num_aux != 0) return fail(CLAW2_EUNSUPPORTED, "aux arrays are not in this build");
+    if (d->num_aux != rp_maux(d->riemann))
+        return fail(CLAW2_EINVAL, "solver %d reads %d aux components per cell (num_aux=%d)", d->riemann,
+                    rp_maux(d->riemann), d->num_aux);
     if (d->mx < 1 || d->my < 1) return fail(CLAW2_EINVAL, "bad sizes mx=%d my=%d", d->mx, d->my);
     if (!(d->dx > 0.0) || !(d->dy > 0.0)) return fail(CLAW2_EINVAL, "dx, dy must be positive");
     const int trans = d->dimensional_split ? -1 : d->transverse;
@@ -857,7 +888,7 @@ int claw2_patch_create(const claw2_desc* d, claw2_patch** out) {
     DeviceGuard g(p->device);
     cudaDeviceGetAttribute(&p->nsm, cudaDevAttrMultiProcessorCount, p->device);
     const size_t nb = (size_t)me * p->L.plane * 8;
-    const size_t ns = (size_t)me * d->mx * d->my * 8;
+    const size_t ns = (size_t)std::max(me, d->num_aux) * d->mx * d->my * 8;
     bool ok = cudaMalloc(&p->q[0], nb) == cudaSuccess && cudaMalloc(&p->q[1], nb) == cudaSuccess &&
               cudaMalloc(&p->stage, ns) == cudaSuccess &&
               cudaMalloc(&p->cfl, sizeof(unsigned long long)) == cudaSuccess &&
@@ -867,6 +898,10 @@ int claw2_patch_create(const claw2_desc* d, claw2_patch** out) {
               cudaStreamCreateWithFlags(&p->own_st, cudaStreamNonBlocking) == cudaSuccess;
     p->st = p->own_st;
     if (ok && d->dimensional_split) ok = cudaMalloc(&p->tmp, nb) == cudaSuccess;
+    if (ok && d->num_aux > 0) {
+        ok = cudaMalloc(&p->aux, (size_t)d->num_aux * p->L.plane * 8) == cudaSuccess;
+        if (ok) cudaMemsetAsync(p->aux, 0, (size_t)d->num_aux * p->L.plane * 8, p->st);
+    }
     if (ok && d->riemann == CLAW2_RP_EULER_EXACT)
         ok = cudaMalloc(&p->guess, 2 * (size_t)p->L.plane * 8) == cudaSuccess &&
              cudaMalloc(&p->counters, 2 * sizeof(unsigned long long)) == cudaSuccess;
@@ -900,6 +935,7 @@ int claw2_patch_destroy(claw2_patch* p) {
         cudaFree(p->q[0]);
         cudaFree(p->q[1]);
         cudaFree(p->tmp);
+        cudaFree(p->aux);
         cudaFree(p->guess);
         cudaFree(p->counters);
         cudaFree(p->tile_cost);
@@ -933,6 +969,23 @@ int claw2_patch_upload_q(claw2_patch* p, const double* q) {
                                                                                    p->d.num_eqn, 0);
     CUDA_TRY(cudaGetLastError());
     p->pending = false;
+    return CLAW2_OK;
+}
+
+int claw2_patch_upload_aux(claw2_patch* p, const double* aux, const int* aux_bc_lower, const int* aux_bc_upper) {
+    if (!p || !aux || !aux_bc_lower || !aux_bc_upper) return fail(CLAW2_EINVAL, "null pointer argument");
+    if (p->d.num_aux < 1) return fail(CLAW2_EINVAL, "this patch has no aux arrays (num_aux = 0)");
+    int rc = check_bc(aux_bc_lower, aux_bc_upper, p->d.mx, p->d.my);
+    if (rc) return rc;
+    DeviceGuard g(p->device);
+    const size_t n = (size_t)p->d.num_aux * p->d.mx * p->d.my;
+    CUDA_TRY(cudaMemcpyAsync(p->stage, aux, n * 8, cudaMemcpyHostToDevice, p->st));
+    k_aos_to_planes<<<grid_blocks((long long)p->d.mx * p->d.my), 256, 0, p->st>>>(p->stage, p->aux, p->L,
+                                                                                   p->d.num_aux, 0);
+    // ghost cells of aux (solver.py:439-519 with name != 'q': a wall mirrors without sign change)
+    launch_bc(p->aux, p->L, p->d.num_aux, aux_bc_lower, aux_bc_upper, nullptr, p->st, 0);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(p->st));
     return CLAW2_OK;
 }
 

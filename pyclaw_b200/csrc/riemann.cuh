@@ -595,6 +595,96 @@ struct RPEulerExact {
     __device__ __forceinline__ static int count(const Iface& f) { return f.iters; }
 };
 
+// ---------------------------------------------------------------------------
+// vc_acoustics_2D: acoustics in a heterogeneous medium; aux = (rho, c) per
+// cell, no cparam.  Cell: q, impedance Z = rho c, sound speed c.  The normal
+// solve splits the jump between cells L and R into a left-going wave with
+// L's impedance at speed -c_L and a right-going wave with R's impedance at
+// speed c_R; the transverse solve sends the part of a fluctuation that enters
+// cell k into the cells below and above k with their own impedances and
+// speeds (LeVeque 2002, sec. 9.6 and 21.5.1).
+// ---------------------------------------------------------------------------
+struct RPVcAcoustics {
+    static constexpr int MEQN = 3, MWAVES = 2, NC = 5, MAUX = 2, ID = CLAW2_RP_VC_ACOUSTICS;
+    static constexpr bool TRANSVERSE_AUX = true;  // rpt2 needs the cells beside the receiving cell
+    enum { ZZ = 3, CC = 4 };
+    struct Iface { double alpha[2]; double zl, zr, cl, cr; };
+
+    __device__ __forceinline__ static void prepare_aux(const double (&q)[MEQN], const double (&aux)[MAUX],
+                                                       const RPParams&, double (&c)[NC]) {
+        c[0] = q[0]; c[1] = q[1]; c[2] = q[2];
+        c[ZZ] = aux[0] * aux[1];
+        c[CC] = aux[1];
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void speeds(const Iface& f, const RPParams&, double (&s)[MWAVES]) {
+        s[0] = -f.cl;
+        s[1] = f.cr;
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void waves(const Iface& f, const RPParams&, double (&w)[MWAVES][MEQN]) {
+        constexpr int MU = Dir<IXY>::MU, MV = Dir<IXY>::MV;
+        w[0][0] = -f.alpha[0] * f.zl; w[0][MU] = f.alpha[0]; w[0][MV] = 0.0;
+        w[1][0] = f.alpha[1] * f.zr;  w[1][MU] = f.alpha[1]; w[1][MV] = 0.0;
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void solve(const double (&cL)[NC], const double (&cR)[NC], const RPParams& p,
+                                                 Iface& f, double (&amdq)[MEQN], double (&apdq)[MEQN]) {
+        constexpr int MU = Dir<IXY>::MU;
+        const double zr = cR[ZZ], zl = cL[ZZ];
+        const double delta1 = cR[0] - cL[0];
+        const double delta2 = cR[MU] - cL[MU];
+        f.alpha[0] = (-delta1 + zr * delta2) / (zl + zr);
+        f.alpha[1] = (delta1 + zl * delta2) / (zl + zr);
+        f.zl = zl; f.zr = zr; f.cl = cL[CC]; f.cr = cR[CC];
+        double w[MWAVES][MEQN], s[MWAVES];
+        waves<IXY>(f, p, w);
+        speeds<IXY>(f, p, s);
+#pragma unroll
+        for (int m = 0; m < MEQN; ++m) {
+            amdq[m] = s[0] * w[0][m];
+            apdq[m] = s[1] * w[1][m];
+        }
+    }
+    // asdq enters the cell c0; cm / cp are the cells below / above it in the
+    // transverse direction (x for IXY = 2, y for IXY = 1)
+    template <int IXY>
+    __device__ __forceinline__ static void rpt2_aux(const double (&asdq)[MEQN], const double (&cm)[NC],
+                                                    const double (&c0)[NC], const double (&cp)[NC],
+                                                    double (&bm)[MEQN], double (&bp)[MEQN]) {
+        constexpr int MU = Dir<IXY>::MU, MV = Dir<IXY>::MV;
+        const double zm = cm[ZZ], zz = c0[ZZ], zp = cp[ZZ];
+        const double a1 = (-asdq[0] + asdq[MV] * zz) / (zm + zz);
+        const double a2 = (asdq[0] + asdq[MV] * zz) / (zz + zp);
+        bm[0] = cm[CC] * a1 * zm; bm[MU] = 0.0; bm[MV] = -cm[CC] * a1;
+        bp[0] = cp[CC] * a2 * zp; bp[MU] = 0.0; bp[MV] = cp[CC] * a2;
+    }
+};
+
+// Traits for solvers whose cells carry aux data (MAUX > 0, prepare_aux) and
+// whose transverse solve needs the neighbouring cells (TRANSVERSE_AUX).
+template <class RP, class = void>
+struct AuxTraits {
+    static constexpr int MAUX = 0;
+    static constexpr bool TRANSVERSE_AUX = false;
+    template <int N>
+    __device__ __forceinline__ static void prep(const double (&q)[RP::MEQN], const double (&)[N], const RPParams& p,
+                                                double (&c)[RP::NC]) {
+        RP::prepare(q, p, c);
+    }
+};
+template <class RP>
+struct AuxTraits<RP, decltype((void)RP::MAUX, void())> {
+    static constexpr int MAUX = RP::MAUX;
+    static constexpr bool TRANSVERSE_AUX = RP::TRANSVERSE_AUX;
+    template <int N>
+    __device__ __forceinline__ static void prep(const double (&q)[RP::MEQN], const double (&aux)[N],
+                                                const RPParams& p, double (&c)[RP::NC]) {
+        static_assert(N == RP::MAUX, "aux vector of the wrong size");
+        RP::prepare_aux(q, aux, p, c);
+    }
+};
+
 // Traits for the optional per-interface guess and iteration count.
 template <class RP, class = void>
 struct GuessTraits {

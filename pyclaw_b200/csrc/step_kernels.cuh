@@ -49,6 +49,8 @@ struct StepArgs {
     const int* tile_order = nullptr;
     unsigned int* tile_cost = nullptr;
     int nstrips = 0;
+    // aux planes (same layout as q) for solvers with aux data, else nullptr
+    const double* __restrict__ aux = nullptr;
 };
 
 // philim.f90:16-35
@@ -152,6 +154,13 @@ __device__ __forceinline__ double iface_cfl(const typename RP::Iface& f, const R
     return c;
 }
 
+// aux of the cell at column pointer ap (already offset by the column), row R
+template <class RP, int MAD>
+__device__ __forceinline__ void load_aux(const double* ap, long long plane, int pitch, int R, double (&av)[MAD]) {
+#pragma unroll
+    for (int k = 0; k < MAD; ++k) av[k] = (AuxTraits<RP>::MAUX > 0) ? __ldg(ap + k * plane + (long long)R * pitch) : 0.0;
+}
+
 // ---------------------------------------------------------------------------
 // TMA row staging: one thread per CTA copies the next row of a strip (NT
 // columns x 1 row x num_eqn planes) from a 3D tensor map of the q planes into
@@ -252,8 +261,23 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
     const double* qo = a.qold + cpl;
     double* qn = a.qnew + cpl;
 
-    // (the copy needs a 128-byte aligned destination; anything else loads directly)
-    const bool tma = (tm != nullptr) && ((smem_u32(qrow) & 127u) == 0);
+    // aux data: loaded with q a row ahead (MA planes); solvers whose transverse
+    // solve needs the cells above and below (TAUX) run the x-interface's
+    // transverse solve one row late, when the row above is prepared
+    constexpr int MA = AuxTraits<RP>::MAUX, MAD = MA > 0 ? MA : 1;
+    constexpr bool TAUX = AuxTraits<RP>::TRANSVERSE_AUX;
+    const double* ao = a.aux + cpl;
+    double pfa[MAD];
+    double cxa1[ME], cxa2[ME];  // deferred x-transverse inputs (A-dq and A+dq of the row above's interface)
+    bool cx_valid = false;
+#pragma unroll
+    for (int m = 0; m < ME; ++m) cxa1[m] = cxa2[m] = 0.0;
+#pragma unroll
+    for (int k = 0; k < MAD; ++k) pfa[k] = (MA > 0) ? __ldg(ao + k * plane + (long long)R0 * pitch) : 0.0;
+
+    // (the copy needs a 128-byte aligned destination; anything else loads
+    // directly; solvers with aux data load directly)
+    const bool tma = (MA == 0) && (tm != nullptr) && ((smem_u32(qrow) & 127u) == 0);
     const int x0 = strip * W;                                     // first column of the strip
     const unsigned row_bytes = (unsigned)(ME * NT * sizeof(double));
     const int tq = cpl - x0;                                      // this thread's staged column
@@ -294,7 +318,14 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
                     for (int m = 0; m < ME; ++m) pf[m] = __ldg(qo + m * plane + (long long)(R + 1) * pitch);
                 }
             }
-            RP::prepare(q, P, c);
+            double av[MAD];
+#pragma unroll
+            for (int k = 0; k < MAD; ++k) av[k] = pfa[k];
+            if (MA > 0 && R < R1) {
+#pragma unroll
+                for (int k = 0; k < MAD; ++k) pfa[k] = __ldg(ao + k * plane + (long long)(R + 1) * pitch);
+            }
+            AuxTraits<RP>::prep(q, av, P, c);
 #pragma unroll
             for (int k = 0; k < NC; ++k) S.cell[s2][k][t] = c[k];
         }
@@ -303,6 +334,47 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
             // every thread has read row R from the staging buffer (before S1)
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             tma_row(tm, qrow, bar, x0, R + 1, row_bytes);
+        }
+
+        // ---- the x-interface of row R-1, deferred transverse solve (TAUX) ----
+        // Its receiving cells (cp-1 or cp, row R-1) and their neighbours in
+        // rows R-2 and R are now in the ring; the increments go to rows R-2,
+        // R-1, R of column cp-1 (exchange slots 0..2) and of this column.
+        double dxl0[ME], dxl1[ME], dxl2[ME];
+#pragma unroll
+        for (int m = 0; m < ME; ++m) dxl0[m] = dxl1[m] = dxl2[m] = 0.0;
+        if constexpr (TAUX) {
+            if (cx_valid) {
+                const double h = 0.5 * dtdx * dtdy;
+                double cm[NC], c0[NC], cu[NC], bm[ME], bp[ME];
+#pragma unroll
+                for (int k = 0; k < NC; ++k) {
+                    cm[k] = S.cell[s0][k][tl];
+                    c0[k] = S.cell[s1][k][tl];
+                    cu[k] = S.cell[s2][k][tl];
+                }
+                RP::template rpt2_aux<1>(cxa1, cm, c0, cu, bm, bp);  // imp = 1 -> column cp-1
+#pragma unroll
+                for (int m = 0; m < ME; ++m) {
+                    dxl1[m] = h * (bp[m] - bm[m]);
+                    dxl0[m] = h * bm[m];
+                    dxl2[m] = -h * bp[m];
+                }
+#pragma unroll
+                for (int k = 0; k < NC; ++k) {
+                    cm[k] = S.cell[s0][k][t];
+                    c0[k] = S.cell[s1][k][t];
+                    cu[k] = S.cell[s2][k][t];
+                }
+                RP::template rpt2_aux<1>(cxa2, cm, c0, cu, bm, bp);  // imp = 2 -> column cp
+#pragma unroll
+                for (int m = 0; m < ME; ++m) {
+                    accB[m] = accB[m] + h * (bp[m] - bm[m]);
+                    accA[m] = accA[m] + h * bm[m];
+                    accC[m] = accC[m] - h * bp[m];
+                }
+            }
+            cx_valid = false;
         }
 
         double ylB[ME], ylA[ME], yrB[ME], yrA[ME];
@@ -359,7 +431,18 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
                     double as2[ME], bm[ME], bp[ME];
 #pragma unroll
                     for (int m = 0; m < ME; ++m) as2[m] = tc ? amY[m] + cq[m] : amY[m];
-                    RP::template rpt2<2>(fY, P, as2, bm, bp);  // imp = 1 -> row R-2
+                    if constexpr (TAUX) {  // cell (cp, R-2) between columns cp-1 and cp+1
+                        double cm[NC], c0[NC], cu[NC];
+#pragma unroll
+                        for (int k = 0; k < NC; ++k) {
+                            cm[k] = S.cell[s0][k][tl];
+                            c0[k] = S.cell[s0][k][t];
+                            cu[k] = S.cell[s0][k][tr];
+                        }
+                        RP::template rpt2_aux<2>(as2, cm, c0, cu, bm, bp);
+                    } else {
+                        RP::template rpt2<2>(fY, P, as2, bm, bp);  // imp = 1 -> row R-2
+                    }
 #pragma unroll
                     for (int m = 0; m < ME; ++m) {
                         accA[m] = accA[m] + h * (bp[m] - bm[m]);
@@ -368,7 +451,18 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
                     }
 #pragma unroll
                     for (int m = 0; m < ME; ++m) as2[m] = tc ? apY[m] - cq[m] : apY[m];
-                    RP::template rpt2<2>(fY, P, as2, bm, bp);  // imp = 2 -> row R-1
+                    if constexpr (TAUX) {  // cell (cp, R-1)
+                        double cm[NC], c0[NC], cu[NC];
+#pragma unroll
+                        for (int k = 0; k < NC; ++k) {
+                            cm[k] = S.cell[s1][k][tl];
+                            c0[k] = S.cell[s1][k][t];
+                            cu[k] = S.cell[s1][k][tr];
+                        }
+                        RP::template rpt2_aux<2>(as2, cm, c0, cu, bm, bp);
+                    } else {
+                        RP::template rpt2<2>(fY, P, as2, bm, bp);  // imp = 2 -> row R-1
+                    }
 #pragma unroll
                     for (int m = 0; m < ME; ++m) {
                         accB[m] = accB[m] + h * (bp[m] - bm[m]);
@@ -388,7 +482,7 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
         // row's exchange slots came before S1.
 #pragma unroll
         for (int m = 0; m < ME; ++m) {
-            S.xl[0][m][t] = ylB[m];
+            S.xl[0][m][t] = ylB[m] + dxl0[m];
             S.yr[0][m][t] = yrB[m];
             S.yr[1][m][t] = yrA[m];
         }
@@ -451,7 +545,16 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
                 accC[m] = accC[m] - dtdx * (apX[m] - f);
                 xcL[m] = -dtdx * (amX[m] + f);
             }
-            if (trans > 0) {
+            if constexpr (TAUX) {
+                if (trans > 0) {  // the transverse solve runs with the next row
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) {
+                        cxa1[m] = tc ? amX[m] + cq[m] : amX[m];
+                        cxa2[m] = tc ? apX[m] - cq[m] : apX[m];
+                    }
+                    cx_valid = true;
+                }
+            } else if (trans > 0) {
                 const double h = 0.5 * dtdx * dtdy;
                 double as2[ME], bm[ME], bp[ME];
 #pragma unroll
@@ -476,8 +579,8 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
         }
 #pragma unroll
         for (int m = 0; m < ME; ++m) {
-            S.xl[1][m][t] = xbL[m] + ylA[m];
-            S.xl[2][m][t] = xcL[m];
+            S.xl[1][m][t] = xbL[m] + ylA[m] + dxl1[m];
+            S.xl[2][m][t] = xcL[m] + dxl2[m];
             S.xl[3][m][t] = xaL[m];
         }
         __syncthreads();  // S3: neighbour increments visible
@@ -615,6 +718,7 @@ struct SplitXSmem {
 template <class RP, int NT>
 __global__ void __launch_bounds__(NT) k_split_x(const StepArgs a) {
     constexpr int ME = RP::MEQN, MW = RP::MWAVES, NC = RP::NC, W = NT - 4;
+    constexpr int MAD = AuxTraits<RP>::MAUX > 0 ? AuxTraits<RP>::MAUX : 1;
     using Iface = typename RP::Iface;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     SplitXSmem<RP, NT>& S = *reinterpret_cast<SplitXSmem<RP, NT>*>(smem_raw);
@@ -645,7 +749,9 @@ __global__ void __launch_bounds__(NT) k_split_x(const StepArgs a) {
             double c[NC];
 #pragma unroll
             for (int m = 0; m < ME; ++m) q[m] = __ldg(qo + m * plane + (long long)R * pitch);
-            RP::prepare(q, P, c);
+            double av[MAD];
+            load_aux<RP, MAD>(a.aux + cpl, plane, pitch, R, av);
+            AuxTraits<RP>::prep(q, av, P, c);
 #pragma unroll
             for (int k = 0; k < NC; ++k) S.cell[buf][k][t] = c[k];
         }
@@ -716,6 +822,7 @@ __global__ void __launch_bounds__(NT) k_split_x(const StepArgs a) {
 template <class RP, int NT>
 __global__ void __launch_bounds__(NT) k_split_y(const StepArgs a) {
     constexpr int ME = RP::MEQN, MW = RP::MWAVES, NC = RP::NC;
+    constexpr int MAD = AuxTraits<RP>::MAUX > 0 ? AuxTraits<RP>::MAUX : 1;
     using Iface = typename RP::Iface;
     __shared__ double sRed[NT / 32];
     const int mx = a.L.mx, my = a.L.my;
@@ -741,7 +848,9 @@ __global__ void __launch_bounds__(NT) k_split_y(const StepArgs a) {
         double q[ME];
 #pragma unroll
         for (int m = 0; m < ME; ++m) q[m] = __ldg(qo + m * plane + (long long)R0 * pitch);
-        RP::prepare(q, P, cB);
+        double av[MAD];
+        load_aux<RP, MAD>(a.aux + cpl, plane, pitch, R0, av);
+        AuxTraits<RP>::prep(q, av, P, cB);
 #pragma unroll
         for (int m = 0; m < ME; ++m) {
             q0[m] = q1[m] = q[m];
@@ -756,7 +865,9 @@ __global__ void __launch_bounds__(NT) k_split_y(const StepArgs a) {
         double q2[ME], cA[NC];
 #pragma unroll
         for (int m = 0; m < ME; ++m) q2[m] = __ldg(qo + m * plane + (long long)R * pitch);
-        RP::prepare(q2, P, cA);
+        double av[MAD];
+        load_aux<RP, MAD>(a.aux + cpl, plane, pitch, R, av);
+        AuxTraits<RP>::prep(q2, av, P, cA);
         Iface fN;
         double amN[ME], apN[ME];
         RP::template solve<2>(cB, cA, P, fN, amN, apN);
@@ -828,6 +939,7 @@ struct BCArgs {
     int meqn;
     int bcl[2], bcu[2];
     unsigned long long* cfl_bits;
+    int negate = 1;  // a wall negates the normal momentum (q); 0 for aux (plain mirror)
 };
 
 __device__ __forceinline__ int bc_src(int c, int n, int lo, int up, bool& flip) {
@@ -874,8 +986,8 @@ static __global__ void k_bc_fill(const BCArgs a) {
     const long long src = (long long)rs * a.L.pitch + cs, dst = (long long)r * a.L.pitch + c;
     for (int m = 0; m < a.meqn; ++m) {
         double v = a.q[m * a.L.plane + src];
-        if (fx && m == 1) v = -v;
-        if (fy && m == 2) v = -v;
+        if (a.negate && fx && m == 1) v = -v;
+        if (a.negate && fy && m == 2) v = -v;
         a.q[m * a.L.plane + dst] = v;
     }
 }

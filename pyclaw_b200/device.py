@@ -57,6 +57,14 @@ class DevicePatch(object):
         self.host_dirty = False
         self.device_newer = False
 
+    def push_aux(self, aux, bc_lower, bc_upper):
+        """Upload State.aux and fill its ghost cells from the aux BCs on the
+        device (claw2_patch_upload_aux)."""
+        a = np.asfortranarray(aux, dtype=np.float64)
+        lo = np.ascontiguousarray([int(b) for b in bc_lower], dtype=np.intc)
+        up = np.ascontiguousarray([int(b) for b in bc_upper], dtype=np.intc)
+        _lib.check(self._lib.claw2_patch_upload_aux(self.h, _lib.dptr(a), _lib.iptr(lo), _lib.iptr(up)))
+
     # ---- stepping -----------------------------------------------------------
     def set_cparam(self, vals):
         arr = (ctypes.c_double * len(vals))(*vals)
