@@ -37,7 +37,8 @@ enum {
     CLAW2_RP_EULER_ROE = 3,    /* euler_4wave_2D:             {gamma, efix}          */
     CLAW2_RP_SHALLOW_ROE = 4,  /* shallow_roe_with_efix_2D:   {grav, efix}           */
     CLAW2_RP_EULER_EXACT = 5,  /* exact Euler (no reference counterpart): {gamma, tol, guess} */
-    CLAW2_RP_VC_ACOUSTICS = 6  /* vc_acoustics_2D: no cparam; aux = {rho, c} per cell        */
+    CLAW2_RP_VC_ACOUSTICS = 6, /* vc_acoustics_2D: no cparam; aux = {rho, c} per cell        */
+    CLAW2_RP_VC_ADVECTION = 7  /* vc_advection_2D: no cparam; aux = {u left edge, v bottom edge} */
 };
 
 /* Boundary-condition codes: pyclaw.BC (src/pyclaw/solver.py:13-19), plus
@@ -63,7 +64,9 @@ enum {
 typedef struct claw2_desc {
     int mx, my;               /* interior cells                                        */
     int num_eqn, num_waves;   /* must match the Riemann solver                         */
-    int num_aux;              /* aux components the solver reads (2 for vc_acoustics_2D, else 0) */
+    int num_aux;              /* aux components per cell on the device: at least the ones the
+                                 solver reads (2 for vc_acoustics_2D, vc_advection_2D) and the
+                                 capacity's; 0 when neither needs aux          */
     int num_ghost;            /* must be 2                                              */
     int riemann;              /* CLAW2_RP_*                                             */
     int order;                /* method(2): 1 or 2                                      */
@@ -76,6 +79,8 @@ typedef struct claw2_desc {
     double cparam[CLAW2_MAX_PARAMS];
     int ncparam;
     int device;               /* CUDA device ordinal                                    */
+    int mcapa;                /* method(6): 0, or 1 + the aux component holding the
+                                 capacity function kappa (state.index_capa + 1)      */
 } claw2_desc;
 
 typedef struct claw2_patch claw2_patch;
@@ -131,6 +136,11 @@ int claw2_patch_download_q(claw2_patch* p, double* q);
  * after changing it. */
 int claw2_patch_upload_aux(claw2_patch* p, const double* aux, const int* aux_bc_lower,
                            const int* aux_bc_upper);
+
+/* auxbc as the host filled it, shape (num_aux, mx+4, my+4), Fortran order,
+ * ghost cells included: for aux BCs the host applies itself (BC.custom, the
+ * user_aux_bc_lower/upper functions that solver.py:378-427 calls). */
+int claw2_patch_upload_auxbc(claw2_patch* p, const double* auxbc);
 
 /* One hyperbolic step from the current q: ghost fill on the device, then the
  * unsplit (or split) step into the pending buffer.  If cfl is non-NULL the

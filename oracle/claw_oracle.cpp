@@ -226,6 +226,35 @@ void rpt2_vc_acoustics(int ixy, int imp, int mbc, int mx, const CSlice& aux1, co
     }
 }
 
+// vc_advection_2D: q_t + u q_x + v q_y = 0 with edge velocities in aux
+// (LeVeque 2002, sec. 9.5 and 20.5): aux(1, i) is u at the left edge of cell
+// i and aux(2, i) is v at its bottom edge.  Normal solve: one wave, the jump,
+// moving at the velocity of the interface it sits on (the left edge of cell
+// i for the interface i-1 | i).
+void rpn2_vc_advection(int ixy, int mbc, int mx, const CSlice& ql, const CSlice& qr, const CSlice& auxl,
+                       const Waves& wave, const Speeds& s, const Slice& amdq, const Slice& apdq) {
+    const int kn = ixy - 1;  // the normal velocity's aux component
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        wave(0, 0, i) = ql(0, i) - qr(0, i - 1);
+        s(0, i) = auxl(kn, i);
+        amdq(0, i) = std::min(auxl(kn, i), 0.0) * wave(0, 0, i);
+        apdq(0, i) = std::max(auxl(kn, i), 0.0) * wave(0, 0, i);
+    }
+}
+// Transverse solve: asdq entered cell i1 (i-1 for imp = 1, i for imp = 2);
+// its down-going part leaves through i1's own lower transverse edge (velocity
+// in aux2) and its up-going part through the lower edge of the cell above
+// (aux3), each at that edge's transverse velocity.
+void rpt2_vc_advection(int ixy, int imp, int mbc, int mx, const CSlice& aux2, const CSlice& aux3,
+                       const Slice& asdq, const Slice& bmasdq, const Slice& bpasdq) {
+    const int kt = (ixy == 1) ? 1 : 0;  // the transverse velocity's aux component
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        const int i1 = (imp == 1) ? i - 1 : i;
+        bmasdq(0, i) = std::min(aux2(kt, i1), 0.0) * asdq(0, i);
+        bpasdq(0, i) = std::max(aux3(kt, i1), 0.0) * asdq(0, i);
+    }
+}
+
 // Euler equations, Roe solver with 4 waves (u-c, entropy, shear, u+c) and an
 // optional Harten-Hyman entropy fix (LeVeque 2002, sec. 15.3.5 and 18.8;
 // Roe 1981).  The wave layout follows the reference's vendored 5-wave solver
@@ -742,8 +771,12 @@ void rpn2_euler_exact(int ixy, int mbc, int mx, int meqn, int mwaves, const CSli
 // ---------------------------------------------------------------------------
 bool rp_known(int rp) {
     return rp == ORC_RP_ADVECTION || rp == ORC_RP_ACOUSTICS || rp == ORC_RP_EULER_ROE ||
-           rp == ORC_RP_SHALLOW_ROE || rp == ORC_RP_EULER_EXACT || rp == ORC_RP_VC_ACOUSTICS;
+           rp == ORC_RP_SHALLOW_ROE || rp == ORC_RP_EULER_EXACT || rp == ORC_RP_VC_ACOUSTICS ||
+           rp == ORC_RP_VC_ADVECTION;
 }
+
+// aux components per cell the solver reads (the leading ones of the aux array)
+int rp_maux(int rp) { return (rp == ORC_RP_VC_ACOUSTICS || rp == ORC_RP_VC_ADVECTION) ? 2 : 0; }
 
 void call_rpn2(int rp, int ixy, int mbc, int mx, int meqn, int mwaves, const CSlice& q, const CSlice& aux2,
                const Waves& wave, const Speeds& s, const Slice& amdq, const Slice& apdq,
@@ -755,6 +788,7 @@ void call_rpn2(int rp, int ixy, int mbc, int mx, int meqn, int mwaves, const CSl
         case ORC_RP_SHALLOW_ROE: rpn2_shallow_roe(ixy, mbc, mx, meqn, mwaves, q, q, wave, s, amdq, apdq, cp); break;
         case ORC_RP_EULER_EXACT: rpn2_euler_exact(ixy, mbc, mx, meqn, mwaves, q, q, wave, s, amdq, apdq, cp); break;
         case ORC_RP_VC_ACOUSTICS: rpn2_vc_acoustics(ixy, mbc, mx, meqn, q, q, aux2, aux2, wave, s, amdq, apdq); break;
+        case ORC_RP_VC_ADVECTION: rpn2_vc_advection(ixy, mbc, mx, q, q, aux2, wave, s, amdq, apdq); break;
     }
 }
 void call_rpt2(int rp, int ixy, int imp, int mbc, int mx, int meqn, int mwaves, const CSlice& q,
@@ -762,6 +796,7 @@ void call_rpt2(int rp, int ixy, int imp, int mbc, int mx, int meqn, int mwaves, 
                const Slice& asdq, const Slice& bm, const Slice& bp, const double* cp) {
     switch (rp) {
         case ORC_RP_VC_ACOUSTICS: rpt2_vc_acoustics(ixy, imp, mbc, mx, aux1, aux2, aux3, asdq, bm, bp); break;
+        case ORC_RP_VC_ADVECTION: rpt2_vc_advection(ixy, imp, mbc, mx, aux2, aux3, asdq, bm, bp); break;
         case ORC_RP_ADVECTION: rpt2_advection(ixy, mbc, mx, asdq, bm, bp, cp); break;
         case ORC_RP_ACOUSTICS: rpt2_acoustics(ixy, mbc, mx, asdq, bm, bp, cp); break;
         case ORC_RP_EULER_ROE: rpt2_euler_roe(ixy, mbc, mx, meqn, mwaves, q, q, asdq, bm, bp, cp); break;
@@ -914,6 +949,7 @@ int oracle_step2(int maxm, int meqn, int mwaves, int maux, int mbc, int mx, int 
     if (maxm < std::max(mx, my)) return 3;
     const int index_capa = method[5];
     if (index_capa > 0 && (aux_p == nullptr || maux < index_capa)) return 4;
+    if (rp_maux(rp) > 0 && (aux_p == nullptr || maux < rp_maux(rp))) return 4;
     Grid2 qold{const_cast<double*>(qold_p), meqn, mbc, mx};
     Grid2 qnew{qnew_p, meqn, mbc, mx};
     Grid2 aux{const_cast<double*>(aux_p), maux > 0 ? maux : 1, mbc, mx};
@@ -1024,6 +1060,7 @@ int oracle_step2ds(int maxm, int meqn, int mwaves, int maux, int mbc, int mx, in
     if (ids != 1 && ids != 2) return 5;
     const int index_capa = method[5];
     if (index_capa > 0 && (aux_p == nullptr || maux < index_capa)) return 4;
+    if (rp_maux(rp) > 0 && (aux_p == nullptr || maux < rp_maux(rp))) return 4;
     Grid2 qold{const_cast<double*>(qold_p), meqn, mbc, mx};
     Grid2 qnew{qnew_p, meqn, mbc, mx};
     Grid2 aux{const_cast<double*>(aux_p), maux > 0 ? maux : 1, mbc, mx};

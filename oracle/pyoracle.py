@@ -127,6 +127,43 @@ def bc_fill(qbc, bc_lower, bc_upper):
         raise RuntimeError("oracle_bc_fill returned %d" % rc)
 
 
+def apply_aux_bcs(solver, state, auxbc):
+    """Solver._apply_bcs for the aux array (src/pyclaw/solver.py:351-437,
+    439-519 with name 'aux'): interior from State.aux, then per dimension the
+    lower and the upper side, a user function for BC.custom (called with
+    qbc = None), else extrap / periodic / wall (a plain mirror)."""
+    from pyclaw_b200.solver import BC
+    ng = 2
+    auxbc[:, ng:-ng, ng:-ng] = state.aux
+    for idim, dim in enumerate(state.grid.dimensions):
+        arr = np.rollaxis(auxbc, idim + 1, 1)
+        for lower in (True, False):
+            kind = (solver.aux_bc_lower if lower else solver.aux_bc_upper)[idim]
+            if kind == BC.custom:
+                fun = solver.user_aux_bc_lower if lower else solver.user_aux_bc_upper
+                fun(state, dim, state.t, None, auxbc, ng)
+            elif kind == BC.extrap:
+                for i in range(ng):
+                    if lower:
+                        arr[:, i, ...] = arr[:, ng, ...]
+                    else:
+                        arr[:, -i - 1, ...] = arr[:, -ng - 1, ...]
+            elif kind == BC.periodic:
+                if lower:
+                    arr[:, :ng, ...] = arr[:, -2 * ng:-ng, ...]
+                else:
+                    arr[:, -ng:, ...] = arr[:, ng:2 * ng, ...]
+            elif kind == BC.wall:
+                for i in range(ng):
+                    if lower:
+                        arr[:, i, ...] = arr[:, 2 * ng - 1 - i, ...]
+                    else:
+                        arr[:, -i - 1, ...] = arr[:, -2 * ng + i, ...]
+            else:
+                raise NotImplementedError("aux boundary condition %r" % (kind,))
+    return auxbc
+
+
 def make_solver_class():
     """ClawSolver2D running the oracle on host arrays (built lazily so that
     importing this module does not import the product package)."""
@@ -163,8 +200,11 @@ def make_solver_class():
             aux = None
             if self.auxbc is not None:  # solver.py:351-437 fills auxbc with qbc every step
                 aux = self.auxbc
-                aux[:, 2:-2, 2:-2] = state.aux
-                bc_fill_aux(aux, self.aux_bc_lower, self.aux_bc_upper)
+                if any(b == 0 for b in list(self.aux_bc_lower) + list(self.aux_bc_upper)):
+                    apply_aux_bcs(self, state, aux)  # user functions (BC.custom)
+                else:
+                    aux[:, 2:-2, 2:-2] = state.aux
+                    bc_fill_aux(aux, self.aux_bc_lower, self.aux_bc_upper)
             qold = qbc.copy('F')
             cp = self.rp.cparam(state.problem_data)
             if self.dimensional_split:

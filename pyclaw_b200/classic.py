@@ -7,6 +7,8 @@ through the C ABI of include/claw2.h: ghost-cell fill, the unsplit step2 (or
 the split step2ds pair) and the CFL reduction all happen on the device, and q
 stays there between steps.
 """
+import numpy as np
+
 from .limiters import tvd
 from .solver import BC, Solver
 from . import _lib
@@ -121,8 +123,19 @@ class ClawSolver2D(ClawSolver):
             raise Exception("pyclaw_b200 runs kernel_language='CUDA' only (got %r)" % self.kernel_language)
         state = solution.states[0]
         self._set_method(state)
+        self._check_bc_signatures()
         self._make_device_patch(solution)
         super(ClawSolver, self).setup(solution)
+
+    def _check_bc_signatures(self):
+        """A custom BC function with 5 arguments has the old signature
+        (state, dim, t, array, num_ghost) (solver.py:328-339)."""
+        import inspect
+        for fun in (self.user_bc_lower, self.user_bc_upper, self.user_aux_bc_lower, self.user_aux_bc_upper):
+            if fun is not None and len(inspect.getfullargspec(fun)[0]) == 5:
+                self.logger.warning("The custom boundary condition function signature has been changed; "
+                                    "the 5-argument form is deprecated.")
+                self._use_old_bc_sig = True
 
     def _device_desc(self, solution):
         state = solution.states[0]
@@ -130,17 +143,16 @@ class ClawSolver2D(ClawSolver):
         if self.rp is None or not hasattr(self.rp, 'rp_id'):
             raise Exception("ClawSolver2D needs a pyclaw_b200.riemann solver")
         need_aux = getattr(self.rp, 'num_aux', 0)
-        if state.index_capa >= 0:
-            raise NotImplementedError("capacity functions are not in this build")
-        if need_aux and state.num_aux != need_aux:
+        if need_aux and state.num_aux < need_aux:
             raise ValueError("Riemann solver %s reads %d aux components per cell; state has num_aux=%d"
                              % (self.rp.name, need_aux, state.num_aux))
-        if need_aux:
+        if state.index_capa >= 0 and state.index_capa >= state.num_aux:
+            raise ValueError("index_capa=%d names no component of the aux array (num_aux=%d)"
+                             % (state.index_capa, state.num_aux))
+        if self._device_aux(state):
             for b in list(self.aux_bc_lower) + list(self.aux_bc_upper):
                 if b is None:
                     raise Exception('One of the aux boundary conditions has not been set.')
-                if b == BC.custom:
-                    raise NotImplementedError("custom aux boundary conditions are not in this build")
         if self.step_source is not None:
             raise NotImplementedError("source terms (step_source) are not in this build")
         for b in list(self.bc_lower) + list(self.bc_upper):
@@ -156,7 +168,8 @@ class ClawSolver2D(ClawSolver):
         if state.num_eqn != self.rp.num_eqn:
             raise ValueError("state has num_eqn=%d, Riemann solver %s needs %d"
                              % (state.num_eqn, self.rp.name, self.rp.num_eqn))
-        d.num_aux = need_aux  # solvers without aux data ignore State.aux
+        d.num_aux = state.num_aux if self._device_aux(state) else 0  # else State.aux is not read
+        d.mcapa = state.index_capa + 1 if state.index_capa >= 0 else 0
         d.num_ghost = self.num_ghost
         d.riemann = self.rp.rp_id
         d.order = self.order
@@ -175,6 +188,31 @@ class ClawSolver2D(ClawSolver):
         d.device = int(self.device)
         return d
 
+    def _device_aux(self, state):
+        """True when the step reads aux data: the Riemann solver's or the
+        capacity function."""
+        return bool(getattr(self.rp, 'num_aux', 0)) or state.index_capa >= 0
+
+    def _push_aux(self, state, force):
+        """Aux data to the device: State.aux with ghost cells filled on the
+        device, or, with a custom aux BC, auxbc filled on the host every step
+        (solver.py:351-437) and uploaded when it changed."""
+        from . import auxbc as _auxbc
+        if not self._device_aux(state):
+            return
+        if _auxbc.needs_host_fill(self):
+            shape = (state.num_aux,) + tuple(n + 2 * self.num_ghost for n in state.grid.num_cells)
+            if self.auxbc is None or self.auxbc.shape != shape:
+                self.auxbc = np.zeros(shape, order='F')
+            new = _auxbc.fill_auxbc(self, state, self.auxbc.copy(order='F'))
+            if force or self._aux_pushed is None or not np.array_equal(new, self._aux_pushed):
+                self._dev.push_auxbc(new)
+            self.auxbc = new
+            self._aux_pushed = new
+        elif force or state.aux is not self._aux_pushed:
+            self._dev.push_aux(state.aux, self.aux_bc_lower, self.aux_bc_upper)
+            self._aux_pushed = state.aux
+
     def _make_device_patch(self, solution):
         from .device import DevicePatch
         if self._dev is not None:
@@ -183,9 +221,7 @@ class ClawSolver2D(ClawSolver):
         self._dev = DevicePatch(self._device_desc(solution))
         state._mirror = self._dev
         self._dev.push(state)
-        if getattr(self.rp, 'num_aux', 0):
-            self._dev.push_aux(state.aux, self.aux_bc_lower, self.aux_bc_upper)
-            self._aux_pushed = state.aux
+        self._push_aux(state, force=True)
 
     # ---- per-step hooks ------------------------------------------------------
     def _begin_step(self, solution):
@@ -204,9 +240,7 @@ class ClawSolver2D(ClawSolver):
             dev = self._dev
         if dev.host_dirty:
             dev.push(state)
-        if getattr(self.rp, 'num_aux', 0) and state.aux is not getattr(self, '_aux_pushed', None):
-            dev.push_aux(state.aux, self.aux_bc_lower, self.aux_bc_upper)  # a new State.aux array
-            self._aux_pushed = state.aux
+        self._push_aux(state, force=False)  # a new State.aux array, or custom aux BCs
         cfl = dev.step(self.dt)
         self.cfl.update_global_max(cfl)
 

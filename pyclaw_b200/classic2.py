@@ -12,7 +12,8 @@ module accepts the same positional arguments and returns the same tuple; the
 step runs on the GPU through claw2_step2 / claw2_step2ds.  ``rpn2`` names the
 Riemann solver: a pyclaw_b200.riemann solver object or its integer id (a
 Fortran function pointer cannot select device code).  ``auxbc`` (ghost cells
-filled) feeds the solvers that read aux data; ``aux1..3`` and ``work`` are
+filled) feeds the solvers that read aux data and the capacity function
+(method(6) > 0); ``aux1..3`` and ``work`` are
 accepted and ignored (the device gathers the aux rows itself and allocates its
 own workspace).
 """
@@ -43,13 +44,14 @@ def _cparam_vector(rp):
                       dtype=np.float64)
 
 
-def _aux(aux, rp):
+def _aux(aux, rp, method):
     """(num_aux, array) of an auxbc array (maux, mx+4, my+4), Fortran order,
-    ghost cells filled, for solvers that read aux; (0, None) otherwise."""
-    if not getattr(rp, 'num_aux', 0):
+    ghost cells filled, for solvers that read aux or a step with a capacity
+    function (method(6) > 0); (0, None) otherwise."""
+    if not getattr(rp, 'num_aux', 0) and int(method[5]) == 0:
         return 0, None
     if aux is None:
-        raise ValueError("Riemann solver %s needs the aux array" % rp.name)
+        raise ValueError("Riemann solver %s with method(6) = %d needs the aux array" % (rp.name, int(method[5])))
     a = np.asfortranarray(aux, dtype=np.float64)
     return a.shape[0], a
 
@@ -72,7 +74,7 @@ def step2(maxm, num_ghost, mx, my, qold, qnew, aux, dx, dy, dt, method, mthlim, 
     meqn = qold.shape[0]
     cfl = np.zeros(1)
     cp = _cparam_vector(rp)
-    maux, auxa = _aux(aux, rp)
+    maux, auxa = _aux(aux, rp, method)
     _lib.check(lib.claw2_step2(int(maxm), meqn, len(mthlim), maux, int(num_ghost), int(mx), int(my),
                                _lib.dptr(qold), _lib.dptr(out), _lib.dptr(auxa) if maux else None,
                                float(dx), float(dy), float(dt),
@@ -92,7 +94,7 @@ def step2ds(maxm, num_ghost, mx, my, qold, qnew, aux, dx, dy, dt, method, mthlim
     meqn = qold.shape[0]
     cfl = np.zeros(1)
     cp = _cparam_vector(rp)
-    maux, auxa = _aux(aux, rp)
+    maux, auxa = _aux(aux, rp, method)
     _lib.check(lib.claw2_step2ds(int(maxm), meqn, len(mthlim), maux, int(num_ghost), int(mx), int(my),
                                  _lib.dptr(qold), _lib.dptr(out), _lib.dptr(auxa) if maux else None,
                                  float(dx), float(dy), float(dt),

@@ -69,12 +69,13 @@ int rp_shape(int rp, int* meqn, int* mwaves) {
         case CLAW2_RP_SHALLOW_ROE: *meqn = 3; *mwaves = 3; return 0;
         case CLAW2_RP_EULER_EXACT: *meqn = 4; *mwaves = 3; return 0;
         case CLAW2_RP_VC_ACOUSTICS: *meqn = 3; *mwaves = 2; return 0;
+        case CLAW2_RP_VC_ADVECTION: *meqn = 1; *mwaves = 1; return 0;
         default: return -1;
     }
 }
 
-// aux components a solver reads per cell
-int rp_maux(int rp) { return rp == CLAW2_RP_VC_ACOUSTICS ? 2 : 0; }
+// aux components a solver reads per cell (the leading ones of the aux array)
+int rp_maux(int rp) { return (rp == CLAW2_RP_VC_ACOUSTICS || rp == CLAW2_RP_VC_ADVECTION) ? 2 : 0; }
 
 RPParams make_params(int rp, const double* cparam, int n) {
     RPParams p;
@@ -198,6 +199,15 @@ void unsplit_tiling(int riemann, int mx, int my, int& nstrips, int& H, int& nblo
     nblocks = (my + H - 1) / H;
 }
 
+// The capacity form (any method, rows loaded directly).
+template <class RP>
+void launch_unsplit_capa(const StepArgs& b, dim3 grid, cudaStream_t st) {
+    constexpr int smem = (int)sizeof(UnsplitSmem<RP, NT_UNSPLIT, true>);
+    static unsigned long long attr = 0;
+    smem_attr(k_step_unsplit<RP, NT_UNSPLIT, 2, SPEC_ANY, true>, smem, attr);
+    k_step_unsplit<RP, NT_UNSPLIT, 2, SPEC_ANY, true><<<grid, NT_UNSPLIT, smem, st>>>(b);
+}
+
 template <class RP, int MB>
 void launch_unsplit_v(const StepArgs& a, cudaStream_t st, const CUtensorMap* tm) {
     StepArgs b = a;
@@ -209,7 +219,8 @@ void launch_unsplit_v(const StepArgs& a, cudaStream_t st, const CUtensorMap* tm)
     }
     const int nbk = (a.L.my + b.H - 1) / b.H;
     dim3 grid(b.nstrips * nbk);
-    if (is_mc2(a.meth, RP::MWAVES)) launch_unsplit_s<RP, MB, SPEC_MC2>(b, grid, st, tm);
+    if (a.capa) launch_unsplit_capa<RP>(b, grid, st);
+    else if (is_mc2(a.meth, RP::MWAVES)) launch_unsplit_s<RP, MB, SPEC_MC2>(b, grid, st, tm);
     else launch_unsplit_s<RP, MB, SPEC_ANY>(b, grid, st, tm);
 }
 
@@ -254,6 +265,7 @@ int dispatch(int rp, A&&... args) {
         case CLAW2_RP_SHALLOW_ROE: F<RPShallowRoe>::run(args...); return 0;
         case CLAW2_RP_EULER_EXACT: F<RPEulerExact>::run(args...); return 0;
         case CLAW2_RP_VC_ACOUSTICS: F<RPVcAcoustics>::run(args...); return 0;
+        case CLAW2_RP_VC_ADVECTION: F<RPVcAdvection>::run(args...); return 0;
         default: return -1;
     }
 }
@@ -385,10 +397,13 @@ int host_step(int maxm, int meqn, int mwaves, int maux, int mbc, int mx, int my,
     if (mx < 1 || my < 1 || maxm < std::max(mx, my))
         return fail(CLAW2_EINVAL, "bad sizes mx=%d my=%d maxm=%d", mx, my, maxm);
     const int need_aux = rp_maux(rp);  // solvers without aux data ignore an aux array
-    if (need_aux > 0 && (maux != need_aux || !aux))
+    if (need_aux > 0 && (maux < need_aux || !aux))
         return fail(CLAW2_EINVAL, "solver %d reads %d aux components per cell (got %d%s)", rp, need_aux, maux,
                     aux ? "" : ", no aux array");
-    if (method[5] != 0) return fail(CLAW2_EUNSUPPORTED, "capacity functions are not in this build");
+    const int mcapa = method[5];  // method(6): 1 + the aux component of kappa, or 0
+    if (mcapa < 0 || (mcapa > 0 && (mcapa > maux || !aux)))
+        return fail(CLAW2_EINVAL, "method(6) = %d names no component of the aux array (num_aux = %d)", mcapa, maux);
+    const int nup = (need_aux > 0 || mcapa > 0) ? maux : 0;  // aux components uploaded
     if (!(dx > 0.0) || !(dy > 0.0)) return fail(CLAW2_EINVAL, "dx, dy must be positive");
     int rc = check_method(method[1], method[2], mthlim, mwaves, use_fwave);
     if (rc) return rc;
@@ -396,13 +411,14 @@ int host_step(int maxm, int meqn, int mwaves, int maux, int mbc, int mx, int my,
     std::lock_guard<std::mutex> lock(g_scr.mu);
     const Layout L = make_layout(mx, my);
     const size_t nplanes = (size_t)meqn * L.plane;
-    const size_t nstage = (size_t)std::max(meqn, need_aux) * (mx + 4) * (my + 4);
+    const size_t nqbc = (size_t)meqn * (mx + 4) * (my + 4);
+    const size_t nstage = (size_t)std::max(meqn, nup) * (mx + 4) * (my + 4);
     rc = scratch_reserve(nplanes, nstage);
     if (rc) return rc;
     cudaStream_t st = g_scr.st;
 
-    if (need_aux > 0) {  // auxbc as the caller filled it, ghost cells included
-        const size_t naux = (size_t)need_aux * L.plane;
+    if (nup > 0) {  // auxbc as the caller filled it, ghost cells included
+        const size_t naux = (size_t)nup * L.plane;
         if (naux > g_scr.aux_cap) {
             cudaFree(g_scr.aux);
             g_scr.aux = nullptr;
@@ -411,12 +427,12 @@ int host_step(int maxm, int meqn, int mwaves, int maux, int mbc, int mx, int my,
                 return fail(CLAW2_ENOMEM, "device allocation of %zu doubles failed", naux);
             g_scr.aux_cap = naux;
         }
-        const size_t na = (size_t)need_aux * (mx + 4) * (my + 4);
+        const size_t na = (size_t)nup * (mx + 4) * (my + 4);
         CUDA_TRY(cudaMemcpyAsync(g_scr.stage, aux, na * 8, cudaMemcpyHostToDevice, st));
         k_aos_to_planes<<<grid_blocks((long long)(mx + 4) * (my + 4)), 256, 0, st>>>(g_scr.stage, g_scr.aux, L,
-                                                                                    need_aux, 2);
+                                                                                    nup, 2);
     }
-    CUDA_TRY(cudaMemcpyAsync(g_scr.stage, qold, (size_t)meqn * (mx + 4) * (my + 4) * 8, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(g_scr.stage, qold, nqbc * 8, cudaMemcpyHostToDevice, st));
     k_aos_to_planes<<<grid_blocks((long long)(mx + 4) * (my + 4)), 256, 0, st>>>(g_scr.stage, g_scr.a, L, meqn, 2);
     CUDA_TRY(cudaMemsetAsync(g_scr.cfl, 0, sizeof(unsigned long long), st));
     CUDA_TRY(cudaMemsetAsync(g_scr.status, 0, sizeof(int), st));
@@ -436,6 +452,7 @@ int host_step(int maxm, int meqn, int mwaves, int maux, int mbc, int mx, int my,
     a.guess = nullptr;
     a.counters = nullptr;
     a.aux = need_aux > 0 ? g_scr.aux : nullptr;
+    a.capa = mcapa > 0 ? g_scr.aux + (size_t)(mcapa - 1) * L.plane : nullptr;
 
     a.qold = g_scr.a;
     a.qnew = g_scr.b;
@@ -451,7 +468,7 @@ int host_step(int maxm, int meqn, int mwaves, int maux, int mbc, int mx, int my,
     if (ids == 1) {
         // the x-sweep of the split step updates every row, ghost rows included,
         // and leaves ghost columns as they were: the whole qbc is the result
-        CUDA_TRY(cudaMemcpyAsync(qnew, g_scr.stage, nstage * 8, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaMemcpyAsync(qnew, g_scr.stage, nqbc * 8, cudaMemcpyDeviceToHost, st));
     } else {
         // interior cells only; ghost cells of qnew keep their entry values
         const size_t rowb = (size_t)meqn * (mx + 4) * 8;
@@ -792,6 +809,7 @@ StepArgs patch_args(claw2_patch* p, double dt) {
     a.meth = p->meth;
     a.cfl_bits = p->cfl;
     a.aux = p->aux;
+    a.capa = p->d.mcapa > 0 ? p->aux + (size_t)(p->d.mcapa - 1) * p->L.plane : nullptr;
     a.status = p->status;
     a.guess = nullptr;
     a.counters = p->counters;
@@ -862,9 +880,12 @@ int claw2_patch_create(const claw2_desc* d, claw2_patch** out) {
         return fail(CLAW2_EINVAL, "solver %d has num_eqn=%d num_waves=%d (got %d, %d)", d->riemann, me, mw,
                     d->num_eqn, d->num_waves);
     if (d->num_ghost != 2) return fail(CLAW2_EINVAL, "num_ghost must be 2 (got %d)", d->num_ghost);
-    if (d->num_aux != rp_maux(d->riemann))
+    if (d->num_aux < rp_maux(d->riemann))
         return fail(CLAW2_EINVAL, "solver %d reads %d aux components per cell (num_aux=%d)", d->riemann,
                     rp_maux(d->riemann), d->num_aux);
+    if (d->mcapa < 0 || d->mcapa > d->num_aux)
+        return fail(CLAW2_EINVAL, "mcapa = %d names no component of the aux array (num_aux = %d)", d->mcapa,
+                    d->num_aux);
     if (d->mx < 1 || d->my < 1) return fail(CLAW2_EINVAL, "bad sizes mx=%d my=%d", d->mx, d->my);
     if (!(d->dx > 0.0) || !(d->dy > 0.0)) return fail(CLAW2_EINVAL, "dx, dy must be positive");
     const int trans = d->dimensional_split ? -1 : d->transverse;
@@ -888,7 +909,8 @@ int claw2_patch_create(const claw2_desc* d, claw2_patch** out) {
     DeviceGuard g(p->device);
     cudaDeviceGetAttribute(&p->nsm, cudaDevAttrMultiProcessorCount, p->device);
     const size_t nb = (size_t)me * p->L.plane * 8;
-    const size_t ns = (size_t)std::max(me, d->num_aux) * d->mx * d->my * 8;
+    // staging: q (interior) or the aux array with its ghost cells
+    const size_t ns = std::max((size_t)me * d->mx * d->my, (size_t)d->num_aux * (d->mx + 4) * (d->my + 4)) * 8;
     bool ok = cudaMalloc(&p->q[0], nb) == cudaSuccess && cudaMalloc(&p->q[1], nb) == cudaSuccess &&
               cudaMalloc(&p->stage, ns) == cudaSuccess &&
               cudaMalloc(&p->cfl, sizeof(unsigned long long)) == cudaSuccess &&
@@ -984,6 +1006,19 @@ int claw2_patch_upload_aux(claw2_patch* p, const double* aux, const int* aux_bc_
                                                                                    p->d.num_aux, 0);
     // ghost cells of aux (solver.py:439-519 with name != 'q': a wall mirrors without sign change)
     launch_bc(p->aux, p->L, p->d.num_aux, aux_bc_lower, aux_bc_upper, nullptr, p->st, 0);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(p->st));
+    return CLAW2_OK;
+}
+
+int claw2_patch_upload_auxbc(claw2_patch* p, const double* auxbc) {
+    if (!p || !auxbc) return fail(CLAW2_EINVAL, "null pointer argument");
+    if (p->d.num_aux < 1) return fail(CLAW2_EINVAL, "this patch has no aux arrays (num_aux = 0)");
+    DeviceGuard g(p->device);
+    const size_t n = (size_t)p->d.num_aux * (p->d.mx + 4) * (p->d.my + 4);
+    CUDA_TRY(cudaMemcpyAsync(p->stage, auxbc, n * 8, cudaMemcpyHostToDevice, p->st));
+    k_aos_to_planes<<<grid_blocks((long long)(p->d.mx + 4) * (p->d.my + 4)), 256, 0, p->st>>>(p->stage, p->aux, p->L,
+                                                                                           p->d.num_aux, 2);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(p->st));
     return CLAW2_OK;
@@ -1464,6 +1499,7 @@ int claw2_batch_create(const claw2_desc* descs, int n, claw2_batch** out) {
         const claw2_desc& d = descs[i];
         if (d.riemann != d0.riemann || d.order != d0.order || d.transverse != d0.transverse || d.fwave != d0.fwave ||
             d.dimensional_split || d.num_eqn != me || d.num_waves != mw || d.num_ghost != 2 || d.num_aux != 0 ||
+            d.mcapa != 0 ||
             d.device != d0.device || std::memcmp(d.mthlim, d0.mthlim, sizeof d.mthlim) ||
             std::memcmp(d.bc_lower, d0.bc_lower, sizeof d.bc_lower) ||
             std::memcmp(d.bc_upper, d0.bc_upper, sizeof d.bc_upper) || d.ncparam != d0.ncparam ||

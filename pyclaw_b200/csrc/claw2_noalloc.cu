@@ -124,8 +124,8 @@ int claw2_step2ds_noalloc(const claw2_desc* d, const double* qold, double* qnew,
     if (d->num_eqn != meqn || d->num_waves != mwaves)
         return fail(CLAW2_EINVAL, "solver %d has num_eqn=%d num_waves=%d (got %d, %d)", d->riemann, meqn,
                     mwaves, d->num_eqn, d->num_waves);
-    if (d->num_ghost != 2 || d->num_aux != 0 || d->fwave)
-        return fail(CLAW2_EUNSUPPORTED, "num_ghost must be 2, without aux arrays or f-waves");
+    if (d->num_ghost != 2 || d->num_aux != 0 || d->mcapa != 0 || d->fwave)
+        return fail(CLAW2_EUNSUPPORTED, "num_ghost must be 2, without aux arrays, capacity or f-waves");
     if (d->mx < 1 || d->my < 1) return fail(CLAW2_EINVAL, "bad sizes mx=%d my=%d", d->mx, d->my);
     if (d->order != 1 && d->order != 2) return fail(CLAW2_EINVAL, "order must be 1 or 2");
     if (!(d->dx > 0.0) || !(d->dy > 0.0) || !(dt >= 0.0)) return fail(CLAW2_EINVAL, "dx, dy > 0 and dt >= 0 required");

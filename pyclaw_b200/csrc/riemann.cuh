@@ -661,6 +661,55 @@ struct RPVcAcoustics {
     }
 };
 
+// ---------------------------------------------------------------------------
+// vc_advection_2D: q_t + u q_x + v q_y = 0 with the velocities given on the
+// cell edges, aux = (u at the left edge, v at the bottom edge) per cell, no
+// cparam.  Cell: q, u, v.  The normal solve's one wave is the jump, moving at
+// the velocity of its interface (the left / bottom edge of the right / upper
+// cell); the transverse solve moves the part of a fluctuation that entered
+// cell k out through k's own lower transverse edge (if that velocity is
+// negative) and through the lower edge of the cell above k (if that one is
+// positive) (LeVeque 2002, sec. 9.5 and 20.5).
+// ---------------------------------------------------------------------------
+struct RPVcAdvection {
+    static constexpr int MEQN = 1, MWAVES = 1, NC = 3, MAUX = 2, ID = CLAW2_RP_VC_ADVECTION;
+    static constexpr bool TRANSVERSE_AUX = true;
+    struct Iface { double alpha[1]; double s; };
+
+    __device__ __forceinline__ static void prepare_aux(const double (&q)[MEQN], const double (&aux)[MAUX],
+                                                       const RPParams&, double (&c)[NC]) {
+        c[0] = q[0];
+        c[1] = aux[0];
+        c[2] = aux[1];
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void speeds(const Iface& f, const RPParams&, double (&s)[MWAVES]) {
+        s[0] = f.s;
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void waves(const Iface& f, const RPParams&, double (&w)[MWAVES][MEQN]) {
+        w[0][0] = f.alpha[0];
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void solve(const double (&cL)[NC], const double (&cR)[NC], const RPParams&,
+                                                 Iface& f, double (&amdq)[MEQN], double (&apdq)[MEQN]) {
+        const double vel = cR[IXY];  // the interface is the left (IXY = 1) / bottom (IXY = 2) edge of cR
+        f.alpha[0] = cR[0] - cL[0];
+        f.s = vel;
+        amdq[0] = fmin(vel, 0.0) * f.alpha[0];
+        apdq[0] = fmax(vel, 0.0) * f.alpha[0];
+    }
+    // asdq entered c0; cp is the cell above it in the transverse direction
+    template <int IXY>
+    __device__ __forceinline__ static void rpt2_aux(const double (&asdq)[MEQN], const double (&)[NC],
+                                                    const double (&c0)[NC], const double (&cp)[NC],
+                                                    double (&bm)[MEQN], double (&bp)[MEQN]) {
+        constexpr int KT = (IXY == 1) ? 2 : 1;  // the transverse velocity
+        bm[0] = fmin(c0[KT], 0.0) * asdq[0];
+        bp[0] = fmax(cp[KT], 0.0) * asdq[0];
+    }
+};
+
 // Traits for solvers whose cells carry aux data (MAUX > 0, prepare_aux) and
 // whose transverse solve needs the neighbouring cells (TRANSVERSE_AUX).
 template <class RP, class = void>

@@ -51,6 +51,11 @@ struct StepArgs {
     int nstrips = 0;
     // aux planes (same layout as q) for solvers with aux data, else nullptr
     const double* __restrict__ aux = nullptr;
+    // capacity function kappa (one plane, same layout), else nullptr: every
+    // increment of a cell is divided by its kappa, a transverse increment also
+    // by the kappa of the cell its fluctuation entered (step2.f90:132-160,
+    // flux2.f90:104-119,134-203 with dtdx1d = dtdx / kappa)
+    const double* __restrict__ capa = nullptr;
 };
 
 // philim.f90:16-35
@@ -154,6 +159,20 @@ __device__ __forceinline__ double iface_cfl(const typename RP::Iface& f, const R
     return c;
 }
 
+// With a capacity function the two sides of an interface have their own
+// dt/(dx kappa): the Courant number is max(dtdx_r s, -dtdx_l s) over the
+// waves (flux2.f90:111-119).
+template <class RP, int IXY>
+__device__ __forceinline__ double iface_cfl2(const typename RP::Iface& f, const RPParams& p, double dtdx_l,
+                                             double dtdx_r) {
+    double s[RP::MWAVES];
+    RP::template speeds<IXY>(f, p, s);
+    double c = 0.0;
+#pragma unroll
+    for (int k = 0; k < RP::MWAVES; ++k) c = fmax(c, fmax(dtdx_r * s[k], -dtdx_l * s[k]));
+    return c;
+}
+
 // aux of the cell at column pointer ap (already offset by the column), row R
 template <class RP, int MAD>
 __device__ __forceinline__ void load_aux(const double* ap, long long plane, int pitch, int R, double (&av)[MAD]) {
@@ -208,13 +227,14 @@ __device__ __forceinline__ void tma_row(const CUtensorMap* tm, double* dst, unsi
 // ---------------------------------------------------------------------------
 // Unsplit step (step2.f90), fused x + y sweeps.
 // ---------------------------------------------------------------------------
-template <class RP, int NT>
+template <class RP, int NT, bool CAPA = false>
 struct UnsplitSmem {
     static constexpr int ME = RP::MEQN, MW = RP::MWAVES, NC = RP::NC;
     double cell[3][NC][NT];  // prepared cells of rows R-2, R-1, R (ring)
     double w[MW][ME][NT];    // unlimited x-waves of row R
     double xl[4][ME][NT];    // increments for column cp-1: rows R-2, R-1, R, R+1
     double yr[2][ME][NT];    // increments for column cp+1: rows R-2, R-1
+    double icap[CAPA ? 3 : 1][CAPA ? NT : 1];  // 1 / kappa of the ring's cells (capacity form)
     double red[NT / 32];
 };
 
@@ -233,8 +253,14 @@ struct UnsplitSmemTma {
 // shared-memory read done, so a persistent CTA can start the next tile).
 // With a tensor map (tm != nullptr; qrow and bar in shared memory) the rows
 // are staged by TMA, else each thread loads its column a row ahead.
-template <class RP, int NT, int SPEC = SPEC_ANY>
-__device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int rb, UnsplitSmem<RP, NT>& S,
+//
+// CAPA: the capacity form.  Increments are summed without the receiving
+// cell's 1/kappa, which multiplies the sum when the cell is written (every
+// term of a cell carries that one factor); transverse increments carry in
+// addition the 1/kappa of the cell their fluctuation entered, the
+// second-order correction the mean of the two cells' dt/(dx kappa).
+template <class RP, int NT, int SPEC = SPEC_ANY, bool CAPA = false>
+__device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int rb, UnsplitSmem<RP, NT, CAPA>& S,
                                              double& cfl, const CUtensorMap* tm = nullptr, double* qrow = nullptr,
                                              unsigned long long* bar = nullptr) {
     constexpr int ME = RP::MEQN, MW = RP::MWAVES, NC = RP::NC, W = NT - 4;
@@ -274,10 +300,12 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
     for (int m = 0; m < ME; ++m) cxa1[m] = cxa2[m] = 0.0;
 #pragma unroll
     for (int k = 0; k < MAD; ++k) pfa[k] = (MA > 0) ? __ldg(ao + k * plane + (long long)R0 * pitch) : 0.0;
+    const double* ko = CAPA ? a.capa + cpl : nullptr;
+    double pfk = CAPA ? __ldg(ko + (long long)R0 * pitch) : 1.0;
 
     // (the copy needs a 128-byte aligned destination; anything else loads
     // directly; solvers with aux data load directly)
-    const bool tma = (MA == 0) && (tm != nullptr) && ((smem_u32(qrow) & 127u) == 0);
+    const bool tma = (MA == 0) && !CAPA && (tm != nullptr) && ((smem_u32(qrow) & 127u) == 0);
     const int x0 = strip * W;                                     // first column of the strip
     const unsigned row_bytes = (unsigned)(ME * NT * sizeof(double));
     const int tq = cpl - x0;                                      // this thread's staged column
@@ -328,6 +356,10 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
             AuxTraits<RP>::prep(q, av, P, c);
 #pragma unroll
             for (int k = 0; k < NC; ++k) S.cell[s2][k][t] = c[k];
+            if constexpr (CAPA) {
+                S.icap[s2][t] = 1.0 / pfk;
+                if (R < R1) pfk = __ldg(ko + (long long)(R + 1) * pitch);
+            }
         }
         __syncthreads();  // S1: cells of row R visible; previous exchange consumed
         if (tma && t == 0 && R < R1) {
@@ -346,6 +378,7 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
         if constexpr (TAUX) {
             if (cx_valid) {
                 const double h = 0.5 * dtdx * dtdy;
+                const double hl = CAPA ? h * S.icap[s1][tl] : h, hr = CAPA ? h * S.icap[s1][t] : h;
                 double cm[NC], c0[NC], cu[NC], bm[ME], bp[ME];
 #pragma unroll
                 for (int k = 0; k < NC; ++k) {
@@ -356,9 +389,9 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
                 RP::template rpt2_aux<1>(cxa1, cm, c0, cu, bm, bp);  // imp = 1 -> column cp-1
 #pragma unroll
                 for (int m = 0; m < ME; ++m) {
-                    dxl1[m] = h * (bp[m] - bm[m]);
-                    dxl0[m] = h * bm[m];
-                    dxl2[m] = -h * bp[m];
+                    dxl1[m] = hl * (bp[m] - bm[m]);
+                    dxl0[m] = hl * bm[m];
+                    dxl2[m] = -hl * bp[m];
                 }
 #pragma unroll
                 for (int k = 0; k < NC; ++k) {
@@ -369,9 +402,9 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
                 RP::template rpt2_aux<1>(cxa2, cm, c0, cu, bm, bp);  // imp = 2 -> column cp
 #pragma unroll
                 for (int m = 0; m < ME; ++m) {
-                    accB[m] = accB[m] + h * (bp[m] - bm[m]);
-                    accA[m] = accA[m] + h * bm[m];
-                    accC[m] = accC[m] - h * bp[m];
+                    accB[m] = accB[m] + hr * (bp[m] - bm[m]);
+                    accA[m] = accA[m] + hr * bm[m];
+                    accC[m] = accC[m] - hr * bp[m];
                 }
             }
             cx_valid = false;
@@ -412,10 +445,13 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
                 }
             }
             if (R >= R0 + 3) {
-                if (ycfl_col) cfl = fmax(cfl, iface_cfl<RP, 2>(fY, P, dtdy));
+                // capacity form: dt/(dy kappa) of the cells below (R-2) and above (R-1)
+                const double ydl = CAPA ? dtdy * S.icap[s0][t] : dtdy, ydr = CAPA ? dtdy * S.icap[s1][t] : dtdy;
+                if (ycfl_col)
+                    cfl = fmax(cfl, CAPA ? iface_cfl2<RP, 2>(fY, P, ydl, ydr) : iface_cfl<RP, 2>(fY, P, dtdy));
                 double cq[ME];
                 if (order != 1) {
-                    correction<RP, 2, SPEC>(fY, P, a.meth, dtdy, dY, dn, cq);
+                    correction<RP, 2, SPEC>(fY, P, a.meth, CAPA ? 0.5 * (ydl + ydr) : dtdy, dY, dn, cq);
                 } else {
 #pragma unroll
                     for (int m = 0; m < ME; ++m) cq[m] = 0.0;
@@ -428,6 +464,7 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
                 }
                 if (trans > 0) {
                     const double h = 0.5 * dtdy * dtdx;
+                    const double hl = CAPA ? h * S.icap[s0][t] : h, hr = CAPA ? h * S.icap[s1][t] : h;
                     double as2[ME], bm[ME], bp[ME];
 #pragma unroll
                     for (int m = 0; m < ME; ++m) as2[m] = tc ? amY[m] + cq[m] : amY[m];
@@ -445,9 +482,9 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
                     }
 #pragma unroll
                     for (int m = 0; m < ME; ++m) {
-                        accA[m] = accA[m] + h * (bp[m] - bm[m]);
-                        ylB[m] = h * bm[m];
-                        yrB[m] = -h * bp[m];
+                        accA[m] = accA[m] + hl * (bp[m] - bm[m]);
+                        ylB[m] = hl * bm[m];
+                        yrB[m] = -hl * bp[m];
                     }
 #pragma unroll
                     for (int m = 0; m < ME; ++m) as2[m] = tc ? apY[m] - cq[m] : apY[m];
@@ -465,9 +502,9 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
                     }
 #pragma unroll
                     for (int m = 0; m < ME; ++m) {
-                        accB[m] = accB[m] + h * (bp[m] - bm[m]);
-                        ylA[m] = h * bm[m];
-                        yrA[m] = -h * bp[m];
+                        accB[m] = accB[m] + hr * (bp[m] - bm[m]);
+                        ylA[m] = hr * bm[m];
+                        yrA[m] = -hr * bp[m];
                     }
                 }
             }
@@ -518,7 +555,9 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
 #pragma unroll
         for (int m = 0; m < ME; ++m) xcL[m] = xbL[m] = xaL[m] = 0.0;
         if (xrow) {
-            if (xcfl_col) cfl = fmax(cfl, iface_cfl<RP, 1>(fX, P, dtdx));
+            // capacity form: dt/(dx kappa) of the cells left (cp-1) and right (cp)
+            const double xdl = CAPA ? dtdx * S.icap[s2][tl] : dtdx, xdr = CAPA ? dtdx * S.icap[s2][t] : dtdx;
+            if (xcfl_col) cfl = fmax(cfl, CAPA ? iface_cfl2<RP, 1>(fX, P, xdl, xdr) : iface_cfl<RP, 1>(fX, P, dtdx));
             double cq[ME];
             if (order != 1) {
                 double dl[MW], dr[MW];
@@ -534,7 +573,7 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
                     dl[k] = x;
                     dr[k] = y;
                 }
-                correction<RP, 1, SPEC>(fX, P, a.meth, dtdx, dl, dr, cq);
+                correction<RP, 1, SPEC>(fX, P, a.meth, CAPA ? 0.5 * (xdl + xdr) : dtdx, dl, dr, cq);
             } else {
 #pragma unroll
                 for (int m = 0; m < ME; ++m) cq[m] = 0.0;
@@ -556,24 +595,25 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
                 }
             } else if (trans > 0) {
                 const double h = 0.5 * dtdx * dtdy;
+                const double hl = CAPA ? h * S.icap[s2][tl] : h, hr = CAPA ? h * S.icap[s2][t] : h;
                 double as2[ME], bm[ME], bp[ME];
 #pragma unroll
                 for (int m = 0; m < ME; ++m) as2[m] = tc ? amX[m] + cq[m] : amX[m];
                 RP::template rpt2<1>(fX, P, as2, bm, bp);  // imp = 1 -> column cp-1
 #pragma unroll
                 for (int m = 0; m < ME; ++m) {
-                    xcL[m] = xcL[m] + h * (bp[m] - bm[m]);
-                    xbL[m] = h * bm[m];
-                    xaL[m] = -h * bp[m];
+                    xcL[m] = xcL[m] + hl * (bp[m] - bm[m]);
+                    xbL[m] = hl * bm[m];
+                    xaL[m] = -hl * bp[m];
                 }
 #pragma unroll
                 for (int m = 0; m < ME; ++m) as2[m] = tc ? apX[m] - cq[m] : apX[m];
                 RP::template rpt2<1>(fX, P, as2, bm, bp);  // imp = 2 -> column cp
 #pragma unroll
                 for (int m = 0; m < ME; ++m) {
-                    accC[m] = accC[m] + h * (bp[m] - bm[m]);
-                    accB[m] = accB[m] + h * bm[m];
-                    accD[m] = accD[m] - h * bp[m];
+                    accC[m] = accC[m] + hr * (bp[m] - bm[m]);
+                    accB[m] = accB[m] + hr * bm[m];
+                    accD[m] = accD[m] - hr * bp[m];
                 }
             }
         }
@@ -595,8 +635,9 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
         // ---- row R-2 is complete ----
         if (R >= R0 + 4 && out_col) {
             double v[ME];
+            const double ik = CAPA ? S.icap[s0][t] : 1.0;
 #pragma unroll
-            for (int m = 0; m < ME; ++m) v[m] = S.cell[s0][m][t] + accA[m];
+            for (int m = 0; m < ME; ++m) v[m] = CAPA ? S.cell[s0][m][t] + ik * accA[m] : S.cell[s0][m][t] + accA[m];
 #pragma unroll
             for (int m = 0; m < ME; ++m) qn[m * plane + (long long)(R - 2) * pitch] = v[m];
             if (!all_finite<ME>(v)) atomicOr(a.status, 1);
@@ -639,10 +680,10 @@ __global__ void __launch_bounds__(NT, MINB) k_step_unsplit_tma(const StepArgs a,
 
 // Grid: 1D over the tiles (strip fastest).  Tile t = (strip t % nstrips, row
 // block t / nstrips); CTA b runs tile_order[b] when a schedule is given.
-template <class RP, int NT, int MINB, int SPEC>
+template <class RP, int NT, int MINB, int SPEC, bool CAPA = false>
 __global__ void __launch_bounds__(NT, MINB) k_step_unsplit(const StepArgs a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    UnsplitSmem<RP, NT>& S = *reinterpret_cast<UnsplitSmem<RP, NT>*>(smem_raw);
+    UnsplitSmem<RP, NT, CAPA>& S = *reinterpret_cast<UnsplitSmem<RP, NT, CAPA>*>(smem_raw);
     int tile = blockIdx.x;
     if (a.tile_order) {
         const int t = a.tile_order[blockIdx.x];
@@ -651,7 +692,7 @@ __global__ void __launch_bounds__(NT, MINB) k_step_unsplit(const StepArgs a) {
     long long t0 = 0;
     if (a.tile_cost && threadIdx.x == 0) t0 = clock64();
     double cfl = 0.0;
-    unsplit_tile<RP, NT, SPEC>(a, tile % a.nstrips, (tile / a.nstrips) * a.H, S, cfl);
+    unsplit_tile<RP, NT, SPEC, CAPA>(a, tile % a.nstrips, (tile / a.nstrips) * a.H, S, cfl);
     cfl_commit(cfl, S.red, a.cfl_bits);
     if (a.tile_cost && threadIdx.x == 0) {
         const long long c = clock64() - t0;
@@ -710,6 +751,7 @@ template <class RP, int NT>
 struct SplitXSmem {
     static constexpr int ME = RP::MEQN, MW = RP::MWAVES, NC = RP::NC;
     double cell[2][NC][NT];
+    double icap[2][NT];  // 1 / kappa (1 without a capacity function)
     double w[MW][ME][NT];
     double xl[ME][NT];
     double red[NT / 32];
@@ -754,6 +796,7 @@ __global__ void __launch_bounds__(NT) k_split_x(const StepArgs a) {
             AuxTraits<RP>::prep(q, av, P, c);
 #pragma unroll
             for (int k = 0; k < NC; ++k) S.cell[buf][k][t] = c[k];
+            S.icap[buf][t] = a.capa ? 1.0 / __ldg(a.capa + cpl + (long long)R * pitch) : 1.0;
         }
         __syncthreads();
         Iface fX;
@@ -774,7 +817,9 @@ __global__ void __launch_bounds__(NT) k_split_x(const StepArgs a) {
                 for (int m = 0; m < ME; ++m) S.w[k][m][t] = wX[k][m];
         }
         __syncthreads();
-        if (xcfl_col) cfl = fmax(cfl, iface_cfl<RP, 1>(fX, P, dtdx));
+        // dt/(dx kappa) left and right of the interface (both dtdx without capacity)
+        const double xdl = dtdx * S.icap[buf][tl], xdr = dtdx * S.icap[buf][t];
+        if (xcfl_col) cfl = fmax(cfl, iface_cfl2<RP, 1>(fX, P, xdl, xdr));
         double cq[ME];
         if (a.meth.order != 1) {
             double dl[MW], dr[MW];
@@ -790,7 +835,7 @@ __global__ void __launch_bounds__(NT) k_split_x(const StepArgs a) {
                 dl[k] = x;
                 dr[k] = y;
             }
-            correction<RP, 1>(fX, P, a.meth, dtdx, dl, dr, cq);
+            correction<RP, 1>(fX, P, a.meth, 0.5 * (xdl + xdr), dl, dr, cq);
         } else {
 #pragma unroll
             for (int m = 0; m < ME; ++m) cq[m] = 0.0;
@@ -800,9 +845,10 @@ __global__ void __launch_bounds__(NT) k_split_x(const StepArgs a) {
         __syncthreads();
         if (out_col) {
             double v[ME];
+            const double ik = S.icap[buf][t];
 #pragma unroll
             for (int m = 0; m < ME; ++m) {
-                v[m] = q[m] + (-dtdx * (apX[m] - 0.5 * cq[m]) + S.xl[m][tr]);
+                v[m] = q[m] + ik * (-dtdx * (apX[m] - 0.5 * cq[m]) + S.xl[m][tr]);
                 qn[m * plane + (long long)R * pitch] = v[m];
             }
             if (!all_finite<ME>(v)) atomicOr(a.status, 1);
@@ -844,6 +890,9 @@ __global__ void __launch_bounds__(NT) k_split_y(const StepArgs a) {
     Iface fY;
     double amY[ME], apY[ME], dY[MW];
     double cfl = 0.0;
+    // 1 / kappa of rows R-2 and R-1 (1 without a capacity function)
+    const double* ko = a.capa ? a.capa + cpl : nullptr;
+    double ic0 = ko ? 1.0 / __ldg(ko + (long long)R0 * pitch) : 1.0, ic1 = ic0;
     {
         double q[ME];
 #pragma unroll
@@ -868,6 +917,7 @@ __global__ void __launch_bounds__(NT) k_split_y(const StepArgs a) {
         double av[MAD];
         load_aux<RP, MAD>(a.aux + cpl, plane, pitch, R, av);
         AuxTraits<RP>::prep(q2, av, P, cA);
+        const double ic2 = ko ? 1.0 / __ldg(ko + (long long)R * pitch) : 1.0;
         Iface fN;
         double amN[ME], apN[ME];
         RP::template solve<2>(cB, cA, P, fN, amN, apN);
@@ -886,10 +936,11 @@ __global__ void __launch_bounds__(NT) k_split_y(const StepArgs a) {
         }
         // acc0 <-> row R-2, acc1 <-> row R-1
         if (R >= R0 + 3) {
-            if (valid) cfl = fmax(cfl, iface_cfl<RP, 2>(fY, P, dtdy));
+            const double ydl = dtdy * ic0, ydr = dtdy * ic1;
+            if (valid) cfl = fmax(cfl, iface_cfl2<RP, 2>(fY, P, ydl, ydr));
             double cq[ME];
             if (a.meth.order != 1) {
-                correction<RP, 2>(fY, P, a.meth, dtdy, dY, dn, cq);
+                correction<RP, 2>(fY, P, a.meth, 0.5 * (ydl + ydr), dY, dn, cq);
             } else {
 #pragma unroll
                 for (int m = 0; m < ME; ++m) cq[m] = 0.0;
@@ -904,7 +955,7 @@ __global__ void __launch_bounds__(NT) k_split_y(const StepArgs a) {
             double v[ME];
 #pragma unroll
             for (int m = 0; m < ME; ++m) {
-                v[m] = q0[m] + acc0[m];
+                v[m] = q0[m] + ic0 * acc0[m];
                 qn[m * plane + (long long)(R - 2) * pitch] = v[m];
             }
             if (!all_finite<ME>(v)) atomicOr(a.status, 1);
@@ -918,6 +969,8 @@ __global__ void __launch_bounds__(NT) k_split_y(const StepArgs a) {
             q0[m] = q1[m];
             q1[m] = q2[m];
         }
+        ic0 = ic1;
+        ic1 = ic2;
 #pragma unroll
         for (int k = 0; k < NC; ++k) cB[k] = cA[k];
 #pragma unroll

@@ -65,6 +65,12 @@ class DevicePatch(object):
         up = np.ascontiguousarray([int(b) for b in bc_upper], dtype=np.intc)
         _lib.check(self._lib.claw2_patch_upload_aux(self.h, _lib.dptr(a), _lib.iptr(lo), _lib.iptr(up)))
 
+    def push_auxbc(self, auxbc):
+        """Upload an aux array with its ghost cells already filled on the host
+        (claw2_patch_upload_auxbc)."""
+        a = np.asfortranarray(auxbc, dtype=np.float64)
+        _lib.check(self._lib.claw2_patch_upload_auxbc(self.h, _lib.dptr(a)))
+
     # ---- stepping -----------------------------------------------------------
     def set_cparam(self, vals):
         arr = (ctypes.c_double * len(vals))(*vals)

@@ -43,8 +43,17 @@ class Dimension(object):
         return np.array([self.lower + (i + 0.5) * self.delta for i in range(self.num_cells)])
 
     def centers_with_ghost(self, num_ghost):
-        return np.array([self.lower + (i + 0.5) * self.delta
-                         for i in range(-num_ghost, self.num_cells + num_ghost)])
+        """Centers of the ghost cells below, the cells, and the ghost cells
+        above, the outer ones measured from lower / upper (geometry.py:583-589)."""
+        pre = self.lower + (np.arange(-num_ghost, 0) + 0.5) * self.delta
+        post = self.upper + self.delta * (np.arange(num_ghost) + 0.5)
+        return np.hstack((pre, self.centers, post))
+
+    def nodes_with_ghost(self, num_ghost):
+        """Edges including those of the ghost cells (geometry.py:591-597)."""
+        pre = np.linspace(self.lower - num_ghost * self.delta, self.lower - self.delta, num_ghost)
+        post = np.linspace(self.upper + self.delta, self.upper + num_ghost * self.delta, num_ghost)
+        return np.hstack((pre, self.nodes, post))
 
     def __str__(self):
         return "Dimension %s:  (num_cells,delta,[lower,upper]) = (%s,%s,[%s,%s])" % (
@@ -92,6 +101,22 @@ class Grid(object):
     @property
     def p_nodes(self):
         return self.mapc2p(*self.c_nodes)
+
+    def c_centers_with_ghost(self, num_ghost):
+        """Cell centers including ghost cells (geometry.py:335-348)."""
+        idx = np.indices([n + 2 * num_ghost for n in self.num_cells])
+        return [d.centers_with_ghost(num_ghost)[idx[i, ...]] for i, d in enumerate(self._dims)]
+
+    def c_nodes_with_ghost(self, num_ghost):
+        """Cell corners including those of ghost cells (geometry.py:350-363)."""
+        idx = np.indices([n + 2 * num_ghost + 1 for n in self.num_cells])
+        return [d.nodes_with_ghost(num_ghost)[idx[i, ...]] for i, d in enumerate(self._dims)]
+
+    def p_centers_with_ghost(self, num_ghost):
+        return self.mapc2p(*self.c_centers_with_ghost(num_ghost))
+
+    def p_nodes_with_ghost(self, num_ghost):
+        return self.mapc2p(*self.c_nodes_with_ghost(num_ghost))
 
     def __getattr__(self, name):
         # grid.x, grid.y address the dimensions by name, as in the reference

@@ -59,7 +59,13 @@ euler_exact_2D = RiemannSolver('euler_exact_2D', _lib.RP_EULER_EXACT, 4, 3, ('ga
 vc_acoustics_2D = RiemannSolver('vc_acoustics_2D', _lib.RP_VC_ACOUSTICS, 3, 2, ())
 vc_acoustics_2D.num_aux = 2
 
-_ALL = [advection_2D, acoustics_2D, euler_4wave_2D, shallow_roe_with_efix_2D, euler_exact_2D, vc_acoustics_2D]
+# Advection with edge velocities: no cparam; aux = (u at the left edge, v at
+# the bottom edge) per cell (clawpack.riemann.vc_advection_2D).
+vc_advection_2D = RiemannSolver('vc_advection_2D', _lib.RP_VC_ADVECTION, 1, 1, ())
+vc_advection_2D.num_aux = 2
+
+_ALL = [advection_2D, acoustics_2D, euler_4wave_2D, shallow_roe_with_efix_2D, euler_exact_2D, vc_acoustics_2D,
+        vc_advection_2D]
 
 static = types.SimpleNamespace(
     num_eqn={s.name: s.num_eqn for s in _ALL},
@@ -75,3 +81,4 @@ shallow_roe_with_efix_2D_constants = types.SimpleNamespace(depth=0, x_momentum=1
                                                            num_eqn=3)
 acoustics_2D_constants = types.SimpleNamespace(pressure=0, x_velocity=1, y_velocity=2, num_eqn=3)
 vc_acoustics_2D_constants = types.SimpleNamespace(pressure=0, x_velocity=1, y_velocity=2, num_eqn=3)
+vc_advection_2D_constants = types.SimpleNamespace(num_eqn=1)

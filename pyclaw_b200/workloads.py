@@ -9,6 +9,7 @@ bit for bit):
   quadrants                 examples/euler_2d/quadrants.py:73-126
   radial_dam_break          examples/shallow_2d/radial_dam_break.py:23-87
   acoustics_variable        examples/acoustics_2d_variable/acoustics_2d_interface.py:23-96
+  advection_annulus         examples/advection_2d_annulus/advection_annulus.py:22-213
 The benchmark workloads are the acoustics, Euler-quadrant and shallow-water
 dam-break problems at the benchmark sizes (unsplit step, transverse
 corrections, MC limiter).
@@ -214,6 +215,99 @@ def acoustics_variable(solver_class=None, n=50, tfinal=0.6, num_output_times=20)
     state.q[0, :, :] = (np.abs(r - rad) <= width) * (1. + np.cos(np.pi * (r - rad) / width))
     state.q[1, :, :] = 0.
     state.q[2, :, :] = 0.
+    return _controller(solver, Solution(state, domain), tfinal, num_output_times=num_output_times)
+
+
+def _annulus_map(xc, yc):
+    """Polar mapping of the annulus: computational (r, theta) -> physical."""
+    return [xc * np.cos(yc), xc * np.sin(yc)]
+
+
+def _annulus_stream(xp, yp):
+    """Stream function of the rigid rotation, one turn per unit time."""
+    return np.pi * (xp ** 2 + yp ** 2)
+
+
+def annulus_edge_aux(xn, yn, dx, dy):
+    """aux of the cells spanned by the physical corner arrays xn, yn
+    (ncells + 1 per axis): [0] the velocity through each cell's left edge and
+    [1] through its bottom edge, differences of the stream function over the
+    edge divided by the computational edge length; [2] the capacity, the
+    physical area of the quadrilateral (shoelace formula) over dx dy."""
+    mx, my = xn.shape[0] - 1, xn.shape[1] - 1
+    aux = np.empty((3, mx, my), order='F')
+    x0, y0 = xn[:mx, :my], yn[:mx, :my]   # lower left
+    x1, y1 = xn[:mx, 1:], yn[:mx, 1:]     # upper left
+    x2, y2 = xn[1:, 1:], yn[1:, 1:]       # upper right
+    x3, y3 = xn[1:, :my], yn[1:, :my]     # lower right
+    aux[0, :mx, :my] = (_annulus_stream(x1, y1) - _annulus_stream(x0, y0)) / dy
+    aux[1, :mx, :my] = -(_annulus_stream(x3, y3) - _annulus_stream(x0, y0)) / dx
+    area = 1. / 2. * ((y0 + y1) * (x1 - x0) + (y1 + y2) * (x2 - x1) +
+                      (y2 + y3) * (x3 - x2) + (y3 + y0) * (x0 - x3))
+    aux[2, :mx, :my] = area / (dx * dy)
+    return aux
+
+
+def _annulus_aux_lower(state, dim, t, qbc, auxbc, num_ghost):
+    """Ghost cells inside the inner radius: the same edge velocities and
+    areas, from the mapped corners of the ghost cells."""
+    grid = state.grid
+    if dim != grid.dimensions[0]:
+        raise Exception('Custom BC for this boundary is not appropriate!')
+    dx, dy = grid.delta
+    xn, yn = grid.p_nodes_with_ghost(num_ghost=2)
+    auxbc[:, 0:num_ghost, :] = annulus_edge_aux(xn[0:num_ghost + 1, :], yn[0:num_ghost + 1, :], dx, dy)
+
+
+def _annulus_aux_upper(state, dim, t, qbc, auxbc, num_ghost):
+    """Ghost cells outside the outer radius (see _annulus_aux_lower)."""
+    grid = state.grid
+    if dim != grid.dimensions[0]:
+        raise Exception('Custom BC for this boundary is not appropriate!')
+    dx, dy = grid.delta
+    xn, yn = grid.p_nodes_with_ghost(num_ghost=2)
+    auxbc[:, -num_ghost:, :] = annulus_edge_aux(xn[-num_ghost - 1:, :], yn[-num_ghost - 1:, :], dx, dy)
+
+
+def advection_annulus(solver_class=None, m_r=40, m_theta=120, tfinal=1.0, num_output_times=10):
+    """Advection by a rigid rotation on the annulus 0.2 <= r <= 1 (a mapped
+    polar grid): vc_advection_2D with edge velocities in aux[0:2] and the
+    cell area as capacity function in aux[2] (index_capa = 2); extrapolation
+    in r and periodic in theta for q, custom (geometric) aux BCs in r;
+    unsplit, transverse corrections, van Leer limiter, cfl 0.4 / 0.5; two
+    Gaussian pulses of opposite sign."""
+    cls = solver_class or ClawSolver2D
+    solver = cls(riemann.vc_advection_2D)
+    solver.dimensional_split = False
+    solver.transverse_waves = 2
+    solver.order = 2
+    solver.bc_lower[0] = BC.extrap
+    solver.bc_upper[0] = BC.extrap
+    solver.bc_lower[1] = BC.periodic
+    solver.bc_upper[1] = BC.periodic
+    solver.aux_bc_lower[0] = BC.custom
+    solver.aux_bc_upper[0] = BC.custom
+    solver.user_aux_bc_lower = _annulus_aux_lower
+    solver.user_aux_bc_upper = _annulus_aux_upper
+    solver.aux_bc_lower[1] = BC.periodic
+    solver.aux_bc_upper[1] = BC.periodic
+    solver.dt_initial = 0.1
+    solver.cfl_max = 0.5
+    solver.cfl_desired = 0.4
+    solver.limiters = tvd.vanleer
+    r = Dimension(0.2, 1.0, m_r, name='r')
+    theta = Dimension(0.0, np.pi * 2.0, m_theta, name='theta')
+    domain = Domain([r, theta])
+    domain.grid.mapc2p = _annulus_map
+    domain.grid.num_ghost = solver.num_ghost
+    state = State(domain, 1)
+    xp, yp = state.grid.p_centers
+    pulse = [(1., 40., -0.5, 0.), (-1., 40., 0.5, 0.)]  # amplitude, decay, x, y of the centre
+    state.q[0, :, :] = sum(a * np.exp(-b * (np.square(xp - x0) + np.square(yp - y0))) for a, b, x0, y0 in pulse)
+    dx, dy = state.grid.delta
+    xn, yn = state.grid.p_nodes
+    state.aux = annulus_edge_aux(xn, yn, dx, dy)
+    state.index_capa = 2
     return _controller(solver, Solution(state, domain), tfinal, num_output_times=num_output_times)
 
 

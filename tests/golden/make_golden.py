@@ -12,6 +12,8 @@ Fortran step2/step2ds with clawpack/riemann solvers:
   examples/acoustics_2d_variable/io_test_verification/fort.q0020, fort.a0000
                                                      (test_acoustics_2d_variable_io.py:7-58)
   examples/acoustics_2d_variable/pressure_classic.txt (test_acoustics_2d_variable.py:6-23)
+  examples/advection_2d_annulus/expected_sols.npy['classic']
+                                                     (test_2d_advection_annulus.py:8-30)
 """
 import os
 import sys
@@ -54,6 +56,8 @@ def main():
     out["acoustics_variable_io_aux0"] = read_ascii_frame(os.path.join(vio, "fort.a0000"), 50, 50, 2)
     out["acoustics_variable_pressure_classic"] = np.loadtxt(
         os.path.join(ex, "acoustics_2d_variable", "pressure_classic.txt"))
+    ann = np.load(os.path.join(ex, "advection_2d_annulus", "expected_sols.npy"), allow_pickle=True).item()
+    out["advection_annulus_classic"] = ann["classic"]
     np.savez_compressed(OUT, **{k: np.asarray(v, dtype=np.float64) for k, v in out.items()})
     print("wrote", OUT, {k: np.asarray(v).shape for k, v in out.items()})
 

@@ -123,3 +123,39 @@ def test_cuda_path_fails_loudly_without_gpu():
     claw = workloads.acoustics_wall(n=16, tfinal=0.01)
     with pytest.raises(_lib.Claw2Error):
         claw.run()
+
+
+def test_host_auxbc_fill_matches_oracle(oracle):
+    # the product's host fill of auxbc for custom aux BCs (dimension by
+    # dimension, user function or built-in rule) against the oracle's
+    # restatement of Solver._apply_bcs, on the annulus (custom in r, periodic in
+    # theta) and on every built-in pair with a custom lower side in y
+    import numpy as np
+    from pyclaw_b200 import auxbc, workloads
+    from pyclaw_b200.solver import BC
+    claw = workloads.advection_annulus(m_r=12, m_theta=20)
+    solver, state = claw.solver, claw.solution.state
+    a = auxbc.fill_auxbc(solver, state, np.zeros((3, 16, 24), order='F'))
+    b = oracle.apply_aux_bcs(solver, state, np.zeros((3, 16, 24), order='F'))
+    assert np.array_equal(a, b)
+    # the ghost cells in r are the geometric values of the cells beyond the annulus
+    dx, dy = state.grid.delta
+    xn, yn = state.grid.p_nodes_with_ghost(2)
+    full = workloads.annulus_edge_aux(xn, yn, dx, dy)
+    assert np.allclose(a[:, :2, 2:-2], full[:, :2, 2:-2], rtol=0, atol=1e-14)
+
+    def lower_y(st, dim, t, qbc, aux, ng):
+        aux[:, :, :ng] = 7.0 + t
+
+    rng = np.random.default_rng(3)
+    state.aux = np.asfortranarray(rng.random((3, 12, 20)))
+    solver.user_aux_bc_lower = lower_y
+    solver.aux_bc_lower[1] = BC.custom
+    for kind in (BC.extrap, BC.wall):
+        solver.aux_bc_upper[1] = kind
+        solver.aux_bc_lower[0] = kind
+        solver.aux_bc_upper[0] = BC.periodic if kind == BC.extrap else BC.wall
+        a = auxbc.fill_auxbc(solver, state, np.zeros((3, 16, 24), order='F'))
+        b = oracle.apply_aux_bcs(solver, state, np.zeros((3, 16, 24), order='F'))
+        assert np.array_equal(a, b)
+        assert np.all(a[:, :, :2] == 7.0)

@@ -85,3 +85,19 @@ def test_vc_acoustics_goldens(oracle, goldens):
     assert rel < 1e-6
     assert rel < 1e-8  # the golden file has 8 significant digits
     assert np.max(np.abs(goldens["acoustics_variable_pressure_classic"] - q[0])) < 1e-14
+
+
+def test_annulus_golden(oracle, goldens):
+    # examples/advection_2d_annulus (classic, 40x120 polar grid, vc_advection_2D
+    # with edge velocities and the cell area as capacity function, custom aux
+    # BCs in r, unsplit trans_cor, van Leer): L1 difference weighted by the
+    # physical cell area at t = 1, < 1e-6 in test_2d_advection_annulus.py:11-30
+    from pyclaw_b200 import workloads
+    claw = workloads.advection_annulus(oracle.make_solver_class())
+    claw.run()
+    q = claw.frames[claw.num_output_times].state.get_q_global().reshape([-1])
+    dx, dy = claw.solution.domain.grid.delta
+    area = claw.frames[0].state.aux[2].reshape([-1]) * dx * dy
+    diff = np.sum(np.abs(area * (q - goldens["advection_annulus_classic"])))
+    assert diff < 1e-6
+    assert diff < 1e-13  # measured 1.8e-15
