@@ -38,7 +38,8 @@ enum {
     CLAW2_RP_SHALLOW_ROE = 4,  /* shallow_roe_with_efix_2D:   {grav, efix}           */
     CLAW2_RP_EULER_EXACT = 5,  /* exact Euler (no reference counterpart): {gamma, tol, guess} */
     CLAW2_RP_VC_ACOUSTICS = 6, /* vc_acoustics_2D: no cparam; aux = {rho, c} per cell        */
-    CLAW2_RP_VC_ADVECTION = 7  /* vc_advection_2D: no cparam; aux = {u left edge, v bottom edge} */
+    CLAW2_RP_VC_ADVECTION = 7, /* vc_advection_2D: no cparam; aux = {u left edge, v bottom edge} */
+    CLAW2_RP_PSYSTEM = 8       /* psystem_2D (f-waves): no cparam; aux = {rho, K, relation, strain} */
 };
 
 /* Boundary-condition codes: pyclaw.BC (src/pyclaw/solver.py:13-19), plus
@@ -129,6 +130,12 @@ int claw2_patch_set_cparam(claw2_patch* p, const double* cparam, int ncparam);
 /* Host <-> device copies of State.q, shape (num_eqn, mx, my), Fortran order. */
 int claw2_patch_upload_q(claw2_patch* p, const double* q);
 int claw2_patch_download_q(claw2_patch* p, double* q);
+
+/* q of the current state at n interior cells: ij holds n (i, j) pairs
+ * (0-based), out receives n * num_eqn values, cell by cell.  The gauge
+ * values of Solver.write_gauge_values (solver.py:680-715) without
+ * downloading the whole array. */
+int claw2_patch_gather_q(claw2_patch* p, int n, const int* ij, double* out);
 
 /* State.aux, shape (num_aux, mx, my), Fortran order, and its ghost cells from
  * the aux BCs (solver.py:351-519 with name 'aux': a wall mirrors without

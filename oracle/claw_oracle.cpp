@@ -255,6 +255,73 @@ void rpt2_vc_advection(int ixy, int imp, int mbc, int mx, const CSlice& aux2, co
     }
 }
 
+// psystem_2D: the two-dimensional p-system (nonlinear elasticity),
+//   eps_t - u_x - v_y = 0,  (rho u)_t - sigma(eps)_x = 0,  (rho v)_t - sigma(eps)_y = 0,
+// q = (eps, rho u, rho v), aux = (rho, K, stress-strain relation, eps at the
+// start of the step), sigma = K eps (relation 1) or exp(K eps) - 1 (relation
+// 2).  f-wave solver (LeVeque 2002, sec. 15.5; Ketcheson & LeVeque 2012 for
+// the p-system in layered media): the flux difference is split into the
+// left cell's eigenvector (1, Z, 0) at speed -c and the right cell's
+// (1, -Z, 0) at speed c, c = sqrt(sigma'(eps) / rho), Z = rho c.
+double psys_sigma(double eps, double K, double rel) { return rel == 1.0 ? K * eps : std::exp(K * eps) - 1.0; }
+double psys_sigmap(double eps, double K, double rel) { return rel == 1.0 ? K : K * std::exp(K * eps); }
+
+void rpn2_psystem(int ixy, int mbc, int mx, const CSlice& ql, const CSlice& qr, const CSlice& auxl,
+                  const CSlice& auxr, const Waves& fwave, const Speeds& s, const Slice& amdq, const Slice& apdq) {
+    const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        const double rhor = auxl(0, i), rhol = auxr(0, i - 1);
+        const double Kr = auxl(1, i), Kl = auxr(1, i - 1);
+        const double relr = auxl(2, i), rell = auxr(2, i - 1);
+        const double epsr = ql(0, i), epsl = qr(0, i - 1);
+        const double ur = ql(mu, i) / rhor, ul = qr(mu, i - 1) / rhol;
+        const double cr = std::sqrt(psys_sigmap(epsr, Kr, relr) / rhor);
+        const double cl = std::sqrt(psys_sigmap(epsl, Kl, rell) / rhol);
+        const double zr = rhor * cr, zl = rhol * cl;
+        const double df1 = -(ur - ul);
+        const double df2 = -(psys_sigma(epsr, Kr, relr) - psys_sigma(epsl, Kl, rell));
+        const double b1 = (df2 + zr * df1) / (zl + zr);
+        const double b2 = (zl * df1 - df2) / (zl + zr);
+        fwave(0, 0, i) = b1;
+        fwave(mu, 0, i) = b1 * zl;
+        fwave(mv, 0, i) = 0.0;
+        s(0, i) = -cl;
+        fwave(0, 1, i) = b2;
+        fwave(mu, 1, i) = -b2 * zr;
+        fwave(mv, 1, i) = 0.0;
+        s(1, i) = cr;
+        for (int m = 0; m < 3; ++m) {
+            amdq(m, i) = fwave(m, 0, i);
+            apdq(m, i) = fwave(m, 1, i);
+        }
+    }
+}
+// Transverse solve: asdq entered cell i1; its part going down (up) in the
+// transverse direction is the component along the cell below's (above's)
+// eigenvector in the two-medium split of the interface it crosses, times that
+// wave's speed.  Sound speeds from the strain at the start of the step
+// (aux component 4, set before each step).
+void rpt2_psystem(int ixy, int imp, int mbc, int mx, const CSlice& aux1, const CSlice& aux2, const CSlice& aux3,
+                  const Slice& asdq, const Slice& bmasdq, const Slice& bpasdq) {
+    const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        const int i1 = (imp == 1) ? i - 1 : i;
+        const double rhom = aux1(0, i1), rho0 = aux2(0, i1), rhop = aux3(0, i1);
+        const double cm = std::sqrt(psys_sigmap(aux1(3, i1), aux1(1, i1), aux1(2, i1)) / rhom);
+        const double c0 = std::sqrt(psys_sigmap(aux2(3, i1), aux2(1, i1), aux2(2, i1)) / rho0);
+        const double cp = std::sqrt(psys_sigmap(aux3(3, i1), aux3(1, i1), aux3(2, i1)) / rhop);
+        const double zm = rhom * cm, z0 = rho0 * c0, zp = rhop * cp;
+        const double bdown = (asdq(mv, i) + z0 * asdq(0, i)) / (zm + z0);
+        const double bup = (z0 * asdq(0, i) - asdq(mv, i)) / (z0 + zp);
+        bmasdq(0, i) = -cm * bdown;
+        bmasdq(mu, i) = 0.0;
+        bmasdq(mv, i) = -cm * bdown * zm;
+        bpasdq(0, i) = cp * bup;
+        bpasdq(mu, i) = 0.0;
+        bpasdq(mv, i) = -cp * bup * zp;
+    }
+}
+
 // Euler equations, Roe solver with 4 waves (u-c, entropy, shear, u+c) and an
 // optional Harten-Hyman entropy fix (LeVeque 2002, sec. 15.3.5 and 18.8;
 // Roe 1981).  The wave layout follows the reference's vendored 5-wave solver
@@ -772,11 +839,14 @@ void rpn2_euler_exact(int ixy, int mbc, int mx, int meqn, int mwaves, const CSli
 bool rp_known(int rp) {
     return rp == ORC_RP_ADVECTION || rp == ORC_RP_ACOUSTICS || rp == ORC_RP_EULER_ROE ||
            rp == ORC_RP_SHALLOW_ROE || rp == ORC_RP_EULER_EXACT || rp == ORC_RP_VC_ACOUSTICS ||
-           rp == ORC_RP_VC_ADVECTION;
+           rp == ORC_RP_VC_ADVECTION || rp == ORC_RP_PSYSTEM;
 }
 
 // aux components per cell the solver reads (the leading ones of the aux array)
-int rp_maux(int rp) { return (rp == ORC_RP_VC_ACOUSTICS || rp == ORC_RP_VC_ADVECTION) ? 2 : 0; }
+int rp_maux(int rp) {
+    if (rp == ORC_RP_PSYSTEM) return 4;
+    return (rp == ORC_RP_VC_ACOUSTICS || rp == ORC_RP_VC_ADVECTION) ? 2 : 0;
+}
 
 void call_rpn2(int rp, int ixy, int mbc, int mx, int meqn, int mwaves, const CSlice& q, const CSlice& aux2,
                const Waves& wave, const Speeds& s, const Slice& amdq, const Slice& apdq,
@@ -789,6 +859,7 @@ void call_rpn2(int rp, int ixy, int mbc, int mx, int meqn, int mwaves, const CSl
         case ORC_RP_EULER_EXACT: rpn2_euler_exact(ixy, mbc, mx, meqn, mwaves, q, q, wave, s, amdq, apdq, cp); break;
         case ORC_RP_VC_ACOUSTICS: rpn2_vc_acoustics(ixy, mbc, mx, meqn, q, q, aux2, aux2, wave, s, amdq, apdq); break;
         case ORC_RP_VC_ADVECTION: rpn2_vc_advection(ixy, mbc, mx, q, q, aux2, wave, s, amdq, apdq); break;
+        case ORC_RP_PSYSTEM: rpn2_psystem(ixy, mbc, mx, q, q, aux2, aux2, wave, s, amdq, apdq); break;
     }
 }
 void call_rpt2(int rp, int ixy, int imp, int mbc, int mx, int meqn, int mwaves, const CSlice& q,
@@ -797,6 +868,7 @@ void call_rpt2(int rp, int ixy, int imp, int mbc, int mx, int meqn, int mwaves, 
     switch (rp) {
         case ORC_RP_VC_ACOUSTICS: rpt2_vc_acoustics(ixy, imp, mbc, mx, aux1, aux2, aux3, asdq, bm, bp); break;
         case ORC_RP_VC_ADVECTION: rpt2_vc_advection(ixy, imp, mbc, mx, aux2, aux3, asdq, bm, bp); break;
+        case ORC_RP_PSYSTEM: rpt2_psystem(ixy, imp, mbc, mx, aux1, aux2, aux3, asdq, bm, bp); break;
         case ORC_RP_ADVECTION: rpt2_advection(ixy, mbc, mx, asdq, bm, bp, cp); break;
         case ORC_RP_ACOUSTICS: rpt2_acoustics(ixy, mbc, mx, asdq, bm, bp, cp); break;
         case ORC_RP_EULER_ROE: rpt2_euler_roe(ixy, mbc, mx, meqn, mwaves, q, q, asdq, bm, bp, cp); break;

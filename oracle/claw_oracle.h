@@ -39,7 +39,8 @@ enum {
     ORC_RP_SHALLOW_ROE = 4, /* shallow_roe_with_efix_2D cparam: grav, efix    */
     ORC_RP_EULER_EXACT = 5, /* exact Euler (new)      cparam: gamma, tol      */
     ORC_RP_VC_ACOUSTICS = 6, /* vc_acoustics_2D       aux: rho, c; no cparam  */
-    ORC_RP_VC_ADVECTION = 7  /* vc_advection_2D       aux: u, v edge velocities */
+    ORC_RP_VC_ADVECTION = 7, /* vc_advection_2D       aux: u, v edge velocities */
+    ORC_RP_PSYSTEM = 8       /* psystem_2D (f-waves)  aux: rho, K, relation, eps */
 };
 
 /* One unsplit step (step2.f90).  qold, qnew: (meqn, mx+2mbc, my+2mbc) F-order;

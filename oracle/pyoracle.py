@@ -207,12 +207,15 @@ def make_solver_class():
                     bc_fill_aux(aux, self.aux_bc_lower, self.aux_bc_upper)
             qold = qbc.copy('F')
             cp = self.rp.cparam(state.problem_data)
+            fw = bool(self.fwave)
             if self.dimensional_split:
-                c1 = step2ds(qold, qbc, dx, dy, self.dt, self._method, self._mthlim, 1, self.rp.rp_id, cp, aux=aux)
-                c2 = step2ds(qbc, qbc, dx, dy, self.dt, self._method, self._mthlim, 2, self.rp.rp_id, cp, aux=aux)
+                c1 = step2ds(qold, qbc, dx, dy, self.dt, self._method, self._mthlim, 1, self.rp.rp_id, cp, fw,
+                             aux=aux)
+                c2 = step2ds(qbc, qbc, dx, dy, self.dt, self._method, self._mthlim, 2, self.rp.rp_id, cp, fw,
+                             aux=aux)
                 cfl = max(c1, c2)
             else:
-                cfl = step2(qold, qbc, dx, dy, self.dt, self._method, self._mthlim, self.rp.rp_id, cp, aux=aux)
+                cfl = step2(qold, qbc, dx, dy, self.dt, self._method, self._mthlim, self.rp.rp_id, cp, fw, aux=aux)
             self.cfl.update_global_max(cfl)
             state._q = np.asfortranarray(qbc[:, 2:-2, 2:-2].copy())
 

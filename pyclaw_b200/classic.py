@@ -102,6 +102,7 @@ class ClawSolver2D(ClawSolver):
         self.device = 0
         self._dev = None
         self._aux_pushed = None  # the State.aux array last uploaded to the device
+        self._aux_copy = None    # its contents then (kept when a before-step hook may edit it)
         super(ClawSolver2D, self).__init__(riemann_solver, claw_package)
 
     def _check_cfl_settings(self):
@@ -160,8 +161,6 @@ class ClawSolver2D(ClawSolver):
                 raise Exception('One of the boundary conditions has not been set.')
             if b == BC.custom:
                 raise NotImplementedError("custom boundary conditions are not in this build")
-        if self.fwave:
-            raise NotImplementedError("f-wave Riemann solvers are not in this build")
         d = _lib.Claw2Desc()
         d.mx, d.my = grid.num_cells
         d.num_eqn, d.num_waves = state.num_eqn, self.num_waves
@@ -175,7 +174,7 @@ class ClawSolver2D(ClawSolver):
         d.order = self.order
         d.transverse = int(self.transverse_waves)
         d.dimensional_split = 1 if self.dimensional_split else 0
-        d.fwave = 0
+        d.fwave = 1 if self.fwave else 0
         for k, v in enumerate(self._mthlim):
             d.mthlim[k] = int(v)
         d.bc_lower[0], d.bc_lower[1] = self.bc_lower
@@ -209,9 +208,12 @@ class ClawSolver2D(ClawSolver):
                 self._dev.push_auxbc(new)
             self.auxbc = new
             self._aux_pushed = new
-        elif force or state.aux is not self._aux_pushed:
+        elif (force or state.aux is not self._aux_pushed or
+              (self.before_step is not None and not np.array_equal(state.aux, self._aux_copy))):
+            # a new State.aux array, or one a before-step hook edited in place
             self._dev.push_aux(state.aux, self.aux_bc_lower, self.aux_bc_upper)
             self._aux_pushed = state.aux
+            self._aux_copy = state.aux.copy(order='F') if self.before_step is not None else None
 
     def _make_device_patch(self, solution):
         from .device import DevicePatch

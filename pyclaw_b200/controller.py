@@ -29,6 +29,23 @@ class Controller(object):
         self.compute_F = None
         self.overwrite = True
         self.start_frame = 0
+        self.F_file_name = 'F'
+
+    @property
+    def F_path(self):
+        import os
+        return os.path.join(self.outdir, self.F_file_name + '.txt')
+
+    def write_F(self, mode='a'):
+        """Functionals: compute_F fills state.F, whose sums of absolute values
+        go to outdir/F.txt with the time (controller.py:399-409)."""
+        if self.compute_F is not None:
+            import os
+            self.compute_F(self.solution.state)
+            F = [self.solution.state.sum_F(i) for i in range(self.solution.state.mF)]
+            os.makedirs(self.outdir, exist_ok=True)
+            with open(self.F_path, mode) as f:
+                f.write(str(self.solution.t) + ' ' + ' '.join(str(j) for j in F) + '\n')
 
     @property
     def t(self):
@@ -42,18 +59,23 @@ class Controller(object):
             raise Exception("Initial solution is not valid.")
 
     def run(self):
-        """controller.py:275-397 without file output."""
+        """controller.py:275-397 without frame files (gauge files and the F
+        functional file are written)."""
         if self.solver is None or self.solution is None:
             raise Exception('To run, a Controller must have a Solver and a Solution.')
         if self.output_format is not None:
             raise NotImplementedError("file output is not part of pyclaw_b200; set output_format=None "
                                       "and keep_copy=True")
         self.start_frame = self.solution.start_frame
+        grid = self.solution.state.grid
+        if len(grid.gauges) > 0:
+            grid.setup_gauge_files(self.outdir)
         frame = self.start_frame
         if not self.solver._is_set_up:
             self.solver.setup(self.solution)
             self.solver.dt = self.solver.dt_initial
         self.check_validity()
+        self.solver.write_gauge_values(self.solution)  # initial gauge values
         if self.output_style == 1:
             output_times = np.linspace(self.solution.t, self.tfinal, self.num_output_times + 1)
         elif self.output_style == 2:
@@ -66,6 +88,7 @@ class Controller(object):
             return None
         if self.keep_copy:
             self.frames.append(copy.deepcopy(self.solution))
+        self.write_F('w')
         status = None
         for t in output_times[1:]:
             if self.output_style < 3:
@@ -76,6 +99,11 @@ class Controller(object):
             frame += 1
             if self.keep_copy:
                 self.frames.append(copy.deepcopy(self.solution))
+            self.write_F()
             self.logger.info("Solution %s computed for time t=%f" % (frame, self.solution.t))
+            for gfile in grid.gauge_files:
+                gfile.flush()
+        for gfile in grid.gauge_files:
+            gfile.close()
         self.solution._start_frame = len(self.frames)
         return status

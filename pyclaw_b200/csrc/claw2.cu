@@ -70,12 +70,16 @@ int rp_shape(int rp, int* meqn, int* mwaves) {
         case CLAW2_RP_EULER_EXACT: *meqn = 4; *mwaves = 3; return 0;
         case CLAW2_RP_VC_ACOUSTICS: *meqn = 3; *mwaves = 2; return 0;
         case CLAW2_RP_VC_ADVECTION: *meqn = 1; *mwaves = 1; return 0;
+        case CLAW2_RP_PSYSTEM: *meqn = 3; *mwaves = 2; return 0;
         default: return -1;
     }
 }
 
 // aux components a solver reads per cell (the leading ones of the aux array)
-int rp_maux(int rp) { return (rp == CLAW2_RP_VC_ACOUSTICS || rp == CLAW2_RP_VC_ADVECTION) ? 2 : 0; }
+int rp_maux(int rp) {
+    if (rp == CLAW2_RP_PSYSTEM) return 4;
+    return (rp == CLAW2_RP_VC_ACOUSTICS || rp == CLAW2_RP_VC_ADVECTION) ? 2 : 0;
+}
 
 RPParams make_params(int rp, const double* cparam, int n) {
     RPParams p;
@@ -163,7 +167,8 @@ struct UnsplitShape {
     int rows;
 };
 
-UnsplitShape g_tune[8] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}, {0, 0}};
+constexpr int TUNE_SLOTS = 16;  // indexed by Riemann solver id
+UnsplitShape g_tune[TUNE_SLOTS] = {};
 
 // true for the method the SPEC_MC2 kernels are compiled for
 bool is_mc2(const Method& m, int mwaves) {
@@ -194,7 +199,7 @@ void launch_unsplit_s(const StepArgs& b, dim3 grid, cudaStream_t st, const CUten
 void unsplit_tiling(int riemann, int mx, int my, int& nstrips, int& H, int& nblocks) {
     constexpr int W = NT_UNSPLIT - 4;
     nstrips = (mx + W - 1) / W;
-    const int rows = g_tune[riemann & 7].rows;
+    const int rows = g_tune[riemann & (TUNE_SLOTS - 1)].rows;
     H = rows > 0 ? rows : pick_rows(nstrips, my);
     nblocks = (my + H - 1) / H;
 }
@@ -228,7 +233,7 @@ void launch_unsplit_v(const StepArgs& a, cudaStream_t st, const CUtensorMap* tm)
 // staged by TMA (only where the caller has a tensor map of qold).
 template <class RP>
 void launch_unsplit(const StepArgs& a, cudaStream_t st, const CUtensorMap* tm) {
-    const UnsplitShape sh = g_tune[RP::ID & 7];
+    const UnsplitShape sh = g_tune[RP::ID & (TUNE_SLOTS - 1)];
     const CUtensorMap* use = (sh.variant & 2) ? tm : nullptr;
     if (sh.variant & 1) launch_unsplit_v<RP, 3>(a, st, use);
     else launch_unsplit_v<RP, 2>(a, st, use);
@@ -266,6 +271,7 @@ int dispatch(int rp, A&&... args) {
         case CLAW2_RP_EULER_EXACT: F<RPEulerExact>::run(args...); return 0;
         case CLAW2_RP_VC_ACOUSTICS: F<RPVcAcoustics>::run(args...); return 0;
         case CLAW2_RP_VC_ADVECTION: F<RPVcAdvection>::run(args...); return 0;
+        case CLAW2_RP_PSYSTEM: F<RPPsystem>::run(args...); return 0;
         default: return -1;
     }
 }
@@ -299,7 +305,7 @@ void launch_bc(double* q, const Layout& L, int meqn, const int* bcl, const int* 
 int check_method(int order, int trans, const int* mthlim, int mwaves, int fwave) {
     if (order != 1 && order != 2) return fail(CLAW2_EINVAL, "order must be 1 or 2 (got %d)", order);
     if (trans < -1 || trans > 2) return fail(CLAW2_EINVAL, "transverse must be -1..2 (got %d)", trans);
-    if (fwave) return fail(CLAW2_EUNSUPPORTED, "f-wave Riemann solvers are not in this build");
+    if (fwave != 0 && fwave != 1) return fail(CLAW2_EINVAL, "use_fwave must be 0 or 1 (got %d)", fwave);
     for (int k = 0; k < mwaves; ++k)
         if (mthlim[k] < 0 || mthlim[k] > 5) return fail(CLAW2_EINVAL, "limiter %d out of range", mthlim[k]);
     return CLAW2_OK;
@@ -731,6 +737,8 @@ struct claw2_patch {
     unsigned long long* h_cfl_hist = nullptr;
     int cfl_hist_cap = 0;
     int nsm = 0;                  // SMs of the patch's device
+    void* gather_buf = nullptr;   // claw2_patch_gather_q: values, then cell indices
+    size_t gather_cap = 0;
     CUtensorMap tmap[2];          // TMA descriptors of q[0], q[1]
     bool has_tmap = false;
     int cur = 0;
@@ -963,6 +971,7 @@ int claw2_patch_destroy(claw2_patch* p) {
         cudaFree(p->tile_cost);
         cudaFree(p->tile_order);
         cudaFree(p->stage);
+        cudaFree(p->gather_buf);
         cudaFree(p->cfl);
         cudaFree(p->status);
         cudaFreeHost(p->h_cfl);
@@ -1020,6 +1029,37 @@ int claw2_patch_upload_auxbc(claw2_patch* p, const double* auxbc) {
     k_aos_to_planes<<<grid_blocks((long long)(p->d.mx + 4) * (p->d.my + 4)), 256, 0, p->st>>>(p->stage, p->aux, p->L,
                                                                                            p->d.num_aux, 2);
     CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(p->st));
+    return CLAW2_OK;
+}
+
+int claw2_patch_gather_q(claw2_patch* p, int n, const int* ij, double* out) {
+    if (!p || (n > 0 && (!ij || !out))) return fail(CLAW2_EINVAL, "null pointer argument");
+    if (n < 0 || n > (1 << 20)) return fail(CLAW2_EINVAL, "gather of %d cells out of range", n);
+    if (n == 0) return CLAW2_OK;
+    for (int g = 0; g < n; ++g)
+        if (ij[2 * g] < 0 || ij[2 * g] >= p->d.mx || ij[2 * g + 1] < 0 || ij[2 * g + 1] >= p->d.my)
+            return fail(CLAW2_EINVAL, "cell (%d, %d) outside the %dx%d grid", ij[2 * g], ij[2 * g + 1], p->d.mx,
+                        p->d.my);
+    DeviceGuard g(p->device);
+    const int me = p->d.num_eqn;
+    const size_t need = (size_t)n * 2 * sizeof(int) + (size_t)n * me * sizeof(double);
+    if (need > p->gather_cap) {
+        cudaFree(p->gather_buf);
+        p->gather_buf = nullptr;
+        p->gather_cap = 0;
+        if (cudaMalloc(&p->gather_buf, need) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(CLAW2_ENOMEM, "gather buffer of %zu bytes could not be allocated", need);
+        }
+        p->gather_cap = need;
+    }
+    double* dout = reinterpret_cast<double*>(p->gather_buf);  // doubles first: 8-byte aligned
+    int* dij = reinterpret_cast<int*>(dout + (size_t)n * me);
+    CUDA_TRY(cudaMemcpyAsync(dij, ij, (size_t)n * 2 * sizeof(int), cudaMemcpyHostToDevice, p->st));
+    k_gather_cells<<<(n * me + 127) / 128, 128, 0, p->st>>>(p->q[p->cur], p->L, me, n, dij, dout);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(out, dout, (size_t)n * me * sizeof(double), cudaMemcpyDeviceToHost, p->st));
     CUDA_TRY(cudaStreamSynchronize(p->st));
     return CLAW2_OK;
 }
@@ -1308,18 +1348,20 @@ int claw2_selftest_rcp(int device, int n, unsigned long long seed, double* max_u
 }
 
 int claw2_tune_set(int riemann, int variant, int rows) {
-    if (riemann < 1 || riemann > 7) return fail(CLAW2_EINVAL, "unknown Riemann solver id %d", riemann);
+    int me = 0, mw = 0;
+    if (rp_shape(riemann, &me, &mw) != 0) return fail(CLAW2_EINVAL, "unknown Riemann solver id %d", riemann);
     if (variant < 0 || variant > 3) return fail(CLAW2_EINVAL, "variant must be 0..3 (got %d)", variant);
     if (rows < 0 || rows > 4096) return fail(CLAW2_EINVAL, "rows must be 0..4096 (got %d)", rows);
-    g_tune[riemann & 7].variant = variant;
-    g_tune[riemann & 7].rows = rows;
+    g_tune[riemann & (TUNE_SLOTS - 1)].variant = variant;
+    g_tune[riemann & (TUNE_SLOTS - 1)].rows = rows;
     return CLAW2_OK;
 }
 
 int claw2_tune_get(int riemann, int* variant, int* rows) {
-    if (riemann < 1 || riemann > 7 || !variant || !rows) return fail(CLAW2_EINVAL, "bad arguments");
-    *variant = g_tune[riemann & 7].variant;
-    *rows = g_tune[riemann & 7].rows;
+    int me = 0, mw = 0;
+    if (rp_shape(riemann, &me, &mw) != 0 || !variant || !rows) return fail(CLAW2_EINVAL, "bad arguments");
+    *variant = g_tune[riemann & (TUNE_SLOTS - 1)].variant;
+    *rows = g_tune[riemann & (TUNE_SLOTS - 1)].rows;
     return CLAW2_OK;
 }
 

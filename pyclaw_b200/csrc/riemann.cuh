@@ -710,6 +710,93 @@ struct RPVcAdvection {
     }
 };
 
+// ---------------------------------------------------------------------------
+// psystem_2D: the p-system of nonlinear elasticity in a heterogeneous medium,
+//   eps_t - u_x - v_y = 0,  (rho u)_t - sigma(eps)_x = 0,  (rho v)_t - sigma(eps)_y = 0,
+// q = (eps, rho u, rho v), aux = (rho, K, stress-strain relation, strain at
+// the start of the step), sigma = K eps (relation 1) or exp(K eps) - 1
+// (relation 2).  f-wave solver: the flux difference across an interface is
+// split into the left cell's eigenvector (1, Z, 0) at speed -c and the right
+// cell's (1, -Z, 0) at speed c, c = sqrt(sigma'(eps) / rho), Z = rho c
+// (LeVeque 2002, sec. 15.5).  The transverse solve splits a fluctuation at
+// the interfaces below and above the cell it entered with the impedances of
+// the cells there, from the strain in aux.
+// Cell: q, u, v, sigma, c, Z (from q) and c, Z (from the aux strain).
+// ---------------------------------------------------------------------------
+struct RPPsystem {
+    static constexpr int MEQN = 3, MWAVES = 2, NC = 10, MAUX = 4, ID = CLAW2_RP_PSYSTEM;
+    static constexpr bool TRANSVERSE_AUX = true;
+    enum { U = 3, V = 4, SIG = 5, C = 6, Z = 7, CT = 8, ZT = 9 };
+    struct Iface { double alpha[2]; double zl, zr, cl, cr; };
+
+    __device__ __forceinline__ static void material(double eps, double K, double rel, double& sig, double& sigp) {
+        if (rel == 1.0) {
+            sig = K * eps;
+            sigp = K;
+        } else {
+            const double e = exp(K * eps);
+            sig = e - 1.0;
+            sigp = K * e;
+        }
+    }
+    __device__ __forceinline__ static void prepare_aux(const double (&q)[MEQN], const double (&aux)[MAUX],
+                                                       const RPParams&, double (&c)[NC]) {
+        const double rho = aux[0], K = aux[1], rel = aux[2];
+        c[0] = q[0]; c[1] = q[1]; c[2] = q[2];
+        c[U] = q[1] / rho;
+        c[V] = q[2] / rho;
+        double sig, sigp;
+        material(q[0], K, rel, sig, sigp);
+        c[SIG] = sig;
+        c[C] = sqrt(sigp / rho);
+        c[Z] = rho * c[C];
+        double sig4, sigp4;
+        material(aux[3], K, rel, sig4, sigp4);
+        c[CT] = sqrt(sigp4 / rho);
+        c[ZT] = rho * c[CT];
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void speeds(const Iface& f, const RPParams&, double (&s)[MWAVES]) {
+        s[0] = -f.cl;
+        s[1] = f.cr;
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void waves(const Iface& f, const RPParams&, double (&w)[MWAVES][MEQN]) {
+        constexpr int MU = Dir<IXY>::MU, MV = Dir<IXY>::MV;
+        w[0][0] = f.alpha[0]; w[0][MU] = f.alpha[0] * f.zl;  w[0][MV] = 0.0;
+        w[1][0] = f.alpha[1]; w[1][MU] = -f.alpha[1] * f.zr; w[1][MV] = 0.0;
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void solve(const double (&cL)[NC], const double (&cR)[NC], const RPParams& p,
+                                                 Iface& f, double (&amdq)[MEQN], double (&apdq)[MEQN]) {
+        constexpr int VN = (IXY == 1) ? U : V;  // the normal velocity
+        const double zl = cL[Z], zr = cR[Z];
+        const double df1 = -(cR[VN] - cL[VN]);
+        const double df2 = -(cR[SIG] - cL[SIG]);
+        f.alpha[0] = (df2 + zr * df1) / (zl + zr);
+        f.alpha[1] = (zl * df1 - df2) / (zl + zr);
+        f.zl = zl; f.zr = zr; f.cl = cL[C]; f.cr = cR[C];
+        double w[MWAVES][MEQN];
+        waves<IXY>(f, p, w);
+#pragma unroll
+        for (int m = 0; m < MEQN; ++m) {
+            amdq[m] = w[0][m];
+            apdq[m] = w[1][m];
+        }
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void rpt2_aux(const double (&asdq)[MEQN], const double (&cm)[NC],
+                                                    const double (&c0)[NC], const double (&cp)[NC],
+                                                    double (&bm)[MEQN], double (&bp)[MEQN]) {
+        constexpr int MU = Dir<IXY>::MU, MV = Dir<IXY>::MV;
+        const double zm = cm[ZT], z0 = c0[ZT], zp = cp[ZT];
+        const double bdown = (asdq[MV] + z0 * asdq[0]) / (zm + z0);
+        const double bup = (z0 * asdq[0] - asdq[MV]) / (z0 + zp);
+        bm[0] = -cm[CT] * bdown; bm[MU] = 0.0; bm[MV] = -cm[CT] * bdown * zm;
+        bp[0] = cp[CT] * bup;    bp[MU] = 0.0; bp[MV] = -cp[CT] * bup * zp;
+    }
+};
+
 // Traits for solvers whose cells carry aux data (MAUX > 0, prepare_aux) and
 // whose transverse solve needs the neighbouring cells (TRANSVERSE_AUX).
 template <class RP, class = void>

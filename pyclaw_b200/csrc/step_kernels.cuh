@@ -1074,6 +1074,17 @@ static __global__ void k_planes_to_aos(const double* __restrict__ src, double* _
     }
 }
 
+// q at n interior cells (i, j) (0-based, pairs in ij) into out[k * meqn + m]:
+// the gauge values of solver.py:680-715 without moving the whole array.
+static __global__ void k_gather_cells(const double* __restrict__ q, Layout L, int meqn, int n,
+                                      const int* __restrict__ ij, double* __restrict__ out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n * meqn) return;
+    const int g = k / meqn, m = k - g * meqn;
+    const int i = ij[2 * g], j = ij[2 * g + 1];
+    out[k] = q[m * L.plane + (long long)(j + 2) * L.pitch + (i + 2)];
+}
+
 // Interior-only copy of qbc-layout planes (for the "ghosts unchanged" rule of
 // claw2_step2: qnew starts as a copy of qold).
 static __global__ void k_copy_planes(const double* __restrict__ src, double* __restrict__ dst, long long n) {

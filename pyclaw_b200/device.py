@@ -71,6 +71,14 @@ class DevicePatch(object):
         a = np.asfortranarray(auxbc, dtype=np.float64)
         _lib.check(self._lib.claw2_patch_upload_auxbc(self.h, _lib.dptr(a)))
 
+    def gather(self, cells):
+        """q at the interior cells [(i, j), ...] of the current device state,
+        shape (len(cells), num_eqn) (claw2_patch_gather_q)."""
+        ij = np.ascontiguousarray(np.asarray(cells, dtype=np.intc).reshape(-1, 2))
+        out = np.empty((len(ij), self.shape[0]))
+        _lib.check(self._lib.claw2_patch_gather_q(self.h, len(ij), _lib.iptr(ij), _lib.dptr(out)))
+        return out
+
     # ---- stepping -----------------------------------------------------------
     def set_cparam(self, vals):
         arr = (ctypes.c_double * len(vals))(*vals)

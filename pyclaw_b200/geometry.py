@@ -67,8 +67,10 @@ class Grid(object):
         if isinstance(dimensions, Dimension):
             dimensions = [dimensions]
         self._dims = list(dimensions)
-        self.gauges = []
+        self.gauges = []            # cell indices of the gauges (add_gauges)
+        self.gauge_file_names = []
         self.gauge_files = []
+        self.gauge_dir_name = '_gauges'
         self.mapc2p = lambda *xs: list(xs)
 
     dimensions = property(lambda self: list(self._dims))
@@ -118,6 +120,27 @@ class Grid(object):
     def p_nodes_with_ghost(self, num_ghost):
         return self.mapc2p(*self.c_nodes_with_ghost(num_ghost))
 
+    def add_gauges(self, gauge_coords):
+        """Record the cell index of every gauge inside this grid (lower <= x <
+        upper in each dimension) and its file name (geometry.py:392-405)."""
+        for gauge in gauge_coords:
+            if all(self.lower[n] <= gauge[n] < self.upper[n] for n in range(self.num_dim)):
+                index = [int((gauge[n] - self.lower[n]) // self.delta[n]) for n in range(self.num_dim)]
+                self.gauge_file_names.append('gauge' + '_'.join(str(c) for c in gauge) + '.txt')
+                self.gauges.append(index)
+
+    def setup_gauge_files(self, outdir):
+        """Open one file per gauge under outdir/_gauges, replacing old ones
+        (geometry.py:407-423)."""
+        import os
+        path = os.path.join(outdir, self.gauge_dir_name)
+        os.makedirs(path, exist_ok=True)
+        for name in self.gauge_file_names:
+            f = os.path.join(path, name)
+            if os.path.isfile(f):
+                os.remove(f)
+            self.gauge_files.append(open(f, 'a'))
+
     def __getattr__(self, name):
         # grid.x, grid.y address the dimensions by name, as in the reference
         for d in self.__dict__.get('_dims', []):
@@ -133,6 +156,16 @@ class Patch(object):
         self.grid = Grid(dimensions)
         self.level = 1
         self.patch_index = 1
+
+    def __deepcopy__(self, memo={}):
+        """A new patch on copies of the dimensions with the same mapping; gauges
+        and their open files stay with the original (geometry.py:725-734)."""
+        import copy
+        result = self.__class__(copy.deepcopy(self.dimensions))
+        result.grid.mapc2p = self.grid.mapc2p
+        result.level = self.level
+        result.patch_index = self.patch_index
+        return result
 
     num_dim = property(lambda self: self.grid.num_dim)
     dimensions = property(lambda self: self.grid.dimensions)

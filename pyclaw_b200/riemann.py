@@ -64,8 +64,15 @@ vc_acoustics_2D.num_aux = 2
 vc_advection_2D = RiemannSolver('vc_advection_2D', _lib.RP_VC_ADVECTION, 1, 1, ())
 vc_advection_2D.num_aux = 2
 
+# The p-system (nonlinear elasticity) in a heterogeneous medium, f-waves: no
+# cparam; aux = (density, bulk modulus, stress-strain relation 1 linear /
+# 2 exponential, strain at the start of the step) per cell
+# (clawpack.riemann.psystem_2D).
+psystem_2D = RiemannSolver('psystem_2D', _lib.RP_PSYSTEM, 3, 2, (), fwave=True)
+psystem_2D.num_aux = 4
+
 _ALL = [advection_2D, acoustics_2D, euler_4wave_2D, shallow_roe_with_efix_2D, euler_exact_2D, vc_acoustics_2D,
-        vc_advection_2D]
+        vc_advection_2D, psystem_2D]
 
 static = types.SimpleNamespace(
     num_eqn={s.name: s.num_eqn for s in _ALL},

@@ -230,6 +230,29 @@ class Solver(object):
         raise NotImplementedError("No stepping routine has been defined!")
 
     def write_gauge_values(self, solution):
-        """Gauges are not part of this package (solver.py:680-715)."""
-        if solution.state.grid.gauges:
-            raise NotImplementedError("gauges are not supported by pyclaw_b200")
+        """Values of compute_gauge_values(q, aux) at every gauge cell, appended
+        to state.gauge_data (keep_gauges) and to the gauge files
+        (solver.py:680-715).  q at the gauge cells is gathered on the device."""
+        state = solution.state
+        gauges = state.grid.gauges
+        if not gauges:
+            return
+        qg = state.gauge_q([tuple(g) for g in gauges])
+        for i, (ix, iy) in enumerate(gauges):
+            aux = state.aux[:, ix, iy] if state.num_aux > 0 else None
+            p = self.compute_gauge_values(qg[i], aux)
+            if not hasattr(p, '__iter__'):
+                p = [p]
+            t = solution.t
+            if state.keep_gauges:
+                gauge_data = state.gauge_data
+                if len(gauge_data) == len(gauges):
+                    gauge_data[i] = np.vstack((gauge_data[i], np.append(t, p)))
+                else:
+                    gauge_data.append(np.append(t, p))
+            try:
+                state.grid.gauge_files[i].write(str(t) + ' ' + ' '.join(str(j) for j in p) + '\n')
+            except IOError:
+                raise Exception("Gauge files are not set up correctly. You should call \nthe method "
+                                "`setup_gauge_files` of the Grid class object \nbefore any call for "
+                                "`write_gauge_values` from the Solver class.")

@@ -70,9 +70,32 @@ class State(object):
     def mp(self):
         return self.p.shape[0] if self.p is not None else 0
 
+    @mp.setter
+    def mp(self, mp):
+        """Allocate p, the derived quantities of compute_p (state.py:90-101)."""
+        if self.p is not None:
+            raise Exception('Cannot change state.mp after p is initialized.')
+        self.p = self.new_array(mp)
+
     @property
     def mF(self):
         return self.F.shape[0] if self.F is not None else 0
+
+    @mF.setter
+    def mF(self, mF):
+        """Allocate F, the integrands of compute_F (state.py:103-114)."""
+        if self.F is not None:
+            raise Exception('Cannot change state.mF after F is initialized.')
+        self.F = self.new_array(mF)
+
+    def gauge_q(self, cells):
+        """q at the interior cells [(i, j), ...]: gathered on the device when it
+        holds the newer q (a few values instead of the whole array)."""
+        m = self._mirror
+        if m is not None and m.device_newer:
+            return m.gather(cells)
+        q = self._q
+        return np.array([q[:, i, j] for i, j in cells]).reshape(len(cells), self.num_eqn)
 
     def is_valid(self):
         """F-contiguity and capacity-index checks (state.py:166-204)."""

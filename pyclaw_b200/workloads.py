@@ -10,6 +10,7 @@ bit for bit):
   radial_dam_break          examples/shallow_2d/radial_dam_break.py:23-87
   acoustics_variable        examples/acoustics_2d_variable/acoustics_2d_interface.py:23-96
   advection_annulus         examples/advection_2d_annulus/advection_annulus.py:22-213
+  psystem                   examples/psystem_2d/psystem_2d.py:26-235
 The benchmark workloads are the acoustics, Euler-quadrant and shallow-water
 dam-break problems at the benchmark sizes (unsplit step, transverse
 corrections, MC limiter).
@@ -309,6 +310,102 @@ def advection_annulus(solver_class=None, m_r=40, m_theta=120, tfinal=1.0, num_ou
     state.aux = annulus_edge_aux(xn, yn, dx, dy)
     state.index_capa = 2
     return _controller(solver, Solution(state, domain), tfinal, num_output_times=num_output_times)
+
+
+def psystem_checkerboard_aux(x, y, KA=1., KB=4., rhoA=1., rhoB=4., stress_rel=2):
+    """aux (4, len(x), len(y)) of the p-system's checkerboard medium of unit
+    period: density and bulk modulus A in the squares where x and y are both
+    in the lower or both in the upper half of their period, B elsewhere; the
+    stress-strain relation; 0 for the strain slot that the step hook fills."""
+    half = 0.5
+    xf = x - np.floor(x / 1.) * 1.
+    yf = y - np.floor(y / 1.) * 1.
+    yg, xg = np.meshgrid(yf, xf)
+    aux = np.zeros((4, len(x), len(y)), order='F')
+    same = (xg <= half) * (yg <= half), (xg > half) * (yg > half)
+    other = (xg > half) * (yg <= half), (xg <= half) * (yg > half)
+    aux[0, :, :] = rhoA * same[0] + rhoA * same[1] + rhoB * other[0] + rhoB * other[1]
+    aux[1, :, :] = KA * same[0] + KA * same[1] + KB * other[0] + KB * other[1]
+    aux[2, :, :] = stress_rel
+    return aux
+
+
+def _psystem_strain_to_aux(solver, state):
+    """Before each step: the strain into aux[3], where the transverse solver
+    reads it."""
+    state.aux[3, :, :] = state.q[0, :, :]
+
+
+def _psystem_gauge_stress(q, aux):
+    p = np.exp(q[0] * aux[1]) - 1
+    return [p, 10 * p]
+
+
+def _psystem_stress(state):
+    K, rel, eps = state.aux[1, :, :], state.aux[2, :, :], state.q[0, :, :]
+    state.p[0, :, :] = np.where(rel == 1, 1, 0) * K * eps + np.where(rel == 2, 1, 0) * (np.exp(eps * K) - 1)
+
+
+def _psystem_energy(state):
+    rho, K = state.aux[0, :, :], state.aux[1, :, :]
+    u, v = state.q[1, :, :] / rho, state.q[2, :, :] / rho
+    kinetic = rho * (u ** 2 + v ** 2) / 2.
+    eps = state.q[0, :, :]
+    sigma = np.exp(K * eps) - 1.
+    potential = (sigma - np.log(sigma + 1.)) / K
+    dx, dy = state.grid.delta
+    state.F[0, :, :] = (potential + kinetic) * dx * dy
+
+
+def psystem(solver_class=None, cells_per_layer=6, tfinal=1., outdir='./_output', num_output_times=10):
+    """The 2D p-system in a checkerboard medium (psystem_2D, f-waves): a
+    Gaussian stress pulse of amplitude 10 in the corner of [0.25, 20.25]^2,
+    wall BCs at the lower and extrapolation at the upper sides (q and aux),
+    superbee limiter, unsplit, cfl 0.8 / 0.9; a before-step hook copies the
+    strain into aux[3]; four stress gauges kept in memory and written under
+    outdir/_gauges; the energy functional written to outdir/F.txt."""
+    cls = solver_class or ClawSolver2D
+    solver = cls(riemann.psystem_2D)
+    solver.dimensional_split = False
+    solver.cfl_max = 0.9
+    solver.cfl_desired = 0.8
+    solver.limiters = tvd.superbee
+    solver.bc_lower[0] = BC.wall
+    solver.bc_upper[0] = BC.extrap
+    solver.bc_lower[1] = BC.wall
+    solver.bc_upper[1] = BC.extrap
+    solver.aux_bc_lower[0] = BC.wall
+    solver.aux_bc_upper[0] = BC.extrap
+    solver.aux_bc_lower[1] = BC.wall
+    solver.aux_bc_upper[1] = BC.extrap
+    solver.fwave = True
+    solver.before_step = _psystem_strain_to_aux
+    x_lower, x_upper, y_lower, y_upper = 0.25, 20.25, 0.25, 20.25
+    mx = int((x_upper - x_lower) * cells_per_layer)
+    my = int((y_upper - y_lower) * cells_per_layer)
+    domain = Domain([Dimension(x_lower, x_upper, mx, name='x'), Dimension(y_lower, y_upper, my, name='y')])
+    state = State(domain, 3, 4)
+    state.mF = 1
+    state.mp = 1
+    grid = state.grid
+    state.aux = psystem_checkerboard_aux(grid.x.centers, grid.y.centers)
+    # Gaussian stress, zero velocities (the first coordinate array of
+    # c_centers is x; the pulse is symmetric in x and y)
+    A, x0, y0, varx, vary = 10., 0.25, 0.25, 0.5, 0.5
+    cx, cy = grid.c_centers
+    stress = A * np.exp(-(cy - x0) ** 2 / (2 * varx) - (cx - y0) ** 2 / (2 * vary))
+    rel, K = state.aux[2, :], state.aux[1, :]
+    state.q[0, :, :] = np.where(rel == 1, 1, 0) * stress / K + np.where(rel == 2, 1, 0) * np.log(stress + 1) / K
+    state.q[1, :, :] = 0
+    state.q[2, :, :] = 0
+    claw = _controller(solver, Solution(state, domain), tfinal, num_output_times=num_output_times)
+    claw.outdir = outdir
+    claw.compute_F = _psystem_energy
+    claw.compute_p = _psystem_stress
+    grid.add_gauges([[0.25, 0.25], [17.85, 1.25], [3.25, 18.75], [11.75, 11.75]])
+    solver.compute_gauge_values = _psystem_gauge_stress
+    state.keep_gauges = True
+    return claw
 
 
 QUADRANT_STATES = {  # (rho, u, v, p) per quadrant, split at x = y = 0.8

@@ -14,6 +14,7 @@ Fortran step2/step2ds with clawpack/riemann solvers:
   examples/acoustics_2d_variable/pressure_classic.txt (test_acoustics_2d_variable.py:6-23)
   examples/advection_2d_annulus/expected_sols.npy['classic']
                                                      (test_2d_advection_annulus.py:8-30)
+  examples/psystem_2d/verify_gauge*.txt              (test_2d_psystem.py:8-24)
 """
 import os
 import sys
@@ -58,6 +59,8 @@ def main():
         os.path.join(ex, "acoustics_2d_variable", "pressure_classic.txt"))
     ann = np.load(os.path.join(ex, "advection_2d_annulus", "expected_sols.npy"), allow_pickle=True).item()
     out["advection_annulus_classic"] = ann["classic"]
+    for g in ("0.25_0.25", "17.85_1.25", "3.25_18.75", "11.75_11.75"):
+        out["psystem_gauge" + g] = np.loadtxt(os.path.join(ex, "psystem_2d", "verify_gauge" + g + ".txt"))
     np.savez_compressed(OUT, **{k: np.asarray(v, dtype=np.float64) for k, v in out.items()})
     print("wrote", OUT, {k: np.asarray(v).shape for k, v in out.items()})
 

@@ -159,3 +159,28 @@ def test_host_auxbc_fill_matches_oracle(oracle):
         b = oracle.apply_aux_bcs(solver, state, np.zeros((3, 16, 24), order='F'))
         assert np.array_equal(a, b)
         assert np.all(a[:, :, :2] == 7.0)
+
+
+def test_gauges_and_functional_files(oracle, tmp_path):
+    # the host loop's gauges (Grid.add_gauges / setup_gauge_files,
+    # Solver.write_gauge_values) and the F functional file on the oracle's
+    # p-system run: one row per accepted step plus the initial one, files equal
+    # to the in-memory data, gauges outside the grid dropped
+    import numpy as np
+    from pyclaw_b200 import workloads
+    claw = workloads.psystem(oracle.make_solver_class(), outdir=str(tmp_path))
+    grid = claw.solution.state.grid
+    assert grid.gauges == [[0, 0], [105, 6], [18, 111], [69, 69]]
+    grid2 = workloads.psystem(oracle.make_solver_class(), outdir=str(tmp_path / "x")).solution.state.grid
+    grid2.add_gauges([[30.0, 1.0], [0.0, 1.0]])
+    assert len(grid2.gauges) == 4
+    claw.run()
+    st = claw.solution.state
+    n = claw.solver.status['numsteps'] + 1
+    for k, f in enumerate(grid.gauge_files):
+        assert f.closed
+        data = np.loadtxt(f.name)
+        assert data.shape == (n, 3) and np.array_equal(data, st.gauge_data[k])
+    assert np.allclose(st.gauge_data[0][:, 2], 10 * st.gauge_data[0][:, 1])
+    F = np.loadtxt(str(tmp_path / "F.txt"))
+    assert F.shape == (11, 2) and np.all(F[:, 1] > 0)
