@@ -39,7 +39,9 @@ enum {
     CLAW2_RP_EULER_EXACT = 5,  /* exact Euler (no reference counterpart): {gamma, tol, guess} */
     CLAW2_RP_VC_ACOUSTICS = 6, /* vc_acoustics_2D: no cparam; aux = {rho, c} per cell        */
     CLAW2_RP_VC_ADVECTION = 7, /* vc_advection_2D: no cparam; aux = {u left edge, v bottom edge} */
-    CLAW2_RP_PSYSTEM = 8       /* psystem_2D (f-waves): no cparam; aux = {rho, K, relation, strain} */
+    CLAW2_RP_PSYSTEM = 8,      /* psystem_2D (f-waves): no cparam; aux = {rho, K, relation, strain} */
+    CLAW2_RP_VC_ADVECTION_VEC = 9 /* examples/advection_reaction_2d's own solver, num_eqn 2: aux =
+                                  {u left edge, v bottom edge}; no transverse solve */
 };
 
 /* Boundary-condition codes: pyclaw.BC (src/pyclaw/solver.py:13-19), plus
@@ -130,6 +132,11 @@ int claw2_patch_set_cparam(claw2_patch* p, const double* cparam, int ncparam);
 /* Host <-> device copies of State.q, shape (num_eqn, mx, my), Fortran order. */
 int claw2_patch_upload_q(claw2_patch* p, const double* q);
 int claw2_patch_download_q(claw2_patch* p, double* q);
+
+/* Source step on the current state (no step pending): q <- q + dt M q_old in
+ * every interior cell, M row-major n x n with n = num_eqn (a linear
+ * step_source of classic/solver.py:126-144 without leaving the device). */
+int claw2_patch_linear_source(claw2_patch* p, const double* m, int n, double dt);
 
 /* q of the current state at n interior cells: ij holds n (i, j) pairs
  * (0-based), out receives n * num_eqn values, cell by cell.  The gauge

@@ -255,6 +255,24 @@ void rpt2_vc_advection(int ixy, int imp, int mbc, int mx, const CSlice& aux2, co
     }
 }
 
+// The advection-reaction example's own solver
+// (examples/advection_reaction_2d/rpn2_vc_advection_vector.f90:40-55): the
+// vc_advection_2D normal solve applied to every component of q; no transverse
+// solve (the example's rpt2 is a stub for the split step).
+void rpn2_vc_advection_vector(int ixy, int mbc, int mx, int meqn, const CSlice& ql, const CSlice& qr,
+                              const CSlice& auxl, const Waves& wave, const Speeds& s, const Slice& amdq,
+                              const Slice& apdq) {
+    const int kn = ixy - 1;
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        s(0, i) = auxl(kn, i);
+        for (int m = 0; m < meqn; ++m) {
+            wave(m, 0, i) = ql(m, i) - qr(m, i - 1);
+            amdq(m, i) = std::min(auxl(kn, i), 0.0) * wave(m, 0, i);
+            apdq(m, i) = std::max(auxl(kn, i), 0.0) * wave(m, 0, i);
+        }
+    }
+}
+
 // psystem_2D: the two-dimensional p-system (nonlinear elasticity),
 //   eps_t - u_x - v_y = 0,  (rho u)_t - sigma(eps)_x = 0,  (rho v)_t - sigma(eps)_y = 0,
 // q = (eps, rho u, rho v), aux = (rho, K, stress-strain relation, eps at the
@@ -839,13 +857,13 @@ void rpn2_euler_exact(int ixy, int mbc, int mx, int meqn, int mwaves, const CSli
 bool rp_known(int rp) {
     return rp == ORC_RP_ADVECTION || rp == ORC_RP_ACOUSTICS || rp == ORC_RP_EULER_ROE ||
            rp == ORC_RP_SHALLOW_ROE || rp == ORC_RP_EULER_EXACT || rp == ORC_RP_VC_ACOUSTICS ||
-           rp == ORC_RP_VC_ADVECTION || rp == ORC_RP_PSYSTEM;
+           rp == ORC_RP_VC_ADVECTION || rp == ORC_RP_PSYSTEM || rp == ORC_RP_VC_ADVECTION_VEC;
 }
 
 // aux components per cell the solver reads (the leading ones of the aux array)
 int rp_maux(int rp) {
     if (rp == ORC_RP_PSYSTEM) return 4;
-    return (rp == ORC_RP_VC_ACOUSTICS || rp == ORC_RP_VC_ADVECTION) ? 2 : 0;
+    return (rp == ORC_RP_VC_ACOUSTICS || rp == ORC_RP_VC_ADVECTION || rp == ORC_RP_VC_ADVECTION_VEC) ? 2 : 0;
 }
 
 void call_rpn2(int rp, int ixy, int mbc, int mx, int meqn, int mwaves, const CSlice& q, const CSlice& aux2,
@@ -860,6 +878,7 @@ void call_rpn2(int rp, int ixy, int mbc, int mx, int meqn, int mwaves, const CSl
         case ORC_RP_VC_ACOUSTICS: rpn2_vc_acoustics(ixy, mbc, mx, meqn, q, q, aux2, aux2, wave, s, amdq, apdq); break;
         case ORC_RP_VC_ADVECTION: rpn2_vc_advection(ixy, mbc, mx, q, q, aux2, wave, s, amdq, apdq); break;
         case ORC_RP_PSYSTEM: rpn2_psystem(ixy, mbc, mx, q, q, aux2, aux2, wave, s, amdq, apdq); break;
+        case ORC_RP_VC_ADVECTION_VEC: rpn2_vc_advection_vector(ixy, mbc, mx, meqn, q, q, aux2, wave, s, amdq, apdq); break;
     }
 }
 void call_rpt2(int rp, int ixy, int imp, int mbc, int mx, int meqn, int mwaves, const CSlice& q,
@@ -1022,6 +1041,7 @@ int oracle_step2(int maxm, int meqn, int mwaves, int maux, int mbc, int mx, int 
     const int index_capa = method[5];
     if (index_capa > 0 && (aux_p == nullptr || maux < index_capa)) return 4;
     if (rp_maux(rp) > 0 && (aux_p == nullptr || maux < rp_maux(rp))) return 4;
+    if (rp == ORC_RP_VC_ADVECTION_VEC && method[2] > 0) return 5;  // no transverse solve
     Grid2 qold{const_cast<double*>(qold_p), meqn, mbc, mx};
     Grid2 qnew{qnew_p, meqn, mbc, mx};
     Grid2 aux{const_cast<double*>(aux_p), maux > 0 ? maux : 1, mbc, mx};

@@ -167,12 +167,17 @@ def apply_aux_bcs(solver, state, auxbc):
 def make_solver_class():
     """ClawSolver2D running the oracle on host arrays (built lazily so that
     importing this module does not import the product package)."""
-    from pyclaw_b200.classic import ClawSolver2D
+    from pyclaw_b200.classic import ClawSolver, ClawSolver2D
 
     class OracleClawSolver2D(ClawSolver2D):
         def __init__(self, riemann_solver=None, claw_package=None):
             self._backup = None
             super().__init__(riemann_solver, claw_package)
+
+        def step(self, solution, take_one_step, tstart, tend):
+            # classic/solver.py:96-146 on host arrays: the source step acts on
+            # state.q, which step_hyperbolic has already replaced
+            return ClawSolver.step(self, solution, take_one_step, tstart, tend)
 
         def setup(self, solution):
             self._check_cfl_settings()

@@ -19,6 +19,7 @@ RP_ADVECTION, RP_ACOUSTICS, RP_EULER_ROE, RP_SHALLOW_ROE, RP_EULER_EXACT = 1, 2,
 RP_VC_ACOUSTICS = 6
 RP_VC_ADVECTION = 7
 RP_PSYSTEM = 8
+RP_VC_ADVECTION_VEC = 9
 
 OK, EINVAL, ECUDA, ENONFINITE, ETIMEOUT, ENOMEM, EUNSUPPORTED = 0, 1, 2, 3, 4, 5, 6
 
@@ -77,6 +78,7 @@ _SIGNATURES = {
     "claw2_patch_upload_aux": (ctypes.c_int, [ctypes.c_void_p, _c_double_p, _c_int_p, _c_int_p]),
     "claw2_patch_upload_auxbc": (ctypes.c_int, [ctypes.c_void_p, _c_double_p]),
     "claw2_patch_gather_q": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _c_int_p, _c_double_p]),
+    "claw2_patch_linear_source": (ctypes.c_int, [ctypes.c_void_p, _c_double_p, ctypes.c_int, ctypes.c_double]),
     "claw2_patch_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _c_double_p]),
     "claw2_patch_run_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
                                             ctypes.POINTER(ctypes.c_void_p), _c_double_p, _c_double_p]),

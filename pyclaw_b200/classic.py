@@ -103,6 +103,8 @@ class ClawSolver2D(ClawSolver):
         self._dev = None
         self._aux_pushed = None  # the State.aux array last uploaded to the device
         self._aux_copy = None    # its contents then (kept when a before-step hook may edit it)
+        self._q_backup = None    # q before the host hooks of a step (before_step, step_source)
+        self._committed = False  # the step's result is already current (a source step followed it)
         super(ClawSolver2D, self).__init__(riemann_solver, claw_package)
 
     def _check_cfl_settings(self):
@@ -154,8 +156,6 @@ class ClawSolver2D(ClawSolver):
             for b in list(self.aux_bc_lower) + list(self.aux_bc_upper):
                 if b is None:
                     raise Exception('One of the aux boundary conditions has not been set.')
-        if self.step_source is not None:
-            raise NotImplementedError("source terms (step_source) are not in this build")
         for b in list(self.bc_lower) + list(self.bc_upper):
             if b is None:
                 raise Exception('One of the boundary conditions has not been set.')
@@ -227,10 +227,43 @@ class ClawSolver2D(ClawSolver):
 
     # ---- per-step hooks ------------------------------------------------------
     def _begin_step(self, solution):
-        pass  # the device keeps the current q untouched until accept
+        """The device keeps the current q untouched until accept, so a plain
+        step needs no backup.  Host hooks (before_step, step_source) may change
+        q before or after the hyperbolic step; for them q is kept as it was
+        before them, like the reference's q_backup (solver.py:610-612)."""
+        self._q_backup = None
+        if self.before_step is not None or self.step_source is not None:
+            self._q_backup = solution.states[0]._read_q().copy(order='F')
 
     def _end_step(self, solution, accept):
-        self._dev.accept(accept)
+        if not self._committed:
+            self._dev.accept(accept)
+        self._committed = False
+        if not accept and self._q_backup is not None:
+            solution.states[0].q = self._q_backup  # uploaded before the next step
+
+    def step(self, solution, take_one_step, tstart, tend):
+        """classic/solver.py:96-146.  With a source step the hyperbolic result
+        is committed on the device first (the source acts on it; a rejected
+        step restores the backup), and a LinearSource runs on the device."""
+        self._committed = False
+        if self.step_source is None:
+            return super(ClawSolver2D, self).step(solution, take_one_step, tstart, tend)
+        state = solution.states[0]
+        self.get_dt(solution.t, tstart, tend, take_one_step)
+        self.cfl.set_global_max(0.)
+        if self.source_split == 2:
+            self.step_source(self, state, self.dt / 2.0)
+        self.step_hyperbolic(solution)
+        if self.cfl.get_cached_max() >= self.cfl_max:
+            return False
+        self._dev.accept(True)
+        self._committed = True
+        if self.source_split == 2:
+            self.step_source(self, state, self.dt / 2.0)
+        if self.source_split == 1:
+            self.step_source(self, state, self.dt)
+        return True
 
     def step_hyperbolic(self, solution):
         """classic/solver.py:498-549 on the device: BC fill + step2 (or the

@@ -71,6 +71,7 @@ int rp_shape(int rp, int* meqn, int* mwaves) {
         case CLAW2_RP_VC_ACOUSTICS: *meqn = 3; *mwaves = 2; return 0;
         case CLAW2_RP_VC_ADVECTION: *meqn = 1; *mwaves = 1; return 0;
         case CLAW2_RP_PSYSTEM: *meqn = 3; *mwaves = 2; return 0;
+        case CLAW2_RP_VC_ADVECTION_VEC: *meqn = 2; *mwaves = 1; return 0;
         default: return -1;
     }
 }
@@ -78,7 +79,7 @@ int rp_shape(int rp, int* meqn, int* mwaves) {
 // aux components a solver reads per cell (the leading ones of the aux array)
 int rp_maux(int rp) {
     if (rp == CLAW2_RP_PSYSTEM) return 4;
-    return (rp == CLAW2_RP_VC_ACOUSTICS || rp == CLAW2_RP_VC_ADVECTION) ? 2 : 0;
+    return (rp == CLAW2_RP_VC_ACOUSTICS || rp == CLAW2_RP_VC_ADVECTION || rp == CLAW2_RP_VC_ADVECTION_VEC) ? 2 : 0;
 }
 
 RPParams make_params(int rp, const double* cparam, int n) {
@@ -272,6 +273,7 @@ int dispatch(int rp, A&&... args) {
         case CLAW2_RP_VC_ACOUSTICS: F<RPVcAcoustics>::run(args...); return 0;
         case CLAW2_RP_VC_ADVECTION: F<RPVcAdvection>::run(args...); return 0;
         case CLAW2_RP_PSYSTEM: F<RPPsystem>::run(args...); return 0;
+        case CLAW2_RP_VC_ADVECTION_VEC: F<RPVcAdvectionVec>::run(args...); return 0;
         default: return -1;
     }
 }
@@ -302,9 +304,11 @@ void launch_bc(double* q, const Layout& L, int meqn, const int* bcl, const int* 
     k_bc_fill<<<(n + 255) / 256, 256, 0, st>>>(b);
 }
 
-int check_method(int order, int trans, const int* mthlim, int mwaves, int fwave) {
+int check_method(int rp, int order, int trans, const int* mthlim, int mwaves, int fwave) {
     if (order != 1 && order != 2) return fail(CLAW2_EINVAL, "order must be 1 or 2 (got %d)", order);
     if (trans < -1 || trans > 2) return fail(CLAW2_EINVAL, "transverse must be -1..2 (got %d)", trans);
+    if (rp == CLAW2_RP_VC_ADVECTION_VEC && trans > 0)
+        return fail(CLAW2_EINVAL, "solver %d has no transverse solve: use the split step or transverse 0", rp);
     if (fwave != 0 && fwave != 1) return fail(CLAW2_EINVAL, "use_fwave must be 0 or 1 (got %d)", fwave);
     for (int k = 0; k < mwaves; ++k)
         if (mthlim[k] < 0 || mthlim[k] > 5) return fail(CLAW2_EINVAL, "limiter %d out of range", mthlim[k]);
@@ -411,7 +415,7 @@ int host_step(int maxm, int meqn, int mwaves, int maux, int mbc, int mx, int my,
         return fail(CLAW2_EINVAL, "method(6) = %d names no component of the aux array (num_aux = %d)", mcapa, maux);
     const int nup = (need_aux > 0 || mcapa > 0) ? maux : 0;  // aux components uploaded
     if (!(dx > 0.0) || !(dy > 0.0)) return fail(CLAW2_EINVAL, "dx, dy must be positive");
-    int rc = check_method(method[1], method[2], mthlim, mwaves, use_fwave);
+    int rc = check_method(rp, method[1], method[2], mthlim, mwaves, use_fwave);
     if (rc) return rc;
 
     std::lock_guard<std::mutex> lock(g_scr.mu);
@@ -897,7 +901,7 @@ int claw2_patch_create(const claw2_desc* d, claw2_patch** out) {
     if (d->mx < 1 || d->my < 1) return fail(CLAW2_EINVAL, "bad sizes mx=%d my=%d", d->mx, d->my);
     if (!(d->dx > 0.0) || !(d->dy > 0.0)) return fail(CLAW2_EINVAL, "dx, dy must be positive");
     const int trans = d->dimensional_split ? -1 : d->transverse;
-    int rc = check_method(d->order, trans, d->mthlim, mw, d->fwave);
+    int rc = check_method(d->riemann, d->order, trans, d->mthlim, mw, d->fwave);
     if (rc) return rc;
     rc = check_bc(d->bc_lower, d->bc_upper, d->mx, d->my);
     if (rc) return rc;
@@ -1061,6 +1065,21 @@ int claw2_patch_gather_q(claw2_patch* p, int n, const int* ij, double* out) {
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(out, dout, (size_t)n * me * sizeof(double), cudaMemcpyDeviceToHost, p->st));
     CUDA_TRY(cudaStreamSynchronize(p->st));
+    return CLAW2_OK;
+}
+
+int claw2_patch_linear_source(claw2_patch* p, const double* m, int n, double dt) {
+    if (!p || !m) return fail(CLAW2_EINVAL, "null pointer argument");
+    if (n != p->d.num_eqn || n > SRC_MAX)
+        return fail(CLAW2_EINVAL, "source matrix of order %d for num_eqn = %d", n, p->d.num_eqn);
+    if (p->pending) return fail(CLAW2_EINVAL, "a step is pending: accept or reject it first");
+    LinearSourceArgs a;
+    for (int k = 0; k < n * n; ++k) a.m[k] = m[k];
+    a.n = n;
+    a.dt = dt;
+    DeviceGuard g(p->device);
+    k_linear_source<<<grid_blocks((long long)p->d.mx * p->d.my), 256, 0, p->st>>>(p->q[p->cur], p->L, a);
+    CUDA_TRY(cudaGetLastError());
     return CLAW2_OK;
 }
 
@@ -1551,7 +1570,7 @@ int claw2_batch_create(const claw2_desc* descs, int n, claw2_batch** out) {
         if (d.mx < 2 || d.my < 2 || !(d.dx > 0.0) || !(d.dy > 0.0))
             return fail(CLAW2_EINVAL, "instance %d: bad sizes", i);
     }
-    int rc = check_method(d0.order, d0.transverse, d0.mthlim, mw, d0.fwave);
+    int rc = check_method(d0.riemann, d0.order, d0.transverse, d0.mthlim, mw, d0.fwave);
     if (rc) return rc;
     rc = check_bc(d0.bc_lower, d0.bc_upper, 2, 2);
     if (rc) return rc;

@@ -711,6 +711,53 @@ struct RPVcAdvection {
 };
 
 // ---------------------------------------------------------------------------
+// The advection-reaction example's own solver
+// (examples/advection_reaction_2d/rpn2_vc_advection_vector.f90): the
+// vc_advection_2D normal solve for each of the two components of q, edge
+// velocities in aux.  No transverse solve (split step, or transverse_waves = 0;
+// the host rejects anything else).  Cell: q0, q1, u, v.
+// ---------------------------------------------------------------------------
+struct RPVcAdvectionVec {
+    static constexpr int MEQN = 2, MWAVES = 1, NC = 4, MAUX = 2, ID = CLAW2_RP_VC_ADVECTION_VEC;
+    static constexpr bool TRANSVERSE_AUX = false;
+    struct Iface { double alpha[2]; double s; };
+
+    __device__ __forceinline__ static void prepare_aux(const double (&q)[MEQN], const double (&aux)[MAUX],
+                                                       const RPParams&, double (&c)[NC]) {
+        c[0] = q[0]; c[1] = q[1];
+        c[2] = aux[0];
+        c[3] = aux[1];
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void speeds(const Iface& f, const RPParams&, double (&s)[MWAVES]) {
+        s[0] = f.s;
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void waves(const Iface& f, const RPParams&, double (&w)[MWAVES][MEQN]) {
+        w[0][0] = f.alpha[0];
+        w[0][1] = f.alpha[1];
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void solve(const double (&cL)[NC], const double (&cR)[NC], const RPParams&,
+                                                 Iface& f, double (&amdq)[MEQN], double (&apdq)[MEQN]) {
+        const double vel = cR[1 + IXY];  // the velocity on the interface: the left / bottom edge of cR
+        f.s = vel;
+#pragma unroll
+        for (int m = 0; m < MEQN; ++m) {
+            f.alpha[m] = cR[m] - cL[m];
+            amdq[m] = fmin(vel, 0.0) * f.alpha[m];
+            apdq[m] = fmax(vel, 0.0) * f.alpha[m];
+        }
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void rpt2(const Iface&, const RPParams&, const double (&)[MEQN],
+                                                double (&bm)[MEQN], double (&bp)[MEQN]) {
+#pragma unroll
+        for (int m = 0; m < MEQN; ++m) bm[m] = bp[m] = 0.0;  // unreachable: the host rejects transverse solves
+    }
+};
+
+// ---------------------------------------------------------------------------
 // psystem_2D: the p-system of nonlinear elasticity in a heterogeneous medium,
 //   eps_t - u_x - v_y = 0,  (rho u)_t - sigma(eps)_x = 0,  (rho v)_t - sigma(eps)_y = 0,
 // q = (eps, rho u, rho v), aux = (rho, K, stress-strain relation, strain at

@@ -1085,6 +1085,35 @@ static __global__ void k_gather_cells(const double* __restrict__ q, Layout L, in
     out[k] = q[m * L.plane + (long long)(j + 2) * L.pitch + (i + 2)];
 }
 
+// Linear source step q <- q + (dt M) q_old in every interior cell, terms with
+// M[m][k] = 0 skipped, each product and sum rounded on its own (no fused
+// multiply-add), so the result is bit for bit the forward-Euler source step a
+// host function computes as q + (M dt) q_k.
+constexpr int SRC_MAX = CLAW2_MAX_WAVES;
+struct LinearSourceArgs {
+    double m[SRC_MAX * SRC_MAX];  // row-major, n x n
+    int n;
+    double dt;
+};
+static __global__ void k_linear_source(double* __restrict__ q, Layout L, const LinearSourceArgs a) {
+    const long long ncell = (long long)L.mx * L.my;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < ncell;
+         k += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(k % L.mx), j = (int)(k / L.mx);
+        double* c = q + (long long)(j + 2) * L.pitch + (i + 2);
+        double old[SRC_MAX];
+        for (int m = 0; m < a.n; ++m) old[m] = c[m * L.plane];
+        for (int m = 0; m < a.n; ++m) {
+            double v = old[m];
+            for (int kk = 0; kk < a.n; ++kk) {
+                const double mk = a.m[m * a.n + kk];
+                if (mk != 0.0) v = __dadd_rn(v, __dmul_rn(__dmul_rn(mk, a.dt), old[kk]));
+            }
+            c[m * L.plane] = v;
+        }
+    }
+}
+
 // Interior-only copy of qbc-layout planes (for the "ghosts unchanged" rule of
 // claw2_step2: qnew starts as a copy of qold).
 static __global__ void k_copy_planes(const double* __restrict__ src, double* __restrict__ dst, long long n) {

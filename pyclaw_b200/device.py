@@ -79,6 +79,12 @@ class DevicePatch(object):
         _lib.check(self._lib.claw2_patch_gather_q(self.h, len(ij), _lib.iptr(ij), _lib.dptr(out)))
         return out
 
+    def linear_source(self, matrix, dt):
+        """q <- q + dt M q on the device's current state (claw2_patch_linear_source)."""
+        M = np.ascontiguousarray(matrix, dtype=np.float64)
+        _lib.check(self._lib.claw2_patch_linear_source(self.h, _lib.dptr(M), M.shape[0], ctypes.c_double(dt)))
+        self.device_newer = True
+
     # ---- stepping -----------------------------------------------------------
     def set_cparam(self, vals):
         arr = (ctypes.c_double * len(vals))(*vals)

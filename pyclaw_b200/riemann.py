@@ -71,8 +71,15 @@ vc_advection_2D.num_aux = 2
 psystem_2D = RiemannSolver('psystem_2D', _lib.RP_PSYSTEM, 3, 2, (), fwave=True)
 psystem_2D.num_aux = 4
 
+# The advection-reaction example's own solver
+# (examples/advection_reaction_2d/rpn2_vc_advection_vector.f90, built there as
+# the module ``advection_2d``): vc_advection_2D's normal solve for two
+# components; no transverse solve (split step or transverse_waves = 0).
+vc_advection_vector_2D = RiemannSolver('vc_advection_vector_2D', _lib.RP_VC_ADVECTION_VEC, 2, 1, ())
+vc_advection_vector_2D.num_aux = 2
+
 _ALL = [advection_2D, acoustics_2D, euler_4wave_2D, shallow_roe_with_efix_2D, euler_exact_2D, vc_acoustics_2D,
-        vc_advection_2D, psystem_2D]
+        vc_advection_2D, psystem_2D, vc_advection_vector_2D]
 
 static = types.SimpleNamespace(
     num_eqn={s.name: s.num_eqn for s in _ALL},

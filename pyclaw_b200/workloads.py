@@ -11,6 +11,7 @@ bit for bit):
   acoustics_variable        examples/acoustics_2d_variable/acoustics_2d_interface.py:23-96
   advection_annulus         examples/advection_2d_annulus/advection_annulus.py:22-213
   psystem                   examples/psystem_2d/psystem_2d.py:26-235
+  advection_reaction        examples/advection_reaction_2d/advection_reaction.py:37-114
 The benchmark workloads are the acoustics, Euler-quadrant and shallow-water
 dam-break problems at the benchmark sizes (unsplit step, transverse
 corrections, MC limiter).
@@ -406,6 +407,74 @@ def psystem(solver_class=None, cells_per_layer=6, tfinal=1., outdir='./_output',
     solver.compute_gauge_values = _psystem_gauge_stress
     state.keep_gauges = True
     return claw
+
+
+REACTION_PERIOD = 4.0
+REACTION_RATE = 0.1
+
+
+def _reaction_source(solver, state, dt):
+    """Forward-Euler step of the reaction p' = eps q, q' = eps p."""
+    qq = state.q.copy()
+    state.q[0, :, :] = state.q[0, :, :] + REACTION_RATE * dt * qq[1, :, :]
+    state.q[1, :, :] = state.q[1, :, :] + REACTION_RATE * dt * qq[0, :, :]
+
+
+def _reaction_psi(x, y):
+    """Stream function of the swirling velocity field."""
+    return (np.sin(np.pi * x)) ** 2 * (np.sin(np.pi * y)) ** 2 / np.pi
+
+
+def _reaction_edge_velocities(aux, xn, yn, dx, dy):
+    """u on the left and v on the bottom edge of every cell from the stream
+    function at the cell corners."""
+    aux[0, :, :] = - (_reaction_psi(xn[:-1, 1:], yn[:-1, 1:]) - _reaction_psi(xn[:-1, :-1], yn[:-1, :-1])) / dy
+    aux[1, :, :] = (_reaction_psi(xn[1:, :-1], yn[1:, :-1]) - _reaction_psi(xn[:-1, :-1], yn[:-1, :-1])) / dx
+
+
+def _reaction_velocities(solver, state):
+    """Before each step: the velocity field at the middle of the step, the
+    steady field scaled by cos(2 pi t / T)."""
+    v_t = np.cos(2 * np.pi * (state.t + solver.dt / 2) / REACTION_PERIOD)
+    xn, yn = state.grid.p_nodes
+    dx, dy = state.grid.delta
+    _reaction_edge_velocities(state.aux, xn, yn, dx, dy)
+    state.aux[:] = v_t * state.aux[:]
+
+
+def advection_reaction(solver_class=None, n=100, tfinal=REACTION_PERIOD, device_source=False,
+                       num_output_times=10):
+    """Two species carried by a time-periodic swirl with edge velocities
+    (vc_advection_vector_2D, split step, no limiter choice: minmod) and a
+    linear reaction coupling them through a Godunov-split source step;
+    extrapolation BCs for q and aux; species 0 = 1 left of x = 0.5, species 1
+    = 1 below y = 0.5.  device_source: the reaction as a LinearSource, which
+    stays on the device, instead of the host function."""
+    from .sources import LinearSource
+    cls = solver_class or ClawSolver2D
+    solver = cls(riemann.vc_advection_vector_2D)
+    solver.dimensional_split = 1
+    solver.all_bcs = BC.extrap
+    solver.aux_bc_lower[0] = BC.extrap
+    solver.aux_bc_upper[0] = BC.extrap
+    solver.aux_bc_lower[1] = BC.extrap
+    solver.aux_bc_upper[1] = BC.extrap
+    domain = Domain((0., 0.), (1., 1.), (n, n))
+    solver.num_eqn = 2
+    solver.num_waves = 1
+    solver.fwave = False
+    state = State(domain, solver.num_eqn, 2)
+    xn, yn = domain.grid.p_nodes
+    xc, yc = domain.grid.p_centers
+    dx, dy = domain.grid.delta
+    _reaction_edge_velocities(state.aux, xn, yn, dx, dy)
+    solver.before_step = _reaction_velocities
+    solver.step_source = (LinearSource([[0., REACTION_RATE], [REACTION_RATE, 0.]]) if device_source
+                          else _reaction_source)
+    solver.source_split = 1
+    state.q[0, :, :] = (xc <= 0.5)
+    state.q[1, :, :] = (yc <= 0.5)
+    return _controller(solver, Solution(state, domain), tfinal, num_output_times=num_output_times)
 
 
 QUADRANT_STATES = {  # (rho, u, v, p) per quadrant, split at x = y = 0.8

@@ -15,6 +15,7 @@ Fortran step2/step2ds with clawpack/riemann solvers:
   examples/advection_2d_annulus/expected_sols.npy['classic']
                                                      (test_2d_advection_annulus.py:8-30)
   examples/psystem_2d/verify_gauge*.txt              (test_2d_psystem.py:8-24)
+  examples/advection_reaction_2d/advection_reaction.txt (test_advection_reaction.py:1-22)
 """
 import os
 import sys
@@ -61,6 +62,8 @@ def main():
     out["advection_annulus_classic"] = ann["classic"]
     for g in ("0.25_0.25", "17.85_1.25", "3.25_18.75", "11.75_11.75"):
         out["psystem_gauge" + g] = np.loadtxt(os.path.join(ex, "psystem_2d", "verify_gauge" + g + ".txt"))
+    out["advection_reaction_density"] = np.loadtxt(os.path.join(ex, "advection_reaction_2d",
+                                                                "advection_reaction.txt"))
     np.savez_compressed(OUT, **{k: np.asarray(v, dtype=np.float64) for k, v in out.items()})
     print("wrote", OUT, {k: np.asarray(v).shape for k, v in out.items()})
 
