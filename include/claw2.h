@@ -40,8 +40,9 @@ enum {
     CLAW2_RP_VC_ACOUSTICS = 6, /* vc_acoustics_2D: no cparam; aux = {rho, c} per cell        */
     CLAW2_RP_VC_ADVECTION = 7, /* vc_advection_2D: no cparam; aux = {u left edge, v bottom edge} */
     CLAW2_RP_PSYSTEM = 8,      /* psystem_2D (f-waves): no cparam; aux = {rho, K, relation, strain} */
-    CLAW2_RP_VC_ADVECTION_VEC = 9 /* examples/advection_reaction_2d's own solver, num_eqn 2: aux =
+    CLAW2_RP_VC_ADVECTION_VEC = 9, /* examples/advection_reaction_2d's own solver, num_eqn 2: aux =
                                   {u left edge, v bottom edge}; no transverse solve */
+    CLAW2_RP_EULER_5WAVE = 10  /* euler_5wave_2D (Roe + tracer):  {gamma, efix}          */
 };
 
 /* Boundary-condition codes: pyclaw.BC (src/pyclaw/solver.py:13-19), plus
@@ -138,6 +139,12 @@ int claw2_patch_download_q(claw2_patch* p, double* q);
  * step_source of classic/solver.py:126-144 without leaving the device). */
 int claw2_patch_linear_source(claw2_patch* p, const double* m, int n, double dt);
 
+/* Source step on the current state (no step pending): the geometric source
+ * of the Euler equations in r-z coordinates with cylindrical symmetry, r the
+ * aux component radius_aux, by a two-stage Runge-Kutta step (the step_source
+ * of examples/euler_2d/shock_bubble_interaction.py:113-146, bit for bit). */
+int claw2_patch_euler_axisymmetric_source(claw2_patch* p, double gamma, int radius_aux, double dt);
+
 /* q of the current state at n interior cells: ij holds n (i, j) pairs
  * (0-based), out receives n * num_eqn values, cell by cell.  The gauge
  * values of Solver.write_gauge_values (solver.py:680-715) without
@@ -150,6 +157,12 @@ int claw2_patch_gather_q(claw2_patch* p, int n, const int* ij, double* out);
  * after changing it. */
 int claw2_patch_upload_aux(claw2_patch* p, const double* aux, const int* aux_bc_lower,
                            const int* aux_bc_upper);
+
+/* qbc as the host filled it, shape (num_eqn, mx+4, my+4), Fortran order,
+ * ghost cells included, into the current state; the next step keeps these
+ * ghost cells instead of filling them (custom BCs: the user_bc_lower/upper
+ * functions that solver.py:378-427 calls). */
+int claw2_patch_upload_qbc(claw2_patch* p, const double* qbc);
 
 /* auxbc as the host filled it, shape (num_aux, mx+4, my+4), Fortran order,
  * ghost cells included: for aux BCs the host applies itself (BC.custom, the

@@ -483,6 +483,164 @@ void rpn2_euler_roe(int ixy, int mbc, int mx, int meqn, int mwaves, const CSlice
         }
 }
 
+// Euler equations with a tracer, Roe solver with five waves (acoustic,
+// shear, entropy, acoustic, tracer) and the Harten-Hyman entropy fix, in the
+// order and form of development/rp_approaches/rpn2_euler_5wave.f:86-297
+// (cparam = gamma, efix).  q = (rho, rho u, rho v, E, tracer); the tracer
+// jump moves at the Roe-averaged normal velocity.
+void rpn2_euler_5wave(int ixy, int mbc, int mx, int meqn, int mwaves, const CSlice& ql, const CSlice& qr,
+                      const Waves& wave, const Speeds& s, const Slice& amdq, const Slice& apdq, const double* cp) {
+    const double gamma = cp[0];
+    const bool efix = cp[1] != 0.0;
+    const double gamma1 = gamma - 1.0;
+    const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        double rhsqrtl = std::sqrt(qr(0, i - 1));
+        double rhsqrtr = std::sqrt(ql(0, i));
+        double pl = gamma1 * (qr(3, i - 1) - 0.5 * (qr(1, i - 1) * qr(1, i - 1) +
+                                                    qr(2, i - 1) * qr(2, i - 1)) / qr(0, i - 1));
+        double pr = gamma1 * (ql(3, i) - 0.5 * (ql(1, i) * ql(1, i) + ql(2, i) * ql(2, i)) / ql(0, i));
+        double rhsq2 = rhsqrtl + rhsqrtr;
+        double u = (qr(mu, i - 1) / rhsqrtl + ql(mu, i) / rhsqrtr) / rhsq2;
+        double v = (qr(mv, i - 1) / rhsqrtl + ql(mv, i) / rhsqrtr) / rhsq2;
+        double enth = (((qr(3, i - 1) + pl) / rhsqrtl + (ql(3, i) + pr) / rhsqrtr)) / rhsq2;
+        double u2v2 = u * u + v * v;
+        double a2 = gamma1 * (enth - 0.5 * u2v2);
+        double a = std::sqrt(a2);
+        double g1a2 = gamma1 / a2;
+        double euv = enth - u2v2;
+        double d0 = ql(0, i) - qr(0, i - 1), d1 = ql(mu, i) - qr(mu, i - 1);
+        double d2 = ql(mv, i) - qr(mv, i - 1), d3 = ql(3, i) - qr(3, i - 1);
+        double a3 = g1a2 * (euv * d0 + u * d1 + v * d2 - d3);
+        double a2w = d2 - v * d0;
+        double a4 = (d1 + (a - u) * d0 - a * a3) / (2.0 * a);
+        double a1 = d0 - a3 - a4;
+        wave(0, 0, i) = a1; wave(mu, 0, i) = a1 * (u - a); wave(mv, 0, i) = a1 * v;
+        wave(3, 0, i) = a1 * (enth - u * a); wave(4, 0, i) = 0.0; s(0, i) = u - a;
+        wave(0, 1, i) = 0.0; wave(mu, 1, i) = 0.0; wave(mv, 1, i) = a2w;
+        wave(3, 1, i) = a2w * v; wave(4, 1, i) = 0.0; s(1, i) = u;
+        wave(0, 2, i) = a3; wave(mu, 2, i) = a3 * u; wave(mv, 2, i) = a3 * v;
+        wave(3, 2, i) = a3 * 0.5 * u2v2; wave(4, 2, i) = 0.0; s(2, i) = u;
+        wave(0, 3, i) = a4; wave(mu, 3, i) = a4 * (u + a); wave(mv, 3, i) = a4 * v;
+        wave(3, 3, i) = a4 * (enth + u * a); wave(4, 3, i) = 0.0; s(3, i) = u + a;
+        wave(0, 4, i) = 0.0; wave(mu, 4, i) = 0.0; wave(mv, 4, i) = 0.0; wave(3, 4, i) = 0.0;
+        wave(4, 4, i) = ql(4, i) - qr(4, i - 1); s(4, i) = u;
+    }
+    if (!efix) {
+        for (int m = 0; m < meqn; ++m)
+            for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+                amdq(m, i) = 0.0;
+                apdq(m, i) = 0.0;
+                for (int mw = 0; mw < mwaves; ++mw) {
+                    if (s(mw, i) < 0.0) amdq(m, i) = amdq(m, i) + s(mw, i) * wave(m, mw, i);
+                    else apdq(m, i) = apdq(m, i) + s(mw, i) * wave(m, mw, i);
+                }
+            }
+        return;
+    }
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        double rhoim1 = qr(0, i - 1);
+        double pim1 = gamma1 * (qr(3, i - 1) - 0.5 * (qr(mu, i - 1) * qr(mu, i - 1) +
+                                                      qr(mv, i - 1) * qr(mv, i - 1)) / rhoim1);
+        double cim1 = std::sqrt(gamma * pim1 / rhoim1);
+        double s0 = qr(mu, i - 1) / rhoim1 - cim1;
+        if (s0 >= 0.0 && s(0, i) > 0.0) {
+            for (int m = 0; m < meqn; ++m) amdq(m, i) = 0.0;
+            continue;
+        }
+        {
+            double rho1 = qr(0, i - 1) + wave(0, 0, i);
+            double rhou1 = qr(mu, i - 1) + wave(mu, 0, i);
+            double rhov1 = qr(mv, i - 1) + wave(mv, 0, i);
+            double en1 = qr(3, i - 1) + wave(3, 0, i);
+            double p1 = gamma1 * (en1 - 0.5 * (rhou1 * rhou1 + rhov1 * rhov1) / rho1);
+            double c1 = std::sqrt(gamma * p1 / rho1);
+            double s1 = rhou1 / rho1 - c1;
+            double sfract;
+            if (s0 < 0.0 && s1 > 0.0) sfract = s0 * (s1 - s(0, i)) / (s1 - s0);
+            else if (s(0, i) < 0.0) sfract = s(0, i);
+            else sfract = 0.0;
+            for (int m = 0; m < meqn; ++m) amdq(m, i) = sfract * wave(m, 0, i);
+        }
+        if (s(1, i) >= 0.0) continue;
+        for (int m = 0; m < meqn; ++m) {
+            amdq(m, i) = amdq(m, i) + s(1, i) * wave(m, 1, i);
+            amdq(m, i) = amdq(m, i) + s(2, i) * wave(m, 2, i);
+            amdq(m, i) = amdq(m, i) + s(4, i) * wave(m, 4, i);
+        }
+        {
+            double rhoi = ql(0, i);
+            double pi = gamma1 * (ql(3, i) - 0.5 * (ql(mu, i) * ql(mu, i) + ql(mv, i) * ql(mv, i)) / rhoi);
+            double ci = std::sqrt(gamma * pi / rhoi);
+            double s3 = ql(mu, i) / rhoi + ci;
+            double rho2 = ql(0, i) - wave(0, 3, i);
+            double rhou2 = ql(mu, i) - wave(mu, 3, i);
+            double rhov2 = ql(mv, i) - wave(mv, 3, i);
+            double en2 = ql(3, i) - wave(3, 3, i);
+            double p2 = gamma1 * (en2 - 0.5 * (rhou2 * rhou2 + rhov2 * rhov2) / rho2);
+            double c2 = std::sqrt(gamma * p2 / rho2);
+            double s2 = rhou2 / rho2 + c2;
+            double sfract;
+            if (s2 < 0.0 && s3 > 0.0) sfract = s2 * (s3 - s(3, i)) / (s3 - s2);
+            else if (s(3, i) < 0.0) sfract = s(3, i);
+            else continue;
+            for (int m = 0; m < meqn; ++m) amdq(m, i) = amdq(m, i) + sfract * wave(m, 3, i);
+        }
+    }
+    for (int m = 0; m < meqn; ++m)
+        for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+            double df = 0.0;
+            for (int mw = 0; mw < mwaves; ++mw) df = df + s(mw, i) * wave(m, mw, i);
+            apdq(m, i) = df - amdq(m, i);
+        }
+}
+
+// Transverse split of the 5-wave solver (rpt2_euler_5wave.f:47-95): the Roe
+// state of the interface, four transverse waves (acoustic, shear+entropy,
+// acoustic, tracer).
+void rpt2_euler_5wave(int ixy, int mbc, int mx, int meqn, const CSlice& ql, const CSlice& qr, const Slice& asdq,
+                      const Slice& bmasdq, const Slice& bpasdq, const double* cp) {
+    const double gamma1 = cp[0] - 1.0;
+    const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
+    double waveb[4][5], sb[4];
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        double rhsqrtl = std::sqrt(qr(0, i - 1));
+        double rhsqrtr = std::sqrt(ql(0, i));
+        double pl = gamma1 * (qr(3, i - 1) - 0.5 * (qr(1, i - 1) * qr(1, i - 1) +
+                                                    qr(2, i - 1) * qr(2, i - 1)) / qr(0, i - 1));
+        double pr = gamma1 * (ql(3, i) - 0.5 * (ql(1, i) * ql(1, i) + ql(2, i) * ql(2, i)) / ql(0, i));
+        double rhsq2 = rhsqrtl + rhsqrtr;
+        double u = (qr(mu, i - 1) / rhsqrtl + ql(mu, i) / rhsqrtr) / rhsq2;
+        double v = (qr(mv, i - 1) / rhsqrtl + ql(mv, i) / rhsqrtr) / rhsq2;
+        double enth = (((qr(3, i - 1) + pl) / rhsqrtl + (ql(3, i) + pr) / rhsqrtr)) / rhsq2;
+        double u2v2 = u * u + v * v;
+        double a2 = gamma1 * (enth - 0.5 * u2v2);
+        double a = std::sqrt(a2);
+        double g1a2 = gamma1 / a2;
+        double euv = enth - u2v2;
+        double a3 = g1a2 * (euv * asdq(0, i) + u * asdq(mu, i) + v * asdq(mv, i) - asdq(3, i));
+        double a2w = asdq(mu, i) - u * asdq(0, i);
+        double a4 = (asdq(mv, i) + (a - v) * asdq(0, i) - a * a3) / (2.0 * a);
+        double a1 = asdq(0, i) - a3 - a4;
+        waveb[0][0] = a1; waveb[0][mu] = a1 * u; waveb[0][mv] = a1 * (v - a);
+        waveb[0][3] = a1 * (enth - v * a); waveb[0][4] = 0.0; sb[0] = v - a;
+        waveb[1][0] = a3; waveb[1][mu] = a3 * u + a2w; waveb[1][mv] = a3 * v;
+        waveb[1][3] = a3 * 0.5 * u2v2 + a2w * u; waveb[1][4] = 0.0; sb[1] = v;
+        waveb[2][0] = a4; waveb[2][mu] = a4 * u; waveb[2][mv] = a4 * (v + a);
+        waveb[2][3] = a4 * (enth + v * a); waveb[2][4] = 0.0; sb[2] = v + a;
+        waveb[3][0] = 0.0; waveb[3][mu] = 0.0; waveb[3][mv] = 0.0; waveb[3][3] = 0.0;
+        waveb[3][4] = asdq(4, i); sb[3] = v;
+        for (int m = 0; m < meqn; ++m) {
+            bmasdq(m, i) = 0.0;
+            bpasdq(m, i) = 0.0;
+            for (int mw = 0; mw < 4; ++mw) {
+                bmasdq(m, i) = bmasdq(m, i) + std::min(sb[mw], 0.0) * waveb[mw][m];
+                bpasdq(m, i) = bpasdq(m, i) + std::max(sb[mw], 0.0) * waveb[mw][m];
+            }
+        }
+    }
+}
+
 // Transverse Roe split for Euler: decompose asdq on the eigenvectors of the
 // transverse Jacobian at the same Roe-averaged state and keep the down- and
 // up-going parts (LeVeque 2002, sec. 21.6; reference structure
@@ -857,7 +1015,8 @@ void rpn2_euler_exact(int ixy, int mbc, int mx, int meqn, int mwaves, const CSli
 bool rp_known(int rp) {
     return rp == ORC_RP_ADVECTION || rp == ORC_RP_ACOUSTICS || rp == ORC_RP_EULER_ROE ||
            rp == ORC_RP_SHALLOW_ROE || rp == ORC_RP_EULER_EXACT || rp == ORC_RP_VC_ACOUSTICS ||
-           rp == ORC_RP_VC_ADVECTION || rp == ORC_RP_PSYSTEM || rp == ORC_RP_VC_ADVECTION_VEC;
+           rp == ORC_RP_VC_ADVECTION || rp == ORC_RP_PSYSTEM || rp == ORC_RP_VC_ADVECTION_VEC ||
+           rp == ORC_RP_EULER_5WAVE;
 }
 
 // aux components per cell the solver reads (the leading ones of the aux array)
@@ -879,6 +1038,7 @@ void call_rpn2(int rp, int ixy, int mbc, int mx, int meqn, int mwaves, const CSl
         case ORC_RP_VC_ADVECTION: rpn2_vc_advection(ixy, mbc, mx, q, q, aux2, wave, s, amdq, apdq); break;
         case ORC_RP_PSYSTEM: rpn2_psystem(ixy, mbc, mx, q, q, aux2, aux2, wave, s, amdq, apdq); break;
         case ORC_RP_VC_ADVECTION_VEC: rpn2_vc_advection_vector(ixy, mbc, mx, meqn, q, q, aux2, wave, s, amdq, apdq); break;
+        case ORC_RP_EULER_5WAVE: rpn2_euler_5wave(ixy, mbc, mx, meqn, mwaves, q, q, wave, s, amdq, apdq, cp); break;
     }
 }
 void call_rpt2(int rp, int ixy, int imp, int mbc, int mx, int meqn, int mwaves, const CSlice& q,
@@ -888,6 +1048,7 @@ void call_rpt2(int rp, int ixy, int imp, int mbc, int mx, int meqn, int mwaves, 
         case ORC_RP_VC_ACOUSTICS: rpt2_vc_acoustics(ixy, imp, mbc, mx, aux1, aux2, aux3, asdq, bm, bp); break;
         case ORC_RP_VC_ADVECTION: rpt2_vc_advection(ixy, imp, mbc, mx, aux2, aux3, asdq, bm, bp); break;
         case ORC_RP_PSYSTEM: rpt2_psystem(ixy, imp, mbc, mx, aux1, aux2, aux3, asdq, bm, bp); break;
+        case ORC_RP_EULER_5WAVE: rpt2_euler_5wave(ixy, mbc, mx, meqn, q, q, asdq, bm, bp, cp); break;
         case ORC_RP_ADVECTION: rpt2_advection(ixy, mbc, mx, asdq, bm, bp, cp); break;
         case ORC_RP_ACOUSTICS: rpt2_acoustics(ixy, mbc, mx, asdq, bm, bp, cp); break;
         case ORC_RP_EULER_ROE: rpt2_euler_roe(ixy, mbc, mx, meqn, mwaves, q, q, asdq, bm, bp, cp); break;

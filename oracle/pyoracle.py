@@ -127,40 +127,62 @@ def bc_fill(qbc, bc_lower, bc_upper):
         raise RuntimeError("oracle_bc_fill returned %d" % rc)
 
 
-def apply_aux_bcs(solver, state, auxbc):
-    """Solver._apply_bcs for the aux array (src/pyclaw/solver.py:351-437,
-    439-519 with name 'aux'): interior from State.aux, then per dimension the
-    lower and the upper side, a user function for BC.custom (called with
-    qbc = None), else extrap / periodic / wall (a plain mirror)."""
+def _rule(kind, arr, ng, lower, reflect):
+    """One built-in rule on one side (solver.py:439-519); arr has the
+    dimension on axis 1; reflect = the component a wall negates, or None."""
+    from pyclaw_b200.solver import BC
+    if kind == BC.extrap:
+        for i in range(ng):
+            if lower:
+                arr[:, i, ...] = arr[:, ng, ...]
+            else:
+                arr[:, -i - 1, ...] = arr[:, -ng - 1, ...]
+    elif kind == BC.periodic:
+        if lower:
+            arr[:, :ng, ...] = arr[:, -2 * ng:-ng, ...]
+        else:
+            arr[:, -ng:, ...] = arr[:, ng:2 * ng, ...]
+    elif kind == BC.wall:
+        for i in range(ng):
+            src = 2 * ng - 1 - i if lower else -2 * ng + i
+            dst = i if lower else -i - 1
+            arr[:, dst, ...] = arr[:, src, ...]
+            if reflect is not None:
+                arr[reflect, dst, ...] = -arr[reflect, src, ...]
+    else:
+        raise NotImplementedError("boundary condition %r" % (kind,))
+
+
+def apply_bcs(solver, state, qbc, auxbc):
+    """Solver._apply_bcs (src/pyclaw/solver.py:351-437) for q and aux:
+    interiors from the state, then per dimension the lower and the upper side,
+    on each side aux before q, a user function for BC.custom (called with the
+    host qbc and auxbc), else the built-in rule.  qbc or auxbc may be None."""
     from pyclaw_b200.solver import BC
     ng = 2
-    auxbc[:, ng:-ng, ng:-ng] = state.aux
+    if qbc is not None:
+        qbc[:, ng:-ng, ng:-ng] = state._q
+    if auxbc is not None:
+        auxbc[:, ng:-ng, ng:-ng] = state.aux
     for idim, dim in enumerate(state.grid.dimensions):
-        arr = np.rollaxis(auxbc, idim + 1, 1)
         for lower in (True, False):
-            kind = (solver.aux_bc_lower if lower else solver.aux_bc_upper)[idim]
-            if kind == BC.custom:
-                fun = solver.user_aux_bc_lower if lower else solver.user_aux_bc_upper
-                fun(state, dim, state.t, None, auxbc, ng)
-            elif kind == BC.extrap:
-                for i in range(ng):
-                    if lower:
-                        arr[:, i, ...] = arr[:, ng, ...]
-                    else:
-                        arr[:, -i - 1, ...] = arr[:, -ng - 1, ...]
-            elif kind == BC.periodic:
-                if lower:
-                    arr[:, :ng, ...] = arr[:, -2 * ng:-ng, ...]
+            items = []
+            if auxbc is not None:
+                items.append((auxbc, solver.aux_bc_lower if lower else solver.aux_bc_upper,
+                              solver.user_aux_bc_lower if lower else solver.user_aux_bc_upper, None))
+            if qbc is not None:
+                items.append((qbc, solver.bc_lower if lower else solver.bc_upper,
+                              solver.user_bc_lower if lower else solver.user_bc_upper, solver.reflect_index[idim]))
+            for arr, kinds, fun, reflect in items:
+                if kinds[idim] == BC.custom:
+                    fun(state, dim, state.t, qbc, auxbc, ng)
                 else:
-                    arr[:, -ng:, ...] = arr[:, ng:2 * ng, ...]
-            elif kind == BC.wall:
-                for i in range(ng):
-                    if lower:
-                        arr[:, i, ...] = arr[:, 2 * ng - 1 - i, ...]
-                    else:
-                        arr[:, -i - 1, ...] = arr[:, -2 * ng + i, ...]
-            else:
-                raise NotImplementedError("aux boundary condition %r" % (kind,))
+                    _rule(kinds[idim], np.rollaxis(arr, idim + 1, 1), ng, lower, reflect)
+
+
+def apply_aux_bcs(solver, state, auxbc):
+    """apply_bcs for the aux array alone (a custom function gets qbc = None)."""
+    apply_bcs(solver, state, None, auxbc)
     return auxbc
 
 
@@ -200,14 +222,15 @@ def make_solver_class():
             state = solution.states[0]
             dx, dy = state.grid.delta
             qbc = self.qbc
-            qbc[:, 2:-2, 2:-2] = state._q
-            bc_fill(qbc, self.bc_lower, self.bc_upper)
-            aux = None
-            if self.auxbc is not None:  # solver.py:351-437 fills auxbc with qbc every step
-                aux = self.auxbc
-                if any(b == 0 for b in list(self.aux_bc_lower) + list(self.aux_bc_upper)):
-                    apply_aux_bcs(self, state, aux)  # user functions (BC.custom)
-                else:
+            aux = self.auxbc
+            custom = any(b == 0 for b in list(self.bc_lower) + list(self.bc_upper) +
+                         (list(self.aux_bc_lower) + list(self.aux_bc_upper) if aux is not None else []))
+            if custom:  # user functions (BC.custom): the reference's order, in numpy
+                apply_bcs(self, state, qbc, aux)
+            else:  # solver.py:351-437 fills qbc and auxbc every step
+                qbc[:, 2:-2, 2:-2] = state._q
+                bc_fill(qbc, self.bc_lower, self.bc_upper)
+                if aux is not None:
                     aux[:, 2:-2, 2:-2] = state.aux
                     bc_fill_aux(aux, self.aux_bc_lower, self.aux_bc_upper)
             qold = qbc.copy('F')

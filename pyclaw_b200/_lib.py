@@ -20,6 +20,7 @@ RP_VC_ACOUSTICS = 6
 RP_VC_ADVECTION = 7
 RP_PSYSTEM = 8
 RP_VC_ADVECTION_VEC = 9
+RP_EULER_5WAVE = 10
 
 OK, EINVAL, ECUDA, ENONFINITE, ETIMEOUT, ENOMEM, EUNSUPPORTED = 0, 1, 2, 3, 4, 5, 6
 
@@ -77,8 +78,11 @@ _SIGNATURES = {
     "claw2_patch_download_q": (ctypes.c_int, [ctypes.c_void_p, _c_double_p]),
     "claw2_patch_upload_aux": (ctypes.c_int, [ctypes.c_void_p, _c_double_p, _c_int_p, _c_int_p]),
     "claw2_patch_upload_auxbc": (ctypes.c_int, [ctypes.c_void_p, _c_double_p]),
+    "claw2_patch_upload_qbc": (ctypes.c_int, [ctypes.c_void_p, _c_double_p]),
     "claw2_patch_gather_q": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _c_int_p, _c_double_p]),
     "claw2_patch_linear_source": (ctypes.c_int, [ctypes.c_void_p, _c_double_p, ctypes.c_int, ctypes.c_double]),
+    "claw2_patch_euler_axisymmetric_source": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int,
+                                                            ctypes.c_double]),
     "claw2_patch_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _c_double_p]),
     "claw2_patch_run_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
                                             ctypes.POINTER(ctypes.c_void_p), _c_double_p, _c_double_p]),

@@ -12,6 +12,7 @@ import numpy as np
 from .limiters import tvd
 from .solver import BC, Solver
 from . import _lib
+from . import hostbc as _hostbc
 
 
 class ClawSolver(Solver):
@@ -159,8 +160,6 @@ class ClawSolver2D(ClawSolver):
         for b in list(self.bc_lower) + list(self.bc_upper):
             if b is None:
                 raise Exception('One of the boundary conditions has not been set.')
-            if b == BC.custom:
-                raise NotImplementedError("custom boundary conditions are not in this build")
         d = _lib.Claw2Desc()
         d.mx, d.my = grid.num_cells
         d.num_eqn, d.num_waves = state.num_eqn, self.num_waves
@@ -177,8 +176,12 @@ class ClawSolver2D(ClawSolver):
         d.fwave = 1 if self.fwave else 0
         for k, v in enumerate(self._mthlim):
             d.mthlim[k] = int(v)
-        d.bc_lower[0], d.bc_lower[1] = self.bc_lower
-        d.bc_upper[0], d.bc_upper[1] = self.bc_upper
+        if _hostbc.has_custom_q(self):
+            # the host supplies every ghost cell each step (claw2_patch_upload_qbc)
+            d.bc_lower[0] = d.bc_lower[1] = d.bc_upper[0] = d.bc_upper[1] = int(BC.extrap)
+        else:
+            d.bc_lower[0], d.bc_lower[1] = self.bc_lower
+            d.bc_upper[0], d.bc_upper[1] = self.bc_upper
         d.dx, d.dy = grid.delta
         vals = self.rp.cparam(state.problem_data)
         for k, v in enumerate(vals):
@@ -188,22 +191,29 @@ class ClawSolver2D(ClawSolver):
         return d
 
     def _device_aux(self, state):
-        """True when the step reads aux data: the Riemann solver's or the
-        capacity function."""
-        return bool(getattr(self.rp, 'num_aux', 0)) or state.index_capa >= 0
+        """True when the device holds aux data: whenever the state has some
+        (the Riemann solver, the capacity function or a device source step
+        reads it)."""
+        return state.num_aux > 0
 
-    def _push_aux(self, state, force):
+    def _bc_shape(self, state, ncomp):
+        return (ncomp,) + tuple(n + 2 * self.num_ghost for n in state.grid.num_cells)
+
+    def _push_aux(self, state, force, auxbc=None):
         """Aux data to the device: State.aux with ghost cells filled on the
-        device, or, with a custom aux BC, auxbc filled on the host every step
-        (solver.py:351-437) and uploaded when it changed."""
-        from . import auxbc as _auxbc
+        device, or, with a custom BC, auxbc filled on the host every step
+        (solver.py:351-437; given as ``auxbc`` when q's custom BCs filled it)
+        and uploaded when it changed."""
         if not self._device_aux(state):
             return
-        if _auxbc.needs_host_fill(self):
-            shape = (state.num_aux,) + tuple(n + 2 * self.num_ghost for n in state.grid.num_cells)
-            if self.auxbc is None or self.auxbc.shape != shape:
-                self.auxbc = np.zeros(shape, order='F')
-            new = _auxbc.fill_auxbc(self, state, self.auxbc.copy(order='F'))
+        if auxbc is not None or _hostbc.needs_host_fill(self):
+            if auxbc is not None:
+                new = auxbc
+            else:
+                shape = self._bc_shape(state, state.num_aux)
+                if self.auxbc is None or self.auxbc.shape != shape:
+                    self.auxbc = np.zeros(shape, order='F')
+                new = _hostbc.fill_auxbc(self, state, self.auxbc.copy(order='F'))
             if force or self._aux_pushed is None or not np.array_equal(new, self._aux_pushed):
                 self._dev.push_auxbc(new)
             self.auxbc = new
@@ -275,7 +285,23 @@ class ClawSolver2D(ClawSolver):
             dev = self._dev
         if dev.host_dirty:
             dev.push(state)
-        self._push_aux(state, force=False)  # a new State.aux array, or custom aux BCs
+        if _hostbc.has_custom_q(self):
+            # custom q BCs: every ghost cell (q and aux) filled on the host
+            shape = self._bc_shape(state, state.num_eqn)
+            if self.qbc is None or self.qbc.shape != shape:
+                self.qbc = np.zeros(shape, order='F')
+            auxbc = None
+            if state.num_aux > 0:
+                ashape = self._bc_shape(state, state.num_aux)
+                auxbc = (self.auxbc if self.auxbc is not None and self.auxbc.shape == ashape
+                         else np.zeros(ashape, order='F')).copy(order='F')
+            _hostbc.fill_bcs(self, state, self.qbc, auxbc)
+            dev.upload_qbc(self.qbc)
+            self._push_aux(state, force=False, auxbc=auxbc if self._device_aux(state) else None)
+            if auxbc is not None:
+                self.auxbc = auxbc
+        else:
+            self._push_aux(state, force=False)  # a new State.aux array, or custom aux BCs
         cfl = dev.step(self.dt)
         self.cfl.update_global_max(cfl)
 

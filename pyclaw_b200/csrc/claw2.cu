@@ -72,6 +72,7 @@ int rp_shape(int rp, int* meqn, int* mwaves) {
         case CLAW2_RP_VC_ADVECTION: *meqn = 1; *mwaves = 1; return 0;
         case CLAW2_RP_PSYSTEM: *meqn = 3; *mwaves = 2; return 0;
         case CLAW2_RP_VC_ADVECTION_VEC: *meqn = 2; *mwaves = 1; return 0;
+        case CLAW2_RP_EULER_5WAVE: *meqn = 5; *mwaves = 5; return 0;
         default: return -1;
     }
 }
@@ -86,7 +87,8 @@ RPParams make_params(int rp, const double* cparam, int n) {
     RPParams p;
     for (int k = 0; k < CLAW2_MAX_PARAMS; ++k) p.c[k] = (cparam && k < n) ? cparam[k] : 0.0;
     p.flags = 0;
-    if (rp == CLAW2_RP_EULER_ROE || rp == CLAW2_RP_SHALLOW_ROE) p.flags = (p.c[1] != 0.0) ? 1 : 0;
+    if (rp == CLAW2_RP_EULER_ROE || rp == CLAW2_RP_SHALLOW_ROE || rp == CLAW2_RP_EULER_5WAVE)
+        p.flags = (p.c[1] != 0.0) ? 1 : 0;
     return p;
 }
 
@@ -274,6 +276,7 @@ int dispatch(int rp, A&&... args) {
         case CLAW2_RP_VC_ADVECTION: F<RPVcAdvection>::run(args...); return 0;
         case CLAW2_RP_PSYSTEM: F<RPPsystem>::run(args...); return 0;
         case CLAW2_RP_VC_ADVECTION_VEC: F<RPVcAdvectionVec>::run(args...); return 0;
+        case CLAW2_RP_EULER_5WAVE: F<RPEuler5>::run(args...); return 0;
         default: return -1;
     }
 }
@@ -715,6 +718,7 @@ struct claw2_patch {
     double* tmp = nullptr;              // intermediate of the split step
     double* aux = nullptr;              // aux planes (solvers with aux data), ghost cells filled at upload
     double* stage = nullptr;            // AoS staging for host copies
+    size_t stage_n = 0;                 // its size in doubles
     unsigned long long* cfl = nullptr;
     int* status = nullptr;
     unsigned long long* h_cfl = nullptr;  // pinned
@@ -741,6 +745,7 @@ struct claw2_patch {
     unsigned long long* h_cfl_hist = nullptr;
     int cfl_hist_cap = 0;
     int nsm = 0;                  // SMs of the patch's device
+    bool ghosts_supplied = false; // claw2_patch_upload_qbc: the next step keeps the uploaded ghost cells
     void* gather_buf = nullptr;   // claw2_patch_gather_q: values, then cell indices
     size_t gather_cap = 0;
     CUtensorMap tmap[2];          // TMA descriptors of q[0], q[1]
@@ -921,8 +926,9 @@ int claw2_patch_create(const claw2_desc* d, claw2_patch** out) {
     DeviceGuard g(p->device);
     cudaDeviceGetAttribute(&p->nsm, cudaDevAttrMultiProcessorCount, p->device);
     const size_t nb = (size_t)me * p->L.plane * 8;
-    // staging: q (interior) or the aux array with its ghost cells
-    const size_t ns = std::max((size_t)me * d->mx * d->my, (size_t)d->num_aux * (d->mx + 4) * (d->my + 4)) * 8;
+    // staging: q or the aux array, with ghost cells
+    const size_t ns = (size_t)std::max(me, d->num_aux) * (d->mx + 4) * (d->my + 4) * 8;
+    p->stage_n = ns / 8;
     bool ok = cudaMalloc(&p->q[0], nb) == cudaSuccess && cudaMalloc(&p->q[1], nb) == cudaSuccess &&
               cudaMalloc(&p->stage, ns) == cudaSuccess &&
               cudaMalloc(&p->cfl, sizeof(unsigned long long)) == cudaSuccess &&
@@ -1024,6 +1030,21 @@ int claw2_patch_upload_aux(claw2_patch* p, const double* aux, const int* aux_bc_
     return CLAW2_OK;
 }
 
+int claw2_patch_upload_qbc(claw2_patch* p, const double* qbc) {
+    if (!p || !qbc) return fail(CLAW2_EINVAL, "null pointer argument");
+    if (p->pending) return fail(CLAW2_EINVAL, "a step is pending: accept or reject it first");
+    DeviceGuard g(p->device);
+    const size_t n = (size_t)p->d.num_eqn * (p->d.mx + 4) * (p->d.my + 4);
+    if (n > p->stage_n) return fail(CLAW2_EINVAL, "staging buffer too small for qbc");
+    CUDA_TRY(cudaMemcpyAsync(p->stage, qbc, n * 8, cudaMemcpyHostToDevice, p->st));
+    k_aos_to_planes<<<grid_blocks((long long)(p->d.mx + 4) * (p->d.my + 4)), 256, 0, p->st>>>(p->stage, p->q[p->cur],
+                                                                                           p->L, p->d.num_eqn, 2);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(p->st));
+    p->ghosts_supplied = true;
+    return CLAW2_OK;
+}
+
 int claw2_patch_upload_auxbc(claw2_patch* p, const double* auxbc) {
     if (!p || !auxbc) return fail(CLAW2_EINVAL, "null pointer argument");
     if (p->d.num_aux < 1) return fail(CLAW2_EINVAL, "this patch has no aux arrays (num_aux = 0)");
@@ -1083,6 +1104,20 @@ int claw2_patch_linear_source(claw2_patch* p, const double* m, int n, double dt)
     return CLAW2_OK;
 }
 
+int claw2_patch_euler_axisymmetric_source(claw2_patch* p, double gamma, int radius_aux, double dt) {
+    if (!p) return fail(CLAW2_EINVAL, "null patch");
+    if (p->d.num_eqn < 4) return fail(CLAW2_EINVAL, "the Euler source needs num_eqn >= 4 (got %d)", p->d.num_eqn);
+    if (radius_aux < 0 || radius_aux >= p->d.num_aux || !p->aux)
+        return fail(CLAW2_EINVAL, "aux component %d (the radius) is not on the device (num_aux = %d)", radius_aux,
+                    p->d.num_aux);
+    if (p->pending) return fail(CLAW2_EINVAL, "a step is pending: accept or reject it first");
+    DeviceGuard g(p->device);
+    k_euler_axisym_source<<<grid_blocks((long long)p->d.mx * p->d.my), 256, 0, p->st>>>(
+        p->q[p->cur], p->aux + (size_t)radius_aux * p->L.plane, p->L, gamma, dt);
+    CUDA_TRY(cudaGetLastError());
+    return CLAW2_OK;
+}
+
 int claw2_patch_download_q(claw2_patch* p, double* q) {
     if (!p || !q) return fail(CLAW2_EINVAL, "null pointer argument");
     DeviceGuard g(p->device);
@@ -1103,7 +1138,12 @@ namespace {
 // its stream; the result goes to the pending buffer.
 int patch_enqueue_step(claw2_patch* p, double dt) {
     double* qc = p->q[p->cur];
-    launch_bc(qc, p->L, p->d.num_eqn, p->d.bc_lower, p->d.bc_upper, p->cfl, p->st);
+    if (p->ghosts_supplied) {  // the host filled every ghost cell (custom BCs)
+        CUDA_TRY(cudaMemsetAsync(p->cfl, 0, sizeof(unsigned long long), p->st));
+        p->ghosts_supplied = false;
+    } else {
+        launch_bc(qc, p->L, p->d.num_eqn, p->d.bc_lower, p->d.bc_upper, p->cfl, p->st);
+    }
     StepArgs a = patch_args(p, dt);
     if (p->timing) CUDA_TRY(cudaEventRecord(p->ev0, p->st));
     if (p->d.riemann == CLAW2_RP_EULER_EXACT && p->mlp && !p->d.dimensional_split) {

@@ -314,6 +314,84 @@ struct RPEulerRoe {
 };
 
 // ---------------------------------------------------------------------------
+// euler_5wave_2D: the Roe solver above with a passive tracer as fifth
+// component (development/rp_approaches/rpn2_euler_5wave.f,
+// rpt2_euler_5wave.f): the tracer jump is a fifth wave moving at the Roe
+// normal velocity, in the transverse split at the Roe transverse velocity;
+// the entropy fix treats it with the contact.  cparam = {gamma, efix}.
+// Cell: the Euler cell, then the tracer.  The Euler parts run the 4-wave code.
+// ---------------------------------------------------------------------------
+struct RPEuler5 {
+    using E = RPEulerRoe;
+    static constexpr int MEQN = 5, MWAVES = 5, NC = E::NC + 1, ID = CLAW2_RP_EULER_5WAVE;
+    static constexpr int TR = E::NC;  // the tracer's slot in the cell
+    struct Iface { E::Iface e; double dtr; };
+
+    __device__ __forceinline__ static const double (&ecell(const double (&c)[NC]))[E::NC] {
+        return *reinterpret_cast<const double(*)[E::NC]>(&c[0]);
+    }
+    __device__ __forceinline__ static void prepare(const double (&q)[MEQN], const RPParams& p, double (&c)[NC]) {
+        const double q4[4] = {q[0], q[1], q[2], q[3]};
+        E::prepare(q4, p, *reinterpret_cast<double(*)[E::NC]>(&c[0]));
+        c[TR] = q[4];
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void speeds(const Iface& f, const RPParams& p, double (&s)[MWAVES]) {
+        double s4[4];
+        E::template speeds<IXY>(f.e, p, s4);
+        s[0] = s4[0]; s[1] = s4[1]; s[2] = s4[2]; s[3] = s4[3];
+        s[4] = f.e.u;
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void waves(const Iface& f, const RPParams& p, double (&w)[MWAVES][MEQN]) {
+        // families in the 5-wave file's order: acoustic, shear, entropy,
+        // acoustic, tracer (the 4-wave code keeps entropy before shear)
+        double w4[4][4];
+        E::template waves<IXY>(f.e, p, w4);
+        constexpr int from[4] = {0, 2, 1, 3};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+#pragma unroll
+            for (int m = 0; m < 4; ++m) w[k][m] = w4[from[k]][m];
+            w[k][4] = 0.0;
+        }
+        w[4][0] = w[4][1] = w[4][2] = w[4][3] = 0.0;
+        w[4][4] = f.dtr;
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void solve(const double (&cL)[NC], const double (&cR)[NC], const RPParams& p,
+                                                 Iface& f, double (&amdq)[MEQN], double (&apdq)[MEQN]) {
+        double am4[4], ap4[4];
+        E::template solve<IXY>(ecell(cL), ecell(cR), p, f.e, am4, ap4);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            amdq[m] = am4[m];
+            apdq[m] = ap4[m];
+        }
+        // tracer: left-going exactly when the contact is (with or without the fix)
+        f.dtr = cR[TR] - cL[TR];
+        const double u = f.e.u;
+        amdq[4] = (u < 0.0) ? u * f.dtr : 0.0;
+        apdq[4] = (u < 0.0) ? 0.0 : u * f.dtr;
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void rpt2(const Iface& f, const RPParams& p, const double (&asdq)[MEQN],
+                                                double (&bm)[MEQN], double (&bp)[MEQN]) {
+        const double a4[4] = {asdq[0], asdq[1], asdq[2], asdq[3]};
+        double bm4[4], bp4[4];
+        E::template rpt2<IXY>(f.e, p, a4, bm4, bp4);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            bm[m] = bm4[m];
+            bp[m] = bp4[m];
+        }
+        const double v = f.e.v;
+        bm[4] = fmin(v, 0.0) * asdq[4];
+        bp[4] = fmax(v, 0.0) * asdq[4];
+    }
+};
+
+// ---------------------------------------------------------------------------
 // shallow_roe_with_efix_2D: cparam = {grav, efix}; q = (h, hu, hv)
 // Cell: q, sqrt(h), u, v, c = sqrt(g h).  Iface: strengths + (u, v, a, 1/a).
 // ---------------------------------------------------------------------------

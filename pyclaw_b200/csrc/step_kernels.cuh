@@ -1114,6 +1114,45 @@ static __global__ void k_linear_source(double* __restrict__ q, Layout L, const L
     }
 }
 
+// Geometric source of the axisymmetric Euler equations (r = the radius plane)
+// in every interior cell: two-stage Runge-Kutta,
+//   q* = q - (dt/2) S(q) / r,  q <- q - dt S(q*) / r,
+//   S = (rho v, rho u v, rho v^2, v (E + p)), p = (gamma-1)(E - rho |u|^2 / 2),
+// components past the fourth unchanged; every operation rounded on its own,
+// in the order of the host function it replaces, so the two agree bit for bit.
+static __global__ void k_euler_axisym_source(double* __restrict__ q, const double* __restrict__ rad, Layout L,
+                                             double gamma, double dt) {
+    const long long ncell = (long long)L.mx * L.my;
+    const double g1 = gamma - 1.0, dt2 = dt / 2.0;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < ncell;
+         k += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(k % L.mx), j = (int)(k / L.mx);
+        const long long o = (long long)(j + 2) * L.pitch + (i + 2);
+        const double r = rad[o];
+        const double q0 = q[o], q1 = q[L.plane + o], q2 = q[2 * L.plane + o], q3 = q[3 * L.plane + o];
+        auto pressure = [&](double rho, double u, double v, double e) {
+            const double ke = __dmul_rn(__dmul_rn(0.5, rho), __dadd_rn(__dmul_rn(u, u), __dmul_rn(v, v)));
+            return __dmul_rn(g1, __dsub_rn(e, ke));
+        };
+        double rho = q0, u = __ddiv_rn(q1, rho), v = __ddiv_rn(q2, rho);
+        double pr = pressure(rho, u, v, q3);
+        const double h = __ddiv_rn(dt2, r);
+        const double s0 = __dsub_rn(q0, __dmul_rn(h, q2));
+        const double s1 = __dsub_rn(q1, __dmul_rn(__dmul_rn(__dmul_rn(h, rho), u), v));
+        const double s2 = __dsub_rn(q2, __dmul_rn(__dmul_rn(__dmul_rn(h, rho), v), v));
+        const double s3 = __dsub_rn(q3, __dmul_rn(__dmul_rn(h, v), __dadd_rn(q3, pr)));
+        rho = s0;
+        u = __ddiv_rn(s1, rho);
+        v = __ddiv_rn(s2, rho);
+        pr = pressure(rho, u, v, s3);
+        const double f = __ddiv_rn(dt, r);
+        q[o] = __dsub_rn(q0, __dmul_rn(f, s2));
+        q[L.plane + o] = __dsub_rn(q1, __dmul_rn(__dmul_rn(__dmul_rn(f, rho), u), v));
+        q[2 * L.plane + o] = __dsub_rn(q2, __dmul_rn(__dmul_rn(__dmul_rn(f, rho), v), v));
+        q[3 * L.plane + o] = __dsub_rn(q3, __dmul_rn(__dmul_rn(f, v), __dadd_rn(s3, pr)));
+    }
+}
+
 // Interior-only copy of qbc-layout planes (for the "ghosts unchanged" rule of
 // claw2_step2: qnew starts as a copy of qold).
 static __global__ void k_copy_planes(const double* __restrict__ src, double* __restrict__ dst, long long n) {

@@ -71,6 +71,14 @@ class DevicePatch(object):
         a = np.asfortranarray(auxbc, dtype=np.float64)
         _lib.check(self._lib.claw2_patch_upload_auxbc(self.h, _lib.dptr(a)))
 
+    def upload_qbc(self, qbc):
+        """Upload q with ghost cells filled on the host; the next step keeps
+        them (claw2_patch_upload_qbc)."""
+        a = np.asfortranarray(qbc, dtype=np.float64)
+        _lib.check(self._lib.claw2_patch_upload_qbc(self.h, _lib.dptr(a)))
+        self.host_dirty = False
+        self.device_newer = False
+
     def gather(self, cells):
         """q at the interior cells [(i, j), ...] of the current device state,
         shape (len(cells), num_eqn) (claw2_patch_gather_q)."""
@@ -83,6 +91,12 @@ class DevicePatch(object):
         """q <- q + dt M q on the device's current state (claw2_patch_linear_source)."""
         M = np.ascontiguousarray(matrix, dtype=np.float64)
         _lib.check(self._lib.claw2_patch_linear_source(self.h, _lib.dptr(M), M.shape[0], ctypes.c_double(dt)))
+        self.device_newer = True
+
+    def euler_axisymmetric_source(self, gamma, radius_aux, dt):
+        """Axisymmetric Euler source step on the device's current state."""
+        _lib.check(self._lib.claw2_patch_euler_axisymmetric_source(self.h, ctypes.c_double(gamma),
+                                                                    int(radius_aux), ctypes.c_double(dt)))
         self.device_newer = True
 
     # ---- stepping -----------------------------------------------------------

@@ -78,8 +78,13 @@ psystem_2D.num_aux = 4
 vc_advection_vector_2D = RiemannSolver('vc_advection_vector_2D', _lib.RP_VC_ADVECTION_VEC, 2, 1, ())
 vc_advection_vector_2D.num_aux = 2
 
+# Euler with a passive tracer (fifth component), Roe solver with five waves
+# (acoustic, shear, entropy, acoustic, tracer) and the entropy fix
+# (clawpack.riemann.euler_5wave_2D).
+euler_5wave_2D = RiemannSolver('euler_5wave_2D', _lib.RP_EULER_5WAVE, 5, 5, ('gamma',), efix=True)
+
 _ALL = [advection_2D, acoustics_2D, euler_4wave_2D, shallow_roe_with_efix_2D, euler_exact_2D, vc_acoustics_2D,
-        vc_advection_2D, psystem_2D, vc_advection_vector_2D]
+        vc_advection_2D, psystem_2D, vc_advection_vector_2D, euler_5wave_2D]
 
 static = types.SimpleNamespace(
     num_eqn={s.name: s.num_eqn for s in _ALL},
@@ -91,6 +96,7 @@ static = types.SimpleNamespace(
 euler_exact_2D_constants = types.SimpleNamespace(density=0, x_momentum=1, y_momentum=2, energy=3, num_eqn=4)
 euler_4wave_2D_constants = types.SimpleNamespace(density=0, x_momentum=1, y_momentum=2, energy=3,
                                                  num_eqn=4)
+euler_5wave_2D_constants = types.SimpleNamespace(density=0, x_momentum=1, y_momentum=2, energy=3, num_eqn=5)
 shallow_roe_with_efix_2D_constants = types.SimpleNamespace(depth=0, x_momentum=1, y_momentum=2,
                                                            num_eqn=3)
 acoustics_2D_constants = types.SimpleNamespace(pressure=0, x_velocity=1, y_velocity=2, num_eqn=3)

@@ -12,6 +12,7 @@ bit for bit):
   advection_annulus         examples/advection_2d_annulus/advection_annulus.py:22-213
   psystem                   examples/psystem_2d/psystem_2d.py:26-235
   advection_reaction        examples/advection_reaction_2d/advection_reaction.py:37-114
+  shock_bubble              examples/euler_2d/shock_bubble_interaction.py:36-220
 The benchmark workloads are the acoustics, Euler-quadrant and shallow-water
 dam-break problems at the benchmark sizes (unsplit step, transverse
 corrections, MC limiter).
@@ -474,6 +475,137 @@ def advection_reaction(solver_class=None, n=100, tfinal=REACTION_PERIOD, device_
     solver.source_split = 1
     state.q[0, :, :] = (xc <= 0.5)
     state.q[1, :, :] = (yc <= 0.5)
+    return _controller(solver, Solution(state, domain), tfinal, num_output_times=num_output_times)
+
+
+BUBBLE_GAMMA = 1.4
+BUBBLE_CENTER, BUBBLE_RADIUS = (0.5, 0.), 0.2
+
+
+def _post_shock_state(pinf=5., gamma=BUBBLE_GAMMA):
+    """Density, velocity and energy behind a shock of pressure ratio pinf
+    moving into gas at rest with unit density and pressure."""
+    gamma1 = gamma - 1.
+    rinf = (gamma1 + pinf * (gamma + 1.)) / ((gamma + 1.) + gamma1 * pinf)
+    vinf = 1. / np.sqrt(gamma) * (pinf - 1.) / np.sqrt(0.5 * ((gamma + 1.) / gamma) * pinf + 0.5 * gamma1 / gamma)
+    einf = 0.5 * rinf * vinf ** 2 + pinf / gamma1
+    return rinf, vinf, einf
+
+
+def _bubble_height(x, ymin, ymax):
+    """Height of the part of the bubble (a disc) above x that lies in [ymin, ymax]."""
+    x0, y0 = BUBBLE_CENTER
+    r0 = BUBBLE_RADIUS
+    if ((x - x0) ** 2) < (r0 ** 2):
+        return max(min(y0 + np.sqrt(r0 ** 2 - (x - x0) ** 2), ymax) - ymin, 0.)
+    return 0
+
+
+def _bubble_qinit(state, rhoin=0.1, pinf=5.):
+    """The shock at x = 0.2 moving right, a low-density bubble ahead of it;
+    cells cut by the bubble's edge get the area-weighted mixture (quadrature
+    of the disc's height over the cell)."""
+    from scipy import integrate
+    gamma = BUBBLE_GAMMA
+    gamma1 = gamma - 1.
+    grid = state.grid
+    rhoout, pout, pin, xshock = 1., 1., 1., 0.2
+    rinf, vinf, einf = _post_shock_state(pinf)
+    X, Y = grid.p_centers
+    x0, y0 = BUBBLE_CENTER
+    r0 = BUBBLE_RADIUS
+    r = np.sqrt((X - x0) ** 2 + (Y - y0) ** 2)
+    state.q[0, :, :] = rinf * (X < xshock) + rhoin * (r <= r0) + rhoout * (r > r0) * (X >= xshock)
+    state.q[1, :, :] = rinf * vinf * (X < xshock)
+    state.q[2, :, :] = 0.
+    state.q[3, :, :] = einf * (X < xshock) + (pin * (r <= r0) + pout * (r > r0) * (X >= xshock)) / gamma1
+    state.q[4, :, :] = 1. * (r <= r0)
+    d2 = np.linalg.norm(state.grid.delta) / 2.
+    dx, dy = state.grid.delta
+    dx2, dy2 = dx / 2., dy / 2.
+    q = state.q
+    for i in range(q.shape[1]):
+        for j in range(q.shape[2]):
+            ydown, yup = Y[i, j] - dy2, Y[i, j] + dy2
+            if abs(r[i, j] - r0) < d2:
+                infrac, _ = integrate.quad(_bubble_height, X[i, j] - dx2, X[i, j] + dx2, args=(ydown, yup),
+                                           epsabs=1.e-8, epsrel=1.e-5)
+                infrac = infrac / (dx * dy)
+                q[0, i, j] = rhoin * infrac + rhoout * (1. - infrac)
+                q[3, i, j] = (pin * infrac + pout * (1. - infrac)) / gamma1
+                q[4, i, j] = 1. * infrac
+
+
+def _incoming_shock(state, dim, t, qbc, auxbc, num_ghost):
+    """Left boundary: the post-shock state flows in."""
+    rinf, vinf, einf = _post_shock_state()
+    for i in range(num_ghost):
+        qbc[0, i, ...] = rinf
+        qbc[1, i, ...] = rinf * vinf
+        qbc[2, i, ...] = 0.
+        qbc[3, i, ...] = einf
+        qbc[4, i, ...] = 0.
+
+
+def _euler_radial_source(solver, state, dt):
+    """Geometric source of the axisymmetric Euler equations (r = aux[0] the
+    radial coordinate): two-stage second-order Runge-Kutta over the step."""
+    gamma = BUBBLE_GAMMA
+    dt2 = dt / 2.
+    q = state.q
+    rad = state.aux[0, :, :]
+    rho = q[0, :, :]
+    u = q[1, :, :] / rho
+    v = q[2, :, :] / rho
+    press = (gamma - 1.) * (q[3, :, :] - 0.5 * rho * (u ** 2 + v ** 2))
+    qstar = np.empty(q.shape)
+    qstar[0, :, :] = q[0, :, :] - dt2 / rad * q[2, :, :]
+    qstar[1, :, :] = q[1, :, :] - dt2 / rad * rho * u * v
+    qstar[2, :, :] = q[2, :, :] - dt2 / rad * rho * v * v
+    qstar[3, :, :] = q[3, :, :] - dt2 / rad * v * (q[3, :, :] + press)
+    rho = qstar[0, :, :]
+    u = qstar[1, :, :] / rho
+    v = qstar[2, :, :] / rho
+    press = (gamma - 1.) * (qstar[3, :, :] - 0.5 * rho * (u ** 2 + v ** 2))
+    q[0, :, :] = q[0, :, :] - dt / rad * qstar[2, :, :]
+    q[1, :, :] = q[1, :, :] - dt / rad * rho * u * v
+    q[2, :, :] = q[2, :, :] - dt / rad * rho * v * v
+    q[3, :, :] = q[3, :, :] - dt / rad * v * (qstar[3, :, :] + press)
+
+
+def shock_bubble(solver_class=None, mx=320, my=80, tfinal=0.6, num_output_times=10, device_source=False):
+    """A planar shock hitting a low-density bubble, in r-z coordinates with
+    cylindrical symmetry (euler_5wave_2D with a tracer marking the bubble):
+    unsplit, MC on the Euler families and superbee on the tracer, cfl 0.45 /
+    0.5; inflow of the post-shock state on the left (custom BC), wall at the
+    axis, extrapolation elsewhere; the geometric source by a Godunov-split
+    step.  device_source: the source as EulerAxisymmetricSource, which stays on
+    the device, instead of the host function."""
+    from .sources import EulerAxisymmetricSource
+    cls = solver_class or ClawSolver2D
+    solver = cls(riemann.euler_5wave_2D)
+    solver.step_source = (EulerAxisymmetricSource(BUBBLE_GAMMA, radius_aux=0) if device_source
+                          else _euler_radial_source)
+    solver.source_split = 1
+    solver.limiters = [4, 4, 4, 4, 2]
+    solver.cfl_max = 0.5
+    solver.cfl_desired = 0.45
+    domain = Domain([Dimension(0.0, 2.0, mx, name='x'), Dimension(0.0, 0.5, my, name='y')])
+    state = State(domain, 5, 1)
+    state.problem_data['gamma'] = BUBBLE_GAMMA
+    _bubble_qinit(state)
+    y = state.grid.y.centers
+    for j, r in enumerate(y):
+        state.aux[0, :, j] = r
+    solver.user_bc_lower = _incoming_shock
+    solver.bc_lower[0] = BC.custom
+    solver.bc_upper[0] = BC.extrap
+    solver.bc_lower[1] = BC.wall
+    solver.bc_upper[1] = BC.extrap
+    solver.aux_bc_lower[0] = BC.extrap
+    solver.aux_bc_upper[0] = BC.extrap
+    solver.aux_bc_lower[1] = BC.extrap
+    solver.aux_bc_upper[1] = BC.extrap
     return _controller(solver, Solution(state, domain), tfinal, num_output_times=num_output_times)
 
 

@@ -16,6 +16,7 @@ Fortran step2/step2ds with clawpack/riemann solvers:
                                                      (test_2d_advection_annulus.py:8-30)
   examples/psystem_2d/verify_gauge*.txt              (test_2d_psystem.py:8-24)
   examples/advection_reaction_2d/advection_reaction.txt (test_advection_reaction.py:1-22)
+  examples/euler_2d/expected_sols.npy['shock_bubble_interaction'] (test_euler2d.py:10-36)
 """
 import os
 import sys
@@ -64,6 +65,7 @@ def main():
         out["psystem_gauge" + g] = np.loadtxt(os.path.join(ex, "psystem_2d", "verify_gauge" + g + ".txt"))
     out["advection_reaction_density"] = np.loadtxt(os.path.join(ex, "advection_reaction_2d",
                                                                 "advection_reaction.txt"))
+    out["euler_shock_bubble"] = eul["shock_bubble_interaction"]
     np.savez_compressed(OUT, **{k: np.asarray(v, dtype=np.float64) for k, v in out.items()})
     print("wrote", OUT, {k: np.asarray(v).shape for k, v in out.items()})
 

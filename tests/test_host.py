@@ -131,7 +131,7 @@ def test_host_auxbc_fill_matches_oracle(oracle):
     # restatement of Solver._apply_bcs, on the annulus (custom in r, periodic in
     # theta) and on every built-in pair with a custom lower side in y
     import numpy as np
-    from pyclaw_b200 import auxbc, workloads
+    from pyclaw_b200 import hostbc as auxbc, workloads
     from pyclaw_b200.solver import BC
     claw = workloads.advection_annulus(m_r=12, m_theta=20)
     solver, state = claw.solver, claw.solution.state

@@ -118,3 +118,18 @@ def test_advection_reaction_golden(oracle, goldens, device_source):
     rel = np.linalg.norm(exp - q0) / np.linalg.norm(exp)
     assert rel < 1e-5
     assert rel < 1e-14  # measured 4.5e-16
+
+
+def test_shock_bubble_golden(oracle, goldens):
+    # examples/euler_2d/shock_bubble_interaction (euler_5wave_2D with a tracer,
+    # custom inflow BC, wall at the axis, geometric source by a Godunov-split
+    # step, limiters [4,4,4,4,2]) at 160x40 to t = 0.2: L1 density difference
+    # times dx dy < 1e-6 in test_euler2d.py:10-36
+    from pyclaw_b200 import workloads
+    claw = workloads.shock_bubble(oracle.make_solver_class(), mx=160, my=40, tfinal=0.2, num_output_times=1)
+    claw.run()
+    d = claw.frames[claw.num_output_times].state.get_q_global()[0].reshape([-1])
+    dx, dy = claw.solution.domain.grid.delta
+    diff = dx * dy * np.sum(np.abs(d - goldens["euler_shock_bubble"]))
+    assert diff < 1e-6
+    assert diff < 1e-13  # measured 1.0e-15
