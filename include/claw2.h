@@ -145,6 +145,22 @@ int claw2_patch_linear_source(claw2_patch* p, const double* m, int n, double dt)
  * of examples/euler_2d/shock_bubble_interaction.py:113-146, bit for bit). */
 int claw2_patch_euler_axisymmetric_source(claw2_patch* p, double gamma, int radius_aux, double dt);
 
+/* PyClaw's ascii frame files (src/pyclaw/fileio/ascii.py:17-123).
+ * claw2_write_ascii writes `header` (the patch header lines) and the array
+ * q (nvar, mx, my), Fortran order, one line of nvar "%18.8e" values per cell,
+ * a blank line after each row; rows are formatted by nthreads threads
+ * (0: all cores).  append: add to the file instead of replacing it.
+ * claw2_patch_write_ascii_async does the same for the patch's current state:
+ * the copy to the host is queued behind the steps already issued, and a host
+ * thread formats and writes the file while later steps run;
+ * claw2_patch_wait_output waits for it and returns its status (one frame in
+ * flight: the next write call waits for the previous one). */
+int claw2_write_ascii(const char* path, int append, const char* header, const double* q, int nvar, int mx,
+                      int my, int nthreads);
+int claw2_patch_write_ascii_async(claw2_patch* p, const char* path, int append, const char* header,
+                                  int nthreads);
+int claw2_patch_wait_output(claw2_patch* p);
+
 /* q of the current state at n interior cells: ij holds n (i, j) pairs
  * (0-based), out receives n * num_eqn values, cell by cell.  The gauge
  * values of Solver.write_gauge_values (solver.py:680-715) without

@@ -79,6 +79,11 @@ _SIGNATURES = {
     "claw2_patch_upload_aux": (ctypes.c_int, [ctypes.c_void_p, _c_double_p, _c_int_p, _c_int_p]),
     "claw2_patch_upload_auxbc": (ctypes.c_int, [ctypes.c_void_p, _c_double_p]),
     "claw2_patch_upload_qbc": (ctypes.c_int, [ctypes.c_void_p, _c_double_p]),
+    "claw2_write_ascii": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, _c_double_p, ctypes.c_int,
+                                         ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "claw2_patch_write_ascii_async": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p,
+                                                     ctypes.c_int]),
+    "claw2_patch_wait_output": (ctypes.c_int, [ctypes.c_void_p]),
     "claw2_patch_gather_q": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _c_int_p, _c_double_p]),
     "claw2_patch_linear_source": (ctypes.c_int, [ctypes.c_void_p, _c_double_p, ctypes.c_int, ctypes.c_double]),
     "claw2_patch_euler_axisymmetric_source": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int,

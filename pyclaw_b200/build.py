@@ -18,7 +18,7 @@ LIB = os.path.join(LIBDIR, "libclaw2.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
               "--expt-relaxed-constexpr", "-I" + os.path.join(ROOT, "include")]
-SOURCES = ["claw2.cu", "claw2_noalloc.cu"]
+SOURCES = ["claw2.cu", "claw2_noalloc.cu", "frame_io.cpp"]
 
 
 def nvcc():

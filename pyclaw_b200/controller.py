@@ -11,8 +11,9 @@ class Controller(object):
         self.solver = None
         self.solution = None
         self.outdir = './_output'
-        self.output_format = None   # frames are kept in memory (keep_copy); no files
+        self.output_format = 'ascii'  # fort.tNNNN / fort.qNNNN files under outdir (None: no files)
         self.output_file_prefix = None
+        self.file_prefix_p = 'claw_p'
         self.output_options = {}
         self.write_aux_init = False
         self.write_aux_always = False
@@ -30,6 +31,11 @@ class Controller(object):
         self.overwrite = True
         self.start_frame = 0
         self.F_file_name = 'F'
+
+    @property
+    def outdir_p(self):
+        import os
+        return os.path.join(self.outdir, '_p')
 
     @property
     def F_path(self):
@@ -58,14 +64,21 @@ class Controller(object):
         if not self.solution.is_valid():
             raise Exception("Initial solution is not valid.")
 
+    def _write_frame(self, frame, write_aux):
+        """controller.py:327-349: the derived quantities p (with compute_p)
+        and the frame itself; a frame whose q is on the GPU is written behind
+        the following steps."""
+        if self.compute_p is not None:
+            self.compute_p(self.solution.state)
+            self.solution.write(frame, self.outdir_p, self.output_format, self.file_prefix_p, write_aux=False,
+                                options=self.output_options, write_p=True)
+        self.solution.write(frame, self.outdir, self.output_format, self.output_file_prefix, write_aux,
+                            self.output_options)
+
     def run(self):
-        """controller.py:275-397 without frame files (gauge files and the F
-        functional file are written)."""
+        """controller.py:275-397."""
         if self.solver is None or self.solution is None:
             raise Exception('To run, a Controller must have a Solver and a Solution.')
-        if self.output_format is not None:
-            raise NotImplementedError("file output is not part of pyclaw_b200; set output_format=None "
-                                      "and keep_copy=True")
         self.start_frame = self.solution.start_frame
         grid = self.solution.state.grid
         if len(grid.gauges) > 0:
@@ -88,6 +101,12 @@ class Controller(object):
             return None
         if self.keep_copy:
             self.frames.append(copy.deepcopy(self.solution))
+        if self.output_format is not None:
+            import os
+            if os.path.exists(self.outdir) and self.overwrite is False:
+                raise Exception("Refusing to overwrite existing output data. \nEither delete/move the directory "
+                                "or set controller.overwrite=True.")
+            self._write_frame(frame, self.write_aux_always or self.write_aux_init)
         self.write_F('w')
         status = None
         for t in output_times[1:]:
@@ -99,11 +118,16 @@ class Controller(object):
             frame += 1
             if self.keep_copy:
                 self.frames.append(copy.deepcopy(self.solution))
+            if self.output_format is not None:
+                self._write_frame(frame, self.write_aux_always)
             self.write_F()
             self.logger.info("Solution %s computed for time t=%f" % (frame, self.solution.t))
             for gfile in grid.gauge_files:
                 gfile.flush()
         for gfile in grid.gauge_files:
             gfile.close()
+        if self.output_format is not None:
+            from . import fileio
+            fileio.wait(self.solution)  # the last frame written from the GPU
         self.solution._start_frame = len(self.frames)
         return status

@@ -15,6 +15,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 
 #include "batch.cuh"
 #include "mlp.cuh"
@@ -24,6 +25,11 @@
 #include <numeric>
 
 using namespace claw2;
+
+// frame_io.cpp: the ascii frame writer
+__attribute__((visibility("hidden"))) int claw2_internal_write_ascii(const char* path, int append,
+                                                                     const char* header, const double* q,
+                                                                     int nvar, int mx, int my, int nthreads);
 
 namespace {
 
@@ -746,6 +752,11 @@ struct claw2_patch {
     int cfl_hist_cap = 0;
     int nsm = 0;                  // SMs of the patch's device
     bool ghosts_supplied = false; // claw2_patch_upload_qbc: the next step keeps the uploaded ghost cells
+    // claw2_patch_write_ascii_async: pinned copy of a frame, its event, the writer thread
+    double* out_host = nullptr;
+    cudaEvent_t out_ev = nullptr;
+    std::thread* writer = nullptr;
+    int writer_rc = 0;
     void* gather_buf = nullptr;   // claw2_patch_gather_q: values, then cell indices
     size_t gather_cap = 0;
     CUtensorMap tmap[2];          // TMA descriptors of q[0], q[1]
@@ -969,6 +980,11 @@ int claw2_patch_create(const claw2_desc* d, claw2_patch** out) {
 
 int claw2_patch_destroy(claw2_patch* p) {
     if (!p) return CLAW2_OK;
+    if (p->writer) {
+        p->writer->join();
+        delete p->writer;
+        p->writer = nullptr;
+    }
     {
         DeviceGuard g(p->device);
         if (p->st) cudaStreamSynchronize(p->st);
@@ -982,6 +998,8 @@ int claw2_patch_destroy(claw2_patch* p) {
         cudaFree(p->tile_order);
         cudaFree(p->stage);
         cudaFree(p->gather_buf);
+        cudaFreeHost(p->out_host);
+        if (p->out_ev) cudaEventDestroy(p->out_ev);
         cudaFree(p->cfl);
         cudaFree(p->status);
         cudaFreeHost(p->h_cfl);
@@ -1115,6 +1133,53 @@ int claw2_patch_euler_axisymmetric_source(claw2_patch* p, double gamma, int radi
     k_euler_axisym_source<<<grid_blocks((long long)p->d.mx * p->d.my), 256, 0, p->st>>>(
         p->q[p->cur], p->aux + (size_t)radius_aux * p->L.plane, p->L, gamma, dt);
     CUDA_TRY(cudaGetLastError());
+    return CLAW2_OK;
+}
+
+int claw2_patch_wait_output(claw2_patch* p) {
+    if (!p) return fail(CLAW2_EINVAL, "null patch");
+    if (!p->writer) return CLAW2_OK;
+    p->writer->join();
+    delete p->writer;
+    p->writer = nullptr;
+    const int rc = p->writer_rc;
+    p->writer_rc = 0;
+    return rc;
+}
+
+int claw2_patch_write_ascii_async(claw2_patch* p, const char* path, int append, const char* header,
+                                  int nthreads) {
+    if (!p || !path || !header) return fail(CLAW2_EINVAL, "null pointer argument");
+    int rc = claw2_patch_wait_output(p);  // one frame in flight at a time
+    if (rc) return rc;
+    DeviceGuard g(p->device);
+    const int me = p->d.num_eqn, mx = p->d.mx, my = p->d.my;
+    const size_t n = (size_t)me * mx * my;
+    if (!p->out_host) {
+        if (cudaMallocHost(&p->out_host, n * 8) != cudaSuccess ||
+            cudaEventCreateWithFlags(&p->out_ev, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            cudaFreeHost(p->out_host);
+            p->out_host = nullptr;
+            return fail(CLAW2_ENOMEM, "pinned frame buffer of %zu bytes could not be allocated", n * 8);
+        }
+    }
+    // the current state, in stream order: later steps cannot overwrite it first
+    k_planes_to_aos<<<grid_blocks((long long)mx * my), 256, 0, p->st>>>(p->q[p->cur], p->stage, p->L, me, 0);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(p->out_host, p->stage, n * 8, cudaMemcpyDeviceToHost, p->st));
+    CUDA_TRY(cudaEventRecord(p->out_ev, p->st));
+    std::string spath(path), shead(header);
+    const int dev = p->device;
+    p->writer = new std::thread([p, spath, shead, append, me, mx, my, nthreads, dev]() {
+        cudaSetDevice(dev);
+        if (cudaEventSynchronize(p->out_ev) != cudaSuccess) {
+            p->writer_rc = CLAW2_ECUDA;
+            return;
+        }
+        p->writer_rc = claw2_internal_write_ascii(spath.c_str(), append, shead.c_str(), p->out_host, me, mx, my,
+                                                  nthreads);
+    });
     return CLAW2_OK;
 }
 

@@ -79,6 +79,14 @@ class DevicePatch(object):
         self.host_dirty = False
         self.device_newer = False
 
+    def write_ascii_async(self, path, append, header):
+        """Queue the current state's ascii frame file (claw2_patch_write_ascii_async)."""
+        _lib.check(self._lib.claw2_patch_write_ascii_async(self.h, path.encode(), 1 if append else 0,
+                                                           header.encode(), 0))
+
+    def wait_output(self):
+        _lib.check(self._lib.claw2_patch_wait_output(self.h))
+
     def gather(self, cells):
         """q at the interior cells [(i, j), ...] of the current device state,
         shape (len(cells), num_eqn) (claw2_patch_gather_q)."""

@@ -60,6 +60,23 @@ class Dimension(object):
             self.name, self.num_cells, self.delta, self.lower, self.upper)
 
 
+def identity_map_2d(x, y):
+    """The default mapping (computational = physical coordinates); a
+    module-level function so frames can pickle it (geometry.py:249)."""
+    return [x, y]
+
+
+def identity_map_1d(x):
+    return [x]
+
+
+def identity_map_3d(x, y, z):
+    return [x, y, z]
+
+
+_IDENTITY = {1: identity_map_1d, 2: identity_map_2d, 3: identity_map_3d}
+
+
 class Grid(object):
     """Cartesian product of Dimensions (geometry.py:16-470)."""
 
@@ -71,7 +88,7 @@ class Grid(object):
         self.gauge_file_names = []
         self.gauge_files = []
         self.gauge_dir_name = '_gauges'
-        self.mapc2p = lambda *xs: list(xs)
+        self.mapc2p = _IDENTITY.get(len(self._dims), identity_map_2d)
 
     dimensions = property(lambda self: list(self._dims))
     num_dim = property(lambda self: len(self._dims))

@@ -17,6 +17,9 @@ Fortran step2/step2ds with clawpack/riemann solvers:
   examples/psystem_2d/verify_gauge*.txt              (test_2d_psystem.py:8-24)
   examples/advection_reaction_2d/advection_reaction.txt (test_advection_reaction.py:1-22)
   examples/euler_2d/expected_sols.npy['shock_bubble_interaction'] (test_euler2d.py:10-36)
+and copies the frame files examples/acoustics_2d_variable/io_test_verification/
+fort.t0020, fort.q0020, fort.a0000 (the reference's ascii writer's output) to
+tests/golden/frames/ for the file-format tests.
 """
 import os
 import sys
@@ -66,6 +69,11 @@ def main():
     out["advection_reaction_density"] = np.loadtxt(os.path.join(ex, "advection_reaction_2d",
                                                                 "advection_reaction.txt"))
     out["euler_shock_bubble"] = eul["shock_bubble_interaction"]
+    import shutil
+    fdir = os.path.join(os.path.dirname(OUT), "frames")
+    os.makedirs(fdir, exist_ok=True)
+    for name in ("fort.t0020", "fort.q0020", "fort.a0000"):
+        shutil.copyfile(os.path.join(vio, name), os.path.join(fdir, name))
     np.savez_compressed(OUT, **{k: np.asarray(v, dtype=np.float64) for k, v in out.items()})
     print("wrote", OUT, {k: np.asarray(v).shape for k, v in out.items()})
 
