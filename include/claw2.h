@@ -42,7 +42,8 @@ enum {
     CLAW2_RP_PSYSTEM = 8,      /* psystem_2D (f-waves): no cparam; aux = {rho, K, relation, strain} */
     CLAW2_RP_VC_ADVECTION_VEC = 9, /* examples/advection_reaction_2d's own solver, num_eqn 2: aux =
                                   {u left edge, v bottom edge}; no transverse solve */
-    CLAW2_RP_EULER_5WAVE = 10  /* euler_5wave_2D (Roe + tracer):  {gamma, efix}          */
+    CLAW2_RP_EULER_5WAVE = 10, /* euler_5wave_2D (Roe + tracer):  {gamma, efix}          */
+    CLAW2_RP_SHALLOW_HLLE = 12 /* shallow_hlle_2D: {grav}; no transverse solve           */
 };
 
 /* Boundary-condition codes: pyclaw.BC (src/pyclaw/solver.py:13-19), plus

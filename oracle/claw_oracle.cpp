@@ -641,6 +641,41 @@ void rpt2_euler_5wave(int ixy, int mbc, int mx, int meqn, const CSlice& ql, cons
     }
 }
 
+// HLLE solver (Harten, Lax & van Leer 1983 with Einfeldt's 1988 speed
+// estimates): two waves through the HLL middle state
+//   q_m = (f(q_r) - f(q_l) - s2 q_r + s1 q_l) / (s1 - s2),
+// s1 = min(u_l - c_l, u_hat - c_hat), s2 = max(u_r + c_r, u_hat + c_hat) with
+// the Roe velocity u_hat and c_hat = sqrt(g (h_l + h_r) / 2); fluctuations =
+// sum of s^-/s^+ times the waves.
+// shallow_hlle_2D: cparam = grav.  No transverse solve (split step).
+void rpn2_shallow_hlle(int ixy, int mbc, int mx, int meqn, const CSlice& ql, const CSlice& qr, const Waves& wave,
+                       const Speeds& s, const Slice& amdq, const Slice& apdq, const double* cp) {
+    const double g = cp[0];
+    const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
+    for (int i = 2 - mbc; i <= mx + mbc; ++i) {
+        const double h_l = qr(0, i - 1), hu_l = qr(mu, i - 1), hv_l = qr(mv, i - 1);
+        const double h_r = ql(0, i), hu_r = ql(mu, i), hv_r = ql(mv, i);
+        const double u_l = hu_l / h_l, v_l = hv_l / h_l, u_r = hu_r / h_r, v_r = hv_r / h_r;
+        const double c_l = std::sqrt(g * h_l), c_r = std::sqrt(g * h_r);
+        const double rsl = std::sqrt(h_l), rsr = std::sqrt(h_r);
+        const double u_hat = (rsl * u_l + rsr * u_r) / (rsl + rsr);
+        const double c_hat = std::sqrt(0.5 * g * (h_l + h_r));
+        const double s1 = std::min(u_l - c_l, u_hat - c_hat);
+        const double s2 = std::max(u_r + c_r, u_hat + c_hat);
+        const double den = s1 - s2;
+        const double h_m = (hu_r - hu_l - s2 * h_r + s1 * h_l) / den;
+        const double hu_m = (hu_r * u_r + 0.5 * g * h_r * h_r - hu_l * u_l - 0.5 * g * h_l * h_l - s2 * hu_r +
+                             s1 * hu_l) / den;
+        const double hv_m = (hu_r * v_r - hu_l * v_l - s2 * hv_r + s1 * hv_l) / den;
+        wave(0, 0, i) = h_m - h_l; wave(mu, 0, i) = hu_m - hu_l; wave(mv, 0, i) = hv_m - hv_l; s(0, i) = s1;
+        wave(0, 1, i) = h_r - h_m; wave(mu, 1, i) = hu_r - hu_m; wave(mv, 1, i) = hv_r - hv_m; s(1, i) = s2;
+        for (int m = 0; m < meqn; ++m) {
+            amdq(m, i) = std::min(s1, 0.0) * wave(m, 0, i) + std::min(s2, 0.0) * wave(m, 1, i);
+            apdq(m, i) = std::max(s1, 0.0) * wave(m, 0, i) + std::max(s2, 0.0) * wave(m, 1, i);
+        }
+    }
+}
+
 // Transverse Roe split for Euler: decompose asdq on the eigenvectors of the
 // transverse Jacobian at the same Roe-averaged state and keep the down- and
 // up-going parts (LeVeque 2002, sec. 21.6; reference structure
@@ -1016,7 +1051,7 @@ bool rp_known(int rp) {
     return rp == ORC_RP_ADVECTION || rp == ORC_RP_ACOUSTICS || rp == ORC_RP_EULER_ROE ||
            rp == ORC_RP_SHALLOW_ROE || rp == ORC_RP_EULER_EXACT || rp == ORC_RP_VC_ACOUSTICS ||
            rp == ORC_RP_VC_ADVECTION || rp == ORC_RP_PSYSTEM || rp == ORC_RP_VC_ADVECTION_VEC ||
-           rp == ORC_RP_EULER_5WAVE;
+           rp == ORC_RP_EULER_5WAVE || rp == ORC_RP_SHALLOW_HLLE;
 }
 
 // aux components per cell the solver reads (the leading ones of the aux array)
@@ -1039,6 +1074,7 @@ void call_rpn2(int rp, int ixy, int mbc, int mx, int meqn, int mwaves, const CSl
         case ORC_RP_PSYSTEM: rpn2_psystem(ixy, mbc, mx, q, q, aux2, aux2, wave, s, amdq, apdq); break;
         case ORC_RP_VC_ADVECTION_VEC: rpn2_vc_advection_vector(ixy, mbc, mx, meqn, q, q, aux2, wave, s, amdq, apdq); break;
         case ORC_RP_EULER_5WAVE: rpn2_euler_5wave(ixy, mbc, mx, meqn, mwaves, q, q, wave, s, amdq, apdq, cp); break;
+        case ORC_RP_SHALLOW_HLLE: rpn2_shallow_hlle(ixy, mbc, mx, meqn, q, q, wave, s, amdq, apdq, cp); break;
     }
 }
 void call_rpt2(int rp, int ixy, int imp, int mbc, int mx, int meqn, int mwaves, const CSlice& q,
@@ -1202,7 +1238,8 @@ int oracle_step2(int maxm, int meqn, int mwaves, int maux, int mbc, int mx, int 
     const int index_capa = method[5];
     if (index_capa > 0 && (aux_p == nullptr || maux < index_capa)) return 4;
     if (rp_maux(rp) > 0 && (aux_p == nullptr || maux < rp_maux(rp))) return 4;
-    if (rp == ORC_RP_VC_ADVECTION_VEC && method[2] > 0) return 5;  // no transverse solve
+    if ((rp == ORC_RP_VC_ADVECTION_VEC || rp == ORC_RP_SHALLOW_HLLE) && method[2] > 0)
+        return 5;  // no transverse solve
     Grid2 qold{const_cast<double*>(qold_p), meqn, mbc, mx};
     Grid2 qnew{qnew_p, meqn, mbc, mx};
     Grid2 aux{const_cast<double*>(aux_p), maux > 0 ? maux : 1, mbc, mx};

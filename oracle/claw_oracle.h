@@ -42,7 +42,8 @@ enum {
     ORC_RP_VC_ADVECTION = 7, /* vc_advection_2D       aux: u, v edge velocities */
     ORC_RP_PSYSTEM = 8,      /* psystem_2D (f-waves)  aux: rho, K, relation, eps */
     ORC_RP_VC_ADVECTION_VEC = 9, /* advection_reaction's vector vc advection, split only */
-    ORC_RP_EULER_5WAVE = 10      /* euler_5wave_2D (Roe + tracer) cparam: gamma, efix */
+    ORC_RP_EULER_5WAVE = 10,     /* euler_5wave_2D (Roe + tracer) cparam: gamma, efix */
+    ORC_RP_SHALLOW_HLLE = 12     /* shallow_hlle_2D, no rpt2       cparam: grav        */
 };
 
 /* One unsplit step (step2.f90).  qold, qnew: (meqn, mx+2mbc, my+2mbc) F-order;

@@ -21,6 +21,7 @@ RP_VC_ADVECTION = 7
 RP_PSYSTEM = 8
 RP_VC_ADVECTION_VEC = 9
 RP_EULER_5WAVE = 10
+RP_SHALLOW_HLLE = 12
 
 OK, EINVAL, ECUDA, ENONFINITE, ETIMEOUT, ENOMEM, EUNSUPPORTED = 0, 1, 2, 3, 4, 5, 6
 

@@ -79,6 +79,7 @@ int rp_shape(int rp, int* meqn, int* mwaves) {
         case CLAW2_RP_PSYSTEM: *meqn = 3; *mwaves = 2; return 0;
         case CLAW2_RP_VC_ADVECTION_VEC: *meqn = 2; *mwaves = 1; return 0;
         case CLAW2_RP_EULER_5WAVE: *meqn = 5; *mwaves = 5; return 0;
+        case CLAW2_RP_SHALLOW_HLLE: *meqn = 3; *mwaves = 2; return 0;
         default: return -1;
     }
 }
@@ -283,6 +284,7 @@ int dispatch(int rp, A&&... args) {
         case CLAW2_RP_PSYSTEM: F<RPPsystem>::run(args...); return 0;
         case CLAW2_RP_VC_ADVECTION_VEC: F<RPVcAdvectionVec>::run(args...); return 0;
         case CLAW2_RP_EULER_5WAVE: F<RPEuler5>::run(args...); return 0;
+        case CLAW2_RP_SHALLOW_HLLE: F<RPShallowHLLE>::run(args...); return 0;
         default: return -1;
     }
 }
@@ -316,7 +318,7 @@ void launch_bc(double* q, const Layout& L, int meqn, const int* bcl, const int* 
 int check_method(int rp, int order, int trans, const int* mthlim, int mwaves, int fwave) {
     if (order != 1 && order != 2) return fail(CLAW2_EINVAL, "order must be 1 or 2 (got %d)", order);
     if (trans < -1 || trans > 2) return fail(CLAW2_EINVAL, "transverse must be -1..2 (got %d)", trans);
-    if (rp == CLAW2_RP_VC_ADVECTION_VEC && trans > 0)
+    if ((rp == CLAW2_RP_VC_ADVECTION_VEC || rp == CLAW2_RP_SHALLOW_HLLE) && trans > 0)
         return fail(CLAW2_EINVAL, "solver %d has no transverse solve: use the split step or transverse 0", rp);
     if (fwave != 0 && fwave != 1) return fail(CLAW2_EINVAL, "use_fwave must be 0 or 1 (got %d)", fwave);
     for (int k = 0; k < mwaves; ++k)

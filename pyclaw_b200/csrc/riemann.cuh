@@ -314,6 +314,78 @@ struct RPEulerRoe {
 };
 
 // ---------------------------------------------------------------------------
+// shallow_hlle_2D: cparam = {grav}; q = (h, hu, hv).  Two waves through the
+// HLL middle state q_m = (f(q_R) - f(q_L) - s2 q_R + s1 q_L) / (s1 - s2) with
+// Einfeldt's speeds s1 = min(u_L - c_L, u_hat - c_hat), s2 = max(u_R + c_R,
+// u_hat + c_hat), u_hat the Roe velocity, c_hat = sqrt(g (h_L + h_R) / 2)
+// (Harten, Lax & van Leer 1983; Einfeldt 1988).  No transverse solve (split
+// step or transverse_waves = 0; the host rejects anything else).
+// Cell: q, sqrt(h), u, v, c = sqrt(g h).
+// ---------------------------------------------------------------------------
+struct RPShallowHLLE {
+    static constexpr int MEQN = 3, MWAVES = 2, NC = 7, ID = CLAW2_RP_SHALLOW_HLLE;
+    enum { RS = 3, UX = 4, UY = 5, CS = 6 };
+    struct Iface { double w[2][3]; double s1, s2; };  // waves as (h, normal, transverse)
+
+    __device__ __forceinline__ static void prepare(const double (&q)[MEQN], const RPParams& p, double (&c)[NC]) {
+        c[0] = q[0]; c[1] = q[1]; c[2] = q[2];
+        c[RS] = sqrt(q[0]);
+        c[UX] = q[1] / q[0];
+        c[UY] = q[2] / q[0];
+        c[CS] = sqrt(p.c[0] * q[0]);
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void speeds(const Iface& f, const RPParams&, double (&s)[MWAVES]) {
+        s[0] = f.s1;
+        s[1] = f.s2;
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void waves(const Iface& f, const RPParams&, double (&w)[MWAVES][MEQN]) {
+        constexpr int MU = Dir<IXY>::MU, MV = Dir<IXY>::MV;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            w[k][0] = f.w[k][0];
+            w[k][MU] = f.w[k][1];
+            w[k][MV] = f.w[k][2];
+        }
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void solve(const double (&cL)[NC], const double (&cR)[NC], const RPParams& p,
+                                                 Iface& f, double (&amdq)[MEQN], double (&apdq)[MEQN]) {
+        constexpr int MU = Dir<IXY>::MU, MV = Dir<IXY>::MV;
+        constexpr int UN = (IXY == 1) ? UX : UY, UT = (IXY == 1) ? UY : UX;
+        const double g = p.c[0];
+        const double hl = cL[0], hr = cR[0], hul = cL[MU], hur = cR[MU], hvl = cL[MV], hvr = cR[MV];
+        const double ul = cL[UN], ur = cR[UN], vl = cL[UT], vr = cR[UT];
+        const double u_hat = (cL[RS] * ul + cR[RS] * ur) / (cL[RS] + cR[RS]);
+        const double c_hat = sqrt(0.5 * g * (hl + hr));
+        const double s1 = fmin(ul - cL[CS], u_hat - c_hat);
+        const double s2 = fmax(ur + cR[CS], u_hat + c_hat);
+        const double den = s1 - s2;
+        const double hm = (hur - hul - s2 * hr + s1 * hl) / den;
+        const double hum = (hur * ur + 0.5 * g * hr * hr - hul * ul - 0.5 * g * hl * hl - s2 * hur + s1 * hul) / den;
+        const double hvm = (hur * vr - hul * vl - s2 * hvr + s1 * hvl) / den;
+        f.w[0][0] = hm - hl; f.w[0][1] = hum - hul; f.w[0][2] = hvm - hvl;
+        f.w[1][0] = hr - hm; f.w[1][1] = hur - hum; f.w[1][2] = hvr - hvm;
+        f.s1 = s1;
+        f.s2 = s2;
+        double w[MWAVES][MEQN];
+        waves<IXY>(f, p, w);
+#pragma unroll
+        for (int m = 0; m < MEQN; ++m) {
+            amdq[m] = fmin(s1, 0.0) * w[0][m] + fmin(s2, 0.0) * w[1][m];
+            apdq[m] = fmax(s1, 0.0) * w[0][m] + fmax(s2, 0.0) * w[1][m];
+        }
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void rpt2(const Iface&, const RPParams&, const double (&)[MEQN],
+                                                double (&bm)[MEQN], double (&bp)[MEQN]) {
+#pragma unroll
+        for (int m = 0; m < MEQN; ++m) bm[m] = bp[m] = 0.0;  // unreachable: the host rejects transverse solves
+    }
+};
+
+// ---------------------------------------------------------------------------
 // euler_5wave_2D: the Roe solver above with a passive tracer as fifth
 // component (development/rp_approaches/rpn2_euler_5wave.f,
 // rpt2_euler_5wave.f): the tracer jump is a fifth wave moving at the Roe
@@ -323,17 +395,24 @@ struct RPEulerRoe {
 // ---------------------------------------------------------------------------
 struct RPEuler5 {
     using E = RPEulerRoe;
+    // cell: q (the kernels read q from the first MEQN slots), then the Euler
+    // cell's derived fields; ecell() rebuilds the Euler cell's layout
     static constexpr int MEQN = 5, MWAVES = 5, NC = E::NC + 1, ID = CLAW2_RP_EULER_5WAVE;
-    static constexpr int TR = E::NC;  // the tracer's slot in the cell
     struct Iface { E::Iface e; double dtr; };
 
-    __device__ __forceinline__ static const double (&ecell(const double (&c)[NC]))[E::NC] {
-        return *reinterpret_cast<const double(*)[E::NC]>(&c[0]);
+    __device__ __forceinline__ static void ecell(const double (&c)[NC], double (&e)[E::NC]) {
+        e[0] = c[0]; e[1] = c[1]; e[2] = c[2]; e[3] = c[3];
+#pragma unroll
+        for (int k = 4; k < E::NC; ++k) e[k] = c[k + 1];
     }
     __device__ __forceinline__ static void prepare(const double (&q)[MEQN], const RPParams& p, double (&c)[NC]) {
         const double q4[4] = {q[0], q[1], q[2], q[3]};
-        E::prepare(q4, p, *reinterpret_cast<double(*)[E::NC]>(&c[0]));
-        c[TR] = q[4];
+        double e[E::NC];
+        E::prepare(q4, p, e);
+        c[0] = e[0]; c[1] = e[1]; c[2] = e[2]; c[3] = e[3];
+        c[4] = q[4];
+#pragma unroll
+        for (int k = 4; k < E::NC; ++k) c[k + 1] = e[k];
     }
     template <int IXY>
     __device__ __forceinline__ static void speeds(const Iface& f, const RPParams& p, double (&s)[MWAVES]) {
@@ -361,15 +440,17 @@ struct RPEuler5 {
     template <int IXY>
     __device__ __forceinline__ static void solve(const double (&cL)[NC], const double (&cR)[NC], const RPParams& p,
                                                  Iface& f, double (&amdq)[MEQN], double (&apdq)[MEQN]) {
-        double am4[4], ap4[4];
-        E::template solve<IXY>(ecell(cL), ecell(cR), p, f.e, am4, ap4);
+        double am4[4], ap4[4], eL[E::NC], eR[E::NC];
+        ecell(cL, eL);
+        ecell(cR, eR);
+        E::template solve<IXY>(eL, eR, p, f.e, am4, ap4);
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
             amdq[m] = am4[m];
             apdq[m] = ap4[m];
         }
         // tracer: left-going exactly when the contact is (with or without the fix)
-        f.dtr = cR[TR] - cL[TR];
+        f.dtr = cR[4] - cL[4];
         const double u = f.e.u;
         amdq[4] = (u < 0.0) ? u * f.dtr : 0.0;
         apdq[4] = (u < 0.0) ? 0.0 : u * f.dtr;

@@ -83,8 +83,13 @@ vc_advection_vector_2D.num_aux = 2
 # (clawpack.riemann.euler_5wave_2D).
 euler_5wave_2D = RiemannSolver('euler_5wave_2D', _lib.RP_EULER_5WAVE, 5, 5, ('gamma',), efix=True)
 
+# Shallow water HLLE solver (two waves through the HLL middle state, Einfeldt
+# speeds); no transverse solve: split step or transverse_waves = 0
+# (clawpack.riemann.shallow_hlle_2D).
+shallow_hlle_2D = RiemannSolver('shallow_hlle_2D', _lib.RP_SHALLOW_HLLE, 3, 2, ('grav',))
+
 _ALL = [advection_2D, acoustics_2D, euler_4wave_2D, shallow_roe_with_efix_2D, euler_exact_2D, vc_acoustics_2D,
-        vc_advection_2D, psystem_2D, vc_advection_vector_2D, euler_5wave_2D]
+        vc_advection_2D, psystem_2D, vc_advection_vector_2D, euler_5wave_2D, shallow_hlle_2D]
 
 static = types.SimpleNamespace(
     num_eqn={s.name: s.num_eqn for s in _ALL},

@@ -136,9 +136,10 @@ def quadrants(solver_class=None, mx=100, my=100, efix=None):
     return _controller(solver, solution, 0.8)
 
 
-def radial_dam_break(solver_class=None, mx=150, my=150, h_in=2., h_out=1., dam_radius=0.5):
+def radial_dam_break(solver_class=None, mx=150, my=150, h_in=2., h_out=1., dam_radius=0.5, riemann_solver='roe'):
     cls = solver_class or ClawSolver2D
-    solver = cls(riemann.shallow_roe_with_efix_2D)
+    rs = {'roe': riemann.shallow_roe_with_efix_2D, 'hlle': riemann.shallow_hlle_2D}[riemann_solver.lower()]
+    solver = cls(rs)
     solver.limiters = tvd.MC
     solver.dimensional_split = 1
     solver.bc_lower[0] = BC.extrap

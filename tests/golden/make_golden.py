@@ -7,7 +7,7 @@ Fortran step2/step2ds with clawpack/riemann solvers:
   examples/advection_2d/expected_sols.npy            (test_2d_advection.py:9-35)
   examples/acoustics_2d_homogeneous/verify_classic.txt (test_2d_acoustics.py:6-15)
   examples/euler_2d/expected_sols.npy['quadrants_roe'] (test_euler2d.py:6-29)
-  examples/shallow_2d/expected_sols.npy['radialdambreak_classic_roe']
+  examples/shallow_2d/expected_sols.npy['radialdambreak_classic_roe'], [..._hlle]
                                                      (test_shallow2d.py:9-28)
   examples/acoustics_2d_variable/io_test_verification/fort.q0020, fort.a0000
                                                      (test_acoustics_2d_variable_io.py:7-58)
@@ -55,6 +55,7 @@ def main():
         "advection_classic_unsplit_trans_cor": adv["classic_unsplit_trans_cor"],
         "acoustics_verify_classic": ac,
         "euler_quadrants_roe": eul["quadrants_roe"],
+        "shallow_radialdambreak_classic_hlle": sw["radialdambreak_classic_hlle"],
         "shallow_radialdambreak_classic_roe": sw["radialdambreak_classic_roe"],
     }
     vio = os.path.join(ex, "acoustics_2d_variable", "io_test_verification")

@@ -133,3 +133,12 @@ def test_shock_bubble_golden(oracle, goldens):
     diff = dx * dy * np.sum(np.abs(d - goldens["euler_shock_bubble"]))
     assert diff < 1e-6
     assert diff < 1e-13  # measured 1.0e-15
+
+
+def test_shallow_hlle_goldens(oracle, goldens):
+    # examples/shallow_2d/test_shallow2d.py:31-37 with the HLLE solver (tolerance 1e-5)
+    claw = workloads.radial_dam_break(oracle.make_solver_class(), riemann_solver='hlle')
+    claw.run()
+    err = _l1(claw, goldens["shallow_radialdambreak_classic_hlle"], comp=0)
+    assert err < 1e-5
+    assert err < 1e-12  # measured 1.4e-14
