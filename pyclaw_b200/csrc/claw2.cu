@@ -173,7 +173,8 @@ void smem_attr(K kernel, int bytes, unsigned long long& done) {
 // (0 = heuristic).  Chosen per call by the tuning table (claw2_tune_set /
 // claw2_autotune) or the heuristic default.
 struct UnsplitShape {
-    int variant;  // bit 0: 3 blocks/SM (register cap) instead of 2; bit 1: TMA row staging
+    int variant;  // bit 0: 3 blocks/SM (register cap) instead of 2; bit 1: TMA row staging;
+                  // 4: the two-barrier tile (deferred x finish)
     int rows;
 };
 
@@ -214,6 +215,15 @@ void unsplit_tiling(int riemann, int mx, int my, int& nstrips, int& H, int& nblo
     nblocks = (my + H - 1) / H;
 }
 
+// The two-barrier tile (deferred x finish), any method, with or without capacity.
+template <class RP, int SPEC, bool CAPA>
+void launch_unsplit2_s(const StepArgs& b, dim3 grid, cudaStream_t st) {
+    constexpr int smem = (int)sizeof(UnsplitSmem2<RP, NT_UNSPLIT, CAPA>);
+    static unsigned long long attr = 0;
+    smem_attr(k_step_unsplit2<RP, NT_UNSPLIT, 2, SPEC, CAPA>, smem, attr);
+    k_step_unsplit2<RP, NT_UNSPLIT, 2, SPEC, CAPA><<<grid, NT_UNSPLIT, smem, st>>>(b);
+}
+
 // The capacity form (any method, rows loaded directly).
 template <class RP>
 void launch_unsplit_capa(const StepArgs& b, dim3 grid, cudaStream_t st) {
@@ -234,12 +244,19 @@ void launch_unsplit_v(const StepArgs& a, cudaStream_t st, const CUtensorMap* tm)
     }
     const int nbk = (a.L.my + b.H - 1) / b.H;
     dim3 grid(b.nstrips * nbk);
+    if (g_tune[RP::ID & (TUNE_SLOTS - 1)].variant & 4) {  // the two-barrier tile
+        if (a.capa) launch_unsplit2_s<RP, SPEC_ANY, true>(b, grid, st);
+        else if (is_mc2(a.meth, RP::MWAVES)) launch_unsplit2_s<RP, SPEC_MC2, false>(b, grid, st);
+        else launch_unsplit2_s<RP, SPEC_ANY, false>(b, grid, st);
+        return;
+    }
     if (a.capa) launch_unsplit_capa<RP>(b, grid, st);
     else if (is_mc2(a.meth, RP::MWAVES)) launch_unsplit_s<RP, MB, SPEC_MC2>(b, grid, st, tm);
     else launch_unsplit_s<RP, MB, SPEC_ANY>(b, grid, st, tm);
 }
 
-// Variants: bit 0 = 3 blocks per SM (register cap) instead of 2, bit 1 = rows
+// Variants: 4 = the two-barrier tile (k_step_unsplit2); otherwise bit 0 = 3
+// blocks per SM (register cap) instead of 2, bit 1 = rows
 // staged by TMA (only where the caller has a tensor map of qold).
 template <class RP>
 void launch_unsplit(const StepArgs& a, cudaStream_t st, const CUtensorMap* tm) {
@@ -1476,7 +1493,7 @@ int claw2_selftest_rcp(int device, int n, unsigned long long seed, double* max_u
 int claw2_tune_set(int riemann, int variant, int rows) {
     int me = 0, mw = 0;
     if (rp_shape(riemann, &me, &mw) != 0) return fail(CLAW2_EINVAL, "unknown Riemann solver id %d", riemann);
-    if (variant < 0 || variant > 3) return fail(CLAW2_EINVAL, "variant must be 0..3 (got %d)", variant);
+    if (variant < 0 || variant > 4) return fail(CLAW2_EINVAL, "variant must be 0..4 (got %d)", variant);
     if (rows < 0 || rows > 4096) return fail(CLAW2_EINVAL, "rows must be 0..4096 (got %d)", rows);
     g_tune[riemann & (TUNE_SLOTS - 1)].variant = variant;
     g_tune[riemann & (TUNE_SLOTS - 1)].rows = rows;

@@ -657,6 +657,405 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
     if (GuessTraits<RP>::USES && a.counters) counter_commit(a.counters, n_it, n_solve);
 }
 
+// ---------------------------------------------------------------------------
+// The two-barrier form of the tile ("deferred x finish").  Each x-interface
+// is solved on its row R as before, but finished (limiter with the
+// neighbours' waves, correction, transverse solves) one row later, together
+// with the y work of that row: at row R every thread
+//   * finishes the x-interface (cp-1 | cp) of row R-1 (its waves and those of
+//     the neighbours wait in a double-buffered shared array, its own record
+//     in shared memory), with the cells of rows R-2, R-1, R in the ring, so
+//     solvers whose transverse solve reads the neighbouring cells need no
+//     extra deferral,
+//   * solves the y-interface (R-1 | R) and finishes (R-2 | R-1),
+//   * solves the x-interface of row R and stores its waves,
+// all between the same two barriers (cells visible; increments visible).  The
+// three independent chains in one block give the scheduler independent
+// FP64 work, and a barrier per row is saved.  Every increment lands in the
+// same cell with the same factors as in unsplit_tile; row R-2 is still
+// complete and written at the end of row R.
+// ---------------------------------------------------------------------------
+template <class RP, int NT, bool CAPA = false>
+struct UnsplitSmem2 {
+    static constexpr int ME = RP::MEQN, MW = RP::MWAVES, NC = RP::NC;
+    static constexpr int NF = (int)(sizeof(typename RP::Iface) / sizeof(double)) + 2 * ME;  // record + A-dq, A+dq
+    double cell[3][NC][NT];   // prepared cells of rows R-2, R-1, R (ring)
+    double w[2][MW][ME][NT];  // unlimited x-waves of rows R-1 and R (by row parity)
+    double fx[NF][NT];        // this column's x-interface of row R-1: record, A-dq, A+dq
+    double xl[3][ME][NT];     // increments for column cp-1: rows R-2, R-1, R
+    double yr[2][ME][NT];     // increments for column cp+1: rows R-2, R-1
+    double icap[CAPA ? 3 : 1][CAPA ? NT : 1];
+    double red[NT / 32];
+};
+
+template <class RP, int NT, int SPEC = SPEC_ANY, bool CAPA = false>
+__device__ __forceinline__ void unsplit_tile2(const StepArgs& a, int strip, int rb, UnsplitSmem2<RP, NT, CAPA>& S,
+                                              double& cfl) {
+    constexpr int ME = RP::MEQN, MW = RP::MWAVES, NC = RP::NC, W = NT - 4;
+    constexpr int NI = (int)(sizeof(typename RP::Iface) / sizeof(double));
+    using Iface = typename RP::Iface;
+    static_assert(sizeof(Iface) % sizeof(double) == 0, "interface records are made of doubles");
+
+    const int t = threadIdx.x;
+    const int mx = a.L.mx, my = a.L.my;
+    const int pitch = a.L.pitch;
+    const long long plane = a.L.plane;
+    const int cp = strip * W + t;
+    const int cpl = min(cp, mx + 3);
+    const int Hb = min(a.H, my - rb);
+    const int R0 = rb, R1 = rb + Hb + 3;
+    const bool out_col = (t >= 2) && (t < W + 2) && (cp <= mx + 1);
+    const bool xcfl_col = (t >= 2) && (t <= W + 2) && (cp <= mx + 2);
+    const bool ycfl_col = (t >= 1) && (t <= W + 2) && (cp <= mx + 2);
+    const int tl = (t > 0) ? t - 1 : 0;
+    const int tr = (t < NT - 1) ? t + 1 : NT - 1;
+    const double dtdx = a.dtdx, dtdy = a.dtdy;
+    const RPParams& P = a.rp;
+    const int order = (SPEC == SPEC_MC2) ? 2 : a.meth.order;
+    const int trans = (SPEC == SPEC_MC2) ? 2 : a.meth.transverse;
+    const bool tc = (order > 1) && (trans == 2);
+    const double* qo = a.qold + cpl;
+    double* qn = a.qnew + cpl;
+
+    constexpr int MA = AuxTraits<RP>::MAUX, MAD = MA > 0 ? MA : 1;
+    constexpr bool TAUX = AuxTraits<RP>::TRANSVERSE_AUX;
+    const double* ao = a.aux + cpl;
+    double pfa[MAD];
+#pragma unroll
+    for (int k = 0; k < MAD; ++k) pfa[k] = (MA > 0) ? __ldg(ao + k * plane + (long long)R0 * pitch) : 0.0;
+    const double* ko = CAPA ? a.capa + cpl : nullptr;
+    double pfk = CAPA ? __ldg(ko + (long long)R0 * pitch) : 1.0;
+
+    double pf[ME];
+    double accA[ME], accB[ME], accC[ME];  // rows R-2, R-1, R
+    Iface fY;                             // y-interface (R-2 | R-1)
+    double amY[ME], apY[ME], dY[MW];
+    unsigned long long n_it = 0, n_solve = 0;
+#pragma unroll
+    for (int m = 0; m < ME; ++m) {
+        pf[m] = __ldg(qo + m * plane + (long long)R0 * pitch);
+        accA[m] = accB[m] = accC[m] = 0.0;
+        amY[m] = apY[m] = 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < MW; ++k) dY[k] = 0.0;
+    memset(&fY, 0, sizeof(fY));
+
+    int s2 = 0, s1 = 2, s0 = 1;  // ring slots of rows R, R-1, R-2
+    for (int R = R0; R <= R1; ++R) {
+        // ---- row R: prepare this column's cell, prefetch the next row ----
+        {
+            double q[ME], c[NC];
+#pragma unroll
+            for (int m = 0; m < ME; ++m) q[m] = pf[m];
+            if (R < R1) {
+#pragma unroll
+                for (int m = 0; m < ME; ++m) pf[m] = __ldg(qo + m * plane + (long long)(R + 1) * pitch);
+            }
+            double av[MAD];
+#pragma unroll
+            for (int k = 0; k < MAD; ++k) av[k] = pfa[k];
+            if (MA > 0 && R < R1) {
+#pragma unroll
+                for (int k = 0; k < MAD; ++k) pfa[k] = __ldg(ao + k * plane + (long long)(R + 1) * pitch);
+            }
+            AuxTraits<RP>::prep(q, av, P, c);
+#pragma unroll
+            for (int k = 0; k < NC; ++k) S.cell[s2][k][t] = c[k];
+            if constexpr (CAPA) {
+                S.icap[s2][t] = 1.0 / pfk;
+                if (R < R1) pfk = __ldg(ko + (long long)(R + 1) * pitch);
+            }
+        }
+        __syncthreads();  // S1: cells of row R and x-waves of row R-1 visible; previous exchange consumed
+
+        double xl0[ME], xl1[ME], xl2[ME], yr0[ME], yr1[ME];  // this row's increments for the neighbours
+#pragma unroll
+        for (int m = 0; m < ME; ++m) xl0[m] = xl1[m] = xl2[m] = yr0[m] = yr1[m] = 0.0;
+
+        // ---- x: finish the interface (cp-1 | cp) of row R-1 ----
+        if (R - 1 > R0 && R - 1 < R1) {  // rows R0+1 .. R1-1 carry x-interfaces
+            const int pb = (R - 1) & 1;
+            Iface fX;
+            double amX[ME], apX[ME];
+            {
+                double* fr = reinterpret_cast<double*>(&fX);
+#pragma unroll
+                for (int k = 0; k < NI; ++k) fr[k] = S.fx[k][t];
+#pragma unroll
+                for (int m = 0; m < ME; ++m) {
+                    amX[m] = S.fx[NI + m][t];
+                    apX[m] = S.fx[NI + ME + m][t];
+                }
+            }
+            const double xdl = CAPA ? dtdx * S.icap[s1][tl] : dtdx, xdr = CAPA ? dtdx * S.icap[s1][t] : dtdx;
+            if (xcfl_col) cfl = fmax(cfl, CAPA ? iface_cfl2<RP, 1>(fX, P, xdl, xdr) : iface_cfl<RP, 1>(fX, P, dtdx));
+            double cq[ME];
+            if (order != 1) {
+                double dl[MW], dr[MW];
+#pragma unroll
+                for (int k = 0; k < MW; ++k) {
+                    double x = 0.0, y = 0.0;
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) {
+                        const double w = S.w[pb][k][m][t];
+                        x = x + S.w[pb][k][m][tl] * w;
+                        y = y + w * S.w[pb][k][m][tr];
+                    }
+                    dl[k] = x;
+                    dr[k] = y;
+                }
+                correction<RP, 1, SPEC>(fX, P, a.meth, CAPA ? 0.5 * (xdl + xdr) : dtdx, dl, dr, cq);
+            } else {
+#pragma unroll
+                for (int m = 0; m < ME; ++m) cq[m] = 0.0;
+            }
+#pragma unroll
+            for (int m = 0; m < ME; ++m) {
+                const double f = 0.5 * cq[m];
+                accB[m] = accB[m] - dtdx * (apX[m] - f);
+                xl1[m] = -dtdx * (amX[m] + f);
+            }
+            if (trans > 0) {
+                const double h = 0.5 * dtdx * dtdy;
+                const double hl = CAPA ? h * S.icap[s1][tl] : h, hr = CAPA ? h * S.icap[s1][t] : h;
+                double as2[ME], bm[ME], bp[ME];
+#pragma unroll
+                for (int m = 0; m < ME; ++m) as2[m] = tc ? amX[m] + cq[m] : amX[m];
+                if constexpr (TAUX) {  // cell (cp-1, R-1) between rows R-2 and R
+                    double cm[NC], c0[NC], cu[NC];
+#pragma unroll
+                    for (int k = 0; k < NC; ++k) {
+                        cm[k] = S.cell[s0][k][tl];
+                        c0[k] = S.cell[s1][k][tl];
+                        cu[k] = S.cell[s2][k][tl];
+                    }
+                    RP::template rpt2_aux<1>(as2, cm, c0, cu, bm, bp);
+                } else {
+                    RP::template rpt2<1>(fX, P, as2, bm, bp);  // imp = 1 -> column cp-1
+                }
+#pragma unroll
+                for (int m = 0; m < ME; ++m) {
+                    xl1[m] = xl1[m] + hl * (bp[m] - bm[m]);
+                    xl0[m] = hl * bm[m];
+                    xl2[m] = -hl * bp[m];
+                }
+#pragma unroll
+                for (int m = 0; m < ME; ++m) as2[m] = tc ? apX[m] - cq[m] : apX[m];
+                if constexpr (TAUX) {  // cell (cp, R-1)
+                    double cm[NC], c0[NC], cu[NC];
+#pragma unroll
+                    for (int k = 0; k < NC; ++k) {
+                        cm[k] = S.cell[s0][k][t];
+                        c0[k] = S.cell[s1][k][t];
+                        cu[k] = S.cell[s2][k][t];
+                    }
+                    RP::template rpt2_aux<1>(as2, cm, c0, cu, bm, bp);
+                } else {
+                    RP::template rpt2<1>(fX, P, as2, bm, bp);  // imp = 2 -> column cp
+                }
+#pragma unroll
+                for (int m = 0; m < ME; ++m) {
+                    accB[m] = accB[m] + hr * (bp[m] - bm[m]);
+                    accA[m] = accA[m] + hr * bm[m];
+                    accC[m] = accC[m] - hr * bp[m];
+                }
+            }
+        }
+
+        // ---- y: solve (R-1 | R), finish (R-2 | R-1) ----
+        if (R > R0) {
+            double cB[NC], cA[NC];
+#pragma unroll
+            for (int k = 0; k < NC; ++k) {
+                cB[k] = S.cell[s1][k][t];
+                cA[k] = S.cell[s2][k][t];
+            }
+            Iface fN;
+            double amN[ME], apN[ME];
+            double gy = 0.0;
+            if (GuessTraits<RP>::USES && a.guess) gy = a.guess[plane + (long long)R * pitch + cpl];
+            GuessTraits<RP>::template solve<2>(cB, cA, P, gy, fN, amN, apN);
+            if (GuessTraits<RP>::USES && cp <= mx + 3) {
+                n_it += GuessTraits<RP>::count(fN);
+                n_solve += 1;
+            }
+            double dn[MW];
+            {
+                double wY[MW][ME], wN[MW][ME];
+                RP::template waves<2>(fY, P, wY);
+                RP::template waves<2>(fN, P, wN);
+#pragma unroll
+                for (int k = 0; k < MW; ++k) {
+                    double d = 0.0;
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) d = d + wY[k][m] * wN[k][m];
+                    dn[k] = d;
+                }
+            }
+            if (R >= R0 + 3) {
+                const double ydl = CAPA ? dtdy * S.icap[s0][t] : dtdy, ydr = CAPA ? dtdy * S.icap[s1][t] : dtdy;
+                if (ycfl_col)
+                    cfl = fmax(cfl, CAPA ? iface_cfl2<RP, 2>(fY, P, ydl, ydr) : iface_cfl<RP, 2>(fY, P, dtdy));
+                double cq[ME];
+                if (order != 1) {
+                    correction<RP, 2, SPEC>(fY, P, a.meth, CAPA ? 0.5 * (ydl + ydr) : dtdy, dY, dn, cq);
+                } else {
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) cq[m] = 0.0;
+                }
+#pragma unroll
+                for (int m = 0; m < ME; ++m) {
+                    const double f = 0.5 * cq[m];
+                    accA[m] = accA[m] - dtdy * (amY[m] + f);
+                    accB[m] = accB[m] - dtdy * (apY[m] - f);
+                }
+                if (trans > 0) {
+                    const double h = 0.5 * dtdy * dtdx;
+                    const double hl = CAPA ? h * S.icap[s0][t] : h, hr = CAPA ? h * S.icap[s1][t] : h;
+                    double as2[ME], bm[ME], bp[ME];
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) as2[m] = tc ? amY[m] + cq[m] : amY[m];
+                    if constexpr (TAUX) {  // cell (cp, R-2) between columns cp-1 and cp+1
+                        double cm[NC], c0[NC], cu[NC];
+#pragma unroll
+                        for (int k = 0; k < NC; ++k) {
+                            cm[k] = S.cell[s0][k][tl];
+                            c0[k] = S.cell[s0][k][t];
+                            cu[k] = S.cell[s0][k][tr];
+                        }
+                        RP::template rpt2_aux<2>(as2, cm, c0, cu, bm, bp);
+                    } else {
+                        RP::template rpt2<2>(fY, P, as2, bm, bp);  // imp = 1 -> row R-2
+                    }
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) {
+                        accA[m] = accA[m] + hl * (bp[m] - bm[m]);
+                        xl0[m] = xl0[m] + hl * bm[m];
+                        yr0[m] = -hl * bp[m];
+                    }
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) as2[m] = tc ? apY[m] - cq[m] : apY[m];
+                    if constexpr (TAUX) {  // cell (cp, R-1)
+                        double cm[NC], c0[NC], cu[NC];
+#pragma unroll
+                        for (int k = 0; k < NC; ++k) {
+                            cm[k] = S.cell[s1][k][tl];
+                            c0[k] = S.cell[s1][k][t];
+                            cu[k] = S.cell[s1][k][tr];
+                        }
+                        RP::template rpt2_aux<2>(as2, cm, c0, cu, bm, bp);
+                    } else {
+                        RP::template rpt2<2>(fY, P, as2, bm, bp);  // imp = 2 -> row R-1
+                    }
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) {
+                        accB[m] = accB[m] + hr * (bp[m] - bm[m]);
+                        xl1[m] = xl1[m] + hr * bm[m];
+                        yr1[m] = -hr * bp[m];
+                    }
+                }
+            }
+            fY = fN;
+#pragma unroll
+            for (int m = 0; m < ME; ++m) { amY[m] = amN[m]; apY[m] = apN[m]; }
+#pragma unroll
+            for (int k = 0; k < MW; ++k) dY[k] = dn[k];
+        }
+
+        // ---- x: solve the interface (cp-1 | cp) of row R, keep it for the next row ----
+        if (R > R0 && R < R1) {
+            double cL[NC], cR[NC];
+#pragma unroll
+            for (int k = 0; k < NC; ++k) {
+                cL[k] = S.cell[s2][k][tl];
+                cR[k] = S.cell[s2][k][t];
+            }
+            Iface fX;
+            double amX[ME], apX[ME];
+            double gx = 0.0;
+            if (GuessTraits<RP>::USES && a.guess) gx = a.guess[(long long)R * pitch + cpl];
+            GuessTraits<RP>::template solve<1>(cL, cR, P, gx, fX, amX, apX);
+            if (GuessTraits<RP>::USES && cp <= mx + 3 && t > 0) {
+                n_it += GuessTraits<RP>::count(fX);
+                n_solve += 1;
+            }
+            double wX[MW][ME];
+            RP::template waves<1>(fX, P, wX);
+            const int pb = R & 1;
+#pragma unroll
+            for (int k = 0; k < MW; ++k)
+#pragma unroll
+                for (int m = 0; m < ME; ++m) S.w[pb][k][m][t] = wX[k][m];
+            const double* fr = reinterpret_cast<const double*>(&fX);
+#pragma unroll
+            for (int k = 0; k < NI; ++k) S.fx[k][t] = fr[k];
+#pragma unroll
+            for (int m = 0; m < ME; ++m) {
+                S.fx[NI + m][t] = amX[m];
+                S.fx[NI + ME + m][t] = apX[m];
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < ME; ++m) {
+            S.xl[0][m][t] = xl0[m];
+            S.xl[1][m][t] = xl1[m];
+            S.xl[2][m][t] = xl2[m];
+            S.yr[0][m][t] = yr0[m];
+            S.yr[1][m][t] = yr1[m];
+        }
+        __syncthreads();  // S2: neighbour increments (and this row's x-waves) visible
+#pragma unroll
+        for (int m = 0; m < ME; ++m) {
+            accA[m] = accA[m] + S.xl[0][m][tr] + S.yr[0][m][tl];
+            accB[m] = accB[m] + S.xl[1][m][tr] + S.yr[1][m][tl];
+            accC[m] = accC[m] + S.xl[2][m][tr];
+        }
+
+        // ---- row R-2 is complete ----
+        if (R >= R0 + 4 && out_col) {
+            double v[ME];
+            const double ik = CAPA ? S.icap[s0][t] : 1.0;
+#pragma unroll
+            for (int m = 0; m < ME; ++m) v[m] = CAPA ? S.cell[s0][m][t] + ik * accA[m] : S.cell[s0][m][t] + accA[m];
+#pragma unroll
+            for (int m = 0; m < ME; ++m) qn[m * plane + (long long)(R - 2) * pitch] = v[m];
+            if (!all_finite<ME>(v)) atomicOr(a.status, 1);
+        }
+#pragma unroll
+        for (int m = 0; m < ME; ++m) {
+            accA[m] = accB[m];
+            accB[m] = accC[m];
+            accC[m] = 0.0;
+        }
+        const int tmp = s0;
+        s0 = s1;
+        s1 = s2;
+        s2 = tmp;
+    }
+    if (GuessTraits<RP>::USES && a.counters) counter_commit(a.counters, n_it, n_solve);
+}
+
+template <class RP, int NT, int MINB, int SPEC, bool CAPA = false>
+__global__ void __launch_bounds__(NT, MINB) k_step_unsplit2(const StepArgs a) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    UnsplitSmem2<RP, NT, CAPA>& S = *reinterpret_cast<UnsplitSmem2<RP, NT, CAPA>*>(smem_raw);
+    int tile = blockIdx.x;
+    if (a.tile_order) {
+        const int t = a.tile_order[blockIdx.x];
+        if (t >= 0 && t < (int)gridDim.x) tile = t;
+    }
+    long long t0 = 0;
+    if (a.tile_cost && threadIdx.x == 0) t0 = clock64();
+    double cfl = 0.0;
+    unsplit_tile2<RP, NT, SPEC, CAPA>(a, tile % a.nstrips, (tile / a.nstrips) * a.H, S, cfl);
+    cfl_commit(cfl, S.red, a.cfl_bits);
+    if (a.tile_cost && threadIdx.x == 0) {
+        const long long c = clock64() - t0;
+        a.tile_cost[tile] = (unsigned int)(c < 0 ? 0 : (c > 0xffffffffll ? 0xffffffffll : c));
+    }
+}
+
 // The same kernel with its rows staged by TMA from the tensor map of qold.
 template <class RP, int NT, int MINB, int SPEC>
 __global__ void __launch_bounds__(NT, MINB) k_step_unsplit_tma(const StepArgs a, const __grid_constant__ CUtensorMap tm) {

@@ -200,3 +200,27 @@ def test_annulus_device_frames_match_oracle(oracle):
     for fg, fo in zip(claw_g.frames, claw_o.frames):
         assert fg.t == fo.t
         assert max_rel(fg.q, fo.q) <= 1e-11
+
+
+@pytest.mark.parametrize("variant", [0, 4])
+def test_capacity_in_both_tiles(oracle, variant):
+    # the capacity form of the one-row-late x finish (variant 4) and of the
+    # original tile, through the stateless step
+    from pyclaw_b200 import tune
+    mx, my = 257, 70
+    qbc = random_qbc(_lib.RP_ADVECTION, mx, my, seed=99)
+    aux = _vc_adv_aux(mx, my, seed=98)
+    method = _method(2, 2, 3)
+    mthlim = np.full(1, 4, dtype=np.intc)
+    dx, dy = 1.0 / mx, 1.0 / my
+    dt = _dt(1.5, aux[2], dx, dy)
+    q_o = qbc.copy(order="F")
+    cfl_o = oracle.step2(qbc, q_o, dx, dy, dt, method, mthlim, VCA, [], aux=aux)
+    tune.set_shape(VCA, variant, 12)
+    try:
+        q_g, cfl_g = classic2.step2(max(mx, my), 2, mx, my, qbc, qbc.copy(order="F"), aux, dx, dy, dt, method,
+                                    mthlim, rpn2=VCA)
+    finally:
+        tune.set_shape(VCA, 0, 0)
+    assert abs(cfl_g - cfl_o) <= PARITY_RTOL * cfl_o
+    assert max_rel(q_g[:, 2:-2, 2:-2], q_o[:, 2:-2, 2:-2]) <= PARITY_RTOL

@@ -237,12 +237,13 @@ def test_run_host_equals_one_call_per_step():
     assert np.array_equal(sol.state.get_q_global(), ref[-1])
 
 
-@pytest.mark.parametrize("variant", [2, 3])
+@pytest.mark.parametrize("variant", [2, 3, 4])
 @pytest.mark.parametrize("name,n", [("euler", 130), ("shallow", 70), ("acoustics", 257), ("advection", 131)])
 def test_tma_row_staging_matches_oracle(oracle, variant, name, n):
     # launch variants 2 and 3 stage every row of a strip by TMA (tensor map of
     # the q planes, mbarrier completion); sizes with a ragged last strip, whose
-    # columns past the grid the copy fills with zeros
+    # columns past the grid the copy fills with zeros; variant 4 is the
+    # two-barrier tile (x-interfaces finished one row late)
     from pyclaw_b200 import tune
     make = {"euler": lambda: workloads.euler_quadrants_unsplit(n=n),
             "shallow": lambda: workloads.shallow_dam_break_unsplit(n=n),

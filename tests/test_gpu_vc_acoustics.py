@@ -99,7 +99,7 @@ def test_vc_device_run_matches_reference_goldens(goldens):
     assert np.max(np.abs(goldens["acoustics_variable_pressure_classic"] - q[0])) < 1e-12
 
 
-@pytest.mark.parametrize("transverse,variant", [(1, 0), (2, 0), (2, 1), (2, 2)])
+@pytest.mark.parametrize("transverse,variant", [(1, 0), (2, 0), (2, 1), (2, 2), (1, 4), (2, 4)])
 def test_vc_device_steps_match_oracle(oracle, transverse, variant):
     # several strips and row blocks; each step of the device patch (aux ghost
     # cells filled on the device from the aux BCs) against the oracle from the
