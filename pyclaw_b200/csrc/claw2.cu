@@ -266,8 +266,16 @@ void launch_unsplit(const StepArgs& a, cudaStream_t st, const CUtensorMap* tm) {
     else launch_unsplit_v<RP, 2>(a, st, use);
 }
 
-template <class RP>
-void launch_split(const StepArgs& ax, const StepArgs& ay, cudaStream_t st, int which) {
+// the split sweeps' specialisation: order 2 with one limiter on every family
+int split_spec(const Method& m, int mwaves) {
+    if (m.order != 2 || m.fwave != 0) return SPEC_ANY;
+    for (int k = 1; k < mwaves; ++k)
+        if (m.mthlim[k] != m.mthlim[0]) return SPEC_ANY;
+    return m.mthlim[0] == 4 ? SPEC_MC2 : m.mthlim[0] == 1 ? SPEC_MM2 : SPEC_ANY;
+}
+
+template <class RP, int SPEC>
+void launch_split_s(const StepArgs& ax, const StepArgs& ay, cudaStream_t st, int which) {
     if (which & 1) {
         constexpr int W = NT_SPLIT_X - 4;
         const int ns = (ax.L.mx + W - 1) / W;
@@ -276,15 +284,24 @@ void launch_split(const StepArgs& ax, const StepArgs& ay, cudaStream_t st, int w
         dim3 grid(ns, (ax.L.my + 4 + b.H - 1) / b.H);
         constexpr int smem = (int)sizeof(SplitXSmem<RP, NT_SPLIT_X>);
         static unsigned long long attr = 0;
-        smem_attr(k_split_x<RP, NT_SPLIT_X>, smem, attr);
-        k_split_x<RP, NT_SPLIT_X><<<grid, NT_SPLIT_X, smem, st>>>(b);
+        smem_attr(k_split_x<RP, NT_SPLIT_X, SPEC>, smem, attr);
+        k_split_x<RP, NT_SPLIT_X, SPEC><<<grid, NT_SPLIT_X, smem, st>>>(b);
     }
     if (which & 2) {
         const int ns = (ay.L.mx + 4 + NT_SPLIT_Y - 1) / NT_SPLIT_Y;
         StepArgs b = ay;
         b.H = pick_rows(ns, ay.L.my);
         dim3 grid(ns, (ay.L.my + b.H - 1) / b.H);
-        k_split_y<RP, NT_SPLIT_Y><<<grid, NT_SPLIT_Y, 0, st>>>(b);
+        k_split_y<RP, NT_SPLIT_Y, SPEC><<<grid, NT_SPLIT_Y, 0, st>>>(b);
+    }
+}
+
+template <class RP>
+void launch_split(const StepArgs& ax, const StepArgs& ay, cudaStream_t st, int which) {
+    switch (split_spec(ax.meth, RP::MWAVES)) {
+        case SPEC_MC2: launch_split_s<RP, SPEC_MC2>(ax, ay, st, which); break;
+        case SPEC_MM2: launch_split_s<RP, SPEC_MM2>(ax, ay, st, which); break;
+        default: launch_split_s<RP, SPEC_ANY>(ax, ay, st, which); break;
     }
 }
 

@@ -116,7 +116,9 @@ __device__ __forceinline__ bool all_finite(const double (&v)[ME]) {
 // high-resolution method with transverse correction waves and the MC limiter
 // on every family (order 2, trans_cor, mthlim = 4, no f-waves), fixed at
 // compile time so the limiter switch and the method branches fold away.
-enum { SPEC_ANY = 0, SPEC_MC2 = 1 };
+// SPEC_MM2 (order 2, minmod on every family, no f-waves: the reference's
+// default limiter) specialises the split sweeps the same way.
+enum { SPEC_ANY = 0, SPEC_MC2 = 1, SPEC_MM2 = 2 };
 
 // Limiter (limiter.f90:29-53 / philim.f90) and second-order correction
 // cqxx = sum_k coef_k * phi_k * w_k (flux2.f90:134-160) for one interface.
@@ -135,14 +137,14 @@ __device__ __forceinline__ void correction(const typename RP::Iface& f, const RP
     for (int m = 0; m < ME; ++m) cq[m] = 0.0;
 #pragma unroll
     for (int k = 0; k < MW; ++k) {
-        const int lim = (SPEC == SPEC_MC2) ? 4 : meth.mthlim[k];
+        const int lim = (SPEC == SPEC_MC2) ? 4 : (SPEC == SPEC_MM2) ? 1 : meth.mthlim[k];
         double wn2 = 0.0;
 #pragma unroll
         for (int m = 0; m < ME; ++m) wn2 = wn2 + w[k][m] * w[k][m];
         double phi = 1.0;
         if (lim != 0 && wn2 != 0.0) phi = philim(wn2, (s[k] > 0.0) ? dl[k] : dr[k], lim);
         const double as = fabs(s[k]);
-        const bool fw = (SPEC == SPEC_MC2) ? false : (meth.fwave != 0);
+        const bool fw = (SPEC != SPEC_ANY) ? false : (meth.fwave != 0);
         const double coef = (fw ? copysign(1.0, s[k]) : as) * (1.0 - as * dtdx);
 #pragma unroll
         for (int m = 0; m < ME; ++m) cq[m] = cq[m] + coef * (phi * w[k][m]);
@@ -1156,7 +1158,7 @@ struct SplitXSmem {
     double red[NT / 32];
 };
 
-template <class RP, int NT>
+template <class RP, int NT, int SPEC = SPEC_ANY>
 __global__ void __launch_bounds__(NT) k_split_x(const StepArgs a) {
     constexpr int ME = RP::MEQN, MW = RP::MWAVES, NC = RP::NC, W = NT - 4;
     constexpr int MAD = AuxTraits<RP>::MAUX > 0 ? AuxTraits<RP>::MAUX : 1;
@@ -1220,7 +1222,7 @@ __global__ void __launch_bounds__(NT) k_split_x(const StepArgs a) {
         const double xdl = dtdx * S.icap[buf][tl], xdr = dtdx * S.icap[buf][t];
         if (xcfl_col) cfl = fmax(cfl, iface_cfl2<RP, 1>(fX, P, xdl, xdr));
         double cq[ME];
-        if (a.meth.order != 1) {
+        if ((SPEC != SPEC_ANY) || a.meth.order != 1) {
             double dl[MW], dr[MW];
 #pragma unroll
             for (int k = 0; k < MW; ++k) {
@@ -1234,7 +1236,7 @@ __global__ void __launch_bounds__(NT) k_split_x(const StepArgs a) {
                 dl[k] = x;
                 dr[k] = y;
             }
-            correction<RP, 1>(fX, P, a.meth, 0.5 * (xdl + xdr), dl, dr, cq);
+            correction<RP, 1, SPEC>(fX, P, a.meth, 0.5 * (xdl + xdr), dl, dr, cq);
         } else {
 #pragma unroll
             for (int m = 0; m < ME; ++m) cq[m] = 0.0;
@@ -1264,7 +1266,7 @@ __global__ void __launch_bounds__(NT) k_split_x(const StepArgs a) {
 // per column marching down the rows; limiter neighbours come from the
 // register pipeline.  Writes the interior cells of qnew.
 // ---------------------------------------------------------------------------
-template <class RP, int NT>
+template <class RP, int NT, int SPEC = SPEC_ANY>
 __global__ void __launch_bounds__(NT) k_split_y(const StepArgs a) {
     constexpr int ME = RP::MEQN, MW = RP::MWAVES, NC = RP::NC;
     constexpr int MAD = AuxTraits<RP>::MAUX > 0 ? AuxTraits<RP>::MAUX : 1;
@@ -1338,8 +1340,8 @@ __global__ void __launch_bounds__(NT) k_split_y(const StepArgs a) {
             const double ydl = dtdy * ic0, ydr = dtdy * ic1;
             if (valid) cfl = fmax(cfl, iface_cfl2<RP, 2>(fY, P, ydl, ydr));
             double cq[ME];
-            if (a.meth.order != 1) {
-                correction<RP, 2>(fY, P, a.meth, 0.5 * (ydl + ydr), dY, dn, cq);
+            if ((SPEC != SPEC_ANY) || a.meth.order != 1) {
+                correction<RP, 2, SPEC>(fY, P, a.meth, 0.5 * (ydl + ydr), dY, dn, cq);
             } else {
 #pragma unroll
                 for (int m = 0; m < ME; ++m) cq[m] = 0.0;
