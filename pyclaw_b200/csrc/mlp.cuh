@@ -388,7 +388,7 @@ static __global__ void __launch_bounds__(128) k_mlp_guess(const MlpPacked* __res
         rows[w][32 + lane][k] = isfinite(fy[k]) ? fy[k] : 0.f;
     }
     __syncthreads();
-    // PVRS as the judge: a weak jump (w below MLP_WMIN) keeps the PVRS guess,
+    // PVRS decides: a weak jump (w below MLP_WMIN) keeps the PVRS guess,
     // which is accurate there and where the network has seen no training data;
     // a warp with only weak jumps skips the network altogether.
     const bool strong = (wx >= MLP_WMIN) || (wy >= MLP_WMIN);

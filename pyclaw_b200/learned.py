@@ -14,7 +14,7 @@ Feature and target definition (also in csrc/exact_euler.h, features()):
 x = (log rho_L/rb, log rho_R/rb, u_L/cb, u_R/cb, log p_L/pb, log p_R/pb),
 rb = sqrt(rho_L rho_R), pb = sqrt(p_L p_R), cb = sqrt(gamma pb / rb);
 target y = log(p*/p_pvrs) / w with w = J^2/(1 + J^2), J^2 the squared
-normalised jump; guess = p_pvrs * exp(w y).  The PVRS guess is the judge:
+normalised jump; guess = p_pvrs * exp(w y).  The PVRS guess decides:
 interfaces with w < 0.05 (weak jumps, where PVRS is accurate and the training
 distribution has no samples) keep it.
 """

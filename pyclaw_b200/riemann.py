@@ -66,8 +66,10 @@ vc_advection_2D.num_aux = 2
 
 # The p-system (nonlinear elasticity) in a heterogeneous medium, f-waves: no
 # cparam; aux = (density, bulk modulus, stress-strain relation 1 linear /
-# 2 exponential, strain at the start of the step) per cell
-# (clawpack.riemann.psystem_2D).
+# 2 exponential, strain at the start of the step) per cell, as
+# clawpack.riemann.psystem_2D takes them.  Restated from the mathematics
+# (linearisation at each cell's own strain); it does not reproduce the
+# reference's p-system gauge files, whose solver makes another choice.
 psystem_2D = RiemannSolver('psystem_2D', _lib.RP_PSYSTEM, 3, 2, (), fwave=True)
 psystem_2D.num_aux = 4
 

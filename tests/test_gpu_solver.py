@@ -256,3 +256,29 @@ def test_tma_row_staging_matches_oracle(oracle, variant, name, n):
         _stepwise(oracle, claw, nsteps=4)
     finally:
         tune.set_shape(rp, 0, 0)
+
+
+def test_largest_benchmark_size_one_step_matches_oracle(oracle):
+    # the shallow-water benchmark size, 4096 x 4096 (50 M unknowns): one unsplit
+    # step through the stateless entry point against the oracle on all cores
+    import os
+    from helpers import method_vector, random_qbc, set_cparam
+    from pyclaw_b200 import classic2
+    mx = my = 4096
+    rp = _lib.RP_SHALLOW_ROE
+    qbc = random_qbc(rp, mx, my, seed=4096)
+    method = method_vector(2, 2)
+    mthlim = np.full(3, 4, dtype=np.intc)
+    dx = dy = 1.0 / mx
+    dt = 0.2 * dx
+    oracle.set_threads(os.cpu_count() or 1)
+    try:
+        q_o = qbc.copy(order="F")
+        cfl_o = oracle.step2(qbc, q_o, dx, dy, dt, method, mthlim, rp, [1.0, 1.0])
+    finally:
+        oracle.set_threads(1)
+    set_cparam(classic2, rp)
+    q_g, cfl_g = classic2.step2(mx, 2, mx, my, qbc, qbc.copy(order="F"), None, dx, dy, dt, method, mthlim,
+                                rpn2=rp)
+    assert abs(cfl_g - cfl_o) <= PARITY_RTOL * cfl_o
+    assert max_rel(q_g[:, 2:-2, 2:-2], q_o[:, 2:-2, 2:-2]) <= PARITY_RTOL
