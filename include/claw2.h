@@ -186,6 +186,27 @@ int claw2_patch_upload_qbc(claw2_patch* p, const double* qbc);
  * user_aux_bc_lower/upper functions that solver.py:378-427 calls). */
 int claw2_patch_upload_auxbc(claw2_patch* p, const double* auxbc);
 
+/* Device-resident time loop: Solver.evolve_to_time (src/pyclaw/solver.py:
+ * 554-666) for a solver without host callbacks, with get_dt, the CFL test,
+ * accept/reject and the clipping to tend done on the GPU after every step, so
+ * the host waits only every few dozen steps.  In: t (solution.t), tstart,
+ * tend, dt (solver.dt), cfl (the solver's cached Courant number), cfl_desired,
+ * cfl_max, dt_max, dtmin/dtmax/cflmax (solver.status), dt_variable,
+ * dt_old_set (solver.dt_old is not None), max_steps (attempts allowed).  Out:
+ * the same fields after the loop, num_steps (accepted), attempts (accepted +
+ * rejected), cfl_error (a fixed-dt step exceeded cfl_max: the reference
+ * raises CFLError).  The current state is the loop's result; a step that
+ * produced a non-finite value ends the loop with that step undone and
+ * CLAW2_ENONFINITE.  Same steps, dt sequence and results as the host loop. */
+typedef struct claw2_evolve_state {
+    double t, tstart, tend, dt, cfl;
+    double cfl_desired, cfl_max, dt_max;
+    double dtmin, dtmax, cflmax;
+    int dt_variable, dt_old_set, max_steps;
+    int num_steps, attempts, cfl_error;
+} claw2_evolve_state;
+int claw2_patch_evolve(claw2_patch* p, claw2_evolve_state* s);
+
 /* One hyperbolic step from the current q: ghost fill on the device, then the
  * unsplit (or split) step into the pending buffer.  If cfl is non-NULL the
  * call waits and returns the Courant number; with NULL it only enqueues. */

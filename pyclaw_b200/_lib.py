@@ -48,6 +48,14 @@ class Claw2Desc(ctypes.Structure):
     ]
 
 
+class Claw2EvolveState(ctypes.Structure):
+    """Mirror of ``claw2_evolve_state``."""
+    _fields_ = [(n, ctypes.c_double) for n in ("t", "tstart", "tend", "dt", "cfl", "cfl_desired", "cfl_max",
+                                               "dt_max", "dtmin", "dtmax", "cflmax")] + \
+               [(n, ctypes.c_int) for n in ("dt_variable", "dt_old_set", "max_steps", "num_steps", "attempts",
+                                            "cfl_error")]
+
+
 class Claw2Error(RuntimeError):
     """A status code other than CLAW2_OK, with the library's message."""
 
@@ -90,6 +98,7 @@ _SIGNATURES = {
     "claw2_patch_euler_axisymmetric_source": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int,
                                                             ctypes.c_double]),
     "claw2_patch_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _c_double_p]),
+    "claw2_patch_evolve": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Claw2EvolveState)]),
     "claw2_patch_run_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
                                             ctypes.POINTER(ctypes.c_void_p), _c_double_p, _c_double_p]),
     "claw2_patch_accept": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),

@@ -10,7 +10,7 @@ stays there between steps.
 import numpy as np
 
 from .limiters import tvd
-from .solver import BC, Solver
+from .solver import BC, CFLError, Solver
 from . import _lib
 from . import hostbc as _hostbc
 
@@ -104,6 +104,7 @@ class ClawSolver2D(ClawSolver):
         self._dev = None
         self._aux_pushed = None  # the State.aux array last uploaded to the device
         self._aux_copy = None    # its contents then (kept when a before-step hook may edit it)
+        self.device_time_loop = True  # evolve_to_time on the GPU when no host callback needs a step
         self._q_backup = None    # q before the host hooks of a step (before_step, step_source)
         self._committed = False  # the step's result is already current (a source step followed it)
         super(ClawSolver2D, self).__init__(riemann_solver, claw_package)
@@ -251,6 +252,71 @@ class ClawSolver2D(ClawSolver):
         self._committed = False
         if not accept and self._q_backup is not None:
             solution.states[0].q = self._q_backup  # uploaded before the next step
+
+    def _device_loop_ok(self, solution, tend):
+        """The whole evolve_to_time can run on the GPU: a target time, no host
+        callback between steps (before_step, step_source, gauges, custom BCs)
+        and none of this class's stepping methods replaced by a subclass."""
+        cls = type(self)
+        return (self.device_time_loop and tend is not None and self.before_step is None and
+                self.step_source is None and not solution.state.grid.gauges and
+                not _hostbc.has_custom_q(self) and not _hostbc.needs_host_fill(self) and
+                cls.step is ClawSolver2D.step and cls.step_hyperbolic is ClawSolver2D.step_hyperbolic and
+                cls._begin_step is ClawSolver2D._begin_step and cls._end_step is ClawSolver2D._end_step and
+                cls.get_dt is ClawSolver2D.get_dt and cls.accept_reject_step is ClawSolver2D.accept_reject_step)
+
+    def evolve_to_time(self, solution, tend=None):
+        """solver.py:554-666.  Without host callbacks between steps the loop
+        runs on the GPU (claw2_patch_evolve: the same get_dt, CFL test,
+        accept/reject and dt sequence, the host waiting only every few dozen
+        steps); otherwise the host loop."""
+        if not self._device_loop_ok(solution, tend):
+            return super(ClawSolver2D, self).evolve_to_time(solution, tend)
+        if not self._is_set_up:
+            self.setup(solution)
+        tstart = solution.t
+        if not self.dt_variable:
+            self.max_steps = int((tend - tstart + 1e-10) / self.dt)
+            if abs(self.max_steps * self.dt - (tend - tstart)) > 1e-5 * (tend - tstart):
+                raise Exception('dt does not divide (tend-tstart) and dt is fixed!')
+        if self.dt_variable == 1 and self.cfl_desired > self.cfl_max:
+            raise Exception('Variable time-stepping and desired CFL > maximum CFL')
+        if tend <= tstart:
+            self.logger.info("Already at or beyond end time: no evolution required.")
+            self.max_steps = 0
+        state = solution.states[0]
+        dev = self._dev
+        if dev is None or state._mirror is not dev:
+            self._make_device_patch(solution)
+            dev = self._dev
+        if dev.host_dirty:
+            dev.push(state)
+        self._push_aux(state, force=False)
+        es = _lib.Claw2EvolveState(
+            t=solution.t, tstart=tstart, tend=tend, dt=self.dt, cfl=self.cfl.get_cached_max(),
+            cfl_desired=self.cfl_desired, cfl_max=self.cfl_max, dt_max=self.dt_max,
+            dtmin=self.status['dtmin'], dtmax=self.status['dtmax'], cflmax=self.status['cflmax'],
+            dt_variable=1 if self.dt_variable else 0, dt_old_set=0 if self.dt_old is None else 1,
+            max_steps=self.max_steps)
+        rc = dev.evolve(es)
+        if es.attempts > 0:
+            solution.t = es.t
+            self.dt = es.dt
+            self.cfl.set_global_max(es.cfl)
+            if es.dt_old_set and self.dt_old is None:
+                self.dt_old = self.dt
+            self.status['dtmin'] = es.dtmin
+            self.status['dtmax'] = es.dtmax
+            self.status['cflmax'] = es.cflmax
+            self.status['numsteps'] += es.num_steps
+        _lib.check(rc)
+        if es.cfl_error:
+            self.accept_step = False
+            raise CFLError('CFL too large, giving up!')
+        self.accept_step = True
+        if self.dt_variable and solution.t < tend and es.num_steps == self.max_steps:
+            raise Exception("Maximum number of timesteps have been taken")
+        return self.status
 
     def step(self, solution, take_one_step, tstart, tend):
         """classic/solver.py:96-146.  With a source step the hyperbolic result

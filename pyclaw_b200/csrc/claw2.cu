@@ -793,6 +793,9 @@ struct claw2_patch {
     // claw2_patch_write_ascii_async: pinned copy of a frame, its event, the writer thread
     double* out_host = nullptr;
     cudaEvent_t out_ev = nullptr;
+    // claw2_patch_evolve: the time loop's state on the device and a pinned copy
+    EvolveDev* evo = nullptr;
+    EvolveDev* h_evo = nullptr;
     std::thread* writer = nullptr;
     int writer_rc = 0;
     void* gather_buf = nullptr;   // claw2_patch_gather_q: values, then cell indices
@@ -1038,6 +1041,8 @@ int claw2_patch_destroy(claw2_patch* p) {
         cudaFree(p->gather_buf);
         cudaFreeHost(p->out_host);
         if (p->out_ev) cudaEventDestroy(p->out_ev);
+        cudaFree(p->evo);
+        cudaFreeHost(p->h_evo);
         cudaFree(p->cfl);
         cudaFree(p->status);
         cudaFreeHost(p->h_cfl);
@@ -1279,6 +1284,121 @@ int patch_enqueue_step(claw2_patch* p, double dt) {
     return CLAW2_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Device-resident time loop (claw2_patch_evolve)
+// ---------------------------------------------------------------------------
+// get_dt of the reference's loop (src/pyclaw/solver.py:524-552) on the loop
+// state, with Python's min/max tie rules (same values), then dt/dx, dt/dy.
+__host__ __device__ inline void evolve_get_dt(EvolveDev& e) {
+    if (e.dt_variable && e.dt_old_set) {
+        if (e.cfl > 0.0) {
+            const double x = e.dt * e.cfl_desired / e.cfl;
+            e.dt = (x < e.dt_max) ? x : e.dt_max;             // min(dt_max, x)
+            e.dtmin = (e.dtmin < e.dt) ? e.dtmin : e.dt;      // min(dt, dtmin)
+            e.dtmax = (e.dtmax > e.dt) ? e.dtmax : e.dt;      // max(dt, dtmax)
+        } else {
+            e.dt = e.dt_max;
+        }
+    } else {
+        e.dt_old_set = 1;
+    }
+    if (e.t + e.dt > e.tend && e.tstart < e.tend) e.dt = e.tend - e.t;
+    if (e.tend - e.t - e.dt < 1.e-14 * e.t) e.dt = e.tend - e.t;
+    e.dtdx = e.dt / e.dx;
+    e.dtdy = e.dt / e.dy;
+}
+
+// After one step of the loop (one thread): the reference's accept/reject
+// (solver.py:554-666): accept when cfl <= cfl_max (t += dt, or t = tstart +
+// (n + 1) dt with a fixed dt); a rejected step keeps t and is restored by
+// k_evolve_restore (a fixed dt ends the loop with cfl_error); the loop is
+// done when t >= tend, after max_steps attempts, or when the step produced a
+// non-finite value (fault, the step restored); otherwise the next dt.
+static __global__ void k_evolve_finalize(EvolveDev* e, const unsigned long long* cfl_bits, const int* status) {
+    if (threadIdx.x != 0 || blockIdx.x != 0 || e->done) return;
+    const double cfl = __longlong_as_double((long long)*cfl_bits);
+    const int n = e->attempts;
+    e->attempts = n + 1;
+    e->cfl = cfl;
+    const int st = *status & 3;
+    if (st) {
+        e->fault = st;
+        e->reject = 1;
+        e->done = 1;
+        return;
+    }
+    if (!(cfl > e->cfl_max)) {
+        e->cflmax = (e->cflmax > cfl) ? e->cflmax : cfl;  // max(cfl, cflmax)
+        e->t = e->dt_variable ? __dadd_rn(e->t, e->dt) : __dadd_rn(e->tstart, __dmul_rn((double)(n + 1), e->dt));
+        e->num_steps += 1;
+        e->reject = 0;
+    } else {
+        e->reject = 1;
+        if (!e->dt_variable) {
+            e->cflmax = (e->cflmax > cfl) ? e->cflmax : cfl;
+            e->cfl_error = 1;
+            e->done = 1;
+            return;
+        }
+    }
+    if (e->t >= e->tend || e->attempts >= e->max_steps) {
+        e->done = 1;
+        return;
+    }
+    evolve_get_dt(*e);
+}
+
+// A rejected step: the state it started from continues in the other buffer.
+static __global__ void k_evolve_restore(const EvolveDev* e, const double* __restrict__ from, double* __restrict__ to,
+                                        long long n) {
+    if (!e->reject) return;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+         k += (long long)gridDim.x * blockDim.x)
+        to[k] = from[k];
+}
+
+// One attempt of the loop from buffer c: ghost fill, step into buffer 1-c
+// with the loop's dt, finalize, restore on reject.
+int evolve_enqueue_attempt(claw2_patch* p, int c) {
+    double* qc = p->q[c];
+    launch_bc(qc, p->L, p->d.num_eqn, p->d.bc_lower, p->d.bc_upper, p->cfl, p->st);
+    StepArgs a = patch_args(p, 0.0);
+    a.qold = p->q[c];
+    a.qnew = p->q[c ^ 1];
+    a.evo = p->evo;
+    if (p->d.riemann == CLAW2_RP_EULER_EXACT && p->mlp && !p->d.dimensional_split) {
+        mlp_guess_launch(p->mlp, qc, p->L, p->rp.c[0], p->guess, p->st);
+        a.guess = p->guess;
+    }
+    int lpt_n = 0;
+    if (p->d.dimensional_split) {
+        StepArgs ax = a, ay = a;
+        ax.qnew = p->tmp;
+        ay.qold = p->tmp;
+        dispatch<SplitF>(p->d.riemann, ax, ay, p->st, 3);
+    } else {
+        int ns, H, nb;
+        unsplit_tiling(p->d.riemann, p->L.mx, p->L.my, ns, H, nb);
+        if (ns * nb > 2 * p->nsm && lpt_prepare(p, ns * nb, H) == CLAW2_OK) {
+            lpt_n = ns * nb;
+            a.H = H;
+            a.nstrips = ns;
+            a.tile_order = p->tile_order;
+            a.tile_cost = p->tile_cost;
+        }
+        dispatch<UnsplitF>(p->d.riemann, a, p->st, p->has_tmap ? &p->tmap[c] : nullptr);
+    }
+    if (lpt_n > 0 && (p->tile_steps++ % LPT_EVERY) == 0) launch_lpt(p->tile_cost, p->tile_order, lpt_n, p->st);
+    k_evolve_finalize<<<1, 32, 0, p->st>>>(p->evo, p->cfl, p->status);
+    const long long n = (long long)p->d.num_eqn * p->L.plane;
+    // grid-stride copy on a few blocks per SM: accepted attempts (almost all)
+    // leave it at once, so its launch stays short
+    const int rb = (int)std::max<long long>(1, std::min<long long>(grid_blocks(n), 4LL * p->nsm));
+    k_evolve_restore<<<rb, 256, 0, p->st>>>(p->evo, p->q[c], p->q[c ^ 1], n);
+    CUDA_TRY(cudaGetLastError());
+    return CLAW2_OK;
+}
+
 // Buffers of claw2_patch_run_host: a copy stream, two input and two output
 // staging buffers, their events and the per-step CFL words.
 int host_pipe_reserve(claw2_patch* p, int nsteps) {
@@ -1325,6 +1445,125 @@ int claw2_patch_step(claw2_patch* p, double dt, double* cfl) {
     const int rc = patch_enqueue_step(p, dt);
     if (rc) return rc;
     if (cfl) return claw2_patch_cfl(p, cfl);
+    return CLAW2_OK;
+}
+
+int claw2_patch_evolve(claw2_patch* p, claw2_evolve_state* s) {
+    if (!p || !s) return fail(CLAW2_EINVAL, "null pointer argument");
+    if (p->pending) return fail(CLAW2_EINVAL, "a step is pending: accept or reject it first");
+    if (p->ghosts_supplied)
+        return fail(CLAW2_EINVAL, "host-filled ghost cells (custom BCs) need the host at every step");
+    if (s->max_steps < 0) return fail(CLAW2_EINVAL, "max_steps must be >= 0");
+    if (!std::isfinite(s->t) || !std::isfinite(s->tend) || !std::isfinite(s->dt) || !(s->dt >= 0.0))
+        return fail(CLAW2_EINVAL, "t, tend and dt must be finite, dt >= 0");
+    s->num_steps = 0;
+    s->attempts = 0;
+    s->cfl_error = 0;
+    if (s->max_steps == 0) return CLAW2_OK;
+    DeviceGuard g(p->device);
+    if (!p->evo) {
+        if (cudaMalloc(&p->evo, sizeof(EvolveDev)) != cudaSuccess ||
+            cudaMallocHost(&p->h_evo, sizeof(EvolveDev)) != cudaSuccess) {
+            cudaGetLastError();
+            cudaFree(p->evo);
+            p->evo = nullptr;
+            return fail(CLAW2_ENOMEM, "time-loop state could not be allocated");
+        }
+    }
+    EvolveDev& e = *p->h_evo;
+    std::memset(&e, 0, sizeof e);
+    e.t = s->t;
+    e.tstart = s->tstart;
+    e.tend = s->tend;
+    e.dt = s->dt;
+    e.cfl = s->cfl;
+    e.cfl_desired = s->cfl_desired;
+    e.cfl_max = s->cfl_max;
+    e.dt_max = s->dt_max;
+    e.dtmin = s->dtmin;
+    e.dtmax = s->dtmax;
+    e.cflmax = s->cflmax;
+    e.dx = p->d.dx;
+    e.dy = p->d.dy;
+    e.dt_variable = s->dt_variable ? 1 : 0;
+    e.dt_old_set = s->dt_old_set ? 1 : 0;
+    e.max_steps = s->max_steps;
+    evolve_get_dt(e);  // the first attempt's dt
+    CUDA_TRY(cudaMemcpyAsync(p->evo, p->h_evo, sizeof(EvolveDev), cudaMemcpyHostToDevice, p->st));
+    CUDA_TRY(cudaMemsetAsync(p->status, 0, sizeof(int), p->st));
+    const int cur0 = p->cur;
+    long long issued = 0;
+    int chunk = 4;
+    // After the first chunk (issued directly: it also sets up launch attributes
+    // and schedule buffers) four attempts are captured as one CUDA graph and
+    // replayed: four attempts return to the same buffer parity, so the same
+    // graph serves every later chunk, and the host no longer pays one launch
+    // per kernel.  Any capture failure falls back to direct launches.
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    constexpr int GRAPH_ATTEMPTS = 4;
+    bool try_graph = true;
+    int rc = CLAW2_OK;
+    for (;;) {
+        if (issued > 0 && try_graph && !exec) {
+            try_graph = false;
+            const int c = (int)((cur0 + issued) & 1);
+            if (cudaStreamBeginCapture(p->st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+                int crc = CLAW2_OK;
+                for (int j = 0; j < GRAPH_ATTEMPTS && crc == CLAW2_OK; ++j) crc = evolve_enqueue_attempt(p, (c + j) & 1);
+                const cudaError_t ec = cudaStreamEndCapture(p->st, &graph);
+                if (crc != CLAW2_OK || ec != cudaSuccess || !graph ||
+                    cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+                    cudaGetLastError();
+                    if (graph) cudaGraphDestroy(graph);
+                    graph = nullptr;
+                    exec = nullptr;
+                }
+            } else {
+                cudaGetLastError();
+            }
+        }
+        if (exec) {
+            for (int j = 0; j < chunk; j += GRAPH_ATTEMPTS, issued += GRAPH_ATTEMPTS)
+                if (cudaGraphLaunch(exec, p->st) != cudaSuccess) {
+                    rc = fail(CLAW2_ECUDA, "graph launch of the time loop failed");
+                    break;
+                }
+        } else {
+            for (int j = 0; j < chunk && rc == CLAW2_OK; ++j, ++issued)
+                rc = evolve_enqueue_attempt(p, (int)((cur0 + issued) & 1));
+        }
+        if (rc == CLAW2_OK) {
+            if (cudaMemcpyAsync(p->h_evo, p->evo, sizeof(EvolveDev), cudaMemcpyDeviceToHost, p->st) != cudaSuccess ||
+                cudaStreamSynchronize(p->st) != cudaSuccess)
+                rc = fail(CLAW2_ECUDA, "reading the time loop's state failed");
+        }
+        if (rc != CLAW2_OK || e.done) break;
+        if (issued > (long long)s->max_steps + 128) {  // the loop marks itself done after max_steps attempts
+            rc = fail(CLAW2_ECUDA, "the device time loop did not finish");
+            break;
+        }
+        chunk = std::min(chunk * 2, 64);
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (rc != CLAW2_OK) return rc;
+    p->cur = (cur0 + e.attempts) & 1;
+    s->t = e.t;
+    s->dt = e.dt;
+    s->cfl = e.cfl;
+    s->dtmin = e.dtmin;
+    s->dtmax = e.dtmax;
+    s->cflmax = e.cflmax;
+    s->dt_old_set = e.dt_old_set;
+    s->num_steps = e.num_steps;
+    s->attempts = e.attempts;
+    s->cfl_error = e.cfl_error;
+    if (e.fault) {
+        cudaMemsetAsync(p->status, 0, sizeof(int), p->st);
+        if (e.fault & 2) return fail(CLAW2_ETIMEOUT, "a TMA row copy did not complete within the kernel's wait bound");
+        return fail(CLAW2_ENONFINITE, "the step produced a non-finite value");
+    }
     return CLAW2_OK;
 }
 

@@ -31,6 +31,14 @@
 
 namespace claw2 {
 
+// Device-resident time loop (claw2_patch_evolve): the loop's state lives in
+// device memory; each step reads its dt/dx, dt/dy from it and does nothing
+// once the loop is done.  Field meanings as in claw2_evolve_state.
+struct EvolveDev {
+    double t, tstart, tend, dt, dtdx, dtdy, cfl, cfl_desired, cfl_max, dt_max, dtmin, dtmax, cflmax, dx, dy;
+    int dt_variable, dt_old_set, max_steps, attempts, num_steps, cfl_error, done, reject, fault;
+};
+
 struct StepArgs {
     const double* __restrict__ qold;
     double* __restrict__ qnew;
@@ -51,6 +59,8 @@ struct StepArgs {
     int nstrips = 0;
     // aux planes (same layout as q) for solvers with aux data, else nullptr
     const double* __restrict__ aux = nullptr;
+    // device-resident time loop: dt from here, no work once it is done (else nullptr)
+    const EvolveDev* evo = nullptr;
     // capacity function kappa (one plane, same layout), else nullptr: every
     // increment of a cell is divided by its kappa, a transverse increment also
     // by the kappa of the cell its fluctuation entered (step2.f90:132-160,
@@ -281,7 +291,7 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
     const bool ycfl_col = (t >= 1) && (t <= W + 2) && (cp <= mx + 2);
     const int tl = (t > 0) ? t - 1 : 0;
     const int tr = (t < NT - 1) ? t + 1 : NT - 1;
-    const double dtdx = a.dtdx, dtdy = a.dtdy;
+    const double dtdx = a.evo ? a.evo->dtdx : a.dtdx, dtdy = a.evo ? a.evo->dtdy : a.dtdy;
     const RPParams& P = a.rp;
     const int order = (SPEC == SPEC_MC2) ? 2 : a.meth.order;
     const int trans = (SPEC == SPEC_MC2) ? 2 : a.meth.transverse;
@@ -711,7 +721,7 @@ __device__ __forceinline__ void unsplit_tile2(const StepArgs& a, int strip, int 
     const bool ycfl_col = (t >= 1) && (t <= W + 2) && (cp <= mx + 2);
     const int tl = (t > 0) ? t - 1 : 0;
     const int tr = (t < NT - 1) ? t + 1 : NT - 1;
-    const double dtdx = a.dtdx, dtdy = a.dtdy;
+    const double dtdx = a.evo ? a.evo->dtdx : a.dtdx, dtdy = a.evo ? a.evo->dtdy : a.dtdy;
     const RPParams& P = a.rp;
     const int order = (SPEC == SPEC_MC2) ? 2 : a.meth.order;
     const int trans = (SPEC == SPEC_MC2) ? 2 : a.meth.transverse;
@@ -1040,6 +1050,7 @@ __device__ __forceinline__ void unsplit_tile2(const StepArgs& a, int strip, int 
 
 template <class RP, int NT, int MINB, int SPEC, bool CAPA = false>
 __global__ void __launch_bounds__(NT, MINB) k_step_unsplit2(const StepArgs a) {
+    if (a.evo && a.evo->done) return;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     UnsplitSmem2<RP, NT, CAPA>& S = *reinterpret_cast<UnsplitSmem2<RP, NT, CAPA>*>(smem_raw);
     int tile = blockIdx.x;
@@ -1061,6 +1072,7 @@ __global__ void __launch_bounds__(NT, MINB) k_step_unsplit2(const StepArgs a) {
 // The same kernel with its rows staged by TMA from the tensor map of qold.
 template <class RP, int NT, int MINB, int SPEC>
 __global__ void __launch_bounds__(NT, MINB) k_step_unsplit_tma(const StepArgs a, const __grid_constant__ CUtensorMap tm) {
+    if (a.evo && a.evo->done) return;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     UnsplitSmemTma<RP, NT>& S = *reinterpret_cast<UnsplitSmemTma<RP, NT>*>(smem_raw);
     int tile = blockIdx.x;
@@ -1083,6 +1095,7 @@ __global__ void __launch_bounds__(NT, MINB) k_step_unsplit_tma(const StepArgs a,
 // block t / nstrips); CTA b runs tile_order[b] when a schedule is given.
 template <class RP, int NT, int MINB, int SPEC, bool CAPA = false>
 __global__ void __launch_bounds__(NT, MINB) k_step_unsplit(const StepArgs a) {
+    if (a.evo && a.evo->done) return;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     UnsplitSmem<RP, NT, CAPA>& S = *reinterpret_cast<UnsplitSmem<RP, NT, CAPA>*>(smem_raw);
     int tile = blockIdx.x;
@@ -1160,6 +1173,7 @@ struct SplitXSmem {
 
 template <class RP, int NT, int SPEC = SPEC_ANY>
 __global__ void __launch_bounds__(NT) k_split_x(const StepArgs a) {
+    if (a.evo && a.evo->done) return;
     constexpr int ME = RP::MEQN, MW = RP::MWAVES, NC = RP::NC, W = NT - 4;
     constexpr int MAD = AuxTraits<RP>::MAUX > 0 ? AuxTraits<RP>::MAUX : 1;
     using Iface = typename RP::Iface;
@@ -1179,7 +1193,7 @@ __global__ void __launch_bounds__(NT) k_split_x(const StepArgs a) {
     const bool xcfl_col = (t >= 2) && (t <= W + 2) && (cp <= mx + 2);
     const int tl = (t > 0) ? t - 1 : 0;
     const int tr = (t < NT - 1) ? t + 1 : NT - 1;
-    const double dtdx = a.dtdx;
+    const double dtdx = a.evo ? a.evo->dtdx : a.dtdx;
     const RPParams& P = a.rp;
     const double* qo = a.qold + cpl;
     double* qn = a.qnew + cpl;
@@ -1268,6 +1282,7 @@ __global__ void __launch_bounds__(NT) k_split_x(const StepArgs a) {
 // ---------------------------------------------------------------------------
 template <class RP, int NT, int SPEC = SPEC_ANY>
 __global__ void __launch_bounds__(NT) k_split_y(const StepArgs a) {
+    if (a.evo && a.evo->done) return;
     constexpr int ME = RP::MEQN, MW = RP::MWAVES, NC = RP::NC;
     constexpr int MAD = AuxTraits<RP>::MAUX > 0 ? AuxTraits<RP>::MAUX : 1;
     using Iface = typename RP::Iface;
@@ -1282,7 +1297,7 @@ __global__ void __launch_bounds__(NT) k_split_y(const StepArgs a) {
     const int rb = blockIdx.y * a.H;
     const int Hb = min(a.H, my - rb);
     const int R0 = rb, R1 = rb + Hb + 3;
-    const double dtdy = a.dtdy;
+    const double dtdy = a.evo ? a.evo->dtdy : a.dtdy;
     const RPParams& P = a.rp;
     const double* qo = a.qold + cpl;
     double* qn = a.qnew + cpl;

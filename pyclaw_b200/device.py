@@ -140,6 +140,15 @@ class DevicePatch(object):
         self.host_dirty = False
         return cfl
 
+    def evolve(self, es):
+        """Run the device-resident time loop on ``es`` (a Claw2EvolveState,
+        updated in place; claw2_patch_evolve).  The status code comes back
+        unchecked so the caller can restore its own state first."""
+        rc = self._lib.claw2_patch_evolve(self.h, ctypes.byref(es))
+        if es.attempts > 0:
+            self.device_newer = True
+        return rc
+
     def accept(self, accept):
         _lib.check(self._lib.claw2_patch_accept(self.h, 1 if accept else 0))
         if accept:
