@@ -192,9 +192,9 @@ bool is_mc2(const Method& m, int mwaves) {
 }
 
 // tm: the tensor map of qold for the TMA-staged kernel, or nullptr
-template <class RP, int MB, int SPEC>
+template <class RP, int MB, int SPEC, bool EVO>
 void launch_unsplit_s(const StepArgs& b, dim3 grid, cudaStream_t st, const CUtensorMap* tm) {
-    if (tm) {
+    if (!EVO && tm) {
         constexpr int smem = (int)sizeof(UnsplitSmemTma<RP, NT_UNSPLIT>);
         static unsigned long long attr = 0;
         smem_attr(k_step_unsplit_tma<RP, NT_UNSPLIT, MB, SPEC>, smem, attr);
@@ -203,8 +203,8 @@ void launch_unsplit_s(const StepArgs& b, dim3 grid, cudaStream_t st, const CUten
     }
     constexpr int smem = (int)sizeof(UnsplitSmem<RP, NT_UNSPLIT>);
     static unsigned long long attr = 0;
-    smem_attr(k_step_unsplit<RP, NT_UNSPLIT, MB, SPEC>, smem, attr);
-    k_step_unsplit<RP, NT_UNSPLIT, MB, SPEC><<<grid, NT_UNSPLIT, smem, st>>>(b);
+    smem_attr(k_step_unsplit<RP, NT_UNSPLIT, MB, SPEC, false, EVO>, smem, attr);
+    k_step_unsplit<RP, NT_UNSPLIT, MB, SPEC, false, EVO><<<grid, NT_UNSPLIT, smem, st>>>(b);
 }
 
 // Tiling of the unsplit kernel: strips of NT_UNSPLIT - 4 output columns,
@@ -218,24 +218,26 @@ void unsplit_tiling(int riemann, int mx, int my, int& nstrips, int& H, int& nblo
 }
 
 // The two-barrier tile (deferred x finish), any method, with or without capacity.
-template <class RP, int SPEC, bool CAPA>
+template <class RP, int SPEC, bool CAPA, bool EVO>
 void launch_unsplit2_s(const StepArgs& b, dim3 grid, cudaStream_t st) {
     constexpr int smem = (int)sizeof(UnsplitSmem2<RP, NT_UNSPLIT, CAPA>);
     static unsigned long long attr = 0;
-    smem_attr(k_step_unsplit2<RP, NT_UNSPLIT, 2, SPEC, CAPA>, smem, attr);
-    k_step_unsplit2<RP, NT_UNSPLIT, 2, SPEC, CAPA><<<grid, NT_UNSPLIT, smem, st>>>(b);
+    smem_attr(k_step_unsplit2<RP, NT_UNSPLIT, 2, SPEC, CAPA, EVO>, smem, attr);
+    k_step_unsplit2<RP, NT_UNSPLIT, 2, SPEC, CAPA, EVO><<<grid, NT_UNSPLIT, smem, st>>>(b);
 }
 
 // The capacity form (any method, rows loaded directly).
-template <class RP>
+template <class RP, bool EVO>
 void launch_unsplit_capa(const StepArgs& b, dim3 grid, cudaStream_t st) {
     constexpr int smem = (int)sizeof(UnsplitSmem<RP, NT_UNSPLIT, true>);
     static unsigned long long attr = 0;
-    smem_attr(k_step_unsplit<RP, NT_UNSPLIT, 2, SPEC_ANY, true>, smem, attr);
-    k_step_unsplit<RP, NT_UNSPLIT, 2, SPEC_ANY, true><<<grid, NT_UNSPLIT, smem, st>>>(b);
+    smem_attr(k_step_unsplit<RP, NT_UNSPLIT, 2, SPEC_ANY, true, EVO>, smem, attr);
+    k_step_unsplit<RP, NT_UNSPLIT, 2, SPEC_ANY, true, EVO><<<grid, NT_UNSPLIT, smem, st>>>(b);
 }
 
-template <class RP, int MB>
+// EVO: a launch of the device time loop (dt read from a.evo; rows loaded
+// directly, never by TMA).
+template <class RP, int MB, bool EVO>
 void launch_unsplit_v(const StepArgs& a, cudaStream_t st, const CUtensorMap* tm) {
     StepArgs b = a;
     int ns, H, nb;
@@ -247,14 +249,14 @@ void launch_unsplit_v(const StepArgs& a, cudaStream_t st, const CUtensorMap* tm)
     const int nbk = (a.L.my + b.H - 1) / b.H;
     dim3 grid(b.nstrips * nbk);
     if (g_tune[RP::ID & (TUNE_SLOTS - 1)].variant & 4) {  // the two-barrier tile
-        if (a.capa) launch_unsplit2_s<RP, SPEC_ANY, true>(b, grid, st);
-        else if (is_mc2(a.meth, RP::MWAVES)) launch_unsplit2_s<RP, SPEC_MC2, false>(b, grid, st);
-        else launch_unsplit2_s<RP, SPEC_ANY, false>(b, grid, st);
+        if (a.capa) launch_unsplit2_s<RP, SPEC_ANY, true, EVO>(b, grid, st);
+        else if (is_mc2(a.meth, RP::MWAVES)) launch_unsplit2_s<RP, SPEC_MC2, false, EVO>(b, grid, st);
+        else launch_unsplit2_s<RP, SPEC_ANY, false, EVO>(b, grid, st);
         return;
     }
-    if (a.capa) launch_unsplit_capa<RP>(b, grid, st);
-    else if (is_mc2(a.meth, RP::MWAVES)) launch_unsplit_s<RP, MB, SPEC_MC2>(b, grid, st, tm);
-    else launch_unsplit_s<RP, MB, SPEC_ANY>(b, grid, st, tm);
+    if (a.capa) launch_unsplit_capa<RP, EVO>(b, grid, st);
+    else if (is_mc2(a.meth, RP::MWAVES)) launch_unsplit_s<RP, MB, SPEC_MC2, EVO>(b, grid, st, tm);
+    else launch_unsplit_s<RP, MB, SPEC_ANY, EVO>(b, grid, st, tm);
 }
 
 // Variants: 4 = the two-barrier tile (k_step_unsplit2); otherwise bit 0 = 3
@@ -263,9 +265,14 @@ void launch_unsplit_v(const StepArgs& a, cudaStream_t st, const CUtensorMap* tm)
 template <class RP>
 void launch_unsplit(const StepArgs& a, cudaStream_t st, const CUtensorMap* tm) {
     const UnsplitShape sh = g_tune[RP::ID & (TUNE_SLOTS - 1)];
+    if (a.evo) {
+        if (sh.variant & 1) launch_unsplit_v<RP, 3, true>(a, st, nullptr);
+        else launch_unsplit_v<RP, 2, true>(a, st, nullptr);
+        return;
+    }
     const CUtensorMap* use = (sh.variant & 2) ? tm : nullptr;
-    if (sh.variant & 1) launch_unsplit_v<RP, 3>(a, st, use);
-    else launch_unsplit_v<RP, 2>(a, st, use);
+    if (sh.variant & 1) launch_unsplit_v<RP, 3, false>(a, st, use);
+    else launch_unsplit_v<RP, 2, false>(a, st, use);
 }
 
 // the split sweeps' specialisation: order 2 with one limiter on every family
@@ -276,7 +283,7 @@ int split_spec(const Method& m, int mwaves) {
     return m.mthlim[0] == 4 ? SPEC_MC2 : m.mthlim[0] == 1 ? SPEC_MM2 : SPEC_ANY;
 }
 
-template <class RP, int SPEC>
+template <class RP, int SPEC, bool EVO>
 void launch_split_s(const StepArgs& ax, const StepArgs& ay, cudaStream_t st, int which) {
     if (which & 1) {
         constexpr int W = NT_SPLIT_X - 4;
@@ -286,25 +293,32 @@ void launch_split_s(const StepArgs& ax, const StepArgs& ay, cudaStream_t st, int
         dim3 grid(ns, (ax.L.my + 4 + b.H - 1) / b.H);
         constexpr int smem = (int)sizeof(SplitXSmem<RP, NT_SPLIT_X>);
         static unsigned long long attr = 0;
-        smem_attr(k_split_x<RP, NT_SPLIT_X, SPEC>, smem, attr);
-        k_split_x<RP, NT_SPLIT_X, SPEC><<<grid, NT_SPLIT_X, smem, st>>>(b);
+        smem_attr(k_split_x<RP, NT_SPLIT_X, SPEC, EVO>, smem, attr);
+        k_split_x<RP, NT_SPLIT_X, SPEC, EVO><<<grid, NT_SPLIT_X, smem, st>>>(b);
     }
     if (which & 2) {
         const int ns = (ay.L.mx + 4 + NT_SPLIT_Y - 1) / NT_SPLIT_Y;
         StepArgs b = ay;
         b.H = pick_rows(ns, ay.L.my);
         dim3 grid(ns, (ay.L.my + b.H - 1) / b.H);
-        k_split_y<RP, NT_SPLIT_Y, SPEC><<<grid, NT_SPLIT_Y, 0, st>>>(b);
+        k_split_y<RP, NT_SPLIT_Y, SPEC, EVO><<<grid, NT_SPLIT_Y, 0, st>>>(b);
     }
 }
 
+template <class RP, bool EVO>
+void launch_split_e(const StepArgs& ax, const StepArgs& ay, cudaStream_t st, int which) {
+    switch (split_spec(ax.meth, RP::MWAVES)) {
+        case SPEC_MC2: launch_split_s<RP, SPEC_MC2, EVO>(ax, ay, st, which); break;
+        case SPEC_MM2: launch_split_s<RP, SPEC_MM2, EVO>(ax, ay, st, which); break;
+        default: launch_split_s<RP, SPEC_ANY, EVO>(ax, ay, st, which); break;
+    }
+}
+
+// (a.evo: the device time loop's launch, dt read from its record)
 template <class RP>
 void launch_split(const StepArgs& ax, const StepArgs& ay, cudaStream_t st, int which) {
-    switch (split_spec(ax.meth, RP::MWAVES)) {
-        case SPEC_MC2: launch_split_s<RP, SPEC_MC2>(ax, ay, st, which); break;
-        case SPEC_MM2: launch_split_s<RP, SPEC_MM2>(ax, ay, st, which); break;
-        default: launch_split_s<RP, SPEC_ANY>(ax, ay, st, which); break;
-    }
+    if (ax.evo) launch_split_e<RP, true>(ax, ay, st, which);
+    else launch_split_e<RP, false>(ax, ay, st, which);
 }
 
 template <template <class> class F, class... A>

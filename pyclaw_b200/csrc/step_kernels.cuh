@@ -271,7 +271,7 @@ struct UnsplitSmemTma {
 // term of a cell carries that one factor); transverse increments carry in
 // addition the 1/kappa of the cell their fluctuation entered, the
 // second-order correction the mean of the two cells' dt/(dx kappa).
-template <class RP, int NT, int SPEC = SPEC_ANY, bool CAPA = false>
+template <class RP, int NT, int SPEC = SPEC_ANY, bool CAPA = false, bool EVO = false>
 __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int rb, UnsplitSmem<RP, NT, CAPA>& S,
                                              double& cfl, const CUtensorMap* tm = nullptr, double* qrow = nullptr,
                                              unsigned long long* bar = nullptr) {
@@ -291,7 +291,10 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
     const bool ycfl_col = (t >= 1) && (t <= W + 2) && (cp <= mx + 2);
     const int tl = (t > 0) ? t - 1 : 0;
     const int tr = (t < NT - 1) ? t + 1 : NT - 1;
-    const double dtdx = a.evo ? a.evo->dtdx : a.dtdx, dtdy = a.evo ? a.evo->dtdy : a.dtdy;
+    // dt/dx, dt/dy: kernel parameters, or (EVO, the device time loop) the
+    // loop's record; a compile-time choice, so ordinary steps keep the
+    // parameters as operands of the FP64 instructions instead of registers
+    const double dtdx = EVO ? a.evo->dtdx : a.dtdx, dtdy = EVO ? a.evo->dtdy : a.dtdy;
     const RPParams& P = a.rp;
     const int order = (SPEC == SPEC_MC2) ? 2 : a.meth.order;
     const int trans = (SPEC == SPEC_MC2) ? 2 : a.meth.transverse;
@@ -700,7 +703,7 @@ struct UnsplitSmem2 {
     double red[NT / 32];
 };
 
-template <class RP, int NT, int SPEC = SPEC_ANY, bool CAPA = false>
+template <class RP, int NT, int SPEC = SPEC_ANY, bool CAPA = false, bool EVO = false>
 __device__ __forceinline__ void unsplit_tile2(const StepArgs& a, int strip, int rb, UnsplitSmem2<RP, NT, CAPA>& S,
                                               double& cfl) {
     constexpr int ME = RP::MEQN, MW = RP::MWAVES, NC = RP::NC, W = NT - 4;
@@ -721,7 +724,10 @@ __device__ __forceinline__ void unsplit_tile2(const StepArgs& a, int strip, int 
     const bool ycfl_col = (t >= 1) && (t <= W + 2) && (cp <= mx + 2);
     const int tl = (t > 0) ? t - 1 : 0;
     const int tr = (t < NT - 1) ? t + 1 : NT - 1;
-    const double dtdx = a.evo ? a.evo->dtdx : a.dtdx, dtdy = a.evo ? a.evo->dtdy : a.dtdy;
+    // dt/dx, dt/dy: kernel parameters, or (EVO, the device time loop) the
+    // loop's record; a compile-time choice, so ordinary steps keep the
+    // parameters as operands of the FP64 instructions instead of registers
+    const double dtdx = EVO ? a.evo->dtdx : a.dtdx, dtdy = EVO ? a.evo->dtdy : a.dtdy;
     const RPParams& P = a.rp;
     const int order = (SPEC == SPEC_MC2) ? 2 : a.meth.order;
     const int trans = (SPEC == SPEC_MC2) ? 2 : a.meth.transverse;
@@ -1048,9 +1054,9 @@ __device__ __forceinline__ void unsplit_tile2(const StepArgs& a, int strip, int 
     if (GuessTraits<RP>::USES && a.counters) counter_commit(a.counters, n_it, n_solve);
 }
 
-template <class RP, int NT, int MINB, int SPEC, bool CAPA = false>
+template <class RP, int NT, int MINB, int SPEC, bool CAPA = false, bool EVO = false>
 __global__ void __launch_bounds__(NT, MINB) k_step_unsplit2(const StepArgs a) {
-    if (a.evo && a.evo->done) return;
+    if (EVO && a.evo->done) return;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     UnsplitSmem2<RP, NT, CAPA>& S = *reinterpret_cast<UnsplitSmem2<RP, NT, CAPA>*>(smem_raw);
     int tile = blockIdx.x;
@@ -1061,7 +1067,7 @@ __global__ void __launch_bounds__(NT, MINB) k_step_unsplit2(const StepArgs a) {
     long long t0 = 0;
     if (a.tile_cost && threadIdx.x == 0) t0 = clock64();
     double cfl = 0.0;
-    unsplit_tile2<RP, NT, SPEC, CAPA>(a, tile % a.nstrips, (tile / a.nstrips) * a.H, S, cfl);
+    unsplit_tile2<RP, NT, SPEC, CAPA, EVO>(a, tile % a.nstrips, (tile / a.nstrips) * a.H, S, cfl);
     cfl_commit(cfl, S.red, a.cfl_bits);
     if (a.tile_cost && threadIdx.x == 0) {
         const long long c = clock64() - t0;
@@ -1072,7 +1078,6 @@ __global__ void __launch_bounds__(NT, MINB) k_step_unsplit2(const StepArgs a) {
 // The same kernel with its rows staged by TMA from the tensor map of qold.
 template <class RP, int NT, int MINB, int SPEC>
 __global__ void __launch_bounds__(NT, MINB) k_step_unsplit_tma(const StepArgs a, const __grid_constant__ CUtensorMap tm) {
-    if (a.evo && a.evo->done) return;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     UnsplitSmemTma<RP, NT>& S = *reinterpret_cast<UnsplitSmemTma<RP, NT>*>(smem_raw);
     int tile = blockIdx.x;
@@ -1093,9 +1098,11 @@ __global__ void __launch_bounds__(NT, MINB) k_step_unsplit_tma(const StepArgs a,
 
 // Grid: 1D over the tiles (strip fastest).  Tile t = (strip t % nstrips, row
 // block t / nstrips); CTA b runs tile_order[b] when a schedule is given.
-template <class RP, int NT, int MINB, int SPEC, bool CAPA = false>
+// EVO: launched by the device time loop (dt from a.evo, nothing to do once
+// the loop is done).
+template <class RP, int NT, int MINB, int SPEC, bool CAPA = false, bool EVO = false>
 __global__ void __launch_bounds__(NT, MINB) k_step_unsplit(const StepArgs a) {
-    if (a.evo && a.evo->done) return;
+    if (EVO && a.evo->done) return;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     UnsplitSmem<RP, NT, CAPA>& S = *reinterpret_cast<UnsplitSmem<RP, NT, CAPA>*>(smem_raw);
     int tile = blockIdx.x;
@@ -1106,7 +1113,7 @@ __global__ void __launch_bounds__(NT, MINB) k_step_unsplit(const StepArgs a) {
     long long t0 = 0;
     if (a.tile_cost && threadIdx.x == 0) t0 = clock64();
     double cfl = 0.0;
-    unsplit_tile<RP, NT, SPEC, CAPA>(a, tile % a.nstrips, (tile / a.nstrips) * a.H, S, cfl);
+    unsplit_tile<RP, NT, SPEC, CAPA, EVO>(a, tile % a.nstrips, (tile / a.nstrips) * a.H, S, cfl);
     cfl_commit(cfl, S.red, a.cfl_bits);
     if (a.tile_cost && threadIdx.x == 0) {
         const long long c = clock64() - t0;
@@ -1171,9 +1178,9 @@ struct SplitXSmem {
     double red[NT / 32];
 };
 
-template <class RP, int NT, int SPEC = SPEC_ANY>
+template <class RP, int NT, int SPEC = SPEC_ANY, bool EVO = false>
 __global__ void __launch_bounds__(NT) k_split_x(const StepArgs a) {
-    if (a.evo && a.evo->done) return;
+    if (EVO && a.evo->done) return;
     constexpr int ME = RP::MEQN, MW = RP::MWAVES, NC = RP::NC, W = NT - 4;
     constexpr int MAD = AuxTraits<RP>::MAUX > 0 ? AuxTraits<RP>::MAUX : 1;
     using Iface = typename RP::Iface;
@@ -1193,7 +1200,7 @@ __global__ void __launch_bounds__(NT) k_split_x(const StepArgs a) {
     const bool xcfl_col = (t >= 2) && (t <= W + 2) && (cp <= mx + 2);
     const int tl = (t > 0) ? t - 1 : 0;
     const int tr = (t < NT - 1) ? t + 1 : NT - 1;
-    const double dtdx = a.evo ? a.evo->dtdx : a.dtdx;
+    const double dtdx = EVO ? a.evo->dtdx : a.dtdx;  // (compile-time choice, as in unsplit_tile)
     const RPParams& P = a.rp;
     const double* qo = a.qold + cpl;
     double* qn = a.qnew + cpl;
@@ -1280,9 +1287,9 @@ __global__ void __launch_bounds__(NT) k_split_x(const StepArgs a) {
 // per column marching down the rows; limiter neighbours come from the
 // register pipeline.  Writes the interior cells of qnew.
 // ---------------------------------------------------------------------------
-template <class RP, int NT, int SPEC = SPEC_ANY>
+template <class RP, int NT, int SPEC = SPEC_ANY, bool EVO = false>
 __global__ void __launch_bounds__(NT) k_split_y(const StepArgs a) {
-    if (a.evo && a.evo->done) return;
+    if (EVO && a.evo->done) return;
     constexpr int ME = RP::MEQN, MW = RP::MWAVES, NC = RP::NC;
     constexpr int MAD = AuxTraits<RP>::MAUX > 0 ? AuxTraits<RP>::MAUX : 1;
     using Iface = typename RP::Iface;
@@ -1297,7 +1304,7 @@ __global__ void __launch_bounds__(NT) k_split_y(const StepArgs a) {
     const int rb = blockIdx.y * a.H;
     const int Hb = min(a.H, my - rb);
     const int R0 = rb, R1 = rb + Hb + 3;
-    const double dtdy = a.evo ? a.evo->dtdy : a.dtdy;
+    const double dtdy = EVO ? a.evo->dtdy : a.dtdy;
     const RPParams& P = a.rp;
     const double* qo = a.qold + cpl;
     double* qn = a.qnew + cpl;
