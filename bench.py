@@ -199,6 +199,38 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # GPU leg
 # ---------------------------------------------------------------------------
+def copy_bound(nbytes, reps):
+    """Wall-clock rate of the copies alone: reps times, nbytes from pinned host
+    memory to the device on one stream while nbytes go the other way on a
+    second one (both PCIe directions at once, as in the e2e pipeline).
+    Returns (seconds per pair, H2D GB/s alone, D2H GB/s alone)."""
+    import torch
+    n = nbytes // 8
+    hi = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    hi.fill_(1.0)
+    ho = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    d1 = torch.empty(n, dtype=torch.float64, device="cuda")
+    d2 = torch.zeros(n, dtype=torch.float64, device="cuda")
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def run(h2d, d2h):
+        for k in range(reps + 2):  # two untimed rounds first
+            if k == 2:
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+            if h2d:
+                with torch.cuda.stream(s1):
+                    d1.copy_(hi, non_blocking=True)
+            if d2h:
+                with torch.cuda.stream(s2):
+                    ho.copy_(d2, non_blocking=True)
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) / reps
+
+    up, down, both = run(True, False), run(False, True), run(True, True)
+    return both, nbytes / up / 1e9, nbytes / down / 1e9
+
+
 def time_patch(patch, dt, steps, flush, stream):
     """Mean step and step-kernel times (ms) of a device patch, L2 flushed
     between steps; the state advances (every step accepted)."""
@@ -517,6 +549,7 @@ def run_ours(args):
         patch.run_host(qin, qout, [dt] * K)
         el = time.perf_counter() - t0
         e2e_val, seq_val = cells * K / el, cells * K / el_seq
+        pair_s, up_gbs, down_gbs = copy_bound(qh.nbytes, K)
         if world > 1:
             t = torch.tensor([el, el_seq], device=dev, dtype=torch.float64)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -526,6 +559,11 @@ def run_ours(args):
                "path": "claw2_patch_run_host: per step, pinned host state -> device, ghost fill + step + CFL, "
                        "result -> pinned host; uploads and downloads on their own streams overlap the "
                        "compute of the neighbouring steps; wall clock",
+               "copy_bound": {"value": cells / pair_s, "unit": UNIT, "frac": e2e_val / world / (cells / pair_s),
+                              "h2d_gbs": up_gbs, "d2h_gbs": down_gbs,
+                              "both_gbs_each": qh.nbytes / pair_s / 1e9,
+                              "what": "the step's upload and download alone (pinned, both directions at once, "
+                                      "no compute): the rate e2e cannot exceed on this host link"},
                "one_call_per_step": {"value": seq_val, "unit": UNIT,
                                      "path": "claw2_patch_upload_q + claw2_patch_step (returns CFL) + "
                                              "claw2_patch_accept + claw2_patch_download_q"}}

@@ -268,6 +268,12 @@ int claw2_probe_fp64(int device, double* tflops);
  * between it and CUDA's IEEE quotient 1.0/a. */
 int claw2_selftest_rcp(int device, int n, unsigned long long seed, double* max_ulp);
 
+/* Self-test of the longest-first tile schedule's sort: n (1..8192) seeded
+ * tile costs with many ties, sorted on the device; *mismatches = positions
+ * where the order differs from a stable descending sort on the host (cost
+ * descending, ties by lower tile first). */
+int claw2_selftest_lpt(int device, int n, unsigned long long seed, int* mismatches);
+
 /* ---- no counterpart in the reference ------------------------------------
  * The split step (x-sweep then y-sweep, as claw2_step2ds with ids = 1 then 2)
  * for callers that cannot allocate device memory: frameworks that reserve the

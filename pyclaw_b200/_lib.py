@@ -111,6 +111,8 @@ _SIGNATURES = {
     "claw2_patch_kernel_ms": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]),
     "claw2_probe_fp64": (ctypes.c_int, [ctypes.c_int, _c_double_p]),
     "claw2_selftest_rcp": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_ulonglong, _c_double_p]),
+    "claw2_selftest_lpt": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_ulonglong,
+                                          ctypes.POINTER(ctypes.c_int)]),
     "claw2_tune_set": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "claw2_tune_get": (ctypes.c_int, [ctypes.c_int, _c_int_p, _c_int_p]),
     "claw2_step2ds_noalloc": (ctypes.c_int, [ctypes.POINTER(Claw2Desc), ctypes.c_void_p, ctypes.c_void_p,

@@ -879,7 +879,9 @@ void launch_lpt(const unsigned int* cost, int* order, int n, cudaStream_t st) {
     while (N < n) N <<= 1;
     static unsigned long long attr = 0;
     smem_attr(k_lpt_order, (int)sizeof(unsigned long long) * LPT_MAX_TILES, attr);
-    k_lpt_order<<<1, 1024, sizeof(unsigned long long) * N, st>>>(cost, order, n);
+    // (the sort of up to 1024 keys double-buffers its shared-memory stages)
+    const size_t smem = sizeof(unsigned long long) * (N >= 32 && N <= 1024 ? 2 * N : N);
+    k_lpt_order<<<1, 1024, smem, st>>>(cost, order, n);
 }
 
 StepArgs patch_args(claw2_patch* p, double dt) {
@@ -1759,6 +1761,42 @@ int claw2_selftest_rcp(int device, int n, unsigned long long seed, double* max_u
     cudaFree(worst);
     if (e != cudaSuccess) return fail(CLAW2_ECUDA, "reciprocal self-test failed: %s", cudaGetErrorString(e));
     *max_ulp = (double)h;
+    return CLAW2_OK;
+}
+
+int claw2_selftest_lpt(int device, int n, unsigned long long seed, int* mismatches) {
+    if (!mismatches) return fail(CLAW2_EINVAL, "null pointer argument");
+    if (n < 1 || n > LPT_MAX_TILES) return fail(CLAW2_EINVAL, "n must be 1..%d (got %d)", LPT_MAX_TILES, n);
+    DeviceGuard g(device);
+    // costs with many ties (a few dozen distinct values) from a 64-bit LCG
+    std::vector<unsigned int> cost(n);
+    unsigned long long z = seed * 2862933555777941757ull + 3037000493ull;
+    for (int i = 0; i < n; ++i) {
+        z = z * 6364136223846793005ull + 1442695040888963407ull;
+        cost[i] = (unsigned int)((z >> 33) % 37u) * 100000u + (unsigned int)((z >> 20) & 1u);
+    }
+    std::vector<int> want(n), got(n);
+    for (int i = 0; i < n; ++i) want[i] = i;
+    std::stable_sort(want.begin(), want.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    unsigned int* dc = nullptr;
+    int* dord = nullptr;
+    if (cudaMalloc(&dc, sizeof(unsigned int) * n) != cudaSuccess || cudaMalloc(&dord, sizeof(int) * n) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(dc);
+        return fail(CLAW2_ENOMEM, "self-test buffers");
+    }
+    cudaError_t e = cudaMemcpy(dc, cost.data(), sizeof(unsigned int) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        launch_lpt(dc, dord, n, 0);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(got.data(), dord, sizeof(int) * n, cudaMemcpyDeviceToHost);
+    cudaFree(dc);
+    cudaFree(dord);
+    if (e != cudaSuccess) return fail(CLAW2_ECUDA, "schedule sort self-test failed: %s", cudaGetErrorString(e));
+    int bad = 0;
+    for (int i = 0; i < n; ++i) bad += got[i] != want[i];
+    *mismatches = bad;
     return CLAW2_OK;
 }
 

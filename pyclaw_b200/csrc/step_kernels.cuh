@@ -1130,10 +1130,38 @@ __global__ void __launch_bounds__(NT, MINB) k_step_unsplit(const StepArgs a) {
 // tail, which evens out the SMs' finishing times.  The order changes only
 // which SM runs a tile: every result is independent of it.
 constexpr int LPT_MAX_TILES = 8192;
+// Up to 1024 tiles (one key per thread): the stages whose partner is in the
+// same warp (j < 32, 40 of the 55 stages at 1024) exchange keys by shuffles,
+// the others through two alternating shared-memory buffers, one barrier each.
 static __global__ void __launch_bounds__(1024) k_lpt_order(const unsigned int* cost, int* order, int n) {
     extern __shared__ unsigned long long keys[];
     int N = 1;
     while (N < n) N <<= 1;
+    if (N >= 32 && N <= (int)blockDim.x) {
+        const int i = threadIdx.x;
+        unsigned long long x = 0ull;
+        if (i < n) x = ((unsigned long long)cost[i] << 32) | (unsigned long long)(0xffffffffu - (unsigned)i);
+        int pb = 0;
+        for (int k = 2; k <= N; k <<= 1) {
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                unsigned long long y;
+                if (j >= 32) {
+                    if (i < N) keys[pb * N + i] = x;
+                    __syncthreads();
+                    y = (i < N) ? keys[pb * N + (i ^ j)] : 0ull;
+                    pb ^= 1;
+                } else {
+                    y = __shfl_xor_sync(0xffffffffu, x, j);
+                }
+                // descending blocks ((i & k) == 0) keep the larger key at the
+                // lower index of the pair, ascending blocks the smaller
+                const bool keep_max = ((i & j) == 0) == ((i & k) == 0);
+                x = keep_max ? (x > y ? x : y) : (x > y ? y : x);
+            }
+        }
+        if (i < n) order[i] = (int)(0xffffffffu - (unsigned)(x & 0xffffffffull));
+        return;
+    }
     for (int i = threadIdx.x; i < N; i += blockDim.x)
         keys[i] = (i < n) ? (((unsigned long long)cost[i] << 32) | (unsigned long long)(0xffffffffu - (unsigned)i))
                           : 0ull;

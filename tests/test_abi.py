@@ -54,3 +54,8 @@ def test_bad_arguments_rejected_without_gpu(lib):
     assert b"null" in L.claw2_last_error()
     rc = L.claw2_selftest_rcp(0, 100, 1, None)
     assert rc == _lib.EINVAL
+    import ctypes
+    bad = ctypes.c_int(-1)
+    assert L.claw2_selftest_lpt(0, 10, 1, None) == _lib.EINVAL
+    assert L.claw2_selftest_lpt(0, 0, 1, ctypes.byref(bad)) == _lib.EINVAL
+    assert L.claw2_selftest_lpt(0, 8193, 1, ctypes.byref(bad)) == _lib.EINVAL

@@ -78,3 +78,32 @@ def test_max_steps_reached():
             claw.run()
         msgs.append((str(ei.value), claw.solution.t, claw.solver.status['numsteps']))
     assert msgs[0] == msgs[1]
+
+
+@pytest.mark.parametrize("variant,rows", [(1, 8), (2, 16), (4, 8)])
+def test_device_loop_launch_variants(variant, rows):
+    # the loop's own kernel instantiations for the 3-CTA register cap, a TMA
+    # request (the loop loads rows directly) and the two-barrier tile
+    from pyclaw_b200 import _lib, tune
+    tune.set_shape(_lib.RP_EULER_ROE, variant, rows)
+    try:
+        a, b = _pair(lambda: workloads.euler_quadrants_unsplit(n=160, tfinal=0.15))
+    finally:
+        tune.set_shape(_lib.RP_EULER_ROE, 0, 0)
+    assert a.solver.status['numsteps'] > 10
+    _same(a, b)
+
+
+def test_device_loop_capacity_form():
+    # the annulus (capacity function, aux edge velocities) with extrapolated
+    # aux ghost cells in r, so no host fill is needed between steps
+    from pyclaw_b200.solver import BC
+
+    def make():
+        claw = workloads.advection_annulus(m_r=40, m_theta=120, tfinal=0.4, num_output_times=2)
+        s = claw.solver
+        s.aux_bc_lower[0] = s.aux_bc_upper[0] = BC.extrap
+        return claw
+    a, b = _pair(make)
+    assert a.solver.status['numsteps'] > 5
+    _same(a, b)

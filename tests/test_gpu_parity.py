@@ -125,3 +125,15 @@ def test_kernel_reciprocal_within_one_ulp_of_ieee_division():
         _lib.check(L.claw2_selftest_rcp(0, 1 << 22, seed, ctypes.byref(ulp)))
         assert 0.0 <= ulp.value <= 1.0, ulp.value
 
+
+@pytest.mark.parametrize("n", [1, 5, 31, 32, 33, 576, 1000, 1024, 1025, 3000, 8192])
+def test_schedule_sort_matches_stable_host_sort(n):
+    # the longest-first schedule's sort (shuffle stages up to 1024 tiles, the
+    # shared-memory network beyond) against a stable descending host sort,
+    # on costs with many ties
+    import ctypes
+    L = _lib.load()
+    for seed in (1, 77):
+        bad = ctypes.c_int(-1)
+        _lib.check(L.claw2_selftest_lpt(0, n, seed, ctypes.byref(bad)))
+        assert bad.value == 0
