@@ -77,11 +77,22 @@ static __global__ void k_batch_bc(const BatchArgs b, int first, int bcl0, int bc
     const int rs = bc_src(r, my, bcl1, bcu1, fy);
     double* q = in.q[s.cur];
     const long long src = (long long)rs * in.L.pitch + cs, dst = (long long)r * in.L.pitch + c;
-    for (int m = 0; m < meqn; ++m) {
-        double v = q[m * in.L.plane + src];
-        if (fx && m == 1) v = -v;
-        if (fy && m == 2) v = -v;
-        q[m * in.L.plane + dst] = v;
+    // loads of a group before its stores (see k_bc_fill)
+    constexpr int G = 4;
+    for (int m0 = 0; m0 < meqn; m0 += G) {
+        double v[G];
+#pragma unroll
+        for (int k = 0; k < G; ++k)
+            if (m0 + k < meqn) v[k] = q[(m0 + k) * in.L.plane + src];
+#pragma unroll
+        for (int k = 0; k < G; ++k) {
+            const int m = m0 + k;
+            if (m >= meqn) break;
+            double x = v[k];
+            if (fx && m == 1) x = -x;
+            if (fy && m == 2) x = -x;
+            q[m * in.L.plane + dst] = x;
+        }
     }
 }
 

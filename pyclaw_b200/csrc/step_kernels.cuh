@@ -1488,11 +1488,24 @@ static __global__ void k_bc_fill(const BCArgs a) {
     const int cs = bc_src(c, mx, a.bcl[0], a.bcu[0], fx);
     const int rs = bc_src(r, my, a.bcl[1], a.bcu[1], fy);
     const long long src = (long long)rs * a.L.pitch + cs, dst = (long long)r * a.L.pitch + c;
-    for (int m = 0; m < a.meqn; ++m) {
-        double v = a.q[m * a.L.plane + src];
-        if (a.negate && fx && m == 1) v = -v;
-        if (a.negate && fy && m == 2) v = -v;
-        a.q[m * a.L.plane + dst] = v;
+    // all loads of a group before its stores: the planes are one array, so a
+    // store could alias the next load and would otherwise serialise the
+    // (cold, after an L2 flush) DRAM round trips one component at a time
+    constexpr int G = 4;
+    for (int m0 = 0; m0 < a.meqn; m0 += G) {
+        double v[G];
+#pragma unroll
+        for (int k = 0; k < G; ++k)
+            if (m0 + k < a.meqn) v[k] = a.q[(m0 + k) * a.L.plane + src];
+#pragma unroll
+        for (int k = 0; k < G; ++k) {
+            const int m = m0 + k;
+            if (m >= a.meqn) break;
+            double x = v[k];
+            if (a.negate && fx && m == 1) x = -x;
+            if (a.negate && fy && m == 2) x = -x;
+            a.q[m * a.L.plane + dst] = x;
+        }
     }
 }
 
