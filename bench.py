@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--n", type=int, default=N, help="grid size override (profiling runs only)")
@@ -492,6 +492,8 @@ def run_ours(args):
 
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     kern_ms = []
+    launches0 = ctypes.c_longlong(0)
+    _lib.check(_lib.load().claw2_patch_launch_count(patch.h, ctypes.byref(launches0)))
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
         for k in range(args.steps):
@@ -504,6 +506,8 @@ def run_ours(args):
         torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
+    launches1 = ctypes.c_longlong(0)
+    _lib.check(_lib.load().claw2_patch_launch_count(patch.h, ctypes.byref(launches1)))
     step_ms = [a.elapsed_time(b) for a, b in ev]
     total_ms = sum(step_ms)
     patch.sync()  # raises if any step produced a non-finite value
@@ -608,7 +612,7 @@ def run_ours(args):
                                      "2.1e10 cell-updates/s (21% of HBM) on this part"},
                 "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
                 "secondary": secondary,
-                "gpu_launches": 2 * args.steps}
+                "gpu_launches": int(launches1.value - launches0.value)}
         print(json.dumps(line), flush=True)
     solver._dev.close()
     if world > 1:

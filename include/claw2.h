@@ -248,6 +248,11 @@ int claw2_patch_set_stream(claw2_patch* p, void* stream);
  * step kernel(s) of each claw2_patch_step (ghost fill excluded).  After a
  * step, claw2_patch_kernel_ms waits for it and returns the elapsed time. */
 int claw2_patch_set_timing(claw2_patch* p, int on);
+
+/* Kernels enqueued so far by the patch's steps (claw2_patch_step and the
+ * host pipeline): ghost fill, step kernel(s), learned-guess pre-pass, tile
+ * schedule sort.  Read before and after a run to count its launches. */
+int claw2_patch_launch_count(claw2_patch* p, long long* n);
 int claw2_patch_kernel_ms(claw2_patch* p, float* ms);
 
 /* Launch shape of the unsplit step kernel for one Riemann solver: variant 0

@@ -111,6 +111,7 @@ _SIGNATURES = {
     "claw2_patch_kernel_ms": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]),
     "claw2_probe_fp64": (ctypes.c_int, [ctypes.c_int, _c_double_p]),
     "claw2_selftest_rcp": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_ulonglong, _c_double_p]),
+    "claw2_patch_launch_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]),
     "claw2_selftest_lpt": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_ulonglong,
                                           ctypes.POINTER(ctypes.c_int)]),
     "claw2_tune_set": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int]),

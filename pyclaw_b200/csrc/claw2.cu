@@ -793,6 +793,7 @@ struct claw2_patch {
     int* tile_order = nullptr;
     int tile_cap = 0, tile_n = 0, tile_H = 0;
     unsigned int tile_steps = 0;  // steps run on the current tiling
+    long long step_launches = 0;  // kernels enqueued by patch_enqueue_step (claw2_patch_launch_count)
     // host pipeline of claw2_patch_run_host
     cudaStream_t cst = nullptr, dst = nullptr;  // upload and download streams
     double* stage_in[2] = {nullptr, nullptr};
@@ -1267,12 +1268,14 @@ int patch_enqueue_step(claw2_patch* p, double dt) {
         p->ghosts_supplied = false;
     } else {
         launch_bc(qc, p->L, p->d.num_eqn, p->d.bc_lower, p->d.bc_upper, p->cfl, p->st);
+        ++p->step_launches;
     }
     StepArgs a = patch_args(p, dt);
     if (p->timing) CUDA_TRY(cudaEventRecord(p->ev0, p->st));
     if (p->d.riemann == CLAW2_RP_EULER_EXACT && p->mlp && !p->d.dimensional_split) {
         mlp_guess_launch(p->mlp, qc, p->L, p->rp.c[0], p->guess, p->st);
         a.guess = p->guess;
+        ++p->step_launches;
     }
     int lpt_n = 0;
     if (p->d.dimensional_split) {
@@ -1280,6 +1283,7 @@ int patch_enqueue_step(claw2_patch* p, double dt) {
         ax.qnew = p->tmp;
         ay.qold = p->tmp;
         dispatch<SplitF>(p->d.riemann, ax, ay, p->st, 3);
+        p->step_launches += 2;
     } else {
         int ns, H, nb;
         unsplit_tiling(p->d.riemann, p->L.mx, p->L.my, ns, H, nb);
@@ -1292,9 +1296,13 @@ int patch_enqueue_step(claw2_patch* p, double dt) {
             a.tile_cost = p->tile_cost;
         }
         dispatch<UnsplitF>(p->d.riemann, a, p->st, p->has_tmap ? &p->tmap[p->cur] : nullptr);
+        ++p->step_launches;
     }
     if (p->timing) CUDA_TRY(cudaEventRecord(p->ev1, p->st));
-    if (lpt_n > 0 && (p->tile_steps++ % LPT_EVERY) == 0) launch_lpt(p->tile_cost, p->tile_order, lpt_n, p->st);
+    if (lpt_n > 0 && (p->tile_steps++ % LPT_EVERY) == 0) {
+        launch_lpt(p->tile_cost, p->tile_order, lpt_n, p->st);
+        ++p->step_launches;
+    }
     CUDA_TRY(cudaGetLastError());
     p->pending = true;
     return CLAW2_OK;
@@ -1815,6 +1823,12 @@ int claw2_tune_get(int riemann, int* variant, int* rows) {
     if (rp_shape(riemann, &me, &mw) != 0 || !variant || !rows) return fail(CLAW2_EINVAL, "bad arguments");
     *variant = g_tune[riemann & (TUNE_SLOTS - 1)].variant;
     *rows = g_tune[riemann & (TUNE_SLOTS - 1)].rows;
+    return CLAW2_OK;
+}
+
+int claw2_patch_launch_count(claw2_patch* p, long long* n) {
+    if (!p || !n) return fail(CLAW2_EINVAL, "null pointer argument");
+    *n = p->step_launches;
     return CLAW2_OK;
 }
 

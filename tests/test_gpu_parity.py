@@ -137,3 +137,23 @@ def test_schedule_sort_matches_stable_host_sort(n):
         bad = ctypes.c_int(-1)
         _lib.check(L.claw2_selftest_lpt(0, n, seed, ctypes.byref(bad)))
         assert bad.value == 0
+
+
+@pytest.mark.parametrize("split,per_step", [(False, 2), (True, 3)])
+def test_step_launch_count(split, per_step):
+    # the counter bench.py reports as gpu_launches: ghost fill + the step
+    # kernel (two sweeps when split); a grid this small runs no schedule sort
+    import ctypes
+    from pyclaw_b200 import workloads
+    claw = workloads.euler_quadrants_unsplit(n=64, tfinal=0.01)
+    claw.solver.dimensional_split = split
+    claw.solver.setup(claw.solution)
+    p = claw.solver._dev
+    L = _lib.load()
+    n0, n1 = ctypes.c_longlong(-1), ctypes.c_longlong(-1)
+    _lib.check(L.claw2_patch_launch_count(p.h, ctypes.byref(n0)))
+    for _ in range(3):
+        p.step(1e-4, want_cfl=False)
+        p.accept(True)
+    _lib.check(L.claw2_patch_launch_count(p.h, ctypes.byref(n1)))
+    assert n1.value - n0.value == 3 * per_step
