@@ -830,22 +830,10 @@ namespace {
 int lpt_prepare(claw2_patch* p, int n, int H) {
     if (n < 1 || n > LPT_MAX_TILES) return CLAW2_EINVAL;
     if (n > p->tile_cap) {
+        // (the patch's stream may still run a step on the old arrays)
+        cudaStreamSynchronize(p->st);
         cudaFree(p->tile_cost);
         cudaFree(p->tile_order);
-        if (p->cst) cudaStreamSynchronize(p->cst);
-        if (p->dst) cudaStreamSynchronize(p->dst);
-        for (int i = 0; i < 2; ++i) {
-            cudaFree(p->stage_in[i]);
-            if (p->h2d_done[i]) cudaEventDestroy(p->h2d_done[i]);
-            if (p->in_free[i]) cudaEventDestroy(p->in_free[i]);
-            if (p->out_ready[i]) cudaEventDestroy(p->out_ready[i]);
-            if (p->out_free[i]) cudaEventDestroy(p->out_free[i]);
-        }
-        cudaFree(p->stage_out1);
-        cudaFree(p->cfl_hist);
-        cudaFreeHost(p->h_cfl_hist);
-        if (p->cst) cudaStreamDestroy(p->cst);
-        if (p->dst) cudaStreamDestroy(p->dst);
         p->tile_cost = nullptr;
         p->tile_order = nullptr;
         p->tile_cap = 0;
@@ -1054,6 +1042,21 @@ int claw2_patch_destroy(claw2_patch* p) {
         cudaFree(p->counters);
         cudaFree(p->tile_cost);
         cudaFree(p->tile_order);
+        // the host pipeline of claw2_patch_run_host
+        if (p->cst) cudaStreamSynchronize(p->cst);
+        if (p->dst) cudaStreamSynchronize(p->dst);
+        for (int i = 0; i < 2; ++i) {
+            cudaFree(p->stage_in[i]);
+            if (p->h2d_done[i]) cudaEventDestroy(p->h2d_done[i]);
+            if (p->in_free[i]) cudaEventDestroy(p->in_free[i]);
+            if (p->out_ready[i]) cudaEventDestroy(p->out_ready[i]);
+            if (p->out_free[i]) cudaEventDestroy(p->out_free[i]);
+        }
+        cudaFree(p->stage_out1);
+        cudaFree(p->cfl_hist);
+        cudaFreeHost(p->h_cfl_hist);
+        if (p->cst) cudaStreamDestroy(p->cst);
+        if (p->dst) cudaStreamDestroy(p->dst);
         cudaFree(p->stage);
         cudaFree(p->gather_buf);
         cudaFreeHost(p->out_host);

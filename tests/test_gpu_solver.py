@@ -282,3 +282,41 @@ def test_largest_benchmark_size_one_step_matches_oracle(oracle):
                                 rpn2=rp)
     assert abs(cfl_g - cfl_o) <= PARITY_RTOL * cfl_o
     assert max_rel(q_g[:, 2:-2, 2:-2], q_o[:, 2:-2, 2:-2]) <= PARITY_RTOL
+
+
+def test_run_host_after_the_tile_schedule_grows():
+    # a step on a finer tiling (more tiles than the schedule arrays held)
+    # reallocates only the schedule; the host pipeline set up by an earlier
+    # claw2_patch_run_host stays valid for the next one
+    from pyclaw_b200 import tune
+    claw = workloads.euler_quadrants_unsplit(n=640, tfinal=0.1)
+    s, sol = claw.solver, claw.solution
+    s.setup(sol)
+    p = s._dev
+    rng = np.random.default_rng(5)
+    q0 = sol.state.get_q_global()
+    qs = [np.asfortranarray(q0 * (1.0 + 0.01 * rng.random(q0.shape))) for _ in range(2)]
+    dts = [2e-4, 1e-4]
+    tune.set_shape(_lib.RP_EULER_ROE, 0, 0)
+    try:
+        outs = [np.empty(q.shape, order="F") for q in qs]
+        p.run_host(qs, outs, dts)           # reserves the pipeline; ~432 tiles
+        tune.set_shape(_lib.RP_EULER_ROE, 0, 2)
+        p.step(1e-4, want_cfl=False)        # 6 strips x 320 row blocks: the schedule grows
+        p.accept(False)
+        outs2 = [np.empty(q.shape, order="F") for q in qs]
+        cfl2 = p.run_host(qs, outs2, dts)
+        ref, cref = [], []
+        for q, dt in zip(qs, dts):
+            sol.state.q = q
+            p.push(sol.state)
+            cref.append(p.step(dt))
+            p.accept(True)
+            out = np.empty(q.shape, order="F")
+            _lib.check(p._lib.claw2_patch_download_q(p.h, _lib.dptr(out)))
+            ref.append(out)
+    finally:
+        tune.set_shape(_lib.RP_EULER_ROE, 0, 0)
+    for a, b in zip(outs2, ref):
+        assert np.array_equal(a, b)
+    assert list(cfl2) == cref
