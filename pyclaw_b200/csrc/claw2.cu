@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -182,6 +183,7 @@ struct UnsplitShape {
 
 constexpr int TUNE_SLOTS = 16;  // indexed by Riemann solver id
 UnsplitShape g_tune[TUNE_SLOTS] = {};
+std::atomic<unsigned> g_tune_gen{0};  // bumped by every claw2_tune_set (cached graphs go stale)
 
 // true for the method the SPEC_MC2 kernels are compiled for
 bool is_mc2(const Method& m, int mwaves) {
@@ -788,6 +790,12 @@ struct claw2_patch {
     double* guess = nullptr;                  // exact solver: learned guesses, x and y planes
     unsigned long long* counters = nullptr;   // exact solver: Newton iterations, solves
     claw2_mlp* mlp = nullptr;
+    // claw2_patch_evolve's captured attempts, one graph per starting buffer
+    // parity, reused while nothing they captured changed: graph_gen counts
+    // changes of the patch's parameters, network and tile schedule arrays
+    cudaGraphExec_t evo_exec[2] = {nullptr, nullptr};
+    unsigned long long evo_stamp[2] = {0, 0};
+    unsigned graph_gen = 1;
     // longest-first tile schedule of the unsplit kernel (k_lpt_order)
     unsigned int* tile_cost = nullptr;
     int* tile_order = nullptr;
@@ -850,6 +858,7 @@ int lpt_prepare(claw2_patch* p, int n, int H) {
         p->tile_n = 0;
     }
     if (p->tile_n != n || p->tile_H != H) {
+        ++p->graph_gen;
         k_iota<<<(n + 255) / 256, 256, 0, p->st>>>(p->tile_order, n);
         cudaMemsetAsync(p->tile_cost, 0, sizeof(unsigned int) * n, p->st);
         p->tile_n = n;
@@ -1061,6 +1070,8 @@ int claw2_patch_destroy(claw2_patch* p) {
         cudaFree(p->gather_buf);
         cudaFreeHost(p->out_host);
         if (p->out_ev) cudaEventDestroy(p->out_ev);
+        for (int i = 0; i < 2; ++i)
+            if (p->evo_exec[i]) cudaGraphExecDestroy(p->evo_exec[i]);
         cudaFree(p->evo);
         cudaFreeHost(p->h_evo);
         cudaFree(p->cfl);
@@ -1079,6 +1090,7 @@ int claw2_patch_set_cparam(claw2_patch* p, const double* cparam, int n) {
     if (!p) return fail(CLAW2_EINVAL, "null patch");
     if (n < 0 || n > CLAW2_MAX_PARAMS) return fail(CLAW2_EINVAL, "ncparam %d out of range", n);
     p->rp = make_params(p->d.riemann, cparam, n);
+    ++p->graph_gen;
     return CLAW2_OK;
 }
 
@@ -1525,8 +1537,9 @@ int claw2_patch_evolve(claw2_patch* p, claw2_evolve_state* s) {
     // and schedule buffers) four attempts are captured as one CUDA graph and
     // replayed: four attempts return to the same buffer parity, so the same
     // graph serves every later chunk, and the host no longer pays one launch
-    // per kernel.  Any capture failure falls back to direct launches.
-    cudaGraph_t graph = nullptr;
+    // per kernel.  The graph is kept for the next call from the same parity
+    // while nothing it captured has changed.  Any capture failure falls back
+    // to direct launches.
     cudaGraphExec_t exec = nullptr;
     constexpr int GRAPH_ATTEMPTS = 4;
     bool try_graph = true;
@@ -1535,16 +1548,25 @@ int claw2_patch_evolve(claw2_patch* p, claw2_evolve_state* s) {
         if (issued > 0 && try_graph && !exec) {
             try_graph = false;
             const int c = (int)((cur0 + issued) & 1);
-            if (cudaStreamBeginCapture(p->st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            const unsigned long long stamp =
+                ((unsigned long long)p->graph_gen << 32) | (unsigned long long)g_tune_gen.load();
+            if (p->evo_exec[c] && p->evo_stamp[c] == stamp) {
+                exec = p->evo_exec[c];
+            } else if (cudaStreamBeginCapture(p->st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+                cudaGraph_t graph = nullptr;
                 int crc = CLAW2_OK;
                 for (int j = 0; j < GRAPH_ATTEMPTS && crc == CLAW2_OK; ++j) crc = evolve_enqueue_attempt(p, (c + j) & 1);
                 const cudaError_t ec = cudaStreamEndCapture(p->st, &graph);
                 if (crc != CLAW2_OK || ec != cudaSuccess || !graph ||
                     cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
                     cudaGetLastError();
-                    if (graph) cudaGraphDestroy(graph);
-                    graph = nullptr;
                     exec = nullptr;
+                }
+                if (graph) cudaGraphDestroy(graph);
+                if (exec) {
+                    if (p->evo_exec[c]) cudaGraphExecDestroy(p->evo_exec[c]);
+                    p->evo_exec[c] = exec;
+                    p->evo_stamp[c] = stamp;
                 }
             } else {
                 cudaGetLastError();
@@ -1572,8 +1594,6 @@ int claw2_patch_evolve(claw2_patch* p, claw2_evolve_state* s) {
         }
         chunk = std::min(chunk * 2, 64);
     }
-    if (exec) cudaGraphExecDestroy(exec);
-    if (graph) cudaGraphDestroy(graph);
     if (rc != CLAW2_OK) return rc;
     p->cur = (cur0 + e.attempts) & 1;
     s->t = e.t;
@@ -1818,6 +1838,7 @@ int claw2_tune_set(int riemann, int variant, int rows) {
     if (rows < 0 || rows > 4096) return fail(CLAW2_EINVAL, "rows must be 0..4096 (got %d)", rows);
     g_tune[riemann & (TUNE_SLOTS - 1)].variant = variant;
     g_tune[riemann & (TUNE_SLOTS - 1)].rows = rows;
+    ++g_tune_gen;
     return CLAW2_OK;
 }
 
@@ -1841,6 +1862,7 @@ int claw2_patch_set_mlp(claw2_patch* p, claw2_mlp* m) {
         return fail(CLAW2_EINVAL, "learned guesses apply to the exact Euler solver only");
     if (m && m->device != p->device) return fail(CLAW2_EINVAL, "network and patch are on different devices");
     p->mlp = m;
+    ++p->graph_gen;
     return CLAW2_OK;
 }
 
