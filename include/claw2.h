@@ -248,15 +248,17 @@ int claw2_patch_set_stream(claw2_patch* p, void* stream);
  * step kernel(s) of each claw2_patch_step (ghost fill excluded).  After a
  * step, claw2_patch_kernel_ms waits for it and returns the elapsed time. */
 int claw2_patch_set_timing(claw2_patch* p, int on);
-
-/* Kernels enqueued so far by the patch's steps (claw2_patch_step and the
- * host pipeline): ghost fill, step kernel(s), learned-guess pre-pass, tile
- * schedule sort.  Read before and after a run to count its launches. */
-int claw2_patch_launch_count(claw2_patch* p, long long* n);
 int claw2_patch_kernel_ms(claw2_patch* p, float* ms);
 
+/* Instrumentation, no counterpart in the reference: the kernels enqueued so
+ * far by the patch's steps (claw2_patch_step and the host pipeline): ghost
+ * fill, step kernel(s), learned-guess pre-pass, tile schedule sort.  Read it
+ * before and after a run to count the run's launches. */
+int claw2_patch_launch_count(claw2_patch* p, long long* n);
+
 /* Launch shape of the unsplit step kernel for one Riemann solver: variant 0
- * compiles for 2 blocks per SM (no register cap), 1 for 3 blocks per SM;
+ * compiles for 2 blocks per SM (no register cap), 1 for 3 blocks per SM,
+ * 2 and 3 the same with rows staged by TMA, 4 the two-barrier tile;
  * rows = row-block height (0 = heuristic).  Process-wide; set by an autotuner
  * (pyclaw_b200.tune) or by hand. */
 int claw2_tune_set(int riemann, int variant, int rows);
@@ -273,10 +275,10 @@ int claw2_probe_fp64(int device, double* tflops);
  * between it and CUDA's IEEE quotient 1.0/a. */
 int claw2_selftest_rcp(int device, int n, unsigned long long seed, double* max_ulp);
 
-/* Self-test of the longest-first tile schedule's sort: n (1..8192) seeded
- * tile costs with many ties, sorted on the device; *mismatches = positions
- * where the order differs from a stable descending sort on the host (cost
- * descending, ties by lower tile first). */
+/* Self-test (no counterpart in the reference) of the longest-first tile
+ * schedule's sort: n (1..8192) seeded tile costs with many ties, sorted on the
+ * device; *mismatches = positions where the order differs from a stable
+ * descending sort on the host (cost descending, ties by lower tile first). */
 int claw2_selftest_lpt(int device, int n, unsigned long long seed, int* mismatches);
 
 /* ---- no counterpart in the reference ------------------------------------
