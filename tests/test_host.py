@@ -184,3 +184,45 @@ def test_gauges_and_functional_files(oracle, tmp_path):
     assert np.allclose(st.gauge_data[0][:, 2], 10 * st.gauge_data[0][:, 1])
     F = np.loadtxt(str(tmp_path / "F.txt"))
     assert F.shape == (11, 2) and np.all(F[:, 1] > 0)
+
+
+def test_device_time_loop_only_without_host_callbacks():
+    # evolve_to_time runs on the GPU only when nothing needs the host between
+    # steps; each host callback of the reference's loop sends it back to the
+    # host loop (the predicate needs no GPU)
+    from pyclaw_b200 import BC, workloads
+    from pyclaw_b200.classic import ClawSolver2D
+
+    def fresh():
+        claw = workloads.euler_quadrants_unsplit(n=16, tfinal=0.1)
+        return claw.solver, claw.solution
+
+    s, sol = fresh()
+    assert s._device_loop_ok(sol, 0.1)
+    assert not s._device_loop_ok(sol, None)          # take_one_step form
+    s.device_time_loop = False
+    assert not s._device_loop_ok(sol, 0.1)
+
+    s, sol = fresh()
+    s.before_step = lambda solver, state: None
+    assert not s._device_loop_ok(sol, 0.1)
+    s, sol = fresh()
+    s.step_source = lambda solver, state, dt: None
+    assert not s._device_loop_ok(sol, 0.1)
+    s, sol = fresh()
+    sol.state.grid.add_gauges([(0.5, 0.5)])
+    assert not s._device_loop_ok(sol, 0.1)
+    s, sol = fresh()
+    s.bc_lower[1] = BC.custom
+    s.user_bc_lower = lambda *a: None
+    assert not s._device_loop_ok(sol, 0.1)
+
+    # a subclass that replaces a stepping method keeps the host loop
+    class Sub(ClawSolver2D):
+        def step_hyperbolic(self, solution):
+            return super().step_hyperbolic(solution)
+    s, sol = fresh()
+    sub = Sub(s.rp)
+    assert sub.rp is s.rp
+    assert not sub._device_loop_ok(sol, 0.1)
+    assert ClawSolver2D(s.rp)._device_loop_ok(sol, 0.1)
