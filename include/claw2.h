@@ -292,7 +292,8 @@ int claw2_selftest_lpt(int device, int n, unsigned long long seed, int* mismatch
  * and the intermediate state plus the CFL/status words live in one fixed
  * device array of CLAW2_NOALLOC_SCRATCH_BYTES held by every GPU that loads
  * the library until exit.  Grids needing more than that (256 bytes +
- * num_eqn*plane*8 bytes) are rejected with CLAW2_EINVAL.  Every
+ * num_eqn*plane*8 bytes), or with mx or my above 2^28, are rejected with
+ * CLAW2_EINVAL before any GPU work.  Every
  * call reuses that array: the call clears the words that must start at zero;
  * calls whose GPU work overlaps race and must be serialised.  The first call
  * on a device looks up the array's address; make it before any stream

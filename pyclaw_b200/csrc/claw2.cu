@@ -150,11 +150,24 @@ bool make_row_tmap(CUtensorMap* tm, double* q, const Layout& L, int meqn) {
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-int pick_rows(int nstrips, int nrows) {
-    // about three CTAs per SM on a 148-SM part, 2..64 rows per CTA: a small
-    // grid gets short row blocks, since its time is one tile's march down its
-    // rows (measured at 100^2-300^2: 2-3 rows 1.5-1.8x faster than 8)
-    const int want_blocks = std::max(1, (3 * 148 + nstrips - 1) / nstrips);
+// SM count of the current device (queried once per device; 148 on a B200).
+int device_sms() {
+    static std::atomic<int> cache[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    int n = cache[dev].load(std::memory_order_relaxed);
+    if (n <= 0) {
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+        cache[dev].store(n, std::memory_order_relaxed);
+    }
+    return n;
+}
+
+int pick_rows(int nstrips, int nrows, int nsm) {
+    // about three CTAs per SM, 2..64 rows per CTA: a small grid gets short
+    // row blocks, since its time is one tile's march down its rows (measured
+    // at 100^2-300^2: 2-3 rows 1.5-1.8x faster than 8)
+    const int want_blocks = std::max(1, (3 * nsm + nstrips - 1) / nstrips);
     int H = (nrows + want_blocks - 1) / want_blocks;
     return std::max(2, std::min(64, H));
 }
@@ -215,7 +228,7 @@ void unsplit_tiling(int riemann, int mx, int my, int& nstrips, int& H, int& nblo
     constexpr int W = NT_UNSPLIT - 4;
     nstrips = (mx + W - 1) / W;
     const int rows = g_tune[riemann & (TUNE_SLOTS - 1)].rows;
-    H = rows > 0 ? rows : pick_rows(nstrips, my);
+    H = rows > 0 ? rows : pick_rows(nstrips, my, device_sms());
     nblocks = (my + H - 1) / H;
 }
 
@@ -291,7 +304,7 @@ void launch_split_s(const StepArgs& ax, const StepArgs& ay, cudaStream_t st, int
         constexpr int W = NT_SPLIT_X - 4;
         const int ns = (ax.L.mx + W - 1) / W;
         StepArgs b = ax;
-        b.H = pick_rows(ns, ax.L.my + 4);
+        b.H = pick_rows(ns, ax.L.my + 4, device_sms());
         dim3 grid(ns, (ax.L.my + 4 + b.H - 1) / b.H);
         constexpr int smem = (int)sizeof(SplitXSmem<RP, NT_SPLIT_X>);
         static unsigned long long attr = 0;
@@ -301,7 +314,7 @@ void launch_split_s(const StepArgs& ax, const StepArgs& ay, cudaStream_t st, int
     if (which & 2) {
         const int ns = (ay.L.mx + 4 + NT_SPLIT_Y - 1) / NT_SPLIT_Y;
         StepArgs b = ay;
-        b.H = pick_rows(ns, ay.L.my);
+        b.H = pick_rows(ns, ay.L.my, device_sms());
         dim3 grid(ns, (ay.L.my + b.H - 1) / b.H);
         k_split_y<RP, NT_SPLIT_Y, SPEC, EVO><<<grid, NT_SPLIT_Y, 0, st>>>(b);
     }
@@ -454,7 +467,7 @@ int scratch_reserve(size_t n, size_t nstage) {
     return CLAW2_OK;
 }
 
-int grid_blocks(long long n) { return (int)std::min<long long>((n + 255) / 256, 148LL * 16); }
+int grid_blocks(long long n) { return (int)std::min<long long>((n + 255) / 256, 16LL * device_sms()); }
 
 // Shared body of claw2_step2 / claw2_step2ds: host qbc -> device planes ->
 // kernels -> host qbc (interior cells).
@@ -902,6 +915,14 @@ StepArgs patch_args(claw2_patch* p, double dt) {
 }
 
 }  // namespace
+
+// The split sweeps on caller-owned buffers, for claw2_step2ds_noalloc
+// (claw2_noalloc.cu): the launches claw2_step2ds makes (same kernels, method
+// specialisations and row heights).  Hidden: not part of the exported ABI.
+__attribute__((visibility("hidden"))) int claw2_internal_launch_split(int rp, const StepArgs& ax, const StepArgs& ay,
+                                                                      cudaStream_t st) {
+    return dispatch<SplitF>(rp, ax, ay, st, 3);
+}
 
 extern "C" {
 
@@ -1924,10 +1945,12 @@ int batch_build_tiles(claw2_batch* b, const int* rows) {
     b->h_tiles.clear();
     b->tile_first.assign(b->n, 0);
     b->tile_count.assign(b->n, 0);
+    int nsm = 0;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->device) != cudaSuccess || nsm <= 0) nsm = 148;
     for (int i : b->order) {
         BatchInst& in = b->h_inst[i];
         in.nstrips = (in.L.mx + W - 1) / W;
-        in.H = (rows && rows[i] > 0) ? rows[i] : pick_rows(in.nstrips, in.L.my);
+        in.H = (rows && rows[i] > 0) ? rows[i] : pick_rows(in.nstrips, in.L.my, nsm);
         const int nblk = (in.L.my + in.H - 1) / in.H;
         b->tile_first[i] = (int)b->h_tiles.size();
         b->tile_count[i] = in.nstrips * nblk;

@@ -23,7 +23,9 @@
 //     threads) race on the array: serialise them;
 //   * the first call on each device looks up the array's device address
 //     (cudaGetSymbolAddress) with that device current; make that first call
-//     before any stream capture.
+//     before any stream capture;
+//   * each call waits for its stream to finish the step (it copies the
+//     Courant number back to the host before it returns).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -38,12 +40,15 @@
 using namespace claw2;
 
 extern "C" void claw2_internal_set_error(const char* msg);  // claw2.cu, not exported
+// claw2.cu, not exported: claw2_step2ds's two sweeps on the given buffers
+int claw2_internal_launch_split(int rp, const StepArgs& ax, const StepArgs& ay, cudaStream_t st);
 
 namespace {
 
 // [0] CFL bit pattern, [1] status word, intermediate state from kHeader on.
 constexpr long long kScratchDoubles = CLAW2_NOALLOC_SCRATCH_BYTES / 8;
 constexpr long long kHeader = 32;  // 256 bytes, so the planes stay 256-byte aligned
+constexpr int kMaxSide = 1 << 28;  // mx, my bound (the scratch limit is far below it anyway)
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 
 std::mutex g_mu;
@@ -78,34 +83,6 @@ int scratch_on_device(double** out) {
     return CLAW2_OK;
 }
 
-int rows_for(int nstrips, int nrows) {
-    const int want = std::max(1, (3 * 148 + nstrips - 1) / nstrips);
-    return std::max(8, std::min(64, (nrows + want - 1) / want));
-}
-
-template <class RP>
-int run_split(const StepArgs& ax, const StepArgs& ay, cudaStream_t st) {
-    constexpr int NTX = 128, NTY = 128, WX = NTX - 4;
-    {
-        const int ns = (ax.L.mx + WX - 1) / WX;
-        StepArgs b = ax;
-        b.H = rows_for(ns, ax.L.my + 4);
-        dim3 grid(ns, (ax.L.my + 4 + b.H - 1) / b.H);
-        const int smem = (int)sizeof(SplitXSmem<RP, NTX>);
-        cudaFuncSetAttribute(k_split_x<RP, NTX>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        k_split_x<RP, NTX><<<grid, NTX, smem, st>>>(b);
-    }
-    {
-        const int ns = (ay.L.mx + 4 + NTY - 1) / NTY;
-        StepArgs b = ay;
-        b.H = rows_for(ns, ay.L.my);
-        dim3 grid(ns, (ay.L.my + b.H - 1) / b.H);
-        k_split_y<RP, NTY><<<grid, NTY, 0, st>>>(b);
-    }
-    cudaError_t e = cudaGetLastError();
-    return e == cudaSuccess ? CLAW2_OK : fail(CLAW2_ECUDA, "launch failed: %s", cudaGetErrorString(e));
-}
-
 }  // namespace
 
 extern "C" {
@@ -126,21 +103,24 @@ int claw2_step2ds_noalloc(const claw2_desc* d, const double* qold, double* qnew,
                     mwaves, d->num_eqn, d->num_waves);
     if (d->num_ghost != 2 || d->num_aux != 0 || d->mcapa != 0 || d->fwave)
         return fail(CLAW2_EUNSUPPORTED, "num_ghost must be 2, without aux arrays, capacity or f-waves");
-    if (d->mx < 1 || d->my < 1) return fail(CLAW2_EINVAL, "bad sizes mx=%d my=%d", d->mx, d->my);
+    // bounded first, so that mx + 4, my + 4 and the products below cannot overflow
+    if (d->mx < 1 || d->my < 1 || d->mx > kMaxSide || d->my > kMaxSide)
+        return fail(CLAW2_EINVAL, "bad sizes mx=%d my=%d (1..%d each)", d->mx, d->my, kMaxSide);
     if (d->order != 1 && d->order != 2) return fail(CLAW2_EINVAL, "order must be 1 or 2");
     if (!(d->dx > 0.0) || !(d->dy > 0.0) || !(dt >= 0.0)) return fail(CLAW2_EINVAL, "dx, dy > 0 and dt >= 0 required");
     for (int k = 0; k < mwaves; ++k)
         if (d->mthlim[k] < 0 || d->mthlim[k] > 5) return fail(CLAW2_EINVAL, "limiter %d out of range", d->mthlim[k]);
-    if (pitch < d->mx + 4 || pitch > (1ll << 30) || plane < pitch * (d->my + 4))
+    if (pitch < d->mx + 4 || pitch > (1ll << 30) || plane < pitch * (long long)(d->my + 4))
         return fail(CLAW2_EINVAL, "layout too small: pitch=%lld plane=%lld for %dx%d cells", pitch, plane, d->mx,
                     d->my);
     if (((uintptr_t)qold | (uintptr_t)qnew) & 7) return fail(CLAW2_EINVAL, "q planes must be 8-byte aligned");
-    const long long need = kHeader + (long long)meqn * plane;
-    if (need > kScratchDoubles)
+    // plane is compared before it is multiplied: meqn * plane cannot overflow
+    if (plane > (kScratchDoubles - kHeader) / meqn)
         return fail(CLAW2_EINVAL,
-                    "problem too large for the fixed scratch array: needs %lld bytes, the maximum is %lld bytes "
-                    "(CLAW2_NOALLOC_SCRATCH_BYTES); use claw2_patch_* for larger grids",
-                    need * 8, kScratchDoubles * 8);
+                    "problem too large for the fixed scratch array: needs %lld planes of %lld doubles, the maximum "
+                    "is %lld bytes (CLAW2_NOALLOC_SCRATCH_BYTES) including a %lld-byte header; use claw2_patch_* "
+                    "for larger grids",
+                    (long long)meqn, plane, kScratchDoubles * 8, kHeader * 8);
 
     double* scr = nullptr;
     int rc = scratch_on_device(&scr);
@@ -178,13 +158,10 @@ int claw2_step2ds_noalloc(const claw2_desc* d, const double* qold, double* qnew,
     ay.qold = qtmp;
     ay.qnew = qnew;  // y-sweep: interior cells
 
-    switch (d->riemann) {
-        case CLAW2_RP_ADVECTION: rc = run_split<RPAdvection>(ax, ay, st); break;
-        case CLAW2_RP_ACOUSTICS: rc = run_split<RPAcoustics>(ax, ay, st); break;
-        case CLAW2_RP_EULER_ROE: rc = run_split<RPEulerRoe>(ax, ay, st); break;
-        default: rc = run_split<RPShallowRoe>(ax, ay, st); break;
-    }
-    if (rc) return rc;
+    if (claw2_internal_launch_split(d->riemann, ax, ay, st) != 0)
+        return fail(CLAW2_EINVAL, "unknown Riemann solver id %d", d->riemann);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(CLAW2_ECUDA, "launch failed: %s", cudaGetErrorString(e));
     unsigned long long bits = 0;
     int stat = 0;
     e = cudaMemcpyAsync(&bits, cfl_bits, sizeof bits, cudaMemcpyDeviceToHost, st);

@@ -129,3 +129,25 @@ def test_transverse_solve_rejected_for_solvers_without_one():
     h = ctypes.c_void_p()
     assert L.claw2_patch_create(ctypes.byref(d), ctypes.byref(h)) == _lib.EINVAL
     assert b"transverse" in L.claw2_last_error()
+
+
+@pytest.mark.parametrize("name,mx,my,pitch,plane", [
+    # a plane so large that num_eqn * plane overflows 64 bits if multiplied first
+    ("huge plane", 40, 30, 48, 1 << 61),
+    # my near INT_MAX: my + 4 overflows int if computed without the bound
+    ("huge my", 40, 2**31 - 2, 48, 1 << 40),
+    ("huge mx", 2**31 - 3, 30, 1 << 30, 1 << 40),
+    ("one cell over the scratch", 1020, 1020, 1024, 1024 * 1024),
+])
+def test_noalloc_sizes_rejected_without_gpu(name, mx, my, pitch, plane):
+    # claw2_step2ds_noalloc checks every size against its fixed scratch array
+    # before its first CUDA call, without integer overflow
+    import ctypes
+    from pyclaw_b200 import _lib
+    L = _lib.load()
+    d = _valid_desc()
+    d.mx, d.my, d.transverse, d.dimensional_split = mx, my, 0, 1
+    cfl = ctypes.c_double(0.0)
+    fake = ctypes.c_void_p(1 << 20)  # never dereferenced: rejected first
+    rc = L.claw2_step2ds_noalloc(ctypes.byref(d), fake, fake, pitch, plane, 1e-4, ctypes.byref(cfl), None)
+    assert rc == _lib.EINVAL, (name, rc, L.claw2_last_error())
