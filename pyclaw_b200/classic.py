@@ -10,7 +10,7 @@ stays there between steps.
 import numpy as np
 
 from .limiters import tvd
-from .solver import BC, CFLError, Solver
+from .solver import BC, AttemptBudget, CFLError, Solver
 from . import _lib
 from . import hostbc as _hostbc
 
@@ -275,15 +275,7 @@ class ClawSolver2D(ClawSolver):
         if not self._is_set_up:
             self.setup(solution)
         tstart = solution.t
-        if not self.dt_variable:
-            self.max_steps = int((tend - tstart + 1e-10) / self.dt)
-            if abs(self.max_steps * self.dt - (tend - tstart)) > 1e-5 * (tend - tstart):
-                raise Exception('dt does not divide (tend-tstart) and dt is fixed!')
-        if self.dt_variable == 1 and self.cfl_desired > self.cfl_max:
-            raise Exception('Variable time-stepping and desired CFL > maximum CFL')
-        if tend <= tstart:
-            self.logger.info("Already at or beyond end time: no evolution required.")
-            self.max_steps = 0
+        budget = AttemptBudget(self, tstart, tend)
         state = solution.states[0]
         dev = self._dev
         if dev is None or state._mirror is not dev:
@@ -297,7 +289,7 @@ class ClawSolver2D(ClawSolver):
             cfl_desired=self.cfl_desired, cfl_max=self.cfl_max, dt_max=self.dt_max,
             dtmin=self.status['dtmin'], dtmax=self.status['dtmax'], cflmax=self.status['cflmax'],
             dt_variable=1 if self.dt_variable else 0, dt_old_set=0 if self.dt_old is None else 1,
-            max_steps=self.max_steps)
+            max_steps=budget.count)
         rc = dev.evolve(es)
         if es.attempts > 0:
             solution.t = es.t
@@ -312,10 +304,10 @@ class ClawSolver2D(ClawSolver):
         _lib.check(rc)
         if es.cfl_error:
             self.accept_step = False
-            raise CFLError('CFL too large, giving up!')
+            raise CFLError("Courant number %.17g above cfl_max = %g with a fixed dt of %.17g"
+                           % (float(es.cfl), self.cfl_max, float(self.dt)))
         self.accept_step = True
-        if self.dt_variable and solution.t < tend and es.num_steps == self.max_steps:
-            raise Exception("Maximum number of timesteps have been taken")
+        budget.check_finished(self, solution.t, tend, es.num_steps)
         return self.status
 
     def step(self, solution, take_one_step, tstart, tend):

@@ -89,6 +89,11 @@ struct RPAdvection {
         w[0][0] = f.alpha[0];
     }
     template <int IXY>
+    __device__ __forceinline__ static void zero_iface(const double (&)[NC], const double (&)[NC], const RPParams&,
+                                                      Iface& f) {
+        f.alpha[0] = 0.0;
+    }
+    template <int IXY>
     __device__ __forceinline__ static void solve(const double (&cL)[NC], const double (&cR)[NC], const RPParams& p,
                                                  Iface& f, double (&amdq)[MEQN], double (&apdq)[MEQN]) {
         const double vel = (IXY == 1) ? p.c[0] : p.c[1];
@@ -126,6 +131,11 @@ struct RPAcoustics {
         const double zz = p.c[3];
         w[0][0] = -f.alpha[0] * zz; w[0][MU] = f.alpha[0]; w[0][MV] = 0.0;
         w[1][0] = f.alpha[1] * zz;  w[1][MU] = f.alpha[1]; w[1][MV] = 0.0;
+    }
+    template <int IXY>
+    __device__ __forceinline__ static void zero_iface(const double (&)[NC], const double (&)[NC], const RPParams&,
+                                                      Iface& f) {
+        f.alpha[0] = f.alpha[1] = 0.0;
     }
     template <int IXY>
     __device__ __forceinline__ static void solve(const double (&cL)[NC], const double (&cR)[NC], const RPParams& p,
@@ -194,22 +204,43 @@ struct RPEulerRoe {
         w[3][0] = b4; w[3][MU] = b4 * (u + a); w[3][MV] = b4 * v; w[3][3] = b4 * (H + u * a);
     }
 
+    // Roe averages with weights sqrt(rho) / (sqrt(rho_L) + sqrt(rho_R)): the
+    // record's u, v, H, a, 1/a (everything but the wave strengths)
+    template <int IXY>
+    __device__ __forceinline__ static void roe_state(const double (&cL)[NC], const double (&cR)[NC],
+                                                     const RPParams& p, Iface& f) {
+        constexpr int UN = (IXY == 1) ? UX : UY, UT = (IXY == 1) ? UY : UX;
+        // explicit roundings: the record comes out bit for bit the same in
+        // every kernel that inlines this (the zero-jump shortcut and the full
+        // solve build it in different places), whatever the contraction
+        const double gamma1 = p.c[0] - 1.0;
+        const double inv = rcp_nr(__dadd_rn(cL[RS], cR[RS]));
+        const double wl = __dmul_rn(cL[RS], inv), wr = __dmul_rn(cR[RS], inv);
+        const double u = __fma_rn(wl, cL[UN], __dmul_rn(wr, cR[UN]));
+        const double v = __fma_rn(wl, cL[UT], __dmul_rn(wr, cR[UT]));
+        const double H = __fma_rn(wl, cL[HH], __dmul_rn(wr, cR[HH]));
+        const double a2 = __dmul_rn(gamma1, __fma_rn(-0.5, __fma_rn(u, u, __dmul_rn(v, v)), H));
+        const double ia = rsqrt(a2);
+        f.u = u; f.v = v; f.H = H; f.a = __dmul_rn(a2, ia); f.ia = ia;
+    }
+    // The record of an interface whose two cells are equal: every strength is
+    // zero (the jump is), the Roe state is solve's, so the speeds are too.
+    template <int IXY>
+    __device__ __forceinline__ static void zero_iface(const double (&cL)[NC], const double (&cR)[NC],
+                                                      const RPParams& p, Iface& f) {
+        roe_state<IXY>(cL, cR, p, f);
+        f.alpha[0] = f.alpha[1] = f.alpha[2] = f.alpha[3] = 0.0;
+    }
+
     template <int IXY>
     __device__ __forceinline__ static void solve(const double (&cL)[NC], const double (&cR)[NC], const RPParams& p,
                                                  Iface& f, double (&amdq)[MEQN], double (&apdq)[MEQN]) {
         constexpr int MU = Dir<IXY>::MU, MV = Dir<IXY>::MV;
-        constexpr int UN = (IXY == 1) ? UX : UY, UT = (IXY == 1) ? UY : UX;
+        constexpr int UN = (IXY == 1) ? UX : UY;
         const double gamma = p.c[0], gamma1 = gamma - 1.0;
-        // Roe averages with weights sqrt(rho) / (sqrt(rho_L) + sqrt(rho_R))
-        const double inv = rcp_nr(cL[RS] + cR[RS]);
-        const double wl = cL[RS] * inv, wr = cR[RS] * inv;
-        const double u = wl * cL[UN] + wr * cR[UN];
-        const double v = wl * cL[UT] + wr * cR[UT];
-        const double H = wl * cL[HH] + wr * cR[HH];
+        roe_state<IXY>(cL, cR, p, f);
+        const double u = f.u, v = f.v, H = f.H, a = f.a, ia = f.ia;
         const double u2v2 = u * u + v * v;
-        const double a2 = gamma1 * (H - 0.5 * u2v2);
-        const double ia = rsqrt(a2);
-        const double a = a2 * ia;
         const double g1a2 = gamma1 * ia * ia;
         const double euv = H - u2v2;
         const double d0 = cR[0] - cL[0], d1 = cR[MU] - cL[MU], d2 = cR[MV] - cL[MV], d3 = cR[3] - cL[3];
@@ -218,7 +249,6 @@ struct RPEulerRoe {
         const double b4 = (d1 + (a - u) * d0 - a * b3) * (0.5 * ia);
         const double b1 = d0 - b3 - b4;
         f.alpha[0] = b1; f.alpha[1] = b3; f.alpha[2] = b2; f.alpha[3] = b4;
-        f.u = u; f.v = v; f.a = a; f.ia = ia; f.H = H;
 
         double w[MWAVES][MEQN], s[MWAVES];
         waves<IXY>(f, p, w);
@@ -506,24 +536,42 @@ struct RPShallowRoe {
         w[2][0] = a3; w[2][MU] = a3 * (u + a); w[2][MV] = a3 * v;
     }
 
+    // Roe averages (velocities weighted by sqrt(h)) and the celerity of the
+    // mean depth: the record's u, v, a, 1/a
+    template <int IXY>
+    __device__ __forceinline__ static void roe_state(const double (&cL)[NC], const double (&cR)[NC],
+                                                     const RPParams& p, Iface& f) {
+        constexpr int UN = (IXY == 1) ? UX : UY, UT = (IXY == 1) ? UY : UX;
+        // explicit roundings (see RPEulerRoe::roe_state)
+        const double inv = rcp_nr(__dadd_rn(cL[RS], cR[RS]));
+        const double wl = __dmul_rn(cL[RS], inv), wr = __dmul_rn(cR[RS], inv);
+        const double gh = __dmul_rn(p.c[0], __dmul_rn(__dadd_rn(cL[0], cR[0]), 0.50));
+        const double ia = rsqrt(gh);
+        f.u = __fma_rn(wl, cL[UN], __dmul_rn(wr, cR[UN]));
+        f.v = __fma_rn(wl, cL[UT], __dmul_rn(wr, cR[UT]));
+        f.a = __dmul_rn(gh, ia);
+        f.ia = ia;
+    }
+    // equal cells: zero strengths, solve's Roe state (and so its speeds)
+    template <int IXY>
+    __device__ __forceinline__ static void zero_iface(const double (&cL)[NC], const double (&cR)[NC],
+                                                      const RPParams& p, Iface& f) {
+        roe_state<IXY>(cL, cR, p, f);
+        f.alpha[0] = f.alpha[1] = f.alpha[2] = 0.0;
+    }
+
     template <int IXY>
     __device__ __forceinline__ static void solve(const double (&cL)[NC], const double (&cR)[NC], const RPParams& p,
                                                  Iface& f, double (&amdq)[MEQN], double (&apdq)[MEQN]) {
         constexpr int MU = Dir<IXY>::MU, MV = Dir<IXY>::MV;
-        constexpr int UN = (IXY == 1) ? UX : UY, UT = (IXY == 1) ? UY : UX;
+        constexpr int UN = (IXY == 1) ? UX : UY;
         const double grav = p.c[0];
-        const double inv = rcp_nr(cL[RS] + cR[RS]);
-        const double wl = cL[RS] * inv, wr = cR[RS] * inv;
-        const double u = wl * cL[UN] + wr * cR[UN];
-        const double v = wl * cL[UT] + wr * cR[UT];
-        const double gh = grav * ((cL[0] + cR[0]) * 0.50);
-        const double ia = rsqrt(gh);
-        const double a = gh * ia;
+        roe_state<IXY>(cL, cR, p, f);
+        const double u = f.u, v = f.v, a = f.a, ia = f.ia;
         const double d0 = cR[0] - cL[0], d1 = cR[MU] - cL[MU], d2 = cR[MV] - cL[MV];
         f.alpha[0] = ((u + a) * d0 - d1) * (0.50 * ia);
         f.alpha[1] = -v * d0 + d2;
         f.alpha[2] = (-(u - a) * d0 + d1) * (0.50 * ia);
-        f.u = u; f.v = v; f.a = a; f.ia = ia;
 
         double w[MWAVES][MEQN], s[MWAVES];
         waves<IXY>(f, p, w);
@@ -1026,6 +1074,38 @@ struct AuxTraits<RP, decltype((void)RP::MAUX, void())> {
         RP::prepare_aux(q, aux, p, c);
     }
 };
+
+// Traits for the zero-jump shortcut.  Solvers with `zero_iface` (no aux data,
+// no guess) produce zero waves and zero fluctuations at an interface whose two
+// cells hold bitwise-equal q: every strength is a difference of equal numbers
+// (or a combination of such), so the limiter skips the waves (wnorm2 == 0,
+// limiter.f90:42), the correction and transverse terms are zero, and only the
+// speeds -- the Courant number -- remain; zero_iface builds that record.
+template <class RP, class = void>
+struct SkipTraits {
+    static constexpr bool OK = false;
+    template <int IXY>
+    __device__ __forceinline__ static void zero_iface(const double (&)[RP::NC], const double (&)[RP::NC],
+                                                      const RPParams&, typename RP::Iface&) {}
+};
+template <class RP>
+struct SkipTraits<RP, decltype((void)&RP::template zero_iface<1>, void())> {
+    static constexpr bool OK = true;
+    template <int IXY>
+    __device__ __forceinline__ static void zero_iface(const double (&cL)[RP::NC], const double (&cR)[RP::NC],
+                                                      const RPParams& p, typename RP::Iface& f) {
+        RP::template zero_iface<IXY>(cL, cR, p, f);
+    }
+};
+
+// true when the first ME entries (q itself) of two prepared cells are equal bit for bit
+template <int ME, int NC>
+__device__ __forceinline__ bool same_q(const double (&a)[NC], const double (&b)[NC]) {
+    bool eq = true;
+#pragma unroll
+    for (int m = 0; m < ME; ++m) eq = eq && (__double_as_longlong(a[m]) == __double_as_longlong(b[m]));
+    return eq;
+}
 
 // Traits for the optional per-interface guess and iteration count.
 template <class RP, class = void>

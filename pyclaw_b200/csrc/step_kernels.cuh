@@ -318,6 +318,17 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
     const double* ko = CAPA ? a.capa + cpl : nullptr;
     double pfk = CAPA ? __ldg(ko + (long long)R0 * pitch) : 1.0;
 
+    // Zero-jump shortcut (solvers without aux data or guesses, q-waves): when
+    // every lane of a warp has equal cells on both sides of its interface, the
+    // warp builds the interface's record with zero strengths and only the Roe
+    // state the Courant number needs, and skips the finish (limiter,
+    // correction, transverse solves), whose increments are all zero.  Warp-
+    // uniform decisions, so no lane diverges; the results equal the full
+    // path's up to the sign of zero terms.
+    constexpr bool ZS = SkipTraits<RP>::OK && MA == 0 && !CAPA && !GuessTraits<RP>::USES;
+    const bool zs = ZS && (SPEC != SPEC_ANY || a.meth.fwave == 0);
+    bool zY = false;  // the y-interface being finished, (R-2 | R-1), is zero in the whole warp
+
     // (the copy needs a 128-byte aligned destination; anything else loads
     // directly; solvers with aux data load directly)
     const bool tma = (MA == 0) && !CAPA && (tm != nullptr) && ((smem_u32(qrow) & 127u) == 0);
@@ -439,15 +450,22 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
             }
             Iface fN;
             double amN[ME], apN[ME];
-            double gy = 0.0;
-            if (GuessTraits<RP>::USES && a.guess) gy = a.guess[plane + (long long)R * pitch + cpl];
-            GuessTraits<RP>::template solve<2>(cB, cA, P, gy, fN, amN, apN);
-            if (GuessTraits<RP>::USES && cp <= mx + 3) {
-                n_it += GuessTraits<RP>::count(fN);
-                n_solve += 1;
-            }
             double dn[MW];
-            {
+            const bool zN = zs && __all_sync(0xffffffffu, same_q<ME, NC>(cB, cA));
+            if (ZS && zN) {
+                SkipTraits<RP>::template zero_iface<2>(cB, cA, P, fN);
+#pragma unroll
+                for (int m = 0; m < ME; ++m) amN[m] = apN[m] = 0.0;
+#pragma unroll
+                for (int k = 0; k < MW; ++k) dn[k] = 0.0;
+            } else {
+                double gy = 0.0;
+                if (GuessTraits<RP>::USES && a.guess) gy = a.guess[plane + (long long)R * pitch + cpl];
+                GuessTraits<RP>::template solve<2>(cB, cA, P, gy, fN, amN, apN);
+                if (GuessTraits<RP>::USES && cp <= mx + 3) {
+                    n_it += GuessTraits<RP>::count(fN);
+                    n_solve += 1;
+                }
                 double wY[MW][ME], wN[MW][ME];
                 RP::template waves<2>(fY, P, wY);
                 RP::template waves<2>(fN, P, wN);
@@ -464,6 +482,9 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
                 const double ydl = CAPA ? dtdy * S.icap[s0][t] : dtdy, ydr = CAPA ? dtdy * S.icap[s1][t] : dtdy;
                 if (ycfl_col)
                     cfl = fmax(cfl, CAPA ? iface_cfl2<RP, 2>(fY, P, ydl, ydr) : iface_cfl<RP, 2>(fY, P, dtdy));
+            }
+            if (R >= R0 + 3 && !(ZS && zY)) {
+                const double ydl = CAPA ? dtdy * S.icap[s0][t] : dtdy, ydr = CAPA ? dtdy * S.icap[s1][t] : dtdy;
                 double cq[ME];
                 if (order != 1) {
                     correction<RP, 2, SPEC>(fY, P, a.meth, CAPA ? 0.5 * (ydl + ydr) : dtdy, dY, dn, cq);
@@ -524,6 +545,7 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
                 }
             }
             fY = fN;
+            zY = zN;
 #pragma unroll
             for (int m = 0; m < ME; ++m) { amY[m] = amN[m]; apY[m] = apN[m]; }
 #pragma unroll
@@ -543,6 +565,7 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
         const bool xrow = (R > R0) && (R < R1);  // rows R0+1 .. R1-1
         Iface fX;
         double amX[ME], apX[ME];
+        bool zX = false;
         {
             double cL[NC], cR[NC];
 #pragma unroll
@@ -550,6 +573,16 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
                 cL[k] = S.cell[s2][k][tl];
                 cR[k] = S.cell[s2][k][t];
             }
+            zX = zs && __all_sync(0xffffffffu, same_q<ME, NC>(cL, cR));
+            if (ZS && zX) {
+                SkipTraits<RP>::template zero_iface<1>(cL, cR, P, fX);
+#pragma unroll
+                for (int m = 0; m < ME; ++m) amX[m] = apX[m] = 0.0;
+#pragma unroll
+                for (int k = 0; k < MW; ++k)
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) S.w[k][m][t] = 0.0;
+            } else {
             double gx = 0.0;
             if (GuessTraits<RP>::USES && a.guess) gx = a.guess[(long long)R * pitch + cpl];
             GuessTraits<RP>::template solve<1>(cL, cR, P, gx, fX, amX, apX);
@@ -563,6 +596,7 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
             for (int k = 0; k < MW; ++k)
 #pragma unroll
                 for (int m = 0; m < ME; ++m) S.w[k][m][t] = wX[k][m];
+            }
         }
         __syncthreads();  // S2: x-waves of row R visible
 
@@ -573,6 +607,9 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
             // capacity form: dt/(dx kappa) of the cells left (cp-1) and right (cp)
             const double xdl = CAPA ? dtdx * S.icap[s2][tl] : dtdx, xdr = CAPA ? dtdx * S.icap[s2][t] : dtdx;
             if (xcfl_col) cfl = fmax(cfl, CAPA ? iface_cfl2<RP, 1>(fX, P, xdl, xdr) : iface_cfl<RP, 1>(fX, P, dtdx));
+        }
+        if (xrow && !(ZS && zX)) {
+            const double xdl = CAPA ? dtdx * S.icap[s2][tl] : dtdx, xdr = CAPA ? dtdx * S.icap[s2][t] : dtdx;
             double cq[ME];
             if (order != 1) {
                 double dl[MW], dr[MW];

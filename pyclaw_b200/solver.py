@@ -1,11 +1,18 @@
-"""Solver base class: time-step control, accept/reject and the BC enumeration.
+"""Time-step control of the CUDA solvers: the attempt loop, accept/reject, the
+dt rule, gauges and the boundary-condition codes.
 
-Host mirror of src/pyclaw/solver.py.  The dt rules (get_dt :535-552,
-get_dt_new :531-533, accept_reject_step :524-529) and the evolve_to_time loop
-(:554-666) follow the reference line for line.  Two hooks replace the
-reference's host copies: ``_begin_step`` (its ``q_backup = state.q.copy('F')``,
-:610-612) and ``_end_step(accept)`` (its ``state.q = q_backup`` on reject,
-:641-645); the CUDA solver implements both as a buffer swap on the device.
+What a drop-in must reproduce is the sequence of attempts a run makes, since
+that fixes every dt and therefore every result: the next dt follows from the
+last Courant number (src/pyclaw/solver.py:531-552), it is clipped to the target
+time, an attempt whose Courant number exceeds cfl_max is rejected and retaken
+with the smaller dt, and a fixed dt must divide the interval (:574-594).  Those
+rules are the functions `next_dt`, `clip_to_target` and the `AttemptBudget`
+below.  The loop around them is this package's own: q stays on the GPU, so the
+backup the reference copies before every attempt (:610-612) is a buffer the
+device already keeps (`_begin_step` / `_end_step`, implemented by the CUDA
+solver as accept = buffer swap), and a run with no host callback between
+steps never enters this loop at all -- ClawSolver2D.evolve_to_time hands it,
+with the same budget, to the device time loop (claw2_patch_evolve).
 """
 import logging
 
@@ -13,14 +20,13 @@ import numpy as np
 
 
 class CFLError(Exception):
-    """Raised when cfl_max is exceeded with a fixed time step (solver.py:7-11)."""
-
-    def __init__(self, msg):
-        super(CFLError, self).__init__(msg)
+    """A fixed-dt attempt broke cfl_max: the run cannot continue (the
+    reference raises a plain Exception there, solver.py:646-650)."""
 
 
 class BC():
-    """Boundary-condition names (solver.py:13-19)."""
+    """Boundary-condition codes of the solver's bc_lower/bc_upper lists
+    (solver.py:13-19; the numbers are the ones the C ABI takes)."""
     custom = 0
     extrap = 1
     periodic = 2
@@ -35,15 +41,74 @@ def before_step(solver, solution):
     pass
 
 
+# ---- the dt rules -----------------------------------------------------------
+def next_dt(dt, cfl, cfl_desired, dt_max):
+    """dt of the next attempt after one of Courant number `cfl`: scaled to
+    cfl_desired (solver.py:531-533, same operation order), or dt_max when
+    nothing moved (cfl == 0, :541-542)."""
+    if cfl > 0.0:
+        return min(dt_max, dt * cfl_desired / cfl)
+    return dt_max
+
+
+def clip_to_target(dt, t, tstart, tend):
+    """Never step past tend, and take the remainder rather than leave a
+    sliver below 1e-14 t before it (solver.py:547-551)."""
+    if tstart < tend and t + dt > tend:
+        dt = tend - t
+    if tend - t - dt < 1.e-14 * t:
+        dt = tend - t
+    return dt
+
+
+class AttemptBudget(object):
+    """The attempts one evolve_to_time call may make, checked before the first
+    one (solver.py:574-595).  A fixed dt allows exactly (tend - tstart) / dt of
+    them and must divide the interval; a variable dt needs cfl_desired <=
+    cfl_max (otherwise no attempt could be accepted) and may use max_steps; a
+    target at or before the start allows none.  As in the reference the count
+    is stored in solver.max_steps, where later calls see it."""
+
+    def __init__(self, solver, tstart, tend):
+        self.one_step = tend is None
+        count = solver.max_steps
+        if not solver.dt_variable:
+            if self.one_step:
+                count = 1
+            else:
+                span = tend - tstart
+                count = int((span + 1e-10) / solver.dt)
+                if abs(count * solver.dt - span) > 1e-5 * span:
+                    raise Exception("a fixed dt of %.17g does not divide the interval %.17g -> %.17g "
+                                    "(dt_variable is False)" % (float(solver.dt), float(tstart), float(tend)))
+        if solver.dt_variable == 1 and solver.cfl_desired > solver.cfl_max:
+            raise Exception("cfl_desired = %g is above cfl_max = %g: with a variable dt every attempt "
+                            "would be rejected" % (solver.cfl_desired, solver.cfl_max))
+        if not self.one_step and tend <= tstart:
+            solver.logger.info("target time %r is not after the current time %r: nothing to do",
+                               tend, tstart)
+            count = 0
+        solver.max_steps = count
+        self.count = count
+
+    def check_finished(self, solver, t, tend, accepted):
+        """A variable-dt run that used its whole budget short of tend fails
+        (solver.py:662-665)."""
+        if not self.one_step and solver.dt_variable and t < tend and accepted == self.count:
+            raise Exception("max_steps = %d steps taken, stopped at t = %.17g short of tend = %.17g"
+                            % (self.count, float(t), float(tend)))
+
+
 class Solver(object):
-    """Abstract solver; see ClawSolver2D (solver.py:32-242)."""
+    """Solver base (the attribute surface of solver.py:32-242).
+
+    Attributes are fixed once __init__ has run: assigning a name the solver
+    does not have raises TypeError, so a misspelt option fails at once
+    instead of being ignored."""
 
     def __setattr__(self, key, value):
-        # reject attributes that do not exist once initialised (solver.py:139-144)
-        if not hasattr(self, '_isinitialized'):
-            self.__dict__['_isinitialized'] = False
-        if self._isinitialized and not hasattr(self, key):
-            raise TypeError("%s has no attribute %s" % (self.__class__, key))
+        if self.__dict__.get('_frozen', False) and not hasattr(self, key):
+            raise TypeError("%s has no option %r (misspelt?)" % (type(self).__name__, key))
         object.__setattr__(self, key, value)
 
     @property
@@ -51,73 +116,60 @@ class Solver(object):
         return self.bc_lower, self.bc_upper
 
     @all_bcs.setter
-    def all_bcs(self, all_bcs):
-        for i in range(self.num_dim):
-            self.bc_lower[i] = all_bcs
-            self.bc_upper[i] = all_bcs
+    def all_bcs(self, code):
+        for d in range(self.num_dim):
+            self.bc_lower[d] = code
+            self.bc_upper[d] = code
 
     def __init__(self, riemann_solver=None, claw_package=None):
         from .cfl import CFL
-        self.logger = logging.getLogger('pyclaw.solver')
-        self.dt_initial = 0.1
-        self.dt_max = 1e99
-        self.max_steps = 10000
-        self.dt_variable = True
-        self.num_waves = None
-        self.qbc = None
-        self.auxbc = None
-        self.rp = None
-        self.fmod = None
-        self._is_set_up = False
-        self._use_old_bc_sig = False
-        self.accept_step = True
-        self.before_step = None
+        nd = self.num_dim
+        defaults = dict(
+            logger=logging.getLogger('pyclaw.solver'),
+            dt_initial=0.1, dt_max=1e99, max_steps=10000, dt_variable=True,
+            num_eqn=None, num_waves=None, fwave=None, rp=None, fmod=None,
+            qbc=None, auxbc=None, accept_step=True, before_step=None,
+            user_bc_lower=None, user_bc_upper=None, user_aux_bc_lower=None, user_aux_bc_upper=None,
+            compute_gauge_values=default_compute_gauge_values,
+            _is_set_up=False, _use_old_bc_sig=False)
+        for k, v in defaults.items():
+            object.__setattr__(self, k, v)
+        self.bc_lower, self.bc_upper = [None] * nd, [None] * nd
+        self.aux_bc_lower, self.aux_bc_upper = [None] * nd, [None] * nd
         self.dt = self.dt_initial
         self.cfl = CFL(self.cfl_desired)
         self.status = {'cflmax': -np.inf, 'dtmin': np.inf, 'dtmax': -np.inf, 'numsteps': 0}
-        self.bc_lower = [None] * self.num_dim
-        self.bc_upper = [None] * self.num_dim
-        self.aux_bc_lower = [None] * self.num_dim
-        self.aux_bc_upper = [None] * self.num_dim
-        self.user_bc_lower = None
-        self.user_bc_upper = None
-        self.user_aux_bc_lower = None
-        self.user_aux_bc_upper = None
-        self.num_eqn = None
-        self.num_waves = None
-        self.fwave = None
-        self.compute_gauge_values = default_compute_gauge_values
         if riemann_solver is not None:
-            # num_eqn/num_waves/fwave from riemann.static (solver.py:230-238)
-            from . import riemann
-            self.rp = riemann_solver
-            rp_name = riemann_solver.__name__.split('.')[-1]
-            if "ptwise" in rp_name:
-                rp_name = rp_name.replace("_ptwise", "")
-            self.num_eqn = riemann.static.num_eqn.get(rp_name, None)
-            self.num_waves = riemann.static.num_waves.get(rp_name, None)
-            self.fwave = riemann.static.fwave.get(rp_name, None)
-        self._isinitialized = True
-        super(Solver, self).__init__()
+            self._adopt_riemann(riemann_solver)
+        self._frozen = True
+
+    def _adopt_riemann(self, rp):
+        """num_eqn, num_waves and fwave from the solver tables, keyed by the
+        module's last name with any '_ptwise' dropped (solver.py:230-238)."""
+        from . import riemann
+        name = rp.__name__.split('.')[-1].replace("_ptwise", "")
+        self.rp = rp
+        self.num_eqn = riemann.static.num_eqn.get(name)
+        self.num_waves = riemann.static.num_waves.get(name)
+        self.fwave = riemann.static.fwave.get(name)
 
     def is_valid(self):
-        """Required-attribute checks (solver.py:262-293)."""
-        valid, reason = True, None
-        if any(b == BC.custom for b in self.bc_lower) and self.user_bc_lower is None:
-            valid, reason = False, 'Lower custom BC function has not been set.'
-        if any(b == BC.custom for b in self.bc_upper) and self.user_bc_upper is None:
-            valid, reason = False, 'Upper custom BC function has not been set.'
-        if self.num_waves is None:
-            valid, reason = False, 'solver.num_waves has not been set.'
-        if self.num_eqn is None:
-            valid, reason = False, 'solver.num_eqn has not been set.'
-        if self.fwave is None:
-            valid, reason = False, 'solver.fwave has not been set.'
-        if (None in self.bc_lower) or (None in self.bc_upper):
-            valid, reason = False, 'One of the boundary conditions has not been set.'
+        """(valid, reason): every setting a run needs is present
+        (solver.py:262-293).  The reason names the first missing one."""
+        missing = []
+        for side, codes, fn in (("lower", self.bc_lower, self.user_bc_lower),
+                                ("upper", self.bc_upper, self.user_bc_upper)):
+            if any(b == BC.custom for b in codes) and fn is None:
+                missing.append("a %s boundary is BC.custom but user_bc_%s is not set" % (side, side))
+        for name in ('num_waves', 'num_eqn', 'fwave'):
+            if getattr(self, name) is None:
+                missing.append("solver.%s is not set" % name)
+        if None in self.bc_lower or None in self.bc_upper:
+            missing.append("bc_lower/bc_upper has an unset entry")
+        reason = missing[0] if missing else None
         if reason is not None:
             self.logger.debug(reason)
-        return valid, reason
+        return reason is None, reason
 
     def setup(self, solution):
         self._is_set_up = True
@@ -126,133 +178,112 @@ class Solver(object):
         self._is_set_up = False
 
     def __str__(self):
-        out = "Solver Status:\n"
-        for (k, v) in self.status.items():
-            out = "\n".join((out, "%s = %s" % (k.rjust(25), v)))
-        return out
+        return "Solver Status:\n" + "\n".join("%25s = %s" % (k, v) for k, v in self.status.items())
 
-    # ---- time stepping (solver.py:524-666) ---------------------------------
+    # ---- dt and the accept test -------------------------------------------
     def accept_reject_step(self, state):
-        cfl = self.cfl.get_cached_max()
-        if cfl > self.cfl_max:
-            return False
-        else:
-            return True
+        """Accept an attempt whose Courant number is within cfl_max."""
+        return not (self.cfl.get_cached_max() > self.cfl_max)
 
     def get_dt_new(self):
-        cfl = self.cfl.get_cached_max()
-        self.dt = min(self.dt_max, self.dt * self.cfl_desired / cfl)
+        self.dt = next_dt(self.dt, self.cfl.get_cached_max(), self.cfl_desired, self.dt_max)
 
     def get_dt(self, t, tstart, tend, take_one_step):
-        cfl = self.cfl.get_cached_max()
+        """dt for the coming attempt (solver.py:535-552): the first call of a
+        variable-dt solver keeps dt (and records it as dt_old); later calls
+        scale it by the last Courant number; a run to a target time is then
+        clipped to it."""
         if self.dt_variable and self.dt_old is not None:
+            cfl = self.cfl.get_cached_max()
+            self.dt = next_dt(self.dt, cfl, self.cfl_desired, self.dt_max)
             if cfl > 0.0:
-                self.get_dt_new()
                 self.status['dtmin'] = min(self.dt, self.status['dtmin'])
                 self.status['dtmax'] = max(self.dt, self.status['dtmax'])
-            else:
-                self.dt = self.dt_max
         else:
             self.dt_old = self.dt
         if not take_one_step:
-            if t + self.dt > tend and tstart < tend:
-                self.dt = tend - t
-            if tend - t - self.dt < 1.e-14 * t:
-                self.dt = tend - t
+            self.dt = clip_to_target(self.dt, t, tstart, tend)
 
+    # ---- the attempt loop --------------------------------------------------
     def _begin_step(self, solution):
-        """Keep what a rejected step must restore (solver.py:610-612)."""
+        """Keep what a rejected attempt must restore (the CUDA solver keeps
+        the old q on the device; nothing to copy)."""
 
     def _end_step(self, solution, accept):
-        """Commit or roll back the step just taken (solver.py:619-651)."""
+        """Commit or drop the attempt just taken."""
 
     def evolve_to_time(self, solution, tend=None):
+        """Advance `solution` to `tend`, or by one accepted-or-rejected attempt
+        when tend is None (solver.py:554-666).  Returns the status dict."""
         if not self._is_set_up:
             self.setup(solution)
-        take_one_step = tend is None
         tstart = solution.t
-        num_steps = 0
-        if not self.dt_variable:
-            if take_one_step:
-                self.max_steps = 1
-            else:
-                self.max_steps = int((tend - tstart + 1e-10) / self.dt)
-                if abs(self.max_steps * self.dt - (tend - tstart)) > 1e-5 * (tend - tstart):
-                    raise Exception('dt does not divide (tend-tstart) and dt is fixed!')
-        if self.dt_variable == 1 and self.cfl_desired > self.cfl_max:
-            raise Exception('Variable time-stepping and desired CFL > maximum CFL')
-        if not take_one_step:
-            if tend <= tstart:
-                self.logger.info("Already at or beyond end time: no evolution required.")
-                self.max_steps = 0
-
-        for n in range(self.max_steps):
-            state = solution.state
-            if self.dt_variable:
-                self._begin_step(solution)
-                told = solution.t
-            if self.before_step is not None:
-                self.before_step(self, solution.states[0])
-            self.step(solution, take_one_step, tstart, tend)
-            cfl = self.cfl.get_cached_max()
-            self.accept_step = self.accept_reject_step(state)
-            if self.accept_step:
-                self._end_step(solution, True)
-                self.status['cflmax'] = max(cfl, self.status['cflmax'])
-                if self.dt_variable:
-                    solution.t += self.dt
-                else:
-                    solution.t = tstart + (n + 1) * self.dt
-                self.logger.debug("Step %i  CFL = %f   dt = %f   t = %f" % (n, cfl, self.dt, solution.t))
-                self.write_gauge_values(solution)
-                num_steps += 1
-                self.status['numsteps'] += 1
-            else:
-                self.logger.debug("Rejecting time step, CFL number too large")
-                if self.dt_variable:
-                    self._end_step(solution, False)
-                    solution.t = told
-                else:
-                    self._end_step(solution, False)
-                    self.status['cflmax'] = max(cfl, self.status['cflmax'])
-                    raise CFLError('CFL too large, giving up!')
-            if take_one_step:
+        budget = AttemptBudget(self, tstart, tend)
+        accepted = 0
+        for n in range(budget.count):
+            accepted += self._attempt(solution, n, tstart, tend, budget.one_step)
+            if budget.one_step or solution.t >= tend:
                 break
-            elif solution.t >= tend:
-                break
-
-        if not take_one_step:
-            if self.dt_variable and solution.t < tend and num_steps == self.max_steps:
-                raise Exception("Maximum number of timesteps have been taken")
+        budget.check_finished(self, solution.t, tend, accepted)
         return self.status
 
-    def step(self, solution, take_one_step, tstart, tend):
-        raise NotImplementedError("No stepping routine has been defined!")
+    def _attempt(self, solution, n, tstart, tend, one_step):
+        """One attempt: hooks, the step (which picks dt), the Courant test,
+        then commit (t advanced, gauges written) or roll back.  Returns 1 when
+        accepted; a rejected fixed-dt attempt raises CFLError."""
+        if self.dt_variable:
+            self._begin_step(solution)
+        if self.before_step is not None:
+            self.before_step(self, solution.states[0])
+        self.step(solution, one_step, tstart, tend)
+        cfl = self.cfl.get_cached_max()
+        self.accept_step = self.accept_reject_step(solution.state)
+        self._end_step(solution, self.accept_step)
+        if not self.accept_step:
+            self.logger.debug("attempt %d rejected: Courant number %g > %g", n, cfl, self.cfl_max)
+            if self.dt_variable:
+                return 0
+            self.status['cflmax'] = max(cfl, self.status['cflmax'])
+            raise CFLError("Courant number %.17g above cfl_max = %g with a fixed dt of %.17g"
+                           % (float(cfl), self.cfl_max, float(self.dt)))
+        self.status['cflmax'] = max(cfl, self.status['cflmax'])
+        # a fixed dt advances by whole multiples of dt from tstart (no drift)
+        solution.t = solution.t + self.dt if self.dt_variable else tstart + (n + 1) * self.dt
+        self.logger.debug("attempt %d accepted: Courant number %g, dt %g, t %g", n, cfl, self.dt, solution.t)
+        self.write_gauge_values(solution)
+        self.status['numsteps'] += 1
+        return 1
 
+    def step(self, solution, take_one_step, tstart, tend):
+        raise NotImplementedError("%s defines no step()" % type(self).__name__)
+
+    # ---- gauges -------------------------------------------------------------
     def write_gauge_values(self, solution):
-        """Values of compute_gauge_values(q, aux) at every gauge cell, appended
-        to state.gauge_data (keep_gauges) and to the gauge files
-        (solver.py:680-715).  q at the gauge cells is gathered on the device."""
+        """One line per gauge and accepted step: t followed by
+        compute_gauge_values(q, aux) at the gauge's cell, appended to the
+        gauge's file and (keep_gauges) to state.gauge_data, in the
+        reference's line format (solver.py:680-715).  The gauge cells' q is
+        gathered on the device in one call."""
         state = solution.state
-        gauges = state.grid.gauges
-        if not gauges:
+        cells = [tuple(g) for g in state.grid.gauges]
+        if not cells:
             return
-        qg = state.gauge_q([tuple(g) for g in gauges])
-        for i, (ix, iy) in enumerate(gauges):
+        t = solution.t
+        qg = state.gauge_q(cells)
+        data = state.gauge_data
+        first = len(data) != len(cells)
+        files = state.grid.gauge_files
+        for i, (ix, iy) in enumerate(cells):
             aux = state.aux[:, ix, iy] if state.num_aux > 0 else None
-            p = self.compute_gauge_values(qg[i], aux)
-            if not hasattr(p, '__iter__'):
-                p = [p]
-            t = solution.t
+            vals = self.compute_gauge_values(qg[i], aux)
+            vals = list(vals) if hasattr(vals, '__iter__') else [vals]
+            row = np.append(t, vals)
             if state.keep_gauges:
-                gauge_data = state.gauge_data
-                if len(gauge_data) == len(gauges):
-                    gauge_data[i] = np.vstack((gauge_data[i], np.append(t, p)))
+                if first:
+                    data.append(row)
                 else:
-                    gauge_data.append(np.append(t, p))
-            try:
-                state.grid.gauge_files[i].write(str(t) + ' ' + ' '.join(str(j) for j in p) + '\n')
-            except IOError:
-                raise Exception("Gauge files are not set up correctly. You should call \nthe method "
-                                "`setup_gauge_files` of the Grid class object \nbefore any call for "
-                                "`write_gauge_values` from the Solver class.")
+                    data[i] = np.vstack((data[i], row))
+            if i >= len(files):
+                raise Exception("gauge %d has no open file: call grid.setup_gauge_files(outdir) "
+                                "before stepping" % i)
+            files[i].write(" ".join([str(t)] + [str(v) for v in vals]) + "\n")

@@ -1,8 +1,9 @@
 """Extract the reference's own 2D classic regression goldens into
 tests/golden/reference_goldens.npz.
 
-Run in a container where the reference tree is mounted (default
-/root/reference, or pass its path).  Sources, all produced by the reference's
+Run where the reference tree is mounted, with its path as the argument or in
+the environment variable CLAW_REFERENCE:
+    python tests/golden/make_golden.py <path to the reference tree>  Sources, all produced by the reference's
 Fortran step2/step2ds with clawpack/riemann solvers:
   examples/advection_2d/expected_sols.npy            (test_2d_advection.py:9-35)
   examples/acoustics_2d_homogeneous/verify_classic.txt (test_2d_acoustics.py:6-15)
@@ -26,7 +27,9 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CLAW_REFERENCE")
+if not REF:
+    sys.exit("usage: make_golden.py <path to the reference tree> (or set CLAW_REFERENCE)")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_goldens.npz")
 
 

@@ -3,12 +3,16 @@ persistent kernel per step with device-side accept/reject and dt, the steps
 captured in a CUDA graph.
 
 Every problem's result must equal the single-problem CUDA path (which is
-itself parity-checked against the oracle) -- bitwise, because a cell's
-increments are summed in the same order whatever the tile shape -- and the
-graph run must equal the plain one-launch-sequence-per-problem loop."""
+itself parity-checked against the oracle): a cell's increments are summed in
+the same order whatever the tile shape, but the batched kernel is its own
+instantiation of the tile code and the compiler may fuse a multiply-add
+differently there, so to a few units in the last place (1e-13 relative) with
+the same step counts; and the graph run must equal the plain
+one-launch-sequence-per-problem loop bit for bit (the same kernel)."""
 import numpy as np
 import pytest
 
+from helpers import max_rel
 from pyclaw_b200 import workloads
 from pyclaw_b200.batch import Batch, autotune_rows
 
@@ -48,8 +52,8 @@ def test_batch_graph_equals_plain_loop_and_single_problems():
         s.dt = s.dt_initial
         for _ in range(nsteps):
             s.evolve_to_time(sol)
-        assert sol.t == st_graph["t"][i]
-        assert np.array_equal(sol.state.get_q_global(), q_graph[i])
+        assert abs(sol.t - st_graph["t"][i]) <= 1e-13 * sol.t
+        assert max_rel(sol.state.get_q_global(), q_graph[i]) <= 1e-13
 
 
 def test_batch_rejects_and_retakes_per_problem():
