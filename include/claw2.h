@@ -258,8 +258,10 @@ int claw2_patch_launch_count(claw2_patch* p, long long* n);
 
 /* Launch shape of the unsplit step kernel for one Riemann solver: variant 0
  * compiles for 2 blocks per SM (no register cap), 1 for 3 blocks per SM,
- * 2 and 3 the same with rows staged by TMA, 4 the two-barrier tile;
- * rows = row-block height (0 = heuristic).  Process-wide; set by an autotuner
+ * 2 and 3 the same with rows staged by TMA, 4 the two-barrier tile, 8 the
+ * direction-split tile (two threads per column: one for the y-interfaces, one
+ * for the x-interfaces; solvers without aux data, no capacity form, others
+ * run variant 0); rows = row-block height (0 = heuristic).  Process-wide; set by an autotuner
  * (pyclaw_b200.tune) or by hand. */
 int claw2_tune_set(int riemann, int variant, int rows);
 int claw2_tune_get(int riemann, int* variant, int* rows);

@@ -190,7 +190,8 @@ void smem_attr(K kernel, int bytes, unsigned long long& done) {
 // claw2_autotune) or the heuristic default.
 struct UnsplitShape {
     int variant;  // bit 0: 3 blocks/SM (register cap) instead of 2; bit 1: TMA row staging;
-                  // 4: the two-barrier tile (deferred x finish)
+                  // 4: the two-barrier tile (deferred x finish); 8: the direction-split
+                  // tile (two threads per column)
     int rows;
 };
 
@@ -241,6 +242,35 @@ void launch_unsplit2_s(const StepArgs& b, dim3 grid, cudaStream_t st) {
     k_step_unsplit2<RP, NT_UNSPLIT, 2, SPEC, CAPA, EVO><<<grid, NT_UNSPLIT, smem, st>>>(b);
 }
 
+// The direction-split tile (two threads per column, 2 CTAs of 256 threads
+// per SM).  For the Euler solvers the Y warps take 136 registers and the X
+// warps 120 (setmaxnreg), which needs exactly 128 registers per thread at
+// launch: checked once per kernel, and a kernel built otherwise is not
+// launched (the caller falls back to the one-thread tile).
+template <class RP> struct WSRegs { static constexpr int Y = 0, X = 0; };
+template <> struct WSRegs<RPEulerRoe> { static constexpr int Y = 136, X = 120; };
+static_assert(WSRegs<RPEulerRoe>::Y * NT_UNSPLIT + WSRegs<RPEulerRoe>::X * NT_UNSPLIT == 2 * NT_UNSPLIT * 128,
+              "the warpgroups' register shares must add up to the launch's 128 per thread");
+
+template <class RP, int SPEC, bool EVO>
+bool launch_unsplit_ws_s(const StepArgs& b, dim3 grid, cudaStream_t st) {
+    constexpr int smem = (int)sizeof(UnsplitSmemWS<RP, NT_UNSPLIT>);
+    constexpr int RY = WSRegs<RP>::Y, RX = WSRegs<RP>::X;
+    auto kern = k_step_unsplit_ws<RP, NT_UNSPLIT, 2, SPEC, EVO, RY, RX>;
+    if (RY > 0) {
+        static int regs = -1;
+        if (regs < 0) {
+            cudaFuncAttributes fa;
+            regs = (cudaFuncGetAttributes(&fa, kern) == cudaSuccess) ? fa.numRegs : 0;
+        }
+        if (regs != 128) return false;
+    }
+    static unsigned long long attr = 0;
+    smem_attr(kern, smem, attr);
+    kern<<<grid, 2 * NT_UNSPLIT, smem, st>>>(b);
+    return true;
+}
+
 // The capacity form (any method, rows loaded directly).
 template <class RP, bool EVO>
 void launch_unsplit_capa(const StepArgs& b, dim3 grid, cudaStream_t st) {
@@ -263,6 +293,13 @@ void launch_unsplit_v(const StepArgs& a, cudaStream_t st, const CUtensorMap* tm)
     }
     const int nbk = (a.L.my + b.H - 1) / b.H;
     dim3 grid(b.nstrips * nbk);
+    if constexpr (AuxTraits<RP>::MAUX == 0 && !GuessTraits<RP>::USES) {
+        if ((g_tune[RP::ID & (TUNE_SLOTS - 1)].variant & 8) && !a.capa) {  // the direction-split tile
+            const bool ok = is_mc2(a.meth, RP::MWAVES) ? launch_unsplit_ws_s<RP, SPEC_MC2, EVO>(b, grid, st)
+                                                       : launch_unsplit_ws_s<RP, SPEC_ANY, EVO>(b, grid, st);
+            if (ok) return;
+        }
+    }
     if (g_tune[RP::ID & (TUNE_SLOTS - 1)].variant & 4) {  // the two-barrier tile
         if (a.capa) launch_unsplit2_s<RP, SPEC_ANY, true, EVO>(b, grid, st);
         else if (is_mc2(a.meth, RP::MWAVES)) launch_unsplit2_s<RP, SPEC_MC2, false, EVO>(b, grid, st);
@@ -1855,7 +1892,8 @@ int claw2_selftest_lpt(int device, int n, unsigned long long seed, int* mismatch
 int claw2_tune_set(int riemann, int variant, int rows) {
     int me = 0, mw = 0;
     if (rp_shape(riemann, &me, &mw) != 0) return fail(CLAW2_EINVAL, "unknown Riemann solver id %d", riemann);
-    if (variant < 0 || variant > 4) return fail(CLAW2_EINVAL, "variant must be 0..4 (got %d)", variant);
+    if (variant < 0 || (variant > 4 && variant != 8))
+        return fail(CLAW2_EINVAL, "variant must be 0..4 or 8 (got %d)", variant);
     if (rows < 0 || rows > 4096) return fail(CLAW2_EINVAL, "rows must be 0..4096 (got %d)", rows);
     g_tune[riemann & (TUNE_SLOTS - 1)].variant = variant;
     g_tune[riemann & (TUNE_SLOTS - 1)].rows = rows;

@@ -573,7 +573,8 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
                 cL[k] = S.cell[s2][k][tl];
                 cR[k] = S.cell[s2][k][t];
             }
-            zX = zs && __all_sync(0xffffffffu, same_q<ME, NC>(cL, cR));
+            // (the first and last rows' x-interfaces are never finished: no solve)
+            zX = ZS && (!xrow || (zs && __all_sync(0xffffffffu, same_q<ME, NC>(cL, cR))));
             if (ZS && zX) {
                 SkipTraits<RP>::template zero_iface<1>(cL, cR, P, fX);
 #pragma unroll
@@ -1105,6 +1106,406 @@ __global__ void __launch_bounds__(NT, MINB) k_step_unsplit2(const StepArgs a) {
     if (a.tile_cost && threadIdx.x == 0) t0 = clock64();
     double cfl = 0.0;
     unsplit_tile2<RP, NT, SPEC, CAPA, EVO>(a, tile % a.nstrips, (tile / a.nstrips) * a.H, S, cfl);
+    cfl_commit(cfl, S.red, a.cfl_bits);
+    if (a.tile_cost && threadIdx.x == 0) {
+        const long long c = clock64() - t0;
+        a.tile_cost[tile] = (unsigned int)(c < 0 ? 0 : (c > 0xffffffffll ? 0xffffffffll : c));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The direction-split tile: two threads per column.  The CTA has 2*NT
+// threads; the first NT (the Y warps) own the y-interfaces of their column
+// and the second NT (the X warps) its x-interfaces, so each thread carries
+// half the live state of unsplit_tile and twice as many warps fit on an SM
+// (16 instead of 8 for Euler), which is what the FP64 pipe of a latency-bound
+// step needs.  The two warp groups are decoupled by named barriers instead
+// of CTA-wide ones, so one group may run up to two rows ahead of the other
+// and rows where only one direction has work do not stall the other:
+//   Y, row R: [wait EMPTY(R-2)] prepare the column's cell of row R into a
+//      4-row ring, prefetch row R+1, [arrive CELLS(R)]; solve (R-1 | R);
+//      finish (R-2 | R-1) (limiter with the waves below and above,
+//      correction, two transverse solves); [Y] exchange with the neighbour
+//      columns [Y]; publish its total for row R-2, [arrive YS(R)].
+//   X, row R: [wait CELLS(R)] solve (cp-1 | cp) of row R, store its waves
+//      [X]; gather the neighbour's increments of row R-1, [wait YS(R)] write
+//      row R-2 = q + (Y's total + X's total); finish row R (limiter with the
+//      neighbours' waves, correction, two transverse solves), publish column
+//      cp-1's increments [X]; [arrive EMPTY(R)]: rows <= R-2 of the ring and
+//      Y's total of R-2 are free.
+// CELLS, YS and EMPTY are pairs of barriers used by row parity (Y arrives,
+// X waits; EMPTY the other way), each with all 2*NT threads; [X] and [Y] are
+// the groups' own barriers.  Every arrival has its wait: Y arrives CELLS and
+// YS on every row, X waits on both on every row; X arrives EMPTY on rows
+// R0..R1-2 and Y waits on rows R0+2..R1.  The y-interface being finished,
+// its fluctuations and its dot products wait in shared memory (per column,
+// touched only by that column's Y thread).  The increments are the same
+// terms as in unsplit_tile; only the order of the per-cell sum differs (the
+// x and y parts are summed apart and then added).  Solvers without aux data
+// or guesses, no capacity form.
+// ---------------------------------------------------------------------------
+template <class RP, int NT>
+struct UnsplitSmemWS {
+    static constexpr int ME = RP::MEQN, MW = RP::MWAVES, NC = RP::NC;
+    static constexpr int NF = (int)(sizeof(typename RP::Iface) / sizeof(double));
+    double cell[4][NC][NT];          // prepared cells, row R in slot R & 3 (Y writes)
+    double w[MW][ME][NT];            // unlimited x-waves of the current row (X)
+    double xl[3][ME][NT];            // X -> column cp-1: rows R-1, R, R+1
+    double yl[2][ME][NT];            // Y -> column cp-1: rows R-2, R-1
+    double yr[2][ME][NT];            // Y -> column cp+1: rows R-2, R-1
+    double ys[2][ME][NT];            // Y's total of row R-2, by row parity (Y -> X)
+    double fy[NF][NT];               // Y: the y-interface being finished, (R-2 | R-1)
+    double amy[ME][NT], apy[ME][NT];  // its fluctuations
+    double dy[MW][NT];               // its waves' dot products with the waves below it
+    double red[2 * NT / 32];
+};
+
+// named barriers of the direction-split tile (0 is __syncthreads)
+enum { NB_X = 1, NB_Y = 2, NB_CELLS = 3, NB_YS = 5, NB_EMPTY = 7 };
+
+template <int ID, int N>
+__device__ __forceinline__ void nb_sync() {
+    asm volatile("bar.sync %0, %1;" ::"n"(ID), "n"(N) : "memory");
+}
+template <int ID, int N>
+__device__ __forceinline__ void nb_arrive() {
+    asm volatile("bar.arrive %0, %1;" ::"n"(ID), "n"(N) : "memory");
+}
+// the barrier of a pair chosen by row parity (compile-time ids)
+template <int ID, int N>
+__device__ __forceinline__ void nb_sync_parity(int R) {
+    if (R & 1) nb_sync<ID + 1, N>();
+    else nb_sync<ID, N>();
+}
+template <int ID, int N>
+__device__ __forceinline__ void nb_arrive_parity(int R) {
+    if (R & 1) nb_arrive<ID + 1, N>();
+    else nb_arrive<ID, N>();
+}
+
+template <class RP, int NT, int SPEC = SPEC_ANY, bool EVO = false, int REG_Y = 0, int REG_X = 0>
+__device__ __forceinline__ void unsplit_tile_ws(const StepArgs& a, int strip, int rb, UnsplitSmemWS<RP, NT>& S,
+                                                double& cfl) {
+    constexpr int ME = RP::MEQN, MW = RP::MWAVES, NC = RP::NC, W = NT - 4;
+    constexpr int NF = UnsplitSmemWS<RP, NT>::NF;
+    using Iface = typename RP::Iface;
+    static_assert(AuxTraits<RP>::MAUX == 0 && !GuessTraits<RP>::USES, "direction-split tile: no aux, no guess");
+
+    const bool yrole = threadIdx.x < NT;
+    const int t = yrole ? threadIdx.x : threadIdx.x - NT;
+    const int mx = a.L.mx, my = a.L.my;
+    const int pitch = a.L.pitch;
+    const long long plane = a.L.plane;
+    const int cp = strip * W + t;
+    const int cpl = min(cp, mx + 3);
+    const int Hb = min(a.H, my - rb);
+    const int R0 = rb, R1 = rb + Hb + 3;
+    const bool out_col = (t >= 2) && (t < W + 2) && (cp <= mx + 1);
+    const bool xcfl_col = (t >= 2) && (t <= W + 2) && (cp <= mx + 2);
+    const bool ycfl_col = (t >= 1) && (t <= W + 2) && (cp <= mx + 2);
+    const int tl = (t > 0) ? t - 1 : 0;
+    const int tr = (t < NT - 1) ? t + 1 : NT - 1;
+    const double dtdx = EVO ? a.evo->dtdx : a.dtdx, dtdy = EVO ? a.evo->dtdy : a.dtdy;
+    const RPParams& P = a.rp;
+    const int order = (SPEC == SPEC_MC2) ? 2 : a.meth.order;
+    const int trans = (SPEC == SPEC_MC2) ? 2 : a.meth.transverse;
+    const bool tc = (order > 1) && (trans == 2);
+    constexpr bool ZS = SkipTraits<RP>::OK;
+    const bool zs = ZS && (SPEC != SPEC_ANY || a.meth.fwave == 0);
+    constexpr int N2 = 2 * NT;
+
+    if (yrole) {
+        // ================= Y warps =================
+        if (REG_Y > 0) asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(REG_Y));
+        const double* qo = a.qold + cpl;
+        double pf[ME], yA[ME], yB[ME];  // prefetched row; increments of rows R-2, R-1
+#pragma unroll
+        for (int m = 0; m < ME; ++m) {
+            pf[m] = __ldg(qo + m * plane + (long long)R0 * pitch);
+            yA[m] = yB[m] = 0.0;
+        }
+        bool zY = false;
+        for (int R = R0; R <= R1; ++R) {
+            const int s2 = R & 3, s1 = (R - 1) & 3;
+            if (R >= R0 + 2) nb_sync_parity<NB_EMPTY, N2>(R);  // X is done with row R-4's slot and ys(R-4)
+            {
+                double q[ME], c[NC];
+#pragma unroll
+                for (int m = 0; m < ME; ++m) q[m] = pf[m];
+                if (R < R1) {
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) pf[m] = __ldg(qo + m * plane + (long long)(R + 1) * pitch);
+                }
+                RP::prepare(q, P, c);
+#pragma unroll
+                for (int k = 0; k < NC; ++k) S.cell[s2][k][t] = c[k];
+            }
+            nb_arrive_parity<NB_CELLS, N2>(R);  // row R prepared
+            double ylB[ME], ylA[ME], yrB[ME], yrA[ME];
+#pragma unroll
+            for (int m = 0; m < ME; ++m) ylB[m] = ylA[m] = yrB[m] = yrA[m] = 0.0;
+            if (R > R0) {
+                double cB[NC], cA[NC];
+#pragma unroll
+                for (int k = 0; k < NC; ++k) {
+                    cB[k] = S.cell[s1][k][t];
+                    cA[k] = S.cell[s2][k][t];
+                }
+                Iface fN, fY;
+                double amN[ME], apN[ME], dn[MW];
+                const bool zN = zs && __all_sync(0xffffffffu, same_q<ME, NC>(cB, cA));
+                {
+                    double* fp = reinterpret_cast<double*>(&fY);
+#pragma unroll
+                    for (int k = 0; k < NF; ++k) fp[k] = S.fy[k][t];
+                }
+                if (ZS && zN) {
+                    SkipTraits<RP>::template zero_iface<2>(cB, cA, P, fN);
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) amN[m] = apN[m] = 0.0;
+#pragma unroll
+                    for (int k = 0; k < MW; ++k) dn[k] = 0.0;
+                } else {
+                    RP::template solve<2>(cB, cA, P, fN, amN, apN);
+                    double wY[MW][ME], wN[MW][ME];
+                    RP::template waves<2>(fY, P, wY);
+                    RP::template waves<2>(fN, P, wN);
+#pragma unroll
+                    for (int k = 0; k < MW; ++k) {
+                        double d = 0.0;
+#pragma unroll
+                        for (int m = 0; m < ME; ++m) d = d + wY[k][m] * wN[k][m];
+                        dn[k] = d;
+                    }
+                }
+                if (R >= R0 + 3) {
+                    if (ycfl_col) cfl = fmax(cfl, iface_cfl<RP, 2>(fY, P, dtdy));
+                    if (!(ZS && zY)) {
+                        double amY[ME], apY[ME], dY[MW], cq[ME];
+#pragma unroll
+                        for (int m = 0; m < ME; ++m) {
+                            amY[m] = S.amy[m][t];
+                            apY[m] = S.apy[m][t];
+                        }
+#pragma unroll
+                        for (int k = 0; k < MW; ++k) dY[k] = S.dy[k][t];
+                        if (order != 1) {
+                            correction<RP, 2, SPEC>(fY, P, a.meth, dtdy, dY, dn, cq);
+                        } else {
+#pragma unroll
+                            for (int m = 0; m < ME; ++m) cq[m] = 0.0;
+                        }
+#pragma unroll
+                        for (int m = 0; m < ME; ++m) {
+                            const double f = 0.5 * cq[m];
+                            yA[m] = yA[m] - dtdy * (amY[m] + f);
+                            yB[m] = yB[m] - dtdy * (apY[m] - f);
+                        }
+                        if (trans > 0) {
+                            const double h = 0.5 * dtdy * dtdx;
+                            double as2[ME], bm[ME], bp[ME];
+#pragma unroll
+                            for (int m = 0; m < ME; ++m) as2[m] = tc ? amY[m] + cq[m] : amY[m];
+                            RP::template rpt2<2>(fY, P, as2, bm, bp);  // imp = 1 -> row R-2
+#pragma unroll
+                            for (int m = 0; m < ME; ++m) {
+                                yA[m] = yA[m] + h * (bp[m] - bm[m]);
+                                ylB[m] = h * bm[m];
+                                yrB[m] = -h * bp[m];
+                            }
+#pragma unroll
+                            for (int m = 0; m < ME; ++m) as2[m] = tc ? apY[m] - cq[m] : apY[m];
+                            RP::template rpt2<2>(fY, P, as2, bm, bp);  // imp = 2 -> row R-1
+#pragma unroll
+                            for (int m = 0; m < ME; ++m) {
+                                yB[m] = yB[m] + h * (bp[m] - bm[m]);
+                                ylA[m] = h * bm[m];
+                                yrA[m] = -h * bp[m];
+                            }
+                        }
+                    }
+                }
+                {
+                    const double* fp = reinterpret_cast<const double*>(&fN);
+#pragma unroll
+                    for (int k = 0; k < NF; ++k) S.fy[k][t] = fp[k];
+                }
+#pragma unroll
+                for (int m = 0; m < ME; ++m) {
+                    S.amy[m][t] = amN[m];
+                    S.apy[m][t] = apN[m];
+                }
+#pragma unroll
+                for (int k = 0; k < MW; ++k) S.dy[k][t] = dn[k];
+                zY = zN;
+            } else {
+                // the first row: an empty record below it (zero waves, zero dots)
+#pragma unroll
+                for (int k = 0; k < NF; ++k) S.fy[k][t] = 0.0;
+            }
+#pragma unroll
+            for (int m = 0; m < ME; ++m) {
+                S.yl[0][m][t] = ylB[m];
+                S.yl[1][m][t] = ylA[m];
+                S.yr[0][m][t] = yrB[m];
+                S.yr[1][m][t] = yrA[m];
+            }
+            nb_sync<NB_Y, NT>();  // the Y warps' neighbour increments visible
+#pragma unroll
+            for (int m = 0; m < ME; ++m) {
+                yA[m] = yA[m] + S.yl[0][m][tr] + S.yr[0][m][tl];
+                yB[m] = yB[m] + S.yl[1][m][tr] + S.yr[1][m][tl];
+            }
+            nb_sync<NB_Y, NT>();  // every read of the exchange done before the next row's writes
+#pragma unroll
+            for (int m = 0; m < ME; ++m) {
+                S.ys[R & 1][m][t] = yA[m];  // row R-2 complete on the y side
+                yA[m] = yB[m];
+                yB[m] = 0.0;
+            }
+            nb_arrive_parity<NB_YS, N2>(R);
+        }
+    } else {
+        // ================= X warps =================
+        if (REG_X > 0) asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(REG_X));
+        double* qn = a.qnew + cpl;
+        double x0[ME], x1[ME], x2[ME];  // increments of rows R-2, R-1, R (this column)
+#pragma unroll
+        for (int m = 0; m < ME; ++m) x0[m] = x1[m] = x2[m] = 0.0;
+        for (int R = R0; R <= R1; ++R) {
+            const int s2 = R & 3;
+            nb_sync_parity<NB_CELLS, N2>(R);  // row R prepared
+            Iface fX;
+            double amX[ME], apX[ME];
+            bool zX;
+            const bool xrow = (R > R0) && (R < R1);
+            {
+                double cL[NC], cR[NC];
+#pragma unroll
+                for (int k = 0; k < NC; ++k) {
+                    cL[k] = S.cell[s2][k][tl];
+                    cR[k] = S.cell[s2][k][t];
+                }
+                // (the first and last rows' x-interfaces are never finished: no solve)
+                zX = ZS && (!xrow || (zs && __all_sync(0xffffffffu, same_q<ME, NC>(cL, cR))));
+                if (ZS && zX) {
+                    SkipTraits<RP>::template zero_iface<1>(cL, cR, P, fX);
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) amX[m] = apX[m] = 0.0;
+#pragma unroll
+                    for (int k = 0; k < MW; ++k)
+#pragma unroll
+                        for (int m = 0; m < ME; ++m) S.w[k][m][t] = 0.0;
+                } else {
+                    RP::template solve<1>(cL, cR, P, fX, amX, apX);
+                    double wX[MW][ME];
+                    RP::template waves<1>(fX, P, wX);
+#pragma unroll
+                    for (int k = 0; k < MW; ++k)
+#pragma unroll
+                        for (int m = 0; m < ME; ++m) S.w[k][m][t] = wX[k][m];
+                }
+            }
+            nb_sync<NB_X, NT>();  // x-waves of row R and column cp-1's increments of row R-1 visible
+#pragma unroll
+            for (int m = 0; m < ME; ++m) {
+                x0[m] = x0[m] + S.xl[0][m][tr];  // rows R-2, R-1, R from the neighbour's row R-1
+                x1[m] = x1[m] + S.xl[1][m][tr];
+                x2[m] = x2[m] + S.xl[2][m][tr];
+            }
+            nb_sync_parity<NB_YS, N2>(R);  // Y's total of row R-2
+            if (R >= R0 + 4 && out_col) {
+                double v[ME];
+#pragma unroll
+                for (int m = 0; m < ME; ++m) v[m] = S.cell[(R - 2) & 3][m][t] + (S.ys[R & 1][m][t] + x0[m]);
+#pragma unroll
+                for (int m = 0; m < ME; ++m) qn[m * plane + (long long)(R - 2) * pitch] = v[m];
+                if (!all_finite<ME>(v)) atomicOr(a.status, 1);
+            }
+            double x3[ME], xbL[ME], xcL[ME], xaL[ME];
+#pragma unroll
+            for (int m = 0; m < ME; ++m) x3[m] = xbL[m] = xcL[m] = xaL[m] = 0.0;
+            if (xrow && xcfl_col) cfl = fmax(cfl, iface_cfl<RP, 1>(fX, P, dtdx));
+            if (xrow && !(ZS && zX)) {
+                double cq[ME];
+                if (order != 1) {
+                    double dl[MW], dr[MW];
+#pragma unroll
+                    for (int k = 0; k < MW; ++k) {
+                        double x = 0.0, y = 0.0;
+#pragma unroll
+                        for (int m = 0; m < ME; ++m) {
+                            const double w = S.w[k][m][t];
+                            x = x + S.w[k][m][tl] * w;
+                            y = y + w * S.w[k][m][tr];
+                        }
+                        dl[k] = x;
+                        dr[k] = y;
+                    }
+                    correction<RP, 1, SPEC>(fX, P, a.meth, dtdx, dl, dr, cq);
+                } else {
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) cq[m] = 0.0;
+                }
+#pragma unroll
+                for (int m = 0; m < ME; ++m) {
+                    const double f = 0.5 * cq[m];
+                    x2[m] = x2[m] - dtdx * (apX[m] - f);
+                    xcL[m] = -dtdx * (amX[m] + f);
+                }
+                if (trans > 0) {
+                    const double h = 0.5 * dtdx * dtdy;
+                    double as2[ME], bm[ME], bp[ME];
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) as2[m] = tc ? amX[m] + cq[m] : amX[m];
+                    RP::template rpt2<1>(fX, P, as2, bm, bp);  // imp = 1 -> column cp-1
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) {
+                        xcL[m] = xcL[m] + h * (bp[m] - bm[m]);
+                        xbL[m] = h * bm[m];
+                        xaL[m] = -h * bp[m];
+                    }
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) as2[m] = tc ? apX[m] - cq[m] : apX[m];
+                    RP::template rpt2<1>(fX, P, as2, bm, bp);  // imp = 2 -> column cp
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) {
+                        x2[m] = x2[m] + h * (bp[m] - bm[m]);
+                        x1[m] = x1[m] + h * bm[m];
+                        x3[m] = x3[m] - h * bp[m];
+                    }
+                }
+            }
+            nb_sync<NB_X, NT>();  // every read of the waves and of the exchange slots done
+#pragma unroll
+            for (int m = 0; m < ME; ++m) {
+                S.xl[0][m][t] = xbL[m];
+                S.xl[1][m][t] = xcL[m];
+                S.xl[2][m][t] = xaL[m];
+                x0[m] = x1[m];
+                x1[m] = x2[m];
+                x2[m] = x3[m];
+            }
+            if (R + 2 <= R1) nb_arrive_parity<NB_EMPTY, N2>(R);  // rows <= R-2 and ys(R-2) released
+        }
+    }
+}
+
+// Grid: 1D over the tiles as k_step_unsplit, 2*NT threads per CTA.
+template <class RP, int NT, int MINB, int SPEC, bool EVO = false, int REG_Y = 0, int REG_X = 0>
+__global__ void __launch_bounds__(2 * NT, MINB) k_step_unsplit_ws(const StepArgs a) {
+    if (EVO && a.evo->done) return;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    UnsplitSmemWS<RP, NT>& S = *reinterpret_cast<UnsplitSmemWS<RP, NT>*>(smem_raw);
+    int tile = blockIdx.x;
+    if (a.tile_order) {
+        const int t = a.tile_order[blockIdx.x];
+        if (t >= 0 && t < (int)gridDim.x) tile = t;
+    }
+    long long t0 = 0;
+    if (a.tile_cost && threadIdx.x == 0) t0 = clock64();
+    double cfl = 0.0;
+    unsplit_tile_ws<RP, NT, SPEC, EVO, REG_Y, REG_X>(a, tile % a.nstrips, (tile / a.nstrips) * a.H, S, cfl);
     cfl_commit(cfl, S.red, a.cfl_bits);
     if (a.tile_cost && threadIdx.x == 0) {
         const long long c = clock64() - t0;

@@ -14,7 +14,45 @@ import types
 from . import _lib
 
 
+class _ParamBlock(object):
+    """A solver's parameters, in both of the forms the reference uses them.
+
+    Called with ``problem_data`` it returns the parameter vector for the C ABI
+    (the device solver's cparam).  Assigned to, it behaves like an f2py
+    module's ``cparam`` COMMON block: the reference's ``state.set_cparam(rp)``
+    (state.py:206-231) lists its attributes and assigns every problem_data
+    entry to it, which it accepts (the device takes the values from
+    problem_data or the step module's cparam, not from here)."""
+
+    def __init__(self, solver):
+        object.__setattr__(self, '_owner', solver)
+
+    def __dir__(self):
+        # nothing to demand: the required keys are checked when the vector is built
+        return []
+
+    def __call__(self, problem_data):
+        rp = self._owner
+        missing = [k for k in rp.cparam_names if k not in problem_data]
+        if missing:
+            raise Exception("Riemann solver %s reads problem_data[%s], which is not set"
+                            % (rp.name, ", ".join(repr(k) for k in missing)))
+        vals = [float(problem_data[k]) for k in rp.cparam_names]
+        if rp.efix is not None:
+            vals.append(1.0 if problem_data.get('efix', rp.efix) else 0.0)
+        for key, default in rp.extra:
+            vals.append(float(problem_data.get(key, default)))
+        return vals
+
+
 class RiemannSolver(object):
+    """One device Riemann solver.  Usable where the reference expects a
+    clawpack.riemann module: ``__name__`` ends in the module name, ``rpn2`` /
+    ``rpt2`` carry ``_cpointer`` (here the solver itself, which
+    pyclaw_b200.classic2 resolves to the device code where an f2py module
+    would receive a Fortran function pointer, classic/solver.py:516-521), and
+    ``cparam`` takes the reference's set_cparam."""
+
     def __init__(self, name, rp_id, num_eqn, num_waves, cparam, fwave=False, efix=None, extra=()):
         self.__name__ = 'clawpack.riemann.' + name
         self.name = name
@@ -25,19 +63,9 @@ class RiemannSolver(object):
         self.fwave = fwave
         self.efix = efix  # entropy fix switch (a compile-time constant in Fortran)
         self.extra = tuple(extra)  # (problem_data key, default) pairs appended to cparam
-
-    def cparam(self, problem_data):
-        """Parameter vector for the C ABI from ``problem_data``."""
-        missing = [k for k in self.cparam_names if k not in problem_data]
-        if missing:
-            raise Exception("Some required value(s) in the cparam common block in the Riemann "
-                            "solver have not been set in problem_data: %s" % ", ".join(missing))
-        vals = [float(problem_data[k]) for k in self.cparam_names]
-        if self.efix is not None:
-            vals.append(1.0 if problem_data.get('efix', self.efix) else 0.0)
-        for key, default in self.extra:
-            vals.append(float(problem_data.get(key, default)))
-        return vals
+        self.cparam = _ParamBlock(self)
+        self.rpn2 = types.SimpleNamespace(_cpointer=self)
+        self.rpt2 = types.SimpleNamespace(_cpointer=self)
 
     def __repr__(self):
         return "<Riemann solver %s>" % self.name

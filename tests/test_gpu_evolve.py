@@ -32,7 +32,7 @@ ULP_RTOL = 1e-13
 
 
 def _close(x, y):
-    return abs(x - y) <= ULP_RTOL * max(abs(x), abs(y))
+    return x == y or abs(x - y) <= ULP_RTOL * max(abs(x), abs(y))
 
 
 def _same(a, b):
