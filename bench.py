@@ -70,6 +70,11 @@ def parse():
                     help="grid size of the learned-guess workload (2048 in the benchmark; smaller for profiling)")
     ap.add_argument("--learned-pre-t", type=float, default=0.4,
                     help="time the learned-guess workload's state is advanced to (0.4 in the benchmark)")
+    ap.add_argument("--replicas", action="store_true",
+                    help="with --gpus N > 1: N independent copies of the problem instead of the row-slab "
+                         "decomposition")
+    ap.add_argument("--slab", action="store_true",
+                    help="use the row-slab code path even on one GPU (one slab: no neighbours)")
     ap.add_argument("--state", default=None,
                     help="profiling aid: .npy file of the advanced state; loaded if it exists (no "
                          "advance), else written after the advance")
@@ -458,14 +463,34 @@ def run_ours(args):
     torch.cuda.set_stream(stream)
     n = args.n
 
-    # weak scaling: every rank steps its own copy of the workload (the
-    # single-grid step has no cross-rank exchange unless a domain is split)
-    claw = workloads.euler_quadrants_unsplit(n=n)
+    # weak scaling.  With N > 1 ranks the default is the row-slab
+    # decomposition: rank r owns an n x n slab of an n x (n N) grid (the
+    # quadrant data repeated along y), and every step exchanges two halo rows
+    # with each neighbour (NCCL, device to device) and reduces the Courant
+    # number (all-reduce MAX) before the accept decision, as petclaw does.
+    # --replicas runs N independent copies instead.
+    slab = (world > 1 and not args.replicas) or args.slab
+    if slab:
+        from pyclaw_b200 import classic, slabs
+        claw = workloads.euler_quadrants_unsplit(slabs.make_slab_solver_class(classic.ClawSolver2D), n=n)
+        claw.solver.slab = (rank, world, False, None)
+        claw.solver.global_delta = tuple(claw.solution.state.grid.delta)
+    else:
+        claw = workloads.euler_quadrants_unsplit(n=n)
     solver, sol = claw.solver, claw.solution
     solver.device = local
     solver.setup(sol)
     patch = solver._dev
     patch.set_stream(stream.cuda_stream)
+
+    def slab_step(dt):
+        """One decomposed step: halo rows in, local step, global Courant number,
+        the same accept decision on every rank."""
+        planes = slabs.DevicePlanes(patch)
+        slabs.exchange_rows(planes.get_rows, planes.set_rows, n, rank, world, False)
+        cfl = slabs.global_cfl(patch.step(dt), device=dev)
+        patch.accept(cfl <= 1.0)
+        return cfl
 
     # advance (untimed) to the middle of the run so the timed steps see a
     # developed flow, with the reference's dt rule (cfl_desired 0.9)
@@ -477,9 +502,13 @@ def run_ours(args):
         t = args.pre_t
     while t < args.pre_t:
         dt = min(dt, args.pre_t - t) if cfl is None else min(dt * 0.9 / cfl, args.pre_t - t)
-        cfl = patch.step(dt)
-        ok = cfl <= 1.0
-        patch.accept(ok)
+        if slab:
+            cfl = slab_step(dt)
+            ok = cfl <= 1.0
+        else:
+            cfl = patch.step(dt)
+            ok = cfl <= 1.0
+            patch.accept(ok)
         if ok:
             t += dt
     if args.state and not os.path.exists(args.state):
@@ -489,6 +518,8 @@ def run_ours(args):
     # fixed dt for CFL 0.9 from a probe step
     cfl = patch.step(dt)
     patch.accept(False)
+    if slab:
+        cfl = slabs.global_cfl(cfl, device=dev)
     dt = dt * 0.9 / cfl
     # launch shape from the autotuner (trial steps are rejected: state unchanged)
     from pyclaw_b200 import tune
@@ -502,8 +533,11 @@ def run_ours(args):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     for _ in range(args.warmup):
         flush.zero_()
-        patch.step(dt, want_cfl=False)
-        patch.accept(True)
+        if slab:
+            slab_step(dt)
+        else:
+            patch.step(dt, want_cfl=False)
+            patch.accept(True)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -517,8 +551,11 @@ def run_ours(args):
         for k in range(args.steps):
             flush.zero_()
             ev[k][0].record(stream)
-            patch.step(dt, want_cfl=False)
-            patch.accept(True)
+            if slab:
+                slab_step(dt)
+            else:
+                patch.step(dt, want_cfl=False)
+                patch.accept(True)
             ev[k][1].record(stream)
             kern_ms.append(patch.kernel_ms())
         torch.cuda.synchronize()
@@ -553,7 +590,16 @@ def run_ours(args):
         qh[:] = sol.state.get_q_global().reshape(-1, order="F")
         qd = torch.empty_like(torch.from_numpy(qh)).pin_memory().numpy()
         L = _lib.load()
-        h = patch.h
+        e2e_patch = patch
+        if slab:
+            # host-to-host steps of independent states (each rank its own
+            # pipeline; a decomposed run keeps its state on the devices)
+            ec = workloads.euler_quadrants_unsplit(n=n)
+            ec.solver.device = local
+            ec.solver.setup(ec.solution)
+            e2e_patch = ec.solver._dev
+            e2e_patch.set_stream(stream.cuda_stream)
+        h = e2e_patch.h
         cflv = ctypes.c_double(0.0)
         K = args.e2e_steps
         # the copies alone, before the e2e runs (and again after them below):
@@ -572,10 +618,10 @@ def run_ours(args):
         # input's copy overlapping this step's compute and result copy
         qin = [qh.reshape((MEQN, n, n), order="F")] * K
         qout = [qd.reshape((MEQN, n, n), order="F")] * K
-        patch.run_host(qin[:2], qout[:2], [dt, dt])  # allocates the staging buffers
+        e2e_patch.run_host(qin[:2], qout[:2], [dt, dt])  # allocates the staging buffers
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        patch.run_host(qin, qout, [dt] * K)
+        e2e_patch.run_host(qin, qout, [dt] * K)
         el = time.perf_counter() - t0
         e2e_val, seq_val = cells * K / el, cells * K / el_seq
         pair_b = copy_bound(qh.nbytes, K)
@@ -619,6 +665,10 @@ def run_ours(args):
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "ours",
                 "config": config({"dt": dt, "cfl_last": last_cfl, "mx": n, "my": n,
+                                  "parallelism": ("row slabs: %d x %d grid, one %d x %d slab per rank, halo "
+                                                  "exchange (NCCL) + CFL all-reduce every step"
+                                                  % (n, n * world, n, n)) if slab else
+                                                 ("%d independent replicas" % world),
                                   "launch_shape": {"variant": shape[0], "rows": shape[1],
                                                    "trials_ms": {"%d/%d" % k: round(v, 4)
                                                                  for k, v in sorted(trials.items())}},

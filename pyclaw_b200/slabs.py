@@ -40,7 +40,81 @@ def neighbours(rank, world, periodic):
     return lower, upper
 
 
-def exchange_rows(get_rows, set_rows, my_local, rank, world, periodic, group=None):
+class DistTransport(object):
+    """Halo messages and the Courant-number reduction over torch.distributed:
+    NCCL over NVLink for device tensors, gloo for host tensors."""
+
+    def __init__(self, group=None):
+        self.group = group
+
+    def exchange(self, sends, recvs):
+        """Post every send ``(tensor, dst)`` and receive ``(buffer, src)`` of one
+        phase together and wait for all of them."""
+        import torch.distributed as dist
+        ops = [dist.P2POp(dist.isend, t, dst, self.group) for t, dst in sends]
+        ops += [dist.P2POp(dist.irecv, b, src, self.group) for b, src in recvs]
+        for r in dist.batch_isend_irecv(ops) if ops else []:
+            r.wait()
+
+    def max(self, value, device=None):
+        import torch
+        import torch.distributed as dist
+        if not dist.is_initialized() or dist.get_world_size(self.group) == 1:
+            return float(value)
+        t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX, group=self.group)
+        return float(t.item())
+
+
+class ThreadTransport(object):
+    """The same two operations between slabs stepped by threads of one
+    process (several slabs on one device, or on the host): a shared mailbox
+    and a barrier.  Device rows are complete before they are posted (the
+    poster synchronises the device), so no kernel ever waits on another
+    slab's kernels."""
+
+    def __init__(self, world, timeout=120.0):
+        import threading
+        self.world = world
+        self.barrier = threading.Barrier(world, timeout=timeout)  # a failed slab breaks it for all
+        self.box = {}
+        self.vals = [0.0] * world
+
+    def endpoint(self, rank):
+        return _ThreadEndpoint(self, rank)
+
+
+class _ThreadEndpoint(object):
+    def __init__(self, hub, rank):
+        self.hub, self.rank = hub, rank
+
+    def exchange(self, sends, recvs):
+        import torch
+        hub = self.hub
+        if any(t.is_cuda for t, _ in sends):
+            torch.cuda.synchronize()
+        for t, dst in sends:
+            hub.box[(self.rank, dst)] = t
+        hub.barrier.wait()
+        for b, src in recvs:
+            b.copy_(hub.box[(src, self.rank)])
+        if any(b.is_cuda for b, _ in recvs):
+            torch.cuda.synchronize()
+        hub.barrier.wait()
+        for t, dst in sends:
+            del hub.box[(self.rank, dst)]
+        hub.barrier.wait()
+
+    def max(self, value, device=None):
+        hub = self.hub
+        hub.vals[self.rank] = float(value)
+        hub.barrier.wait()
+        m = max(hub.vals)
+        hub.barrier.wait()
+        return m
+
+
+def exchange_rows(get_rows, set_rows, my_local, rank, world, periodic, group=None, transport=None):
     """Fill the two ghost rows on each internal side from the neighbours.
 
     ``get_rows(j0, j1)`` returns a contiguous tensor with padded rows
@@ -48,45 +122,31 @@ def exchange_rows(get_rows, set_rows, my_local, rank, world, periodic, group=Non
     ``set_rows(j0, j1, t)`` stores one.  Two phases, each with at most one
     message per ordered pair of ranks, so matching never depends on tags
     (NCCL ignores them): first every rank sends its top rows up, then its
-    bottom rows down.
+    bottom rows down.  ``transport`` carries the messages (default: a
+    DistTransport over ``group``).
     """
-    import torch.distributed as dist
-    lower, upper = neighbours(rank, world, periodic)
     if world == 1:
         return
+    tr = transport if transport is not None else DistTransport(group)
+    lower, upper = neighbours(rank, world, periodic)
     # phase 1: top interior rows -> upper neighbour's lower halo
-    ops, recv = [], None
-    if upper is not None:
-        ops.append(dist.P2POp(dist.isend, get_rows(my_local, my_local + 2), upper, group))
-    if lower is not None:
-        recv = get_rows(0, 2).clone()
-        ops.append(dist.P2POp(dist.irecv, recv, lower, group))
-    for r in dist.batch_isend_irecv(ops) if ops else []:
-        r.wait()
+    sends = [(get_rows(my_local, my_local + 2), upper)] if upper is not None else []
+    recv = get_rows(0, 2).clone() if lower is not None else None
+    tr.exchange(sends, [(recv, lower)] if recv is not None else [])
     if recv is not None:
         set_rows(0, 2, recv)
     # phase 2: bottom interior rows -> lower neighbour's upper halo
-    ops, recv = [], None
-    if lower is not None:
-        ops.append(dist.P2POp(dist.isend, get_rows(2, 4), lower, group))
-    if upper is not None:
-        recv = get_rows(my_local + 2, my_local + 4).clone()
-        ops.append(dist.P2POp(dist.irecv, recv, upper, group))
-    for r in dist.batch_isend_irecv(ops) if ops else []:
-        r.wait()
+    sends = [(get_rows(2, 4), lower)] if lower is not None else []
+    recv = get_rows(my_local + 2, my_local + 4).clone() if upper is not None else None
+    tr.exchange(sends, [(recv, upper)] if recv is not None else [])
     if recv is not None:
         set_rows(my_local + 2, my_local + 4, recv)
 
 
-def global_cfl(local_cfl, device=None, group=None):
+def global_cfl(local_cfl, device=None, group=None, transport=None):
     """MAX of the Courant number over ranks (src/petclaw/cfl.py:34-35)."""
-    import torch
-    import torch.distributed as dist
-    if not dist.is_initialized() or dist.get_world_size(group) == 1:
-        return float(local_cfl)
-    t = torch.tensor([float(local_cfl)], dtype=torch.float64, device=device)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
-    return float(t.item())
+    tr = transport if transport is not None else DistTransport(group)
+    return tr.max(local_cfl, device=device)
 
 
 def local_bcs(bc_lower, bc_upper, rank, world):
@@ -172,6 +232,8 @@ def make_slab_solver_class(base):
         def __init__(self, riemann_solver=None, claw_package=None):
             self.slab = None          # (rank, world, periodic_y, group)
             self.global_delta = None  # (dx, dy) of the global grid
+            self.transport = None     # halo/CFL transport (None: torch.distributed over the group)
+            self._stream_set = False  # the patch runs on torch's current stream (with the halo copies)
             super().__init__(riemann_solver, claw_package)
 
         def _device_desc(self, solution):
@@ -192,15 +254,15 @@ def make_slab_solver_class(base):
                 dev = self._dev
             if dev.host_dirty:
                 dev.push(state)
-            if not getattr(self, "_stream_set", False):
+            if not self._stream_set:
                 import torch
                 dev.set_stream(torch.cuda.current_stream().cuda_stream)  # one stream for NCCL + kernels
                 self._stream_set = True
             my = state.grid.num_cells[1]
             if world > 1:
                 planes = DevicePlanes(dev)
-                exchange_rows(planes.get_rows, planes.set_rows, my, rank, world, periodic, group)
+                exchange_rows(planes.get_rows, planes.set_rows, my, rank, world, periodic, group, self.transport)
             cfl = dev.step(self.dt)
-            self.cfl.update_global_max(global_cfl(cfl, device="cuda", group=group))
+            self.cfl.update_global_max(global_cfl(cfl, device="cuda", group=group, transport=self.transport))
 
     return SlabClawSolver2D

@@ -30,6 +30,7 @@ def _oracle_slab_class():
         def __init__(self, riemann_solver=None, claw_package=None):
             self.slab = None
             self.global_delta = None
+            self.transport = None
             super().__init__(riemann_solver, claw_package)
 
         def step_hyperbolic(self, solution):
@@ -41,13 +42,14 @@ def _oracle_slab_class():
             qbc[:, 2:-2, 2:-2] = state._q
             t = torch.from_numpy(qbc)  # (meqn, mx+4, my+4); rows are the last axis
             slabs.exchange_rows(lambda a, b: t[:, :, a:b].contiguous(),
-                                lambda a, b, x: t[:, :, a:b].copy_(x), my, rank, world, periodic, group)
+                                lambda a, b, x: t[:, :, a:b].copy_(x), my, rank, world, periodic, group,
+                                self.transport)
             lo, up = slabs.local_bcs(self.bc_lower, self.bc_upper, rank, world)
             pyoracle.bc_fill(qbc, lo, up)
             qold = qbc.copy(order="F")
             cp = self.rp.cparam(state.problem_data)
             cfl = pyoracle.step2(qold, qbc, dx, dy, self.dt, self._method, self._mthlim, self.rp.rp_id, cp)
-            self.cfl.update_global_max(slabs.global_cfl(cfl, group=group))
+            self.cfl.update_global_max(slabs.global_cfl(cfl, group=group, transport=self.transport))
             state._q = np.asfortranarray(qbc[:, 2:-2, 2:-2].copy())
 
     return OracleSlab
@@ -115,6 +117,46 @@ def test_slab_run_equals_single_domain(oracle, tmp_path, name, world):
     assert np.array_equal(parts[0]["dts"], np.array(dts))
     assert float(parts[0]["t"]) == sol.t
     assert np.array_equal(q_slabs, sol.state.get_q_global())
+
+
+@pytest.mark.parametrize("name,world", [("euler_extrap", 2), ("advection_periodic", 3)])
+def test_thread_transport_slabs_equal_single_domain(oracle, name, world):
+    # the same decomposition with the in-process transport (threads, one
+    # mailbox and barrier) that the one-GPU device test uses
+    import threading
+    from pyclaw_b200 import slabs
+    nsteps = 8
+    hub = slabs.ThreadTransport(world)
+    out, errs = {}, []
+
+    def worker(rank):
+        try:
+            claw, (start, count) = slabs.localize(_problem(name, _oracle_slab_class()), rank, world)
+            s, sol = claw.solver, claw.solution
+            s.transport = hub.endpoint(rank)
+            s.setup(sol)
+            s.dt = s.dt_initial
+            for _ in range(nsteps):
+                s.evolve_to_time(sol)
+            out[rank] = (sol.state.get_q_global(), sol.t)
+        except BaseException as e:  # noqa: B902
+            errs.append(e)
+            hub.barrier.abort()
+
+    threads = [threading.Thread(target=worker, args=(r,)) for r in range(world)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join(120)
+    assert not errs, errs
+    claw = _problem(name, oracle.make_solver_class())
+    s, sol = claw.solver, claw.solution
+    s.setup(sol)
+    s.dt = s.dt_initial
+    for _ in range(nsteps):
+        s.evolve_to_time(sol)
+    assert np.array_equal(np.concatenate([out[r][0] for r in range(world)], axis=2), sol.state.get_q_global())
+    assert all(out[r][1] == sol.t for r in range(world))
 
 
 def test_partition_and_bcs():
