@@ -363,6 +363,18 @@ int claw2_mlp_infer(claw2_mlp* m, const float* x8, int n, float* y);
  * adaptive PVRS guess); Newton updates and Riemann solves since the last reset. */
 int claw2_patch_set_mlp(claw2_patch* p, claw2_mlp* m);
 int claw2_patch_counters(claw2_patch* p, unsigned long long* iters_and_solves, int reset);
+/* Newton counts since the last reset: out[0] steps needed (a final step below
+ * the tolerance is applied but not counted), out[1] steps applied (the needed
+ * ones plus that final step, for every interface whose two states differ),
+ * out[2] Riemann solves. */
+int claw2_patch_newton_counts(claw2_patch* p, unsigned long long* out, int reset);
+/* Measurement aid for exact-solver patches (unsplit steps): mode 1 runs a
+ * pre-pass before every step that solves each interface to the tolerance and
+ * hands the converged p* to the step as its Newton guess, outside the
+ * kernel timing (claw2_patch_kernel_ms): the step kernel's time with perfect
+ * guesses, the floor for any guess.  Mode 0 (default) turns it off; the
+ * device time loop ignores it. */
+int claw2_patch_set_exact_guess(claw2_patch* p, int mode);
 
 /* Description of the last error on this thread (never NULL). */
 const char* claw2_last_error(void);

@@ -145,6 +145,8 @@ _SIGNATURES = {
                                        ctypes.POINTER(ctypes.c_float)]),
     "claw2_patch_set_mlp": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "claw2_patch_counters": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_int]),
+    "claw2_patch_newton_counts": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_int]),
+    "claw2_patch_set_exact_guess": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "claw2_last_error": (ctypes.c_char_p, []),
     "claw2_version": (ctypes.c_char_p, []),
 }

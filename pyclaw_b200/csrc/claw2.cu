@@ -838,7 +838,8 @@ struct claw2_patch {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool timing = false;
     double* guess = nullptr;                  // exact solver: learned guesses, x and y planes
-    unsigned long long* counters = nullptr;   // exact solver: Newton iterations, solves
+    unsigned long long* counters = nullptr;   // exact solver: Newton steps needed, solves, steps applied
+    int exact_guess = 0;                      // exact solver: 1 = start from the converged p* (measurement)
     claw2_mlp* mlp = nullptr;
     // claw2_patch_evolve's captured attempts, one graph per starting buffer
     // parity, reused while nothing they captured changed: graph_gen counts
@@ -1068,7 +1069,7 @@ int claw2_patch_create(const claw2_desc* d, claw2_patch** out) {
     }
     if (ok && d->riemann == CLAW2_RP_EULER_EXACT)
         ok = cudaMalloc(&p->guess, 2 * (size_t)p->L.plane * 8) == cudaSuccess &&
-             cudaMalloc(&p->counters, 2 * sizeof(unsigned long long)) == cudaSuccess;
+             cudaMalloc(&p->counters, 3 * sizeof(unsigned long long)) == cudaSuccess;
     if (!ok) {
         cudaGetLastError();
         claw2_patch_destroy(p);
@@ -1080,7 +1081,7 @@ int claw2_patch_create(const claw2_desc* d, claw2_patch** out) {
     cudaMemsetAsync(p->q[0], 0, nb, p->st);
     cudaMemsetAsync(p->q[1], 0, nb, p->st);
     if (p->tmp) cudaMemsetAsync(p->tmp, 0, nb, p->st);
-    if (p->counters) cudaMemsetAsync(p->counters, 0, 2 * sizeof(unsigned long long), p->st);
+    if (p->counters) cudaMemsetAsync(p->counters, 0, 3 * sizeof(unsigned long long), p->st);
     cudaMemsetAsync(p->cfl, 0, sizeof(unsigned long long), p->st);
     cudaMemsetAsync(p->status, 0, sizeof(int), p->st);
     if (cudaStreamSynchronize(p->st) != cudaSuccess) {
@@ -1344,8 +1345,17 @@ int patch_enqueue_step(claw2_patch* p, double dt) {
         ++p->step_launches;
     }
     StepArgs a = patch_args(p, dt);
+    const bool exact_unsplit = p->d.riemann == CLAW2_RP_EULER_EXACT && !p->d.dimensional_split;
+    if (exact_unsplit && p->exact_guess == 1) {
+        // converged pressures as guesses, outside the timed region: the step
+        // kernel's time with them is the floor for any guess
+        dim3 grid((p->L.mx + 4 + 31) / 32, (p->L.my + 4 + 3) / 4);
+        k_exact_pstar_guess<<<grid, 128, 0, p->st>>>(qc, p->L, p->rp.c[0], p->rp.c[1], p->guess);
+        a.guess = p->guess;
+        ++p->step_launches;
+    }
     if (p->timing) CUDA_TRY(cudaEventRecord(p->ev0, p->st));
-    if (p->d.riemann == CLAW2_RP_EULER_EXACT && p->mlp && !p->d.dimensional_split) {
+    if (exact_unsplit && p->mlp && p->exact_guess == 0) {
         mlp_guess_launch(p->mlp, qc, p->L, p->rp.c[0], p->guess, p->st);
         a.guess = p->guess;
         ++p->step_launches;
@@ -1927,12 +1937,36 @@ int claw2_patch_set_mlp(claw2_patch* p, claw2_mlp* m) {
 
 int claw2_patch_counters(claw2_patch* p, unsigned long long* out, int reset) {
     if (!p || !out) return fail(CLAW2_EINVAL, "null pointer argument");
-    out[0] = out[1] = 0;
+    unsigned long long c[3];
+    const int rc = claw2_patch_newton_counts(p, c, reset);
+    out[0] = c[0];
+    out[1] = c[2];
+    return rc;
+}
+
+int claw2_patch_newton_counts(claw2_patch* p, unsigned long long* out, int reset) {
+    if (!p || !out) return fail(CLAW2_EINVAL, "null pointer argument");
+    out[0] = out[1] = out[2] = 0;
     if (!p->counters) return CLAW2_OK;
     DeviceGuard g(p->device);
-    CUDA_TRY(cudaMemcpyAsync(out, p->counters, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, p->st));
+    unsigned long long c[3];
+    CUDA_TRY(cudaMemcpyAsync(c, p->counters, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, p->st));
     CUDA_TRY(cudaStreamSynchronize(p->st));
-    if (reset) CUDA_TRY(cudaMemsetAsync(p->counters, 0, 2 * sizeof(unsigned long long), p->st));
+    if (reset) CUDA_TRY(cudaMemsetAsync(p->counters, 0, 3 * sizeof(unsigned long long), p->st));
+    out[0] = c[0];  // needed
+    out[1] = c[2];  // applied
+    out[2] = c[1];  // solves
+    return CLAW2_OK;
+}
+
+int claw2_patch_set_exact_guess(claw2_patch* p, int mode) {
+    if (!p) return fail(CLAW2_EINVAL, "null patch");
+    if (mode != 0 && mode != 1) return fail(CLAW2_EINVAL, "mode must be 0 or 1 (got %d)", mode);
+    if (mode && p->d.riemann != CLAW2_RP_EULER_EXACT)
+        return fail(CLAW2_EINVAL, "converged guesses apply to the exact Euler solver only");
+    if (mode && !p->guess) return fail(CLAW2_EUNSUPPORTED, "this patch has no guess planes");
+    p->exact_guess = mode;
+    ++p->graph_gen;
     return CLAW2_OK;
 }
 

@@ -409,4 +409,47 @@ static __global__ void __launch_bounds__(128) k_mlp_guess(const MlpPacked* __res
     guess[L.plane + o] = gy0 * exp(wy * (double)res[w][32 + lane]);
 }
 
+// The converged pressures as guesses (a measurement aid, no network): thread
+// (cp, R) solves the x-interface (cp-1 | cp) and the y-interface (R-1 | R)
+// exactly as the step kernel's Newton iteration would from the adaptive
+// guess, to the same tolerance, and writes p* into the guess planes.  A step
+// that starts from these needs no Newton update beyond the one that confirms
+// convergence, so its time bounds from below what any guess can achieve.
+static __global__ void __launch_bounds__(128) k_exact_pstar_guess(const double* __restrict__ q, Layout L,
+                                                                  double gamma, double tol, double* guess) {
+    const int cp = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int R = blockIdx.y * 4 + (threadIdx.x >> 5);
+    if (cp > L.mx + 3 || R > L.my + 3) return;
+    const exact_euler::Gas G = exact_euler::make_gas(gamma);
+    const double g1 = gamma - 1.0;
+    // the primitive values and sound speed exactly as RPEulerExact::prepare
+    // forms them for the step, so the step's Newton starts at its own root
+    auto prim = [&](int cc, int rr, double& rho, double& u, double& v, double& p, double& c) {
+        const long long o = (long long)rr * L.pitch + cc;
+        rho = q[o];
+        const double irho = 1.0 / rho;
+        u = q[L.plane + o] * irho;
+        v = q[2 * L.plane + o] * irho;
+        p = g1 * (q[3 * L.plane + o] - 0.5 * (q[L.plane + o] * u + q[2 * L.plane + o] * v));
+        c = sqrt(gamma * p * irho);
+    };
+    double r0, u0, v0, p0, c0, rl, ul, vl, pl, cl, rb, ub, vb, pb, cb;
+    prim(cp, R, r0, u0, v0, p0, c0);
+    prim(max(cp - 1, 0), R, rl, ul, vl, pl, cl);
+    prim(cp, max(R - 1, 0), rb, ub, vb, pb, cb);
+    double ps, us;
+    int it;
+    const long long o = (long long)R * L.pitch + cp;
+    guess[o] = 0.0;  // vacuum or a failed solve: the step falls back to the adaptive guess
+    guess[L.plane + o] = 0.0;
+    if (!exact_euler::vacuum(G, ul, cl, u0, c0)) {
+        exact_euler::star(G, rl, ul, pl, cl, r0, u0, p0, c0, 0.0, tol, 50, ps, us, it);
+        guess[o] = ps;
+    }
+    if (!exact_euler::vacuum(G, vb, cb, v0, c0)) {
+        exact_euler::star(G, rb, vb, pb, cb, r0, v0, p0, c0, 0.0, tol, 50, ps, us, it);
+        guess[L.plane + o] = ps;
+    }
+}
+
 }  // namespace claw2

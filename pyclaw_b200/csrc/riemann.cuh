@@ -665,7 +665,8 @@ struct RPEulerExact {
         double w[3][4];
         double s[3];
         double u, v, a, ia, H;  // Roe state for rpt2
-        int iters;
+        int iters;    // Newton steps needed (exact_euler::star's count)
+        int applied;  // Newton steps applied: the needed ones plus the final sub-tolerance step
     };
 
     __device__ __forceinline__ static void prepare(const double (&q)[MEQN], const RPParams& p, double (&c)[NC]) {
@@ -753,12 +754,16 @@ struct RPEulerExact {
             }
             f.s[0] = fr.u - fr.a; f.s[1] = fr.u; f.s[2] = fr.u + fr.a;
             f.iters = 0;
+            f.applied = 0;
             return;
         }
         double ps, us;
         int it;
         exact_euler::star(G, rl, ul, pl, cl, rr, ur, pr, cr, guess, tol, 50, ps, us, it);
         f.iters = it;
+        // star() returns at once for equal states; otherwise it also applies
+        // the step that falls below the tolerance (unless it stopped at its cap)
+        f.applied = (rl == rr && ul == ur && pl == pr) ? 0 : (it < 50 ? it + 1 : it);
         const exact_euler::Fan F = exact_euler::fan(G, rl, ul, pl, cl, rr, ur, pr, cr, ps, us);
         double QL[MEQN], QR[MEQN], QsL[MEQN], QsR[MEQN];
 #pragma unroll
@@ -800,6 +805,7 @@ struct RPEulerExact {
         RPEulerRoe::template rpt2<IXY>(r, p, asdq, bm, bp);
     }
     __device__ __forceinline__ static int count(const Iface& f) { return f.iters; }
+    __device__ __forceinline__ static int count_applied(const Iface& f) { return f.applied; }
 };
 
 // ---------------------------------------------------------------------------
@@ -1118,6 +1124,7 @@ struct GuessTraits {
         RP::template solve<IXY>(cL, cR, p, f, am, ap);
     }
     __device__ __forceinline__ static int count(const typename RP::Iface&) { return 0; }
+    __device__ __forceinline__ static int count_applied(const typename RP::Iface&) { return 0; }
 };
 template <class RP>
 struct GuessTraits<RP, decltype((void)RP::USES_GUESS, void())> {
@@ -1129,6 +1136,7 @@ struct GuessTraits<RP, decltype((void)RP::USES_GUESS, void())> {
         RP::template solve_g<IXY>(cL, cR, p, g, f, am, ap);
     }
     __device__ __forceinline__ static int count(const typename RP::Iface& f) { return RP::count(f); }
+    __device__ __forceinline__ static int count_applied(const typename RP::Iface& f) { return RP::count_applied(f); }
 };
 
 }  // namespace claw2

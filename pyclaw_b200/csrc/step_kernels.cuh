@@ -96,16 +96,20 @@ __device__ __forceinline__ void cfl_commit(double cfl, double* s_red, unsigned l
     }
 }
 
-// Warp-sum two counters and add them once per warp.
-__device__ __forceinline__ void counter_commit(unsigned long long* c, unsigned long long a, unsigned long long b) {
+// Warp-sum three counters (Newton steps needed, solves, Newton steps
+// applied) and add them once per warp.
+__device__ __forceinline__ void counter_commit(unsigned long long* c, unsigned long long a, unsigned long long b,
+                                               unsigned long long d) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         a += __shfl_xor_sync(0xffffffffu, a, o);
         b += __shfl_xor_sync(0xffffffffu, b, o);
+        d += __shfl_xor_sync(0xffffffffu, d, o);
     }
     if ((threadIdx.x & 31) == 0 && c) {
         atomicAdd(c, a);
         atomicAdd(c + 1, b);
+        atomicAdd(c + 2, d);
     }
 }
 
@@ -242,11 +246,17 @@ __device__ __forceinline__ void tma_row(const CUtensorMap* tm, double* dst, unsi
 template <class RP, int NT, bool CAPA = false>
 struct UnsplitSmem {
     static constexpr int ME = RP::MEQN, MW = RP::MWAVES, NC = RP::NC;
+    // solvers with a large interface record (the exact solver's carries its
+    // waves) keep the y-interface being finished in shared memory between
+    // rows, so it does not occupy registers during the x work
+    static constexpr int NF = (int)(sizeof(typename RP::Iface) / sizeof(double));
+    static constexpr bool YS = NF > 12;
     double cell[3][NC][NT];  // prepared cells of rows R-2, R-1, R (ring)
     double w[MW][ME][NT];    // unlimited x-waves of row R
     double xl[4][ME][NT];    // increments for column cp-1: rows R-2, R-1, R, R+1
     double yr[2][ME][NT];    // increments for column cp+1: rows R-2, R-1
     double icap[CAPA ? 3 : 1][CAPA ? NT : 1];  // 1 / kappa of the ring's cells (capacity form)
+    double yrec[YS ? NF + 2 * ME + MW : 1][YS ? NT : 1];  // (YS) record, A-dq, A+dq, dots of (R-2 | R-1)
     double red[NT / 32];
 };
 
@@ -339,7 +349,7 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
     double accA[ME], accB[ME], accC[ME], accD[ME];  // rows R-2, R-1, R, R+1
     Iface fY;                                       // y-interface (R-2 | R-1)
     double amY[ME], apY[ME], dY[MW];
-    unsigned long long n_it = 0, n_solve = 0;
+    unsigned long long n_it = 0, n_solve = 0, n_app = 0;
     if (tma) {
         if (t == 0) mbar_init(bar);
         __syncthreads();
@@ -354,6 +364,12 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
 #pragma unroll
     for (int k = 0; k < MW; ++k) dY[k] = 0.0;
     memset(&fY, 0, sizeof(fY));
+    constexpr bool YS = UnsplitSmem<RP, NT, CAPA>::YS;
+    constexpr int NFY = UnsplitSmem<RP, NT, CAPA>::NF;
+    if constexpr (YS) {
+#pragma unroll
+        for (int k = 0; k < NFY + 2 * ME + MW; ++k) S.yrec[k][t] = 0.0;
+    }
 
     int s2 = 0, s1 = 2, s0 = 1;  // ring slots of rows R, R-1, R-2
     for (int R = R0; R <= R1; ++R) {
@@ -442,6 +458,18 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
 
         // ---- y: solve (R-1 | R), finish (R-2 | R-1) ----
         if (R > R0) {
+            if constexpr (YS) {  // the record of (R-2 | R-1) back from shared memory
+                double* fp = reinterpret_cast<double*>(&fY);
+#pragma unroll
+                for (int k = 0; k < NFY; ++k) fp[k] = S.yrec[k][t];
+#pragma unroll
+                for (int m = 0; m < ME; ++m) {
+                    amY[m] = S.yrec[NFY + m][t];
+                    apY[m] = S.yrec[NFY + ME + m][t];
+                }
+#pragma unroll
+                for (int k = 0; k < MW; ++k) dY[k] = S.yrec[NFY + 2 * ME + k][t];
+            }
             double cB[NC], cA[NC];
 #pragma unroll
             for (int k = 0; k < NC; ++k) {
@@ -464,6 +492,7 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
                 GuessTraits<RP>::template solve<2>(cB, cA, P, gy, fN, amN, apN);
                 if (GuessTraits<RP>::USES && cp <= mx + 3) {
                     n_it += GuessTraits<RP>::count(fN);
+                    n_app += GuessTraits<RP>::count_applied(fN);
                     n_solve += 1;
                 }
                 double wY[MW][ME], wN[MW][ME];
@@ -544,12 +573,25 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
                     }
                 }
             }
-            fY = fN;
             zY = zN;
+            if constexpr (YS) {
+                const double* fp = reinterpret_cast<const double*>(&fN);
 #pragma unroll
-            for (int m = 0; m < ME; ++m) { amY[m] = amN[m]; apY[m] = apN[m]; }
+                for (int k = 0; k < NFY; ++k) S.yrec[k][t] = fp[k];
 #pragma unroll
-            for (int k = 0; k < MW; ++k) dY[k] = dn[k];
+                for (int m = 0; m < ME; ++m) {
+                    S.yrec[NFY + m][t] = amN[m];
+                    S.yrec[NFY + ME + m][t] = apN[m];
+                }
+#pragma unroll
+                for (int k = 0; k < MW; ++k) S.yrec[NFY + 2 * ME + k][t] = dn[k];
+            } else {
+                fY = fN;
+#pragma unroll
+                for (int m = 0; m < ME; ++m) { amY[m] = amN[m]; apY[m] = apN[m]; }
+#pragma unroll
+                for (int k = 0; k < MW; ++k) dY[k] = dn[k];
+            }
         }
         // Publish the y sweep's neighbour increments now, which ends their live
         // range before the x work (fewer registers); every read of the previous
@@ -589,6 +631,7 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
             GuessTraits<RP>::template solve<1>(cL, cR, P, gx, fX, amX, apX);
             if (GuessTraits<RP>::USES && cp <= mx + 3 && t > 0) {
                 n_it += GuessTraits<RP>::count(fX);
+                n_app += GuessTraits<RP>::count_applied(fX);
                 n_solve += 1;
             }
             double wX[MW][ME];
@@ -707,7 +750,7 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
         s1 = s2;
         s2 = tmp;
     }
-    if (GuessTraits<RP>::USES && a.counters) counter_commit(a.counters, n_it, n_solve);
+    if (GuessTraits<RP>::USES && a.counters) counter_commit(a.counters, n_it, n_solve, n_app);
 }
 
 // ---------------------------------------------------------------------------
@@ -786,7 +829,7 @@ __device__ __forceinline__ void unsplit_tile2(const StepArgs& a, int strip, int 
     double accA[ME], accB[ME], accC[ME];  // rows R-2, R-1, R
     Iface fY;                             // y-interface (R-2 | R-1)
     double amY[ME], apY[ME], dY[MW];
-    unsigned long long n_it = 0, n_solve = 0;
+    unsigned long long n_it = 0, n_solve = 0, n_app = 0;
 #pragma unroll
     for (int m = 0; m < ME; ++m) {
         pf[m] = __ldg(qo + m * plane + (long long)R0 * pitch);
@@ -934,6 +977,7 @@ __device__ __forceinline__ void unsplit_tile2(const StepArgs& a, int strip, int 
             GuessTraits<RP>::template solve<2>(cB, cA, P, gy, fN, amN, apN);
             if (GuessTraits<RP>::USES && cp <= mx + 3) {
                 n_it += GuessTraits<RP>::count(fN);
+                n_app += GuessTraits<RP>::count_applied(fN);
                 n_solve += 1;
             }
             double dn[MW];
@@ -1034,6 +1078,7 @@ __device__ __forceinline__ void unsplit_tile2(const StepArgs& a, int strip, int 
             GuessTraits<RP>::template solve<1>(cL, cR, P, gx, fX, amX, apX);
             if (GuessTraits<RP>::USES && cp <= mx + 3 && t > 0) {
                 n_it += GuessTraits<RP>::count(fX);
+                n_app += GuessTraits<RP>::count_applied(fX);
                 n_solve += 1;
             }
             double wX[MW][ME];
@@ -1089,7 +1134,7 @@ __device__ __forceinline__ void unsplit_tile2(const StepArgs& a, int strip, int 
         s1 = s2;
         s2 = tmp;
     }
-    if (GuessTraits<RP>::USES && a.counters) counter_commit(a.counters, n_it, n_solve);
+    if (GuessTraits<RP>::USES && a.counters) counter_commit(a.counters, n_it, n_solve, n_app);
 }
 
 template <class RP, int NT, int MINB, int SPEC, bool CAPA = false, bool EVO = false>

@@ -108,3 +108,21 @@ def counters(solver, reset=True):
     out = (ctypes.c_ulonglong * 2)()
     _lib.check(dev._lib.claw2_patch_counters(dev.h, out, 1 if reset else 0))
     return int(out[0]), int(out[1])
+
+
+def newton_counts(solver, reset=True):
+    """(Newton steps needed, Newton steps applied, Riemann solves) since the
+    last reset: "applied" also counts the final step below the tolerance,
+    which every interface with two different states takes."""
+    dev = solver._dev
+    out = (ctypes.c_ulonglong * 3)()
+    _lib.check(dev._lib.claw2_patch_newton_counts(dev.h, out, 1 if reset else 0))
+    return int(out[0]), int(out[1]), int(out[2])
+
+
+def converged_guess(solver, on=True):
+    """Measurement aid: every step of the exact solver starts Newton from the
+    converged pressures (a pre-pass outside the kernel timing), so the step
+    kernel's time is the floor for any guess, learned or not."""
+    dev = solver._dev
+    _lib.check(dev._lib.claw2_patch_set_exact_guess(dev.h, 1 if on else 0))

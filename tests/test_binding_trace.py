@@ -44,3 +44,22 @@ def test_kept_calls_match_the_oracle(oracle, trace, key, k):
                              rp.rp_id, cp)
     assert cfl == float(trace[p + "cfl"])
     assert np.array_equal(q, trace[p + "qout"])
+
+
+def test_binding_preconditions_without_gpu():
+    # what the reference's unmodified ClawSolver2D does with the step module
+    # and the Riemann solver object before its first step
+    # (classic/solver.py:208-232, state.py:206-231, solver.py:230-238)
+    import importlib
+    import pyclaw_b200.classic2 as fmod
+    from pyclaw_b200 import riemann
+    importlib.reload(fmod)  # setup() reloads the module to flush its cparam block
+    assert vars(fmod.cparam) == {}
+    for name in ("advection_2D", "acoustics_2D", "euler_4wave_2D", "shallow_roe_with_efix_2D"):
+        rp = getattr(riemann, name)
+        assert rp.__name__.split('.')[-1] == name
+        assert rp.rpn2._cpointer is rp and rp.rpt2._cpointer is rp
+        assert name in riemann.static.num_eqn and name in riemann.static.num_waves
+        # state.set_cparam(rp): lists the block's parameters (none demanded), then assigns
+        assert [p for p in rp.cparam.__dir__() if '__' not in p] == []
+        setattr(rp.cparam, "gamma", 1.4)
