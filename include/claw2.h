@@ -212,6 +212,18 @@ int claw2_patch_evolve(claw2_patch* p, claw2_evolve_state* s);
  * call waits and returns the Courant number; with NULL it only enqueues. */
 int claw2_patch_step(claw2_patch* p, double dt, double* cfl);
 
+/* The same step in two parts around a halo exchange (no counterpart in the
+ * reference; petclaw exchanges before its step, src/petclaw/state.py:223-229):
+ * part 1 enqueues the ghost fill of every cell but the ghost rows of sides
+ * marked CLAW2_BC_NONE, and the step of the row blocks that read no ghost row;
+ * the caller then fills those ghost rows (the exchange may run on another
+ * stream meanwhile: part 1 neither reads nor writes them); part 2, enqueued
+ * after the exchange, fills their ghost columns and steps the first and last
+ * row blocks, and with cfl non-NULL waits and returns the Courant number.
+ * The result equals claw2_patch_step's.  A split step, the exact solver, host
+ * ghost cells or fewer than three row blocks run whole in part 2. */
+int claw2_patch_step_part(claw2_patch* p, double dt, int part, double* cfl);
+
 /* Many independent steps from host buffers (no counterpart in the reference,
  * whose step2 call moves one host qbc per step through f2py): for k < nsteps,
  * q_out[k] = one step (ghost fill, step, CFL) of q_in[k] with dt[k], each

@@ -98,6 +98,7 @@ _SIGNATURES = {
     "claw2_patch_euler_axisymmetric_source": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int,
                                                             ctypes.c_double]),
     "claw2_patch_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _c_double_p]),
+    "claw2_patch_step_part": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, _c_double_p]),
     "claw2_patch_evolve": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Claw2EvolveState)]),
     "claw2_patch_run_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
                                             ctypes.POINTER(ctypes.c_void_p), _c_double_p, _c_double_p]),

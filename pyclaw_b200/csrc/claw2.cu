@@ -292,7 +292,7 @@ void launch_unsplit_v(const StepArgs& a, cudaStream_t st, const CUtensorMap* tm)
         b.nstrips = ns;
     }
     const int nbk = (a.L.my + b.H - 1) / b.H;
-    dim3 grid(b.nstrips * nbk);
+    dim3 grid(b.tile_count > 0 ? b.tile_count : b.nstrips * nbk);
     if constexpr (AuxTraits<RP>::MAUX == 0 && !GuessTraits<RP>::USES) {
         if ((g_tune[RP::ID & (TUNE_SLOTS - 1)].variant & 8) && !a.capa) {  // the direction-split tile
             const bool ok = is_mc2(a.meth, RP::MWAVES) ? launch_unsplit_ws_s<RP, SPEC_MC2, EVO>(b, grid, st)
@@ -404,9 +404,10 @@ struct SplitF {
 };
 
 void launch_bc(double* q, const Layout& L, int meqn, const int* bcl, const int* bcu,
-               unsigned long long* cfl_bits, cudaStream_t st, int negate = 1) {
+               unsigned long long* cfl_bits, cudaStream_t st, int negate = 1, int part = 0) {
     BCArgs b;
     b.negate = negate;
+    b.part = part;
     b.q = q;
     b.L = L;
     b.meqn = meqn;
@@ -840,6 +841,7 @@ struct claw2_patch {
     double* guess = nullptr;                  // exact solver: learned guesses, x and y planes
     unsigned long long* counters = nullptr;   // exact solver: Newton steps needed, solves, steps applied
     int exact_guess = 0;                      // exact solver: 1 = start from the converged p* (measurement)
+    int split_part = 0;                       // 1 after claw2_patch_step_part(.., 1): part 2 must follow
     claw2_mlp* mlp = nullptr;
     // claw2_patch_evolve's captured attempts, one graph per starting buffer
     // parity, reused while nothing they captured changed: graph_gen counts
@@ -1334,17 +1336,56 @@ int claw2_patch_download_q(claw2_patch* p, double* q) {
 namespace {
 
 // Ghost fill + step (+ learned guess pre-pass, + tile schedule) of a patch on
-// its stream; the result goes to the pending buffer.
-int patch_enqueue_step(claw2_patch* p, double dt) {
+// its stream; the result goes to the pending buffer.  part 0: the whole step.
+// part 1 / part 2 (claw2_patch_step_part): a plain unsplit step split around a
+// halo exchange -- part 1 fills every ghost cell but the ghost rows of
+// internal sides and steps the row blocks that read no ghost row; part 2
+// fills those rows' ghost columns and steps the first and last row blocks.
+// Any other step (split, exact solver, custom BCs, no row block clear of the
+// ghost rows) runs whole in part 2.
+int patch_enqueue_step(claw2_patch* p, double dt, int part = 0) {
     double* qc = p->q[p->cur];
+    int ns = 0, H = 0, nb = 0;
+    unsplit_tiling(p->d.riemann, p->L.mx, p->L.my, ns, H, nb);
+    // row block b reads padded rows H b .. H b + min(H, my - H b) + 3: blocks
+    // 1 .. b_hi read no ghost row (H (b+1) + 3 <= my + 1 for a full block;
+    // a ragged last block of one row pushes its neighbour into the edge set)
+    const int b_hi = std::min(nb - 2, (p->L.my - 2) / std::max(H, 1) - 1);
+    if (part != 0) {
+        const bool simple = !p->d.dimensional_split && !p->ghosts_supplied &&
+                            p->d.riemann != CLAW2_RP_EULER_EXACT && b_hi >= 1;
+        if (!simple) {
+            if (part == 1) return CLAW2_OK;  // nothing runs before the exchange
+            part = 0;                        // part 2: the whole step
+        }
+    }
     if (p->ghosts_supplied) {  // the host filled every ghost cell (custom BCs)
         CUDA_TRY(cudaMemsetAsync(p->cfl, 0, sizeof(unsigned long long), p->st));
         p->ghosts_supplied = false;
     } else {
-        launch_bc(qc, p->L, p->d.num_eqn, p->d.bc_lower, p->d.bc_upper, p->cfl, p->st);
+        launch_bc(qc, p->L, p->d.num_eqn, p->d.bc_lower, p->d.bc_upper, p->cfl, p->st, 1, part);
         ++p->step_launches;
     }
     StepArgs a = patch_args(p, dt);
+    if (part != 0) {
+        a.H = H;
+        a.nstrips = ns;
+        if (part == 1) {  // row blocks 1 .. b_hi
+            a.tile_offset = ns;
+            a.tile_count = ns * b_hi;
+        } else {          // row block 0 and b_hi+1 .. nb-1
+            a.tile_jump_at = ns;
+            a.tile_jump = ns * b_hi;
+            a.tile_count = ns * (nb - b_hi);
+        }
+        if (part == 1 && p->timing) CUDA_TRY(cudaEventRecord(p->ev0, p->st));
+        dispatch<UnsplitF>(p->d.riemann, a, p->st, p->has_tmap ? &p->tmap[p->cur] : nullptr);
+        ++p->step_launches;
+        if (part == 2 && p->timing) CUDA_TRY(cudaEventRecord(p->ev1, p->st));
+        CUDA_TRY(cudaGetLastError());
+        if (part == 2) p->pending = true;
+        return CLAW2_OK;
+    }
     const bool exact_unsplit = p->d.riemann == CLAW2_RP_EULER_EXACT && !p->d.dimensional_split;
     if (exact_unsplit && p->exact_guess == 1) {
         // converged pressures as guesses, outside the timed region: the step
@@ -1368,8 +1409,6 @@ int patch_enqueue_step(claw2_patch* p, double dt) {
         dispatch<SplitF>(p->d.riemann, ax, ay, p->st, 3);
         p->step_launches += 2;
     } else {
-        int ns, H, nb;
-        unsplit_tiling(p->d.riemann, p->L.mx, p->L.my, ns, H, nb);
         // a schedule only matters when the tiles outnumber the CTA slots (2 per SM)
         if (ns * nb > 2 * p->nsm && lpt_prepare(p, ns * nb, H) == CLAW2_OK) {
             lpt_n = ns * nb;
@@ -1547,11 +1586,30 @@ extern "C" {
 
 int claw2_patch_step(claw2_patch* p, double dt, double* cfl) {
     if (!p) return fail(CLAW2_EINVAL, "null patch");
+    if (p->split_part == 1) return fail(CLAW2_EINVAL, "part 1 of a split step is enqueued: finish it with part 2");
     if (!(dt >= 0.0) || !std::isfinite(dt)) return fail(CLAW2_EINVAL, "dt must be finite and >= 0");
     DeviceGuard g(p->device);
     const int rc = patch_enqueue_step(p, dt);
     if (rc) return rc;
     if (cfl) return claw2_patch_cfl(p, cfl);
+    return CLAW2_OK;
+}
+
+int claw2_patch_step_part(claw2_patch* p, double dt, int part, double* cfl) {
+    if (!p) return fail(CLAW2_EINVAL, "null patch");
+    if (part != 1 && part != 2) return fail(CLAW2_EINVAL, "part must be 1 or 2 (got %d)", part);
+    if (!(dt >= 0.0) || !std::isfinite(dt)) return fail(CLAW2_EINVAL, "dt must be finite and >= 0");
+    if (p->pending) return fail(CLAW2_EINVAL, "a step is pending: accept or reject it first");
+    if (part == 2 && p->split_part != 1) return fail(CLAW2_EINVAL, "part 2 must follow part 1 of the same step");
+    if (part == 1 && p->split_part == 1) return fail(CLAW2_EINVAL, "part 1 of this step is already enqueued");
+    DeviceGuard g(p->device);
+    const int rc = patch_enqueue_step(p, dt, part);
+    if (rc) {
+        p->split_part = 0;
+        return rc;
+    }
+    p->split_part = part == 1 ? 1 : 0;
+    if (part == 2 && cfl) return claw2_patch_cfl(p, cfl);
     return CLAW2_OK;
 }
 

@@ -57,6 +57,10 @@ struct StepArgs {
     const int* tile_order = nullptr;
     unsigned int* tile_cost = nullptr;
     int nstrips = 0;
+    // a launch over a subset of the tiles (no schedule): CTA b runs tile
+    // b + tile_offset, plus tile_jump from CTA tile_jump_at on (the interior
+    // row blocks, or the first and last ones, of a slab's overlapped step)
+    int tile_offset = 0, tile_jump_at = 1 << 30, tile_jump = 0, tile_count = 0;
     // aux planes (same layout as q) for solvers with aux data, else nullptr
     const double* __restrict__ aux = nullptr;
     // device-resident time loop: dt from here, no work once it is done (else nullptr)
@@ -67,6 +71,18 @@ struct StepArgs {
     // flux2.f90:104-119,134-203 with dtdx1d = dtdx / kappa)
     const double* __restrict__ capa = nullptr;
 };
+
+// The tile a CTA of a step launch runs (see StepArgs::tile_order, tile_offset).
+__device__ __forceinline__ int tile_index(const StepArgs& a) {
+    int tile = blockIdx.x;
+    if (a.tile_order) {
+        const int t = a.tile_order[blockIdx.x];
+        if (t >= 0 && t < (int)gridDim.x) tile = t;  // a schedule is a permutation; anything else is ignored
+    } else {
+        tile += a.tile_offset + ((int)blockIdx.x >= a.tile_jump_at ? a.tile_jump : 0);
+    }
+    return tile;
+}
 
 // philim.f90:16-35
 __device__ __forceinline__ double philim(double a, double b, int meth) {
@@ -1142,11 +1158,7 @@ __global__ void __launch_bounds__(NT, MINB) k_step_unsplit2(const StepArgs a) {
     if (EVO && a.evo->done) return;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     UnsplitSmem2<RP, NT, CAPA>& S = *reinterpret_cast<UnsplitSmem2<RP, NT, CAPA>*>(smem_raw);
-    int tile = blockIdx.x;
-    if (a.tile_order) {
-        const int t = a.tile_order[blockIdx.x];
-        if (t >= 0 && t < (int)gridDim.x) tile = t;
-    }
+    const int tile = tile_index(a);
     long long t0 = 0;
     if (a.tile_cost && threadIdx.x == 0) t0 = clock64();
     double cfl = 0.0;
@@ -1164,26 +1176,27 @@ __global__ void __launch_bounds__(NT, MINB) k_step_unsplit2(const StepArgs a) {
 // and the second NT (the X warps) its x-interfaces, so each thread carries
 // half the live state of unsplit_tile and twice as many warps fit on an SM
 // (16 instead of 8 for Euler), which is what the FP64 pipe of a latency-bound
-// step needs.  The two warp groups are decoupled by named barriers instead
-// of CTA-wide ones, so one group may run up to two rows ahead of the other
-// and rows where only one direction has work do not stall the other:
-//   Y, row R: [wait EMPTY(R-2)] prepare the column's cell of row R into a
+// step needs.  The two warp groups meet only through named barriers used by
+// row parity, so the x work of a row overlaps the y work of the same row:
+//   Y, row R: [wait EMPTY(R-1)] prepare the column's cell of row R into a
 //      4-row ring, prefetch row R+1, [arrive CELLS(R)]; solve (R-1 | R);
 //      finish (R-2 | R-1) (limiter with the waves below and above,
 //      correction, two transverse solves); [Y] exchange with the neighbour
-//      columns [Y]; publish its total for row R-2, [arrive YS(R)].
+//      columns [Y]; write row R-3 = q + (its y total + the X group's total);
+//      after the last row, [wait EMPTY(R1)] and write row R1-2.
 //   X, row R: [wait CELLS(R)] solve (cp-1 | cp) of row R, store its waves
-//      [X]; gather the neighbour's increments of row R-1, [wait YS(R)] write
-//      row R-2 = q + (Y's total + X's total); finish row R (limiter with the
-//      neighbours' waves, correction, two transverse solves), publish column
-//      cp-1's increments [X]; [arrive EMPTY(R)]: rows <= R-2 of the ring and
-//      Y's total of R-2 are free.
-// CELLS, YS and EMPTY are pairs of barriers used by row parity (Y arrives,
-// X waits; EMPTY the other way), each with all 2*NT threads; [X] and [Y] are
-// the groups' own barriers.  Every arrival has its wait: Y arrives CELLS and
-// YS on every row, X waits on both on every row; X arrives EMPTY on rows
-// R0..R1-2 and Y waits on rows R0+2..R1.  The y-interface being finished,
-// its fluctuations and its dot products wait in shared memory (per column,
+//      [X]; gather the neighbour's increments of row R-1, publish its total of
+//      row R-2; finish row R (limiter with the neighbours' waves, correction,
+//      two transverse solves), publish column cp-1's increments [X];
+//      [arrive EMPTY(R)].
+// CELLS(R): row R's cells are in the ring.  EMPTY(R): the X group is done
+// with row R (so the ring slot that row R+1 reuses, rows R-3's, and the
+// total buffer Y reads next are free).  Both are pairs of barriers used by
+// row parity, each with all 2*NT threads; [X] and [Y] are the groups' own
+// barriers.  Every arrival has its wait: Y arrives CELLS on every row and X
+// waits on every row; X arrives EMPTY on every row and Y waits on rows
+// R0+1..R1 and once after the loop.  The y-interface being finished, its
+// fluctuations and its dot products wait in shared memory (per column,
 // touched only by that column's Y thread).  The increments are the same
 // terms as in unsplit_tile; only the order of the per-cell sum differs (the
 // x and y parts are summed apart and then added).  Solvers without aux data
@@ -1198,7 +1211,7 @@ struct UnsplitSmemWS {
     double xl[3][ME][NT];            // X -> column cp-1: rows R-1, R, R+1
     double yl[2][ME][NT];            // Y -> column cp-1: rows R-2, R-1
     double yr[2][ME][NT];            // Y -> column cp+1: rows R-2, R-1
-    double ys[2][ME][NT];            // Y's total of row R-2, by row parity (Y -> X)
+    double xs[2][ME][NT];            // X's total of row R-2, by row parity (X -> Y)
     double fy[NF][NT];               // Y: the y-interface being finished, (R-2 | R-1)
     double amy[ME][NT], apy[ME][NT];  // its fluctuations
     double dy[MW][NT];               // its waves' dot products with the waves below it
@@ -1206,7 +1219,7 @@ struct UnsplitSmemWS {
 };
 
 // named barriers of the direction-split tile (0 is __syncthreads)
-enum { NB_X = 1, NB_Y = 2, NB_CELLS = 3, NB_YS = 5, NB_EMPTY = 7 };
+enum { NB_X = 1, NB_Y = 2, NB_CELLS = 3, NB_EMPTY = 5 };
 
 template <int ID, int N>
 __device__ __forceinline__ void nb_sync() {
@@ -1263,16 +1276,17 @@ __device__ __forceinline__ void unsplit_tile_ws(const StepArgs& a, int strip, in
         // ================= Y warps =================
         if (REG_Y > 0) asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(REG_Y));
         const double* qo = a.qold + cpl;
-        double pf[ME], yA[ME], yB[ME];  // prefetched row; increments of rows R-2, R-1
+        double* qn = a.qnew + cpl;
+        double pf[ME], yA[ME], yB[ME], yC[ME];  // prefetched row; increments of rows R-2, R-1; total of R-3
 #pragma unroll
         for (int m = 0; m < ME; ++m) {
             pf[m] = __ldg(qo + m * plane + (long long)R0 * pitch);
-            yA[m] = yB[m] = 0.0;
+            yA[m] = yB[m] = yC[m] = 0.0;
         }
         bool zY = false;
         for (int R = R0; R <= R1; ++R) {
             const int s2 = R & 3, s1 = (R - 1) & 3;
-            if (R >= R0 + 2) nb_sync_parity<NB_EMPTY, N2>(R);  // X is done with row R-4's slot and ys(R-4)
+            if (R >= R0 + 1) nb_sync_parity<NB_EMPTY, N2>(R - 1);  // X done with row R-1: the slot of R-4 is free
             {
                 double q[ME], c[NC];
 #pragma unroll
@@ -1402,18 +1416,33 @@ __device__ __forceinline__ void unsplit_tile_ws(const StepArgs& a, int strip, in
                 yB[m] = yB[m] + S.yl[1][m][tr] + S.yr[1][m][tl];
             }
             nb_sync<NB_Y, NT>();  // every read of the exchange done before the next row's writes
+            if (R >= R0 + 5 && out_col) {  // row R-3: both totals complete (X's since its row R-1)
+                double v[ME];
+#pragma unroll
+                for (int m = 0; m < ME; ++m) v[m] = S.cell[(R - 3) & 3][m][t] + (yC[m] + S.xs[(R - 3) & 1][m][t]);
+#pragma unroll
+                for (int m = 0; m < ME; ++m) qn[m * plane + (long long)(R - 3) * pitch] = v[m];
+                if (!all_finite<ME>(v)) atomicOr(a.status, 1);
+            }
 #pragma unroll
             for (int m = 0; m < ME; ++m) {
-                S.ys[R & 1][m][t] = yA[m];  // row R-2 complete on the y side
+                yC[m] = yA[m];  // row R-2 complete on the y side
                 yA[m] = yB[m];
                 yB[m] = 0.0;
             }
-            nb_arrive_parity<NB_YS, N2>(R);
+        }
+        nb_sync_parity<NB_EMPTY, N2>(R1);  // X done with the last row: its total of row R1-2
+        if (R1 >= R0 + 4 && out_col) {
+            double v[ME];
+#pragma unroll
+            for (int m = 0; m < ME; ++m) v[m] = S.cell[(R1 - 2) & 3][m][t] + (yC[m] + S.xs[(R1 - 2) & 1][m][t]);
+#pragma unroll
+            for (int m = 0; m < ME; ++m) qn[m * plane + (long long)(R1 - 2) * pitch] = v[m];
+            if (!all_finite<ME>(v)) atomicOr(a.status, 1);
         }
     } else {
         // ================= X warps =================
         if (REG_X > 0) asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(REG_X));
-        double* qn = a.qnew + cpl;
         double x0[ME], x1[ME], x2[ME];  // increments of rows R-2, R-1, R (this column)
 #pragma unroll
         for (int m = 0; m < ME; ++m) x0[m] = x1[m] = x2[m] = 0.0;
@@ -1457,15 +1486,7 @@ __device__ __forceinline__ void unsplit_tile_ws(const StepArgs& a, int strip, in
                 x0[m] = x0[m] + S.xl[0][m][tr];  // rows R-2, R-1, R from the neighbour's row R-1
                 x1[m] = x1[m] + S.xl[1][m][tr];
                 x2[m] = x2[m] + S.xl[2][m][tr];
-            }
-            nb_sync_parity<NB_YS, N2>(R);  // Y's total of row R-2
-            if (R >= R0 + 4 && out_col) {
-                double v[ME];
-#pragma unroll
-                for (int m = 0; m < ME; ++m) v[m] = S.cell[(R - 2) & 3][m][t] + (S.ys[R & 1][m][t] + x0[m]);
-#pragma unroll
-                for (int m = 0; m < ME; ++m) qn[m * plane + (long long)(R - 2) * pitch] = v[m];
-                if (!all_finite<ME>(v)) atomicOr(a.status, 1);
+                S.xs[R & 1][m][t] = x0[m];  // row R-2 complete on the x side
             }
             double x3[ME], xbL[ME], xcL[ME], xaL[ME];
 #pragma unroll
@@ -1531,7 +1552,7 @@ __device__ __forceinline__ void unsplit_tile_ws(const StepArgs& a, int strip, in
                 x1[m] = x2[m];
                 x2[m] = x3[m];
             }
-            if (R + 2 <= R1) nb_arrive_parity<NB_EMPTY, N2>(R);  // rows <= R-2 and ys(R-2) released
+            nb_arrive_parity<NB_EMPTY, N2>(R);  // done with row R; its total of row R-2 published
         }
     }
 }
@@ -1542,11 +1563,7 @@ __global__ void __launch_bounds__(2 * NT, MINB) k_step_unsplit_ws(const StepArgs
     if (EVO && a.evo->done) return;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     UnsplitSmemWS<RP, NT>& S = *reinterpret_cast<UnsplitSmemWS<RP, NT>*>(smem_raw);
-    int tile = blockIdx.x;
-    if (a.tile_order) {
-        const int t = a.tile_order[blockIdx.x];
-        if (t >= 0 && t < (int)gridDim.x) tile = t;
-    }
+    const int tile = tile_index(a);
     long long t0 = 0;
     if (a.tile_cost && threadIdx.x == 0) t0 = clock64();
     double cfl = 0.0;
@@ -1563,11 +1580,7 @@ template <class RP, int NT, int MINB, int SPEC>
 __global__ void __launch_bounds__(NT, MINB) k_step_unsplit_tma(const StepArgs a, const __grid_constant__ CUtensorMap tm) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     UnsplitSmemTma<RP, NT>& S = *reinterpret_cast<UnsplitSmemTma<RP, NT>*>(smem_raw);
-    int tile = blockIdx.x;
-    if (a.tile_order) {
-        const int t = a.tile_order[blockIdx.x];
-        if (t >= 0 && t < (int)gridDim.x) tile = t;
-    }
+    const int tile = tile_index(a);
     long long t0 = 0;
     if (a.tile_cost && threadIdx.x == 0) t0 = clock64();
     double cfl = 0.0;
@@ -1588,11 +1601,7 @@ __global__ void __launch_bounds__(NT, MINB) k_step_unsplit(const StepArgs a) {
     if (EVO && a.evo->done) return;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     UnsplitSmem<RP, NT, CAPA>& S = *reinterpret_cast<UnsplitSmem<RP, NT, CAPA>*>(smem_raw);
-    int tile = blockIdx.x;
-    if (a.tile_order) {
-        const int t = a.tile_order[blockIdx.x];
-        if (t >= 0 && t < (int)gridDim.x) tile = t;  // a schedule is a permutation; anything else is ignored
-    }
+    const int tile = tile_index(a);
     long long t0 = 0;
     if (a.tile_cost && threadIdx.x == 0) t0 = clock64();
     double cfl = 0.0;
@@ -1927,6 +1936,10 @@ struct BCArgs {
     int bcl[2], bcu[2];
     unsigned long long* cfl_bits;
     int negate = 1;  // a wall negates the normal momentum (q); 0 for aux (plain mirror)
+    // 0: every ghost cell; 1: all but the ghost rows of internal sides
+    // (CLAW2_BC_NONE), which a halo exchange may be writing; 2: only the
+    // ghost columns of those rows (their corners), after the exchange
+    int part = 0;
 };
 
 __device__ __forceinline__ int bc_src(int c, int n, int lo, int up, bool& flip) {
@@ -1954,7 +1967,7 @@ static __global__ void k_bc_fill(const BCArgs a) {
     const int nrow = 4 * (mx + 4);   // cells of the 4 ghost rows
     const int ncol = 4 * my;         // ghost-column cells of interior rows
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k == 0 && a.cfl_bits) *a.cfl_bits = 0ull;
+    if (k == 0 && a.cfl_bits && a.part != 2) *a.cfl_bits = 0ull;
     if (k >= nrow + ncol) return;
     int c, r;
     if (k < nrow) {
@@ -1966,6 +1979,11 @@ static __global__ void k_bc_fill(const BCArgs a) {
         const int g = kk & 3;
         r = 2 + (kk >> 2);
         c = (g < 2) ? g : mx + g;
+    }
+    if (a.part != 0) {
+        const bool halo_row = (r < 2 && a.bcl[1] == CLAW2_BC_NONE) || (r >= my + 2 && a.bcu[1] == CLAW2_BC_NONE);
+        if (a.part == 1 && halo_row) return;
+        if (a.part == 2 && !(halo_row && (c < 2 || c >= mx + 2))) return;
     }
     bool fx, fy;
     const int cs = bc_src(c, mx, a.bcl[0], a.bcu[0], fx);

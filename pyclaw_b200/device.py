@@ -119,6 +119,17 @@ class DevicePatch(object):
         _lib.check(self._lib.claw2_patch_step(self.h, ctypes.c_double(dt), None))
         return None
 
+    def step_part(self, dt, part, want_cfl=True):
+        """One half of a step split around a halo exchange
+        (claw2_patch_step_part): part 1 the interior row blocks, part 2 the
+        ghost corners and the first and last row blocks; part 2 returns the
+        Courant number (waits) unless want_cfl is False."""
+        if part == 2 and want_cfl:
+            _lib.check(self._lib.claw2_patch_step_part(self.h, ctypes.c_double(dt), 2, ctypes.byref(self._cfl)))
+            return self._cfl.value
+        _lib.check(self._lib.claw2_patch_step_part(self.h, ctypes.c_double(dt), int(part), None))
+        return None
+
     def run_host(self, q_in, q_out, dt):
         """Independent steps from host arrays: q_out[k] = step of q_in[k] with
         dt[k] (claw2_patch_run_host; copies overlap compute).  q_in / q_out

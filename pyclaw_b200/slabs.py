@@ -233,7 +233,9 @@ def make_slab_solver_class(base):
             self.slab = None          # (rank, world, periodic_y, group)
             self.global_delta = None  # (dx, dy) of the global grid
             self.transport = None     # halo/CFL transport (None: torch.distributed over the group)
+            self.overlap = False      # step the interior row blocks while the halo rows move
             self._stream_set = False  # the patch runs on torch's current stream (with the halo copies)
+            self._side = None         # the halo exchange's stream when overlapping
             super().__init__(riemann_solver, claw_package)
 
         def _device_desc(self, solution):
@@ -259,10 +261,31 @@ def make_slab_solver_class(base):
                 dev.set_stream(torch.cuda.current_stream().cuda_stream)  # one stream for NCCL + kernels
                 self._stream_set = True
             my = state.grid.num_cells[1]
-            if world > 1:
-                planes = DevicePlanes(dev)
-                exchange_rows(planes.get_rows, planes.set_rows, my, rank, world, periodic, group, self.transport)
-            cfl = dev.step(self.dt)
+            if world > 1 and self.overlap:
+                # interior row blocks on the patch's stream while the halo rows
+                # move on a side stream (the interior neither reads nor writes
+                # them), then the ghost corners and the edge row blocks
+                import torch
+                main = torch.cuda.current_stream()
+                if self._side is None:
+                    self._side = torch.cuda.Stream()
+                ready = torch.cuda.Event()
+                ready.record(main)              # the current q (last step accepted) is complete
+                dev.step_part(self.dt, 1)
+                with torch.cuda.stream(self._side):
+                    self._side.wait_event(ready)
+                    planes = DevicePlanes(dev)
+                    exchange_rows(planes.get_rows, planes.set_rows, my, rank, world, periodic, group, self.transport)
+                    moved = torch.cuda.Event()
+                    moved.record(self._side)
+                main.wait_event(moved)
+                cfl = dev.step_part(self.dt, 2)
+            else:
+                if world > 1:
+                    planes = DevicePlanes(dev)
+                    exchange_rows(planes.get_rows, planes.set_rows, my, rank, world, periodic, group,
+                                  self.transport)
+                cfl = dev.step(self.dt)
             self.cfl.update_global_max(global_cfl(cfl, device="cuda", group=group, transport=self.transport))
 
     return SlabClawSolver2D
