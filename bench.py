@@ -73,8 +73,10 @@ def parse():
     ap.add_argument("--replicas", action="store_true",
                     help="with --gpus N > 1: N independent copies of the problem instead of the row-slab "
                          "decomposition")
-    ap.add_argument("--no-overlap", action="store_true",
-                    help="row slabs: exchange the halo rows before the step instead of during its interior part")
+    ap.add_argument("--overlap", action="store_true",
+                    help="row slabs: step the interior row blocks while the halo rows move (two launches per "
+                         "step; off by default: at 1024^2 the second launch's tail costs more than the "
+                         "exchange it hides)")
     ap.add_argument("--slab", action="store_true",
                     help="use the row-slab code path even on one GPU (one slab: no neighbours)")
     ap.add_argument("--state", default=None,
@@ -502,11 +504,11 @@ def run_ours(args):
     side = torch.cuda.Stream(dev) if slab else None
 
     def slab_step(dt):
-        """One decomposed step: the interior row blocks on the patch's stream
-        while the halo rows move on a side stream, then the edge row blocks;
-        the global Courant number and the same accept decision on every rank
-        (--no-overlap: the exchange first, then the whole step)."""
-        if args.no_overlap:
+        """One decomposed step: the halo rows in, the local step, the global
+        Courant number and the same accept decision on every rank (--overlap:
+        the interior row blocks on the patch's stream while the halo rows move
+        on a side stream, then the edge row blocks)."""
+        if not args.overlap:
             planes = slabs.DevicePlanes(patch)
             slabs.exchange_rows(planes.get_rows, planes.set_rows, n, rank, world, False)
             local = patch.step(dt)
@@ -702,8 +704,8 @@ def run_ours(args):
                                   "parallelism": ("row slabs: %d x %d grid, one %d x %d slab per rank, halo "
                                                   "exchange (NCCL%s) + CFL all-reduce every step"
                                                   % (n, n * world, n, n,
-                                                     "" if args.no_overlap else ", overlapping the interior "
-                                                     "row blocks")) if slab else
+                                                     ", overlapping the interior row blocks" if args.overlap
+                                                     else "")) if slab else
                                                  ("%d independent replicas" % world),
                                   "launch_shape": {"variant": shape[0], "rows": shape[1],
                                                    "trials_ms": {"%d/%d" % k: round(v, 4)
