@@ -797,6 +797,37 @@ struct RPEulerExact {
                                                  Iface& f, double (&amdq)[MEQN], double (&apdq)[MEQN]) {
         solve_g<IXY>(cL, cR, p, 0.0, f, amdq, apdq);
     }
+    // Two equal states: star() returns p* = p, u* = u at once, the fan is two
+    // rarefactions of zero width, so the waves and fluctuations are zero and
+    // the speeds are solve_g's expressions at ps = p (pow(1, .) = 1):
+    // 0.5 ((u - c) + (u* - c)) and 0.5 ((u + c) + (u* + c)).  (States that
+    // generate vacuum -- c = 0 -- take the Roe fallback's record, as solve_g.)
+    template <int IXY>
+    __device__ __forceinline__ static void zero_iface(const double (&cL)[NC], const double (&cR)[NC],
+                                                      const RPParams& p, Iface& f) {
+        constexpr int UN = (IXY == 1) ? UX : UY;
+        const exact_euler::Gas G = exact_euler::make_gas(p.c[0]);
+        const double ul = cL[UN], cl = cL[CS], ur = cR[UN], cr = cR[CS];
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int m = 0; m < 4; ++m) f.w[k][m] = 0.0;
+        f.iters = 0;
+        f.applied = 0;
+        if (exact_euler::vacuum(G, ul, cl, ur, cr)) {
+            double cl9[9], cr9[9];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) { cl9[k] = cL[k]; cr9[k] = cR[k]; }
+            RPEulerRoe::Iface fr;
+            RPEulerRoe::template zero_iface<IXY>(cl9, cr9, p, fr);
+            f.s[0] = fr.u - fr.a; f.s[1] = fr.u; f.s[2] = fr.u + fr.a;
+            return;
+        }
+        const double us = ul;
+        f.s[0] = 0.5 * ((ul - cl) + (us - cl));
+        f.s[1] = us;
+        f.s[2] = 0.5 * ((ur + cr) + (us + cr));
+    }
     template <int IXY>
     __device__ __forceinline__ static void rpt2(const Iface& f, const RPParams& p, const double (&asdq)[MEQN],
                                                 double (&bm)[MEQN], double (&bp)[MEQN]) {

@@ -344,14 +344,14 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
     const double* ko = CAPA ? a.capa + cpl : nullptr;
     double pfk = CAPA ? __ldg(ko + (long long)R0 * pitch) : 1.0;
 
-    // Zero-jump shortcut (solvers without aux data or guesses, q-waves): when
+    // Zero-jump shortcut (solvers without aux data, q-waves): when
     // every lane of a warp has equal cells on both sides of its interface, the
     // warp builds the interface's record with zero strengths and only the Roe
     // state the Courant number needs, and skips the finish (limiter,
     // correction, transverse solves), whose increments are all zero.  Warp-
     // uniform decisions, so no lane diverges; the results equal the full
     // path's up to the sign of zero terms.
-    constexpr bool ZS = SkipTraits<RP>::OK && MA == 0 && !CAPA && !GuessTraits<RP>::USES;
+    constexpr bool ZS = SkipTraits<RP>::OK && MA == 0 && !CAPA;
     const bool zs = ZS && (SPEC != SPEC_ANY || a.meth.fwave == 0);
     bool zY = false;  // the y-interface being finished, (R-2 | R-1), is zero in the whole warp
 
@@ -502,6 +502,7 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
                 for (int m = 0; m < ME; ++m) amN[m] = apN[m] = 0.0;
 #pragma unroll
                 for (int k = 0; k < MW; ++k) dn[k] = 0.0;
+                if (GuessTraits<RP>::USES && cp <= mx + 3) n_solve += 1;  // a solve with no Newton step
             } else {
                 double gy = 0.0;
                 if (GuessTraits<RP>::USES && a.guess) gy = a.guess[plane + (long long)R * pitch + cpl];
@@ -635,6 +636,7 @@ __device__ __forceinline__ void unsplit_tile(const StepArgs& a, int strip, int r
             zX = ZS && (!xrow || (zs && __all_sync(0xffffffffu, same_q<ME, NC>(cL, cR))));
             if (ZS && zX) {
                 SkipTraits<RP>::template zero_iface<1>(cL, cR, P, fX);
+                if (GuessTraits<RP>::USES && xrow && cp <= mx + 3 && t > 0) n_solve += 1;
 #pragma unroll
                 for (int m = 0; m < ME; ++m) amX[m] = apX[m] = 0.0;
 #pragma unroll
