@@ -314,23 +314,24 @@ void rpn2_psystem(int ixy, int mbc, int mx, const CSlice& ql, const CSlice& qr, 
         }
     }
 }
-// Transverse solve: asdq entered cell i1; its part going down (up) in the
-// transverse direction is the component along the cell below's (above's)
-// eigenvector in the two-medium split of the interface it crosses, times that
-// wave's speed.  Sound speeds from the strain at the start of the step
-// (aux component 4, set before each step).
-void rpt2_psystem(int ixy, int imp, int mbc, int mx, const CSlice& aux1, const CSlice& aux2, const CSlice& aux3,
+// Transverse solve: asdq entered cell i1; it is split into the cell below's
+// down-going eigenvector (1, 0, Zm) and the cell above's up-going one
+// (1, 0, -Zp) -- one decomposition with the two neighbours' impedances -- and
+// each part is multiplied by its cell's speed.  Sound speeds from the strain
+// at the start of the step (aux component 4, set before each step).  This
+// split reproduces the reference's psystem_2d gauges
+// (examples/psystem_2d/test_2d_psystem.py:8-24) to their printed digits.
+void rpt2_psystem(int ixy, int imp, int mbc, int mx, const CSlice& aux1, const CSlice& /*aux2*/, const CSlice& aux3,
                   const Slice& asdq, const Slice& bmasdq, const Slice& bpasdq) {
     const int mu = (ixy == 1) ? 1 : 2, mv = (ixy == 1) ? 2 : 1;
     for (int i = 2 - mbc; i <= mx + mbc; ++i) {
         const int i1 = (imp == 1) ? i - 1 : i;
-        const double rhom = aux1(0, i1), rho0 = aux2(0, i1), rhop = aux3(0, i1);
+        const double rhom = aux1(0, i1), rhop = aux3(0, i1);
         const double cm = std::sqrt(psys_sigmap(aux1(3, i1), aux1(1, i1), aux1(2, i1)) / rhom);
-        const double c0 = std::sqrt(psys_sigmap(aux2(3, i1), aux2(1, i1), aux2(2, i1)) / rho0);
         const double cp = std::sqrt(psys_sigmap(aux3(3, i1), aux3(1, i1), aux3(2, i1)) / rhop);
-        const double zm = rhom * cm, z0 = rho0 * c0, zp = rhop * cp;
-        const double bdown = (asdq(mv, i) + z0 * asdq(0, i)) / (zm + z0);
-        const double bup = (z0 * asdq(0, i) - asdq(mv, i)) / (z0 + zp);
+        const double zm = rhom * cm, zp = rhop * cp;
+        const double bdown = (asdq(mv, i) + zp * asdq(0, i)) / (zm + zp);
+        const double bup = (zm * asdq(0, i) - asdq(mv, i)) / (zm + zp);
         bmasdq(0, i) = -cm * bdown;
         bmasdq(mu, i) = 0.0;
         bmasdq(mv, i) = -cm * bdown * zm;

@@ -1009,9 +1009,10 @@ struct RPVcAdvectionVec {
 // (relation 2).  f-wave solver: the flux difference across an interface is
 // split into the left cell's eigenvector (1, Z, 0) at speed -c and the right
 // cell's (1, -Z, 0) at speed c, c = sqrt(sigma'(eps) / rho), Z = rho c
-// (LeVeque 2002, sec. 15.5).  The transverse solve splits a fluctuation at
-// the interfaces below and above the cell it entered with the impedances of
-// the cells there, from the strain in aux.
+// (LeVeque 2002, sec. 15.5).  The transverse solve splits a fluctuation
+// into the cell below's down-going and the cell above's up-going eigenvector
+// in one decomposition, with those cells' impedances from the strain in aux
+// (the split that reproduces the reference's psystem_2d gauges).
 // Cell: q, u, v, sigma, c, Z (from q) and c, Z (from the aux strain).
 // ---------------------------------------------------------------------------
 struct RPPsystem {
@@ -1077,12 +1078,14 @@ struct RPPsystem {
     }
     template <int IXY>
     __device__ __forceinline__ static void rpt2_aux(const double (&asdq)[MEQN], const double (&cm)[NC],
-                                                    const double (&c0)[NC], const double (&cp)[NC],
+                                                    const double (&)[NC], const double (&cp)[NC],
                                                     double (&bm)[MEQN], double (&bp)[MEQN]) {
         constexpr int MU = Dir<IXY>::MU, MV = Dir<IXY>::MV;
-        const double zm = cm[ZT], z0 = c0[ZT], zp = cp[ZT];
-        const double bdown = (asdq[MV] + z0 * asdq[0]) / (zm + z0);
-        const double bup = (z0 * asdq[0] - asdq[MV]) / (z0 + zp);
+        // one split of asdq into the cell below's down-going eigenvector
+        // (1, 0, Zm) and the cell above's up-going one (1, 0, -Zp)
+        const double zm = cm[ZT], zp = cp[ZT];
+        const double bdown = (asdq[MV] + zp * asdq[0]) / (zm + zp);
+        const double bup = (zm * asdq[0] - asdq[MV]) / (zm + zp);
         bm[0] = -cm[CT] * bdown; bm[MU] = 0.0; bm[MV] = -cm[CT] * bdown * zm;
         bp[0] = cp[CT] * bup;    bp[MU] = 0.0; bp[MV] = -cp[CT] * bup * zp;
     }

@@ -7,7 +7,7 @@ branch (with the f-wave p-system and with q-wave solvers run as the reference
 would run them with fwave = True) and the p-system's normal and transverse
 solves to the oracle at 1e-12 relative, and the p-system example's device run
 (gauges gathered on the device every step, the strain copied into aux by the
-before-step hook) to the oracle's run.
+before-step hook) to the oracle's run and to the reference's own gauge files.
 """
 import os
 
@@ -145,6 +145,21 @@ def test_psystem_device_run_matches_oracle(oracle, tmp_path):
     Fg = np.loadtxt(os.path.join(str(tmp_path / "g"), "F.txt"))
     Fo = np.loadtxt(os.path.join(str(tmp_path / "o"), "F.txt"))
     assert Fg.shape == (11, 2) and np.allclose(Fg, Fo, rtol=1e-11, atol=0)
+
+
+def test_psystem_gauge_goldens_on_device(goldens, tmp_path):
+    # examples/psystem_2d/test_2d_psystem.py:8-24 on the device path: the
+    # reference's four gauges (in memory and in the files) after the run to t = 1
+    claw = workloads.psystem(cells_per_layer=6, tfinal=1., outdir=str(tmp_path))
+    claw.run()
+    st = claw.solution.state
+    for k, g in enumerate(("0.25_0.25", "17.85_1.25", "3.25_18.75", "11.75_11.75")):
+        expected = goldens["psystem_gauge" + g]
+        mem = np.asarray(st.gauge_data[k])
+        assert mem.shape == expected.shape
+        assert np.allclose(expected, mem)
+        assert np.allclose(expected, np.loadtxt(st.grid.gauge_files[k].name))
+        assert np.max(np.abs(mem - expected)) <= 1e-9
 
 
 def test_gauge_gather_matches_download(tmp_path):
