@@ -339,7 +339,11 @@ def learned_workload(stream, flush, n=2048, steps=10, n_train=1 << 24, epochs=16
     q_mid = sol.state.get_q_global()
     p.close()
     res = {}
-    for mode in ("pvrs", "learned", "converged"):
+    # converged guesses with a fixed relative error of the size a guess of
+    # that precision carries (half an ulp of BF16, FP16, FP32), where the
+    # adaptive guess needs Newton steps (the adaptive guess elsewhere)
+    precision = {"bf16": 2.0 ** -9, "fp16": 2.0 ** -12, "fp32": 2.0 ** -25}
+    for mode in ("pvrs", "learned", "converged") + tuple(precision):
         ce = workloads.euler_quadrants_unsplit(n=n)
         ce.solver.rp = riemann.euler_exact_2D
         ce.solver.num_waves = 3
@@ -351,6 +355,8 @@ def learned_workload(stream, flush, n=2048, steps=10, n_train=1 << 24, epochs=16
             # the floor for any guess: every step starts from the converged p*
             # (pre-pass outside the kernel timing)
             learned.converged_guess(ce.solver)
+        elif mode in precision:
+            learned.converged_guess(ce.solver, rel_error=precision[mode])
         c1 = pe.step(dt)
         pe.accept(False)
         dte = dt * 0.9 / c1
@@ -379,11 +385,22 @@ def learned_workload(stream, flush, n=2048, steps=10, n_train=1 << 24, epochs=16
     out["max_rel_diff_one_step_converged"] = float(np.max(np.abs(qa - qc)) / np.max(np.abs(qa)))
     out["speedup"] = res["learned"]["value"] / res["pvrs"]["value"]
     out["speedup_ceiling"] = res["pvrs"]["kernel_ms"] / res["converged"]["kernel_ms"]
+    out["precision_ceilings"] = {}
+    for mode, rel in precision.items():
+        r = res[mode]
+        r.pop("_q")
+        out["precision_ceilings"][mode] = {
+            "rel_error": rel, "newton_per_interface": r["newton_per_interface"],
+            "kernel_ms": r["kernel_ms"], "speedup_ceiling": res["pvrs"]["kernel_ms"] / r["kernel_ms"]}
     out["note"] = ("kernel_ms of the learned guess includes its tensor-core guess pre-pass; that of the "
                    "converged-guess floor excludes its pre-pass (the step kernel alone with perfect "
                    "guesses): speedup_ceiling = PVRS step kernel / that, the most any guess can gain on "
                    "this workload.  newton_per_interface counts the steps needed (a final step below "
-                   "tolerance is applied but not counted), newton_applied_per_interface counts it too")
+                   "tolerance is applied but not counted), newton_applied_per_interface counts it too.  "
+                   "precision_ceilings: the same floor with the converged p* off by a fixed relative "
+                   "error of up to half an ulp of that format where the PVRS guess needs Newton steps "
+                   "(PVRS elsewhere), i.e. the most a guess of that precision can gain with PVRS as "
+                   "its fallback (tolerance 1e-12)")
     net.close()
     return out
 

@@ -387,6 +387,13 @@ int claw2_patch_newton_counts(claw2_patch* p, unsigned long long* out, int reset
  * guesses, the floor for any guess.  Mode 0 (default) turns it off; the
  * device time loop ignores it. */
 int claw2_patch_set_exact_guess(claw2_patch* p, int mode);
+/* With mode 1 and rel > 0 (0 <= rel < 0.5): where the adaptive guess needs
+ * Newton steps, start from the converged p* carrying a relative error of at
+ * most rel (p* (1 + rel u), u in [-1, 1) fixed per interface), elsewhere
+ * from the adaptive guess, so the step measures the most a guess of that
+ * precision can save with the adaptive guess as fallback; 0 (default) keeps
+ * the exact converged values everywhere. */
+int claw2_patch_set_exact_guess_error(claw2_patch* p, double rel);
 
 /* Description of the last error on this thread (never NULL). */
 const char* claw2_last_error(void);

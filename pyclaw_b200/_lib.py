@@ -148,6 +148,7 @@ _SIGNATURES = {
     "claw2_patch_counters": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_int]),
     "claw2_patch_newton_counts": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_int]),
     "claw2_patch_set_exact_guess": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "claw2_patch_set_exact_guess_error": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "claw2_last_error": (ctypes.c_char_p, []),
     "claw2_version": (ctypes.c_char_p, []),
 }

@@ -841,6 +841,7 @@ struct claw2_patch {
     double* guess = nullptr;                  // exact solver: learned guesses, x and y planes
     unsigned long long* counters = nullptr;   // exact solver: Newton steps needed, solves, steps applied
     int exact_guess = 0;                      // exact solver: 1 = start from the converged p* (measurement)
+    double exact_guess_err = 0.0;             // mode 1: relative error put on the converged p*
     int split_part = 0;                       // 1 after claw2_patch_step_part(.., 1): part 2 must follow
     claw2_mlp* mlp = nullptr;
     // claw2_patch_evolve's captured attempts, one graph per starting buffer
@@ -1391,7 +1392,8 @@ int patch_enqueue_step(claw2_patch* p, double dt, int part = 0) {
         // converged pressures as guesses, outside the timed region: the step
         // kernel's time with them is the floor for any guess
         dim3 grid((p->L.mx + 4 + 31) / 32, (p->L.my + 4 + 3) / 4);
-        k_exact_pstar_guess<<<grid, 128, 0, p->st>>>(qc, p->L, p->rp.c[0], p->rp.c[1], p->guess);
+        k_exact_pstar_guess<<<grid, 128, 0, p->st>>>(qc, p->L, p->rp.c[0], p->rp.c[1], p->exact_guess_err,
+                                                     p->guess);
         a.guess = p->guess;
         ++p->step_launches;
     }
@@ -2024,6 +2026,14 @@ int claw2_patch_set_exact_guess(claw2_patch* p, int mode) {
         return fail(CLAW2_EINVAL, "converged guesses apply to the exact Euler solver only");
     if (mode && !p->guess) return fail(CLAW2_EUNSUPPORTED, "this patch has no guess planes");
     p->exact_guess = mode;
+    ++p->graph_gen;
+    return CLAW2_OK;
+}
+
+int claw2_patch_set_exact_guess_error(claw2_patch* p, double rel) {
+    if (!p) return fail(CLAW2_EINVAL, "null patch");
+    if (!(rel >= 0.0 && rel < 0.5)) return fail(CLAW2_EINVAL, "relative error must be in [0, 0.5) (got %g)", rel);
+    p->exact_guess_err = rel;
     ++p->graph_gen;
     return CLAW2_OK;
 }

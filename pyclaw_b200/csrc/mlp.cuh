@@ -415,8 +415,24 @@ static __global__ void __launch_bounds__(128) k_mlp_guess(const MlpPacked* __res
 // guess, to the same tolerance, and writes p* into the guess planes.  A step
 // that starts from these needs no Newton update beyond the one that confirms
 // convergence, so its time bounds from below what any guess can achieve.
+// A deterministic number in [-1, 1) per interface (splitmix64 finaliser of
+// its index): the sign and size of the error put on a converged guess.
+__device__ __forceinline__ double guess_noise(unsigned long long k) {
+    k += 0x9e3779b97f4a7c15ull;
+    k = (k ^ (k >> 30)) * 0xbf58476d1ce4e5b9ull;
+    k = (k ^ (k >> 27)) * 0x94d049bb133111ebull;
+    k ^= k >> 31;
+    return (double)(k >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+}
+
+// rel > 0: where the adaptive guess needs Newton steps, the converged p* is
+// multiplied by 1 + rel * noise, noise in [-1, 1) -- a guess of that
+// relative precision -- and elsewhere the step keeps the adaptive guess
+// (guess 0): the most a guess of that precision can save with the adaptive
+// guess as its fallback, used only where it would help.
 static __global__ void __launch_bounds__(128) k_exact_pstar_guess(const double* __restrict__ q, Layout L,
-                                                                  double gamma, double tol, double* guess) {
+                                                                  double gamma, double tol, double rel,
+                                                                  double* guess) {
     const int cp = blockIdx.x * 32 + (threadIdx.x & 31);
     const int R = blockIdx.y * 4 + (threadIdx.x >> 5);
     if (cp > L.mx + 3 || R > L.my + 3) return;
@@ -444,10 +460,12 @@ static __global__ void __launch_bounds__(128) k_exact_pstar_guess(const double* 
     guess[L.plane + o] = 0.0;
     if (!exact_euler::vacuum(G, ul, cl, u0, c0)) {
         exact_euler::star(G, rl, ul, pl, cl, r0, u0, p0, c0, 0.0, tol, 50, ps, us, it);
+        if (rel > 0.0) ps = it > 0 ? ps * (1.0 + rel * guess_noise(2ull * (unsigned long long)o)) : 0.0;
         guess[o] = ps;
     }
     if (!exact_euler::vacuum(G, vb, cb, v0, c0)) {
         exact_euler::star(G, rb, vb, pb, cb, r0, v0, p0, c0, 0.0, tol, 50, ps, us, it);
+        if (rel > 0.0) ps = it > 0 ? ps * (1.0 + rel * guess_noise(2ull * (unsigned long long)o + 1ull)) : 0.0;
         guess[L.plane + o] = ps;
     }
 }

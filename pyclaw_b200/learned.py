@@ -120,9 +120,14 @@ def newton_counts(solver, reset=True):
     return int(out[0]), int(out[1]), int(out[2])
 
 
-def converged_guess(solver, on=True):
+def converged_guess(solver, on=True, rel_error=0.0):
     """Measurement aid: every step of the exact solver starts Newton from the
     converged pressures (a pre-pass outside the kernel timing), so the step
-    kernel's time is the floor for any guess, learned or not."""
+    kernel's time is the floor for any guess, learned or not.  With
+    rel_error > 0 the interfaces where the adaptive guess needs Newton steps
+    start from the converged pressure off by a fixed relative error of at
+    most that size, the others from the adaptive guess: the step time of a
+    guess of that precision with the adaptive guess as fallback."""
     dev = solver._dev
+    _lib.check(dev._lib.claw2_patch_set_exact_guess_error(dev.h, float(rel_error)))
     _lib.check(dev._lib.claw2_patch_set_exact_guess(dev.h, 1 if on else 0))

@@ -209,3 +209,41 @@ def test_converged_guess_gives_the_same_step(oracle):
     (c0, q0, c1, q1) = outs
     assert c0[0] > 0 and c1[0] == 0 and c1[2] == c0[2]
     assert max_rel(q1, q0) <= PARITY_RTOL
+
+
+def test_converged_guess_with_error_bounds_a_guess_of_that_precision(oracle):
+    # the measurement aid with a relative error on the converged p* where
+    # the adaptive guess needs Newton steps: a coarser guess never needs fewer
+    # steps than a finer one, none needs more than the adaptive guess alone
+    # where that needs none, none changes the step beyond the parity bar, and
+    # an error of half an FP32 ulp already needs steps where the exact
+    # converged value needs none
+    claw = _exact_claw(130)
+    st = claw.solution.state
+    qbc = _euler_qbc(130, 130, seed=11)
+    q_init = np.asfortranarray(qbc[:, 2:-2, 2:-2])
+    st.q = q_init.copy(order="F")
+    s = claw.solver
+    s.setup(claw.solution)
+    counts, qs = [], []
+    for rel in (None, 2.0 ** -9, 2.0 ** -12, 2.0 ** -25, 0.0):
+        if rel is None:
+            learned.converged_guess(s, False)
+        else:
+            learned.converged_guess(s, True, rel_error=rel)
+        learned.newton_counts(s)
+        s._dev.step(2e-4, want_cfl=False)
+        s._dev.accept(True)
+        counts.append(learned.newton_counts(s))
+        qs.append(st.get_q_global())
+        st.q = q_init.copy(order="F")
+        s._dev.push(st)
+    learned.converged_guess(s, False)
+    needed = [c[0] for c in counts]
+    assert all(c[2] == counts[0][2] for c in counts)
+    assert needed[1] >= needed[2] >= needed[3] >= needed[4] == 0, needed
+    assert needed[3] > 0
+    for q in qs[1:]:
+        assert max_rel(q, qs[0]) <= PARITY_RTOL
+    with pytest.raises(_lib.Claw2Error):
+        learned.converged_guess(s, True, rel_error=0.5)
