@@ -5,7 +5,9 @@
   each launch shape the autotuner can pick for it -- 576 tiles at 16 rows,
   more than the CTA slots, so the longest-first tile schedule and its sort
   run -- each step compared with the oracle's step2 on the same state and dt
-  (interior cells and the Courant number within 1e-12 relative);
+  (interior cells and the Courant number within 1e-12 relative); and the
+  whole run from t = 0 to 0.8 on the device time loop against the oracle's
+  host loop (same steps, final state within 1e-8);
 * the exact Euler solver at 2048^2 on the same problem's t = 0.4 state, one
   step with the PVRS guess and one with a learned guess, against the oracle;
 * the batched form at its benchmark size (512 problems, 100 steps): the
@@ -212,3 +214,31 @@ def test_batched_512_instances_match_oracle_runs(oracle):
     finally:
         oracle.set_threads(1)
         bat.close()
+
+
+def test_headline_euler_1024_whole_run_matches_oracle(oracle):
+    # the benchmark problem's whole run, t = 0 to 0.8 (about 1.7k steps,
+    # cfl_desired 0.9), on the device time loop against the oracle's host
+    # loop over the same dt rule: the same accepted and rejected steps, the
+    # same dt to the last steps, and the final state within 1e-8 relative
+    # (each step's roundoff-level differences feed the next steps' dt and
+    # data through the limiters; measured 3.9e-9 after 1.7k steps)
+    claw_g = workloads.euler_quadrants_unsplit(n=1024)
+    claw_o = workloads.euler_quadrants_unsplit(oracle.make_solver_class(), n=1024)
+    for c in (claw_g, claw_o):
+        c.num_output_times = 1
+        c.output_format = None
+    _all_cores(oracle)
+    try:
+        claw_o.run()
+    finally:
+        oracle.set_threads(1)
+    claw_g.run()
+    sg, so = claw_g.solver.status, claw_o.solver.status
+    assert sg['numsteps'] == so['numsteps'] and sg['numsteps'] > 1000
+    assert abs(sg['dtmin'] - so['dtmin']) <= 1e-9 * so['dtmin']
+    assert abs(sg['cflmax'] - so['cflmax']) <= 1e-9 * so['cflmax']
+    qg = claw_g.frames[-1].state.get_q_global()
+    qo = claw_o.frames[-1].state.get_q_global()
+    assert np.isfinite(qg).all()
+    assert max_rel(qg, qo) <= 1e-8
