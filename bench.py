@@ -308,10 +308,12 @@ def batched_workload(n_instances=512, steps=100, plain=True):
     return out
 
 
-def learned_workload(stream, flush, n=2048, steps=10, n_train=1 << 24, epochs=16, pre_t=0.4):
+def learned_workload(stream, flush, n=2048, steps=10, n_train=1 << 24, epochs=16, pre_t=0.4, shape=None):
     """Exact Euler solver on the quadrant problem (n^2, unsplit trans_cor, MC),
     Newton started from the adaptive PVRS guess vs from the learned guess of a
-    network trained here on n_train seeded problems by the library's kernels."""
+    network trained here on n_train seeded problems by the library's kernels.
+    shape: a fixed launch shape (variant, rows) instead of the autotuner's."""
+    fixed_shape = tuple(shape) if shape is not None else None
     import numpy as np
     import torch
     from pyclaw_b200 import learned, riemann, workloads
@@ -363,7 +365,11 @@ def learned_workload(stream, flush, n=2048, steps=10, n_train=1 << 24, epochs=16
         # launch shape tuned once on the PVRS run (cached per solver and size,
         # so the learned run uses the same one)
         from pyclaw_b200 import tune
-        shape, _ = tune.autotune(pe, dte)
+        if fixed_shape is not None:
+            tune.set_shape(pe.desc.riemann, *fixed_shape)
+            shape = fixed_shape
+        else:
+            shape, _ = tune.autotune(pe, dte)
         learned.newton_counts(ce.solver)
         step_ms, kern_ms = time_patch(pe, dte, steps, flush, stream)
         it, applied, ns = learned.newton_counts(ce.solver)
@@ -475,7 +481,7 @@ def run_one(args):
     else:
         out = {"learned_exact_euler_%d" % args.learned_n: learned_workload(
             stream, flush, n=args.learned_n, n_train=args.train_problems, epochs=args.epochs,
-            pre_t=args.learned_pre_t)}
+            pre_t=args.learned_pre_t, shape=shape)}
     torch.cuda.synchronize()
     print(json.dumps(out), flush=True)
     return 0
