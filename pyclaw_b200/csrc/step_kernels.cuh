@@ -1727,6 +1727,9 @@ __global__ void __launch_bounds__(NT) k_split_x(const StepArgs a) {
     const double* qo = a.qold + cpl;
     double* qn = a.qnew + cpl;
     double cfl = 0.0;
+    // zero-jump shortcut (q-wave solvers without aux data), as in unsplit_tile
+    constexpr bool ZS = SkipTraits<RP>::OK && AuxTraits<RP>::MAUX == 0;
+    const bool zs = ZS && (SPEC != SPEC_ANY || a.meth.fwave == 0);
 
     for (int R = rb; R < re; ++R) {
         const int buf = R & 1;
@@ -1745,6 +1748,7 @@ __global__ void __launch_bounds__(NT) k_split_x(const StepArgs a) {
         __syncthreads();
         Iface fX;
         double amX[ME], apX[ME];
+        bool zX = false;  // every lane of the warp has equal cells on both sides
         {
             double cL[NC], cR[NC];
 #pragma unroll
@@ -1752,20 +1756,31 @@ __global__ void __launch_bounds__(NT) k_split_x(const StepArgs a) {
                 cL[k] = S.cell[buf][k][tl];
                 cR[k] = S.cell[buf][k][t];
             }
-            RP::template solve<1>(cL, cR, P, fX, amX, apX);
-            double wX[MW][ME];
-            RP::template waves<1>(fX, P, wX);
+            zX = ZS && zs && __all_sync(0xffffffffu, same_q<ME, NC>(cL, cR));
+            if (ZS && zX) {
+                SkipTraits<RP>::template zero_iface<1>(cL, cR, P, fX);
 #pragma unroll
-            for (int k = 0; k < MW; ++k)
+                for (int m = 0; m < ME; ++m) amX[m] = apX[m] = 0.0;
 #pragma unroll
-                for (int m = 0; m < ME; ++m) S.w[k][m][t] = wX[k][m];
+                for (int k = 0; k < MW; ++k)
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) S.w[k][m][t] = 0.0;
+            } else {
+                RP::template solve<1>(cL, cR, P, fX, amX, apX);
+                double wX[MW][ME];
+                RP::template waves<1>(fX, P, wX);
+#pragma unroll
+                for (int k = 0; k < MW; ++k)
+#pragma unroll
+                    for (int m = 0; m < ME; ++m) S.w[k][m][t] = wX[k][m];
+            }
         }
         __syncthreads();
         // dt/(dx kappa) left and right of the interface (both dtdx without capacity)
         const double xdl = dtdx * S.icap[buf][tl], xdr = dtdx * S.icap[buf][t];
         if (xcfl_col) cfl = fmax(cfl, iface_cfl2<RP, 1>(fX, P, xdl, xdr));
         double cq[ME];
-        if ((SPEC != SPEC_ANY) || a.meth.order != 1) {
+        if (!(ZS && zX) && ((SPEC != SPEC_ANY) || a.meth.order != 1)) {
             double dl[MW], dr[MW];
 #pragma unroll
             for (int k = 0; k < MW; ++k) {
@@ -1831,6 +1846,10 @@ __global__ void __launch_bounds__(NT) k_split_y(const StepArgs a) {
     const double* qo = a.qold + cpl;
     double* qn = a.qnew + cpl;
 
+    // zero-jump shortcut (q-wave solvers without aux data), as in unsplit_tile
+    constexpr bool ZS = SkipTraits<RP>::OK && AuxTraits<RP>::MAUX == 0;
+    const bool zs = ZS && (SPEC != SPEC_ANY || a.meth.fwave == 0);
+    bool zY = false;  // the interface (R-2 | R-1) being finished is zero in the whole warp
     double q0[ME], q1[ME], cB[NC], acc0[ME], acc1[ME];
     Iface fY;
     double amY[ME], apY[ME], dY[MW];
@@ -1865,9 +1884,16 @@ __global__ void __launch_bounds__(NT) k_split_y(const StepArgs a) {
         const double ic2 = ko ? 1.0 / __ldg(ko + (long long)R * pitch) : 1.0;
         Iface fN;
         double amN[ME], apN[ME];
-        RP::template solve<2>(cB, cA, P, fN, amN, apN);
         double dn[MW];
-        {
+        const bool zN = ZS && zs && __all_sync(0xffffffffu, same_q<ME, NC>(cB, cA));
+        if (ZS && zN) {
+            SkipTraits<RP>::template zero_iface<2>(cB, cA, P, fN);
+#pragma unroll
+            for (int m = 0; m < ME; ++m) amN[m] = apN[m] = 0.0;
+#pragma unroll
+            for (int k = 0; k < MW; ++k) dn[k] = 0.0;
+        } else {
+            RP::template solve<2>(cB, cA, P, fN, amN, apN);
             double wY[MW][ME], wN[MW][ME];
             RP::template waves<2>(fY, P, wY);
             RP::template waves<2>(fN, P, wN);
@@ -1883,6 +1909,9 @@ __global__ void __launch_bounds__(NT) k_split_y(const StepArgs a) {
         if (R >= R0 + 3) {
             const double ydl = dtdy * ic0, ydr = dtdy * ic1;
             if (valid) cfl = fmax(cfl, iface_cfl2<RP, 2>(fY, P, ydl, ydr));
+        }
+        if (R >= R0 + 3 && !(ZS && zY)) {
+            const double ydl = dtdy * ic0, ydr = dtdy * ic1;
             double cq[ME];
             if ((SPEC != SPEC_ANY) || a.meth.order != 1) {
                 correction<RP, 2, SPEC>(fY, P, a.meth, 0.5 * (ydl + ydr), dY, dn, cq);
@@ -1921,6 +1950,7 @@ __global__ void __launch_bounds__(NT) k_split_y(const StepArgs a) {
 #pragma unroll
         for (int k = 0; k < MW; ++k) dY[k] = dn[k];
         fY = fN;
+        zY = zN;
     }
     cfl_commit(cfl, sRed, a.cfl_bits);
 }

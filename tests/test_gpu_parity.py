@@ -90,6 +90,31 @@ def test_step2ds_sweeps(oracle, rp, ids, mx, my):
         assert max_rel(q_g[:, 2:-2, 2:-2], q_o[:, 2:-2, 2:-2]) <= PARITY_RTOL
 
 
+@pytest.mark.parametrize("rp", sorted(RP_INFO))
+@pytest.mark.parametrize("ids", [1, 2])
+@pytest.mark.parametrize("order,mthlim_kind", [(2, "mc"), (2, "mixed"), (1, "mc")])
+def test_step2ds_sweeps_zero_jump_shortcut(oracle, rp, ids, order, mthlim_kind):
+    # data with long constant runs (1% noisy cells): whole warps of a sweep
+    # have equal cells on both sides and take the zero-jump shortcut; the
+    # generic and the method-specialised sweep kernels both
+    name, meqn, mwaves, cp = RP_INFO[rp]
+    mx, my = 300, 150
+    qbc = random_qbc(rp, mx, my, seed=7 * rp + ids + order, smooth_frac=0.01)
+    method = method_vector(order, 0, split=True)
+    mthlim = np.full(mwaves, 4, dtype=np.intc) if mthlim_kind == "mc" else \
+        np.array([4, 1, 2, 3, 5][:mwaves], dtype=np.intc)
+    dx, dy = 1.0 / mx, 1.0 / my
+    dt = _dt_for(oracle, qbc, rp, cp, method, mthlim, dx, dy, split=True)
+    q_o = qbc.copy(order="F")
+    cfl_o = oracle.step2ds(qbc, q_o, dx, dy, dt, method, mthlim, ids, rp, cp)
+    set_cparam(classic2, rp)
+    q_g, cfl_g = classic2.step2ds(max(mx, my), 2, mx, my, qbc, qbc.copy(order="F"), None, dx, dy, dt, method,
+                                  mthlim, ids=ids, rpn2=rp)
+    assert abs(cfl_g - cfl_o) <= PARITY_RTOL * cfl_o
+    rows = slice(None) if ids == 1 else slice(2, -2)
+    assert max_rel(q_g[:, 2:-2, rows], q_o[:, 2:-2, rows]) <= PARITY_RTOL
+
+
 @pytest.mark.parametrize("bcl,bcu", [((1, 1), (1, 1)), ((2, 2), (2, 2)), ((3, 3), (3, 3)), ((1, 3), (3, 1)),
                                      ((2, 1), (2, 3)), ((3, 2), (1, 2))])
 @pytest.mark.parametrize("mx,my", [(2, 2), (2, 3), (17, 29)])
