@@ -345,14 +345,17 @@ def learned_workload(stream, flush, n=2048, steps=10, n_train=1 << 24, epochs=16
     # that precision carries (half an ulp of BF16, FP16, FP32), where the
     # adaptive guess needs Newton steps (the adaptive guess elsewhere)
     precision = {"bf16": 2.0 ** -9, "fp16": 2.0 ** -12, "fp32": 2.0 ** -25}
-    for mode in ("pvrs", "learned", "converged") + tuple(precision):
+    for mode in ("pvrs", "learned", "learned_mma_sync", "converged") + tuple(precision):
         ce = workloads.euler_quadrants_unsplit(n=n)
         ce.solver.rp = riemann.euler_exact_2D
         ce.solver.num_waves = 3
         ce.solution.state.q = q_mid
         ce.solver.setup(ce.solution)
         pe = ce.solver._dev
-        learned.attach(ce.solver, net if mode == "learned" else None)
+        # the network's tensor-core path: tcgen05 (the default) or, for the
+        # comparison, the warp-level mma.sync form
+        net.set_engine("mma.sync" if mode == "learned_mma_sync" else "tcgen05")
+        learned.attach(ce.solver, net if mode.startswith("learned") else None)
         if mode == "converged":
             # the floor for any guess: every step starts from the converged p*
             # (pre-pass outside the kernel timing)
@@ -385,9 +388,12 @@ def learned_workload(stream, flush, n=2048, steps=10, n_train=1 << 24, epochs=16
         res[mode]["_q"] = ce.solution.state.get_q_global()
         pe.close()
     qa, qb, qc = res["pvrs"].pop("_q"), res["learned"].pop("_q"), res["converged"].pop("_q")
+    qm = res["learned_mma_sync"].pop("_q")
     out["pvrs_guess"], out["learned_guess"] = res["pvrs"], res["learned"]
+    out["learned_guess_mma_sync"] = res["learned_mma_sync"]
     out["converged_guess_floor"] = res["converged"]
     out["max_rel_diff_one_step"] = float(np.max(np.abs(qa - qb)) / np.max(np.abs(qa)))
+    out["max_rel_diff_one_step_mma_sync"] = float(np.max(np.abs(qa - qm)) / np.max(np.abs(qa)))
     out["max_rel_diff_one_step_converged"] = float(np.max(np.abs(qa - qc)) / np.max(np.abs(qa)))
     out["speedup"] = res["learned"]["value"] / res["pvrs"]["value"]
     out["speedup_ceiling"] = res["pvrs"]["kernel_ms"] / res["converged"]["kernel_ms"]

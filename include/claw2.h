@@ -286,8 +286,14 @@ int claw2_probe_fp64(int device, double* tflops);
  * (no counterpart in the reference; Newton-Raphson refinement of the hardware
  * approximation): over n seeded values a = +-(1+u)*2^e, e uniform in
  * [-1000, 1000], *max_ulp = the largest distance in units in the last place
- * between it and CUDA's IEEE quotient 1.0/a. */
+ * between it and CUDA's IEEE quotient 1.0/a.  Special values (+-0, +-inf,
+ * NaN, a subnormal, 1e308) that do not give the documented results make
+ * *max_ulp huge. */
 int claw2_selftest_rcp(int device, int n, unsigned long long seed, double* max_ulp);
+/* The same for the square root the solvers use per cell and per interface
+ * (no counterpart in the reference; Goldschmidt iteration from the hardware's
+ * reciprocal square root): x = (1+u)*2^e, against CUDA's IEEE sqrt(x). */
+int claw2_selftest_sqrt(int device, int n, unsigned long long seed, double* max_ulp);
 
 /* Self-test (no counterpart in the reference) of the longest-first tile
  * schedule's sort: n (1..8192) seeded tile costs with many ties, sorted on the
@@ -371,6 +377,12 @@ int claw2_mlp_gradient(claw2_mlp* m, long long first, int count, float* grad, fl
 int claw2_mlp_train(claw2_mlp* m, int epochs, int batch, float lr, float* last_loss);
 /* Network outputs for n rows of 8 floats (BF16 tensor cores, FP32 accumulation). */
 int claw2_mlp_infer(claw2_mlp* m, const float* x8, int n, float* y);
+/* The tensor-core path of claw2_mlp_infer and of the exact solver's guess
+ * pass: tcgen05.mma with TMEM accumulators (the default), or the warp-level
+ * mma.sync form kept for comparison.  Both round operands to BF16 and
+ * accumulate in FP32. */
+enum { CLAW2_MLP_TCGEN05 = 0, CLAW2_MLP_MMA_SYNC = 1 };
+int claw2_mlp_set_engine(claw2_mlp* m, int engine);
 /* Exact-solver patches: start Newton from the network's guesses (NULL: the
  * adaptive PVRS guess); Newton updates and Riemann solves since the last reset. */
 int claw2_patch_set_mlp(claw2_patch* p, claw2_mlp* m);

@@ -112,6 +112,7 @@ _SIGNATURES = {
     "claw2_patch_kernel_ms": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]),
     "claw2_probe_fp64": (ctypes.c_int, [ctypes.c_int, _c_double_p]),
     "claw2_selftest_rcp": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_ulonglong, _c_double_p]),
+    "claw2_selftest_sqrt": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_ulonglong, _c_double_p]),
     "claw2_patch_launch_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]),
     "claw2_selftest_lpt": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_ulonglong,
                                           ctypes.POINTER(ctypes.c_int)]),
@@ -144,6 +145,7 @@ _SIGNATURES = {
                                        ctypes.POINTER(ctypes.c_float)]),
     "claw2_mlp_infer": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float), ctypes.c_int,
                                        ctypes.POINTER(ctypes.c_float)]),
+    "claw2_mlp_set_engine": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "claw2_patch_set_mlp": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "claw2_patch_counters": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_int]),
     "claw2_patch_newton_counts": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_int]),

@@ -621,7 +621,12 @@ struct claw2_mlp {
     float* M1 = nullptr;     // Adam moments
     float* M2 = nullptr;
     float* loss = nullptr;
-    MlpPacked* packed = nullptr;
+    MlpPacked* packed = nullptr;   // mma.sync fragments
+    MlpTcImage* tc = nullptr;      // tcgen05 operand image
+    int engine = CLAW2_MLP_TCGEN05;
+    int* status = nullptr;         // bit 1: an MMA completion wait gave up (claw2_mlp_infer)
+    int nsm = 148;
+    int guess_per_sm = 0, eval_per_sm = 0;  // resident CTAs of the tcgen05 kernels (0: not yet queried)
     int adam_step = 0;
     float* x = nullptr;      // samples: 8 floats each
     float* y = nullptr;
@@ -638,10 +643,46 @@ int mlp_repack(claw2_mlp* m) {
     MlpPacked pk;
     mlp_pack(h.data(), pk);
     CUDA_TRY(cudaMemcpy(m->packed, &pk, sizeof pk, cudaMemcpyHostToDevice));
+    MlpTcImage ti;
+    mlp_pack_tc(h.data(), ti);
+    CUDA_TRY(cudaMemcpy(m->tc, &ti, sizeof ti, cudaMemcpyHostToDevice));
     return CLAW2_OK;
 }
 
-void mlp_guess_launch(claw2_mlp* m, const double* q, const Layout& L, double gamma, double* guess, cudaStream_t st) {
+// CTAs of a tcgen05 kernel: the resident ones only (each allocates TMEM once
+// and loops over its tiles).  Residency per SM (cached in *per_sm) from the
+// kernel's registers and static shared memory against the SM's register
+// file, shared memory (with the per-CTA reservation) and thread slots, for
+// 128-thread CTAs.
+template <class K>
+int mlp_tc_grid(const claw2_mlp* m, K kernel, int* per_sm, long long tiles) {
+    if (*per_sm <= 0) {
+        int b = 1;
+        cudaFuncAttributes fa;
+        cudaDeviceProp pr;
+        if (cudaFuncGetAttributes(&fa, kernel) == cudaSuccess && cudaGetDeviceProperties(&pr, m->device) == cudaSuccess) {
+            const int regs = std::max(8, (fa.numRegs + 7) / 8 * 8);
+            const int by_regs = pr.regsPerMultiprocessor / (regs * 128);
+            const int by_smem = (int)(pr.sharedMemPerMultiprocessor /
+                                      (fa.sharedSizeBytes + std::max<size_t>(pr.reservedSharedMemPerBlock, 1)));
+            const int by_threads = pr.maxThreadsPerMultiProcessor / 128;
+            b = std::max(1, std::min(std::min(by_regs, by_smem), std::min(by_threads, 32)));
+        } else {
+            cudaGetLastError();
+        }
+        *per_sm = b;
+    }
+    return (int)std::max(1ll, std::min(tiles, (long long)m->nsm * *per_sm));
+}
+
+void mlp_guess_launch(claw2_mlp* m, const double* q, const Layout& L, double gamma, double* guess, int* status,
+                      cudaStream_t st) {
+    if (m->engine == CLAW2_MLP_TCGEN05) {
+        const long long tiles = (long long)((L.mx + 4 + 31) / 32) * ((L.my + 4 + 3) / 4);
+        const int grid = mlp_tc_grid(m, k_mlp_guess_tc, &m->guess_per_sm, tiles);
+        k_mlp_guess_tc<<<grid, 128, 0, st>>>(m->tc, q, L, gamma, guess, status);
+        return;
+    }
     dim3 grid((L.mx + 4 + 31) / 32, (L.my + 4 + 3) / 4);
     k_mlp_guess<<<grid, 128, 0, st>>>(m->packed, q, L, gamma, guess);
 }
@@ -659,12 +700,22 @@ int claw2_mlp_create(int device, unsigned long long seed, claw2_mlp** out) {
     bool ok = cudaMalloc(&m->P, MLP_NPARAM * 4) == cudaSuccess && cudaMalloc(&m->G, MLP_NPARAM * 4) == cudaSuccess &&
               cudaMalloc(&m->M1, MLP_NPARAM * 4) == cudaSuccess && cudaMalloc(&m->M2, MLP_NPARAM * 4) == cudaSuccess &&
               cudaMalloc(&m->loss, 4) == cudaSuccess && cudaMalloc(&m->packed, sizeof(MlpPacked)) == cudaSuccess &&
+              cudaMalloc(&m->tc, sizeof(MlpTcImage)) == cudaSuccess && cudaMalloc(&m->status, 4) == cudaSuccess &&
               cudaStreamCreateWithFlags(&m->st, cudaStreamNonBlocking) == cudaSuccess;
     if (!ok) {
         cudaGetLastError();
         claw2_mlp_destroy(m);
         return fail(CLAW2_ENOMEM, "device allocation for the network failed");
     }
+    if (cudaDeviceGetAttribute(&m->nsm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || m->nsm <= 0)
+        m->nsm = 148;
+    // the tcgen05 kernels' residency, found here (not inside a stream capture),
+    // with the whole shared-memory carveout asked for so it is reached
+    cudaFuncSetAttribute(k_mlp_guess_tc, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaFuncSetAttribute(k_mlp_eval_tc, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaGetLastError();
+    mlp_tc_grid(m, k_mlp_guess_tc, &m->guess_per_sm, 1);
+    mlp_tc_grid(m, k_mlp_eval_tc, &m->eval_per_sm, 1);
     // Glorot-uniform weights from the counter RNG, zero biases
     std::vector<float> h(MLP_NPARAM, 0.f);
     auto fill = [&](int off, int fan_out, int fan_in) {
@@ -693,7 +744,7 @@ int claw2_mlp_destroy(claw2_mlp* m) {
         DeviceGuard g(m->device);
         if (m->st) cudaStreamSynchronize(m->st);
         cudaFree(m->P); cudaFree(m->G); cudaFree(m->M1); cudaFree(m->M2); cudaFree(m->loss);
-        cudaFree(m->packed); cudaFree(m->x); cudaFree(m->y); cudaFree(m->ok);
+        cudaFree(m->packed); cudaFree(m->tc); cudaFree(m->status); cudaFree(m->x); cudaFree(m->y); cudaFree(m->ok);
         if (m->st) cudaStreamDestroy(m->st);
     }
     delete m;
@@ -804,12 +855,27 @@ int claw2_mlp_infer(claw2_mlp* m, const float* x8, int n, float* y) {
         return fail(CLAW2_ENOMEM, "device allocation failed");
     }
     cudaMemcpy(dx, x8, (size_t)n * 32, cudaMemcpyHostToDevice);
-    k_mlp_eval<<<(n + 255) / 256, 128, 0, m->st>>>(m->packed, dx, n, dy);
+    cudaMemsetAsync(m->status, 0, 4, m->st);
+    if (m->engine == CLAW2_MLP_TCGEN05)
+        k_mlp_eval_tc<<<mlp_tc_grid(m, k_mlp_eval_tc, &m->eval_per_sm, (n + 255) / 256), 128, 0, m->st>>>(
+            m->tc, dx, n, dy, m->status);
+    else
+        k_mlp_eval<<<(n + 255) / 256, 128, 0, m->st>>>(m->packed, dx, n, dy);
     cudaError_t e = cudaStreamSynchronize(m->st);
+    int st = 0;
     if (e == cudaSuccess) e = cudaMemcpy(y, dy, (size_t)n * 4, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(&st, m->status, 4, cudaMemcpyDeviceToHost);
     cudaFree(dx);
     cudaFree(dy);
     if (e != cudaSuccess) return fail(CLAW2_ECUDA, "inference failed: %s", cudaGetErrorString(e));
+    if (st & 2) return fail(CLAW2_ETIMEOUT, "a tensor-core completion wait gave up");
+    return CLAW2_OK;
+}
+
+int claw2_mlp_set_engine(claw2_mlp* m, int engine) {
+    if (!m || (engine != CLAW2_MLP_TCGEN05 && engine != CLAW2_MLP_MMA_SYNC))
+        return fail(CLAW2_EINVAL, "engine must be CLAW2_MLP_TCGEN05 or CLAW2_MLP_MMA_SYNC");
+    m->engine = engine;
     return CLAW2_OK;
 }
 
@@ -1399,7 +1465,7 @@ int patch_enqueue_step(claw2_patch* p, double dt, int part = 0) {
     }
     if (p->timing) CUDA_TRY(cudaEventRecord(p->ev0, p->st));
     if (exact_unsplit && p->mlp && p->exact_guess == 0) {
-        mlp_guess_launch(p->mlp, qc, p->L, p->rp.c[0], p->guess, p->st);
+        mlp_guess_launch(p->mlp, qc, p->L, p->rp.c[0], p->guess, p->status, p->st);
         a.guess = p->guess;
         ++p->step_launches;
     }
@@ -1515,7 +1581,7 @@ int evolve_enqueue_attempt(claw2_patch* p, int c) {
     a.qnew = p->q[c ^ 1];
     a.evo = p->evo;
     if (p->d.riemann == CLAW2_RP_EULER_EXACT && p->mlp && !p->d.dimensional_split) {
-        mlp_guess_launch(p->mlp, qc, p->L, p->rp.c[0], p->guess, p->st);
+        mlp_guess_launch(p->mlp, qc, p->L, p->rp.c[0], p->guess, p->status, p->st);
         a.guess = p->guess;
     }
     int lpt_n = 0;
@@ -1919,6 +1985,22 @@ int claw2_selftest_rcp(int device, int n, unsigned long long seed, double* max_u
     cudaError_t e = cudaMemcpy(&h, worst, sizeof(h), cudaMemcpyDeviceToHost);
     cudaFree(worst);
     if (e != cudaSuccess) return fail(CLAW2_ECUDA, "reciprocal self-test failed: %s", cudaGetErrorString(e));
+    *max_ulp = (double)h;
+    return CLAW2_OK;
+}
+
+int claw2_selftest_sqrt(int device, int n, unsigned long long seed, double* max_ulp) {
+    if (!max_ulp) return fail(CLAW2_EINVAL, "null pointer argument");
+    if (n < 1) return fail(CLAW2_EINVAL, "n must be positive (got %d)", n);
+    DeviceGuard g(device);
+    unsigned long long* worst = nullptr;
+    CUDA_TRY(cudaMalloc(&worst, sizeof(unsigned long long)));
+    cudaMemset(worst, 0, sizeof(unsigned long long));
+    k_selftest_sqrt<<<(n + 255) / 256, 256>>>(n, seed, worst);
+    unsigned long long h = 0;
+    cudaError_t e = cudaMemcpy(&h, worst, sizeof(h), cudaMemcpyDeviceToHost);
+    cudaFree(worst);
+    if (e != cudaSuccess) return fail(CLAW2_ECUDA, "square-root self-test failed: %s", cudaGetErrorString(e));
     *max_ulp = (double)h;
     return CLAW2_OK;
 }

@@ -11,12 +11,15 @@
 // forward and backward for a minibatch (one sample per thread, gradients
 // reduced per warp with shuffles, then atomically added); k_adam applies Adam.
 //
-// Inference: k_mlp_guess, one thread per grid site, solves the MLP for the
-// x- and y-interface of the site (interfaces with a weak jump keep the PVRS
-// guess) in BF16 on the tensor cores with FP32 accumulation (mma.sync m16n8k16 per warp: 64 interfaces = 4 row tiles; a
-// layer's accumulator fragments are exactly the next layer's A fragments, so
-// activations never leave registers) and writes the guesses that the step
-// kernel's Newton iteration starts from.
+// Inference: k_mlp_guess_tc, one thread per grid site, evaluates the MLP for
+// the x- and y-interface of the site (interfaces with a weak jump keep the
+// PVRS guess) in BF16 on the tensor cores with FP32 accumulation --
+// tcgen05.mma from shared-memory operands into TMEM accumulators, 128
+// interfaces per MMA tile -- and writes the guesses that the step kernel's
+// Newton iteration starts from.  k_mlp_guess is the same pass on the
+// warp-level mma.sync.m16n8k16 (64 interfaces = 4 row tiles per warp; a
+// layer's accumulator fragments are exactly the next layer's A fragments),
+// kept as the comparison path (claw2_mlp_set_engine).
 #pragma once
 
 #include <cuda_bf16.h>
@@ -407,6 +410,378 @@ static __global__ void __launch_bounds__(128) k_mlp_guess(const MlpPacked* __res
     const long long o = (long long)R * L.pitch + cp;
     guess[o] = gx0 * exp(wx * (double)res[w][lane]);
     guess[L.plane + o] = gy0 * exp(wy * (double)res[w][32 + lane]);
+}
+
+// ---- BF16 inference on the 5th-generation tensor cores (tcgen05 + TMEM) -----
+// One CTA of 128 threads evaluates the network for two M = 128 row tiles at a
+// time (the x- and the y-interfaces of 128 grid sites, or 256 rows of
+// features): thread t owns row t of both tiles, which is TMEM lane t of the
+// accumulators, so warp w reads back exactly the lanes 32w..32w+31 it may
+// access.  Per tile pair: layer 1 is one tcgen05.mma (M 128, N 32, K 16) per
+// tile, the 32 FP32 accumulators of a row come back with one tcgen05.ld,
+// tanh and the BF16 rounding run in registers and the row goes back to
+// shared memory as layer 2's A operand; layer 2 is two K = 16 MMAs per tile
+// into the same TMEM columns; layer 3 (32 -> 1) is a 32-term FP32 dot product
+// of the BF16-rounded activations in each thread.  Operands are BF16 in the
+// no-swizzle K-major layout of the tcgen05 shared-memory descriptors: element
+// (r, k) of an R x K matrix at byte (r/8)*16K + (k/8)*128 + (r%8)*16 + (k%8)*2
+// (8 x 16-byte core matrices; the leading, K, offset 128 bytes; the stride
+// between 8-row groups 16K bytes).  One elected thread issues the MMAs and
+// commits them to an mbarrier; every wait on it is bounded (status bit 1).
+struct MlpTcImage {                  // device image of the weights, copied into shared memory
+    unsigned short w1[MLP_H * 16];   // layer 1 B operand: N = 32 x K = 16 (6 inputs + zeros)
+    unsigned short w2[MLP_H * MLP_H];  // layer 2 B operand: N = 32 x K = 32
+    float b1[MLP_H], b2[MLP_H];
+    float w3[MLP_H];                 // BF16-rounded, as FP32
+    float b3;
+    float pad[3];
+};
+static_assert(sizeof(MlpTcImage) % 16 == 0, "weight image is copied in 16-byte words");
+
+// byte offset of element (r, k) in the no-swizzle K-major image of an R x K matrix
+__host__ __device__ constexpr int umma_kmajor_off(int r, int k, int K) {
+    return (r >> 3) * (K * 16) + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2;
+}
+
+inline float bf16_round(float f) {
+    const unsigned int u = (unsigned int)bf16_bits(f) << 16;
+    float r;
+    memcpy(&r, &u, 4);
+    return r;
+}
+
+// Fill the weight image (host) from the FP32 parameters: B[n][k] = W[n][k]
+// (the MMA computes D = A B^T with both operands K-major).
+inline void mlp_pack_tc(const float* P, MlpTcImage& M) {
+    memset(&M, 0, sizeof M);
+    for (int n = 0; n < MLP_H; ++n) {
+        for (int k = 0; k < 16; ++k)
+            M.w1[umma_kmajor_off(n, k, 16) / 2] = bf16_bits(k < MLP_IN ? P[OFF_W1 + n * MLP_IN + k] : 0.f);
+        for (int k = 0; k < MLP_H; ++k)
+            M.w2[umma_kmajor_off(n, k, MLP_H) / 2] = bf16_bits(P[OFF_W2 + n * MLP_H + k]);
+        M.b1[n] = P[OFF_B1 + n];
+        M.b2[n] = P[OFF_B2 + n];
+        M.w3[n] = bf16_round(P[OFF_W3 + n]);
+    }
+    M.b3 = P[OFF_B3];
+}
+
+struct MlpTcSmem {
+    alignas(128) unsigned short a1[2][128 * 16];  // layer 1 A operands (features), tiles 0 and 1
+    alignas(128) unsigned short a2[2][128 * MLP_H];  // layer 2 A operands (tanh of layer 1)
+    alignas(128) MlpTcImage W;
+    unsigned long long bar;  // MMA completion
+    unsigned int tmem;       // TMEM base address from tcgen05.alloc
+};
+constexpr int MLP_TC_COLS = 64;  // TMEM columns: tile 0 accumulators 0..31, tile 1 32..63
+// With this footprint at most 8 CTAs fit on an SM (228 KB of shared memory,
+// 1 KB reserved per CTA), so their 64-column TMEM allocations (8 x 64 = 512
+// columns) never wait for one another.
+static_assert(9 * (sizeof(MlpTcSmem) + 1024) > 228 * 1024, "TMEM columns would be oversubscribed");
+
+// Shared-memory matrix descriptor: start address, leading (K) byte offset,
+// stride (8-row group) byte offset, descriptor version 1, no swizzle.
+__device__ __forceinline__ unsigned long long umma_desc(const void* p, unsigned lbo, unsigned sbo) {
+    return (unsigned long long)((smem_u32(p) & 0x3FFFFu) >> 4) | ((unsigned long long)(lbo >> 4) << 16) |
+           ((unsigned long long)(sbo >> 4) << 32) | (1ull << 46);
+}
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both
+// K-major, N = 32, M = 128.
+constexpr unsigned MLP_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(MLP_H >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ void umma_bf16(unsigned tmem_d, unsigned long long da, unsigned long long db, int acc) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(MLP_IDESC), "r"(acc)
+        : "memory");
+}
+__device__ __forceinline__ void umma_commit(unsigned long long* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+
+// 16 consecutive FP32 columns of this thread's TMEM lane (warp-collective)
+__device__ __forceinline__ void tmem_ld16(unsigned taddr, float (&v)[16]) {
+    unsigned r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr)
+        : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
+}
+
+// two FP32 values to packed BF16 (round to nearest even), lo in the low half
+__device__ __forceinline__ unsigned int pack2_rn(float lo, float hi) {
+    unsigned int r;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
+}
+
+// CTA set-up: weights into shared memory, the MMA barrier, and the TMEM
+// columns (allocated by warp 0, which also frees them in mlp_tc_teardown).
+__device__ __forceinline__ void mlp_tc_setup(MlpTcSmem& S, const MlpTcImage* __restrict__ Mg) {
+    const uint4* src = reinterpret_cast<const uint4*>(Mg);
+    uint4* dst = reinterpret_cast<uint4*>(&S.W);
+    for (int k = threadIdx.x; k < (int)(sizeof(MlpTcImage) / 16); k += blockDim.x) dst[k] = src[k];
+    if (threadIdx.x == 0) mbar_init(&S.bar);
+    if (threadIdx.x < 32) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem)),
+                     "r"(MLP_TC_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+}
+
+__device__ __forceinline__ void mlp_tc_teardown(MlpTcSmem& S) {
+    tc_fence_before();
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(S.tmem), "r"(MLP_TC_COLS)
+                     : "memory");
+    }
+}
+
+// Write this thread's 6 features as row t of layer 1's A operand of tile j.
+__device__ __forceinline__ void mlp_tc_put_features(MlpTcSmem& S, int j, const float (&f)[MLP_IN]) {
+    const int t = threadIdx.x;
+    uint4 lo, hi;
+    lo.x = pack2_rn(f[0], f[1]);
+    lo.y = pack2_rn(f[2], f[3]);
+    lo.z = pack2_rn(f[4], f[5]);
+    lo.w = 0u;
+    hi.x = hi.y = hi.z = hi.w = 0u;
+    unsigned char* base = reinterpret_cast<unsigned char*>(S.a1[j]);
+    *reinterpret_cast<uint4*>(base + umma_kmajor_off(t, 0, 16)) = lo;
+    *reinterpret_cast<uint4*>(base + umma_kmajor_off(t, 8, 16)) = hi;
+}
+
+// Wait for the phase `phase` of the MMA barrier (bounded); then TMEM reads may start.
+__device__ __forceinline__ void mlp_tc_wait(MlpTcSmem& S, unsigned& phase, int* status) {
+    if (!mbar_wait(&S.bar, phase & 1u) && status) atomicOr(status, 2);
+    ++phase;
+    tc_fence_after();
+}
+
+// The network for row t of both tiles (features already written with
+// mlp_tc_put_features by every thread).  All 128 threads call this together;
+// need0 / need1: this thread's row of tile 0 / 1 wants the output.  Rows are
+// independent in the products, so a warp none of whose rows of a tile want
+// it skips that tile's read-back and activations (its rows of the next
+// operand keep stale values, whose results nobody reads); its output is 0.
+__device__ __forceinline__ void mlp_tc_pair(MlpTcSmem& S, unsigned& phase, int* status, bool need0, bool need1,
+                                            float& out0, float& out1) {
+    const int t = threadIdx.x, w = t >> 5;
+    const unsigned tm = S.tmem;
+    const unsigned lane_base = (unsigned)(32 * w) << 16;
+    const bool wj[2] = {__any_sync(0xffffffffu, need0), __any_sync(0xffffffffu, need1)};
+    // layer 1: D_j = A1_j W1^T
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    if (t == 0) {
+        tc_fence_after();
+        const unsigned long long db = umma_desc(S.W.w1, 128, 16 * 16);
+#pragma unroll
+        for (int j = 0; j < 2; ++j) umma_bf16(tm + 32 * j, umma_desc(S.a1[j], 128, 16 * 16), db, 0);
+        umma_commit(&S.bar);
+    }
+    mlp_tc_wait(S, phase, status);
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        if (!wj[j]) continue;
+        unsigned char* base = reinterpret_cast<unsigned char*>(S.a2[j]);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            float d[16];
+            tmem_ld16(tm + lane_base + 32 * j + 16 * h, d);
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const int k0 = 16 * h + 8 * c;
+                uint4 v;
+                v.x = pack2_rn(tanh_fast(d[8 * c + 0] + S.W.b1[k0 + 0]), tanh_fast(d[8 * c + 1] + S.W.b1[k0 + 1]));
+                v.y = pack2_rn(tanh_fast(d[8 * c + 2] + S.W.b1[k0 + 2]), tanh_fast(d[8 * c + 3] + S.W.b1[k0 + 3]));
+                v.z = pack2_rn(tanh_fast(d[8 * c + 4] + S.W.b1[k0 + 4]), tanh_fast(d[8 * c + 5] + S.W.b1[k0 + 5]));
+                v.w = pack2_rn(tanh_fast(d[8 * c + 6] + S.W.b1[k0 + 6]), tanh_fast(d[8 * c + 7] + S.W.b1[k0 + 7]));
+                *reinterpret_cast<uint4*>(base + umma_kmajor_off(t, k0, MLP_H)) = v;
+            }
+        }
+    }
+    // layer 2: D_j = A2_j W2^T, two K = 16 steps (the K offset is two core matrices, 256 bytes)
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    if (t == 0) {
+        tc_fence_after();
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+            for (int kk = 0; kk < 2; ++kk)
+                umma_bf16(tm + 32 * j, umma_desc(reinterpret_cast<const unsigned char*>(S.a2[j]) + 256 * kk, 128, 16 * MLP_H),
+                          umma_desc(reinterpret_cast<const unsigned char*>(S.W.w2) + 256 * kk, 128, 16 * MLP_H), kk);
+        umma_commit(&S.bar);
+    }
+    mlp_tc_wait(S, phase, status);
+    float o[2] = {0.f, 0.f};
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        if (!wj[j]) continue;
+        float acc = S.W.b3;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            float d[16];
+            tmem_ld16(tm + lane_base + 32 * j + 16 * h, d);
+#pragma unroll
+            for (int k = 0; k < 16; k += 2) {
+                const unsigned int u =
+                    pack2_rn(tanh_fast(d[k] + S.W.b2[16 * h + k]), tanh_fast(d[k + 1] + S.W.b2[16 * h + k + 1]));
+                acc = fmaf(__uint_as_float(u << 16), S.W.w3[16 * h + k], acc);
+                acc = fmaf(__uint_as_float(u & 0xffff0000u), S.W.w3[16 * h + k + 1], acc);
+            }
+        }
+        o[j] = acc;
+    }
+    out0 = o[0];
+    out1 = o[1];
+    // the next pair's MMAs overwrite the accumulators and operands: every
+    // thread's reads are done before any thread passes the next barrier
+    tc_fence_before();
+}
+
+// Network outputs for n feature rows (x[i*8 + 0..5]) -- the raw evaluator
+// behind claw2_mlp_infer: 256 rows per tile pair, CTAs loop over the pairs.
+static __global__ void __launch_bounds__(128) k_mlp_eval_tc(const MlpTcImage* __restrict__ Mg,
+                                                            const float* __restrict__ x, int n, float* y,
+                                                            int* status) {
+    __shared__ MlpTcSmem S;
+    mlp_tc_setup(S, Mg);
+    unsigned phase = 0;
+    const int t = threadIdx.x;
+    const int npairs = (n + 255) / 256;
+    for (int pr = blockIdx.x; pr < npairs; pr += gridDim.x) {
+        const long long r0 = (long long)pr * 256 + t, r1 = r0 + 128;
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const long long r = j ? r1 : r0;
+            float f[MLP_IN];
+#pragma unroll
+            for (int c = 0; c < MLP_IN; ++c) f[c] = (r < n) ? x[r * 8 + c] : 0.f;
+            mlp_tc_put_features(S, j, f);
+        }
+        float o0, o1;
+        mlp_tc_pair(S, phase, status, r0 < n, r1 < n, o0, o1);
+        if (r0 < n) y[r0] = o0;
+        if (r1 < n) y[r1] = o1;
+    }
+    mlp_tc_teardown(S);
+}
+
+// exact_euler::features in FP32 for the inference pass (the features enter
+// the network as BF16, so FP32 arithmetic loses nothing that counts): a and
+// b are the (rho, u, v, p, c) of the cells left/below and right/above, dir 1
+// or 2 picks the normal velocity.  Non-finite features become 0; a
+// non-finite jump weight leaves the interface to the PVRS guess.
+__device__ __forceinline__ void features_f32(float g, const double (&a)[5], const double (&b)[5], int dir,
+                                             float (&x)[MLP_IN], float& w) {
+    const float rl = (float)a[0], ul = (float)a[dir], pl = (float)a[3];
+    const float rr = (float)b[0], ur = (float)b[dir], pr = (float)b[3];
+    const float rb = sqrtf(rl * rr), pb = sqrtf(pl * pr);
+    const float cb = sqrtf(__fdividef(g * pb, rb));
+    const float icb = __fdividef(1.f, cb);
+    const float lr = 0.5f * __logf(__fdividef(rl, rr)), lp = 0.5f * __logf(__fdividef(pl, pr));
+    x[0] = lr;
+    x[1] = -lr;
+    x[2] = ul * icb;
+    x[3] = ur * icb;
+    x[4] = lp;
+    x[5] = -lp;
+#pragma unroll
+    for (int k = 0; k < MLP_IN; ++k) x[k] = isfinite(x[k]) ? x[k] : 0.f;
+    const float dr = __fdividef(rr - rl, rb), dp = __fdividef(pr - pl, pb), du = (ur - ul) * icb;
+    const float j2 = dr * dr + dp * dp + du * du;
+    w = __fdividef(j2, 1.f + j2);
+}
+
+// Learned guesses for every interface of a grid (as k_mlp_guess, with the
+// network on tcgen05): thread (cp, R) of a 32 x 4 site tile computes the
+// x-interface (cp-1 | cp) on row R (tile 0, row t) and the y-interface
+// (R-1 | R) on column cp (tile 1, row t).  CTAs loop over the site tiles.
+static __global__ void __launch_bounds__(128, 5) k_mlp_guess_tc(const MlpTcImage* __restrict__ Mg,
+                                                             const double* __restrict__ q, Layout L, double gamma,
+                                                             double* guess, int* status) {
+    __shared__ MlpTcSmem S;
+    __shared__ double sprim[4][5][32];  // each warp's cells (rho, u, v, p, c): the row above's lower neighbours
+    mlp_tc_setup(S, Mg);
+    unsigned phase = 0;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tx = (L.mx + 4 + 31) / 32, ty = (L.my + 4 + 3) / 4;
+    const long long ntiles = (long long)tx * ty;
+    const exact_euler::Gas G = exact_euler::make_gas(gamma);
+    const double g1 = gamma - 1.0;
+    // primitive values and sound speed of one cell
+    auto prim = [&](int cc, int rr, double (&v)[5]) {
+        const long long o = (long long)rr * L.pitch + cc;
+        const double rho = q[o], irho = rcp_nr(rho);
+        v[0] = rho;
+        v[1] = q[L.plane + o] * irho;
+        v[2] = q[2 * L.plane + o] * irho;
+        v[3] = g1 * (q[3 * L.plane + o] - 0.5 * rho * (v[1] * v[1] + v[2] * v[2]));
+        v[4] = sqrt_nr(gamma * v[3] * irho);
+    };
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int cp = (int)(tile % tx) * 32 + lane;
+        const int R = (int)(tile / tx) * 4 + w;
+        const int c = min(cp, L.mx + 3), r = min(R, L.my + 3);
+        // this thread's cell; its left neighbour is the previous lane's cell
+        // and its lower neighbour the previous warp's (each computed once),
+        // except on the tile's first column and row
+        double me[5], lf[5], lo[5];
+        prim(c, r, me);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            lf[k] = __shfl_up_sync(0xffffffffu, me[k], 1);
+            sprim[w][k][lane] = me[k];
+        }
+        if (lane == 0) prim(max(c - 1, 0), r, lf);
+        __syncthreads();
+        if (w > 0) {
+#pragma unroll
+            for (int k = 0; k < 5; ++k) lo[k] = sprim[w - 1][k][lane];
+        } else {
+            prim(c, max(r - 1, 0), lo);
+        }
+        // features in FP32 (they enter the network as BF16)
+        float wxf, wyf;
+        float fx[MLP_IN], fy[MLP_IN];
+        features_f32((float)gamma, lf, me, 1, fx, wxf);
+        features_f32((float)gamma, lo, me, 2, fy, wyf);
+        // PVRS decides: a weak jump (w below MLP_WMIN) keeps the PVRS guess;
+        // a tile pair with only weak jumps skips the network
+        const bool sx = wxf >= (float)MLP_WMIN, sy = wyf >= (float)MLP_WMIN;
+        float ox = 0.f, oy = 0.f;
+        if (__syncthreads_or(sx || sy)) {
+            mlp_tc_put_features(S, 0, fx);
+            mlp_tc_put_features(S, 1, fy);
+            mlp_tc_pair(S, phase, status, sx, sy, ox, oy);
+        }
+        if (cp > L.mx + 3 || R > L.my + 3) continue;
+        const double gx0 = exact_euler::guess_pvrs(G, lf[0], lf[1], lf[3], lf[4], me[0], me[1], me[3], me[4]);
+        const double gy0 = exact_euler::guess_pvrs(G, lo[0], lo[2], lo[3], lo[4], me[0], me[2], me[3], me[4]);
+        const long long o = (long long)R * L.pitch + cp;
+        guess[o] = sx ? gx0 * (double)__expf(wxf * ox) : gx0;
+        guess[L.plane + o] = sy ? gy0 * (double)__expf(wyf * oy) : gy0;
+    }
+    mlp_tc_teardown(S);
 }
 
 // The converged pressures as guesses (a measurement aid, no network): thread

@@ -144,8 +144,9 @@ struct RPAcoustics {
         const double cc = p.c[2], zz = p.c[3];
         const double delta1 = cR[0] - cL[0];
         const double delta2 = cR[MU] - cL[MU];
-        const double a1 = (-delta1 + zz * delta2) / (2.0 * zz);
-        const double a2 = (delta1 + zz * delta2) / (2.0 * zz);
+        const double i2z = rcp_nr(2.0 * zz);
+        const double a1 = (-delta1 + zz * delta2) * i2z;
+        const double a2 = (delta1 + zz * delta2) * i2z;
         f.alpha[0] = a1;
         f.alpha[1] = a2;
         amdq[0] = -cc * (-a1 * zz); amdq[MU] = -cc * a1; amdq[MV] = 0.0;
@@ -156,8 +157,9 @@ struct RPAcoustics {
                                                 double (&bm)[MEQN], double (&bp)[MEQN]) {
         constexpr int MU = Dir<IXY>::MU, MV = Dir<IXY>::MV;
         const double cc = p.c[2], zz = p.c[3];
-        const double a1 = (-asdq[0] + zz * asdq[MV]) / (2.0 * zz);
-        const double a2 = (asdq[0] + zz * asdq[MV]) / (2.0 * zz);
+        const double i2z = rcp_nr(2.0 * zz);
+        const double a1 = (-asdq[0] + zz * asdq[MV]) * i2z;
+        const double a2 = (asdq[0] + zz * asdq[MV]) * i2z;
         bm[0] = cc * a1 * zz; bm[MU] = 0.0; bm[MV] = -cc * a1;
         bp[0] = cc * a2 * zz; bp[MU] = 0.0; bp[MV] = cc * a2;
     }
@@ -180,11 +182,11 @@ struct RPEulerRoe {
         const double u = q[1] * irho, v = q[2] * irho;
         const double pr = gamma1 * (q[3] - 0.5 * (q[1] * u + q[2] * v));
         c[0] = q[0]; c[1] = q[1]; c[2] = q[2]; c[3] = q[3];
-        c[RS] = sqrt(q[0]);
+        c[RS] = sqrt_nr(q[0]);
         c[UX] = u;
         c[UY] = v;
         c[HH] = (q[3] + pr) * irho;
-        c[CS] = sqrt(gamma * pr * irho);
+        c[CS] = sqrt_nr(gamma * pr * irho);
     }
     template <int IXY>
     __device__ __forceinline__ static void speeds(const Iface& f, const RPParams&, double (&s)[MWAVES]) {
@@ -272,9 +274,9 @@ struct RPEulerRoe {
                 const double en1 = cL[3] + w[0][3];
                 const double ir1 = rcp_nr(rho1);
                 const double p1 = gamma1 * (en1 - 0.5 * (rhou1 * rhou1 + rhov1 * rhov1) * ir1);
-                const double s1 = rhou1 * ir1 - sqrt(gamma * p1 * ir1);  // u - c right of the 1-wave
+                const double s1 = rhou1 * ir1 - sqrt_nr(gamma * p1 * ir1);  // u - c right of the 1-wave
                 double sfract;
-                if (s0 < 0.0 && s1 > 0.0) sfract = s0 * (s1 - s[0]) / (s1 - s0);
+                if (s0 < 0.0 && s1 > 0.0) sfract = s0 * (s1 - s[0]) * rcp_nr(s1 - s0);
                 else if (s[0] < 0.0) sfract = s[0];
                 else sfract = 0.0;
 #pragma unroll
@@ -291,10 +293,10 @@ struct RPEulerRoe {
             const double en2 = cR[3] - w[3][3];
             const double ir2 = rcp_nr(rho2);
             const double p2 = gamma1 * (en2 - 0.5 * (rhou2 * rhou2 + rhov2 * rhov2) * ir2);
-            const double s2 = rhou2 * ir2 + sqrt(gamma * p2 * ir2);  // u + c left of the 4-wave
+            const double s2 = rhou2 * ir2 + sqrt_nr(gamma * p2 * ir2);  // u + c left of the 4-wave
             double sfract = 0.0;
             bool add = true;
-            if (s2 < 0.0 && s3 > 0.0) sfract = s2 * (s3 - s[3]) / (s3 - s2);
+            if (s2 < 0.0 && s3 > 0.0) sfract = s2 * (s3 - s[3]) * rcp_nr(s3 - s2);
             else if (s[3] < 0.0) sfract = s[3];
             else add = false;
             if (add) {
@@ -515,10 +517,10 @@ struct RPShallowRoe {
         const double grav = p.c[0];
         const double ih = rcp_nr(q[0]);
         c[0] = q[0]; c[1] = q[1]; c[2] = q[2];
-        c[RS] = sqrt(q[0]);
+        c[RS] = sqrt_nr(q[0]);
         c[UX] = q[1] * ih;
         c[UY] = q[2] * ih;
-        c[CS] = sqrt(grav * q[0]);
+        c[CS] = sqrt_nr(grav * q[0]);
     }
     template <int IXY>
     __device__ __forceinline__ static void speeds(const Iface& f, const RPParams&, double (&s)[MWAVES]) {
@@ -590,9 +592,9 @@ struct RPShallowRoe {
             } else {
                 const double h1 = cL[0] + w[0][0];
                 const double hu1 = cL[MU] + w[0][MU];
-                const double s1 = hu1 / h1 - sqrt(grav * h1);  // speed just right of the 1-wave
+                const double s1 = hu1 * rcp_nr(h1) - sqrt_nr(grav * h1);  // speed just right of the 1-wave
                 double sfract;
-                if (s0 < 0.0 && s1 > 0.0) sfract = s0 * ((s1 - s[0]) / (s1 - s0));
+                if (s0 < 0.0 && s1 > 0.0) sfract = s0 * ((s1 - s[0]) * rcp_nr(s1 - s0));
                 else if (s[0] < 0.0) sfract = s[0];
                 else sfract = 0.0;
 #pragma unroll
@@ -605,10 +607,10 @@ struct RPShallowRoe {
             const double s03 = cR[UN] + cR[CS];
             const double h3 = cR[0] - w[2][0];
             const double hu3 = cR[MU] - w[2][MU];
-            const double s3 = hu3 / h3 + sqrt(grav * h3);  // speed just left of the 3-wave
+            const double s3 = hu3 * rcp_nr(h3) + sqrt_nr(grav * h3);  // speed just left of the 3-wave
             double sfract = 0.0;
             bool add = true;
-            if (s3 < 0.0 && s03 > 0.0) sfract = s3 * ((s03 - s[2]) / (s03 - s3));
+            if (s3 < 0.0 && s03 > 0.0) sfract = s3 * ((s03 - s[2]) * rcp_nr(s03 - s3));
             else if (s[2] < 0.0) sfract = s[2];
             else add = false;
             if (add) {

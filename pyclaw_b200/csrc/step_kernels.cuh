@@ -2176,9 +2176,20 @@ static __global__ void k_fp64_fma(double* out, int iters, double b) {
 
 // Self-test of rcp_nr: a = +-(1 + u) 2^e, e uniform in [-1000, 1000], u in
 // [0, 1) from a counter hash of (seed, i); the largest distance in units in
-// the last place between rcp_nr(a) and the IEEE quotient 1.0 / a.
+// the last place between rcp_nr(a) and the IEEE quotient 1.0 / a.  The first
+// threads also check the special values against the documented results
+// (+-0 -> +-inf, +-inf -> +-0, NaN -> NaN, a subnormal -> +inf, 1e308 ->
+// +0); a mismatch reports the largest distance there is.
 static __global__ void k_selftest_rcp(int n, unsigned long long seed, unsigned long long* worst) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < 7) {
+        const double inf = __longlong_as_double(0x7ff0000000000000ll);
+        const double in[7] = {0.0, -0.0, inf, -inf, __longlong_as_double(0x7ff8000000000000ll), 1e-310, 1e308};
+        const double want[7] = {inf, -inf, 0.0, -0.0, 0.0, inf, 0.0};
+        const double r = rcp_nr(in[i]);
+        const bool ok = (i == 4) ? (r != r) : (__double_as_longlong(r) == __double_as_longlong(want[i]));
+        if (!ok) atomicMax(worst, ~0ull);
+    }
     if (i >= n) return;
     unsigned long long z = seed ^ (0x9E3779B97F4A7C15ull * (unsigned long long)(i + 1));
     z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
@@ -2189,6 +2200,30 @@ static __global__ void k_selftest_rcp(int n, unsigned long long seed, unsigned l
     const double a = ((z >> 63) ? -1.0 : 1.0) * ldexp(1.0 + u, e);
     const double r = rcp_nr(a), q = 1.0 / a;
     const long long d = __double_as_longlong(r) - __double_as_longlong(q);
+    atomicMax(worst, (unsigned long long)(d < 0 ? -d : d));
+}
+
+// Self-test of sqrt_nr: x = (1 + u) 2^e as above (positive), the largest
+// distance in ulps from CUDA's IEEE sqrt(x); the first threads check +-0,
+// +inf, -1, NaN and a subnormal against the documented results.
+static __global__ void k_selftest_sqrt(int n, unsigned long long seed, unsigned long long* worst) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < 6) {
+        const double inf = __longlong_as_double(0x7ff0000000000000ll);
+        const double in[6] = {0.0, -0.0, inf, -1.0, __longlong_as_double(0x7ff8000000000000ll), 1e-310};
+        const double r = sqrt_nr(in[i]);
+        const bool ok = (i == 3 || i == 4) ? (r != r) : (__double_as_longlong(r) == __double_as_longlong(in[i]));
+        if (!ok) atomicMax(worst, ~0ull);
+    }
+    if (i >= n) return;
+    unsigned long long z = seed ^ (0x9E3779B97F4A7C15ull * (unsigned long long)(i + 1));
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    const double u = (double)(z >> 11) * (1.0 / 9007199254740992.0);
+    const int e = (int)((z & 2047ull) % 2001ull) - 1000;
+    const double x = ldexp(1.0 + u, e);
+    const long long d = __double_as_longlong(sqrt_nr(x)) - __double_as_longlong(sqrt(x));
     atomicMax(worst, (unsigned long long)(d < 0 ? -d : d));
 }
 

@@ -25,6 +25,7 @@ import numpy as np
 from . import _lib
 
 NPARAM = 1313
+MLP_TCGEN05, MLP_MMA_SYNC = 0, 1  # claw2_mlp_set_engine
 _fp = ctypes.POINTER(ctypes.c_float)
 
 
@@ -92,6 +93,12 @@ class Network(object):
         y = np.zeros(x8.shape[0], dtype=np.float32)
         _lib.check(self._lib.claw2_mlp_infer(self.h, _f(x8), x8.shape[0], _f(y)))
         return y
+
+    def set_engine(self, engine):
+        """Tensor-core path of the inference and the guess pass: "tcgen05"
+        (tcgen05.mma with TMEM accumulators, the default) or "mma.sync"."""
+        code = {"tcgen05": MLP_TCGEN05, "mma.sync": MLP_MMA_SYNC}[engine]
+        _lib.check(self._lib.claw2_mlp_set_engine(self.h, code))
 
 
 def attach(solver, net):

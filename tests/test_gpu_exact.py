@@ -101,16 +101,38 @@ def test_gradient_kernel_matches_fp64_reference():
     assert rel < 1e-4, rel
 
 
-def test_tensor_core_inference_matches_reference():
+@pytest.mark.parametrize("engine", ["tcgen05", "mma.sync"])
+@pytest.mark.parametrize("n", [1000, 256, 1, 70001])
+def test_tensor_core_inference_matches_reference(engine, n):
+    """BF16 operands, FP32 accumulation, on either tensor-core path: against
+    the same rounding in numpy and against the FP64 network.  The sizes cover
+    a partial tile pair, one row, and more tile pairs than resident CTAs."""
     net = learned.Network(seed=7)
+    net.set_engine(engine)
     rng = np.random.default_rng(1)
-    x = np.zeros((1000, 8), dtype=np.float32)
-    x[:, :6] = rng.normal(0, 1.0, (1000, 6))
+    x = np.zeros((n, 8), dtype=np.float32)
+    x[:, :6] = rng.normal(0, 1.0, (n, 6))
     y_gpu = net.infer(x)
     y_ref = mlp_ref.forward_bf16(net.params, x[:, :6])
     y_fp64, _, _ = mlp_ref.forward(net.params, x[:, :6].astype(np.float64))
     assert np.max(np.abs(y_gpu - y_ref)) < 2e-2
     assert np.max(np.abs(y_gpu - y_fp64)) < 5e-2
+
+
+def test_tcgen05_and_mma_sync_inference_agree():
+    """The two tensor-core paths round the same operands to BF16; they differ
+    only in the order of the FP32 sums and where the bias is added."""
+    net = learned.Network(seed=3)
+    rng = np.random.default_rng(2)
+    x = np.zeros((5000, 8), dtype=np.float32)
+    x[:, :6] = rng.normal(0, 1.5, (5000, 6))
+    ys = {}
+    for engine in ("tcgen05", "mma.sync"):
+        net.set_engine(engine)
+        ys[engine] = net.infer(x)
+        ys[engine + "2"] = net.infer(x)  # a second call on the same CTAs' barriers and TMEM
+    assert np.array_equal(ys["tcgen05"], ys["tcgen052"])
+    assert np.max(np.abs(ys["tcgen05"] - ys["mma.sync"])) < 5e-3
 
 
 def test_training_reduces_loss_and_guess_error():

@@ -139,15 +139,18 @@ def test_bc_fill_rejects_wall_on_single_cell():
         classic2.bc_fill(qbc, (3, 1), (3, 1))
 
 
-def test_kernel_reciprocal_within_one_ulp_of_ieee_division():
+@pytest.mark.parametrize("name", ["claw2_selftest_rcp", "claw2_selftest_sqrt"])
+def test_kernel_reciprocal_and_root_within_one_ulp_of_ieee(name):
     # the limiter ratio and the Roe solvers' reciprocal densities use a
-    # Newton-Raphson reciprocal; over 2^22 values spanning 2^-1000..2^1000 it
-    # stays within 1 ulp of CUDA's IEEE quotient
+    # Newton-Raphson reciprocal, their square roots a Goldschmidt iteration;
+    # over 2^22 values spanning 2^-1000..2^1000 each stays within 1 ulp of
+    # CUDA's IEEE quotient / square root, and the special values (zeros,
+    # infinities, NaN, subnormals) give the documented results
     import ctypes
     L = _lib.load()
     for seed in (1, 2024):
         ulp = ctypes.c_double(-1.0)
-        _lib.check(L.claw2_selftest_rcp(0, 1 << 22, seed, ctypes.byref(ulp)))
+        _lib.check(getattr(L, name)(0, 1 << 22, seed, ctypes.byref(ulp)))
         assert 0.0 <= ulp.value <= 1.0, ulp.value
 
 
