@@ -29,7 +29,42 @@
 #define EX_HD inline
 #endif
 
+#ifdef __CUDACC__
+#include "claw2_types.cuh"
+#endif
+
 namespace exact_euler {
+
+// Powers and square roots.  On the device x^y = exp(y ln x) (x > 0 wherever
+// the solver takes a power) and the branch-free claw2::sqrt_nr: CUDA's pow
+// handles every sign and integer case of its arguments in code that, inlined
+// at the Newton, fan and sampling sites, outgrew the instruction cache of the
+// step kernel (whose top stall was instruction fetch); the relative error of
+// exp(y ln x) is about |y ln x| ulps, 1e-14 at most for the pressure and
+// density ratios met here.  The host keeps the library functions.
+EX_HD double ex_pow(double x, double y) {
+#ifdef __CUDA_ARCH__
+    return exp(y * log(x));
+#else
+    return pow(x, y);
+#endif
+}
+EX_HD double ex_sqrt(double x) {
+#ifdef __CUDA_ARCH__
+    return claw2::sqrt_nr(x);
+#else
+    return sqrt(x);
+#endif
+}
+// 1/x: the branch-free claw2::rcp_nr on the device (quotients in the Newton
+// loop and the fan become products with it)
+EX_HD double ex_rcp(double x) {
+#ifdef __CUDA_ARCH__
+    return claw2::rcp_nr(x);
+#else
+    return 1.0 / x;
+#endif
+}
 
 struct Gas {
     double g, g1, g2, g3, g4, g5, g6, g7;  // gamma and Toro's constants G1..G7
@@ -51,16 +86,17 @@ EX_HD Gas make_gas(double gamma) {
 // f_K and f_K' at pressure p (Toro eqs. 4.6, 4.7, 4.37)
 EX_HD void prefun(const Gas& G, double p, double rk, double pk, double ck, double& f, double& fd) {
     if (p <= pk) {
-        const double prat = p / pk;
-        const double pw = pow(prat, G.g1);
+        const double prat = p * ex_rcp(pk);
+        const double pw = ex_pow(prat, G.g1);
         f = G.g4 * ck * (pw - 1.0);
-        fd = pw / (prat * rk * ck);  // (1/(rho c)) * prat^(-g2), with prat^(-g2) = prat^g1 / prat
+        fd = pw * ex_rcp(prat * rk * ck);  // (1/(rho c)) * prat^(-g2), with prat^(-g2) = prat^g1 / prat
     } else {
-        const double ak = G.g5 / rk;
+        const double ak = G.g5 * ex_rcp(rk);
         const double bk = G.g6 * pk;
-        const double qrt = sqrt(ak / (bk + p));
+        const double ibp = ex_rcp(bk + p);
+        const double qrt = ex_sqrt(ak * ibp);
         f = (p - pk) * qrt;
-        fd = (1.0 - 0.5 * (p - pk) / (bk + p)) * qrt;
+        fd = (1.0 - 0.5 * (p - pk) * ibp) * qrt;
     }
 }
 
@@ -76,14 +112,14 @@ EX_HD double guess_pvrs(const Gas& G, double rl, double ul, double pl, double cl
     const double qmax = pmax / pmin;
     if (qmax <= 2.0 && pmin <= ppv && ppv <= pmax) return ppv;
     if (ppv < pmin) {
-        const double pq = pow(pl / pr, G.g1);
+        const double pq = ex_pow(pl / pr, G.g1);
         const double um = (pq * ul / cl + ur / cr + G.g4 * (pq - 1.0)) / (pq / cl + 1.0 / cr);
         const double ptl = 1.0 + G.g7 * (ul - um) / cl;
         const double ptr = 1.0 + G.g7 * (um - ur) / cr;
-        return 0.5 * (pl * pow(ptl, G.g3) + pr * pow(ptr, G.g3));
+        return 0.5 * (pl * ex_pow(ptl, G.g3) + pr * ex_pow(ptr, G.g3));
     }
-    const double gel = sqrt((G.g5 / rl) / (G.g6 * pl + ppv));
-    const double ger = sqrt((G.g5 / rr) / (G.g6 * pr + ppv));
+    const double gel = ex_sqrt((G.g5 / rl) / (G.g6 * pl + ppv));
+    const double ger = ex_sqrt((G.g5 / rr) / (G.g6 * pr + ppv));
     return (gel * pl + ger * pr - (ur - ul)) / (gel + ger);
 }
 
@@ -109,7 +145,7 @@ EX_HD void star(const Gas& G, double rl, double ul, double pl, double cl, double
         double fld, frd;
         prefun(G, p, rl, pl, cl, fl, fld);
         prefun(G, p, rr, pr, cr, fr, frd);
-        const double step = (fl + fr + du) / (fld + frd);
+        const double step = (fl + fr + du) * ex_rcp(fld + frd);
         double pn = p - step;
         if (pn < 0.0) pn = tol;
         if (fabs(step) <= tol * p || k == maxit) {
@@ -139,24 +175,25 @@ struct Fan {
 EX_HD Fan fan(const Gas& G, double rl, double ul, double pl, double cl, double rr, double ur, double pr, double cr,
               double ps, double us) {
     Fan F;
+    // (exactly 1 for ps equal to the side's pressure, as a quotient would be:
+    // the record of two equal states stays the zero-jump shortcut's)
+    const double pml = (ps == pl) ? 1.0 : ps * ex_rcp(pl), pmr = (ps == pr) ? 1.0 : ps * ex_rcp(pr);
     if (ps > pl) {
-        const double pml = ps / pl;
-        F.rsl = rl * (pml + G.g6) / (pml * G.g6 + 1.0);
-        F.s1 = ul - cl * sqrt(G.g2 * pml + G.g1);
+        F.rsl = rl * (pml + G.g6) * ex_rcp(pml * G.g6 + 1.0);
+        F.s1 = ul - cl * ex_sqrt(G.g2 * pml + G.g1);
     } else {
-        const double pw = pow(ps / pl, 1.0 / G.g);
+        const double pw = ex_pow(pml, 1.0 / G.g);
         F.rsl = rl * pw;
-        const double cml = cl * pow(ps / pl, G.g1);
+        const double cml = cl * ex_pow(pml, G.g1);
         F.s1 = 0.5 * ((ul - cl) + (us - cml));
     }
     if (ps > pr) {
-        const double pmr = ps / pr;
-        F.rsr = rr * (pmr + G.g6) / (pmr * G.g6 + 1.0);
-        F.s3 = ur + cr * sqrt(G.g2 * pmr + G.g1);
+        F.rsr = rr * (pmr + G.g6) * ex_rcp(pmr * G.g6 + 1.0);
+        F.s3 = ur + cr * ex_sqrt(G.g2 * pmr + G.g1);
     } else {
-        const double pw = pow(ps / pr, 1.0 / G.g);
+        const double pw = ex_pow(pmr, 1.0 / G.g);
         F.rsr = rr * pw;
-        const double cmr = cr * pow(ps / pr, G.g1);
+        const double cmr = cr * ex_pow(pmr, G.g1);
         F.s3 = 0.5 * ((ur + cr) + (us + cmr));
     }
     return F;
@@ -171,35 +208,35 @@ EX_HD void sample0(const Gas& G, double rl, double ul, double pl, double cl, dou
         if (ps <= pl) {
             const double shl = ul - cl;
             if (s <= shl) { r = rl; u = ul; p = pl; return; }
-            const double cml = cl * pow(ps / pl, G.g1);
+            const double cml = cl * ex_pow(ps / pl, G.g1);
             const double stl = us - cml;
             if (s > stl) { r = F.rsl; u = us; p = ps; return; }
             u = G.g5 * (cl + G.g7 * ul + s);
             const double c = G.g5 * (cl + G.g7 * (ul - s));
-            r = rl * pow(c / cl, G.g4);
-            p = pl * pow(c / cl, G.g3);
+            r = rl * ex_pow(c / cl, G.g4);
+            p = pl * ex_pow(c / cl, G.g3);
         } else {
             const double pml = ps / pl;
-            const double sl = ul - cl * sqrt(G.g2 * pml + G.g1);
+            const double sl = ul - cl * ex_sqrt(G.g2 * pml + G.g1);
             if (s <= sl) { r = rl; u = ul; p = pl; }
             else { r = F.rsl; u = us; p = ps; }
         }
     } else {
         if (ps > pr) {
             const double pmr = ps / pr;
-            const double sr = ur + cr * sqrt(G.g2 * pmr + G.g1);
+            const double sr = ur + cr * ex_sqrt(G.g2 * pmr + G.g1);
             if (s >= sr) { r = rr; u = ur; p = pr; }
             else { r = F.rsr; u = us; p = ps; }
         } else {
             const double shr = ur + cr;
             if (s >= shr) { r = rr; u = ur; p = pr; return; }
-            const double cmr = cr * pow(ps / pr, G.g1);
+            const double cmr = cr * ex_pow(ps / pr, G.g1);
             const double str = us + cmr;
             if (s <= str) { r = F.rsr; u = us; p = ps; return; }
             u = G.g5 * (-cr + G.g7 * ur + s);
             const double c = G.g5 * (cr - G.g7 * (ur - s));
-            r = rr * pow(c / cr, G.g4);
-            p = pr * pow(c / cr, G.g3);
+            r = rr * ex_pow(c / cr, G.g4);
+            p = pr * ex_pow(c / cr, G.g3);
         }
     }
 }

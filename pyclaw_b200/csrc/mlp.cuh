@@ -584,7 +584,7 @@ __device__ __forceinline__ void mlp_tc_pair(MlpTcSmem& S, unsigned& phase, int* 
     const int t = threadIdx.x, w = t >> 5;
     const unsigned tm = S.tmem;
     const unsigned lane_base = (unsigned)(32 * w) << 16;
-    const bool wj[2] = {__any_sync(0xffffffffu, need0), __any_sync(0xffffffffu, need1)};
+    const bool wj[2] = {__any_sync(0xffffffffu, need0) != 0, __any_sync(0xffffffffu, need1) != 0};
     // layer 1: D_j = A1_j W1^T
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tc_fence_before();
@@ -818,11 +818,11 @@ static __global__ void __launch_bounds__(128) k_exact_pstar_guess(const double* 
     auto prim = [&](int cc, int rr, double& rho, double& u, double& v, double& p, double& c) {
         const long long o = (long long)rr * L.pitch + cc;
         rho = q[o];
-        const double irho = 1.0 / rho;
+        const double irho = rcp_nr(rho);
         u = q[L.plane + o] * irho;
         v = q[2 * L.plane + o] * irho;
         p = g1 * (q[3 * L.plane + o] - 0.5 * (q[L.plane + o] * u + q[2 * L.plane + o] * v));
-        c = sqrt(gamma * p * irho);
+        c = sqrt_nr(gamma * p * irho);
     };
     double r0, u0, v0, p0, c0, rl, ul, vl, pl, cl, rb, ub, vb, pb, cb;
     prim(cp, R, r0, u0, v0, p0, c0);

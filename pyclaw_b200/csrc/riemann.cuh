@@ -673,15 +673,16 @@ struct RPEulerExact {
 
     __device__ __forceinline__ static void prepare(const double (&q)[MEQN], const RPParams& p, double (&c)[NC]) {
         const double gamma = p.c[0], gamma1 = gamma - 1.0;
-        const double irho = 1.0 / q[0];
+        // (k_exact_pstar_guess forms these the same way)
+        const double irho = rcp_nr(q[0]);
         const double u = q[1] * irho, v = q[2] * irho;
         const double pr = gamma1 * (q[3] - 0.5 * (q[1] * u + q[2] * v));
         c[0] = q[0]; c[1] = q[1]; c[2] = q[2]; c[3] = q[3];
-        c[RS] = sqrt(q[0]);
+        c[RS] = sqrt_nr(q[0]);
         c[UX] = u;
         c[UY] = v;
         c[HH] = (q[3] + pr) * irho;
-        c[CS] = sqrt(gamma * pr * irho);
+        c[CS] = sqrt_nr(gamma * pr * irho);
         c[PP] = pr;
     }
     template <int IXY>

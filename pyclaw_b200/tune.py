@@ -11,7 +11,7 @@ import statistics
 
 from . import _lib
 
-ROWS = (2, 4, 8, 12, 16, 24, 32, 48, 64)
+ROWS = (2, 4, 8, 12, 14, 16, 18, 20, 24, 28, 32, 48, 64)
 VARIANTS = (0, 1, 2, 3, 4, 8)
 _cache = {}
 
