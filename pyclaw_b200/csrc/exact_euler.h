@@ -109,18 +109,19 @@ EX_HD double guess_pvrs(const Gas& G, double rl, double ul, double pl, double cl
     double ppv = 0.5 * (pl + pr) + 0.5 * (ul - ur) * cup;
     ppv = fmax(0.0, ppv);
     const double pmin = fmin(pl, pr), pmax = fmax(pl, pr);
-    const double qmax = pmax / pmin;
-    if (qmax <= 2.0 && pmin <= ppv && ppv <= pmax) return ppv;
+    // (the pressure ratio pmax / pmin <= 2, compared without the quotient)
+    if (pmax <= 2.0 * pmin && pmin <= ppv && ppv <= pmax) return ppv;
     if (ppv < pmin) {
-        const double pq = ex_pow(pl / pr, G.g1);
-        const double um = (pq * ul / cl + ur / cr + G.g4 * (pq - 1.0)) / (pq / cl + 1.0 / cr);
-        const double ptl = 1.0 + G.g7 * (ul - um) / cl;
-        const double ptr = 1.0 + G.g7 * (um - ur) / cr;
+        const double icl = ex_rcp(cl), icr = ex_rcp(cr);
+        const double pq = ex_pow(pl * ex_rcp(pr), G.g1);
+        const double um = (pq * ul * icl + ur * icr + G.g4 * (pq - 1.0)) * ex_rcp(pq * icl + icr);
+        const double ptl = 1.0 + G.g7 * (ul - um) * icl;
+        const double ptr = 1.0 + G.g7 * (um - ur) * icr;
         return 0.5 * (pl * ex_pow(ptl, G.g3) + pr * ex_pow(ptr, G.g3));
     }
-    const double gel = ex_sqrt((G.g5 / rl) / (G.g6 * pl + ppv));
-    const double ger = ex_sqrt((G.g5 / rr) / (G.g6 * pr + ppv));
-    return (gel * pl + ger * pr - (ur - ul)) / (gel + ger);
+    const double gel = ex_sqrt(G.g5 * ex_rcp(rl * (G.g6 * pl + ppv)));
+    const double ger = ex_sqrt(G.g5 * ex_rcp(rr * (G.g6 * pr + ppv)));
+    return (gel * pl + ger * pr - (ur - ul)) * ex_rcp(gel + ger);
 }
 
 // true if the data generate vacuum (Toro eq. 4.82)
@@ -169,7 +170,8 @@ EX_HD void star(const Gas& G, double rl, double ul, double pl, double cl, double
 // or the mean of head and tail speeds of a rarefaction).
 struct Fan {
     double rsl, rsr;  // rho*_L, rho*_R
-    double s1, s3;    // left / right acoustic wave speeds
+    double s1, s3;    // left / right acoustic wave speeds (the shock speed of a shock)
+    double cml, cmr;  // sound speeds behind a left / right rarefaction (0 for a shock)
 };
 
 EX_HD Fan fan(const Gas& G, double rl, double ul, double pl, double cl, double rr, double ur, double pr, double cr,
@@ -181,25 +183,28 @@ EX_HD Fan fan(const Gas& G, double rl, double ul, double pl, double cl, double r
     if (ps > pl) {
         F.rsl = rl * (pml + G.g6) * ex_rcp(pml * G.g6 + 1.0);
         F.s1 = ul - cl * ex_sqrt(G.g2 * pml + G.g1);
+        F.cml = 0.0;
     } else {
         const double pw = ex_pow(pml, 1.0 / G.g);
         F.rsl = rl * pw;
-        const double cml = cl * ex_pow(pml, G.g1);
-        F.s1 = 0.5 * ((ul - cl) + (us - cml));
+        F.cml = cl * ex_pow(pml, G.g1);
+        F.s1 = 0.5 * ((ul - cl) + (us - F.cml));
     }
     if (ps > pr) {
         F.rsr = rr * (pmr + G.g6) * ex_rcp(pmr * G.g6 + 1.0);
         F.s3 = ur + cr * ex_sqrt(G.g2 * pmr + G.g1);
+        F.cmr = 0.0;
     } else {
         const double pw = ex_pow(pmr, 1.0 / G.g);
         F.rsr = rr * pw;
-        const double cmr = cr * ex_pow(pmr, G.g1);
-        F.s3 = 0.5 * ((ur + cr) + (us + cmr));
+        F.cmr = cr * ex_pow(pmr, G.g1);
+        F.s3 = 0.5 * ((ur + cr) + (us + F.cmr));
     }
     return F;
 }
 
 // Sample at x/t = 0: returns (rho, u, p) and whether the point is left of the contact.
+// The shock speeds and the sound speeds behind the rarefactions are the fan's.
 EX_HD void sample0(const Gas& G, double rl, double ul, double pl, double cl, double rr, double ur, double pr, double cr,
                    double ps, double us, const Fan& F, double& r, double& u, double& p, bool& left) {
     const double s = 0.0;
@@ -208,35 +213,33 @@ EX_HD void sample0(const Gas& G, double rl, double ul, double pl, double cl, dou
         if (ps <= pl) {
             const double shl = ul - cl;
             if (s <= shl) { r = rl; u = ul; p = pl; return; }
-            const double cml = cl * ex_pow(ps / pl, G.g1);
-            const double stl = us - cml;
+            const double stl = us - F.cml;
             if (s > stl) { r = F.rsl; u = us; p = ps; return; }
             u = G.g5 * (cl + G.g7 * ul + s);
             const double c = G.g5 * (cl + G.g7 * (ul - s));
-            r = rl * ex_pow(c / cl, G.g4);
-            p = pl * ex_pow(c / cl, G.g3);
+            const double crat = c * ex_rcp(cl);
+            r = rl * ex_pow(crat, G.g4);
+            p = pl * ex_pow(crat, G.g3);
         } else {
-            const double pml = ps / pl;
-            const double sl = ul - cl * ex_sqrt(G.g2 * pml + G.g1);
+            const double sl = F.s1;
             if (s <= sl) { r = rl; u = ul; p = pl; }
             else { r = F.rsl; u = us; p = ps; }
         }
     } else {
         if (ps > pr) {
-            const double pmr = ps / pr;
-            const double sr = ur + cr * ex_sqrt(G.g2 * pmr + G.g1);
+            const double sr = F.s3;
             if (s >= sr) { r = rr; u = ur; p = pr; }
             else { r = F.rsr; u = us; p = ps; }
         } else {
             const double shr = ur + cr;
             if (s >= shr) { r = rr; u = ur; p = pr; return; }
-            const double cmr = cr * ex_pow(ps / pr, G.g1);
-            const double str = us + cmr;
+            const double str = us + F.cmr;
             if (s <= str) { r = F.rsr; u = us; p = ps; return; }
             u = G.g5 * (-cr + G.g7 * ur + s);
             const double c = G.g5 * (cr - G.g7 * (ur - s));
-            r = rr * ex_pow(c / cr, G.g4);
-            p = pr * ex_pow(c / cr, G.g3);
+            const double crat = c * ex_rcp(cr);
+            r = rr * ex_pow(crat, G.g4);
+            p = pr * ex_pow(crat, G.g3);
         }
     }
 }

@@ -726,7 +726,7 @@ struct RPEulerExact {
         const double tol = p.c[1];
         // Roe state for the transverse solver
         {
-            const double inv = 1.0 / (cL[RS] + cR[RS]);
+            const double inv = rcp_nr(cL[RS] + cR[RS]);
             const double wl = cL[RS] * inv, wr = cR[RS] * inv;
             f.u = wl * cL[UN] + wr * cR[UN];
             f.v = wl * cL[UT] + wr * cR[UT];
