@@ -372,7 +372,8 @@ def learned_workload(stream, flush, n=2048, steps=10, n_train=1 << 24, epochs=16
             tune.set_shape(pe.desc.riemann, *fixed_shape)
             shape = fixed_shape
         else:
-            shape, _ = tune.autotune(pe, dte)
+            pe.set_stream(stream.cuda_stream)
+            shape, _ = tune.autotune(pe, dte, before_step=flush.zero_)
         learned.newton_counts(ce.solver)
         step_ms, kern_ms = time_patch(pe, dte, steps, flush, stream)
         it, applied, ns = learned.newton_counts(ce.solver)
@@ -442,7 +443,7 @@ def secondary_workloads(stream, flush, peaks, only=None, shape=None):
             use = tuple(shape)
             tune.set_shape(p.desc.riemann, *use)
         else:
-            use, _ = tune.autotune(p, dt)
+            use, _ = tune.autotune(p, dt, before_step=flush.zero_)
         steps = 200 if name.startswith("shallow") else int(math.ceil(0.6 / dt))
         step_ms, kern_ms = time_patch(p, dt, steps, flush, stream)
         n = sol.state.grid.num_cells[0] * sol.state.grid.num_cells[1]
@@ -586,16 +587,16 @@ def run_ours(args):
     if slab:
         cfl = slabs.global_cfl(cfl, device=dev)
     dt = dt * 0.9 / cfl
-    # launch shape from the autotuner (trial steps are rejected: state unchanged)
+    # launch shape from the autotuner (trial steps are rejected: state unchanged),
+    # each trial after the same L2 flush as the timed steps
     from pyclaw_b200 import tune
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     if args.shape:
         shape, trials = tuple(int(x) for x in args.shape.split(",")), {}
         tune.set_shape(patch.desc.riemann, *shape)
     else:
-        shape, trials = tune.autotune(patch, dt)
+        shape, trials = tune.autotune(patch, dt, before_step=flush.zero_)
     patch.set_timing(True)
-
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     for _ in range(args.warmup):
         flush.zero_()
         if slab:

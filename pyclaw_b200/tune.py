@@ -26,9 +26,12 @@ def get_shape(rp_id):
     return v.value, r.value
 
 
-def autotune(patch, dt, reps=5, rows=ROWS, variants=VARIANTS):
+def autotune(patch, dt, reps=5, rows=ROWS, variants=VARIANTS, before_step=None):
     """Pick the fastest (variant, rows) for ``patch`` (a pyclaw_b200.device.DevicePatch)
-    at time step ``dt``; returns (best, {shape: median ms})."""
+    at time step ``dt``; returns (best, {shape: median ms}).  ``before_step``, if
+    given, is called before every trial step (e.g. a write that evicts the
+    state from L2, so the trials see the memory system the real steps see;
+    it must run on the patch's stream)."""
     d = patch.desc
     key = (d.riemann, d.mx, d.my)
     if key in _cache:
@@ -41,6 +44,8 @@ def autotune(patch, dt, reps=5, rows=ROWS, variants=VARIANTS):
             set_shape(d.riemann, v, r)
             times = []
             for _ in range(reps + 1):
+                if before_step is not None:
+                    before_step()
                 patch.step(dt, want_cfl=False)
                 patch.accept(False)
                 times.append(patch.kernel_ms())
