@@ -294,6 +294,10 @@ int claw2_selftest_rcp(int device, int n, unsigned long long seed, double* max_u
  * (no counterpart in the reference; Goldschmidt iteration from the hardware's
  * reciprocal square root): x = (1+u)*2^e, against CUDA's IEEE sqrt(x). */
 int claw2_selftest_sqrt(int device, int n, unsigned long long seed, double* max_ulp);
+/* The same for the reciprocal square root of the Roe averages (no counterpart
+ * in the reference; Newton steps from the hardware approximation), against
+ * CUDA's 1.0 / sqrt(x): two roundings there, so up to 2 ulps apart. */
+int claw2_selftest_rsqrt(int device, int n, unsigned long long seed, double* max_ulp);
 
 /* Self-test (no counterpart in the reference) of the longest-first tile
  * schedule's sort: n (1..8192) seeded tile costs with many ties, sorted on the

@@ -113,6 +113,7 @@ _SIGNATURES = {
     "claw2_probe_fp64": (ctypes.c_int, [ctypes.c_int, _c_double_p]),
     "claw2_selftest_rcp": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_ulonglong, _c_double_p]),
     "claw2_selftest_sqrt": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_ulonglong, _c_double_p]),
+    "claw2_selftest_rsqrt": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_ulonglong, _c_double_p]),
     "claw2_patch_launch_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]),
     "claw2_selftest_lpt": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_ulonglong,
                                           ctypes.POINTER(ctypes.c_int)]),

@@ -1989,20 +1989,36 @@ int claw2_selftest_rcp(int device, int n, unsigned long long seed, double* max_u
     return CLAW2_OK;
 }
 
-int claw2_selftest_sqrt(int device, int n, unsigned long long seed, double* max_ulp) {
+}  // extern "C"
+
+namespace {
+// one seeded self-test kernel over n values; *max_ulp = its largest distance
+int run_selftest(void (*kernel)(int, unsigned long long, unsigned long long*), const char* what, int device, int n,
+                 unsigned long long seed, double* max_ulp) {
     if (!max_ulp) return fail(CLAW2_EINVAL, "null pointer argument");
     if (n < 1) return fail(CLAW2_EINVAL, "n must be positive (got %d)", n);
     DeviceGuard g(device);
     unsigned long long* worst = nullptr;
     CUDA_TRY(cudaMalloc(&worst, sizeof(unsigned long long)));
     cudaMemset(worst, 0, sizeof(unsigned long long));
-    k_selftest_sqrt<<<(n + 255) / 256, 256>>>(n, seed, worst);
+    kernel<<<(n + 255) / 256, 256>>>(n, seed, worst);
     unsigned long long h = 0;
     cudaError_t e = cudaMemcpy(&h, worst, sizeof(h), cudaMemcpyDeviceToHost);
     cudaFree(worst);
-    if (e != cudaSuccess) return fail(CLAW2_ECUDA, "square-root self-test failed: %s", cudaGetErrorString(e));
+    if (e != cudaSuccess) return fail(CLAW2_ECUDA, "%s self-test failed: %s", what, cudaGetErrorString(e));
     *max_ulp = (double)h;
     return CLAW2_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int claw2_selftest_sqrt(int device, int n, unsigned long long seed, double* max_ulp) {
+    return run_selftest(k_selftest_sqrt, "square-root", device, n, seed, max_ulp);
+}
+
+int claw2_selftest_rsqrt(int device, int n, unsigned long long seed, double* max_ulp) {
+    return run_selftest(k_selftest_rsqrt, "reciprocal square-root", device, n, seed, max_ulp);
 }
 
 int claw2_selftest_lpt(int device, int n, unsigned long long seed, int* mismatches) {

@@ -81,4 +81,22 @@ __device__ __forceinline__ double sqrt_nr(double x) {
     return (g == g) ? g : (x >= 0.0 ? x : g);
 }
 
+// 1/sqrt(x) by two Newton steps y <- y + (y/2)(1 - x y^2) on Newton's method
+// for f(y) = 1/y^2 - x, from rsqrt.approx.ftz.f64 (the residual by one fused
+// multiply-add).  Within 2 ulps of the IEEE 1.0 / sqrt(x) (claw2_selftest_rsqrt).
+// No branch: +-0, +inf and NaN, whose residual is NaN, return the
+// approximation itself (+-inf, +0, NaN); subnormal arguments flush to +inf.
+// Used for the reciprocal sound speed of the Roe averages.
+__device__ __forceinline__ double rsqrt_nr(double x) {
+    double y0;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y0) : "d"(x));
+    double t = x * y0;
+    double e = fma(-t, y0, 1.0);
+    double y = fma(0.5 * y0, e, y0);
+    t = x * y;
+    e = fma(-t, y, 1.0);
+    y = fma(0.5 * y, e, y);
+    return (y == y) ? y : y0;
+}
+
 }  // namespace claw2

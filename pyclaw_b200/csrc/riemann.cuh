@@ -222,7 +222,7 @@ struct RPEulerRoe {
         const double v = __fma_rn(wl, cL[UT], __dmul_rn(wr, cR[UT]));
         const double H = __fma_rn(wl, cL[HH], __dmul_rn(wr, cR[HH]));
         const double a2 = __dmul_rn(gamma1, __fma_rn(-0.5, __fma_rn(u, u, __dmul_rn(v, v)), H));
-        const double ia = rsqrt(a2);
+        const double ia = rsqrt_nr(a2);
         f.u = u; f.v = v; f.H = H; f.a = __dmul_rn(a2, ia); f.ia = ia;
     }
     // The record of an interface whose two cells are equal: every strength is
@@ -548,7 +548,7 @@ struct RPShallowRoe {
         const double inv = rcp_nr(__dadd_rn(cL[RS], cR[RS]));
         const double wl = __dmul_rn(cL[RS], inv), wr = __dmul_rn(cR[RS], inv);
         const double gh = __dmul_rn(p.c[0], __dmul_rn(__dadd_rn(cL[0], cR[0]), 0.50));
-        const double ia = rsqrt(gh);
+        const double ia = rsqrt_nr(gh);
         f.u = __fma_rn(wl, cL[UN], __dmul_rn(wr, cR[UN]));
         f.v = __fma_rn(wl, cL[UT], __dmul_rn(wr, cR[UT]));
         f.a = __dmul_rn(gh, ia);
@@ -732,7 +732,7 @@ struct RPEulerExact {
             f.v = wl * cL[UT] + wr * cR[UT];
             f.H = wl * cL[HH] + wr * cR[HH];
             const double a2 = gamma1 * (f.H - 0.5 * (f.u * f.u + f.v * f.v));
-            f.ia = rsqrt(a2);
+            f.ia = rsqrt_nr(a2);
             f.a = a2 * f.ia;
         }
         const exact_euler::Gas G = exact_euler::make_gas(gamma);

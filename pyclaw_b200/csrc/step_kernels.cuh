@@ -2227,4 +2227,29 @@ static __global__ void k_selftest_sqrt(int n, unsigned long long seed, unsigned 
     atomicMax(worst, (unsigned long long)(d < 0 ? -d : d));
 }
 
+// Self-test of rsqrt_nr against the IEEE 1.0 / sqrt(x) (two roundings, so a
+// distance of up to 2 ulps is expected), same arguments; the first threads
+// check +-0, +inf, -1 and NaN against the documented results.
+static __global__ void k_selftest_rsqrt(int n, unsigned long long seed, unsigned long long* worst) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < 5) {
+        const double inf = __longlong_as_double(0x7ff0000000000000ll);
+        const double in[5] = {0.0, -0.0, inf, -1.0, __longlong_as_double(0x7ff8000000000000ll)};
+        const double want[5] = {inf, -inf, 0.0, 0.0, 0.0};
+        const double r = rsqrt_nr(in[i]);
+        const bool ok = (i >= 3) ? (r != r) : (__double_as_longlong(r) == __double_as_longlong(want[i]));
+        if (!ok) atomicMax(worst, ~0ull);
+    }
+    if (i >= n) return;
+    unsigned long long z = seed ^ (0x9E3779B97F4A7C15ull * (unsigned long long)(i + 1));
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    const double u = (double)(z >> 11) * (1.0 / 9007199254740992.0);
+    const int e = (int)((z & 2047ull) % 2001ull) - 1000;
+    const double x = ldexp(1.0 + u, e);
+    const long long d = __double_as_longlong(rsqrt_nr(x)) - __double_as_longlong(1.0 / sqrt(x));
+    atomicMax(worst, (unsigned long long)(d < 0 ? -d : d));
+}
+
 }  // namespace claw2

@@ -55,6 +55,7 @@ def test_bad_arguments_rejected_without_gpu(lib):
     rc = L.claw2_selftest_rcp(0, 100, 1, None)
     assert rc == _lib.EINVAL
     assert L.claw2_selftest_sqrt(0, 100, 1, None) == _lib.EINVAL
+    assert L.claw2_selftest_rsqrt(0, 100, 1, None) == _lib.EINVAL
     import ctypes
     bad = ctypes.c_int(-1)
     assert L.claw2_selftest_lpt(0, 10, 1, None) == _lib.EINVAL
