@@ -115,6 +115,64 @@ def test_step2ds_sweeps_zero_jump_shortcut(oracle, rp, ids, order, mthlim_kind):
     assert max_rel(q_g[:, 2:-2, rows], q_o[:, 2:-2, rows]) <= PARITY_RTOL
 
 
+@pytest.mark.parametrize("rp", sorted(RP_INFO))
+@pytest.mark.parametrize("variant,rows", [(0, 2), (0, 16), (1, 7), (2, 16), (3, 16), (3, 40), (4, 8)])
+def test_step2_piecewise_constant_tiles(oracle, rp, variant, rows):
+    # piecewise-constant quadrants with one noisy patch: most tiles read one
+    # state only (every warp of them takes the zero-jump shortcut), some
+    # straddle a quadrant edge or the patch; every launch shape, ragged last
+    # strip and row block
+    from pyclaw_b200 import tune
+    name, meqn, mwaves, cp = RP_INFO[rp]
+    mx, my = 300, 170
+    qbc = random_qbc(rp, mx, my, seed=11 * rp + variant, smooth_frac=0.0)
+    noisy = random_qbc(rp, mx, my, seed=5 * rp + 1, smooth_frac=1.0)
+    qbc[:, 40:60, 100:130] = noisy[:, 40:60, 100:130]
+    method = method_vector(2, 2)
+    mthlim = np.full(mwaves, 4, dtype=np.intc)
+    dx, dy = 1.0 / mx, 1.0 / my
+    dt = _dt_for(oracle, qbc, rp, cp, method, mthlim, dx, dy)
+    q_o = qbc.copy(order="F")
+    cfl_o = oracle.step2(qbc, q_o, dx, dy, dt, method, mthlim, rp, cp)
+    set_cparam(classic2, rp)
+    tune.set_shape(rp, variant, rows)
+    try:
+        q_g, cfl_g = classic2.step2(max(mx, my), 2, mx, my, qbc, qbc.copy(order="F"), None, dx, dy, dt, method,
+                                    mthlim, rpn2=rp)
+    finally:
+        tune.set_shape(rp, 0, 0)
+    assert abs(cfl_g - cfl_o) <= PARITY_RTOL * cfl_o
+    assert max_rel(q_g[:, 2:-2, 2:-2], q_o[:, 2:-2, 2:-2]) <= PARITY_RTOL
+
+
+@pytest.mark.parametrize("rp", sorted(RP_INFO))
+def test_step2_all_uniform_grid(oracle, rp):
+    # one state everywhere: every interface joins equal cells; the cells come
+    # back unchanged and the Courant number is the oracle's
+    from pyclaw_b200 import tune
+    name, meqn, mwaves, cp = RP_INFO[rp]
+    mx, my = 260, 90
+    base = random_qbc(rp, 4, 4, seed=rp, smooth_frac=0.0)
+    qbc = np.asfortranarray(np.broadcast_to(base[:, :1, :1], (meqn, mx + 4, my + 4)).copy())
+    method = method_vector(2, 2)
+    mthlim = np.full(mwaves, 4, dtype=np.intc)
+    dx, dy = 1.0 / mx, 1.0 / my
+    dt = 1e-4
+    q_o = qbc.copy(order="F")
+    cfl_o = oracle.step2(qbc, q_o, dx, dy, dt, method, mthlim, rp, cp)
+    set_cparam(classic2, rp)
+    for variant in (0, 3):
+        tune.set_shape(rp, variant, 16)
+        try:
+            q_g, cfl_g = classic2.step2(max(mx, my), 2, mx, my, qbc, qbc.copy(order="F"), None, dx, dy, dt,
+                                        method, mthlim, rpn2=rp)
+        finally:
+            tune.set_shape(rp, 0, 0)
+        assert abs(cfl_g - cfl_o) <= PARITY_RTOL * cfl_o
+        assert np.array_equal(q_g[:, 2:-2, 2:-2], qbc[:, 2:-2, 2:-2])
+        assert np.array_equal(q_o[:, 2:-2, 2:-2], qbc[:, 2:-2, 2:-2])
+
+
 @pytest.mark.parametrize("bcl,bcu", [((1, 1), (1, 1)), ((2, 2), (2, 2)), ((3, 3), (3, 3)), ((1, 3), (3, 1)),
                                      ((2, 1), (2, 3)), ((3, 2), (1, 2))])
 @pytest.mark.parametrize("mx,my", [(2, 2), (2, 3), (17, 29)])
