@@ -41,8 +41,17 @@ WORKLOAD = "euler_quadrants_roe_1024x1024_unsplit_trans_cor_mc"
 # One ncu capture of the step kernel on this workload (profiles/k_step_unsplit_euler_roe_1024.md):
 # dram__bytes_read.sum + dram__bytes_write.sum per launch, and the FP64 pipe's busy fraction.
 # The launch's 33.5 MB of output stays in L2 while it runs, so DRAM shows the reads only.
-NCU_TRAFFIC_BYTES = {1024: 34.282e6 + 0.733e6}
-NCU_FP64_PIPE_ACTIVE = {1024: 0.327}
+NCU_TRAFFIC_BYTES = {1024: 34.801e6 + 0.926e6}
+NCU_FP64_PIPE_ACTIVE = {1024: 0.435}
+
+
+def step_kernel_name(variant):
+    """The unsplit step kernel a launch variant runs (claw2_tune_set)."""
+    if variant == 8:
+        return "k_step_unsplit_ws<RPEulerRoe,128>"
+    if variant == 4:
+        return "k_step_unsplit2<RPEulerRoe,128>"
+    return "k_step_unsplit%s<RPEulerRoe,128,%d>" % ("_tma" if variant & 2 else "", 3 if variant & 1 else 2)
 
 
 def parse():
@@ -746,14 +755,17 @@ def run_ours(args):
                              "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch "
                                                "(profiles/k_step_unsplit_euler_roe_1024.md)",
                              "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_src,
-                             "kernel": "k_step_unsplit<RPEulerRoe,128>", "kernel_ms": kms,
+                             "kernel": "%s (launch variant %d, H = %d)" % (step_kernel_name(shape[0]), shape[0],
+                                                                           shape[1]),
+                             "kernel_ms": kms,
                              "algorithmic_bytes_per_launch": cells * BYTES_PER_CELL,
                              "fp64_probe_tflops": fp64.value,
                              "fp64_pipe_active_ncu": NCU_FP64_PIPE_ACTIVE.get(n),
-                             "note": "FP64-latency-bound kernel (8 warps/SM, dependency waits the top stall): "
-                                     "~870 FP64 instructions per developed cell-update cap it near 2.1e10 "
-                                     "cell-updates/s (21% of HBM) on this part; warps whose interfaces all have "
-                                     "equal cells on both sides (37% of this state's) skip the finish"},
+                             "note": "FP64-latency-bound kernel (10.8 warps/SM at the tuned 3-CTA shape, "
+                                     "dependency waits the top stall): ~870 FP64 instructions per developed "
+                                     "cell-update cap it near 2.1e10 cell-updates/s (21% of HBM) on this part; "
+                                     "warps whose interfaces all have equal cells on both sides (37% of this "
+                                     "state's) skip the finish"},
                 "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
                 "secondary": secondary,
                 "gpu_launches": int(launches1.value - launches0.value)}
