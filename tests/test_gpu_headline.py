@@ -70,7 +70,7 @@ def euler_1024_t04():
     return q
 
 
-SHAPES_1024 = [(0, 16), (1, 16), (4, 16), (0, 8), (8, 16), (8, 12)]
+SHAPES_1024 = [(3, 16), (2, 16), (3, 18), (0, 16), (1, 16), (4, 16), (0, 8), (8, 16), (8, 12)]
 
 
 @pytest.mark.parametrize("variant,rows", SHAPES_1024)
