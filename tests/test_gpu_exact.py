@@ -50,6 +50,29 @@ def test_exact_step_matches_oracle(oracle):
         assert max_rel(q_g[:, 2:-2, 2:-2], q_o[:, 2:-2, 2:-2]) <= PARITY_RTOL
 
 
+@pytest.mark.parametrize("variant,rows", [(2, 12), (3, 32), (1, 7), (8, 16)])
+def test_exact_step_matches_oracle_every_launch_shape(oracle, variant, rows):
+    # the shapes the autotuner picks for the exact solver (rows staged by TMA,
+    # 2 or 3 CTAs per SM) and the others, against the oracle
+    from pyclaw_b200 import tune
+    mx, my = 150, 97
+    qbc = _euler_qbc(mx, my, seed=variant + 3)
+    method = method_vector(2, 2)
+    mthlim = np.full(3, 4, dtype=np.intc)
+    dx, dy, dt = 1.0 / mx, 1.0 / my, 0.1 / max(mx, my)
+    q_o = qbc.copy(order="F")
+    cfl_o = oracle.step2(qbc, q_o, dx, dy, dt, method, mthlim, _lib.RP_EULER_EXACT, [G, 1e-12])
+    classic2.cparam.gamma = G
+    tune.set_shape(_lib.RP_EULER_EXACT, variant, rows)
+    try:
+        q_g, cfl_g = classic2.step2(max(mx, my), 2, mx, my, qbc, qbc.copy(order="F"), None, dx, dy, dt, method,
+                                    mthlim, rpn2=rmod.euler_exact_2D)
+    finally:
+        tune.set_shape(_lib.RP_EULER_EXACT, 0, 0)
+    assert abs(cfl_g - cfl_o) <= PARITY_RTOL * cfl_o
+    assert max_rel(q_g[:, 2:-2, 2:-2], q_o[:, 2:-2, 2:-2]) <= PARITY_RTOL
+
+
 def _exact_claw(n):
     claw = workloads.euler_quadrants_unsplit(n=n)
     claw.solver.rp = rmod.euler_exact_2D
