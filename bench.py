@@ -172,8 +172,9 @@ def measured_peaks():
 # ---------------------------------------------------------------------------
 # CPU legs (the oracle): single-thread baseline and the all-core reference arm
 # ---------------------------------------------------------------------------
-def cpu_rate(threads, budget_s, max_steps=None):
-    """cell-updates/s of the oracle's step2 on the benchmark workload."""
+def cpu_rate(threads, budget_s, max_steps=None, warmup=1):
+    """cell-updates/s of the oracle's step2 on the benchmark workload, after
+    `warmup` untimed steps (the first also sets dt near CFL 0.9)."""
     from oracle import pyoracle
     from pyclaw_b200 import workloads
     pyoracle.set_threads(threads)
@@ -183,6 +184,8 @@ def cpu_rate(threads, budget_s, max_steps=None):
     s.dt = 2.5e-4
     s.step_hyperbolic(sol)  # warm-up (also sets dt near CFL 0.9)
     s.dt = s.dt * 0.9 / max(s.cfl.get_cached_max(), 1e-12)
+    for _ in range(max(warmup, 1) - 1):
+        s.step_hyperbolic(sol)
     steps, t0 = 0, time.perf_counter()
     while True:
         s.step_hyperbolic(sol)
@@ -199,11 +202,12 @@ def run_reference(args):
         return 0
     ncores = len(os.sched_getaffinity(0))
     budget = max(5.0, min(120.0, 0.5 * args.steps))
-    value, steps, el = cpu_rate(ncores, budget, max_steps=args.steps)
+    warmup = max(args.warmup, 1)
+    value, steps, el = cpu_rate(ncores, budget, max_steps=args.steps, warmup=warmup)
     sample = ("%d full steps of the %dx%d workload (oracle step2 + host ghost fill), OpenMP over row "
               "colours, %.1f s" % (steps, N, N, el))
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
-            "warmup": 1, "ms_per_step": 1e3 * el / steps, "higher_is_better": True, "scaling": "weak",
+            "warmup": warmup, "ms_per_step": 1e3 * el / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
             "config": config({"reference": "C++ restatement of step2.f90/flux2.f90/limiter.f90/philim.f90 "
                                            "(oracle/claw_oracle.cpp); the reference Fortran needs gfortran, "
